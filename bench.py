@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Throughput of the texture-space (Mesh Colors) path-integration iteration.
+
+Workload: one TextureSpacePathTracer iteration over every surface texel of a
+seeded 200,688-triangle scene (313x313-vertex displaced terrain + 500 boxes
+with sides U[0.2, 3] and random yaw, albedo U[0.1, 0.9]); 16 texels/unit,
+per-triangle lattice resolution 4..64, 1 hemisphere sample per texel, 3
+bounces, sun at 45 deg with irradiance 3, constant sky 0.5. One step = one
+iteration (one kernel launch). Metric: Mrays/s, every closest-hit (extend)
+and any-hit (shadow) ray counted on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nan|reference]
+
+N > 1 runs under torchrun: each rank traces a contiguous 1/N range of the
+surface texels (no data-path collective; strong scaling of a fixed frame).
+``--impl reference`` times the reference's own CPU ray caster (tinybvh,
+vertex_baker/cpp/tinybvh_visibility.cpp, built from the reference sources
+into oracle/_ref/) on bounded samples of the same scene.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = ("texture-space Mesh Colors iteration: seeded 200,688-triangle terrain (313x313 grid, "
+            "height amplitude 2) + 500 boxes, 16 texels/unit, resolution 4-64, 1 sample/texel, 3 bounces")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["nan", "reference"], default="nan")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--grid", type=int, default=313)
+    ap.add_argument("--boxes", type=int, default=500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region.
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU caster (tinybvh) through ctypes.
+# ---------------------------------------------------------------------------
+def load_reference_caster():
+    for name in ("libvbake_bvh8.so", "libvbake_bvh.so"):
+        path = ROOT / "oracle" / "_ref" / name
+        if path.exists():
+            lib = ctypes.CDLL(str(path))
+            lib.vbake_tinybvh_has_bvh8_cpu.restype = ctypes.c_int
+            lib.vbake_pmr_visibility_sh_tinybvh.restype = ctypes.c_int
+            lib.vbake_last_error.restype = ctypes.c_char_p
+            layout = 1 if lib.vbake_tinybvh_has_bvh8_cpu() else 0
+            return lib, layout, name
+    return None, None, None
+
+
+def reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, max_distance):
+    vp = ctypes.c_void_p
+    out = np.zeros((sites.shape[0], 16), np.float32)
+    build_ms, trace_ms = ctypes.c_double(), ctypes.c_double()
+    visible, threads = ctypes.c_ulonglong(), ctypes.c_int()
+    rc = lib.vbake_pmr_visibility_sh_tinybvh(
+        ctypes.c_int(positions.shape[0]), ctypes.c_int(indices.shape[0]), vp(positions.ctypes.data),
+        vp(indices.ctypes.data), ctypes.c_int(sites.shape[0]), vp(sites.ctypes.data), vp(normals.ctypes.data),
+        ctypes.c_int(rays_per_site), ctypes.c_float(max_distance), ctypes.c_float(1e-3), ctypes.c_int(0),
+        ctypes.c_int(layout), vp(out.ctypes.data), ctypes.byref(build_ms), ctypes.byref(trace_ms),
+        ctypes.byref(visible), ctypes.byref(threads))
+    if rc != 0:
+        raise RuntimeError(lib.vbake_last_error().decode())
+    return trace_ms.value, build_ms.value, int(visible.value), int(threads.value)
+
+
+def flattened_geometry(node):
+    """World-space vertices/indices of every instance (the caster has no instancing)."""
+    pos, idx, base = [], [], 0
+    for mesh_id, _, transform_id in node.instances:
+        mesh = node.meshes[mesh_id]
+        m = node.transforms[transform_id].astype(np.float64)
+        p = mesh.vertices[:, 0:3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
+        pos.append(p.astype(np.float32))
+        idx.append(mesh.indices.astype(np.uint32) + base)
+        base += mesh.vertex_count
+    return np.ascontiguousarray(np.concatenate(pos)), np.ascontiguousarray(np.concatenate(idx))
+
+
+def cpu_baseline(node, seconds: float, rays_per_site: int = 512):
+    """Reference tinybvh caster on a bounded sample of surface sites of the same scene."""
+    from nan_b200 import scenes
+
+    lib, layout, name = load_reference_caster()
+    if lib is None:
+        return None
+    positions, indices = flattened_geometry(node)
+    probes, _ = scenes.surface_sites(node, 1024, seed=11, double_sided_backs=False)
+    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
+    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
+    trace_ms, _, _, threads = reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, 1000.0)
+    scale = max(1.0, seconds * 1000.0 / max(trace_ms, 1e-3))
+    count = int(min(1024 * scale, 2_000_000))
+    probes, _ = scenes.surface_sites(node, count, seed=12, double_sided_backs=False)
+    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
+    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
+    times = []
+    reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, 1000.0)  # warm-up
+    for _ in range(3):
+        t, build, visible, threads = reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site,
+                                                    1000.0)
+        times.append(t)
+    t = statistics.median(times)
+    rays = sites.shape[0] * rays_per_site
+    return {"value": rays / (t * 1e3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
+            "sample": f"tinybvh {'BVH8_CPU' if layout == 1 else 'BVH'} any-hit ({name}), {sites.shape[0]} surface "
+                      f"sites x {rays_per_site} rays on the same flattened scene, median of 3 runs "
+                      f"({t:.0f} ms each), build {build:.0f} ms, {os.cpu_count()} host cpus"}
+
+
+def roofline_bytes_per_ray(node, layout, lighting, sample_units: int = 6000):
+    """Algorithmic bytes per ray = 32 + 16 + 32*N_node + 36*N_tri, with the node
+    and triangle counts of the oracle's binned-SAH (8 bins) binary BVH on the
+    same texel paths (sampled)."""
+    from oracle.oracle import OracleScene
+
+    orc = OracleScene(**node.pack())
+    units = layout.units()
+    rng = np.random.default_rng(3)
+    pick = units[rng.choice(units.shape[0], size=min(sample_units, units.shape[0]), replace=False)]
+    slots = np.zeros((layout.total_payload_count, 4), np.uint32)
+    c = orc.trace_texels(lighting, slots, layout.face_array, layout.instance_array, layout.side_array, pick, 0, 1,
+                         3, True)
+    rays = c["extend_rays"] + c["shadow_rays"]
+    n_node = c["node_fetches"] / rays
+    n_tri = c["triangle_tests"] / rays
+    return 32.0 + 16.0 + 32.0 * n_node + 36.0 * n_tri, n_node, n_tri
+
+
+def measured_peak_gbs():
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    try:
+        data = json.loads((ROOT / "profiles" / "traffic.json").read_text())
+        return data.get("k_trace_texels_bytes_per_launch")
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from nan_b200 import scenes
+
+    node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
+    lib, layout, name = load_reference_caster()
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref caster library not built"}))
+        return
+    positions, indices = flattened_geometry(node)
+    probes, _ = scenes.surface_sites(node, 4096, seed=11, double_sided_backs=False)
+    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
+    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
+    for _ in range(max(args.warmup, 0)):
+        reference_cast(lib, layout, positions, indices, sites, normals, 512, 1000.0)
+    total_ms, threads = 0.0, 0
+    for _ in range(args.steps):
+        t, _, _, threads = reference_cast(lib, layout, positions, indices, sites, normals, 512, 1000.0)
+        total_ms += t
+    rays = args.steps * sites.shape[0] * 512
+    value = rays / (total_ms * 1e3)
+    line = {"impl": "reference", "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "reference_step": "any-hit sample"},
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
+                             "sample": f"tinybvh {'BVH8_CPU' if layout == 1 else 'BVH'} ({name}): "
+                                       f"{sites.shape[0]} surface sites x 512 rays per step"},
+            "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_nan(args):
+    import torch
+    import torch.distributed as dist
+
+    import nan_b200
+    from nan_b200 import scenes
+    from nan_b200.mesh_colors import MeshColorsLayout
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    device = nan_b200.Device(local)
+    node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
+    scene = nan_b200.Scene(device, node)
+    layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
+    tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
+    total = layout.total_surface_texels
+    begin, end = total * rank // world, total * (rank + 1) // world
+    slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
+    stream = torch.cuda.current_stream()
+
+    it = 0
+    for _ in range(args.warmup):
+        tracer.execute(stream, slots, it, reset=(it == 0), texel_range=(begin, end))
+        it += 1
+    torch.cuda.synchronize()
+    device.check()
+    device.context.read_counters(reset=True)
+    launches0 = device.context.launch_count
+
+    clocks = ClockSampler(local)
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        events[k][0].record(stream)
+        tracer.execute(stream, slots, it, texel_range=(begin, end))
+        events[k][1].record(stream)
+        it += 1
+    t1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    elapsed_ms = t0.elapsed_time(t1)
+    launch_ms = [a.elapsed_time(b) for a, b in events]
+    launches = device.context.launch_count - launches0
+    counters = device.context.read_counters(reset=True)
+    device.check()
+    rays_local = counters["extend_rays"] + counters["shadow_rays"]
+
+    # e2e through the public API with host buffers: pinned H2D of the slot
+    # buffer, the iteration, D2H of the updated slots, every step.
+    host_slots = torch.zeros_like(slots, device="cpu").pin_memory()
+    host_slots.copy_(slots)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(args.steps):
+        slots.copy_(host_slots, non_blocking=True)
+        tracer.execute(stream, slots, it, texel_range=(begin, end))
+        host_slots.copy_(slots, non_blocking=True)
+        it += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_counters = device.context.read_counters(reset=True)
+    e2e_rays_local = e2e_counters["extend_rays"] + e2e_counters["shadow_rays"]
+
+    stats = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device=device.torch_device)
+    sums = torch.tensor([float(rays_local), float(e2e_rays_local)], dtype=torch.float64, device=device.torch_device)
+    if world > 1:
+        dist.all_reduce(stats, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sums, op=dist.ReduceOp.SUM)
+    elapsed_ms, e2e_ms = float(stats[0]), float(stats[1])
+    rays_total, e2e_rays = float(sums[0]), float(sums[1])
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    value = rays_total / (elapsed_ms * 1e3)
+    bytes_per_ray, n_node, n_tri = roofline_bytes_per_ray(node, layout, scene.lighting)
+    avg_launch_s = statistics.mean(launch_ms) * 1e-3
+    rays_per_launch = rays_local / args.steps
+    achieved = rays_per_launch * bytes_per_ray / avg_launch_s / 1e9
+    peak, peak_kind = measured_peak_gbs()
+    traffic = ncu_traffic()
+    line = {
+        "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD, "triangles": scene.triangle_count, "surface_texels": total,
+            "payload_slots": layout.total_payload_count, "samples_per_texel": 1, "max_bounces": 3,
+            "parallelism": f"texel-range shards x{world}" if world > 1 else "single GPU",
+            "l2": f"slot buffer {layout.total_payload_count * 16 / 1e6:.0f} MB read-modify-written per step "
+                  "(> 126 MB L2)",
+        },
+        "rays_per_step": rays_total / args.steps,
+        "extend_rays_per_step": counters["extend_rays"] / args.steps,
+        "shadow_rays_per_step": counters["shadow_rays"] / args.steps,
+        "bvh_build_ms": scene.info()["build_ms"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "bytes_per_ray": bytes_per_ray, "nodes_per_ray": n_node, "tris_per_ray": n_tri,
+                     "peak_source": peak_kind},
+        "e2e": {"value": e2e_rays / (e2e_ms * 1e3), "unit": "Mrays/s",
+                "h2d_bytes_per_step": int(slots.numel() * 4), "d2h_bytes_per_step": int(slots.numel() * 4)},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_nan(args)
+
+
+if __name__ == "__main__":
+    main()

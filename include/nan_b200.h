@@ -1,0 +1,205 @@
+/* nan_b200.h -- C ABI of libnan_b200.so, the B200 (sm_100a) path-integration
+ * library: GPU BVH construction and traversal, Lambert path integration with
+ * sun next-event estimation, and irradiance accumulation into screen pixels,
+ * Mesh Colors texel slots and surface-probe sites.
+ *
+ * Conventions
+ *   - Every call returns an int status (NAN_OK == 0). On failure
+ *     nan_last_error() (thread-local) describes the error.
+ *   - Every buffer argument is a DEVICE pointer owned by the caller, except
+ *     the small parameter structs (NanLighting, NanCamera, NanSceneDesc,
+ *     NanMeshColorsDesc, ...), which are read from host memory during the
+ *     call. Record layouts are the reference's (4-byte little-endian words).
+ *   - Work is enqueued on the given cudaStream_t (passed as void*; NULL is
+ *     the legacy default stream). Calls return before the GPU finishes,
+ *     except where noted ("synchronises").
+ *   - Trace calls allocate nothing. nan_scene_build allocates the BVH it
+ *     owns inside the context.
+ *   - A context is not re-entrant from several host threads at once.
+ *
+ * The reference interfaces each call replaces are cited as path:line inside
+ * the reference project (WeakKnight/Nan).
+ */
+#ifndef NAN_B200_H
+#define NAN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NAN_B200_API __attribute__((visibility("default")))
+
+enum NanStatus {
+    NAN_OK = 0,
+    NAN_ERR_INVALID_ARGUMENT = 1,
+    NAN_ERR_OUT_OF_MEMORY = 2,
+    NAN_ERR_LIMIT = 3,       /* a device loop or stack cap was hit */
+    NAN_ERR_CUDA = 4,
+    NAN_ERR_NO_SCENE = 5,
+};
+
+typedef struct NanContext NanContext;
+
+/* Sun + sky lighting of the scene. Replaces Scene.bind()'s directional light
+ * and sky bindings (scene.py:1338-1382, scene.slang:6-17); the sky-view LUT
+ * (scene.slang:469-518) is reduced to a constant radiance and the sun
+ * transmittance LUT (scene.slang:997-1009) to a constant RGB factor. */
+typedef struct NanLighting {
+    float sun_direction[3];     /* unit vector toward the sun */
+    float sun_cos_half_angle;   /* cos of the sun disk's half apex angle */
+    float sun_color[3];
+    float sun_intensity;        /* outer-space illuminance = color * intensity */
+    float sun_transmittance[3]; /* ground-level factor (LUT stand-in) */
+    float ray_t_max;            /* t_max of bounce and shadow rays (Ray default 1000) */
+    float sky_radiance[3];      /* constant sky radiance on misses */
+    uint32_t flags;             /* bit 0: add the sun disk on primary misses */
+} NanLighting;
+
+/* Pinhole camera: the fields compute_ray_pinhole reads (camera.slang:173-236,
+ * bound by Camera.bind camera.py:98-115). */
+typedef struct NanCamera {
+    float position[3];
+    float jitter_x;
+    float image_u[3];
+    float jitter_y;
+    float image_v[3];
+    float near_clip;
+    float image_w[3];
+    float far_clip;
+} NanCamera;
+
+/* Scene buffers in the reference's layouts (scene.py:84-108, 386-436). */
+typedef struct NanSceneDesc {
+    const float* vertices;            /* f32[V][8]: position, normal, uv */
+    uint32_t vertex_count;
+    const uint32_t* indices;          /* u32[T][3], mesh-local */
+    uint32_t index_triangle_count;    /* T */
+    const uint32_t* mesh_descs;       /* u32[M][4]: vtx count, idx count, vtx off, idx off */
+    uint32_t mesh_count;
+    const uint32_t* instance_descs;   /* u32[I][4]: mesh, material, transform, flags */
+    uint32_t instance_count;
+    const float* transforms;          /* f32[X][16] row-major */
+    const float* inverse_transposes;  /* f32[X][16] */
+    uint32_t transform_count;
+    const float* materials;           /* f32[N][8]: base rgb, flags(u32), emissive rgb, pad */
+    uint32_t material_count;
+} NanSceneDesc;
+
+typedef struct NanSceneInfo {
+    uint32_t triangle_count;   /* world triangles after flattening instances */
+    uint32_t node_count;       /* BVH interior nodes */
+    uint32_t leaf_count;
+    uint32_t max_depth;
+    uint64_t device_bytes;     /* BVH + triangle storage owned by the context */
+    double build_ms;           /* device time of the last build */
+    double sah_cost;           /* SAH cost of the BVH (C_trav = C_int = 1) */
+} NanSceneInfo;
+
+/* Mesh Colors layout buffers (mesh_colors.py:82-119, 310-337). */
+typedef struct NanMeshColorsDesc {
+    const uint32_t* face_infos;      /* u32[F][2]: address, resolution */
+    uint32_t face_count;
+    const uint32_t* instance_infos;  /* u32[I][4]: face off, face count, texel off, texel count */
+    const uint32_t* side_infos;      /* u32[I][2]: back texel offset, flags */
+    uint32_t instance_count;
+    const uint32_t* surface_prefix;  /* u32[I+1]: exclusive prefix of texel_count */
+    uint32_t total_surface_texels;
+    uint32_t payload_count;          /* slots in the payload buffer */
+} NanMeshColorsDesc;
+
+/* Device-side counters accumulated by the trace calls. */
+typedef struct NanCounters {
+    uint64_t extend_rays;   /* closest-hit rays */
+    uint64_t shadow_rays;   /* any-hit rays */
+    uint64_t units;         /* pixels / texels / probes processed */
+    uint64_t paths;         /* light paths started */
+} NanCounters;
+
+NAN_B200_API const char* nan_last_error(void);
+NAN_B200_API int nan_version(void);
+
+/* Context: device ordinal, device status word and counters. */
+NAN_B200_API int nan_ctx_create(int device, NanContext** out_ctx);
+NAN_B200_API int nan_ctx_destroy(NanContext* ctx);
+/* Synchronises `stream`, then reads (and clears) the device status word.
+ * Returns NAN_ERR_LIMIT if a kernel hit its traversal-stack cap. */
+NAN_B200_API int nan_ctx_check(NanContext* ctx, void* stream);
+/* Synchronises `stream`, copies the counters, optionally zeroes them. */
+NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int reset,
+                                       void* stream);
+/* Number of kernels this context has launched. */
+NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx);
+
+/* Flatten the instances to world space and build the BVH on the GPU.
+ * Replaces Scene.__init__'s buffer packing + build_blas/build_tlas
+ * (scene.py:386-533). The scene buffers must stay alive and unchanged while
+ * the context traces them (shading reads them in place). Synchronises. */
+NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void* stream);
+NAN_B200_API int nan_scene_info(NanContext* ctx, NanSceneInfo* out);
+/* World triangles in flat (instance-major) order, f32[T][9]; out may be a
+ * device pointer of at least 36*T bytes. */
+NAN_B200_API int nan_scene_world_triangles(NanContext* ctx, float* out, void* stream);
+
+/* Closest hit per ray (Scene.intersect with t, scene.slang:1071-1124).
+ * rays f32[N][8]: origin, t_min, dir, t_max.
+ * hit_ids u32[N][4]: valid, instance, primitive, flat triangle index;
+ * hit_tb f32[N][3]: t, bary.x, bary.y. */
+NAN_B200_API int nan_intersect(NanContext* ctx, const float* rays, uint32_t count,
+                               uint32_t* hit_ids, float* hit_tb, void* stream);
+/* Any hit per ray: visibility 1.0 when nothing is hit in [t_min, t_max]
+ * (Scene.get_visibility, scene.slang:1126-1172). */
+NAN_B200_API int nan_occluded(NanContext* ctx, const float* rays, uint32_t count,
+                              float* visibility, void* stream);
+
+/* One 1-spp frame of the screen path tracer into out_rgba f32[H][W][4]
+ * (PathTracer.execute, path_tracer.py:21-40; path_tracer.slang:40-130).
+ * max_vertices is the reference's hard-coded 5 (path_tracer.slang:42). */
+NAN_B200_API int nan_trace_screen(NanContext* ctx, float* out_rgba, uint32_t width,
+                                  uint32_t height, uint32_t frame, uint32_t max_vertices,
+                                  const NanCamera* camera, const NanLighting* lighting,
+                                  void* stream);
+
+/* Running average of frames (Accumulator.execute, accumulator.py:32-58;
+ * accumulator.slang:9-19). All buffers f32[H][W][4]. */
+NAN_B200_API int nan_accumulate(NanContext* ctx, const float* input, float* output,
+                                float* history, uint32_t width, uint32_t height, int reset,
+                                void* stream);
+
+/* One iteration of the texture-space tracer over surface texels
+ * [texel_begin, texel_end) of the layout, all instances in ONE launch
+ * (TextureSpacePathTracer.execute, texture_space_path_tracer.py:33-58;
+ * texture_space_path_tracer.slang:57-216). slots u8[P][16]: RGB f32 + u32
+ * count, updated in place as a running mean. */
+NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layout,
+                                  uint8_t* slots, uint32_t iteration,
+                                  uint32_t samples_per_texel, uint32_t max_bounces, int reset,
+                                  const NanLighting* lighting, uint32_t texel_begin,
+                                  uint32_t texel_end, void* stream);
+
+/* One iteration of the surface-probe irradiance baker over probes
+ * [probe_begin, probe_end) (SurfaceProbeDiffuseIrradianceBaker.execute,
+ * surface_probe_path_tracer.py:49-83; surface_probe_path_tracer.slang:47-315).
+ * values f32[N][3], sample_counts u32[N], self_hits u32[N],
+ * radial u32[N][16] (RG16F moments), probes u8[N][48],
+ * probe_instances u8[I][48]. */
+NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* sample_counts,
+                                  uint32_t* self_hits, uint32_t* radial,
+                                  const uint8_t* probes, uint32_t probe_count,
+                                  const uint8_t* probe_instances,
+                                  uint32_t probe_instance_count, uint32_t iteration,
+                                  uint32_t samples_per_probe, uint32_t max_bounces, int reset,
+                                  const NanLighting* lighting, uint32_t probe_begin,
+                                  uint32_t probe_end, void* stream);
+
+/* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
+ * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */
+NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out,
+                                 uint32_t count, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NAN_B200_H */

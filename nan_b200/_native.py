@@ -1,0 +1,222 @@
+"""ctypes binding of libnan_b200.so (the C ABI in include/nan_b200.h).
+
+There is no fallback: importing a tracer class without the compiled library
+raises, so no CPU path can stand in for the CUDA kernels by accident.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("NAN_B200_LIBRARY", PKG / "libnan_b200.so"))
+
+NAN_OK = 0
+NAN_ERR_INVALID_ARGUMENT = 1
+NAN_ERR_OUT_OF_MEMORY = 2
+NAN_ERR_LIMIT = 3
+NAN_ERR_CUDA = 4
+NAN_ERR_NO_SCENE = 5
+
+_STATUS_NAMES = {
+    NAN_ERR_INVALID_ARGUMENT: "invalid argument",
+    NAN_ERR_OUT_OF_MEMORY: "out of memory",
+    NAN_ERR_LIMIT: "device limit hit",
+    NAN_ERR_CUDA: "CUDA error",
+    NAN_ERR_NO_SCENE: "no scene",
+}
+
+
+class NanError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class NanLighting(ctypes.Structure):
+    _fields_ = [
+        ("sun_direction", ctypes.c_float * 3),
+        ("sun_cos_half_angle", ctypes.c_float),
+        ("sun_color", ctypes.c_float * 3),
+        ("sun_intensity", ctypes.c_float),
+        ("sun_transmittance", ctypes.c_float * 3),
+        ("ray_t_max", ctypes.c_float),
+        ("sky_radiance", ctypes.c_float * 3),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+class NanCamera(ctypes.Structure):
+    _fields_ = [
+        ("position", ctypes.c_float * 3),
+        ("jitter_x", ctypes.c_float),
+        ("image_u", ctypes.c_float * 3),
+        ("jitter_y", ctypes.c_float),
+        ("image_v", ctypes.c_float * 3),
+        ("near_clip", ctypes.c_float),
+        ("image_w", ctypes.c_float * 3),
+        ("far_clip", ctypes.c_float),
+    ]
+
+
+class NanSceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("vertices", ctypes.c_void_p),
+        ("vertex_count", ctypes.c_uint32),
+        ("indices", ctypes.c_void_p),
+        ("index_triangle_count", ctypes.c_uint32),
+        ("mesh_descs", ctypes.c_void_p),
+        ("mesh_count", ctypes.c_uint32),
+        ("instance_descs", ctypes.c_void_p),
+        ("instance_count", ctypes.c_uint32),
+        ("transforms", ctypes.c_void_p),
+        ("inverse_transposes", ctypes.c_void_p),
+        ("transform_count", ctypes.c_uint32),
+        ("materials", ctypes.c_void_p),
+        ("material_count", ctypes.c_uint32),
+    ]
+
+
+class NanSceneInfo(ctypes.Structure):
+    _fields_ = [
+        ("triangle_count", ctypes.c_uint32),
+        ("node_count", ctypes.c_uint32),
+        ("leaf_count", ctypes.c_uint32),
+        ("max_depth", ctypes.c_uint32),
+        ("device_bytes", ctypes.c_uint64),
+        ("build_ms", ctypes.c_double),
+        ("sah_cost", ctypes.c_double),
+    ]
+
+
+class NanMeshColorsDesc(ctypes.Structure):
+    _fields_ = [
+        ("face_infos", ctypes.c_void_p),
+        ("face_count", ctypes.c_uint32),
+        ("instance_infos", ctypes.c_void_p),
+        ("side_infos", ctypes.c_void_p),
+        ("instance_count", ctypes.c_uint32),
+        ("surface_prefix", ctypes.c_void_p),
+        ("total_surface_texels", ctypes.c_uint32),
+        ("payload_count", ctypes.c_uint32),
+    ]
+
+
+class NanCounters(ctypes.Structure):
+    _fields_ = [
+        ("extend_rays", ctypes.c_uint64),
+        ("shadow_rays", ctypes.c_uint64),
+        ("units", ctypes.c_uint64),
+        ("paths", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+# (name, restype, argtypes) of every entry point declared in include/nan_b200.h.
+_VP, _U32, _I, _U64 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64
+EXPORTS = {
+    "nan_last_error": (ctypes.c_char_p, []),
+    "nan_version": (_I, []),
+    "nan_ctx_create": (_I, [_I, ctypes.POINTER(_VP)]),
+    "nan_ctx_destroy": (_I, [_VP]),
+    "nan_ctx_check": (_I, [_VP, _VP]),
+    "nan_ctx_read_counters": (_I, [_VP, ctypes.POINTER(NanCounters), _I, _VP]),
+    "nan_ctx_launch_count": (_U64, [_VP]),
+    "nan_scene_build": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP]),
+    "nan_scene_info": (_I, [_VP, ctypes.POINTER(NanSceneInfo)]),
+    "nan_scene_world_triangles": (_I, [_VP, _VP, _VP]),
+    "nan_intersect": (_I, [_VP, _VP, _U32, _VP, _VP, _VP]),
+    "nan_occluded": (_I, [_VP, _VP, _U32, _VP, _VP]),
+    "nan_trace_screen": (_I, [_VP, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
+                              ctypes.POINTER(NanLighting), _VP]),
+    "nan_accumulate": (_I, [_VP, _VP, _VP, _VP, _U32, _U32, _I, _VP]),
+    "nan_trace_texels": (_I, [_VP, ctypes.POINTER(NanMeshColorsDesc), _VP, _U32, _U32, _U32, _I,
+                              ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
+    "nan_trace_probes": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, _I,
+                              ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
+    "nan_pack_rgb9e5": (_I, [_VP, _VP, _VP, _U32, _VP]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libnan_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m nan_b200.build` "
+                "(there is no CPU fallback for the tracer)"
+            )
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, (restype, argtypes) in EXPORTS.items():
+            fn = getattr(handle, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = handle
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != NAN_OK:
+        message = lib().nan_last_error()
+        raise NanError(status, message.decode() if message else "")
+
+
+def stream_handle(command_encoder) -> int | None:
+    """Map the reference's command_encoder argument to a CUDA stream handle.
+
+    Accepts None (the current torch stream), a torch.cuda.Stream, or a raw
+    cudaStream_t integer.
+    """
+    import torch
+
+    if command_encoder is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(command_encoder, int):
+        return command_encoder
+    if hasattr(command_encoder, "cuda_stream"):
+        return command_encoder.cuda_stream
+    raise TypeError(f"cannot use {type(command_encoder).__name__} as a CUDA stream")
+
+
+def ptr(tensor) -> int:
+    return int(tensor.data_ptr()) if tensor is not None else 0
+
+
+class Context:
+    """Owns one NanContext (device status word, counters, BVH)."""
+
+    def __init__(self, device_index: int = 0):
+        handle = ctypes.c_void_p()
+        check(lib().nan_ctx_create(int(device_index), ctypes.byref(handle)))
+        self.handle = handle
+        self.device_index = int(device_index)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            lib().nan_ctx_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, stream=None) -> None:
+        check(lib().nan_ctx_check(self.handle, stream_handle(stream)))
+
+    def read_counters(self, reset: bool = False, stream=None) -> dict:
+        c = NanCounters()
+        check(lib().nan_ctx_read_counters(self.handle, ctypes.byref(c), int(reset), stream_handle(stream)))
+        return c.as_dict()
+
+    @property
+    def launch_count(self) -> int:
+        return int(lib().nan_ctx_launch_count(self.handle))

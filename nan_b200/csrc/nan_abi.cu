@@ -1,0 +1,256 @@
+// nan_abi.cu -- the extern "C" entry points declared in include/nan_b200.h.
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "nan_internal.h"
+
+namespace nan_host {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int cuda_fail(cudaError_t err, const char* what) {
+    if (err == cudaSuccess) return NAN_OK;
+    set_error(std::string(what) + ": " + cudaGetErrorString(err));
+    return err == cudaErrorMemoryAllocation ? NAN_ERR_OUT_OF_MEMORY : NAN_ERR_CUDA;
+}
+
+}  // namespace nan_host
+
+namespace {
+
+using nan_host::cuda_fail;
+using nan_host::set_error;
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+int invalid(const char* msg) {
+    set_error(msg);
+    return NAN_ERR_INVALID_ARGUMENT;
+}
+
+int enter(NanContext* ctx) {
+    if (!ctx) return invalid("null context");
+    const cudaError_t err = cudaSetDevice(ctx->device);
+    return cuda_fail(err, "cudaSetDevice");
+}
+
+int need_scene(NanContext* ctx) {
+    if (!ctx->has_scene) {
+        set_error("no scene has been built on this context");
+        return NAN_ERR_NO_SCENE;
+    }
+    return NAN_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
+
+}  // namespace
+
+extern "C" {
+
+NAN_B200_API const char* nan_last_error(void) { return nan_host::g_last_error.c_str(); }
+
+NAN_B200_API int nan_version(void) { return 1; }
+
+NAN_B200_API int nan_ctx_create(int device, NanContext** out_ctx) {
+    if (!out_ctx) return invalid("null output pointer");
+    *out_ctx = nullptr;
+    int count = 0;
+    cudaError_t err = cudaGetDeviceCount(&count);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaGetDeviceCount");
+    if (device < 0 || device >= count) return invalid("device ordinal out of range");
+    err = cudaSetDevice(device);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaSetDevice");
+    NanContext* ctx = new NanContext();
+    ctx->device = device;
+    if (cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&ctx->d_counters, sizeof(NanCounters)) != cudaSuccess) {
+        cudaFree(ctx->d_status);
+        cudaFree(ctx->d_counters);
+        delete ctx;
+        set_error("out of device memory for the context");
+        return NAN_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemset(ctx->d_status, 0, sizeof(uint32_t));
+    cudaMemset(ctx->d_counters, 0, sizeof(NanCounters));
+    err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) return cuda_fail(err, "context init");
+    *out_ctx = ctx;
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_ctx_destroy(NanContext* ctx) {
+    if (!ctx) return NAN_OK;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    nan_host::free_scene(ctx);
+    cudaFree(ctx->d_status);
+    cudaFree(ctx->d_counters);
+    delete ctx;
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_ctx_check(NanContext* ctx, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    uint32_t status = 0;
+    cudaError_t err = cudaMemcpyAsync(&status, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                      as_stream(stream));
+    if (err == cudaSuccess) err = cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), as_stream(stream));
+    if (err == cudaSuccess) err = cudaStreamSynchronize(as_stream(stream));
+    if (err != cudaSuccess) return cuda_fail(err, "status read");
+    if (status & 1u) {
+        set_error("a traversal stack overflowed (device status 1)");
+        return NAN_ERR_LIMIT;
+    }
+    if (status & 2u) {
+        set_error("a slot index fell outside the payload buffer (device status 2)");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int reset, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!out) return invalid("null counters pointer");
+    cudaError_t err = cudaMemcpyAsync(out, ctx->d_counters, sizeof(NanCounters), cudaMemcpyDeviceToHost,
+                                      as_stream(stream));
+    if (err == cudaSuccess && reset)
+        err = cudaMemsetAsync(ctx->d_counters, 0, sizeof(NanCounters), as_stream(stream));
+    if (err == cudaSuccess) err = cudaStreamSynchronize(as_stream(stream));
+    return cuda_fail(err, "counter read");
+}
+
+NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx) { return ctx ? ctx->launches : 0; }
+
+NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!desc) return invalid("null scene description");
+    if (desc->instance_count > 0 &&
+        (!desc->vertices || !desc->indices || !desc->mesh_descs || !desc->instance_descs || !desc->transforms ||
+         !desc->inverse_transposes || !desc->materials))
+        return invalid("null scene buffer");
+    if (desc->mesh_descs && !aligned16(desc->mesh_descs)) return invalid("mesh_descs must be 16-byte aligned");
+    if (desc->instance_descs && !aligned16(desc->instance_descs))
+        return invalid("instance_descs must be 16-byte aligned");
+    return nan_host::build_scene(ctx, desc, as_stream(stream));
+}
+
+NAN_B200_API int nan_scene_info(NanContext* ctx, NanSceneInfo* out) {
+    if (!ctx || !out) return invalid("null argument");
+    int rc = need_scene(ctx);
+    if (rc) return rc;
+    out->triangle_count = ctx->tri_count;
+    out->node_count = ctx->node_count;
+    out->leaf_count = ctx->leaf_count;
+    out->max_depth = ctx->max_depth;
+    out->device_bytes = ctx->device_bytes;
+    out->build_ms = ctx->build_ms;
+    out->sah_cost = ctx->sah_cost;
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_scene_world_triangles(NanContext* ctx, float* out, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (!out) return invalid("null output");
+    return nan_host::world_triangles(ctx, out, as_stream(stream));
+}
+
+NAN_B200_API int nan_intersect(NanContext* ctx, const float* rays, uint32_t count, uint32_t* hit_ids, float* hit_tb,
+                               void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (count && (!rays || !hit_ids || !hit_tb)) return invalid("null ray buffer");
+    if (count && (!aligned16(rays) || !aligned16(hit_ids))) return invalid("rays and hit_ids must be 16-byte aligned");
+    return nan_host::launch_intersect(ctx, rays, count, hit_ids, hit_tb, as_stream(stream));
+}
+
+NAN_B200_API int nan_occluded(NanContext* ctx, const float* rays, uint32_t count, float* visibility, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (count && (!rays || !visibility)) return invalid("null ray buffer");
+    if (count && !aligned16(rays)) return invalid("rays must be 16-byte aligned");
+    return nan_host::launch_occluded(ctx, rays, count, visibility, as_stream(stream));
+}
+
+NAN_B200_API int nan_trace_screen(NanContext* ctx, float* out_rgba, uint32_t width, uint32_t height, uint32_t frame,
+                                  uint32_t max_vertices, const NanCamera* camera, const NanLighting* lighting,
+                                  void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (!camera || !lighting) return invalid("null camera or lighting");
+    if ((width || height) && (!out_rgba || !aligned16(out_rgba))) return invalid("output must be 16-byte aligned");
+    if (max_vertices > 64) return invalid("max_vertices above 64");
+    return nan_host::launch_trace_screen(ctx, out_rgba, width, height, frame, max_vertices, camera, lighting,
+                                         as_stream(stream));
+}
+
+NAN_B200_API int nan_accumulate(NanContext* ctx, const float* input, float* output, float* history, uint32_t width,
+                                uint32_t height, int reset, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((width && height) && (!input || !output || !history)) return invalid("null image buffer");
+    if ((width && height) && (!aligned16(input) || !aligned16(output) || !aligned16(history)))
+        return invalid("image buffers must be 16-byte aligned");
+    return nan_host::launch_accumulate(ctx, input, output, history, width, height, reset, as_stream(stream));
+}
+
+NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layout, uint8_t* slots,
+                                  uint32_t iteration, uint32_t samples_per_texel, uint32_t max_bounces, int reset,
+                                  const NanLighting* lighting, uint32_t texel_begin, uint32_t texel_end,
+                                  void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (!layout || !lighting) return invalid("null layout or lighting");
+    if (layout->instance_count == 0) return invalid("layout has no instances");
+    if (!layout->face_infos || !layout->instance_infos || !layout->side_infos || !layout->surface_prefix || !slots)
+        return invalid("null layout buffer");
+    if (!aligned16(slots) || !aligned16(layout->instance_infos))
+        return invalid("slots and instance_infos must be 16-byte aligned");
+    if (texel_end > layout->total_surface_texels) return invalid("texel range beyond the layout");
+    if (max_bounces > 64) return invalid("max_bounces above 64");
+    return nan_host::launch_trace_texels(ctx, layout, slots, iteration, samples_per_texel, max_bounces, reset,
+                                         lighting, texel_begin, texel_end, as_stream(stream));
+}
+
+NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* sample_counts, uint32_t* self_hits,
+                                  uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                                  const uint8_t* probe_instances, uint32_t probe_instance_count,
+                                  uint32_t iteration, uint32_t samples_per_probe, uint32_t max_bounces, int reset,
+                                  const NanLighting* lighting, uint32_t probe_begin, uint32_t probe_end,
+                                  void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (!lighting) return invalid("null lighting");
+    if (probe_count && (!values || !sample_counts || !self_hits || !radial || !probes || !probe_instances))
+        return invalid("null probe buffer");
+    if (probe_count && (!aligned16(probes) || !aligned16(probe_instances)))
+        return invalid("probe records must be 16-byte aligned");
+    if (probe_end > probe_count) return invalid("probe range beyond probe_count");
+    if (max_bounces > 64) return invalid("max_bounces above 64");
+    return nan_host::launch_trace_probes(ctx, values, sample_counts, self_hits, radial, probes, probe_count,
+                                         probe_instances, probe_instance_count, iteration, samples_per_probe,
+                                         max_bounces, reset, lighting, probe_begin, probe_end, as_stream(stream));
+}
+
+NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (count && (!slots || !out)) return invalid("null buffer");
+    if (count && !aligned16(slots)) return invalid("slots must be 16-byte aligned");
+    return nan_host::launch_pack_rgb9e5(ctx, slots, out, count, as_stream(stream));
+}
+
+}  // extern "C"

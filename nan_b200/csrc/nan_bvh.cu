@@ -1,0 +1,468 @@
+// nan_bvh.cu -- GPU scene flattening and BVH construction.
+//
+// Replaces the reference's driver-built BLAS/TLAS (scene.py:445-533): the
+// instances are flattened into one world-space triangle array (each triangle
+// keeps its (instance, primitive) identity), and a binary BVH is built over
+// it entirely on the GPU:
+//   1. per-instance triangle counts + exclusive scan (CUB),
+//   2. flatten: transform every triangle to world space, write its box,
+//   3. scene bounds of the centroids (block reduction + ordered-int atomics),
+//   4. 63-bit Morton codes of the centroids, radix sort (CUB),
+//   5. hierarchy from the sorted codes (Karras 2012, "Maximizing parallelism
+//      in the construction of BVHs, octrees, and k-d trees"),
+//   6. bottom-up box refit with one atomic arrival counter per node,
+//   7. emission of 64-byte two-box nodes and leaf-ordered triangles.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "nan_internal.h"
+
+namespace {
+
+using nan_host::cuda_fail;
+using nan_host::set_error;
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ uint32_t float_to_ordered(float f) {
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void k_instance_counts(const uint4* __restrict__ instance_descs, const uint4* __restrict__ mesh_descs,
+                                  uint32_t instance_count, uint32_t* __restrict__ counts) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > instance_count) return;
+    if (i == instance_count) {
+        counts[i] = 0u;
+        return;
+    }
+    const uint4 id = instance_descs[i];
+    counts[i] = mesh_descs[id.x].y / 3u;
+}
+
+// mul(M, float4(p, 1)).xyz, unfused, left to right (the CPU oracle's order).
+__device__ __forceinline__ float3 xform(const float* __restrict__ m, float x, float y, float z) {
+    return make_float3(((m[0] * x + m[1] * y) + m[2] * z) + m[3], ((m[4] * x + m[5] * y) + m[6] * z) + m[7],
+                       ((m[8] * x + m[9] * y) + m[10] * z) + m[11]);
+}
+
+struct Bounds {
+    uint32_t lo[3];  // ordered ints
+    uint32_t hi[3];
+    uint32_t max_abs;
+};
+
+__global__ void k_flatten(NanSceneDesc sd, const uint32_t* __restrict__ offsets, uint32_t tri_count,
+                          float4* __restrict__ tris, uint2* __restrict__ refs, float4* __restrict__ box_lo,
+                          float4* __restrict__ box_hi, Bounds* __restrict__ bounds) {
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    float c[3] = {INFINITY, INFINITY, INFINITY};
+    float ch[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float mabs = 0.0f;
+    if (f < tri_count) {
+        // instance = last i with offsets[i] <= f
+        uint32_t lo = 0, hi = sd.instance_count;  // search in [0, I]
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (offsets[mid] <= f) lo = mid; else hi = mid - 1u;
+        }
+        const uint32_t inst = lo;
+        const uint32_t prim = f - offsets[inst];
+        const uint4 id = reinterpret_cast<const uint4*>(sd.instance_descs)[inst];
+        const uint4 md = reinterpret_cast<const uint4*>(sd.mesh_descs)[id.x];
+        const float* m = sd.transforms + 16u * id.z;
+        float3 w[3];
+        for (int k = 0; k < 3; ++k) {
+            const uint32_t vi = md.z + sd.indices[md.w + 3u * prim + (uint32_t)k];
+            const float* v = sd.vertices + 8u * vi;
+            w[k] = xform(m, v[0], v[1], v[2]);
+        }
+        tris[3u * f + 0] = make_float4(w[0].x, w[0].y, w[0].z, __uint_as_float(f));
+        tris[3u * f + 1] = make_float4(w[1].x, w[1].y, w[1].z, 0.0f);
+        tris[3u * f + 2] = make_float4(w[2].x, w[2].y, w[2].z, 0.0f);
+        refs[f] = make_uint2(inst, prim);
+        float3 l = make_float3(fminf(fminf(w[0].x, w[1].x), w[2].x), fminf(fminf(w[0].y, w[1].y), w[2].y),
+                               fminf(fminf(w[0].z, w[1].z), w[2].z));
+        float3 h = make_float3(fmaxf(fmaxf(w[0].x, w[1].x), w[2].x), fmaxf(fmaxf(w[0].y, w[1].y), w[2].y),
+                               fmaxf(fmaxf(w[0].z, w[1].z), w[2].z));
+        box_lo[f] = make_float4(l.x, l.y, l.z, 0.0f);
+        box_hi[f] = make_float4(h.x, h.y, h.z, 0.0f);
+        c[0] = ch[0] = 0.5f * (l.x + h.x);
+        c[1] = ch[1] = 0.5f * (l.y + h.y);
+        c[2] = ch[2] = 0.5f * (l.z + h.z);
+        mabs = fmaxf(fmaxf(fmaxf(fabsf(l.x), fabsf(h.x)), fmaxf(fabsf(l.y), fabsf(h.y))),
+                     fmaxf(fabsf(l.z), fabsf(h.z)));
+    }
+    typedef cub::BlockReduce<float, kThreads> Reduce;
+    __shared__ typename Reduce::TempStorage tmp;
+    for (int a = 0; a < 3; ++a) {
+        const float mn = Reduce(tmp).Reduce(c[a], cub::Min());
+        __syncthreads();
+        const float mx = Reduce(tmp).Reduce(ch[a], cub::Max());
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            atomicMin(&bounds->lo[a], float_to_ordered(mn));
+            atomicMax(&bounds->hi[a], float_to_ordered(mx));
+        }
+    }
+    const float ma = Reduce(tmp).Reduce(mabs, cub::Max());
+    if (threadIdx.x == 0) atomicMax(&bounds->max_abs, float_to_ordered(ma));
+}
+
+__device__ __forceinline__ uint64_t expand21(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void k_morton(const float4* __restrict__ box_lo, const float4* __restrict__ box_hi, uint32_t n,
+                         const Bounds* __restrict__ bounds, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 l = box_lo[i], h = box_hi[i];
+    const float c[3] = {0.5f * (l.x + h.x), 0.5f * (l.y + h.y), 0.5f * (l.z + h.z)};
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        const float lo = ordered_to_float(bounds->lo[a]);
+        const float hi = ordered_to_float(bounds->hi[a]);
+        const float ext = hi - lo;
+        float u = ext > 0.0f ? (c[a] - lo) / ext : 0.0f;
+        u = fminf(fmaxf(u, 0.0f), 1.0f);
+        q[a] = min((uint32_t)(u * 2097152.0f), 2097151u);
+    }
+    keys[i] = (expand21(q[0]) << 2) | (expand21(q[1]) << 1) | expand21(q[2]);
+    vals[i] = i;
+}
+
+__device__ __forceinline__ int delta(const uint64_t* __restrict__ k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = k[i], b = k[j];
+    if (a == b) return 64 + __clz((uint32_t)(i ^ j));
+    return __clzll((long long)(a ^ b));
+}
+
+// Interior node i of n-1; children < n-1 are interior, leaves are encoded as
+// ~leaf. parent arrays: interior parents (n-1) and leaf parents (n).
+__global__ void k_hierarchy(const uint64_t* __restrict__ keys, int n, int2* __restrict__ children,
+                            int* __restrict__ node_parent, int* __restrict__ leaf_parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(keys, n, i, j);
+    int s = 0, t = l;
+    do {
+        t = (t + 1) >> 1;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    const int gamma = i + s * d + min(d, 0);
+    const int left = (min(i, j) == gamma) ? ~gamma : gamma;
+    const int right = (max(i, j) == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    children[i] = make_int2(left, right);
+    if (left < 0) leaf_parent[~left] = i; else node_parent[left] = i;
+    if (right < 0) leaf_parent[~right] = i; else node_parent[right] = i;
+    if (i == 0) node_parent[0] = -1;
+}
+
+// Leaf-ordered triangles and boxes.
+__global__ void k_gather_leaves(const uint32_t* __restrict__ order, uint32_t n, const float4* __restrict__ tris_flat,
+                                const float4* __restrict__ lo_flat, const float4* __restrict__ hi_flat,
+                                float4* __restrict__ tris, float4* __restrict__ leaf_lo, float4* __restrict__ leaf_hi) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t f = order[i];
+    tris[3u * i + 0] = tris_flat[3u * f + 0];
+    tris[3u * i + 1] = tris_flat[3u * f + 1];
+    tris[3u * i + 2] = tris_flat[3u * f + 2];
+    leaf_lo[i] = lo_flat[f];
+    leaf_hi[i] = hi_flat[f];
+}
+
+__device__ __forceinline__ void child_box(int c, const float4* node_lo, const float4* node_hi, const float4* leaf_lo,
+                                          const float4* leaf_hi, float4* lo, float4* hi) {
+    if (c < 0) {
+        *lo = leaf_lo[~c];
+        *hi = leaf_hi[~c];
+    } else {
+        *lo = __ldcg(node_lo + c);
+        *hi = __ldcg(node_hi + c);
+    }
+}
+
+// Bottom-up refit: the second thread to reach a node computes its box.
+__global__ void k_refit(uint32_t n, const int2* __restrict__ children, const int* __restrict__ node_parent,
+                        const int* __restrict__ leaf_parent, const float4* __restrict__ leaf_lo,
+                        const float4* __restrict__ leaf_hi, float4* node_lo, float4* node_hi,
+                        uint32_t* __restrict__ arrivals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = leaf_parent[i];
+    while (p >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0u) return;
+        const int2 ch = children[p];
+        float4 al, ah, bl, bh;
+        child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
+        child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
+        __stcg(node_lo + p, make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f));
+        __stcg(node_hi + p, make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f));
+        p = node_parent[p];
+    }
+}
+
+// Depth of every leaf (steps to the root); max over leaves is the tree depth.
+__global__ void k_depth(uint32_t n, const int* __restrict__ node_parent, const int* __restrict__ leaf_parent,
+                        uint32_t* __restrict__ max_depth) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t depth = 1;
+    int p = leaf_parent[i];
+    while (p >= 0 && depth < 4096u) {
+        ++depth;
+        p = node_parent[p];
+    }
+    atomicMax(max_depth, depth);
+}
+
+__device__ __forceinline__ float half_area(float4 l, float4 h) {
+    const float x = h.x - l.x, y = h.y - l.y, z = h.z - l.z;
+    return x * y + y * z + z * x;
+}
+
+// 64-byte nodes with padded child boxes; also accumulates the SAH cost.
+__global__ void k_emit(uint32_t interior, const int2* __restrict__ children, const float4* __restrict__ node_lo,
+                       const float4* __restrict__ node_hi, const float4* __restrict__ leaf_lo,
+                       const float4* __restrict__ leaf_hi, const Bounds* __restrict__ bounds,
+                       float4* __restrict__ nodes, double* __restrict__ sah) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= interior) return;
+    const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;  // 2^-18 relative
+    const int2 ch = children[i];
+    float4 al, ah, bl, bh;
+    child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
+    child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
+    nodes[4u * i + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
+    nodes[4u * i + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
+    nodes[4u * i + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
+    nodes[4u * i + 3] = make_float4(__int_as_float(ch.x), __int_as_float(ch.y), 0.0f, 0.0f);
+    const float root_area = fmaxf(half_area(node_lo[0], node_hi[0]), 1e-30f);
+    double cost = (double)(half_area(node_lo[i], node_hi[i]) / root_area);  // one traversal step
+    if (ch.x < 0) cost += (double)(half_area(al, ah) / root_area);          // one triangle per leaf
+    if (ch.y < 0) cost += (double)(half_area(bl, bh) / root_area);
+    atomicAdd(sah, cost);
+}
+
+template <class T> T* dmalloc(size_t count, cudaStream_t s, cudaError_t* err) {
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
+    if (e != cudaSuccess && *err == cudaSuccess) *err = e;
+    return static_cast<T*>(p);
+}
+
+uint32_t blocks(uint64_t n) { return (uint32_t)((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+
+namespace nan_host {
+
+void free_scene(NanContext* ctx) {
+    cudaFree(ctx->nodes);
+    cudaFree(ctx->tris);
+    cudaFree(ctx->tri_refs);
+    ctx->nodes = nullptr;
+    ctx->tris = nullptr;
+    ctx->tri_refs = nullptr;
+    ctx->has_scene = false;
+    ctx->tri_count = ctx->node_count = ctx->leaf_count = ctx->max_depth = 0;
+    ctx->device_bytes = 0;
+}
+
+int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    free_scene(ctx);
+    ctx->scene = *sd;
+    const uint32_t I = sd->instance_count;
+
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, s);
+
+    // 1. flat offsets
+    uint32_t* counts = dmalloc<uint32_t>(I + 1, s, &err);
+    uint32_t* offsets = dmalloc<uint32_t>(I + 1, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "scene build allocation");
+    k_instance_counts<<<blocks(I + 1), kThreads, 0, s>>>(reinterpret_cast<const uint4*>(sd->instance_descs),
+                                                         reinterpret_cast<const uint4*>(sd->mesh_descs), I, counts);
+    ctx->launches++;
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, offsets, I + 1, s);
+    void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, I + 1, s);
+    ctx->launches++;
+    uint32_t total = 0;
+    err = cudaMemcpyAsync(&total, offsets + I, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "scene build (triangle count)");
+    cudaFreeAsync(scan_tmp, s);
+    cudaFreeAsync(counts, s);
+    if (total > (1u << 30)) {
+        cudaFreeAsync(offsets, s);
+        set_error("scene has more than 2^30 triangles");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    const uint32_t n = total;
+    ctx->tri_count = n;
+
+    // Persistent storage.
+    const uint32_t interior = n > 1 ? n - 1 : 0;
+    if (cudaMalloc(&ctx->tris, std::max<size_t>(n, 1) * 3 * sizeof(float4)) != cudaSuccess ||
+        cudaMalloc(&ctx->tri_refs, std::max<size_t>(n, 1) * sizeof(uint2)) != cudaSuccess ||
+        cudaMalloc(&ctx->nodes, std::max<size_t>(interior, 1) * 4 * sizeof(float4)) != cudaSuccess) {
+        cudaFreeAsync(offsets, s);
+        free_scene(ctx);
+        set_error("out of device memory for the BVH");
+        return NAN_ERR_OUT_OF_MEMORY;
+    }
+    ctx->device_bytes = (uint64_t)n * 3 * sizeof(float4) + (uint64_t)n * sizeof(uint2) +
+                        (uint64_t)std::max<uint32_t>(interior, 1) * 4 * sizeof(float4);
+
+    if (n == 0) {
+        cudaFreeAsync(offsets, s);
+        ctx->has_scene = true;
+        ctx->root = 0;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        return NAN_OK;
+    }
+
+    // Scratch.
+    float4* tris_flat = dmalloc<float4>(3ull * n, s, &err);
+    float4* lo_flat = dmalloc<float4>(n, s, &err);
+    float4* hi_flat = dmalloc<float4>(n, s, &err);
+    Bounds* bounds = dmalloc<Bounds>(1, s, &err);
+    uint64_t* keys = dmalloc<uint64_t>(n, s, &err);
+    uint64_t* keys_sorted = dmalloc<uint64_t>(n, s, &err);
+    uint32_t* vals = dmalloc<uint32_t>(n, s, &err);
+    uint32_t* order = dmalloc<uint32_t>(n, s, &err);
+    float4* leaf_lo = dmalloc<float4>(n, s, &err);
+    float4* leaf_hi = dmalloc<float4>(n, s, &err);
+    int2* children = dmalloc<int2>(std::max<uint32_t>(interior, 1), s, &err);
+    int* node_parent = dmalloc<int>(std::max<uint32_t>(interior, 1), s, &err);
+    int* leaf_parent = dmalloc<int>(n, s, &err);
+    float4* node_lo = dmalloc<float4>(std::max<uint32_t>(interior, 1), s, &err);
+    float4* node_hi = dmalloc<float4>(std::max<uint32_t>(interior, 1), s, &err);
+    uint32_t* arrivals = dmalloc<uint32_t>(std::max<uint32_t>(interior, 1), s, &err);
+    uint32_t* depth = dmalloc<uint32_t>(1, s, &err);
+    double* sah = dmalloc<double>(1, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "scene build scratch allocation");
+
+    Bounds init;
+    for (int a = 0; a < 3; ++a) {
+        init.lo[a] = 0xffffffffu;
+        init.hi[a] = 0u;
+    }
+    init.max_abs = 0u;
+    cudaMemcpyAsync(bounds, &init, sizeof(Bounds), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(arrivals, 0, std::max<uint32_t>(interior, 1) * sizeof(uint32_t), s);
+    cudaMemsetAsync(depth, 0, sizeof(uint32_t), s);
+    cudaMemsetAsync(sah, 0, sizeof(double), s);
+
+    // 2-3. flatten + bounds
+    k_flatten<<<blocks(n), kThreads, 0, s>>>(*sd, offsets, n, tris_flat, ctx->tri_refs, lo_flat, hi_flat, bounds);
+    // 4. Morton codes + sort
+    k_morton<<<blocks(n), kThreads, 0, s>>>(lo_flat, hi_flat, n, bounds, keys, vals);
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
+    void* sort_tmp = dmalloc<uint8_t>(sort_bytes, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "scene build sort allocation");
+    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
+    k_gather_leaves<<<blocks(n), kThreads, 0, s>>>(order, n, tris_flat, lo_flat, hi_flat, ctx->tris, leaf_lo, leaf_hi);
+    ctx->launches += 4;
+    if (n == 1) {
+        ctx->root = ~0;
+        ctx->node_count = 0;
+        ctx->leaf_count = 1;
+        ctx->max_depth = 1;
+        ctx->sah_cost = 1.0;
+    } else {
+        // 5-7. hierarchy, refit, depth, emit
+        k_hierarchy<<<blocks(interior), kThreads, 0, s>>>(keys_sorted, (int)n, children, node_parent, leaf_parent);
+        k_refit<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, leaf_lo, leaf_hi, node_lo,
+                                               node_hi, arrivals);
+        k_depth<<<blocks(n), kThreads, 0, s>>>(n, node_parent, leaf_parent, depth);
+        k_emit<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_lo, node_hi, leaf_lo, leaf_hi, bounds,
+                                                     ctx->nodes, sah);
+        ctx->launches += 4;
+        ctx->root = 0;
+        ctx->node_count = interior;
+        ctx->leaf_count = n;
+        uint32_t max_depth = 0;
+        double sah_host = 0.0;
+        cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+        err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_fail(err, "scene build");
+        ctx->max_depth = max_depth;
+        ctx->sah_cost = sah_host;
+    }
+    cudaEventRecord(ev1, s);
+    for (void* p : {(void*)offsets, (void*)tris_flat, (void*)lo_flat, (void*)hi_flat, (void*)bounds, (void*)keys,
+                    (void*)keys_sorted, (void*)vals, (void*)order, (void*)leaf_lo, (void*)leaf_hi, (void*)children,
+                    (void*)node_parent, (void*)leaf_parent, (void*)node_lo, (void*)node_hi, (void*)arrivals,
+                    (void*)depth, (void*)sah, sort_tmp})
+        cudaFreeAsync(p, s);
+    err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "scene build");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    ctx->build_ms = ms;
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (ctx->max_depth > 96u) {
+        set_error("BVH deeper than the traversal stack (96)");
+        free_scene(ctx);
+        return NAN_ERR_LIMIT;
+    }
+    ctx->has_scene = true;
+    return NAN_OK;
+}
+
+namespace {
+__global__ void k_world_tris(const float4* __restrict__ tris, uint32_t n, float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = tris[3u * i], b = tris[3u * i + 1], c = tris[3u * i + 2];
+    const uint32_t f = __float_as_uint(a.w);
+    float* o = out + 9ull * f;
+    o[0] = a.x; o[1] = a.y; o[2] = a.z;
+    o[3] = b.x; o[4] = b.y; o[5] = b.z;
+    o[6] = c.x; o[7] = c.y; o[8] = c.z;
+}
+}  // namespace
+
+int world_triangles(NanContext* ctx, float* out, cudaStream_t s) {
+    if (ctx->tri_count == 0) return NAN_OK;
+    k_world_tris<<<blocks(ctx->tri_count), kThreads, 0, s>>>(ctx->tris, ctx->tri_count, out);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "world triangles");
+}
+
+}  // namespace nan_host

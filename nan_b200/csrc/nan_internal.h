@@ -1,0 +1,62 @@
+// nan_internal.h -- context object and host-side launchers shared by the
+// translation units of libnan_b200.so (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/nan_b200.h"
+
+struct NanContext {
+    int device = 0;
+    uint32_t* d_status = nullptr;              // device status word
+    unsigned long long* d_counters = nullptr;  // NanCounters on the device
+    // Scene (caller-owned buffers, read in place by the shading code).
+    NanSceneDesc scene{};
+    bool has_scene = false;
+    // BVH storage owned by the context.
+    float4* nodes = nullptr;        // 4 float4 per interior node
+    float4* tris = nullptr;         // 3 float4 per triangle, leaf order
+    uint2* tri_refs = nullptr;      // flat index -> (instance, primitive)
+    int root = 0;
+    uint32_t tri_count = 0;
+    uint32_t node_count = 0;
+    uint32_t leaf_count = 0;
+    uint32_t max_depth = 0;
+    uint64_t device_bytes = 0;
+    double build_ms = 0.0;
+    double sah_cost = 0.0;
+    uint64_t launches = 0;
+};
+
+namespace nan_host {
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what);
+
+void free_scene(NanContext* ctx);
+int build_scene(NanContext* ctx, const NanSceneDesc* desc, cudaStream_t stream);
+int world_triangles(NanContext* ctx, float* out, cudaStream_t stream);
+
+int launch_intersect(NanContext* ctx, const float* rays, uint32_t count, uint32_t* ids, float* tb,
+                     cudaStream_t stream);
+int launch_occluded(NanContext* ctx, const float* rays, uint32_t count, float* vis, cudaStream_t stream);
+int launch_trace_screen(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame,
+                        uint32_t max_vertices, const NanCamera* cam, const NanLighting* light,
+                        cudaStream_t stream);
+int launch_accumulate(NanContext* ctx, const float* input, float* output, float* history, uint32_t w,
+                      uint32_t h, int reset, cudaStream_t stream);
+int launch_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layout, uint8_t* slots, uint32_t iteration,
+                        uint32_t spt, uint32_t max_bounces, int reset, const NanLighting* light,
+                        uint32_t begin, uint32_t end, cudaStream_t stream);
+int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits,
+                        uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                        const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
+                        uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
+                        uint32_t begin, uint32_t end, cudaStream_t stream);
+int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
+                       cudaStream_t stream);
+
+}  // namespace nan_host

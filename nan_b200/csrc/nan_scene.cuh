@@ -1,0 +1,480 @@
+// nan_scene.cuh -- device view of a built scene: BVH traversal, shading data,
+// spawn offsets and lights. Included by translation units compiled with
+// --fmad=false (see nan_math.cuh).
+#pragma once
+
+#include <cstdint>
+
+#include "nan_math.cuh"
+
+namespace nbd {
+
+constexpr int kTraversalStack = 96;
+constexpr uint32_t kStatusStackOverflow = 1u;
+
+// Binary BVH node, 64 bytes: both children's boxes live in the parent so one
+// node fetch tests two boxes.
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, -, -): child >= 0 is an interior node, child < 0 a
+//       leaf holding the single triangle ~child (leaf order).
+// Triangles in leaf order: 3 float4 each, (v0, flat index bits), (v1, 0),
+// (v2, 0), world space.
+struct SceneView {
+    const float4* nodes;
+    const float4* tris;
+    const uint2* tri_refs;          // flat index -> (instance, primitive)
+    const float* vertices;          // f32[V][8]
+    const uint32_t* indices;        // u32[T][3]
+    const uint4* mesh_descs;
+    const uint4* instance_descs;
+    const float* transforms;        // f32[X][16]
+    const float* inverse_transposes;
+    const float* materials;         // f32[N][8]
+    int root;
+    uint32_t tri_count;
+    uint32_t* status;               // device status word
+};
+
+struct HitInfo {
+    bool valid;
+    uint32_t flat;
+    float t;
+    float b1, b2;  // weights of v1 and v2 (Slang HitInfo.bary)
+};
+
+// Per-ray constants of the watertight test (Woop, Benthin, Wald 2013).
+struct WtRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+__device__ __forceinline__ WtRay wt_setup(f3 d) {
+    WtRay r;
+    const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = 0;
+    float m = ax;
+    if (ay > m) { kz = 1; m = ay; }
+    if (az > m) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    const float dz = comp(d, kz);
+    if (dz < 0.0f) { int t = kx; kx = ky; ky = t; }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.sx = comp(d, kx) / dz;
+    r.sy = comp(d, ky) / dz;
+    r.sz = 1.0f / dz;
+    return r;
+}
+
+// Edge functions and scaled distance; returns false when the ray misses the
+// closed triangle or the triangle is degenerate along the ray.
+__device__ __forceinline__ bool wt_test(const WtRay& r, f3 o, f3 v0, f3 v1, f3 v2, float* t,
+                                        float* out_v, float* out_w, float* out_det) {
+    const f3 A = v0 - o, B = v1 - o, C = v2 - o;
+    const float akz = comp(A, r.kz), bkz = comp(B, r.kz), ckz = comp(C, r.kz);
+    const float ax = comp(A, r.kx) - r.sx * akz;
+    const float ay = comp(A, r.ky) - r.sy * akz;
+    const float bx = comp(B, r.kx) - r.sx * bkz;
+    const float by = comp(B, r.ky) - r.sy * bkz;
+    const float cx = comp(C, r.kx) - r.sx * ckz;
+    const float cy = comp(C, r.ky) - r.sy * ckz;
+    float U = cx * by - cy * bx;
+    float V = ax * cy - ay * cx;
+    float W = bx * ay - by * ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)cx * (double)by - (double)cy * (double)bx);
+        V = (float)((double)ax * (double)cy - (double)ay * (double)cx);
+        W = (float)((double)bx * (double)ay - (double)by * (double)ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = (U + V) + W;
+    if (det == 0.0f) return false;
+    const float tt = (U * (r.sz * akz) + V * (r.sz * bkz)) + W * (r.sz * ckz);
+    *t = tt / det;
+    *out_v = V;
+    *out_w = W;
+    *out_det = det;
+    return true;
+}
+
+__device__ __forceinline__ void load_tri(const SceneView& s, int i, f3* v0, f3* v1, f3* v2, uint32_t* flat) {
+    const float4 a = __ldg(s.tris + 3 * i);
+    const float4 b = __ldg(s.tris + 3 * i + 1);
+    const float4 c = __ldg(s.tris + 3 * i + 2);
+    *v0 = mk3(a.x, a.y, a.z);
+    *v1 = mk3(b.x, b.y, b.z);
+    *v2 = mk3(c.x, c.y, c.z);
+    *flat = __float_as_uint(a.w);
+}
+
+// Slab test of both children of a node. Node boxes are padded outward at
+// build time by more than the rounding of the fused slab arithmetic, so the
+// test never rejects a box the exact ray crosses.
+struct BoxRay {
+    float ix, iy, iz, ox, oy, oz;
+};
+
+__device__ __forceinline__ BoxRay box_setup(f3 o, f3 d) {
+    BoxRay b;
+    const float e = 1e-20f;
+    b.ix = 1.0f / (fabsf(d.x) > e ? d.x : copysignf(e, d.x));
+    b.iy = 1.0f / (fabsf(d.y) > e ? d.y : copysignf(e, d.y));
+    b.iz = 1.0f / (fabsf(d.z) > e ? d.z : copysignf(e, d.z));
+    b.ox = o.x * b.ix;
+    b.oy = o.y * b.iy;
+    b.oz = o.z * b.iz;
+    return b;
+}
+
+__device__ __forceinline__ void box2(const BoxRay& r, float4 na, float4 nb, float4 nc, float tmin, float tmax,
+                                     float* t0, float* t1, bool* h0, bool* h1) {
+    const float x0a = __fmaf_rn(na.x, r.ix, -r.ox), x0b = __fmaf_rn(na.y, r.ix, -r.ox);
+    const float y0a = __fmaf_rn(na.z, r.iy, -r.oy), y0b = __fmaf_rn(na.w, r.iy, -r.oy);
+    const float z0a = __fmaf_rn(nc.x, r.iz, -r.oz), z0b = __fmaf_rn(nc.y, r.iz, -r.oz);
+    const float x1a = __fmaf_rn(nb.x, r.ix, -r.ox), x1b = __fmaf_rn(nb.y, r.ix, -r.ox);
+    const float y1a = __fmaf_rn(nb.z, r.iy, -r.oy), y1b = __fmaf_rn(nb.w, r.iy, -r.oy);
+    const float z1a = __fmaf_rn(nc.z, r.iz, -r.oz), z1b = __fmaf_rn(nc.w, r.iz, -r.oz);
+    const float lo0 = fmaxf(fmaxf(fminf(x0a, x0b), fminf(y0a, y0b)), fmaxf(fminf(z0a, z0b), tmin));
+    const float hi0 = fminf(fminf(fmaxf(x0a, x0b), fmaxf(y0a, y0b)), fminf(fmaxf(z0a, z0b), tmax));
+    const float lo1 = fmaxf(fmaxf(fminf(x1a, x1b), fminf(y1a, y1b)), fmaxf(fminf(z1a, z1b), tmin));
+    const float hi1 = fminf(fminf(fmaxf(x1a, x1b), fmaxf(y1a, y1b)), fminf(fmaxf(z1a, z1b), tmax));
+    *t0 = lo0;
+    *t1 = lo1;
+    *h0 = lo0 <= hi0;
+    *h1 = lo1 <= hi1;
+}
+
+// Closest hit in [tmin, tmax]; ties in t go to the lower flat triangle index
+// (lexicographic (instance, primitive)), so the result does not depend on
+// the traversal order.
+__device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    HitInfo hit;
+    hit.valid = false;
+    hit.flat = 0xffffffffu;
+    hit.t = tmax;
+    hit.b1 = 0.0f;
+    hit.b2 = 0.0f;
+    if (s.tri_count == 0) return hit;
+    const WtRay wr = wt_setup(d);
+    const BoxRay br = box_setup(o, d);
+    int stack[kTraversalStack];
+    int sp = 0;
+    int node = s.root;
+    float best_t = tmax;
+    uint32_t best_key = 0xffffffffu;
+    int best_tri = -1;
+    for (;;) {
+        if (node >= 0) {
+            const float4* n = s.nodes + 4 * node;
+            const float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+            const int4 nd = __ldg(reinterpret_cast<const int4*>(n + 3));
+            float t0, t1;
+            bool h0, h1;
+            box2(br, na, nb, nc, tmin, best_t, &t0, &t1, &h0, &h1);
+            if (h0 && h1) {
+                int near_child = nd.x, far_child = nd.y;
+                if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
+                if (sp < kTraversalStack) stack[sp++] = far_child;
+                else atomicOr(s.status, kStatusStackOverflow);
+                node = near_child;
+                continue;
+            }
+            if (h0) { node = nd.x; continue; }
+            if (h1) { node = nd.y; continue; }
+        } else {
+            const int tri = ~node;
+            f3 v0, v1, v2;
+            uint32_t flat;
+            load_tri(s, tri, &v0, &v1, &v2, &flat);
+            float t, V, W, det;
+            if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin &&
+                (t < best_t || (t == best_t && flat < best_key))) {
+                best_t = t;
+                best_key = flat;
+                best_tri = tri;
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    if (best_tri >= 0) {
+        f3 v0, v1, v2;
+        uint32_t flat;
+        load_tri(s, best_tri, &v0, &v1, &v2, &flat);
+        float t, V, W, det;
+        wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det);
+        hit.valid = true;
+        hit.flat = best_key;
+        hit.t = best_t;
+        hit.b1 = V / det;
+        hit.b2 = W / det;
+    }
+    return hit;
+}
+
+// Any hit in [tmin, tmax].
+__device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    if (s.tri_count == 0) return false;
+    const WtRay wr = wt_setup(d);
+    const BoxRay br = box_setup(o, d);
+    int stack[kTraversalStack];
+    int sp = 0;
+    int node = s.root;
+    for (;;) {
+        if (node >= 0) {
+            const float4* n = s.nodes + 4 * node;
+            const float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+            const int4 nd = __ldg(reinterpret_cast<const int4*>(n + 3));
+            float t0, t1;
+            bool h0, h1;
+            box2(br, na, nb, nc, tmin, tmax, &t0, &t1, &h0, &h1);
+            if (h0 && h1) {
+                int near_child = nd.x, far_child = nd.y;
+                if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
+                if (sp < kTraversalStack) stack[sp++] = far_child;
+                else atomicOr(s.status, kStatusStackOverflow);
+                node = near_child;
+                continue;
+            }
+            if (h0) { node = nd.x; continue; }
+            if (h1) { node = nd.y; continue; }
+        } else {
+            f3 v0, v1, v2;
+            uint32_t flat;
+            load_tri(s, ~node, &v0, &v1, &v2, &flat);
+            float t, V, W, det;
+            if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) return true;
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Shading (scene.slang:178-406, opaque and untextured materials).
+// ---------------------------------------------------------------------------
+struct Shading {
+    f3 position;
+    f3 origin_front;
+    float offset;
+    f3 face_normal;
+    f3 diffuse;
+    f3 emissive;
+    Frame frame;  // shading frame
+};
+
+struct TriRefs {
+    const float* v0;
+    const float* v1;
+    const float* v2;
+    const float* m;
+    const float* it;
+    const float* mat;
+    uint32_t flags;
+};
+
+__device__ __forceinline__ TriRefs tri_refs(const SceneView& s, uint32_t inst, uint32_t prim) {
+    const uint4 idesc = __ldg(s.instance_descs + inst);
+    const uint4 mdesc = __ldg(s.mesh_descs + idesc.x);
+    const uint32_t base = mdesc.w + prim * 3u;
+    TriRefs r;
+    r.v0 = s.vertices + 8u * (mdesc.z + __ldg(s.indices + base));
+    r.v1 = s.vertices + 8u * (mdesc.z + __ldg(s.indices + base + 1));
+    r.v2 = s.vertices + 8u * (mdesc.z + __ldg(s.indices + base + 2));
+    r.m = s.transforms + 16u * idesc.z;
+    r.it = s.inverse_transposes + 16u * idesc.z;
+    r.mat = s.materials + 8u * idesc.y;
+    r.flags = idesc.w;
+    return r;
+}
+
+// get_triangle_spawn_data, scene.slang:178-269.
+__device__ __forceinline__ void triangle_spawn(f3 v0, f3 v1, f3 v2, float bx, float by, const float* m,
+                                               const float* it, f3* pos, f3* nrm, float* off) {
+    const float c0 = 5.9604644775390625e-8f;
+    const float c1 = 1.7881397695873602e-7f;
+    const float c2 = 1.1920931797249068e-7f;
+    float M[12], I[16];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) M[k] = __ldg(m + k);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) I[k] = __ldg(it + k);
+    const f3 e1 = v1 - v0, e2 = v2 - v0;
+    const f3 op = mk3(v0.x + __fmaf_rn(bx, e1.x, by * e2.x), v0.y + __fmaf_rn(bx, e1.y, by * e2.y),
+                      v0.z + __fmaf_rn(bx, e1.z, by * e2.z));
+    const f3 on = cross3(e1, e2);
+    f3 wp;
+    wp.x = M[3] + __fmaf_rn(M[0], op.x, __fmaf_rn(M[1], op.y, M[2] * op.z));
+    wp.y = M[7] + __fmaf_rn(M[4], op.x, __fmaf_rn(M[5], op.y, M[6] * op.z));
+    wp.z = M[11] + __fmaf_rn(M[8], op.x, __fmaf_rn(M[9], op.y, M[10] * op.z));
+    const f3 wnu = mk3((I[0] * on.x + I[1] * on.y) + I[2] * on.z, (I[4] * on.x + I[5] * on.y) + I[6] * on.z,
+                       (I[8] * on.x + I[9] * on.y) + I[10] * on.z);
+    const float ws = 1.0f / sqrtf(maxf(dot3(wnu, wnu), 1e-30f));
+    const f3 wn = wnu * ws;
+    const f3 ext3 = (abs3(e1) + abs3(e2)) + abs3(abs3(e1) - abs3(e2));
+    const float ext = maxf(maxf(ext3.x, ext3.y), ext3.z);
+    const f3 av0 = abs3(v0);
+    f3 oe = mk3(c0 * av0.x + c1 * ext, c0 * av0.y + c1 * ext, c0 * av0.z + c1 * ext);
+    const f3 aop = abs3(op);
+    f3 we;
+    we.x = c1 * dot3(abs3(mk3(M[0], M[1], M[2])), aop) + c2 * fabsf(M[3]);
+    we.y = c1 * dot3(abs3(mk3(M[4], M[5], M[6])), aop) + c2 * fabsf(M[7]);
+    we.z = c1 * dot3(abs3(mk3(M[8], M[9], M[10])), aop) + c2 * fabsf(M[11]);
+    const f3 awp = abs3(wp);
+    f3 te;
+    te.x = ((fabsf(I[0]) * awp.x + fabsf(I[4]) * awp.y) + fabsf(I[8]) * awp.z) + fabsf(I[12]) * 1.0f;
+    te.y = ((fabsf(I[1]) * awp.x + fabsf(I[5]) * awp.y) + fabsf(I[9]) * awp.z) + fabsf(I[13]) * 1.0f;
+    te.z = ((fabsf(I[2]) * awp.x + fabsf(I[6]) * awp.y) + fabsf(I[10]) * awp.z) + fabsf(I[14]) * 1.0f;
+    oe = oe + mk3(c2 * te.x, c2 * te.y, c2 * te.z);
+    const float oo = dot3(oe, abs3(on));
+    float wo = dot3(we, abs3(wn));
+    wo = __fmaf_rn(ws, oo, wo);
+    *pos = wp;
+    *nrm = wn;
+    *off = wo;
+}
+
+// get_shading_data, scene.slang:271-406.
+__device__ __forceinline__ Shading shading_data(const SceneView& s, uint32_t inst, uint32_t prim, float bx,
+                                                float by, f3 view) {
+    const TriRefs r = tri_refs(s, inst, prim);
+    const float b0 = (1.0f - bx) - by;
+    const f3 p0 = ld3(r.v0), p1 = ld3(r.v1), p2 = ld3(r.v2);
+    f3 pos, fn;
+    float off;
+    triangle_spawn(p0, p1, p2, bx, by, r.m, r.it, &pos, &fn, &off);
+    const f3 n0 = ld3(r.v0 + 3), n1 = ld3(r.v1 + 3), n2 = ld3(r.v2 + 3);
+    const f3 ni = (b0 * n0 + bx * n1) + by * n2;
+    const float* it = r.it;
+    const f3 gnu = mk3(((__ldg(it + 0) * ni.x + __ldg(it + 1) * ni.y) + __ldg(it + 2) * ni.z) + __ldg(it + 3) * 0.0f,
+                       ((__ldg(it + 4) * ni.x + __ldg(it + 5) * ni.y) + __ldg(it + 6) * ni.z) + __ldg(it + 7) * 0.0f,
+                       ((__ldg(it + 8) * ni.x + __ldg(it + 9) * ni.y) + __ldg(it + 10) * ni.z) + __ldg(it + 11) * 0.0f);
+    f3 gn = normalize3(gnu);
+    f3 sn = gn;
+    const uint32_t mflags = __float_as_uint(__ldg(r.mat + 3));
+    const bool double_sided = (mflags & 1u) != 0u;
+    const bool front = dot3(fn, view) > 0.0f;
+    const float sign = (double_sided && !front) ? -1.0f : 1.0f;
+    fn = fn * sign;
+    gn = gn * sign;
+    sn = sn * sign;
+    sn = adjust_shading_normal(sn, fn, -view);
+    Shading sd;
+    sd.position = pos;
+    sd.origin_front = pos + off * fn;
+    sd.offset = off;
+    sd.face_normal = fn;
+    sd.frame = Frame(sn);
+    sd.diffuse = ld3(r.mat);
+    sd.emissive = ld3(r.mat + 4);
+    return sd;
+}
+
+// get_world_flat_normal, texture_space_path_tracer.slang:39-55, with
+// compute_flat_normal, common.slang:101-111.
+__device__ __forceinline__ f3 world_flat_normal(const SceneView& s, uint32_t inst, uint32_t prim) {
+    const TriRefs r = tri_refs(s, inst, prim);
+    const f3 p0 = ld3(r.v0), p1 = ld3(r.v1), p2 = ld3(r.v2);
+    f3 n = normalize3(cross3(p1 - p0, p2 - p0));
+    if (r.flags & 1u) n = -n;
+    const float* it = r.it;
+    const f3 w = mk3((__ldg(it + 0) * n.x + __ldg(it + 1) * n.y) + __ldg(it + 2) * n.z,
+                     (__ldg(it + 4) * n.x + __ldg(it + 5) * n.y) + __ldg(it + 6) * n.z,
+                     (__ldg(it + 8) * n.x + __ldg(it + 9) * n.y) + __ldg(it + 10) * n.z);
+    return normalize3(w);
+}
+
+// ---------------------------------------------------------------------------
+// Lights (scene.slang:408-527, 940-1009) with the LUTs reduced to constants.
+// ---------------------------------------------------------------------------
+struct LightParams {
+    f3 sun_dir;
+    float cos_half;
+    f3 outer;   // color * intensity
+    f3 trans;   // transmittance
+    f3 illum;   // outer * trans
+    f3 sky;
+    float t_max;
+    bool sun_disk;
+};
+
+struct LightingRaw {  // layout of NanLighting
+    float sun_direction[3];
+    float sun_cos_half_angle;
+    float sun_color[3];
+    float sun_intensity;
+    float sun_transmittance[3];
+    float ray_t_max;
+    float sky_radiance[3];
+    uint32_t flags;
+};
+
+__device__ __forceinline__ LightParams make_light(const LightingRaw& p) {
+    LightParams L;
+    L.sun_dir = mk3(p.sun_direction[0], p.sun_direction[1], p.sun_direction[2]);
+    L.cos_half = p.sun_cos_half_angle;
+    L.outer = mk3(p.sun_color[0], p.sun_color[1], p.sun_color[2]) * p.sun_intensity;
+    L.trans = mk3(p.sun_transmittance[0], p.sun_transmittance[1], p.sun_transmittance[2]);
+    L.illum = L.outer * L.trans;
+    L.sky = mk3(p.sky_radiance[0], p.sky_radiance[1], p.sky_radiance[2]);
+    L.t_max = p.ray_t_max;
+    L.sun_disk = (p.flags & 1u) != 0u;
+    return L;
+}
+
+// get_sun_disk_luminance, scene.slang:408-465.
+__device__ __forceinline__ f3 sun_disk(const LightParams& L, f3 dir) {
+    const f3 vp = mk3(0.0f, 6.360f + 0.0002f, 0.0f);
+    const float a = dot3(dir, dir);
+    const float b = 2.0f * dot3(vp, dir);
+    const float gr = 6.360f;
+    const float c = dot3(vp, vp) - gr * gr;
+    const float disc = b * b - 4.0f * a * c;
+    if (disc >= 0.0f) {
+        const float sq = sqrtf(disc);
+        const float t0 = (-b - sq) / (2.0f * a);
+        const float t1 = (-b + sq) / (2.0f * a);
+        if (t0 > 0.0f || t1 > 0.0f) return mk3(0.0f, 0.0f, 0.0f);
+    }
+    const float vdl = dot3(dir, L.sun_dir);
+    if (vdl > L.cos_half) {
+        const float solid = (2.0f * kPi) * (1.0f - L.cos_half);
+        const f3 lum = L.outer / solid;
+        const float soft = sat(2.0f * (vdl - L.cos_half) / (1.0f - L.cos_half));
+        return (L.trans * lum) * soft;
+    }
+    return mk3(0.0f, 0.0f, 0.0f);
+}
+
+struct RayTally {
+    uint32_t extend;
+    uint32_t shadow;
+};
+
+// sample_directional_light_with_visibility(sd, u, 1, 0), scene.slang:954-990.
+__device__ __forceinline__ f3 sun_nee(const SceneView& s, const LightParams& L, const Shading& sd, float ux,
+                                      float uy, RayTally& tally) {
+    const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, ux, uy);
+    tally.shadow++;
+    const float vis = trace_any(s, sd.origin_front, l, 0.0f, L.t_max) ? 0.0f : 1.0f;
+    const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+    const f3 f = sd.diffuse * kInvPi;
+    return ((vis * f) * L.illum) * ndl;
+}
+
+// sample_directional_irradiance, scene.slang:940-952.
+__device__ __forceinline__ f3 sun_irradiance(const SceneView& s, const LightParams& L, const Shading& sd,
+                                             float ux, float uy, RayTally& tally) {
+    const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, ux, uy);
+    tally.shadow++;
+    const float vis = trace_any(s, sd.origin_front, l, 0.0f, L.t_max) ? 0.0f : 1.0f;
+    const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+    return (vis * L.illum) * ndl;
+}
+
+}  // namespace nbd

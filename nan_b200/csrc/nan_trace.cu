@@ -1,0 +1,643 @@
+// nan_trace.cu -- ray queries, the three integrators, accumulation, RGB9E5.
+// Compiled with --fmad=false (see nan_math.cuh).
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
+#include "nan_internal.h"
+#include "nan_scene.cuh"
+
+namespace {
+
+using namespace nbd;
+using nan_host::cuda_fail;
+using nan_host::set_error;
+
+struct CameraRaw {  // layout of NanCamera
+    float position[3];
+    float jitter_x;
+    float image_u[3];
+    float jitter_y;
+    float image_v[3];
+    float near_clip;
+    float image_w[3];
+    float far_clip;
+};
+
+SceneView scene_view(const NanContext* ctx) {
+    SceneView v;
+    v.nodes = ctx->nodes;
+    v.tris = ctx->tris;
+    v.tri_refs = ctx->tri_refs;
+    v.vertices = ctx->scene.vertices;
+    v.indices = ctx->scene.indices;
+    v.mesh_descs = reinterpret_cast<const uint4*>(ctx->scene.mesh_descs);
+    v.instance_descs = reinterpret_cast<const uint4*>(ctx->scene.instance_descs);
+    v.transforms = ctx->scene.transforms;
+    v.inverse_transposes = ctx->scene.inverse_transposes;
+    v.materials = ctx->scene.materials;
+    v.root = ctx->root;
+    v.tri_count = ctx->tri_count;
+    v.status = ctx->d_status;
+    return v;
+}
+
+// Warp-aggregated update of the context counters.
+__device__ __forceinline__ void flush_tally(unsigned long long* counters, const RayTally& t, uint32_t units,
+                                            uint32_t paths) {
+    const unsigned mask = __activemask();
+    const uint32_t e = __reduce_add_sync(mask, t.extend);
+    const uint32_t s = __reduce_add_sync(mask, t.shadow);
+    const uint32_t u = __reduce_add_sync(mask, units);
+    const uint32_t p = __reduce_add_sync(mask, paths);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(mask) - 1)) {
+        atomicAdd(counters + 0, (unsigned long long)e);
+        atomicAdd(counters + 1, (unsigned long long)s);
+        atomicAdd(counters + 2, (unsigned long long)u);
+        atomicAdd(counters + 3, (unsigned long long)p);
+    }
+}
+
+__device__ __forceinline__ HitInfo closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax, RayTally& t) {
+    t.extend++;
+    return trace_closest(s, o, d, tmin, tmax);
+}
+
+// ---------------------------------------------------------------------------
+// Ray queries.
+// ---------------------------------------------------------------------------
+__global__ void k_intersect(SceneView s, const float4* __restrict__ rays, uint32_t n, uint4* __restrict__ ids,
+                            float* __restrict__ tb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = rays[2u * i], b = rays[2u * i + 1];
+    const HitInfo h = trace_closest(s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w);
+    uint2 ref = make_uint2(0u, 0u);
+    if (h.valid) ref = __ldg(s.tri_refs + h.flat);
+    ids[i] = make_uint4(h.valid ? 1u : 0u, ref.x, ref.y, h.valid ? h.flat : 0xffffffffu);
+    tb[3u * i + 0] = h.valid ? h.t : 0.0f;
+    tb[3u * i + 1] = h.b1;
+    tb[3u * i + 2] = h.b2;
+}
+
+__global__ void k_occluded(SceneView s, const float4* __restrict__ rays, uint32_t n, float* __restrict__ vis) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = rays[2u * i], b = rays[2u * i + 1];
+    vis[i] = trace_any(s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w) ? 0.0f : 1.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Screen path tracer: path_tracer.slang:40-130 and camera.slang:201-236.
+// 128-thread blocks cover 16x8 pixel tiles; each warp an 8x4 tile.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_trace_screen(SceneView s, LightingRaw lraw, CameraRaw cam,
+                                                      float4* __restrict__ out, uint32_t w, uint32_t h,
+                                                      uint32_t frame, uint32_t max_vertices,
+                                                      unsigned long long* counters) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= w || py >= h) return;
+    const LightParams L = make_light(lraw);
+    RayTally tally{0u, 0u};
+    Rng rng(px, py, frame * 1u + 0u);
+    rng.next_1d();
+    rng.next_1d();  // the unused jitter draw (path_tracer.slang:121)
+    float pxf = ((float)px + 0.5f) / (float)w;
+    float pyf = ((float)py + 0.5f) / (float)h;
+    pxf = pxf + (-cam.jitter_x);
+    pyf = pyf + cam.jitter_y;
+    const float nx = 2.0f * pxf + -1.0f;
+    const float ny = -2.0f * pyf + 1.0f;
+    const f3 U = mk3(cam.image_u[0], cam.image_u[1], cam.image_u[2]);
+    const f3 V = mk3(cam.image_v[0], cam.image_v[1], cam.image_v[2]);
+    const f3 W = mk3(cam.image_w[0], cam.image_w[1], cam.image_w[2]);
+    f3 dir = normalize3((nx * U + ny * V) + W);
+    const float inv_cos = 1.0f / dot3(normalize3(W), dir);
+    float tmin = cam.near_clip * inv_cos;
+    float tmax = cam.far_clip * inv_cos;
+    f3 o = mk3(cam.position[0], cam.position[1], cam.position[2]);
+    f3 thp = mk3(1.0f, 1.0f, 1.0f), Lr = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t vi = 0; vi < max_vertices; ++vi) {
+        const HitInfo hit = closest(s, o, dir, tmin, tmax, tally);
+        if (!hit.valid) {
+            f3 sky = L.sky;
+            if (vi == 0u && L.sun_disk) sky = sky + sun_disk(L, dir);
+            Lr = Lr + thp * sky;
+            break;
+        }
+        const uint2 ref = __ldg(s.tri_refs + hit.flat);
+        const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
+        Lr = Lr + thp * sd.emissive;
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        Lr = Lr + thp * sun_nee(s, L, sd, u0, u1, tally);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 wo = cosine_sample_hemisphere(e0, e1, &pdf);
+        pdf = maxf(pdf, 1e-6f);
+        const f3 f = sd.diffuse * kInvPi;
+        thp = thp * ((f * fabsf(wo.z)) / pdf);
+        o = sd.origin_front;
+        dir = sd.frame.to_global(wo);
+        tmin = 0.0f;
+        tmax = L.t_max;
+    }
+    out[(size_t)py * w + px] = make_float4(Lr.x, Lr.y, Lr.z, 1.0f);
+    flush_tally(counters, tally, 1u, 1u);
+}
+
+// accumulator.slang:9-19
+__global__ void k_accumulate(const float4* __restrict__ input, float4* __restrict__ output,
+                             float4* __restrict__ history, uint32_t n, int reset) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 in = input[i];
+    float4 a = reset ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : history[i];
+    a = make_float4(a.x + in.x, a.y + in.y, a.z + in.z, a.w + 1.0f);
+    history[i] = a;
+    output[i] = make_float4(a.x / a.w, a.y / a.w, a.z / a.w, 1.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Mesh Colors lattice (mesh_colors.slang:37-65, 272-363).
+// ---------------------------------------------------------------------------
+struct McView {
+    const uint2* face_infos;
+    const uint4* instance_infos;
+    const uint2* side_infos;
+    const uint32_t* surface_prefix;
+    uint32_t instance_count;
+    uint32_t payload_count;
+};
+
+__device__ __forceinline__ uint32_t mc_address(uint32_t i, uint32_t j, uint32_t texel_offset, uint2 face) {
+    const uint32_t row = i * (face.y + 1u) - i * (i - 1u) / 2u;
+    return texel_offset + face.x + row + j;
+}
+
+__device__ __forceinline__ void mc_address_to_ij(uint32_t address, uint32_t r, uint32_t* oi, uint32_t* oj) {
+    uint32_t left = 0u, right = r;
+    while (left < right) {
+        const uint32_t mid = (left + right + 1u) / 2u;
+        const uint32_t ma = mid * (r + 1u) - mid * (mid - 1u) / 2u;
+        if (ma <= address) left = mid; else right = mid - 1u;
+    }
+    *oi = left;
+    *oj = address - (left * (r + 1u) - left * (left - 1u) / 2u);
+}
+
+__device__ __forceinline__ float fracf(float x) { return x - floorf(x); }
+
+__device__ __forceinline__ uint32_t mc_nearest_texel(float b0, float b1, float b2, uint32_t texel_offset, uint2 face) {
+    const uint32_t R = face.y;
+    const float rf = (float)R;
+    const float s0 = sat(b0) * rf, s1 = sat(b1) * rf, s2 = sat(b2) * rf;
+    uint32_t i = (uint32_t)s0, j = (uint32_t)s1;
+    i = min(i, R);
+    j = min(j, R - i);
+    float w0 = fracf(s0), w1 = fracf(s1), w2 = fracf(s2);
+    const bool upper = fabsf(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
+    if (upper) {
+        w0 = 1.0f - w0;
+        w1 = 1.0f - w1;
+        w2 = 1.0f - w2;
+    }
+    if ((w0 + w1) + w2 <= 1e-6f || i >= R || j >= R - i) return mc_address(i, j, texel_offset, face);
+    const float largest = maxf(w0, maxf(w1, w2));
+    if (upper) {
+        if (fabsf(largest - w0) < 1e-3f) return mc_address(i, j + 1u, texel_offset, face);
+        if (fabsf(largest - w1) < 1e-3f) return mc_address(i + 1u, j, texel_offset, face);
+        return mc_address(i + 1u, j + 1u, texel_offset, face);
+    }
+    if (fabsf(largest - w0) < 1e-3f) return mc_address(i + 1u, j, texel_offset, face);
+    if (fabsf(largest - w1) < 1e-3f) return mc_address(i, j + 1u, texel_offset, face);
+    return mc_address(i, j, texel_offset, face);
+}
+
+// trace_radiance, texture_space_path_tracer.slang:57-84.
+__device__ __forceinline__ f3 ts_trace_radiance(const SceneView& s, const LightParams& L, f3 o, f3 d, Rng& rng,
+                                                uint32_t max_bounces, RayTally& tally) {
+    f3 thp = mk3(1.0f, 1.0f, 1.0f), rad = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+        const HitInfo hit = closest(s, o, d, 0.0f, L.t_max, tally);
+        if (!hit.valid) return rad + thp * L.sky;
+        const uint2 ref = __ldg(s.tri_refs + hit.flat);
+        const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -d);
+        rad = rad + thp * sd.emissive;
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        rad = rad + thp * sun_nee(s, L, sd, u0, u1, tally);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 sdir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf <= 1e-6f) return rad;
+        const f3 f = sd.diffuse * kInvPi;
+        thp = thp * ((f * fabsf(sdir.z)) / pdf);
+        o = sd.origin_front;
+        d = sd.frame.to_global(sdir);
+    }
+    return rad;
+}
+
+// estimate_surface_irradiance, texture_space_path_tracer.slang:86-117.
+__device__ __forceinline__ f3 ts_estimate(const SceneView& s, const LightParams& L, uint32_t inst, uint32_t prim,
+                                          float bx, float by, f3 view, uint32_t n, Rng& rng, uint32_t max_bounces,
+                                          RayTally& tally) {
+    const Shading sd = shading_data(s, inst, prim, bx, by, view);
+    f3 irr = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t k = 0; k < n; ++k) {
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        f3 si = sun_irradiance(s, L, sd, u0, u1, tally);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 dir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf > 1e-6f) {
+            const f3 rad = ts_trace_radiance(s, L, sd.origin_front, sd.frame.to_global(dir), rng, max_bounces, tally);
+            si = si + ((rad * fabsf(dir.z)) / pdf);
+        }
+        irr = irr + si;
+    }
+    return irr / (float)n;
+}
+
+// store_accumulated_irradiance, texture_space_path_tracer.slang:119-138.
+__device__ __forceinline__ void store_running_mean(uint4* __restrict__ slots, uint32_t texel, f3 v, int reset) {
+    uint4 old = make_uint4(0u, 0u, 0u, 0u);
+    if (!reset) old = slots[texel];
+    const uint32_t prev = reset ? 0u : old.w;
+    f3 pv = mk3(0.0f, 0.0f, 0.0f);
+    if (prev != 0u) pv = mk3(__uint_as_float(old.x), __uint_as_float(old.y), __uint_as_float(old.z));
+    const uint32_t next = min(prev + 1u, 65535u);
+    const float weight = 1.0f / (float)(prev + 1u);
+    const f3 acc = pv + weight * (v - pv);
+    slots[texel] = make_uint4(__float_as_uint(acc.x), __float_as_uint(acc.y), __float_as_uint(acc.z), next);
+}
+
+// compute_main, texture_space_path_tracer.slang:140-216, one thread per
+// surface texel of every instance.
+__global__ void __launch_bounds__(128) k_trace_texels(SceneView s, LightingRaw lraw, McView mc,
+                                                      uint4* __restrict__ slots, uint32_t iteration, uint32_t spt,
+                                                      uint32_t max_bounces, int reset, uint32_t begin, uint32_t end,
+                                                      unsigned long long* counters) {
+    const uint32_t u = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= end) return;
+    // instance = last i with surface_prefix[i] <= u
+    uint32_t lo = 0u, hi = mc.instance_count - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(mc.surface_prefix + mid) <= u) lo = mid; else hi = mid - 1u;
+    }
+    const uint32_t inst_index = lo;
+    const uint32_t local = u - __ldg(mc.surface_prefix + inst_index);
+    const uint4 inst = __ldg(mc.instance_infos + inst_index);  // face off, face count, texel off, texel count
+    const uint2 side = __ldg(mc.side_infos + inst_index);
+    RayTally tally{0u, 0u};
+    if (local >= inst.w) return;
+    // mesh_colors_find_face (mesh_colors.slang:272-305)
+    int left = (int)inst.x, right = (int)(inst.x + inst.y) - 1;
+    uint2 face = make_uint2(0u, 1u);
+    uint32_t prim = 0u;
+    bool found = false;
+    while (left <= right) {
+        const int mid = (left + right) / 2;
+        face = __ldg(mc.face_infos + mid);
+        const int loc = (int)local - (int)face.x;
+        const int count = (int)((face.y + 1u) * (face.y + 2u) / 2u);
+        if (loc < 0) right = mid - 1;
+        else if (loc >= count) left = mid + 1;
+        else {
+            prim = (uint32_t)mid - inst.x;
+            found = true;
+            break;
+        }
+    }
+    if (!found) return;
+    const uint32_t global_texel = inst.z + local;
+    uint32_t ti, tj;
+    mc_address_to_ij(local - face.x, face.y, &ti, &tj);
+    const float rf = (float)face.y;
+    const float base_x = (float)ti / rf, base_y = (float)tj / rf;
+    const uint32_t n = max(spt, 1u);
+    Rng rng(global_texel, inst_index, iteration * n);
+    float bx = base_x, by = base_y;
+    for (uint32_t attempt = 0; attempt < 32u; ++attempt) {
+        const float r0 = rng.next_1d(), r1 = rng.next_1d();
+        const float cx = base_x + (r0 - 0.5f) / rf;
+        const float cy = base_y + (r1 - 0.5f) / rf;
+        if (cx < 0.0f || cy < 0.0f || cx + cy > 1.0f) continue;
+        if (mc_nearest_texel(cx, cy, (1.0f - cx) - cy, inst.z, face) == global_texel) {
+            bx = cx;
+            by = cy;
+            break;
+        }
+    }
+    const float hb1 = by, hb2 = maxf(0.0f, (1.0f - bx) - by);
+    const LightParams L = make_light(lraw);
+    const f3 fnrm = world_flat_normal(s, inst_index, prim);
+    const f3 front = ts_estimate(s, L, inst_index, prim, hb1, hb2, fnrm, n, rng, max_bounces, tally);
+    uint32_t paths = n;
+    if (global_texel < mc.payload_count) store_running_mean(slots, global_texel, front, reset);
+    else atomicOr(s.status, 2u);
+    if (side.y & 1u) {
+        const f3 back = ts_estimate(s, L, inst_index, prim, hb1, hb2, -fnrm, n, rng, max_bounces, tally);
+        const uint32_t bt = side.x + (global_texel - inst.z);
+        if (bt < mc.payload_count) store_running_mean(slots, bt, back, reset);
+        else atomicOr(s.status, 2u);
+        paths += n;
+    }
+    flush_tally(counters, tally, 1u, paths);
+}
+
+// ---------------------------------------------------------------------------
+// Surface-probe baker: surface_probe_path_tracer.slang:47-315.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float radial_texel_cosine_probability(uint32_t texel) {
+    const uint32_t cx = texel % 4u, cy = texel / 4u;
+    const bool hb = cx == 0u || cx == 3u;
+    const bool vb = cy == 0u || cy == 3u;
+    if (hb && vb) return 0.02221812f;
+    if (hb || vb) return 0.06578385f;
+    return 0.09621418f;
+}
+
+// surface_probe_hemi_oct_encode + radial texel, surface_probes.slang:134-167.
+__device__ __forceinline__ uint32_t radial_texel(f3 d) {
+    f3 h = mk3(d.x, d.y, maxf(d.z, 0.0f));
+    const float l2 = dot3(h, h);
+    float u = 0.5f, v = 0.5f;
+    if (!(l2 <= 1e-12f)) {
+        h = h * (1.0f / sqrtf(l2));
+        const float inv_l1 = 1.0f / maxf((fabsf(h.x) + fabsf(h.y)) + h.z, 1e-6f);
+        const float ox = h.x * inv_l1, oy = h.y * inv_l1;
+        u = sat((ox + oy) * 0.5f + 0.5f);
+        v = sat((ox - oy) * 0.5f + 0.5f);
+    }
+    const uint32_t x = min((uint32_t)(sat(u) * 4.0f), 3u);
+    const uint32_t y = min((uint32_t)(sat(v) * 4.0f), 3u);
+    return y * 4u + x;
+}
+
+struct ProbeOut {
+    float* values;
+    uint32_t* counts;
+    uint32_t* self_hits;
+    uint32_t* radial;
+};
+
+// accumulate_radial_moment, surface_probe_path_tracer.slang:111-149.
+__device__ __forceinline__ void accumulate_radial_moment(uint32_t* __restrict__ radial, uint32_t probe, uint32_t texel,
+                                                         float nd, uint32_t prev_iter, uint32_t local_count,
+                                                         uint32_t spp) {
+    uint32_t* slot = radial + 16u * probe + texel;
+    const uint32_t packed = *slot;
+    float px = __half2float(__ushort_as_half((unsigned short)(packed & 0xffffu)));
+    float py = __half2float(__ushort_as_half((unsigned short)(packed >> 16)));
+    const float sample = minf(maxf(nd, 0.0f), 2.0f);
+    const float smx = sample, smy = sample * sample;
+    if (py <= 0.0f) {
+        px = smx;
+        py = smy;
+    } else {
+        const float pop = ((float)prev_iter * (float)max(spp, 1u)) * radial_texel_cosine_probability(texel);
+        const uint32_t expected = prev_iter == 0u ? local_count - 1u : max((uint32_t)pop, 1u);
+        const float alpha = 1.0f / (float)max(min(expected + local_count, 4096u), 1u);
+        px = px + alpha * (smx - px);
+        py = py + alpha * (smy - py);
+    }
+    px = minf(maxf(px, 0.0f), 4.0f);
+    py = minf(maxf(py, 0.0f), 4.0f);
+    *slot = (uint32_t)__half_as_ushort(__float2half_rn(px)) | ((uint32_t)__half_as_ushort(__float2half_rn(py)) << 16);
+}
+
+__global__ void __launch_bounds__(128) k_trace_probes(SceneView s, LightingRaw lraw, ProbeOut out,
+                                                      const float4* __restrict__ probes,
+                                                      const float4* __restrict__ pinst, uint32_t probe_count,
+                                                      uint32_t iteration, uint32_t spp, uint32_t max_bounces,
+                                                      int reset, uint32_t begin, uint32_t end,
+                                                      unsigned long long* counters) {
+    const uint32_t p = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= end || p >= probe_count) return;
+    const float4 nrm = __ldg(probes + 3u * p + 1u);
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(probes) + 3u * p + 2u);
+    const uint32_t inst = meta.w >> 8;
+    const float4 params = __ldg(pinst + 3u * inst + 2u);
+    const float bx = __uint_as_float(meta.y), by = __uint_as_float(meta.z);
+    const uint32_t prim = meta.x;
+    const uint32_t n = max(spp, 1u);
+    Rng rng(p, inst, iteration * n);
+    const f3 view = normalize3(mk3(nrm.x, nrm.y, nrm.z));
+    const float kr = maxf(params.x, 1e-6f);
+    const LightParams L = make_light(lraw);
+    RayTally tally{0u, 0u};
+    const Shading sd = shading_data(s, inst, prim, bx, by, view);
+    f3 irr = mk3(0.0f, 0.0f, 0.0f);
+    uint32_t self_total = 0u;
+    const uint32_t prev_iter = reset ? 0u : out.counts[p];
+    uint32_t local_counts[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) local_counts[t] = 0u;
+    if (reset)
+        for (int t = 0; t < 16; ++t) out.radial[16u * p + (uint32_t)t] = 0u;
+    const Frame surface_frame(normalize3(sd.face_normal));
+    for (uint32_t k = 0; k < n; ++k) {
+        f3 si = mk3(0.0f, 0.0f, 0.0f);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 dir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf > 1e-6f) {
+            f3 o = sd.origin_front;
+            f3 d = surface_frame.to_global(dir);
+            f3 thp = mk3(1.0f, 1.0f, 1.0f), rad = mk3(0.0f, 0.0f, 0.0f);
+            uint32_t src_inst = inst, src_prim = prim;
+            float src_off = len3(o - sd.position);
+            uint32_t self_hits = 0u;
+            const float radial_max = 2.0f * kr;
+            float first_hit = 2.0f * kr;
+            // trace_radiance, surface_probe_path_tracer.slang:151-204
+            for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+                const HitInfo hit = closest(s, o, d, 0.0f, L.t_max, tally);
+                if (!hit.valid) {
+                    if (bounce == 0u) first_hit = radial_max;
+                    rad = rad + thp * L.sky;
+                    break;
+                }
+                if (bounce == 0u) first_hit = minf(hit.t, radial_max);
+                const uint2 ref = __ldg(s.tri_refs + hit.flat);
+                const bool same_prim = ref.x == src_inst && ref.y == src_prim;
+                const float thr = maxf(4.0f * src_off, 1e-6f);
+                const bool adjacent = ref.x == src_inst && hit.t <= thr;
+                if (same_prim || adjacent) self_hits += 1u;
+                const Shading hs = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -d);
+                rad = rad + thp * hs.emissive;
+                const float u0 = rng.next_1d(), u1 = rng.next_1d();
+                rad = rad + thp * sun_nee(s, L, hs, u0, u1, tally);
+                const float f0 = rng.next_1d(), f1 = rng.next_1d();
+                float spdf;
+                const f3 sdir = cosine_sample_hemisphere(f0, f1, &spdf);
+                if (spdf <= 1e-6f) break;
+                const f3 f = hs.diffuse * kInvPi;
+                thp = thp * ((f * fabsf(sdir.z)) / spdf);
+                const f3 next_origin = hs.origin_front;
+                d = Frame(normalize3(hs.face_normal)).to_global(sdir);
+                o = next_origin;
+                src_inst = ref.x;
+                src_prim = ref.y;
+                src_off = len3(next_origin - hs.position);
+            }
+            self_total += self_hits;
+            const uint32_t texel = radial_texel(dir);
+            local_counts[texel] += 1u;
+            accumulate_radial_moment(out.radial, p, texel, first_hit / maxf(kr, 1e-6f), prev_iter,
+                                     local_counts[texel], spp);
+            si = si + ((rad * fabsf(dir.z)) / pdf);
+        }
+        irr = irr + si;
+    }
+    irr = irr / (float)n;
+    // store_accumulated_irradiance (:47-65)
+    const uint32_t prev = reset ? 0u : out.counts[p];
+    f3 pv = mk3(0.0f, 0.0f, 0.0f);
+    if (prev != 0u) pv = mk3(out.values[3u * p], out.values[3u * p + 1u], out.values[3u * p + 2u]);
+    const float weight = 1.0f / (float)(prev + 1u);
+    const f3 acc = pv + weight * (irr - pv);
+    out.values[3u * p] = acc.x;
+    out.values[3u * p + 1u] = acc.y;
+    out.values[3u * p + 2u] = acc.z;
+    out.counts[p] = min(prev + 1u, 65535u);
+    // store_accumulated_self_hit_count (:67-79)
+    const uint32_t prev_self = reset ? 0u : out.self_hits[p];
+    out.self_hits[p] = prev_self + self_total;
+    flush_tally(counters, tally, 1u, n);
+}
+
+// ---------------------------------------------------------------------------
+// RGB9E5: mesh_colors.slang:218-253 and mesh_colors_rgb9e5_pack.slang:7-16.
+// floor(log2(max)) is taken exactly from the binary exponent.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack_rgb9e5(float r, float g, float b) {
+    const float kMax = 65408.0f;
+    float v[3] = {isnan(r) ? 0.0f : r, isnan(g) ? 0.0f : g, isnan(b) ? 0.0f : b};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = fminf(fmaxf(v[i], 0.0f), kMax);
+    const float m = fmaxf(v[0], fmaxf(v[1], v[2]));
+    if (m < 0x1p-25f) return 0u;
+    const int e2 = (int)((__float_as_uint(m) >> 23) & 0xffu) - 126;  // m is normal here
+    const int exponent = max(-15, e2);
+    uint32_t shared = (uint32_t)(exponent + 15);
+    float scale = __uint_as_float((uint32_t)((int)shared - 24 + 127) << 23);
+    uint32_t mant[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) mant[i] = (uint32_t)floorf(v[i] / scale + 0.5f);
+    if (max(mant[0], max(mant[1], mant[2])) == 512u && shared < 31u) {
+        shared += 1u;
+        scale *= 2.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) mant[i] = (uint32_t)floorf(v[i] / scale + 0.5f);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) mant[i] = min(mant[i], 511u);
+    return mant[0] | (mant[1] << 9) | (mant[2] << 18) | (shared << 27);
+}
+
+__global__ void k_pack_rgb9e5(const uint4* __restrict__ slots, uint32_t* __restrict__ out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 s = slots[i];
+    out[i] = pack_rgb9e5(__uint_as_float(s.x), __uint_as_float(s.y), __uint_as_float(s.z));
+}
+
+uint32_t blocks_for(uint64_t n, uint32_t threads) { return (uint32_t)((n + threads - 1) / threads); }
+
+LightingRaw to_raw(const NanLighting* l) {
+    LightingRaw r;
+    static_assert(sizeof(LightingRaw) == sizeof(NanLighting), "lighting layout");
+    memcpy(&r, l, sizeof(r));
+    return r;
+}
+
+}  // namespace
+
+namespace nan_host {
+
+int launch_intersect(NanContext* ctx, const float* rays, uint32_t count, uint32_t* ids, float* tb, cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    k_intersect<<<blocks_for(count, 128), 128, 0, st>>>(scene_view(ctx), reinterpret_cast<const float4*>(rays), count,
+                                                        reinterpret_cast<uint4*>(ids), tb);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "intersect launch");
+}
+
+int launch_occluded(NanContext* ctx, const float* rays, uint32_t count, float* vis, cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    k_occluded<<<blocks_for(count, 128), 128, 0, st>>>(scene_view(ctx), reinterpret_cast<const float4*>(rays), count,
+                                                       vis);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "occluded launch");
+}
+
+int launch_trace_screen(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame, uint32_t max_vertices,
+                        const NanCamera* cam, const NanLighting* light, cudaStream_t st) {
+    if (w == 0 || h == 0) return NAN_OK;
+    CameraRaw c;
+    static_assert(sizeof(CameraRaw) == sizeof(NanCamera), "camera layout");
+    memcpy(&c, cam, sizeof(c));
+    dim3 grid(blocks_for(w, 16), blocks_for(h, 8));
+    k_trace_screen<<<grid, 128, 0, st>>>(scene_view(ctx), to_raw(light), c, reinterpret_cast<float4*>(out), w, h, frame,
+                                         max_vertices, ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "trace_screen launch");
+}
+
+int launch_accumulate(NanContext* ctx, const float* input, float* output, float* history, uint32_t w, uint32_t h,
+                      int reset, cudaStream_t st) {
+    const uint64_t n = (uint64_t)w * h;
+    if (n == 0) return NAN_OK;
+    k_accumulate<<<blocks_for(n, 256), 256, 0, st>>>(reinterpret_cast<const float4*>(input),
+                                                     reinterpret_cast<float4*>(output),
+                                                     reinterpret_cast<float4*>(history), (uint32_t)n, reset);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "accumulate launch");
+}
+
+int launch_trace_texels(NanContext* ctx, const NanMeshColorsDesc* lay, uint8_t* slots, uint32_t iteration,
+                        uint32_t spt, uint32_t max_bounces, int reset, const NanLighting* light, uint32_t begin,
+                        uint32_t end, cudaStream_t st) {
+    if (end <= begin) return NAN_OK;
+    McView mc;
+    mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
+    mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
+    mc.side_infos = reinterpret_cast<const uint2*>(lay->side_infos);
+    mc.surface_prefix = lay->surface_prefix;
+    mc.instance_count = lay->instance_count;
+    mc.payload_count = lay->payload_count;
+    k_trace_texels<<<blocks_for(end - begin, 128), 128, 0, st>>>(scene_view(ctx), to_raw(light), mc,
+                                                                  reinterpret_cast<uint4*>(slots), iteration, spt,
+                                                                  max_bounces, reset, begin, end, ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "trace_texels launch");
+}
+
+int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits, uint32_t* radial,
+                        const uint8_t* probes, uint32_t probe_count, const uint8_t* probe_instances,
+                        uint32_t probe_instance_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces,
+                        int reset, const NanLighting* light, uint32_t begin, uint32_t end, cudaStream_t st) {
+    (void)probe_instance_count;
+    end = std::min(end, probe_count);
+    if (end <= begin) return NAN_OK;
+    ProbeOut o{values, counts, self_hits, radial};
+    k_trace_probes<<<blocks_for(end - begin, 128), 128, 0, st>>>(
+        scene_view(ctx), to_raw(light), o, reinterpret_cast<const float4*>(probes),
+        reinterpret_cast<const float4*>(probe_instances), probe_count, iteration, spp, max_bounces, reset, begin, end,
+        ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "trace_probes launch");
+}
+
+int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    k_pack_rgb9e5<<<blocks_for(count, 256), 256, 0, st>>>(reinterpret_cast<const uint4*>(slots), out, count);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "pack_rgb9e5 launch");
+}
+
+}  // namespace nan_host

@@ -1,0 +1,231 @@
+"""Mesh Colors layout (host side): mesh_colors.py:24-337 of the reference.
+
+Each triangle gets a power-of-two lattice resolution R from its longest
+world-space edge, R = min(nextpow2(max(min_res, ceil(edge * texels_per_unit))),
+max_res), and (R+1)(R+2)/2 texels. Instances are laid out front range first,
+then (for double-sided materials) a back range of the same size. When the
+running total would exceed the texel budget, later triangles are halved
+greedily toward min_res (mesh_colors.py:231-251), and a layout that cannot
+fit raises ValueError("Mesh Colors texel budget exceeded ...").
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+MESH_COLORS_PAYLOAD_SIZE = 16
+MESH_COLORS_INVALID_OFFSET = 0xFFFFFFFF
+MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED = 1 << 0
+
+
+def colors_per_patch(resolution: int) -> int:
+    resolution = int(resolution)
+    if resolution < 1:
+        raise ValueError("resolution must be positive")
+    return (resolution + 1) * (resolution + 2) // 2
+
+
+def address_to_ij(address: int, resolution: int) -> tuple[int, int]:
+    """Triangle-local linear address -> lattice (i, j) (closed form + fix-up)."""
+    address, resolution = int(address), int(resolution)
+    if address < 0 or address >= colors_per_patch(resolution):
+        raise ValueError("address is outside the triangle patch")
+    b = 2 * resolution + 3
+    i = int((b - math.sqrt(b * b - 8 * address)) * 0.5)
+    cumulative = i * (resolution + 1) - i * (i - 1) // 2
+    while cumulative > address:
+        i -= 1
+        cumulative = i * (resolution + 1) - i * (i - 1) // 2
+    while i < resolution:
+        nxt = (i + 1) * (resolution + 1) - (i + 1) * i // 2
+        if nxt > address:
+            break
+        i += 1
+        cumulative = nxt
+    return i, address - cumulative
+
+
+def ij_to_address(i: int, j: int, resolution: int) -> int:
+    i, j, resolution = int(i), int(j), int(resolution)
+    if i < 0 or i > resolution or j < 0 or j > resolution - i:
+        raise ValueError("(i, j) is outside the triangle patch")
+    return i * (resolution + 1) - i * (i - 1) // 2 + j
+
+
+def barycentric_at(i: int, j: int, resolution: int) -> tuple[float, float, float]:
+    if resolution <= 0:
+        raise ValueError("resolution must be positive")
+    u = float(i) / float(resolution)
+    v = float(j) / float(resolution)
+    return u, v, 1.0 - u - v
+
+
+def next_power_of_two(value: int) -> int:
+    value = max(1, int(value))
+    return 1 << (value - 1).bit_length()
+
+
+def previous_power_of_two(value: int) -> int:
+    value = max(1, int(value))
+    return 1 << (value.bit_length() - 1)
+
+
+@dataclass(frozen=True)
+class MeshColorsFaceInfo:
+    address: int
+    resolution: int
+
+
+@dataclass(frozen=True)
+class MeshColorsInstanceInfo:
+    face_offset: int
+    face_count: int
+    texel_offset: int
+    texel_count: int
+
+
+@dataclass(frozen=True)
+class MeshColorsSideInfo:
+    back_texel_offset: int
+    flags: int
+
+    @property
+    def is_double_sided(self) -> bool:
+        return bool(self.flags & MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED)
+
+
+def _patch(r: np.ndarray) -> np.ndarray:
+    r = r.astype(np.int64)
+    return (r + 1) * (r + 2) // 2
+
+
+class MeshColorsLayout:
+    """Layout arrays: face_infos u32[F,2], instance_infos u32[I,4], side_infos u32[I,2]."""
+
+    def __init__(self, face_infos, instance_infos, side_infos, total_surface_texels, total_payload_count,
+                 texels_per_unit, min_resolution, max_resolution):
+        self.face_array = np.ascontiguousarray(face_infos, dtype=np.uint32).reshape(-1, 2)
+        self.instance_array = np.ascontiguousarray(instance_infos, dtype=np.uint32).reshape(-1, 4)
+        self.side_array = np.ascontiguousarray(side_infos, dtype=np.uint32).reshape(-1, 2)
+        self.total_surface_texels = int(total_surface_texels)
+        self.total_payload_count = int(total_payload_count)
+        self.texels_per_unit = float(texels_per_unit)
+        self.min_resolution = int(min_resolution)
+        self.max_resolution = int(max_resolution)
+
+    @property
+    def total_texel_count(self) -> int:
+        return self.total_surface_texels
+
+    @property
+    def face_infos(self) -> tuple:
+        return tuple(MeshColorsFaceInfo(int(a), int(r)) for a, r in self.face_array)
+
+    @property
+    def instance_infos(self) -> tuple:
+        return tuple(MeshColorsInstanceInfo(*(int(x) for x in row)) for row in self.instance_array)
+
+    @property
+    def side_infos(self) -> tuple:
+        return tuple(MeshColorsSideInfo(int(a), int(f)) for a, f in self.side_array)
+
+    @property
+    def surface_prefix(self) -> np.ndarray:
+        """Exclusive prefix of the instances' surface texel counts, u32[I+1]."""
+        counts = self.instance_array[:, 3].astype(np.int64)
+        return np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+
+    @classmethod
+    def build(cls, scene_node, *, texels_per_unit: float = 16.0, min_resolution: int = 4,
+              max_resolution: int = 64, max_total_texels: int = 16_777_216) -> "MeshColorsLayout":
+        texels_per_unit = max(float(texels_per_unit), 1e-6)
+        min_resolution = next_power_of_two(max(1, int(min_resolution)))
+        max_resolution = previous_power_of_two(max(1, int(max_resolution)))
+        if min_resolution > max_resolution:
+            raise ValueError(
+                "Mesh Colors min_resolution must not exceed max_resolution after power-of-two normalization"
+            )
+        max_total_texels = max(1, int(max_total_texels))
+        faces, instances, sides = [], [], []
+        total_surface = 0
+        total_payload = 0
+        for mesh_id, material_id, transform_id in scene_node.instances:
+            mesh = scene_node.meshes[mesh_id]
+            material = scene_node.materials[material_id]
+            double_sided = bool(getattr(material, "double_sided", False))
+            mult = 2 if double_sided else 1
+            m = np.asarray(scene_node.transforms[transform_id], dtype=np.float32)
+            p = mesh.vertices[:, 0:3].astype(np.float32)
+            world = (p @ m[:3, :3].T + m[:3, 3]).astype(np.float32).astype(np.float64)
+            tri = world[mesh.indices.astype(np.int64)]  # [T,3,3]
+            e = np.stack([
+                np.linalg.norm(tri[:, 1] - tri[:, 0], axis=1),
+                np.linalg.norm(tri[:, 2] - tri[:, 1], axis=1),
+                np.linalg.norm(tri[:, 0] - tri[:, 2], axis=1),
+            ], axis=1).max(axis=1)
+            want = np.maximum(min_resolution, np.ceil(e * texels_per_unit)).astype(np.int64)
+            want = np.maximum(want, 1)
+            res = np.left_shift(1, np.ceil(np.log2(want)).astype(np.int64))
+            res = np.where(res < want, res * 2, res)  # guard log2 rounding
+            res = np.minimum(res, max_resolution)
+            patch = _patch(res)
+            cum = np.cumsum(patch)
+            face_offset = len(faces) and sum(len(f) for f in faces)
+            if mesh.triangle_count and total_payload + int(cum[-1]) * mult > max_total_texels:
+                res = res.copy()
+                local = 0
+                for k in range(mesh.triangle_count):
+                    r = int(res[k])
+                    pt = colors_per_patch(r)
+                    if total_payload + (local + pt) * mult > max_total_texels:
+                        cand = r
+                        fitted = False
+                        while cand > min_resolution:
+                            cand //= 2
+                            pt = colors_per_patch(cand)
+                            if total_payload + (local + pt) * mult <= max_total_texels:
+                                r = cand
+                                fitted = True
+                                break
+                        if not fitted:
+                            raise ValueError(
+                                "Mesh Colors texel budget exceeded; lower --texture-space-texels-per-unit "
+                                "or --texture-space-min-resolution, or increase --texture-space-max-texels"
+                            )
+                    res[k] = r
+                    local += pt
+                patch = _patch(res)
+                cum = np.cumsum(patch)
+            addresses = (cum - patch).astype(np.uint32)
+            faces.append(np.stack([addresses, res.astype(np.uint32)], axis=1))
+            local_total = int(cum[-1]) if mesh.triangle_count else 0
+            instances.append((face_offset, mesh.triangle_count, total_payload, local_total))
+            back = total_payload + local_total if double_sided else MESH_COLORS_INVALID_OFFSET
+            sides.append((back, MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED if double_sided else 0))
+            total_surface += local_total
+            total_payload += local_total * mult
+        if total_surface == 0:
+            raise ValueError("Texture-space rendering requires at least one triangle")
+        face_array = np.concatenate(faces, axis=0) if faces else np.zeros((0, 2), np.uint32)
+        return cls(face_array, np.asarray(instances, dtype=np.uint32), np.asarray(sides, dtype=np.uint32),
+                   total_surface, total_payload, texels_per_unit, min_resolution, max_resolution)
+
+    def create_gpu_buffers(self, device):
+        """(face_infos, instance_infos, side_infos, surface_prefix) as int32 CUDA tensors."""
+        import torch
+
+        td = device.torch_device if hasattr(device, "torch_device") else device
+        def up(a):
+            return torch.from_numpy(np.ascontiguousarray(a).view(np.int32)).to(td)
+        return up(self.face_array), up(self.instance_array), up(self.side_array), up(self.surface_prefix)
+
+    def units(self) -> np.ndarray:
+        """Every (instance, instance-local texel) pair in surface-texel order, u32[N,2]."""
+        counts = self.instance_array[:, 3].astype(np.int64)
+        inst = np.repeat(np.arange(len(counts), dtype=np.uint32), counts)
+        local = np.arange(int(counts.sum()), dtype=np.int64) - np.repeat(self.surface_prefix[:-1].astype(np.int64),
+                                                                         counts)
+        return np.stack([inst, local.astype(np.uint32)], axis=1)

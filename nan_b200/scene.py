@@ -1,0 +1,174 @@
+"""Device, lighting and the GPU scene (the reference's Scene, scene.py:32-1382).
+
+``Scene(device, scene_node)`` uploads the scene in the reference's record
+layouts as torch tensors (buffers only) and builds the BVH on the GPU through
+``nan_scene_build``. The tensors stay alive as long as the Scene, because the
+shading code reads them in place.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from ._native import NanLighting, NanSceneDesc, NanSceneInfo, check, lib, ptr, stream_handle
+from .scene_node import SceneNode
+
+
+class Device:
+    """One CUDA device plus the native context used by every pass on it."""
+
+    def __init__(self, index: int = 0):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("nan_b200 needs a CUDA device (there is no CPU path)")
+        self.index = int(index)
+        self.torch_device = torch.device("cuda", self.index)
+        self.context = _native.Context(self.index)
+
+    def synchronize(self) -> None:
+        import torch
+
+        torch.cuda.synchronize(self.torch_device)
+
+    def check(self, stream=None) -> None:
+        """Raise if a kernel reported a device-side limit since the last check."""
+        self.context.check(stream)
+
+
+@dataclass
+class Lighting:
+    """Directional sun + constant sky.
+
+    Defaults follow Scene.__init__ (scene.py:135-147): sun toward
+    (0, 0.5, 0.866), color white, intensity pi, half apex angle 0.26785 deg.
+    The sky-view and transmittance LUTs are replaced by constants.
+    """
+
+    sun_direction: tuple = (0.0, 0.5, 0.866)
+    sun_cos_half_angle: float = math.cos(math.radians(0.5357 / 2.0))
+    sun_color: tuple = (1.0, 1.0, 1.0)
+    sun_intensity: float = math.pi
+    sun_transmittance: tuple = (1.0, 1.0, 1.0)
+    ray_t_max: float = 1000.0
+    sky_radiance: tuple = (0.0, 0.0, 0.0)
+    sun_disk: bool = True
+
+    def __post_init__(self):
+        d = np.asarray(self.sun_direction, dtype=np.float64)
+        n = np.linalg.norm(d)
+        self.sun_direction = tuple(float(x) for x in (d / n if n > 0 else d))
+
+    @property
+    def flags(self) -> int:
+        return 1 if self.sun_disk else 0
+
+    def to_struct(self) -> NanLighting:
+        s = NanLighting()
+        s.sun_direction[:] = [float(x) for x in self.sun_direction]
+        s.sun_cos_half_angle = float(self.sun_cos_half_angle)
+        s.sun_color[:] = [float(x) for x in self.sun_color]
+        s.sun_intensity = float(self.sun_intensity)
+        s.sun_transmittance[:] = [float(x) for x in self.sun_transmittance]
+        s.ray_t_max = float(self.ray_t_max)
+        s.sky_radiance[:] = [float(x) for x in self.sky_radiance]
+        s.flags = self.flags
+        return s
+
+    @classmethod
+    def sun_elevation(cls, elevation_deg: float, azimuth_deg: float = 0.0, irradiance: float = 3.0,
+                      sky: float = 0.5, **kw) -> "Lighting":
+        """Sun at the given elevation with color*intensity = irradiance."""
+        e, a = math.radians(elevation_deg), math.radians(azimuth_deg)
+        direction = (math.cos(e) * math.sin(a), math.sin(e), math.cos(e) * math.cos(a))
+        return cls(sun_direction=direction, sun_intensity=irradiance, sky_radiance=(sky, sky, sky), **kw)
+
+
+class Scene:
+    """Scene buffers on the GPU + BVH (replaces Scene.__init__/bind)."""
+
+    def __init__(self, device: Device, scene_node: SceneNode, lighting: Lighting | None = None, stream=None):
+        import torch
+
+        self.device = device
+        self.scene_node = scene_node
+        self.camera = scene_node.camera
+        self.lighting = lighting or scene_node.lighting or Lighting()
+        self.frame_index = 0
+        packed = scene_node.pack()
+        self.host = packed
+        td = device.torch_device
+        self.vertices = torch.from_numpy(packed["vertices"]).to(td)
+        self.indices = torch.from_numpy(packed["indices"].view(np.int32)).to(td)
+        self.mesh_descs = torch.from_numpy(packed["mesh_descs"].view(np.int32)).to(td)
+        self.instance_descs = torch.from_numpy(packed["instance_descs"].view(np.int32)).to(td)
+        self.transforms = torch.from_numpy(packed["transforms"]).to(td)
+        self.inverse_transposes = torch.from_numpy(packed["inverse_transposes"]).to(td)
+        self.materials = torch.from_numpy(packed["materials"]).to(td)
+        desc = NanSceneDesc()
+        desc.vertices = ptr(self.vertices)
+        desc.vertex_count = packed["vertices"].shape[0]
+        desc.indices = ptr(self.indices)
+        desc.index_triangle_count = packed["indices"].shape[0]
+        desc.mesh_descs = ptr(self.mesh_descs)
+        desc.mesh_count = packed["mesh_descs"].shape[0]
+        desc.instance_descs = ptr(self.instance_descs)
+        desc.instance_count = packed["instance_descs"].shape[0]
+        desc.transforms = ptr(self.transforms)
+        desc.inverse_transposes = ptr(self.inverse_transposes)
+        desc.transform_count = packed["transforms"].shape[0]
+        desc.materials = ptr(self.materials)
+        desc.material_count = packed["materials"].shape[0]
+        self._desc = desc
+        check(lib().nan_scene_build(device.context.handle, ctypes.byref(desc), stream_handle(stream)))
+
+    @property
+    def context(self) -> _native.Context:
+        return self.device.context
+
+    def info(self) -> dict:
+        info = NanSceneInfo()
+        check(lib().nan_scene_info(self.context.handle, ctypes.byref(info)))
+        return {name: getattr(info, name) for name, _ in NanSceneInfo._fields_}
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.info()["triangle_count"])
+
+    def update(self) -> None:
+        """Per-frame update (scene.py:1213-1216)."""
+        self.frame_index += 1
+
+    def world_triangles(self):
+        import torch
+
+        n = self.triangle_count
+        out = torch.empty((n, 9), dtype=torch.float32, device=self.device.torch_device)
+        check(lib().nan_scene_world_triangles(self.context.handle, ptr(out), stream_handle(None)))
+        return out
+
+    def intersect(self, rays, stream=None):
+        """Closest hit of rays f32[N,8] -> (ids i32[N,4], tb f32[N,3])."""
+        import torch
+
+        rays = rays.contiguous()
+        n = rays.shape[0]
+        ids = torch.empty((n, 4), dtype=torch.int32, device=rays.device)
+        tb = torch.empty((n, 3), dtype=torch.float32, device=rays.device)
+        check(lib().nan_intersect(self.context.handle, ptr(rays), n, ptr(ids), ptr(tb), stream_handle(stream)))
+        return ids, tb
+
+    def occluded(self, rays, stream=None):
+        """Visibility (1 = unoccluded) of rays f32[N,8]."""
+        import torch
+
+        rays = rays.contiguous()
+        n = rays.shape[0]
+        vis = torch.empty((n,), dtype=torch.float32, device=rays.device)
+        check(lib().nan_occluded(self.context.handle, ptr(rays), n, ptr(vis), stream_handle(stream)))
+        return vis

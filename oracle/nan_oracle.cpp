@@ -1,0 +1,1513 @@
+// nan_oracle.cpp -- CPU restatement of the reference's path integration.
+//
+// TEST INFRASTRUCTURE ONLY (the checker, never the product): see
+// nan_oracle.h. Citations are path:line inside the reference project.
+//
+// Arithmetic convention of the float "spec" mode (the Slang source leaves
+// fusion and a few intrinsics to the driver; this fixes one reading of it):
+//   * a*b+c written in Slang is an unfused multiply then add; only Slang's
+//     explicit mad() is a fused multiply-add (fmaf);
+//   * dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z; vector sums are left to right;
+//   * normalize(v) = v * (1/sqrt(dot(v,v))), rsqrt(x) = 1/sqrt(x), both with
+//     correctly rounded sqrt and division;
+//   * lerp(a,b,s) = a + s*(b - a);
+//   * sin/cos come from own_sincos() below (Cody-Waite reduction by pi/2 and
+//     the Taylor polynomials of sin/cos), not from a math library, so the
+//     CPU and GPU produce the same bits;
+//   * floor(log2(x)) in the RGB9E5 pack is the exact binary exponent (frexp).
+// Intersection is the watertight ray/triangle test of Woop, Benthin and Wald
+// (JCGT 2013) against world-space triangles, with the closest hit chosen by
+// (t, flat triangle index) so ties on shared edges resolve the same way in
+// any traversal order.
+
+#include "nan_oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+// ---------------------------------------------------------------------------
+// Scalar operations per precision.
+// ---------------------------------------------------------------------------
+
+// sin/cos of a float angle by Cody-Waite reduction (two-part pi/2) and the
+// degree-9 / degree-10 Taylor polynomials on |r| <= pi/4 (truncation error
+// below 3e-9, under half an ulp of the result).
+void own_sincos(float a, float* s, float* c) {
+    const float two_over_pi = 0.636619772367581343f;
+    const float pio2_hi = 1.57079637050628662109375f;
+    const float pio2_lo = -4.37113900018624283e-8f;
+    float kf = std::rint(a * two_over_pi);
+    int k = (int)kf;
+    float r = std::fmaf(-kf, pio2_hi, a);
+    r = std::fmaf(-kf, pio2_lo, r);
+    float r2 = r * r;
+    float ps = std::fmaf(r2, 2.75573192239858907e-6f, -1.98412698412698413e-4f);
+    ps = std::fmaf(r2, ps, 8.33333333333333333e-3f);
+    ps = std::fmaf(r2, ps, -1.66666666666666667e-1f);
+    float sn = std::fmaf(r * r2, ps, r);
+    float pc = std::fmaf(r2, -2.75573192239858907e-7f, 2.48015873015873016e-5f);
+    pc = std::fmaf(r2, pc, -1.38888888888888889e-3f);
+    pc = std::fmaf(r2, pc, 4.16666666666666667e-2f);
+    pc = std::fmaf(r2, pc, -0.5f);
+    float cs = std::fmaf(r2, pc, 1.0f);
+    switch (k & 3) {
+        case 0: *s = sn; *c = cs; break;
+        case 1: *s = cs; *c = -sn; break;
+        case 2: *s = -sn; *c = -cs; break;
+        default: *s = -cs; *c = sn; break;
+    }
+}
+
+template <class T> struct Ops;
+template <> struct Ops<float> {
+    static float fma(float a, float b, float c) { return std::fmaf(a, b, c); }
+    static float sqrt(float a) { return std::sqrt(a); }
+    static void sincos(float a, float* s, float* c) { own_sincos(a, s, c); }
+};
+template <> struct Ops<double> {
+    static double fma(double a, double b, double c) { return std::fma(a, b, c); }
+    static double sqrt(double a) { return std::sqrt(a); }
+    static void sincos(double a, double* s, double* c) {
+        *s = std::sin(a);
+        *c = std::cos(a);
+    }
+};
+
+template <class T> struct V3 {
+    T x, y, z;
+    T operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+template <class T> V3<T> mk(T x, T y, T z) { return V3<T>{x, y, z}; }
+template <class T> V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> V3<T> operator*(V3<T> a, V3<T> b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <class T> V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> V3<T> operator/(V3<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class T> V3<T> operator-(V3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <class T> T dot(V3<T> a, V3<T> b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+template <class T> V3<T> cross(V3<T> a, V3<T> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T> V3<T> vabs(V3<T> a) { return {std::fabs(a.x), std::fabs(a.y), std::fabs(a.z)}; }
+template <class T> T length(V3<T> a) { return Ops<T>::sqrt(dot(a, a)); }
+template <class T> V3<T> normalize(V3<T> a) { return a * (T(1) / Ops<T>::sqrt(dot(a, a))); }
+template <class T> T vmax(T a, T b) { return a > b ? a : b; }  // HLSL max for non-NaN
+template <class T> T vmin(T a, T b) { return a < b ? a : b; }
+template <class T> T saturate(T a) { return vmin(vmax(a, T(0)), T(1)); }
+
+template <class T> struct Consts;
+template <> struct Consts<float> {
+    static constexpr float PI = 3.14159265358979323846f;
+    static constexpr float TWO_PI = 6.28318530717958647692f;
+    static constexpr float INV_PI = 0.31830988618379067154f;
+};
+template <> struct Consts<double> {
+    static constexpr double PI = 3.14159265358979323846;
+    static constexpr double TWO_PI = 6.28318530717958647692;
+    static constexpr double INV_PI = 0.31830988618379067154;
+};
+
+// ---------------------------------------------------------------------------
+// RNG: common.slang:164-210 (LCG, not PCG).
+// ---------------------------------------------------------------------------
+struct Rng {
+    uint32_t state;
+    Rng(uint32_t x, uint32_t y, uint32_t sample_index)
+        : state((x * 100591u) ^ (y * 102191u) ^ (sample_index * 103643u)) {}
+    uint32_t next() {
+        state = 1664525u * state + 1013904223u;
+        return state;
+    }
+    float next_1d() { return (float)(next() >> 8) * 0x1p-24f; }
+};
+
+// ---------------------------------------------------------------------------
+// Sampling and frames: common.slang:54-68, 139-162, 452-470, 475-490.
+// ---------------------------------------------------------------------------
+template <class T> struct Frame {
+    V3<T> n, t, b;
+    explicit Frame(V3<T> nn) {  // common.slang:145-151 (Spencer & Jones eq. 3)
+        n = nn;
+        t = normalize(cross(nn, mk<T>(-nn.z, nn.x, -nn.y)));
+        b = cross(nn, t);
+    }
+    V3<T> to_local(V3<T> w) const { return {dot(t, w), dot(b, w), dot(n, w)}; }
+    V3<T> to_global(V3<T> w) const { return (w.x * t + w.y * b) + w.z * n; }
+};
+
+// common.slang:54-68
+template <class T> void cosine_sample_hemisphere(T ex, T ey, V3<T>* h, T* pdf) {
+    T phi = T(2) * Consts<T>::PI * ex;
+    T cos_theta = Ops<T>::sqrt(ey);
+    T sin_theta = Ops<T>::sqrt(T(1) - cos_theta * cos_theta);
+    T s, c;
+    Ops<T>::sincos(phi, &s, &c);
+    *h = mk<T>(sin_theta * c, sin_theta * s, cos_theta);
+    *pdf = cos_theta * (T(1) / Consts<T>::PI);
+}
+
+// common.slang:452-470
+template <class T> V3<T> sample_cone_direction(V3<T> axis, T cos_half, T ux, T uy) {
+    T cos_theta = T(1) - ux * (T(1) - cos_half);
+    T sin_theta = Ops<T>::sqrt(vmax(T(0), T(1) - cos_theta * cos_theta));
+    T phi = Consts<T>::TWO_PI * uy;
+    T s, c;
+    Ops<T>::sincos(phi, &s, &c);
+    V3<T> local = mk<T>(c * sin_theta, s * sin_theta, cos_theta);
+    return Frame<T>(axis).to_global(local);
+}
+
+// HLSL reflect(i, n) = i - 2*dot(n, i)*n
+template <class T> V3<T> reflect(V3<T> i, V3<T> n) { return i - (T(2) * dot(n, i)) * n; }
+
+// common.slang:475-490
+template <class T> V3<T> adjust_shading_normal(V3<T> sn, V3<T> gn, V3<T> d) {
+    V3<T> r = reflect(d, sn);
+    T k = dot(r, gn);
+    if (k < T(0)) return normalize(normalize(r - k * gn) - d);
+    return sn;
+}
+
+// ---------------------------------------------------------------------------
+// RGB9E5: mesh_colors.slang:218-253.
+// ---------------------------------------------------------------------------
+uint32_t pack_rgb9e5(float r, float g, float b) {
+    const float kMax = 65408.0f;
+    float v[3] = {std::isnan(r) ? 0.0f : r, std::isnan(g) ? 0.0f : g, std::isnan(b) ? 0.0f : b};
+    for (float& x : v) x = std::min(std::max(x, 0.0f), kMax);
+    float m = std::max(v[0], std::max(v[1], v[2]));
+    if (m < 0x1p-25f) return 0;
+    int e2 = 0;
+    std::frexp(m, &e2);  // m = f * 2^e2, f in [0.5, 1): floor(log2 m) = e2 - 1
+    int exponent = std::max(-15, e2);
+    uint32_t shared = (uint32_t)(exponent + 15);
+    float scale = std::ldexp(1.0f, (int)shared - 24);
+    uint32_t mant[3];
+    for (int i = 0; i < 3; ++i) mant[i] = (uint32_t)std::floor(v[i] / scale + 0.5f);
+    if (std::max(mant[0], std::max(mant[1], mant[2])) == 512u && shared < 31u) {
+        shared += 1;
+        scale *= 2.0f;
+        for (int i = 0; i < 3; ++i) mant[i] = (uint32_t)std::floor(v[i] / scale + 0.5f);
+    }
+    for (int i = 0; i < 3; ++i) mant[i] = std::min(mant[i], 511u);
+    return mant[0] | (mant[1] << 9) | (mant[2] << 18) | (shared << 27);
+}
+
+void unpack_rgb9e5(uint32_t p, float* out) {
+    float scale = std::ldexp(1.0f, (int)(p >> 27) - 24);
+    out[0] = (float)(p & 0x1ffu) * scale;
+    out[1] = (float)((p >> 9) & 0x1ffu) * scale;
+    out[2] = (float)((p >> 18) & 0x1ffu) * scale;
+}
+
+// IEEE binary32 -> binary16, round to nearest even (f32tof16 in
+// surface_probes.slang:84-96).
+uint16_t f32_to_f16(float f) {
+    uint32_t x;
+    std::memcpy(&x, &f, 4);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    uint32_t ax = x & 0x7fffffffu;
+    if (ax >= 0x7f800000u) return (uint16_t)(sign | (ax > 0x7f800000u ? 0x7e00u : 0x7c00u));
+    if (ax >= 0x477ff000u) return (uint16_t)(sign | 0x7c00u);  // >= 65520 rounds to inf
+    if (ax < 0x38800000u) {  // below the smallest normal half: subnormal or zero
+        if (ax < 0x33000000u) return (uint16_t)sign;  // < 2^-25 rounds to zero
+        uint32_t e = ax >> 23;
+        uint32_t m = (ax & 0x7fffffu) | 0x800000u;
+        uint32_t shift = 126u - e;  // value = m * 2^(e-150); half subnormal unit 2^-24
+        uint32_t q = m >> shift;
+        uint32_t rem = m & ((1u << shift) - 1u);
+        uint32_t half = 1u << (shift - 1);
+        if (rem > half || (rem == half && (q & 1u))) q += 1;
+        return (uint16_t)(sign | q);
+    }
+    uint32_t e = (ax >> 23) - 112u;  // rebias 127 -> 15
+    uint32_t m = ax & 0x7fffffu;
+    uint32_t q = (e << 10) | (m >> 13);
+    uint32_t rem = m & 0x1fffu;
+    if (rem > 0x1000u || (rem == 0x1000u && (q & 1u))) q += 1;  // carry may bump the exponent
+    return (uint16_t)(sign | q);
+}
+
+float f16_to_f32(uint16_t h) {
+    uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+    uint32_t e = (h >> 10) & 0x1fu;
+    uint32_t m = h & 0x3ffu;
+    uint32_t bits;
+    if (e == 0) {
+        if (m == 0) {
+            bits = sign;
+        } else {
+            float v = (float)m * 0x1p-24f;
+            std::memcpy(&bits, &v, 4);
+            bits |= sign;
+        }
+    } else if (e == 31) {
+        bits = sign | 0x7f800000u | (m << 13);
+    } else {
+        bits = sign | ((e + 112u) << 23) | (m << 13);
+    }
+    float out;
+    std::memcpy(&out, &bits, 4);
+    return out;
+}
+
+// ---------------------------------------------------------------------------
+// Hemi-oct mapping: surface_probes.slang:134-167.
+// ---------------------------------------------------------------------------
+void hemi_oct_encode(float dx, float dy, float dz, float* u, float* v) {
+    V3<float> h = mk<float>(dx, dy, vmax(dz, 0.0f));
+    float l2 = dot(h, h);
+    if (l2 <= 1e-12f) {
+        *u = 0.5f;
+        *v = 0.5f;
+        return;
+    }
+    h = h * (1.0f / std::sqrt(l2));
+    float inv_l1 = 1.0f / vmax((std::fabs(h.x) + std::fabs(h.y)) + h.z, 1e-6f);
+    float ox = h.x * inv_l1, oy = h.y * inv_l1;
+    float sx = ox + oy, sy = ox - oy;
+    *u = saturate(sx * 0.5f + 0.5f);
+    *v = saturate(sy * 0.5f + 0.5f);
+}
+
+// Inverse of the encode above (the decode the reference's round-trip test
+// uses): rotate back by 45 degrees and unfold the L1 diamond.
+void hemi_oct_decode(float u, float v, float* out) {
+    double sx = 2.0 * u - 1.0, sy = 2.0 * v - 1.0;
+    double ox = 0.5 * (sx + sy), oy = 0.5 * (sx - sy);
+    double oz = 1.0 - std::fabs(ox) - std::fabs(oy);
+    if (oz < 0.0) oz = 0.0;
+    double len = std::sqrt(ox * ox + oy * oy + oz * oz);
+    out[0] = (float)(ox / len);
+    out[1] = (float)(oy / len);
+    out[2] = (float)(oz / len);
+}
+
+uint32_t radial_texel_index(float u, float v) {  // surface_probes.slang:157-167
+    uint32_t x = std::min((uint32_t)(saturate(u) * 4.0f), 3u);
+    uint32_t y = std::min((uint32_t)(saturate(v) * 4.0f), 3u);
+    return y * 4u + x;
+}
+
+// surface_probe_path_tracer.slang:95-109
+float radial_texel_cosine_probability(uint32_t texel) {
+    uint32_t cx = texel % 4u, cy = texel / 4u;
+    bool hb = cx == 0u || cx == 3u;
+    bool vb = cy == 0u || cy == 3u;
+    if (hb && vb) return 0.02221812f;
+    if (hb || vb) return 0.06578385f;
+    return 0.09621418f;
+}
+
+// ---------------------------------------------------------------------------
+// Mesh Colors lattice: mesh_colors.slang:37-65, 272-363.
+// ---------------------------------------------------------------------------
+struct FaceInfo { uint32_t address, resolution; };
+struct InstInfo { uint32_t face_offset, face_count, texel_offset, texel_count; };
+
+uint32_t patch_texel_count(uint32_t r) { return (r + 1u) * (r + 2u) / 2u; }
+
+uint32_t mc_address(uint32_t i, uint32_t j, const InstInfo& inst, const FaceInfo& f) {
+    uint32_t row = i * (f.resolution + 1u) - i * (i - 1u) / 2u;
+    return inst.texel_offset + f.address + row + j;
+}
+
+void address_to_ij(uint32_t address, uint32_t r, uint32_t* oi, uint32_t* oj) {
+    uint32_t left = 0, right = r;
+    while (left < right) {
+        uint32_t mid = (left + right + 1u) / 2u;
+        uint32_t ma = mid * (r + 1u) - mid * (mid - 1u) / 2u;
+        if (ma <= address) left = mid; else right = mid - 1u;
+    }
+    uint32_t cum = left * (r + 1u) - left * (left - 1u) / 2u;
+    *oi = left;
+    *oj = address - cum;
+}
+
+bool find_face(const uint32_t* face_infos, const InstInfo& inst, uint32_t texel,
+               FaceInfo* out, uint32_t* prim) {
+    out->address = 0;
+    out->resolution = 1;
+    *prim = 0;
+    int left = (int)inst.face_offset;
+    int right = (int)(inst.face_offset + inst.face_count) - 1;
+    while (left <= right) {
+        int mid = (left + right) / 2;
+        out->address = face_infos[2 * mid];
+        out->resolution = face_infos[2 * mid + 1];
+        int local = (int)texel - (int)out->address;
+        int count = (int)patch_texel_count(out->resolution);
+        if (local < 0) right = mid - 1;
+        else if (local >= count) left = mid + 1;
+        else {
+            *prim = (uint32_t)mid - inst.face_offset;
+            return true;
+        }
+    }
+    return false;
+}
+
+float frac(float x) { return x - std::floor(x); }
+
+uint32_t nearest_texel(float b0, float b1, float b2, const InstInfo& inst, const FaceInfo& f) {
+    float rf = (float)f.resolution;
+    float s0 = saturate(b0) * rf, s1 = saturate(b1) * rf, s2 = saturate(b2) * rf;
+    uint32_t i = (uint32_t)s0, j = (uint32_t)s1;
+    i = std::min(i, f.resolution);
+    j = std::min(j, f.resolution - i);
+    float w0 = frac(s0), w1 = frac(s1), w2 = frac(s2);
+    bool upper = std::fabs(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
+    if (upper) { w0 = 1.0f - w0; w1 = 1.0f - w1; w2 = 1.0f - w2; }
+    if ((w0 + w1) + w2 <= 1e-6f || i >= f.resolution || j >= f.resolution - i)
+        return mc_address(i, j, inst, f);
+    float largest = vmax(w0, vmax(w1, w2));
+    if (upper) {
+        if (std::fabs(largest - w0) < 1e-3f) return mc_address(i, j + 1u, inst, f);
+        if (std::fabs(largest - w1) < 1e-3f) return mc_address(i + 1u, j, inst, f);
+        return mc_address(i + 1u, j + 1u, inst, f);
+    }
+    if (std::fabs(largest - w0) < 1e-3f) return mc_address(i + 1u, j, inst, f);
+    if (std::fabs(largest - w1) < 1e-3f) return mc_address(i, j + 1u, inst, f);
+    return mc_address(i, j, inst, f);
+}
+
+// ---------------------------------------------------------------------------
+// Scene: flattened world-space triangles + binned-SAH BVH (8 bins, the
+// tinybvh BVH::Build heuristic: centroid bins, half-area SAH, C_trav = C_int
+// = 1, split only while cheaper than a leaf).
+// ---------------------------------------------------------------------------
+struct Box {
+    float lo[3], hi[3];
+    void reset() {
+        for (int a = 0; a < 3; ++a) { lo[a] = INFINITY; hi[a] = -INFINITY; }
+    }
+    void grow(const float* p) {
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], p[a]); hi[a] = std::max(hi[a], p[a]); }
+    }
+    void grow(const Box& b) {
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], b.lo[a]); hi[a] = std::max(hi[a], b.hi[a]); }
+    }
+    float half_area() const {
+        float e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = hi[2] - lo[2];
+        if (e0 < 0 || e1 < 0 || e2 < 0) return 0.0f;
+        return e0 * e1 + e1 * e2 + e2 * e0;
+    }
+};
+
+struct BvhNode {
+    Box box;
+    uint32_t left_first;  // first child index (interior) or first prim (leaf)
+    uint32_t count;       // 0 for interior
+};
+
+struct Scene {
+    std::vector<float> vertices;
+    std::vector<uint32_t> indices, mesh_descs, instance_descs;
+    std::vector<float> transforms, inv_transposes, materials;
+    std::vector<uint32_t> flat_instance, flat_prim, instance_first_flat;
+    std::vector<float> world_f;   // [T][9] float world triangles
+    std::vector<double> world_d;  // [T][9] double world triangles
+    std::vector<BvhNode> nodes;
+    std::vector<uint32_t> prim_order;
+    float pad = 0.0f;
+    uint32_t tri_count() const { return (uint32_t)flat_instance.size(); }
+};
+
+// mul(M, float4(p, 1)).xyz, unfused left to right.
+template <class T> V3<T> xform_point(const float* m, V3<T> p) {
+    return {((T(m[0]) * p.x + T(m[1]) * p.y) + T(m[2]) * p.z) + T(m[3]),
+            ((T(m[4]) * p.x + T(m[5]) * p.y) + T(m[6]) * p.z) + T(m[7]),
+            ((T(m[8]) * p.x + T(m[9]) * p.y) + T(m[10]) * p.z) + T(m[11])};
+}
+
+void build_bvh(Scene& s) {
+    uint32_t n = s.tri_count();
+    std::vector<Box> boxes(n);
+    std::vector<float> cent(3 * (size_t)n);
+    Box root;
+    root.reset();
+    float max_abs = 0.0f;
+    for (uint32_t t = 0; t < n; ++t) {
+        boxes[t].reset();
+        for (int k = 0; k < 3; ++k) {
+            const float* p = &s.world_f[9 * (size_t)t + 3 * k];
+            boxes[t].grow(p);
+            for (int a = 0; a < 3; ++a) max_abs = std::max(max_abs, std::fabs(p[a]));
+        }
+        for (int a = 0; a < 3; ++a) cent[3 * (size_t)t + a] = (boxes[t].lo[a] + boxes[t].hi[a]) * 0.5f;
+        root.grow(boxes[t]);
+    }
+    s.pad = max_abs * 1e-5f + 1e-20f;
+    s.prim_order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) s.prim_order[i] = i;
+    s.nodes.clear();
+    s.nodes.reserve(2 * (size_t)n + 1);
+    BvhNode r;
+    r.box = root;
+    r.left_first = 0;
+    r.count = n;
+    s.nodes.push_back(r);
+    std::vector<uint32_t> stack{0};
+    const int B = 8;
+    while (!stack.empty()) {
+        uint32_t ni = stack.back();
+        stack.pop_back();
+        BvhNode node = s.nodes[ni];
+        float sa = node.box.half_area();
+        if (node.count <= 1 || sa <= 0.0f) continue;
+        Box cb;
+        cb.reset();
+        for (uint32_t i = 0; i < node.count; ++i) cb.grow(&cent[3 * (size_t)s.prim_order[node.left_first + i]]);
+        float best_cost = INFINITY;
+        int best_axis = -1, best_pos = 0;
+        float best_scale = 0.0f, best_min = 0.0f;
+        for (int a = 0; a < 3; ++a) {
+            float ext = cb.hi[a] - cb.lo[a];
+            if (!(ext > 0.0f)) continue;
+            float scale = (float)B / ext;
+            Box bins[B];
+            uint32_t cnt[B] = {0};
+            for (int b = 0; b < B; ++b) bins[b].reset();
+            for (uint32_t i = 0; i < node.count; ++i) {
+                uint32_t p = s.prim_order[node.left_first + i];
+                int bi = (int)((cent[3 * (size_t)p + a] - cb.lo[a]) * scale);
+                bi = std::min(std::max(bi, 0), B - 1);
+                bins[bi].grow(boxes[p]);
+                cnt[bi]++;
+            }
+            float left_area[B - 1], right_area[B - 1];
+            uint32_t left_n[B - 1], right_n[B - 1];
+            Box lb, rb;
+            lb.reset();
+            rb.reset();
+            uint32_t ln = 0, rn = 0;
+            for (int i = 0; i < B - 1; ++i) {
+                lb.grow(bins[i]);
+                ln += cnt[i];
+                left_area[i] = lb.half_area();
+                left_n[i] = ln;
+                rb.grow(bins[B - 1 - i]);
+                rn += cnt[B - 1 - i];
+                right_area[B - 2 - i] = rb.half_area();
+                right_n[B - 2 - i] = rn;
+            }
+            for (int i = 0; i < B - 1; ++i) {
+                if (left_n[i] == 0 || right_n[i] == 0) continue;
+                float c = left_area[i] * (float)left_n[i] + right_area[i] * (float)right_n[i];
+                if (c < best_cost) {
+                    best_cost = c;
+                    best_axis = a;
+                    best_pos = i;
+                    best_scale = scale;
+                    best_min = cb.lo[a];
+                }
+            }
+        }
+        if (best_axis < 0) continue;
+        float split_cost = 1.0f + best_cost / sa;
+        if (split_cost >= (float)node.count) continue;
+        uint32_t i = node.left_first, j = node.left_first + node.count;
+        while (i < j) {
+            uint32_t p = s.prim_order[i];
+            int bi = (int)((cent[3 * (size_t)p + best_axis] - best_min) * best_scale);
+            bi = std::min(std::max(bi, 0), B - 1);
+            if (bi <= best_pos) ++i;
+            else std::swap(s.prim_order[i], s.prim_order[--j]);
+        }
+        uint32_t left_count = i - node.left_first;
+        if (left_count == 0 || left_count == node.count) continue;
+        uint32_t c0 = (uint32_t)s.nodes.size();
+        BvhNode L, R;
+        L.left_first = node.left_first;
+        L.count = left_count;
+        R.left_first = i;
+        R.count = node.count - left_count;
+        L.box.reset();
+        R.box.reset();
+        for (uint32_t k = 0; k < L.count; ++k) L.box.grow(boxes[s.prim_order[L.left_first + k]]);
+        for (uint32_t k = 0; k < R.count; ++k) R.box.grow(boxes[s.prim_order[R.left_first + k]]);
+        s.nodes.push_back(L);
+        s.nodes.push_back(R);
+        s.nodes[ni].left_first = c0;
+        s.nodes[ni].count = 0;
+        stack.push_back(c0);
+        stack.push_back(c0 + 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Watertight ray/triangle test (Woop, Benthin, Wald 2013).
+// ---------------------------------------------------------------------------
+template <class T> struct RayPre {
+    V3<T> o, d;
+    T tmin, tmax;
+    int kx, ky, kz;
+    T sx, sy, sz;
+};
+
+template <class T> RayPre<T> make_ray(V3<T> o, V3<T> d, T tmin, T tmax) {
+    RayPre<T> r;
+    r.o = o;
+    r.d = d;
+    r.tmin = tmin;
+    r.tmax = tmax;
+    T a[3] = {std::fabs(d.x), std::fabs(d.y), std::fabs(d.z)};
+    int kz = 0;
+    if (a[1] > a[kz]) kz = 1;
+    if (a[2] > a[kz]) kz = 2;
+    int kx = kz + 1 == 3 ? 0 : kz + 1;
+    int ky = kx + 1 == 3 ? 0 : kx + 1;
+    if (d[kz] < T(0)) std::swap(kx, ky);
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.sx = d[kx] / d[kz];
+    r.sy = d[ky] / d[kz];
+    r.sz = T(1) / d[kz];
+    return r;
+}
+
+// Returns true with t, b1 (weight of v1), b2 (weight of v2) when the ray
+// crosses the triangle's interior or edges (no culling); range not checked.
+template <class T> bool tri_intersect(const RayPre<T>& r, const T* v, T* t_out, T* b1, T* b2) {
+    V3<T> A = mk<T>(v[0], v[1], v[2]) - r.o;
+    V3<T> B = mk<T>(v[3], v[4], v[5]) - r.o;
+    V3<T> C = mk<T>(v[6], v[7], v[8]) - r.o;
+    T ax = A[r.kx] - r.sx * A[r.kz];
+    T ay = A[r.ky] - r.sy * A[r.kz];
+    T bx = B[r.kx] - r.sx * B[r.kz];
+    T by = B[r.ky] - r.sy * B[r.kz];
+    T cx = C[r.kx] - r.sx * C[r.kz];
+    T cy = C[r.ky] - r.sy * C[r.kz];
+    T U = cx * by - cy * bx;
+    T V = ax * cy - ay * cx;
+    T W = bx * ay - by * ax;
+    if (sizeof(T) == 4 && (U == T(0) || V == T(0) || W == T(0))) {
+        U = (T)((double)cx * (double)by - (double)cy * (double)bx);
+        V = (T)((double)ax * (double)cy - (double)ay * (double)cx);
+        W = (T)((double)bx * (double)ay - (double)by * (double)ax);
+    }
+    if ((U < T(0) || V < T(0) || W < T(0)) && (U > T(0) || V > T(0) || W > T(0))) return false;
+    T det = (U + V) + W;
+    if (det == T(0)) return false;
+    T az = r.sz * A[r.kz];
+    T bz = r.sz * B[r.kz];
+    T cz = r.sz * C[r.kz];
+    T tt = (U * az + V * bz) + W * cz;
+    *t_out = tt / det;
+    *b1 = V / det;
+    *b2 = W / det;
+    return true;
+}
+
+struct HitRec {
+    bool valid = false;
+    uint32_t flat = 0xffffffffu;
+    double t = 0.0;
+    double b1 = 0.0, b2 = 0.0;
+};
+
+// Conservative slab test in double precision against the padded box.
+bool box_hit(const Box& b, float pad, const double* o, const double* id, double tmin, double tmax,
+             double* tenter) {
+    double t0 = tmin, t1 = tmax;
+    for (int a = 0; a < 3; ++a) {
+        double lo = (double)b.lo[a] - pad, hi = (double)b.hi[a] + pad;
+        double ta = (lo - o[a]) * id[a];
+        double tb = (hi - o[a]) * id[a];
+        if (std::isnan(ta) || std::isnan(tb)) { ta = -INFINITY; tb = INFINITY; }
+        if (ta > tb) std::swap(ta, tb);
+        t0 = std::max(t0, ta);
+        t1 = std::min(t1, tb);
+    }
+    *tenter = t0;
+    return t0 <= t1;
+}
+
+template <class T> const T* tri_ptr(const Scene& s, uint32_t flat);
+template <> const float* tri_ptr<float>(const Scene& s, uint32_t flat) { return &s.world_f[9 * (size_t)flat]; }
+template <> const double* tri_ptr<double>(const Scene& s, uint32_t flat) { return &s.world_d[9 * (size_t)flat]; }
+
+// mode: 0 BVH, otherwise brute force. any: stop at the first hit in range.
+template <class T>
+HitRec trace(const Scene& s, const RayPre<T>& r, bool any, bool use_bvh, OracleRayCounts* cnt) {
+    HitRec best;
+    T best_t = r.tmax;
+    uint32_t best_key = 0xffffffffu;
+    T best_b1 = 0, best_b2 = 0;
+    auto test = [&](uint32_t flat) -> bool {
+        if (cnt) cnt->triangle_tests++;
+        T t, b1, b2;
+        if (!tri_intersect<T>(r, tri_ptr<T>(s, flat), &t, &b1, &b2)) return false;
+        if (!(t >= r.tmin)) return false;
+        if (any) {
+            if (t <= r.tmax) {
+                best.valid = true;
+                best.flat = flat;
+                best.t = (double)t;
+                return true;
+            }
+            return false;
+        }
+        if (t < best_t || (t == best_t && flat < best_key)) {
+            best.valid = true;
+            best_t = t;
+            best_key = flat;
+            best_b1 = b1;
+            best_b2 = b2;
+        }
+        return false;
+    };
+    if (!use_bvh) {
+        for (uint32_t f = 0; f < s.tri_count(); ++f)
+            if (test(f)) return best;
+    } else {
+        double o[3] = {(double)r.o.x, (double)r.o.y, (double)r.o.z};
+        double id[3] = {1.0 / (double)r.d.x, 1.0 / (double)r.d.y, 1.0 / (double)r.d.z};
+        uint32_t stack[128];
+        int sp = 0;
+        double te;
+        if (cnt) cnt->node_fetches++;
+        if (box_hit(s.nodes[0].box, s.pad, o, id, (double)r.tmin, (double)r.tmax, &te)) stack[sp++] = 0;
+        while (sp > 0) {
+            const BvhNode& n = s.nodes[stack[--sp]];
+            if (n.count > 0) {
+                for (uint32_t k = 0; k < n.count; ++k)
+                    if (test(s.prim_order[n.left_first + k])) return best;
+                continue;
+            }
+            double limit = any ? (double)r.tmax : (double)best_t;
+            double t0, t1;
+            if (cnt) cnt->node_fetches += 2;
+            bool h0 = box_hit(s.nodes[n.left_first].box, s.pad, o, id, (double)r.tmin, limit, &t0);
+            bool h1 = box_hit(s.nodes[n.left_first + 1].box, s.pad, o, id, (double)r.tmin, limit, &t1);
+            uint32_t c0 = n.left_first, c1 = n.left_first + 1;
+            if (h0 && h1) {
+                if (t1 < t0) { std::swap(c0, c1); }
+                stack[sp++] = c1;  // far
+                stack[sp++] = c0;  // near (popped first)
+            } else if (h0) {
+                stack[sp++] = c0;
+            } else if (h1) {
+                stack[sp++] = c1;
+            }
+            if (sp > 126) { g_error = "oracle BVH stack overflow"; return best; }
+        }
+    }
+    if (!any && best.valid) {
+        best.flat = best_key;
+        best.t = (double)best_t;
+        best.b1 = (double)best_b1;
+        best.b2 = (double)best_b2;
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------------------
+// Shading: scene.slang:178-406.
+// ---------------------------------------------------------------------------
+struct Lighting {
+    OracleLighting p;
+};
+
+template <class T> struct Shading {
+    V3<T> position, origin_front, origin_back;
+    T offset;
+    V3<T> view_direction, face_normal, diffuse, emissive;
+    Frame<T> shading_frame{mk<T>(0, 0, 1)};
+};
+
+template <class T> V3<T> load3(const float* p) { return mk<T>(T(p[0]), T(p[1]), T(p[2])); }
+
+struct TriRefs {
+    const float* v0;
+    const float* v1;
+    const float* v2;
+    const float* m;
+    const float* it;
+    const float* mat;
+    uint32_t flags;
+};
+
+TriRefs tri_refs(const Scene& s, uint32_t inst, uint32_t prim) {
+    const uint32_t* idesc = &s.instance_descs[4 * (size_t)inst];
+    const uint32_t* mdesc = &s.mesh_descs[4 * (size_t)idesc[0]];
+    uint32_t base = mdesc[3] + prim * 3u;
+    TriRefs r;
+    r.v0 = &s.vertices[8 * (size_t)(mdesc[2] + s.indices[base + 0])];
+    r.v1 = &s.vertices[8 * (size_t)(mdesc[2] + s.indices[base + 1])];
+    r.v2 = &s.vertices[8 * (size_t)(mdesc[2] + s.indices[base + 2])];
+    r.m = &s.transforms[16 * (size_t)idesc[2]];
+    r.it = &s.inv_transposes[16 * (size_t)idesc[2]];
+    r.mat = &s.materials[8 * (size_t)idesc[1]];
+    r.flags = idesc[3];
+    return r;
+}
+
+// scene.slang:178-269
+template <class T>
+void triangle_spawn(V3<T> v0, V3<T> v1, V3<T> v2, T bx, T by, const float* m, const float* it,
+                    V3<T>* pos, V3<T>* nrm, T* off) {
+    const T c0 = T(5.9604644775390625e-8f);
+    const T c1 = T(1.7881397695873602e-7f);
+    const T c2 = T(1.1920931797249068e-7f);
+    V3<T> e1 = v1 - v0, e2 = v2 - v0;
+    V3<T> op = {v0.x + Ops<T>::fma(bx, e1.x, by * e2.x), v0.y + Ops<T>::fma(bx, e1.y, by * e2.y),
+                v0.z + Ops<T>::fma(bx, e1.z, by * e2.z)};
+    V3<T> on = cross(e1, e2);
+    V3<T> wp;
+    wp.x = T(m[3]) + Ops<T>::fma(T(m[0]), op.x, Ops<T>::fma(T(m[1]), op.y, T(m[2]) * op.z));
+    wp.y = T(m[7]) + Ops<T>::fma(T(m[4]), op.x, Ops<T>::fma(T(m[5]), op.y, T(m[6]) * op.z));
+    wp.z = T(m[11]) + Ops<T>::fma(T(m[8]), op.x, Ops<T>::fma(T(m[9]), op.y, T(m[10]) * op.z));
+    V3<T> wnu = {(T(it[0]) * on.x + T(it[1]) * on.y) + T(it[2]) * on.z,
+                 (T(it[4]) * on.x + T(it[5]) * on.y) + T(it[6]) * on.z,
+                 (T(it[8]) * on.x + T(it[9]) * on.y) + T(it[10]) * on.z};
+    T ws = T(1) / Ops<T>::sqrt(vmax(dot(wnu, wnu), T(1e-30f)));
+    V3<T> wn = wnu * ws;
+    V3<T> ext3 = (vabs(e1) + vabs(e2)) + vabs(vabs(e1) - vabs(e2));
+    T ext = vmax(vmax(ext3.x, ext3.y), ext3.z);
+    V3<T> av0 = vabs(v0);
+    V3<T> oe = {c0 * av0.x + c1 * ext, c0 * av0.y + c1 * ext, c0 * av0.z + c1 * ext};
+    V3<T> aop = vabs(op);
+    V3<T> we;
+    we.x = c1 * dot(vabs(mk<T>(T(m[0]), T(m[1]), T(m[2]))), aop) + c2 * std::fabs(T(m[3]));
+    we.y = c1 * dot(vabs(mk<T>(T(m[4]), T(m[5]), T(m[6]))), aop) + c2 * std::fabs(T(m[7]));
+    we.z = c1 * dot(vabs(mk<T>(T(m[8]), T(m[9]), T(m[10]))), aop) + c2 * std::fabs(T(m[11]));
+    V3<T> awp = vabs(wp);
+    T te[3];
+    for (int c = 0; c < 3; ++c) {
+        // dot(abs(float4(it[0][c], it[1][c], it[2][c], it[3][c])), float4(|wp|, 1))
+        te[c] = ((std::fabs(T(it[c])) * awp.x + std::fabs(T(it[4 + c])) * awp.y) +
+                 std::fabs(T(it[8 + c])) * awp.z) +
+                std::fabs(T(it[12 + c])) * T(1);
+    }
+    oe = oe + mk<T>(c2 * te[0], c2 * te[1], c2 * te[2]);
+    T oo = dot(oe, vabs(on));
+    T wo = dot(we, vabs(wn));
+    wo = Ops<T>::fma(ws, oo, wo);
+    *pos = wp;
+    *nrm = wn;
+    *off = wo;
+}
+
+// scene.slang:271-406 (opaque, untextured subset)
+template <class T>
+Shading<T> shading_data(const Scene& s, uint32_t inst, uint32_t prim, T bx, T by, V3<T> view) {
+    TriRefs r = tri_refs(s, inst, prim);
+    T b0 = (T(1) - bx) - by;
+    V3<T> pos, fn;
+    T off;
+    triangle_spawn<T>(load3<T>(r.v0), load3<T>(r.v1), load3<T>(r.v2), bx, by, r.m, r.it, &pos, &fn, &off);
+    V3<T> n0 = load3<T>(r.v0 + 3), n1 = load3<T>(r.v1 + 3), n2 = load3<T>(r.v2 + 3);
+    V3<T> ni = (b0 * n0 + bx * n1) + by * n2;
+    const float* it = r.it;
+    V3<T> gnu = {((T(it[0]) * ni.x + T(it[1]) * ni.y) + T(it[2]) * ni.z) + T(it[3]) * T(0),
+                 ((T(it[4]) * ni.x + T(it[5]) * ni.y) + T(it[6]) * ni.z) + T(it[7]) * T(0),
+                 ((T(it[8]) * ni.x + T(it[9]) * ni.y) + T(it[10]) * ni.z) + T(it[11]) * T(0)};
+    V3<T> gn = normalize(gnu);
+    V3<T> sn = gn;
+    uint32_t mflags;
+    std::memcpy(&mflags, &r.mat[3], 4);
+    bool double_sided = (mflags & 1u) != 0;
+    bool front = dot(fn, view) > T(0);
+    T sign = (double_sided && !front) ? T(-1) : T(1);
+    fn = fn * sign;
+    gn = gn * sign;
+    sn = sn * sign;
+    sn = adjust_shading_normal(sn, fn, -view);
+    Shading<T> sd;
+    sd.position = pos;
+    sd.origin_front = pos + off * fn;
+    sd.origin_back = pos - off * fn;
+    sd.offset = off;
+    sd.view_direction = view;
+    sd.face_normal = fn;
+    sd.shading_frame = Frame<T>(sn);
+    sd.diffuse = load3<T>(r.mat);
+    sd.emissive = load3<T>(r.mat + 4);
+    return sd;
+}
+
+// texture_space_path_tracer.slang:39-55
+template <class T> V3<T> world_flat_normal(const Scene& s, uint32_t inst, uint32_t prim) {
+    TriRefs r = tri_refs(s, inst, prim);
+    V3<T> p0 = load3<T>(r.v0), p1 = load3<T>(r.v1), p2 = load3<T>(r.v2);
+    V3<T> n = normalize(cross(p1 - p0, p2 - p0));  // common.slang:101-111
+    if (r.flags & 1u) n = -n;
+    const float* it = r.it;
+    V3<T> w = {(T(it[0]) * n.x + T(it[1]) * n.y) + T(it[2]) * n.z,
+               (T(it[4]) * n.x + T(it[5]) * n.y) + T(it[6]) * n.z,
+               (T(it[8]) * n.x + T(it[9]) * n.y) + T(it[10]) * n.z};
+    return normalize(w);
+}
+
+// ---------------------------------------------------------------------------
+// Lights: scene.slang:940-990 (sun NEE), constant sky stand-in for the LUT
+// (scene.slang:469-518), sun disk (scene.slang:408-465).
+// ---------------------------------------------------------------------------
+template <class T> struct LightCtx {
+    V3<T> sun_dir, outer, trans, illum, sky;
+    T cos_half, t_max;
+    bool sun_disk;
+    explicit LightCtx(const OracleLighting& p) {
+        sun_dir = mk<T>(T(p.sun_direction[0]), T(p.sun_direction[1]), T(p.sun_direction[2]));
+        V3<T> color = mk<T>(T(p.sun_color[0]), T(p.sun_color[1]), T(p.sun_color[2]));
+        outer = color * T(p.sun_intensity);
+        trans = mk<T>(T(p.sun_transmittance[0]), T(p.sun_transmittance[1]), T(p.sun_transmittance[2]));
+        illum = outer * trans;
+        sky = mk<T>(T(p.sky_radiance[0]), T(p.sky_radiance[1]), T(p.sky_radiance[2]));
+        cos_half = T(p.sun_cos_half_angle);
+        t_max = T(p.ray_t_max);
+        sun_disk = (p.flags & 1u) != 0;
+    }
+};
+
+template <class T> struct Tracer {
+    const Scene& s;
+    LightCtx<T> L;
+    bool use_bvh;
+    OracleRayCounts cnt{};
+    Tracer(const Scene& sc, const OracleLighting& p) : s(sc), L(p), use_bvh(true) {}
+
+    HitRec closest(V3<T> o, V3<T> d, T tmin, T tmax) {
+        cnt.extend_rays++;
+        RayPre<T> r = make_ray<T>(o, d, tmin, tmax);
+        return trace<T>(s, r, false, use_bvh, &cnt);
+    }
+    T visibility(V3<T> o, V3<T> d) {
+        cnt.shadow_rays++;
+        RayPre<T> r = make_ray<T>(o, d, T(0), L.t_max);
+        return trace<T>(s, r, true, use_bvh, &cnt).valid ? T(0) : T(1);
+    }
+    // scene.slang:954-990 (use_visibility_override == 0)
+    V3<T> sun_nee(const Shading<T>& sd, T ux, T uy) {
+        V3<T> l = sample_cone_direction<T>(L.sun_dir, L.cos_half, ux, uy);
+        T vis = visibility(sd.origin_front, l);
+        T ndl = vmax(T(0), dot(sd.shading_frame.n, l));
+        V3<T> f = sd.diffuse * Consts<T>::INV_PI;
+        return ((vis * f) * L.illum) * ndl;
+    }
+    // scene.slang:940-952
+    V3<T> sun_irradiance(const Shading<T>& sd, T ux, T uy) {
+        V3<T> l = sample_cone_direction<T>(L.sun_dir, L.cos_half, ux, uy);
+        T vis = visibility(sd.origin_front, l);
+        T ndl = vmax(T(0), dot(sd.shading_frame.n, l));
+        return (vis * L.illum) * ndl;
+    }
+    // scene.slang:408-465
+    V3<T> sun_disk(V3<T> dir) {
+        V3<T> vp = mk<T>(T(0), T(6.360f + 0.0002f), T(0));
+        V3<T> oc = vp;  // center at origin
+        T a = dot(dir, dir);
+        T b = T(2) * dot(oc, dir);
+        T gr = T(6.360f);
+        T c = dot(oc, oc) - gr * gr;
+        T disc = b * b - T(4) * a * c;
+        if (disc >= T(0)) {
+            T sq = Ops<T>::sqrt(disc);
+            T t0 = (-b - sq) / (T(2) * a);
+            T t1 = (-b + sq) / (T(2) * a);
+            if (t0 > T(0) || t1 > T(0)) return mk<T>(0, 0, 0);
+        }
+        T vdl = dot(dir, L.sun_dir);
+        if (vdl > L.cos_half) {
+            T solid = T(2) * Consts<T>::PI * (T(1) - L.cos_half);
+            V3<T> lum = L.outer / solid;
+            T soft = saturate(T(2) * (vdl - L.cos_half) / (T(1) - L.cos_half));
+            return (L.trans * lum) * soft;
+        }
+        return mk<T>(0, 0, 0);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Screen path tracer: path_tracer.slang:40-130, camera.slang:201-236.
+// ---------------------------------------------------------------------------
+template <class T>
+void screen_pixel(Tracer<T>& tr, const OracleLighting& lp, const OracleCamera& cam, uint32_t w,
+                  uint32_t h, uint32_t frame, uint32_t max_vertices, uint32_t px, uint32_t py,
+                  float* out) {
+    Rng rng(px, py, frame * 1u + 0u);
+    rng.next_1d();
+    rng.next_1d();  // the unused jitter draw (path_tracer.slang:121)
+    // camera.slang:223-236
+    T pxf = (T((float)px) + T(0.5)) / T((float)w);
+    T pyf = (T((float)py) + T(0.5)) / T((float)h);
+    pxf = pxf + (-T(cam.jitter_x));
+    pyf = pyf + T(cam.jitter_y);
+    T nx = T(2) * pxf + T(-1);
+    T ny = T(-2) * pyf + T(1);
+    V3<T> U = load3<T>(cam.image_u), Vv = load3<T>(cam.image_v), W = load3<T>(cam.image_w);
+    V3<T> dir = normalize((nx * U + ny * Vv) + W);
+    T inv_cos = T(1) / dot(normalize(W), dir);
+    T tmin = T(cam.near_clip) * inv_cos;
+    T tmax = T(cam.far_clip) * inv_cos;
+    V3<T> o = load3<T>(cam.position);
+    V3<T> thp = mk<T>(1, 1, 1), Lr = mk<T>(0, 0, 0);
+    (void)lp;
+    for (uint32_t vi = 0; vi < max_vertices; ++vi) {
+        HitRec hit = tr.closest(o, dir, tmin, tmax);
+        if (!hit.valid) {
+            V3<T> sky = tr.L.sky;
+            if (vi == 0 && tr.L.sun_disk) sky = sky + tr.sun_disk(dir);
+            Lr = Lr + thp * sky;
+            break;
+        }
+        uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
+        Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(hit.b1), T(hit.b2), -dir);
+        Lr = Lr + thp * sd.emissive;
+        T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
+        V3<T> nee = tr.sun_nee(sd, u0, u1);
+        Lr = Lr + thp * nee;
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> wo;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &wo, &pdf);
+        pdf = vmax(pdf, T(1e-6f));
+        V3<T> f = sd.diffuse * Consts<T>::INV_PI;
+        thp = thp * ((f * std::fabs(wo.z)) / pdf);
+        o = sd.origin_front;
+        dir = sd.shading_frame.to_global(wo);
+        tmin = T(0);
+        tmax = tr.L.t_max;
+    }
+    out[0] = (float)Lr.x;
+    out[1] = (float)Lr.y;
+    out[2] = (float)Lr.z;
+    out[3] = 1.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Texture-space tracer: texture_space_path_tracer.slang:57-216.
+// ---------------------------------------------------------------------------
+template <class T>
+V3<T> ts_trace_radiance(Tracer<T>& tr, V3<T> o, V3<T> d, Rng& rng, uint32_t max_bounces) {
+    V3<T> thp = mk<T>(1, 1, 1), rad = mk<T>(0, 0, 0);
+    for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+        HitRec hit = tr.closest(o, d, T(0), tr.L.t_max);
+        if (!hit.valid) {
+            rad = rad + thp * tr.L.sky;
+            return rad;
+        }
+        uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
+        Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(hit.b1), T(hit.b2), -d);
+        rad = rad + thp * sd.emissive;
+        T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
+        rad = rad + thp * tr.sun_nee(sd, u0, u1);
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> sdir;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &sdir, &pdf);
+        if (pdf <= T(1e-6f)) return rad;
+        V3<T> f = sd.diffuse * Consts<T>::INV_PI;
+        thp = thp * ((f * std::fabs(sdir.z)) / pdf);
+        o = sd.origin_front;
+        d = sd.shading_frame.to_global(sdir);
+    }
+    return rad;
+}
+
+template <class T>
+V3<T> ts_estimate(Tracer<T>& tr, uint32_t inst, uint32_t prim, T bx, T by, V3<T> view, uint32_t n,
+                  Rng& rng, uint32_t max_bounces) {
+    Shading<T> sd = shading_data<T>(tr.s, inst, prim, bx, by, view);
+    V3<T> irr = mk<T>(0, 0, 0);
+    for (uint32_t k = 0; k < n; ++k) {
+        T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
+        V3<T> si = tr.sun_irradiance(sd, u0, u1);
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> dir;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &dir, &pdf);
+        if (pdf > T(1e-6f)) {
+            V3<T> rad = ts_trace_radiance<T>(tr, sd.origin_front, sd.shading_frame.to_global(dir), rng,
+                                             max_bounces);
+            si = si + ((rad * std::fabs(dir.z)) / pdf);
+        }
+        irr = irr + si;
+    }
+    return irr / T((float)n);
+}
+
+// texture_space_path_tracer.slang:119-138 (float storage in the slot)
+void store_running_mean(uint8_t* slots, uint32_t texel, const float* sample, bool reset) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(slots + 16 * (size_t)texel);
+    uint32_t prev = reset ? 0u : w[3];
+    float pv[3] = {0, 0, 0};
+    if (prev != 0) std::memcpy(pv, w, 12);
+    uint32_t next = std::min(prev + 1u, 65535u);
+    float weight = 1.0f / (float)(prev + 1u);
+    float acc[3];
+    for (int c = 0; c < 3; ++c) acc[c] = pv[c] + weight * (sample[c] - pv[c]);
+    std::memcpy(w, acc, 12);
+    w[3] = next;
+}
+
+// ---------------------------------------------------------------------------
+// Surface-probe baker: surface_probe_path_tracer.slang:47-315.
+// ---------------------------------------------------------------------------
+template <class T> struct ProbePath {
+    V3<T> o, d, thp, rad;
+    uint32_t src_inst, src_prim;
+    T src_off;
+    uint32_t self_hits;
+    T first_hit, radial_max;
+};
+
+template <class T> void probe_trace_radiance(Tracer<T>& tr, ProbePath<T>& p, Rng& rng, uint32_t max_bounces) {
+    for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+        HitRec hit = tr.closest(p.o, p.d, T(0), tr.L.t_max);
+        if (!hit.valid) {
+            if (bounce == 0u) p.first_hit = p.radial_max;
+            p.rad = p.rad + p.thp * tr.L.sky;
+            return;
+        }
+        T ht = T(hit.t);
+        if (bounce == 0u) p.first_hit = vmin(ht, p.radial_max);
+        uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
+        bool same_prim = inst == p.src_inst && prim == p.src_prim;
+        T thr = vmax(T(4) * p.src_off, T(1e-6f));
+        bool adjacent = inst == p.src_inst && ht <= thr;
+        if (same_prim || adjacent) p.self_hits += 1u;
+        Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(hit.b1), T(hit.b2), -p.d);
+        p.rad = p.rad + p.thp * sd.emissive;
+        T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
+        p.rad = p.rad + p.thp * tr.sun_nee(sd, u0, u1);
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> sdir;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &sdir, &pdf);
+        if (pdf <= T(1e-6f)) return;
+        V3<T> f = sd.diffuse * Consts<T>::INV_PI;
+        p.thp = p.thp * ((f * std::fabs(sdir.z)) / pdf);
+        V3<T> next_origin = sd.origin_front;
+        V3<T> out_dir = Frame<T>(normalize(sd.face_normal)).to_global(sdir);
+        p.o = next_origin;
+        p.d = out_dir;
+        p.src_inst = inst;
+        p.src_prim = prim;
+        p.src_off = length(next_origin - sd.position);
+    }
+}
+
+struct ProbeBuffers {
+    float* values;
+    uint32_t* counts;
+    uint32_t* self_hits;
+    uint32_t* radial;
+};
+
+// surface_probe_path_tracer.slang:111-149 (moments kept as RG16F)
+template <class T>
+void accumulate_radial_moment(ProbeBuffers& b, uint32_t probe, uint32_t texel, T nd, uint32_t prev_iter,
+                              uint32_t local_count, uint32_t spp) {
+    uint32_t packed = b.radial[16 * (size_t)probe + texel];
+    float px = f16_to_f32((uint16_t)(packed & 0xffffu));
+    float py = f16_to_f32((uint16_t)(packed >> 16));
+    float sample = (float)std::min(std::max(nd, T(0)), T(2));
+    float smx = sample, smy = sample * sample;
+    if (py <= 0.0f) {
+        px = smx;
+        py = smy;
+    } else {
+        float pop = ((float)prev_iter * (float)std::max(spp, 1u)) * radial_texel_cosine_probability(texel);
+        uint32_t expected = prev_iter == 0u ? local_count - 1u : std::max((uint32_t)pop, 1u);
+        float alpha = 1.0f / (float)std::max(std::min(expected + local_count, 4096u), 1u);
+        px = px + alpha * (smx - px);
+        py = py + alpha * (smy - py);
+    }
+    px = std::min(std::max(px, 0.0f), 4.0f);
+    py = std::min(std::max(py, 0.0f), 4.0f);
+    b.radial[16 * (size_t)probe + texel] = (uint32_t)f32_to_f16(px) | ((uint32_t)f32_to_f16(py) << 16);
+}
+
+template <class T>
+void probe_unit(Tracer<T>& tr, ProbeBuffers& b, const uint8_t* probes, const uint8_t* pinst, uint32_t probe,
+                uint32_t iteration, uint32_t spp, uint32_t max_bounces, bool reset) {
+    const uint8_t* rec = probes + 48 * (size_t)probe;
+    float nrm[4];
+    uint32_t meta[4];
+    std::memcpy(nrm, rec + 16, 16);
+    std::memcpy(meta, rec + 32, 16);
+    uint32_t inst = meta[3] >> 8;
+    float params[4];
+    std::memcpy(params, pinst + 48 * (size_t)inst + 32, 16);
+    float bx, by;
+    std::memcpy(&bx, &meta[1], 4);
+    std::memcpy(&by, &meta[2], 4);
+    uint32_t prim = meta[0];
+    uint32_t n = std::max(spp, 1u);
+    Rng rng(probe, inst, iteration * n);
+    V3<T> view = normalize(mk<T>(T(nrm[0]), T(nrm[1]), T(nrm[2])));
+    T kr = vmax(T(params[0]), T(1e-6f));
+    // estimate_surface_irradiance (surface_probe_path_tracer.slang:206-278)
+    Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(bx), T(by), view);
+    V3<T> irr = mk<T>(0, 0, 0);
+    uint32_t self_total = 0;
+    uint32_t prev_iter = reset ? 0u : b.counts[probe];
+    uint32_t local_counts[16] = {0};
+    if (reset)
+        for (int t = 0; t < 16; ++t) b.radial[16 * (size_t)probe + t] = 0u;
+    for (uint32_t k = 0; k < n; ++k) {
+        V3<T> si = mk<T>(0, 0, 0);
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> dir;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &dir, &pdf);
+        if (pdf > T(1e-6f)) {
+            ProbePath<T> p;
+            V3<T> origin = sd.origin_front;
+            p.o = origin;
+            p.d = Frame<T>(normalize(sd.face_normal)).to_global(dir);
+            p.thp = mk<T>(1, 1, 1);
+            p.rad = mk<T>(0, 0, 0);
+            p.src_inst = inst;
+            p.src_prim = prim;
+            p.src_off = length(origin - sd.position);
+            p.self_hits = 0;
+            p.first_hit = T(2) * kr;
+            p.radial_max = T(2) * kr;
+            probe_trace_radiance<T>(tr, p, rng, max_bounces);
+            self_total += p.self_hits;
+            float u, v;
+            hemi_oct_encode((float)dir.x, (float)dir.y, (float)dir.z, &u, &v);
+            uint32_t texel = radial_texel_index(u, v);
+            local_counts[texel] += 1u;
+            accumulate_radial_moment<T>(b, probe, texel, p.first_hit / vmax(kr, T(1e-6f)), prev_iter,
+                                        local_counts[texel], spp);
+            si = si + ((p.rad * std::fabs(dir.z)) / pdf);
+        }
+        irr = irr + si;
+    }
+    irr = irr / T((float)n);
+    // store_accumulated_irradiance (:47-65)
+    uint32_t prev = reset ? 0u : b.counts[probe];
+    float pv[3] = {0, 0, 0};
+    if (prev != 0) std::memcpy(pv, b.values + 3 * (size_t)probe, 12);
+    uint32_t next = std::min(prev + 1u, 65535u);
+    float weight = 1.0f / (float)(prev + 1u);
+    float smp[3] = {(float)irr.x, (float)irr.y, (float)irr.z};
+    for (int c = 0; c < 3; ++c) b.values[3 * (size_t)probe + c] = pv[c] + weight * (smp[c] - pv[c]);
+    b.counts[probe] = next;
+    // store_accumulated_self_hit_count (:67-79)
+    uint32_t prev_self = reset ? 0u : b.self_hits[probe];
+    b.self_hits[probe] = prev_self + self_total;
+}
+
+template <class F> void parallel_for(int count, int threads, F&& fn) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    threads = std::max(1, std::min(threads, count));
+    if (threads == 1) {
+        for (int i = 0; i < count; ++i) fn(i, 0);
+        return;
+    }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t)
+        pool.emplace_back([&, t]() {
+            for (;;) {
+                int i = next.fetch_add(1);
+                if (i >= count) break;
+                fn(i, t);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
+void add_counts(OracleRayCounts* dst, const OracleRayCounts& src) {
+    if (!dst) return;
+    dst->extend_rays += src.extend_rays;
+    dst->shadow_rays += src.shadow_rays;
+    dst->node_fetches += src.node_fetches;
+    dst->triangle_tests += src.triangle_tests;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* oracle_last_error(void) { return g_error.c_str(); }
+
+void oracle_rng_sequence(uint32_t x, uint32_t y, uint32_t sample_index, int count, float* out) {
+    Rng r(x, y, sample_index);
+    for (int i = 0; i < count; ++i) out[i] = r.next_1d();
+}
+
+void oracle_sincos(const float* a, int count, float* s, float* c) {
+    for (int i = 0; i < count; ++i) own_sincos(a[i], &s[i], &c[i]);
+}
+
+void oracle_pack_rgb9e5(const float* rgb, int count, uint32_t* out) {
+    for (int i = 0; i < count; ++i) out[i] = pack_rgb9e5(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+}
+
+void oracle_unpack_rgb9e5(const uint32_t* p, int count, float* out) {
+    for (int i = 0; i < count; ++i) unpack_rgb9e5(p[i], out + 3 * i);
+}
+
+void oracle_f32_to_f16(const float* v, int count, uint16_t* out) {
+    for (int i = 0; i < count; ++i) out[i] = f32_to_f16(v[i]);
+}
+
+void oracle_hemi_oct_encode(const float* d, int count, float* uv) {
+    for (int i = 0; i < count; ++i) hemi_oct_encode(d[3 * i], d[3 * i + 1], d[3 * i + 2], &uv[2 * i], &uv[2 * i + 1]);
+}
+
+void oracle_hemi_oct_decode(const float* uv, int count, float* d) {
+    for (int i = 0; i < count; ++i) hemi_oct_decode(uv[2 * i], uv[2 * i + 1], d + 3 * i);
+}
+
+void oracle_cosine_sample_hemisphere(const float* u, int count, float* out4) {
+    for (int i = 0; i < count; ++i) {
+        V3<float> h;
+        float pdf;
+        cosine_sample_hemisphere<float>(u[2 * i], u[2 * i + 1], &h, &pdf);
+        out4[4 * i] = h.x;
+        out4[4 * i + 1] = h.y;
+        out4[4 * i + 2] = h.z;
+        out4[4 * i + 3] = pdf;
+    }
+}
+
+void oracle_mesh_colors_address_to_ij(const uint32_t* a, const uint32_t* r, int count, uint32_t* ij) {
+    for (int i = 0; i < count; ++i) address_to_ij(a[i], r[i], &ij[2 * i], &ij[2 * i + 1]);
+}
+
+void* oracle_scene_create(const float* vertices, int vertex_count, const uint32_t* indices, int triangle_count,
+                          const uint32_t* mesh_descs, int mesh_count, const uint32_t* instance_descs,
+                          int instance_count, const float* transforms, const float* inverse_transposes,
+                          int transform_count, const float* materials, int material_count) {
+    Scene* s = new Scene();
+    s->vertices.assign(vertices, vertices + 8 * (size_t)vertex_count);
+    s->indices.assign(indices, indices + 3 * (size_t)triangle_count);
+    s->mesh_descs.assign(mesh_descs, mesh_descs + 4 * (size_t)mesh_count);
+    s->instance_descs.assign(instance_descs, instance_descs + 4 * (size_t)instance_count);
+    s->transforms.assign(transforms, transforms + 16 * (size_t)transform_count);
+    s->inv_transposes.assign(inverse_transposes, inverse_transposes + 16 * (size_t)transform_count);
+    s->materials.assign(materials, materials + 8 * (size_t)material_count);
+    for (int i = 0; i < instance_count; ++i) {
+        const uint32_t* id = &s->instance_descs[4 * (size_t)i];
+        const uint32_t* md = &s->mesh_descs[4 * (size_t)id[0]];
+        uint32_t tris = md[1] / 3u;
+        s->instance_first_flat.push_back((uint32_t)s->flat_instance.size());
+        const float* m = &s->transforms[16 * (size_t)id[2]];
+        for (uint32_t p = 0; p < tris; ++p) {
+            s->flat_instance.push_back((uint32_t)i);
+            s->flat_prim.push_back(p);
+            for (int k = 0; k < 3; ++k) {
+                const float* v = &s->vertices[8 * (size_t)(md[2] + s->indices[md[3] + 3 * p + k])];
+                V3<float> wf = xform_point<float>(m, mk<float>(v[0], v[1], v[2]));
+                V3<double> wd = xform_point<double>(m, mk<double>(v[0], v[1], v[2]));
+                s->world_f.push_back(wf.x);
+                s->world_f.push_back(wf.y);
+                s->world_f.push_back(wf.z);
+                s->world_d.push_back(wd.x);
+                s->world_d.push_back(wd.y);
+                s->world_d.push_back(wd.z);
+            }
+        }
+    }
+    build_bvh(*s);
+    return s;
+}
+
+void oracle_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+int oracle_scene_triangle_count(void* s) { return (int)static_cast<Scene*>(s)->tri_count(); }
+
+void oracle_scene_world_triangles(void* sp, float* out9) {
+    Scene* s = static_cast<Scene*>(sp);
+    std::memcpy(out9, s->world_f.data(), s->world_f.size() * sizeof(float));
+}
+
+void oracle_scene_bvh_stats(void* sp, double* out3) {
+    Scene* s = static_cast<Scene*>(sp);
+    double leaves = 0, sah = 0;
+    double root_area = s->nodes.empty() ? 1.0 : (double)s->nodes[0].box.half_area();
+    for (const BvhNode& n : s->nodes) {
+        double a = (double)n.box.half_area() / std::max(root_area, 1e-30);
+        if (n.count > 0) {
+            leaves += 1;
+            sah += a * (double)n.count;
+        } else {
+            sah += a;
+        }
+    }
+    out3[0] = (double)s->nodes.size();
+    out3[1] = leaves;
+    out3[2] = sah;
+}
+
+void oracle_intersect(void* sp, const float* rays, int count, int mode, uint32_t* ids, float* tb,
+                      OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    for (int i = 0; i < count; ++i) {
+        const float* r = rays + 8 * (size_t)i;
+        HitRec h;
+        OracleRayCounts c{};
+        if (mode == 2) {
+            RayPre<double> rp = make_ray<double>(mk<double>(r[0], r[1], r[2]), mk<double>(r[4], r[5], r[6]), r[3], r[7]);
+            h = trace<double>(*s, rp, false, false, &c);
+        } else {
+            RayPre<float> rp = make_ray<float>(mk<float>(r[0], r[1], r[2]), mk<float>(r[4], r[5], r[6]), r[3], r[7]);
+            h = trace<float>(*s, rp, false, mode == 0, &c);
+        }
+        add_counts(counts, c);
+        ids[4 * i + 0] = h.valid ? 1u : 0u;
+        ids[4 * i + 1] = h.valid ? s->flat_instance[h.flat] : 0u;
+        ids[4 * i + 2] = h.valid ? s->flat_prim[h.flat] : 0u;
+        ids[4 * i + 3] = h.valid ? h.flat : 0xffffffffu;
+        tb[3 * i + 0] = (float)h.t;
+        tb[3 * i + 1] = (float)h.b1;
+        tb[3 * i + 2] = (float)h.b2;
+    }
+}
+
+void oracle_visibility(void* sp, const float* rays, int count, int mode, float* vis, OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    for (int i = 0; i < count; ++i) {
+        const float* r = rays + 8 * (size_t)i;
+        HitRec h;
+        OracleRayCounts c{};
+        if (mode == 2) {
+            RayPre<double> rp = make_ray<double>(mk<double>(r[0], r[1], r[2]), mk<double>(r[4], r[5], r[6]), r[3], r[7]);
+            h = trace<double>(*s, rp, true, false, &c);
+        } else {
+            RayPre<float> rp = make_ray<float>(mk<float>(r[0], r[1], r[2]), mk<float>(r[4], r[5], r[6]), r[3], r[7]);
+            h = trace<float>(*s, rp, true, mode == 0, &c);
+        }
+        add_counts(counts, c);
+        vis[i] = h.valid ? 0.0f : 1.0f;
+    }
+}
+
+int oracle_trace_screen(void* sp, const OracleLighting* lighting, const OracleCamera* camera, uint32_t width,
+                        uint32_t height, uint32_t frame, uint32_t max_vertices, const uint32_t* pixels,
+                        int pixel_count, int precision, int threads, float* out, OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    std::vector<OracleRayCounts> per(std::max(1, threads <= 0 ? (int)std::thread::hardware_concurrency() : threads) + 1);
+    std::vector<OracleRayCounts> unit_counts((size_t)pixel_count);
+    parallel_for(pixel_count, threads, [&](int i, int) {
+        uint32_t px = pixels[2 * i], py = pixels[2 * i + 1];
+        if (precision == ORACLE_F64) {
+            Tracer<double> tr(*s, *lighting);
+            screen_pixel<double>(tr, *lighting, *camera, width, height, frame, max_vertices, px, py, out + 4 * (size_t)i);
+            unit_counts[i] = tr.cnt;
+        } else {
+            Tracer<float> tr(*s, *lighting);
+            screen_pixel<float>(tr, *lighting, *camera, width, height, frame, max_vertices, px, py, out + 4 * (size_t)i);
+            unit_counts[i] = tr.cnt;
+        }
+    });
+    for (auto& c : unit_counts) add_counts(counts, c);
+    return 0;
+}
+
+int oracle_trace_texels(void* sp, const OracleLighting* lighting, uint8_t* slots, uint32_t payload_count,
+                        const uint32_t* face_infos, uint32_t face_count, const uint32_t* instance_infos,
+                        const uint32_t* side_infos, uint32_t instance_count, const uint32_t* units, int unit_count,
+                        uint32_t iteration, uint32_t spt, uint32_t max_bounces, int reset, int precision, int threads,
+                        OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    (void)face_count;
+    std::vector<OracleRayCounts> unit_counts((size_t)unit_count);
+    std::atomic<int> bad{0};
+    parallel_for(unit_count, threads, [&](int u, int) {
+        uint32_t inst_index = units[2 * u], local = units[2 * u + 1];
+        if (inst_index >= instance_count) { bad = 1; return; }
+        InstInfo inst{instance_infos[4 * inst_index], instance_infos[4 * inst_index + 1],
+                      instance_infos[4 * inst_index + 2], instance_infos[4 * inst_index + 3]};
+        uint32_t back_offset = side_infos[2 * inst_index], side_flags = side_infos[2 * inst_index + 1];
+        if (local >= inst.texel_count) return;
+        FaceInfo face;
+        uint32_t prim;
+        if (!find_face(face_infos, inst, local, &face, &prim)) return;
+        uint32_t global_texel = inst.texel_offset + local;
+        uint32_t i, j;
+        address_to_ij(local - face.address, face.resolution, &i, &j);
+        float rf = (float)face.resolution;
+        float base_x = (float)i / rf, base_y = (float)j / rf;
+        uint32_t n = std::max(spt, 1u);
+        Rng rng(global_texel, inst_index, iteration * n);
+        float bx = base_x, by = base_y;
+        for (uint32_t attempt = 0; attempt < 32; ++attempt) {
+            float r0 = rng.next_1d(), r1 = rng.next_1d();
+            float cx = base_x + (r0 - 0.5f) / rf;
+            float cy = base_y + (r1 - 0.5f) / rf;
+            if (cx < 0.0f || cy < 0.0f || cx + cy > 1.0f) continue;
+            if (nearest_texel(cx, cy, (1.0f - cx) - cy, inst, face) == global_texel) {
+                bx = cx;
+                by = cy;
+                break;
+            }
+        }
+        float hb1 = by, hb2 = std::max(0.0f, (1.0f - bx) - by);
+        bool two = (side_flags & 1u) != 0;
+        float front[3], back[3];
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            Tracer<T> tr(*s, *lighting);
+            V3<T> fnrm = world_flat_normal<T>(*s, inst_index, prim);
+            V3<T> f = ts_estimate<T>(tr, inst_index, prim, T(hb1), T(hb2), fnrm, n, rng, max_bounces);
+            front[0] = (float)f.x; front[1] = (float)f.y; front[2] = (float)f.z;
+            if (two) {
+                V3<T> b = ts_estimate<T>(tr, inst_index, prim, T(hb1), T(hb2), -fnrm, n, rng, max_bounces);
+                back[0] = (float)b.x; back[1] = (float)b.y; back[2] = (float)b.z;
+            }
+            unit_counts[u] = tr.cnt;
+        };
+        if (precision == ORACLE_F64) run(double(0)); else run(float(0));
+        if (global_texel >= payload_count) { bad = 1; return; }
+        store_running_mean(slots, global_texel, front, reset != 0);
+        if (two) {
+            uint32_t bt = back_offset + (global_texel - inst.texel_offset);
+            if (bt >= payload_count) { bad = 1; return; }
+            store_running_mean(slots, bt, back, reset != 0);
+        }
+    });
+    for (auto& c : unit_counts) add_counts(counts, c);
+    if (bad) { g_error = "texel index out of range"; return 1; }
+    return 0;
+}
+
+int oracle_trace_probes(void* sp, const OracleLighting* lighting, float* values, uint32_t* sample_counts,
+                        uint32_t* self_hits, uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                        const uint8_t* probe_instances, uint32_t probe_instance_count, const uint32_t* units,
+                        int unit_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset,
+                        int precision, int threads, OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    (void)probe_instance_count;
+    ProbeBuffers b{values, sample_counts, self_hits, radial};
+    std::vector<OracleRayCounts> unit_counts((size_t)unit_count);
+    parallel_for(unit_count, threads, [&](int u, int) {
+        uint32_t p = units[u];
+        if (p >= probe_count) return;
+        if (precision == ORACLE_F64) {
+            Tracer<double> tr(*s, *lighting);
+            probe_unit<double>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0);
+            unit_counts[u] = tr.cnt;
+        } else {
+            Tracer<float> tr(*s, *lighting);
+            probe_unit<float>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0);
+            unit_counts[u] = tr.cnt;
+        }
+    });
+    for (auto& c : unit_counts) add_counts(counts, c);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,150 @@
+/* nan_oracle.h -- CPU restatement of the reference's path-integration math.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path:
+ * tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may load
+ * it; the product (nan_b200/) never does.
+ *
+ * Every function restates a reference Slang/Python function; the citation
+ * (path:line, relative to the reference project root) sits beside each
+ * definition in nan_oracle.cpp.
+ *
+ * Two precisions:
+ *   ORACLE_F32  float arithmetic in the reference's operation order (the
+ *               "spec" mode the CUDA kernels are compared with bit for bit);
+ *   ORACLE_F64  the same algorithm in double precision (the FP64 oracle the
+ *               converged estimates are compared with).
+ *
+ * Record layouts are the reference's (all little-endian, 4-byte words):
+ *   vertices        f32[V][8]   position, normal, uv      (scene.py:386-400)
+ *   indices         u32[T][3]   mesh-local vertex indices
+ *   mesh_descs      u32[M][4]   vertex_count, index_count, vertex_offset,
+ *                               index_offset              (scene.py:84-98)
+ *   instance_descs  u32[I][4]   mesh_id, material_id, transform_id, flags
+ *   transforms      f32[X][16]  row-major float4x4 (mul(M, float4(p, 1)))
+ *   inv_transposes  f32[X][16]  transpose(inverse(M))
+ *   materials       f32[N][8]   base_color.rgb, flags(u32), emissive.rgb, pad
+ */
+#ifndef NAN_ORACLE_H
+#define NAN_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORACLE_F32 = 0, ORACLE_F64 = 1 };
+
+typedef struct OracleLighting {
+    float sun_direction[3];
+    float sun_cos_half_angle;
+    float sun_color[3];
+    float sun_intensity;
+    float sun_transmittance[3];
+    float ray_t_max;
+    float sky_radiance[3];
+    uint32_t flags; /* bit 0: sun disk on primary misses */
+} OracleLighting;
+
+typedef struct OracleCamera {
+    float position[3];
+    float jitter_x;
+    float image_u[3];
+    float jitter_y;
+    float image_v[3];
+    float near_clip;
+    float image_w[3];
+    float far_clip;
+} OracleCamera;
+
+typedef struct OracleRayCounts {
+    uint64_t extend_rays;
+    uint64_t shadow_rays;
+    uint64_t node_fetches;
+    uint64_t triangle_tests;
+} OracleRayCounts;
+
+const char* oracle_last_error(void);
+
+/* ---- scalar building blocks ------------------------------------------- */
+void oracle_rng_sequence(uint32_t x, uint32_t y, uint32_t sample_index,
+                         int count, float* out);
+void oracle_sincos(const float* angles, int count, float* out_sin,
+                   float* out_cos);
+void oracle_pack_rgb9e5(const float* rgb, int count, uint32_t* out);
+void oracle_unpack_rgb9e5(const uint32_t* packed, int count, float* out_rgb);
+void oracle_f32_to_f16(const float* values, int count, uint16_t* out);
+void oracle_hemi_oct_encode(const float* dirs, int count, float* out_uv);
+void oracle_hemi_oct_decode(const float* uv, int count, float* out_dirs);
+void oracle_cosine_sample_hemisphere(const float* u, int count, float* out4);
+void oracle_mesh_colors_address_to_ij(const uint32_t* address,
+                                      const uint32_t* resolution, int count,
+                                      uint32_t* out_ij);
+
+/* ---- scenes ------------------------------------------------------------ */
+void* oracle_scene_create(const float* vertices, int vertex_count,
+                          const uint32_t* indices, int triangle_count,
+                          const uint32_t* mesh_descs, int mesh_count,
+                          const uint32_t* instance_descs, int instance_count,
+                          const float* transforms,
+                          const float* inverse_transposes,
+                          int transform_count, const float* materials,
+                          int material_count);
+void oracle_scene_destroy(void* scene);
+int oracle_scene_triangle_count(void* scene);
+/* World-space triangles in flat order (instance-major), f32[T][9]. */
+void oracle_scene_world_triangles(void* scene, float* out9);
+/* Binned-SAH (8 bins) BVH statistics: node count, leaf count, SAH cost. */
+void oracle_scene_bvh_stats(void* scene, double* out3);
+
+/* rays f32[N][8] = origin, t_min, dir, t_max.
+ * hits: u32[N][4] = valid, instance, primitive, flat index;
+ *       f32[N][3] = t, bary.x, bary.y.
+ * mode: 0 float BVH, 1 float brute force, 2 double brute force. */
+void oracle_intersect(void* scene, const float* rays, int count, int mode,
+                      uint32_t* out_hit_ids, float* out_hit_tb,
+                      OracleRayCounts* counts);
+void oracle_visibility(void* scene, const float* rays, int count, int mode,
+                       float* out_visibility, OracleRayCounts* counts);
+
+/* ---- integrators (float spec or FP64) ---------------------------------- */
+/* Screen path tracer (path_tracer.slang:86-130) for the listed pixels
+ * (u32 pairs x, y); writes float4 per listed pixel. */
+int oracle_trace_screen(void* scene, const OracleLighting* lighting,
+                        const OracleCamera* camera, uint32_t width,
+                        uint32_t height, uint32_t frame,
+                        uint32_t max_vertices, const uint32_t* pixels,
+                        int pixel_count, int precision, int threads,
+                        float* out_rgba, OracleRayCounts* counts);
+
+/* Texture-space tracer (texture_space_path_tracer.slang:140-216) for the
+ * listed (instance, instance-local texel) pairs. slots is the whole payload
+ * buffer (u32[P][4], RGB f32 bits + count) and is updated in place. */
+int oracle_trace_texels(void* scene, const OracleLighting* lighting,
+                        uint8_t* slots, uint32_t payload_count,
+                        const uint32_t* face_infos, uint32_t face_count,
+                        const uint32_t* instance_infos,
+                        const uint32_t* side_infos, uint32_t instance_count,
+                        const uint32_t* units, int unit_count,
+                        uint32_t iteration, uint32_t samples_per_texel,
+                        uint32_t max_bounces, int reset, int precision,
+                        int threads, OracleRayCounts* counts);
+
+/* Surface-probe irradiance baker (surface_probe_path_tracer.slang:280-315)
+ * for the listed probe indices. Buffers are updated in place. */
+int oracle_trace_probes(void* scene, const OracleLighting* lighting,
+                        float* values, uint32_t* sample_counts,
+                        uint32_t* self_hits, uint32_t* radial,
+                        const uint8_t* probes, uint32_t probe_count,
+                        const uint8_t* probe_instances,
+                        uint32_t probe_instance_count,
+                        const uint32_t* units, int unit_count,
+                        uint32_t iteration, uint32_t samples_per_probe,
+                        uint32_t max_bounces, int reset, int precision,
+                        int threads, OracleRayCounts* counts);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,327 @@
+"""ctypes binding of the CPU oracle (``liboracle.so``).
+
+TEST INFRASTRUCTURE ONLY. The oracle is the checker for the CUDA path; the
+product package ``nan_b200`` never imports this module. ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg are its only
+users.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+F32 = 0
+F64 = 1
+
+
+class OracleLighting(ctypes.Structure):
+    _fields_ = [
+        ("sun_direction", ctypes.c_float * 3),
+        ("sun_cos_half_angle", ctypes.c_float),
+        ("sun_color", ctypes.c_float * 3),
+        ("sun_intensity", ctypes.c_float),
+        ("sun_transmittance", ctypes.c_float * 3),
+        ("ray_t_max", ctypes.c_float),
+        ("sky_radiance", ctypes.c_float * 3),
+        ("flags", ctypes.c_uint32),
+    ]
+
+
+class OracleCamera(ctypes.Structure):
+    _fields_ = [
+        ("position", ctypes.c_float * 3),
+        ("jitter_x", ctypes.c_float),
+        ("image_u", ctypes.c_float * 3),
+        ("jitter_y", ctypes.c_float),
+        ("image_v", ctypes.c_float * 3),
+        ("near_clip", ctypes.c_float),
+        ("image_w", ctypes.c_float * 3),
+        ("far_clip", ctypes.c_float),
+    ]
+
+
+class OracleRayCounts(ctypes.Structure):
+    _fields_ = [
+        ("extend_rays", ctypes.c_uint64),
+        ("shadow_rays", ctypes.c_uint64),
+        ("node_fetches", ctypes.c_uint64),
+        ("triangle_tests", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name, _ in self._fields_}
+
+
+def build() -> Path:
+    """Compile liboracle.so (and, where the reference tree exists, _ref/)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _declare(_lib)
+    return _lib
+
+
+def _p(array: np.ndarray):
+    return array.ctypes.data_as(ctypes.c_void_p)
+
+
+def _declare(l: ctypes.CDLL) -> None:
+    vp, i, u32 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32
+    l.oracle_last_error.restype = ctypes.c_char_p
+    l.oracle_rng_sequence.argtypes = [u32, u32, u32, i, vp]
+    l.oracle_sincos.argtypes = [vp, i, vp, vp]
+    l.oracle_pack_rgb9e5.argtypes = [vp, i, vp]
+    l.oracle_unpack_rgb9e5.argtypes = [vp, i, vp]
+    l.oracle_f32_to_f16.argtypes = [vp, i, vp]
+    l.oracle_hemi_oct_encode.argtypes = [vp, i, vp]
+    l.oracle_hemi_oct_decode.argtypes = [vp, i, vp]
+    l.oracle_cosine_sample_hemisphere.argtypes = [vp, i, vp]
+    l.oracle_mesh_colors_address_to_ij.argtypes = [vp, vp, i, vp]
+    l.oracle_scene_create.restype = vp
+    l.oracle_scene_create.argtypes = [vp, i, vp, i, vp, i, vp, i, vp, vp, i, vp, i]
+    l.oracle_scene_destroy.argtypes = [vp]
+    l.oracle_scene_triangle_count.argtypes = [vp]
+    l.oracle_scene_world_triangles.argtypes = [vp, vp]
+    l.oracle_scene_bvh_stats.argtypes = [vp, vp]
+    l.oracle_intersect.argtypes = [vp, vp, i, i, vp, vp, vp]
+    l.oracle_visibility.argtypes = [vp, vp, i, i, vp, vp]
+    l.oracle_trace_screen.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, i, i, i, vp, vp]
+    l.oracle_trace_texels.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, u32, vp, i,
+                                      u32, u32, u32, i, i, i, vp]
+    l.oracle_trace_probes.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, vp, u32, vp, i,
+                                      u32, u32, u32, i, i, i, vp]
+
+
+# ---- scalar helpers --------------------------------------------------------
+
+def rng_sequence(x: int, y: int, sample_index: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.float32)
+    lib().oracle_rng_sequence(x, y, sample_index, count, _p(out))
+    return out
+
+
+def sincos(angles: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    a = np.ascontiguousarray(angles, dtype=np.float32)
+    s = np.zeros_like(a)
+    c = np.zeros_like(a)
+    lib().oracle_sincos(_p(a), a.size, _p(s), _p(c))
+    return s, c
+
+
+def pack_rgb9e5(rgb: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(rgb, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros(v.shape[0], dtype=np.uint32)
+    lib().oracle_pack_rgb9e5(_p(v), v.shape[0], _p(out))
+    return out
+
+
+def unpack_rgb9e5(packed: np.ndarray) -> np.ndarray:
+    p = np.ascontiguousarray(packed, dtype=np.uint32).reshape(-1)
+    out = np.zeros((p.size, 3), dtype=np.float32)
+    lib().oracle_unpack_rgb9e5(_p(p), p.size, _p(out))
+    return out
+
+
+def f32_to_f16(values: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+    out = np.zeros(v.size, dtype=np.uint16)
+    lib().oracle_f32_to_f16(_p(v), v.size, _p(out))
+    return out
+
+
+def hemi_oct_encode(dirs: np.ndarray) -> np.ndarray:
+    d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros((d.shape[0], 2), dtype=np.float32)
+    lib().oracle_hemi_oct_encode(_p(d), d.shape[0], _p(out))
+    return out
+
+
+def hemi_oct_decode(uv: np.ndarray) -> np.ndarray:
+    u = np.ascontiguousarray(uv, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros((u.shape[0], 3), dtype=np.float32)
+    lib().oracle_hemi_oct_decode(_p(u), u.shape[0], _p(out))
+    return out
+
+
+def cosine_sample_hemisphere(u: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(u, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros((a.shape[0], 4), dtype=np.float32)
+    lib().oracle_cosine_sample_hemisphere(_p(a), a.shape[0], _p(out))
+    return out
+
+
+def address_to_ij(address: np.ndarray, resolution: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(address, dtype=np.uint32)
+    r = np.ascontiguousarray(resolution, dtype=np.uint32)
+    out = np.zeros((a.size, 2), dtype=np.uint32)
+    lib().oracle_mesh_colors_address_to_ij(_p(a), _p(r), a.size, _p(out))
+    return out
+
+
+# ---- scenes and integrators ------------------------------------------------
+
+def lighting_struct(lighting) -> OracleLighting:
+    """Build the C struct from any object with the NanLighting field names."""
+    s = OracleLighting()
+    s.sun_direction[:] = [float(x) for x in lighting.sun_direction]
+    s.sun_cos_half_angle = float(lighting.sun_cos_half_angle)
+    s.sun_color[:] = [float(x) for x in lighting.sun_color]
+    s.sun_intensity = float(lighting.sun_intensity)
+    s.sun_transmittance[:] = [float(x) for x in lighting.sun_transmittance]
+    s.ray_t_max = float(lighting.ray_t_max)
+    s.sky_radiance[:] = [float(x) for x in lighting.sky_radiance]
+    s.flags = int(lighting.flags)
+    return s
+
+
+def camera_struct(camera) -> OracleCamera:
+    c = OracleCamera()
+    c.position[:] = [float(x) for x in camera.position]
+    c.image_u[:] = [float(x) for x in camera.image_u]
+    c.image_v[:] = [float(x) for x in camera.image_v]
+    c.image_w[:] = [float(x) for x in camera.image_w]
+    c.jitter_x = float(camera.jitter[0])
+    c.jitter_y = float(camera.jitter[1])
+    c.near_clip = float(camera.near_clip_plane)
+    c.far_clip = float(camera.far_clip_plane)
+    return c
+
+
+class OracleScene:
+    """CPU copy of a scene in the reference's record layouts."""
+
+    def __init__(self, vertices, indices, mesh_descs, instance_descs, transforms,
+                 inverse_transposes, materials):
+        self._keep = [
+            np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 8),
+            np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3),
+            np.ascontiguousarray(mesh_descs, dtype=np.uint32).reshape(-1, 4),
+            np.ascontiguousarray(instance_descs, dtype=np.uint32).reshape(-1, 4),
+            np.ascontiguousarray(transforms, dtype=np.float32).reshape(-1, 16),
+            np.ascontiguousarray(inverse_transposes, dtype=np.float32).reshape(-1, 16),
+            np.ascontiguousarray(materials, dtype=np.float32).reshape(-1, 8),
+        ]
+        v, ix, md, idesc, tr, it, mat = self._keep
+        self.handle = lib().oracle_scene_create(
+            _p(v), v.shape[0], _p(ix), ix.shape[0], _p(md), md.shape[0], _p(idesc),
+            idesc.shape[0], _p(tr), _p(it), tr.shape[0], _p(mat), mat.shape[0])
+
+    @classmethod
+    def from_scene(cls, scene) -> "OracleScene":
+        """From any object carrying the reference arrays as numpy/torch."""
+        def a(x):
+            return x.detach().cpu().numpy() if hasattr(x, "detach") else np.asarray(x)
+        return cls(a(scene.vertices), a(scene.indices), a(scene.mesh_descs),
+                   a(scene.instance_descs), a(scene.transforms),
+                   a(scene.inverse_transposes), a(scene.materials))
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().oracle_scene_destroy(self.handle)
+            self.handle = None
+
+    @property
+    def triangle_count(self) -> int:
+        return int(lib().oracle_scene_triangle_count(self.handle))
+
+    def world_triangles(self) -> np.ndarray:
+        out = np.zeros((self.triangle_count, 9), dtype=np.float32)
+        lib().oracle_scene_world_triangles(self.handle, _p(out))
+        return out
+
+    def bvh_stats(self) -> dict:
+        out = np.zeros(3, dtype=np.float64)
+        lib().oracle_scene_bvh_stats(self.handle, _p(out))
+        return {"nodes": int(out[0]), "leaves": int(out[1]), "sah_cost": float(out[2])}
+
+    def intersect(self, rays: np.ndarray, mode: int = 0):
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        ids = np.zeros((r.shape[0], 4), dtype=np.uint32)
+        tb = np.zeros((r.shape[0], 3), dtype=np.float32)
+        counts = OracleRayCounts()
+        lib().oracle_intersect(self.handle, _p(r), r.shape[0], mode, _p(ids), _p(tb),
+                               ctypes.byref(counts))
+        return ids, tb, counts.as_dict()
+
+    def visibility(self, rays: np.ndarray, mode: int = 0):
+        r = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        vis = np.zeros(r.shape[0], dtype=np.float32)
+        counts = OracleRayCounts()
+        lib().oracle_visibility(self.handle, _p(r), r.shape[0], mode, _p(vis),
+                                ctypes.byref(counts))
+        return vis, counts.as_dict()
+
+    def trace_screen(self, lighting, camera, width, height, frame, max_vertices,
+                     pixels, precision=F32, threads=0):
+        px = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+        out = np.zeros((px.shape[0], 4), dtype=np.float32)
+        counts = OracleRayCounts()
+        L = lighting_struct(lighting)
+        C = camera_struct(camera)
+        rc = lib().oracle_trace_screen(self.handle, ctypes.byref(L), ctypes.byref(C),
+                                       width, height, frame, max_vertices, _p(px),
+                                       px.shape[0], precision, threads, _p(out),
+                                       ctypes.byref(counts))
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return out, counts.as_dict()
+
+    def trace_texels(self, lighting, slots, face_infos, instance_infos, side_infos,
+                     units, iteration, samples_per_texel, max_bounces, reset,
+                     precision=F32, threads=0):
+        """Updates ``slots`` (uint32 [P,4] or uint8 [P,16]) in place."""
+        assert slots.flags["C_CONTIGUOUS"]
+        fi = np.ascontiguousarray(face_infos, dtype=np.uint32).reshape(-1, 2)
+        ii = np.ascontiguousarray(instance_infos, dtype=np.uint32).reshape(-1, 4)
+        si = np.ascontiguousarray(side_infos, dtype=np.uint32).reshape(-1, 2)
+        un = np.ascontiguousarray(units, dtype=np.uint32).reshape(-1, 2)
+        counts = OracleRayCounts()
+        L = lighting_struct(lighting)
+        payload = slots.nbytes // 16
+        rc = lib().oracle_trace_texels(self.handle, ctypes.byref(L), _p(slots), payload,
+                                       _p(fi), fi.shape[0], _p(ii), _p(si), ii.shape[0],
+                                       _p(un), un.shape[0], iteration, samples_per_texel,
+                                       max_bounces, int(bool(reset)), precision, threads,
+                                       ctypes.byref(counts))
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return counts.as_dict()
+
+    def trace_probes(self, lighting, values, sample_counts, self_hits, radial, probes,
+                     probe_instances, units, iteration, samples_per_probe, max_bounces,
+                     reset, precision=F32, threads=0):
+        """Updates values/sample_counts/self_hits/radial in place."""
+        for buf in (values, sample_counts, self_hits, radial):
+            assert buf.flags["C_CONTIGUOUS"]
+        pr = np.ascontiguousarray(probes).view(np.uint8).reshape(-1)
+        pi = np.ascontiguousarray(probe_instances).view(np.uint8).reshape(-1)
+        un = np.ascontiguousarray(units, dtype=np.uint32).reshape(-1)
+        counts = OracleRayCounts()
+        L = lighting_struct(lighting)
+        rc = lib().oracle_trace_probes(self.handle, ctypes.byref(L), _p(values),
+                                       _p(sample_counts), _p(self_hits), _p(radial), _p(pr),
+                                       pr.size // 48, _p(pi), pi.size // 48, _p(un), un.size,
+                                       iteration, samples_per_probe, max_bounces,
+                                       int(bool(reset)), precision, threads,
+                                       ctypes.byref(counts))
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return counts.as_dict()

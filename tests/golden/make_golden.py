@@ -1,0 +1,146 @@
+"""Generate golden input/output vectors from the reference's own Python code.
+
+Run in a container that holds the reference project (default root
+``/root/reference``, override with ``NAN_REFERENCE_ROOT``)::
+
+    python tests/golden/make_golden.py
+
+It imports the reference's numpy reference functions -- the RGB9E5 pack/unpack
+of ``test_mesh_colors_rgb9e5.py:15-50``, the hemi-oct encode/decode of
+``surface_probes.py:45-110``, the Mesh Colors lattice math of
+``mesh_colors.py:24-79`` and the FP64 brute-force any-hit caster of
+``vertex_baker/visibility_baker.py:348-402`` -- with the graphics-only modules
+(slangpy, trimesh, pygltflib, PIL) replaced by inert stand-ins, evaluates them
+on seeded inputs, and writes ``reference_vectors.npz`` next to this file.
+The GPU box never runs this script; tests read the committed ``.npz`` only.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = Path(os.environ.get("NAN_REFERENCE_ROOT", "/root/reference"))
+
+
+class _Inert:
+    """Stand-in for any attribute of a stubbed graphics module."""
+
+    def __init__(self, *args, **kwargs):
+        pass
+
+    def __call__(self, *args, **kwargs):
+        return _Inert()
+
+    def __getattr__(self, name):
+        return _Inert()
+
+
+def _stub(name: str) -> None:
+    module = types.ModuleType(name)
+    module.__getattr__ = lambda attr: _Inert  # type: ignore[attr-defined]
+    sys.modules[name] = module
+
+
+def _install_stubs() -> None:
+    for name in ("slangpy", "slangpy.math", "trimesh", "pygltflib", "PIL",
+                 "PIL.Image", "OpenEXR", "event_dispatching"):
+        _stub(name)
+    sys.modules["slangpy"].math = sys.modules["slangpy.math"]  # type: ignore[attr-defined]
+    scene_node = types.ModuleType("scene_node")
+    scene_node.SceneNode = _Inert  # type: ignore[attr-defined]
+    sys.modules["scene_node"] = scene_node
+
+
+def main() -> None:
+    _install_stubs()
+    sys.path.insert(0, str(REF))
+    sys.path.insert(0, str(REF / "vertex_baker"))
+
+    import mesh_colors  # noqa: E402
+    import surface_probes  # noqa: E402
+    import test_mesh_colors_rgb9e5 as rgb9e5_test  # noqa: E402
+    import visibility_baker  # noqa: E402
+
+    rng = np.random.default_rng(20261203)
+    out: dict[str, np.ndarray] = {}
+
+    # RGB9E5: the reference test's seven values first, then seeded values
+    # spread over the representable exponent range (plus clamped extremes).
+    golden = np.asarray(
+        [
+            [0.0, 0.0, 0.0],
+            [1.0, 1.0, 1.0],
+            [0.25, 0.5, 1.0],
+            [100.0, 10.0, 1.0],
+            [65408.0, 65408.0, 65408.0],
+            [-1.0, np.nan, np.inf],
+            [2.0**-24, 2.0**-20, 2.0**-16],
+        ],
+        dtype=np.float32,
+    )
+    magnitudes = np.exp2(rng.uniform(-28.0, 17.0, size=(4000, 1)))
+    randoms = (rng.uniform(0.0, 1.0, size=(4000, 3)) * magnitudes).astype(np.float32)
+    values = np.concatenate([golden, randoms], axis=0)
+    packed = np.asarray(
+        [rgb9e5_test._pack_rgb9e5_reference(v) for v in values], dtype=np.uint32
+    )
+    decoded = np.stack([rgb9e5_test._unpack_rgb9e5_reference(p) for p in packed])
+    out["rgb9e5_values"] = values
+    out["rgb9e5_packed"] = packed
+    out["rgb9e5_decoded"] = decoded.astype(np.float32)
+
+    # Hemi-oct: canonical directions of test_surface_probes.py:95-116, then a
+    # seeded hemisphere set as in its round-trip test.
+    canonical = np.asarray(
+        [[0, 0, 1], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0]], dtype=np.float32
+    )
+    dirs = rng.normal(size=(4096, 3)).astype(np.float32)
+    dirs[:, 2] = np.abs(dirs[:, 2])
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    dirs = np.concatenate([canonical, dirs], axis=0).astype(np.float32)
+    uv = surface_probes.surface_probe_hemi_oct_encode(dirs)
+    out["hemi_dirs"] = dirs
+    out["hemi_uv"] = uv.astype(np.float32)
+    out["hemi_decoded"] = surface_probes.surface_probe_hemi_oct_decode(uv).astype(np.float32)
+
+    # Mesh Colors lattice addressing.
+    addr, res, ij = [], [], []
+    for resolution in (1, 2, 4, 8, 16, 32, 64):
+        for address in range(mesh_colors.colors_per_patch(resolution)):
+            i, j = mesh_colors.address_to_ij(address, resolution)
+            assert mesh_colors.ij_to_address(i, j, resolution) == address
+            addr.append(address)
+            res.append(resolution)
+            ij.append((i, j))
+    out["mc_address"] = np.asarray(addr, dtype=np.uint32)
+    out["mc_resolution"] = np.asarray(res, dtype=np.uint32)
+    out["mc_ij"] = np.asarray(ij, dtype=np.uint32)
+
+    # Any-hit visibility against a seeded triangle soup with the reference's
+    # FP64 Moller-Trumbore brute force.
+    tris = rng.uniform(-1.0, 1.0, size=(64, 3, 3)).astype(np.float32)
+    origins = rng.uniform(-1.5, 1.5, size=(2048, 3)).astype(np.float32)
+    directions = rng.normal(size=(2048, 3)).astype(np.float32)
+    directions /= np.linalg.norm(directions, axis=1, keepdims=True)
+    directions = directions.astype(np.float32)
+    occluded = visibility_baker._intersects_any_bruteforce(
+        origins, directions, tris, max_distance=1.25, ray_epsilon=1e-6
+    )
+    out["vis_triangles"] = tris
+    out["vis_origins"] = origins
+    out["vis_directions"] = directions
+    out["vis_max_distance"] = np.asarray([1.25], dtype=np.float32)
+    out["vis_occluded"] = occluded.astype(np.uint8)
+
+    np.savez_compressed(HERE / "reference_vectors.npz", **out)
+    print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()
