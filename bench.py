@@ -290,8 +290,8 @@ def run_nan(args):
         it += 1
     torch.cuda.synchronize()
     device.check()
-    device.context.read_counters(reset=True)
-    launches0 = device.context.launch_count
+    scene.context.read_counters(reset=True)
+    launches0 = scene.context.launch_count
 
     clocks = ClockSampler(local)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -312,8 +312,8 @@ def run_nan(args):
     clock_info = clocks.stop()
     elapsed_ms = t0.elapsed_time(t1)
     launch_ms = [a.elapsed_time(b) for a, b in events]
-    launches = device.context.launch_count - launches0
-    counters = device.context.read_counters(reset=True)
+    launches = scene.context.launch_count - launches0
+    counters = scene.context.read_counters(reset=True)
     device.check()
     rays_local = counters["extend_rays"] + counters["shadow_rays"]
 
@@ -335,7 +335,7 @@ def run_nan(args):
     torch.cuda.synchronize()
     barrier()
     e2e_ms = e0.elapsed_time(e1)
-    e2e_counters = device.context.read_counters(reset=True)
+    e2e_counters = scene.context.read_counters(reset=True)
     e2e_rays_local = e2e_counters["extend_rays"] + e2e_counters["shadow_rays"]
 
     stats = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device=device.torch_device)

@@ -110,6 +110,10 @@ NAN_B200_API int nan_ctx_check(NanContext* ctx, void* stream) {
         set_error("a slot index fell outside the payload buffer (device status 2)");
         return NAN_ERR_INVALID_ARGUMENT;
     }
+    if (status & 4u) {
+        set_error("a texel or probe record names a triangle outside the scene (device status 4)");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
     return NAN_OK;
 }
 

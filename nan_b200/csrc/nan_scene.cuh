@@ -34,8 +34,20 @@ struct SceneView {
     const float* materials;         // f32[N][8]
     int root;
     uint32_t tri_count;
+    uint32_t instance_count;
     uint32_t* status;               // device status word
 };
+
+constexpr uint32_t kStatusBadRecord = 4u;
+
+// True when (instance, primitive) names a triangle of the scene; records that
+// do not are skipped by the kernels and flagged in the status word.
+__device__ __forceinline__ bool valid_prim(const SceneView& s, uint32_t inst, uint32_t prim) {
+    if (inst >= s.instance_count) return false;
+    const uint4 idesc = __ldg(s.instance_descs + inst);
+    const uint4 mdesc = __ldg(s.mesh_descs + idesc.x);
+    return prim < mdesc.y / 3u;
+}
 
 struct HitInfo {
     bool valid;

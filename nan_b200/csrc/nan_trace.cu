@@ -38,6 +38,7 @@ SceneView scene_view(const NanContext* ctx) {
     v.materials = ctx->scene.materials;
     v.root = ctx->root;
     v.tri_count = ctx->tri_count;
+    v.instance_count = ctx->scene.instance_count;
     v.status = ctx->d_status;
     return v;
 }
@@ -312,6 +313,10 @@ __global__ void __launch_bounds__(128) k_trace_texels(SceneView s, LightingRaw l
         }
     }
     if (!found) return;
+    if (!valid_prim(s, inst_index, prim)) {
+        atomicOr(s.status, kStatusBadRecord);
+        return;
+    }
     const uint32_t global_texel = inst.z + local;
     uint32_t ti, tj;
     mc_address_to_ij(local - face.x, face.y, &ti, &tj);
@@ -412,7 +417,7 @@ __device__ __forceinline__ void accumulate_radial_moment(uint32_t* __restrict__ 
 __global__ void __launch_bounds__(128) k_trace_probes(SceneView s, LightingRaw lraw, ProbeOut out,
                                                       const float4* __restrict__ probes,
                                                       const float4* __restrict__ pinst, uint32_t probe_count,
-                                                      uint32_t iteration, uint32_t spp, uint32_t max_bounces,
+                                                      uint32_t probe_instance_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces,
                                                       int reset, uint32_t begin, uint32_t end,
                                                       unsigned long long* counters) {
     const uint32_t p = begin + blockIdx.x * blockDim.x + threadIdx.x;
@@ -420,6 +425,10 @@ __global__ void __launch_bounds__(128) k_trace_probes(SceneView s, LightingRaw l
     const float4 nrm = __ldg(probes + 3u * p + 1u);
     const uint4 meta = __ldg(reinterpret_cast<const uint4*>(probes) + 3u * p + 2u);
     const uint32_t inst = meta.w >> 8;
+    if (inst >= probe_instance_count || !valid_prim(s, inst, meta.x)) {
+        atomicOr(s.status, kStatusBadRecord);
+        return;
+    }
     const float4 params = __ldg(pinst + 3u * inst + 2u);
     const float bx = __uint_as_float(meta.y), by = __uint_as_float(meta.z);
     const uint32_t prim = meta.x;
@@ -621,13 +630,13 @@ int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32
                         const uint8_t* probes, uint32_t probe_count, const uint8_t* probe_instances,
                         uint32_t probe_instance_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces,
                         int reset, const NanLighting* light, uint32_t begin, uint32_t end, cudaStream_t st) {
-    (void)probe_instance_count;
     end = std::min(end, probe_count);
     if (end <= begin) return NAN_OK;
     ProbeOut o{values, counts, self_hits, radial};
     k_trace_probes<<<blocks_for(end - begin, 128), 128, 0, st>>>(
         scene_view(ctx), to_raw(light), o, reinterpret_cast<const float4*>(probes),
-        reinterpret_cast<const float4*>(probe_instances), probe_count, iteration, spp, max_bounces, reset, begin, end,
+        reinterpret_cast<const float4*>(probe_instances), probe_count, probe_instance_count, iteration, spp,
+        max_bounces, reset, begin, end,
         ctx->d_counters);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "trace_probes launch");

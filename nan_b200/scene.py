@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -30,6 +31,13 @@ class Device:
         self.index = int(index)
         self.torch_device = torch.device("cuda", self.index)
         self.context = _native.Context(self.index)
+        self._contexts = weakref.WeakSet()
+
+    def new_context(self) -> _native.Context:
+        """A further native context on this device (one per scene/BVH)."""
+        ctx = _native.Context(self.index)
+        self._contexts.add(ctx)
+        return ctx
 
     def synchronize(self) -> None:
         import torch
@@ -37,8 +45,15 @@ class Device:
         torch.cuda.synchronize(self.torch_device)
 
     def check(self, stream=None) -> None:
-        """Raise if a kernel reported a device-side limit since the last check."""
+        """Raise if a kernel on this device reported a device-side limit or a
+        bad record since the last check (every context of the device)."""
         self.context.check(stream)
+        for ctx in list(self._contexts):
+            ctx.check(stream)
+
+    @property
+    def launch_count(self) -> int:
+        return self.context.launch_count + sum(c.launch_count for c in list(self._contexts))
 
 
 @dataclass
@@ -125,11 +140,13 @@ class Scene:
         desc.materials = ptr(self.materials)
         desc.material_count = packed["materials"].shape[0]
         self._desc = desc
-        check(lib().nan_scene_build(device.context.handle, ctypes.byref(desc), stream_handle(stream)))
+        self._context = device.new_context()
+        check(lib().nan_scene_build(self._context.handle, ctypes.byref(desc), stream_handle(stream)))
 
     @property
     def context(self) -> _native.Context:
-        return self.device.context
+        """The native context that owns this scene's BVH."""
+        return self._context
 
     def info(self) -> dict:
         info = NanSceneInfo()
