@@ -137,6 +137,28 @@ NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx);
  * (scene.py:386-533). The scene buffers must stay alive and unchanged while
  * the context traces them (shading reads them in place). Synchronises. */
 NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void* stream);
+/* nan_scene_build for callers that cannot allocate device memory: code that
+ * runs inside another framework's memory pool, or a real-time loop that must
+ * never call cudaMalloc/cudaFree. No counterpart in the reference (its BVH is
+ * built by the graphics driver).
+ *
+ * It allocates nothing. Build scratch comes from one fixed 64 MiB array in
+ * device memory (a file-scope __device__ array: every GPU that loads the
+ * library holds it until the process exits), enough for scenes of about 300k
+ * triangles; larger scenes return NAN_ERR_LIMIT. The BVH is written into the
+ * caller's buffers, which must stay alive while the context traces them:
+ *   out_nodes  >= 64 * max(T - 1, 1) bytes, 16-byte aligned
+ *   out_tris   >= 48 * T bytes, 16-byte aligned
+ *   out_refs   >= 8 * T bytes, 8-byte aligned
+ * where T is the number of triangles over all instances. The context must
+ * not hold a BVH from nan_scene_build. The first call on a device looks up
+ * the scratch array's device address (cudaGetSymbolAddress); make that first
+ * call before any stream capture. Every call shares the scratch array, so
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * Synchronises `stream`. */
+NAN_B200_API int nan_scene_build_noalloc(NanContext* ctx, const NanSceneDesc* desc, float* out_nodes,
+                                         uint64_t nodes_bytes, float* out_tris, uint64_t tris_bytes,
+                                         uint32_t* out_refs, uint64_t refs_bytes, void* stream);
 NAN_B200_API int nan_scene_info(NanContext* ctx, NanSceneInfo* out);
 /* World triangles in flat (instance-major) order, f32[T][9]; out may be a
  * device pointer of at least 36*T bytes. */

@@ -127,6 +127,7 @@ EXPORTS = {
     "nan_ctx_read_counters": (_I, [_VP, ctypes.POINTER(NanCounters), _I, _VP]),
     "nan_ctx_launch_count": (_U64, [_VP]),
     "nan_scene_build": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP]),
+    "nan_scene_build_noalloc": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP, _U64, _VP, _U64, _VP, _U64, _VP]),
     "nan_scene_info": (_I, [_VP, ctypes.POINTER(NanSceneInfo)]),
     "nan_scene_world_triangles": (_I, [_VP, _VP, _VP]),
     "nan_intersect": (_I, [_VP, _VP, _U32, _VP, _VP, _VP]),

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "nan_internal.h"
@@ -283,9 +284,12 @@ uint32_t blocks(uint64_t n) { return (uint32_t)((n + kThreads - 1) / kThreads); 
 namespace nan_host {
 
 void free_scene(NanContext* ctx) {
-    cudaFree(ctx->nodes);
-    cudaFree(ctx->tris);
-    cudaFree(ctx->tri_refs);
+    if (!ctx->caller_owned_bvh) {
+        cudaFree(ctx->nodes);
+        cudaFree(ctx->tris);
+        cudaFree(ctx->tri_refs);
+    }
+    ctx->caller_owned_bvh = false;
     ctx->nodes = nullptr;
     ctx->tris = nullptr;
     ctx->tri_refs = nullptr;
@@ -466,3 +470,216 @@ int world_triangles(NanContext* ctx, float* out, cudaStream_t s) {
 }
 
 }  // namespace nan_host
+
+// ---------------------------------------------------------------------------
+// nan_scene_build_noalloc: the scene build for callers that cannot allocate
+// device memory (code running where cudaMalloc is unavailable or forbidden,
+// e.g. inside another framework's memory pool or a real-time loop that must
+// never allocate). All scratch lives in the fixed array below; the BVH goes
+// into caller-provided buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Scratch shared by every nan_scene_build_noalloc call on a device. The CUDA
+// loader places one copy on each GPU that loads this library, held until the
+// process exits. Calls that overlap on the GPU race on it.
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device ordinal. In host code the
+// symbol is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress, taken once per device with that device current.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[128] = {};
+
+int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= 128) {
+        set_error("device ordinal out of range for the no-alloc scratch table");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_address[device] == nullptr) {
+        void* p = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (err != cudaSuccess) return cuda_fail(err, "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_address[device] = p;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_address[device]);
+    return NAN_OK;
+}
+
+// Bump carving of the static scratch, 256-byte aligned.
+struct Carver {
+    unsigned char* base;
+    size_t used = 0;
+    size_t capacity;
+    template <class T> T* take(size_t count) {
+        used = (used + 255u) & ~size_t(255u);
+        T* p = reinterpret_cast<T*>(base + used);
+        used += std::max<size_t>(count, 1) * sizeof(T);
+        return p;
+    }
+    bool fits() const { return used <= capacity; }
+};
+
+}  // namespace
+
+extern "C" NAN_B200_API int nan_scene_build_noalloc(NanContext* ctx, const NanSceneDesc* sd, float* out_nodes,
+                                                    uint64_t nodes_bytes, float* out_tris, uint64_t tris_bytes,
+                                                    uint32_t* out_refs, uint64_t refs_bytes, void* stream) {
+    if (!ctx || !sd) {
+        set_error("null context or scene description");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    cudaError_t err = cudaSetDevice(ctx->device);
+    if (err != cudaSuccess) return cuda_fail(err, "cudaSetDevice");
+    if (!ctx->caller_owned_bvh && (ctx->nodes || ctx->tris || ctx->tri_refs)) {
+        set_error("context holds a BVH allocated by nan_scene_build; use a context without one");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    // Forget the previous caller-owned BVH without freeing anything.
+    auto forget_bvh = [ctx]() {
+        ctx->nodes = nullptr;
+        ctx->tris = nullptr;
+        ctx->tri_refs = nullptr;
+        ctx->caller_owned_bvh = false;
+        ctx->has_scene = false;
+        ctx->tri_count = ctx->node_count = ctx->leaf_count = ctx->max_depth = 0;
+        ctx->device_bytes = 0;
+    };
+    if (sd->instance_count == 0 || !sd->vertices || !sd->indices || !sd->mesh_descs || !sd->instance_descs ||
+        !sd->transforms || !sd->inverse_transposes || !sd->materials) {
+        set_error("scene needs at least one instance and non-null buffers");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    if (!out_nodes || !out_tris || !out_refs || (reinterpret_cast<uintptr_t>(out_nodes) & 15u) ||
+        (reinterpret_cast<uintptr_t>(out_tris) & 15u) || (reinterpret_cast<uintptr_t>(out_refs) & 7u)) {
+        set_error("output buffers must be non-null; nodes and tris 16-byte aligned, refs 8-byte aligned");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* scratch = nullptr;
+    int rc = noalloc_scratch(ctx->device, &scratch);
+    if (rc) return rc;
+    const uint32_t I = sd->instance_count;
+
+    // Triangle count (per-instance counts + scan in the scratch).
+    Carver head{scratch, 0, kNoAllocScratchBytes};
+    uint32_t* counts = head.take<uint32_t>(I + 1);
+    uint32_t* offsets = head.take<uint32_t>(I + 1);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, counts, offsets, I + 1, s);
+    unsigned char* scan_tmp = head.take<unsigned char>(scan_bytes);
+    if (!head.fits()) {
+        set_error("too many instances for the no-alloc scratch (64 MiB)");
+        return NAN_ERR_LIMIT;
+    }
+    k_instance_counts<<<blocks(I + 1), kThreads, 0, s>>>(reinterpret_cast<const uint4*>(sd->instance_descs),
+                                                         reinterpret_cast<const uint4*>(sd->mesh_descs), I, counts);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, I + 1, s);
+    ctx->launches += 2;
+    uint32_t n = 0;
+    err = cudaMemcpyAsync(&n, offsets + I, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "no-alloc scene build (triangle count)");
+    if (n == 0) {
+        set_error("scene has no triangles");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    const uint32_t interior = n > 1 ? n - 1 : 0;
+    if (nodes_bytes < (uint64_t)std::max<uint32_t>(interior, 1) * 64u || tris_bytes < (uint64_t)n * 48u ||
+        refs_bytes < (uint64_t)n * 8u) {
+        set_error("output buffers too small: need 64*max(T-1,1) node, 48*T triangle and 8*T ref bytes");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+
+    // Carve the rest of the build's scratch after the offsets.
+    Carver c = head;
+    float4* tris_flat = c.take<float4>(3ull * n);
+    float4* lo_flat = c.take<float4>(n);
+    float4* hi_flat = c.take<float4>(n);
+    Bounds* bounds = c.take<Bounds>(1);
+    uint64_t* keys = c.take<uint64_t>(n);
+    uint64_t* keys_sorted = c.take<uint64_t>(n);
+    uint32_t* vals = c.take<uint32_t>(n);
+    uint32_t* order = c.take<uint32_t>(n);
+    float4* leaf_lo = c.take<float4>(n);
+    float4* leaf_hi = c.take<float4>(n);
+    int2* children = c.take<int2>(interior);
+    int* node_parent = c.take<int>(interior);
+    int* leaf_parent = c.take<int>(n);
+    float4* node_lo = c.take<float4>(interior);
+    float4* node_hi = c.take<float4>(interior);
+    uint32_t* arrivals = c.take<uint32_t>(interior);
+    uint32_t* depth = c.take<uint32_t>(1);
+    double* sah = c.take<double>(1);
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
+    unsigned char* sort_tmp = c.take<unsigned char>(sort_bytes);
+    if (!c.fits()) {
+        set_error("scene too large for the no-alloc scratch (64 MiB, about 300k triangles)");
+        return NAN_ERR_LIMIT;
+    }
+
+    // Previous calls leave their contents behind: clear what must start at zero.
+    Bounds init;
+    for (int a = 0; a < 3; ++a) {
+        init.lo[a] = 0xffffffffu;
+        init.hi[a] = 0u;
+    }
+    init.max_abs = 0u;
+    err = cudaMemcpyAsync(bounds, &init, sizeof(Bounds), cudaMemcpyHostToDevice, s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(arrivals, 0, std::max<uint32_t>(interior, 1) * sizeof(uint32_t), s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(depth, 0, sizeof(uint32_t), s);
+    if (err == cudaSuccess) err = cudaMemsetAsync(sah, 0, sizeof(double), s);
+    if (err != cudaSuccess) return cuda_fail(err, "no-alloc scene build (scratch clear)");
+
+    forget_bvh();
+    ctx->scene = *sd;
+    ctx->caller_owned_bvh = true;
+    ctx->nodes = reinterpret_cast<float4*>(out_nodes);
+    ctx->tris = reinterpret_cast<float4*>(out_tris);
+    ctx->tri_refs = reinterpret_cast<uint2*>(out_refs);
+    ctx->tri_count = n;
+    ctx->device_bytes = 0;
+
+    k_flatten<<<blocks(n), kThreads, 0, s>>>(*sd, offsets, n, tris_flat, ctx->tri_refs, lo_flat, hi_flat, bounds);
+    k_morton<<<blocks(n), kThreads, 0, s>>>(lo_flat, hi_flat, n, bounds, keys, vals);
+    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
+    k_gather_leaves<<<blocks(n), kThreads, 0, s>>>(order, n, tris_flat, lo_flat, hi_flat, ctx->tris, leaf_lo, leaf_hi);
+    ctx->launches += 4;
+    uint32_t max_depth = 1;
+    double sah_host = 1.0;
+    if (n == 1) {
+        ctx->root = ~0;
+        ctx->node_count = 0;
+    } else {
+        k_hierarchy<<<blocks(interior), kThreads, 0, s>>>(keys_sorted, (int)n, children, node_parent, leaf_parent);
+        k_refit<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, leaf_lo, leaf_hi, node_lo,
+                                               node_hi, arrivals);
+        k_depth<<<blocks(n), kThreads, 0, s>>>(n, node_parent, leaf_parent, depth);
+        k_emit<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_lo, node_hi, leaf_lo, leaf_hi, bounds,
+                                                     ctx->nodes, sah);
+        ctx->launches += 4;
+        ctx->root = 0;
+        ctx->node_count = interior;
+        cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+    }
+    err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) {
+        forget_bvh();
+        return cuda_fail(err, "no-alloc scene build");
+    }
+    ctx->leaf_count = n;
+    ctx->max_depth = max_depth;
+    ctx->sah_cost = sah_host;
+    ctx->build_ms = 0.0;
+    if (ctx->max_depth > 96u) {
+        forget_bvh();
+        set_error("BVH deeper than the traversal stack (96)");
+        return NAN_ERR_LIMIT;
+    }
+    ctx->has_scene = true;
+    return NAN_OK;
+}

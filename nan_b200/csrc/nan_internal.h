@@ -17,6 +17,7 @@ struct NanContext {
     NanSceneDesc scene{};
     bool has_scene = false;
     // BVH storage owned by the context.
+    bool caller_owned_bvh = false;  // BVH storage passed in by the caller (not freed here)
     float4* nodes = nullptr;        // 4 float4 per interior node
     float4* tris = nullptr;         // 3 float4 per triangle, leaf order
     uint2* tri_refs = nullptr;      // flat index -> (instance, primitive)
