@@ -49,6 +49,8 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--grid", type=int, default=313)
     ap.add_argument("--boxes", type=int, default=500)
+    ap.add_argument("--integrator", choices=["wavefront", "megakernel"], default="wavefront")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent traversal blocks per SM (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
@@ -279,6 +281,7 @@ def run_nan(args):
     scene = nan_b200.Scene(device, node)
     layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm)
     total = layout.total_surface_texels
     begin, end = total * rank // world, total * (rank + 1) // world
     slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
@@ -365,6 +368,7 @@ def run_nan(args):
             "workload": WORKLOAD, "triangles": scene.triangle_count, "surface_texels": total,
             "payload_slots": layout.total_payload_count, "samples_per_texel": 1, "max_bounces": 3,
             "parallelism": f"texel-range shards x{world}" if world > 1 else "single GPU",
+            "integrator": args.integrator,
             "l2": f"slot buffer {layout.total_payload_count * 16 / 1e6:.0f} MB read-modify-written per step "
                   "(> 126 MB L2)",
         },

@@ -109,6 +109,16 @@ typedef struct NanMeshColorsDesc {
     uint32_t payload_count;          /* slots in the payload buffer */
 } NanMeshColorsDesc;
 
+/* Execution choices of a context. The defaults (all zero) are the wavefront
+ * integrator with occupancy-sized persistent traversal grids and as many
+ * paths in flight as the reserved scratch holds. */
+typedef struct NanTuning {
+    uint32_t integrator;           /* 0: wavefront; 1: one thread per pixel/texel/probe */
+    uint32_t trace_blocks_per_sm;  /* persistent traversal blocks per SM, 0 = occupancy limit */
+    uint32_t max_paths_in_flight;  /* wavefront chunk size, 0 = as many as the scratch holds */
+    uint32_t reserved;
+} NanTuning;
+
 /* Device-side counters accumulated by the trace calls. */
 typedef struct NanCounters {
     uint64_t extend_rays;   /* closest-hit rays */
@@ -129,6 +139,13 @@ NAN_B200_API int nan_ctx_check(NanContext* ctx, void* stream);
 /* Synchronises `stream`, copies the counters, optionally zeroes them. */
 NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int reset,
                                        void* stream);
+/* Scratch arena for the wavefront integrator: path state and ray queues,
+ * nan_wavefront_bytes_per_path() bytes per path in flight. Allocates (grow
+ * only; never inside a trace call). Synchronises the device. */
+NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes);
+NAN_B200_API uint64_t nan_wavefront_bytes_per_path(void);
+/* Select the integrator form and its launch shapes (see NanTuning). */
+NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning);
 /* Number of kernels this context has launched. */
 NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx);
 

@@ -104,6 +104,18 @@ class NanMeshColorsDesc(ctypes.Structure):
     ]
 
 
+class NanTuning(ctypes.Structure):
+    _fields_ = [
+        ("integrator", ctypes.c_uint32),
+        ("trace_blocks_per_sm", ctypes.c_uint32),
+        ("max_paths_in_flight", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+INTEGRATORS = {"wavefront": 0, "megakernel": 1}
+
+
 class NanCounters(ctypes.Structure):
     _fields_ = [
         ("extend_rays", ctypes.c_uint64),
@@ -126,6 +138,9 @@ EXPORTS = {
     "nan_ctx_check": (_I, [_VP, _VP]),
     "nan_ctx_read_counters": (_I, [_VP, ctypes.POINTER(NanCounters), _I, _VP]),
     "nan_ctx_launch_count": (_U64, [_VP]),
+    "nan_ctx_reserve": (_I, [_VP, _U64]),
+    "nan_wavefront_bytes_per_path": (_U64, []),
+    "nan_ctx_configure": (_I, [_VP, ctypes.POINTER(NanTuning)]),
     "nan_scene_build": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP]),
     "nan_scene_build_noalloc": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP, _U64, _VP, _U64, _VP, _U64, _VP]),
     "nan_scene_info": (_I, [_VP, ctypes.POINTER(NanSceneInfo)]),
@@ -221,3 +236,20 @@ class Context:
     @property
     def launch_count(self) -> int:
         return int(lib().nan_ctx_launch_count(self.handle))
+
+    def reserve(self, scratch_bytes: int) -> None:
+        """Grow the wavefront scratch arena to at least scratch_bytes."""
+        check(lib().nan_ctx_reserve(self.handle, int(scratch_bytes)))
+
+    def reserve_paths(self, paths: int) -> None:
+        """Scratch for `paths` wavefront paths in flight (plus control words)."""
+        per = int(lib().nan_wavefront_bytes_per_path())
+        self.reserve(int(paths) * per + (1 << 22))
+
+    def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
+                  max_paths_in_flight: int = 0) -> None:
+        t = NanTuning()
+        t.integrator = INTEGRATORS[integrator]
+        t.trace_blocks_per_sm = int(trace_blocks_per_sm)
+        t.max_paths_in_flight = int(max_paths_in_flight)
+        check(lib().nan_ctx_configure(self.handle, ctypes.byref(t)))

@@ -87,6 +87,7 @@ NAN_B200_API int nan_ctx_destroy(NanContext* ctx) {
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     nan_host::free_scene(ctx);
+    cudaFree(ctx->scratch);
     cudaFree(ctx->d_status);
     cudaFree(ctx->d_counters);
     delete ctx;
@@ -130,6 +131,34 @@ NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int re
 }
 
 NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx) { return ctx ? ctx->launches : 0; }
+
+NAN_B200_API uint64_t nan_wavefront_bytes_per_path(void) { return nan_host::wavefront_bytes_per_path(); }
+
+NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (scratch_bytes <= ctx->scratch_bytes) return NAN_OK;
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) return cuda_fail(err, "reserve (synchronize)");
+    cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    err = cudaMalloc(&ctx->scratch, scratch_bytes);
+    if (err != cudaSuccess) {
+        ctx->scratch = nullptr;
+        return cuda_fail(err, "reserve wavefront scratch");
+    }
+    ctx->scratch_bytes = scratch_bytes;
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
+    if (!ctx || !tuning) return invalid("null argument");
+    if (tuning->integrator > 1) return invalid("integrator must be 0 (wavefront) or 1 (one thread per unit)");
+    if (tuning->trace_blocks_per_sm > 64) return invalid("trace_blocks_per_sm above 64");
+    ctx->tuning = *tuning;
+    return NAN_OK;
+}
 
 NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void* stream) {
     int rc = enter(ctx);
@@ -224,6 +253,9 @@ NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layo
         return invalid("slots and instance_infos must be 16-byte aligned");
     if (texel_end > layout->total_surface_texels) return invalid("texel range beyond the layout");
     if (max_bounces > 64) return invalid("max_bounces above 64");
+    if (ctx->tuning.integrator == 0)
+        return nan_host::launch_trace_texels_wavefront(ctx, layout, slots, iteration, samples_per_texel, max_bounces,
+                                                       reset, lighting, texel_begin, texel_end, as_stream(stream));
     return nan_host::launch_trace_texels(ctx, layout, slots, iteration, samples_per_texel, max_bounces, reset,
                                          lighting, texel_begin, texel_end, as_stream(stream));
 }

@@ -30,6 +30,10 @@ struct NanContext {
     double build_ms = 0.0;
     double sah_cost = 0.0;
     uint64_t launches = 0;
+    // Wavefront scratch arena (nan_ctx_reserve) and tuning (nan_ctx_configure).
+    void* scratch = nullptr;
+    uint64_t scratch_bytes = 0;
+    NanTuning tuning{};
 };
 
 namespace nan_host {
@@ -57,6 +61,10 @@ int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32
                         const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
                         uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
                         uint32_t begin, uint32_t end, cudaStream_t stream);
+size_t wavefront_bytes_per_path();
+int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* layout, uint8_t* slots,
+                                  uint32_t iteration, uint32_t spt, uint32_t max_bounces, int reset,
+                                  const NanLighting* light, uint32_t begin, uint32_t end, cudaStream_t stream);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

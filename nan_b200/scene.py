@@ -148,6 +148,12 @@ class Scene:
         """The native context that owns this scene's BVH."""
         return self._context
 
+    def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
+                  max_paths_in_flight: int = 0) -> None:
+        """Integrator form for passes on this scene: "wavefront" (default) or
+        "megakernel" (one thread per pixel/texel/probe), plus launch shapes."""
+        self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight)
+
     def info(self) -> dict:
         info = NanSceneInfo()
         check(lib().nan_scene_info(self.context.handle, ctypes.byref(info)))

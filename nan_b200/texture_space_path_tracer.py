@@ -18,7 +18,8 @@ class TextureSpacePathTracer:
     ``texel_range`` restricts the launch to surface texels [begin, end).
     """
 
-    def __init__(self, device, scene, layout, *, samples_per_texel: int = 1, max_bounces: int = 3):
+    def __init__(self, device, scene, layout, *, samples_per_texel: int = 1, max_bounces: int = 3,
+                 max_paths_in_flight: int | None = None):
         self.device = device
         self.scene = scene
         self.layout = layout
@@ -36,6 +37,9 @@ class TextureSpacePathTracer:
         d.total_surface_texels = layout.total_surface_texels
         d.payload_count = layout.total_payload_count
         self._desc = d
+        # wavefront scratch: one path per surface texel in flight (or the cap)
+        paths = layout.total_surface_texels if max_paths_in_flight is None else int(max_paths_in_flight)
+        scene.context.reserve_paths(max(1, min(paths, layout.total_surface_texels)))
 
     def execute(self, command_encoder, output, iteration: int, *, reset: bool = False,
                 texel_range: tuple[int, int] | None = None) -> None:

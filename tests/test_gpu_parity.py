@@ -151,11 +151,13 @@ def _layout_and_buffers(device, scene):
     return layout, slots
 
 
+@pytest.mark.parametrize("integrator", ["wavefront", "megakernel"])
 @pytest.mark.parametrize("which", ["cornell", "terrain"])
-def test_texel_tracer_matches_oracle(which, request, device):
+def test_texel_tracer_matches_oracle(which, integrator, request, device):
     import nan_b200
 
     scene, orc = request.getfixturevalue(which)
+    scene.configure(integrator)
     if which == "terrain":
         scene.lighting = nan_b200.Lighting.sun_elevation(45.0, azimuth_deg=30.0, irradiance=3.0, sky=0.5)
     layout, slots = _layout_and_buffers(device, scene)
@@ -185,6 +187,49 @@ def test_texel_tracer_matches_oracle(which, request, device):
     rel = np.max(np.abs(gv - ov) / np.maximum(np.abs(ov), 1e-3), axis=1)
     assert exact.mean() >= 0.999, exact.mean()
     assert (rel <= 1e-4).mean() >= 0.999
+    device.check()
+    scene.configure("wavefront")
+
+
+@pytest.mark.parametrize("spt,chunk", [(1, 0), (2, 5000), (1, 777)])
+def test_texel_wavefront_equals_megakernel(terrain, device, spt, chunk):
+    """Every slot of the full layout, several iterations, chunked wavefronts."""
+    import torch
+
+    import nan_b200
+
+    scene, _ = terrain
+    scene.lighting = nan_b200.Lighting.sun_elevation(45.0, azimuth_deg=30.0, irradiance=3.0, sky=0.5)
+    layout, slots_a = _layout_and_buffers(device, scene)
+    slots_b = torch.zeros_like(slots_a)
+    tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=spt, max_bounces=3)
+    for it in range(2):
+        scene.configure("megakernel")
+        tracer.execute(None, slots_a, it, reset=(it == 0))
+        scene.configure("wavefront", max_paths_in_flight=chunk)
+        tracer.execute(None, slots_b, it, reset=(it == 0))
+    scene.configure("wavefront")
+    torch.testing.assert_close(slots_b, slots_a, rtol=0, atol=0)
+    device.check()
+
+
+def test_texel_wavefront_two_sided(cornell, device):
+    """Cornell walls are double sided: back slots run after the front path."""
+    import torch
+
+    import nan_b200
+
+    scene, _ = cornell
+    layout, slots_a = _layout_and_buffers(device, scene)
+    assert (layout.side_array[:, 1] & 1).any()
+    slots_b = torch.zeros_like(slots_a)
+    tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=3, max_bounces=4)
+    for it in range(2):
+        scene.configure("megakernel")
+        tracer.execute(None, slots_a, it, reset=(it == 0))
+        scene.configure("wavefront")
+        tracer.execute(None, slots_b, it, reset=(it == 0))
+    torch.testing.assert_close(slots_b, slots_a, rtol=0, atol=0)
     device.check()
 
 
