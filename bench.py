@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--boxes", type=int, default=500)
     ap.add_argument("--integrator", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent traversal blocks per SM (0 = auto)")
+    ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
@@ -202,6 +203,7 @@ def roofline_bytes_per_ray(node, layout, lighting, sample_units: int = 6000):
     rays = c["extend_rays"] + c["shadow_rays"]
     n_node = c["node_fetches"] / rays
     n_tri = c["triangle_tests"] / rays
+    roofline_bytes_per_ray.sah_cost = orc.bvh_stats()["sah_cost"]
     return 32.0 + 16.0 + 32.0 * n_node + 36.0 * n_tri, n_node, n_tri
 
 
@@ -278,7 +280,7 @@ def run_nan(args):
 
     device = nan_b200.Device(local)
     node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
-    scene = nan_b200.Scene(device, node)
+    scene = nan_b200.Scene(device, node, bvh_builder=args.bvh)
     layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm)
@@ -369,6 +371,7 @@ def run_nan(args):
             "payload_slots": layout.total_payload_count, "samples_per_texel": 1, "max_bounces": 3,
             "parallelism": f"texel-range shards x{world}" if world > 1 else "single GPU",
             "integrator": args.integrator,
+            "bvh": args.bvh,
             "l2": f"slot buffer {layout.total_payload_count * 16 / 1e6:.0f} MB read-modify-written per step "
                   "(> 126 MB L2)",
         },
@@ -376,6 +379,8 @@ def run_nan(args):
         "extend_rays_per_step": counters["extend_rays"] / args.steps,
         "shadow_rays_per_step": counters["shadow_rays"] / args.steps,
         "bvh_build_ms": scene.info()["build_ms"],
+        "bvh_sah_cost": scene.info()["sah_cost"],
+        "reference_sah_cost": getattr(roofline_bytes_per_ray, "sah_cost", None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "bytes_per_ray": bytes_per_ray, "nodes_per_ray": n_node, "tris_per_ray": n_tri,

@@ -110,13 +110,13 @@ typedef struct NanMeshColorsDesc {
 } NanMeshColorsDesc;
 
 /* Execution choices of a context. The defaults (all zero) are the wavefront
- * integrator with occupancy-sized persistent traversal grids and as many
- * paths in flight as the reserved scratch holds. */
+ * integrator with occupancy-sized persistent traversal grids, as many paths
+ * in flight as the reserved scratch holds, and the PLOC BVH builder. */
 typedef struct NanTuning {
     uint32_t integrator;           /* 0: wavefront; 1: one thread per pixel/texel/probe */
     uint32_t trace_blocks_per_sm;  /* persistent traversal blocks per SM, 0 = occupancy limit */
     uint32_t max_paths_in_flight;  /* wavefront chunk size, 0 = as many as the scratch holds */
-    uint32_t reserved;
+    uint32_t bvh_builder;          /* nan_scene_build: 0 = PLOC + SAH leaf collapse, 1 = LBVH */
 } NanTuning;
 
 /* Device-side counters accumulated by the trace calls. */

@@ -109,11 +109,12 @@ class NanTuning(ctypes.Structure):
         ("integrator", ctypes.c_uint32),
         ("trace_blocks_per_sm", ctypes.c_uint32),
         ("max_paths_in_flight", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("bvh_builder", ctypes.c_uint32),
     ]
 
 
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
+BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
 
 class NanCounters(ctypes.Structure):
@@ -247,8 +248,9 @@ class Context:
         self.reserve(int(paths) * per + (1 << 22))
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0) -> None:
+                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc") -> None:
         t = NanTuning()
+        t.bvh_builder = BVH_BUILDERS[bvh_builder]
         t.integrator = INTEGRATORS[integrator]
         t.trace_blocks_per_sm = int(trace_blocks_per_sm)
         t.max_paths_in_flight = int(max_paths_in_flight)

@@ -262,11 +262,280 @@ __global__ void k_emit(uint32_t interior, const int2* __restrict__ children, con
     nodes[4u * i + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
     nodes[4u * i + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
     nodes[4u * i + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
-    nodes[4u * i + 3] = make_float4(__int_as_float(ch.x), __int_as_float(ch.y), 0.0f, 0.0f);
+    // leaves (single triangles in LBVH) as ~(first << 3 | count - 1)
+    const int rx = ch.x < 0 ? ~((~ch.x) << 3) : ch.x;
+    const int ry = ch.y < 0 ? ~((~ch.y) << 3) : ch.y;
+    nodes[4u * i + 3] = make_float4(__int_as_float(rx), __int_as_float(ry), 0.0f, 0.0f);
     const float root_area = fmaxf(half_area(node_lo[0], node_hi[0]), 1e-30f);
     double cost = (double)(half_area(node_lo[i], node_hi[i]) / root_area);  // one traversal step
     if (ch.x < 0) cost += (double)(half_area(al, ah) / root_area);          // one triangle per leaf
     if (ch.y < 0) cost += (double)(half_area(bl, bh) / root_area);
+    atomicAdd(sah, cost);
+}
+
+
+// ---------------------------------------------------------------------------
+// PLOC: parallel locally-ordered clustering (Meister and Bittner 2018).
+// Clusters start as the Morton-sorted triangles; every iteration each cluster
+// finds the neighbour within +-kPlocRadius positions whose union box has the
+// smallest surface area, mutual nearest neighbours merge into a new interior
+// node, and the cluster list is compacted (order preserved).
+// ---------------------------------------------------------------------------
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock = 256;
+constexpr int kMaxLeafTris = 4;
+
+__device__ __forceinline__ float area_union(float4 al, float4 ah, float4 bl, float4 bh) {
+    const float x = fmaxf(ah.x, bh.x) - fminf(al.x, bl.x);
+    const float y = fmaxf(ah.y, bh.y) - fminf(al.y, bl.y);
+    const float z = fmaxf(ah.z, bh.z) - fminf(al.z, bl.z);
+    return x * y + y * z + z * x;
+}
+
+__global__ void k_ploc_init(uint32_t n, int* __restrict__ idx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) idx[i] = ~(int)i;
+}
+
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(int c, const float4* __restrict__ lo,
+                                                         const float4* __restrict__ hi, int* __restrict__ nn) {
+    __shared__ float4 slo[kPlocBlock + 2 * kPlocRadius];
+    __shared__ float4 shi[kPlocBlock + 2 * kPlocRadius];
+    const int b0 = blockIdx.x * kPlocBlock;
+    for (int k = threadIdx.x; k < kPlocBlock + 2 * kPlocRadius; k += blockDim.x) {
+        const int g = b0 - kPlocRadius + k;
+        if (g >= 0 && g < c) {
+            slo[k] = lo[g];
+            shi[k] = hi[g];
+        }
+    }
+    __syncthreads();
+    const int i = b0 + (int)threadIdx.x;
+    if (i >= c) return;
+    const float4 ml = slo[threadIdx.x + kPlocRadius], mh = shi[threadIdx.x + kPlocRadius];
+    float best = INFINITY;
+    int bj = -1;
+    for (int dj = -kPlocRadius; dj <= kPlocRadius; ++dj) {
+        const int j = i + dj;
+        if (dj == 0 || j < 0 || j >= c) continue;
+        const float a = area_union(ml, mh, slo[threadIdx.x + kPlocRadius + dj], shi[threadIdx.x + kPlocRadius + dj]);
+        if (a < best) {  // ties keep the lower index (dj ascending)
+            best = a;
+            bj = j;
+        }
+    }
+    nn[i] = bj;
+}
+
+__global__ void k_ploc_merge(int c, const int* __restrict__ nn, const int* __restrict__ idx,
+                             const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ idx2,
+                             float4* __restrict__ lo2, float4* __restrict__ hi2, uint32_t* __restrict__ valid,
+                             int2* __restrict__ children, int* __restrict__ node_parent, int* __restrict__ leaf_parent,
+                             float4* __restrict__ node_lo, float4* __restrict__ node_hi, uint32_t* node_counter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c) return;
+    const int j = nn[i];
+    if (j >= 0 && nn[j] == i) {
+        if (i > j) {
+            valid[i] = 0u;
+            return;
+        }
+        const int id = (int)atomicAdd(node_counter, 1u);
+        const int a = idx[i], b = idx[j];
+        const float4 al = lo[i], ah = hi[i], bl = lo[j], bh = hi[j];
+        const float4 l = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.0f);
+        const float4 h = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.0f);
+        children[id] = make_int2(a, b);
+        if (a < 0) leaf_parent[~a] = id; else node_parent[a] = id;
+        if (b < 0) leaf_parent[~b] = id; else node_parent[b] = id;
+        node_lo[id] = l;
+        node_hi[id] = h;
+        idx2[i] = id;
+        lo2[i] = l;
+        hi2[i] = h;
+    } else {
+        idx2[i] = idx[i];
+        lo2[i] = lo[i];
+        hi2[i] = hi[i];
+    }
+    valid[i] = 1u;
+}
+
+__global__ void k_ploc_compact(int c, const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos,
+                               const int* __restrict__ idx2, const float4* __restrict__ lo2,
+                               const float4* __restrict__ hi2, int* __restrict__ idx, float4* __restrict__ lo,
+                               float4* __restrict__ hi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c || !valid[i]) return;
+    const uint32_t p = pos[i];
+    idx[p] = idx2[i];
+    lo[p] = lo2[i];
+    hi[p] = hi2[i];
+}
+
+__device__ __forceinline__ float half_area4(float4 l, float4 h) {
+    const float x = h.x - l.x, y = h.y - l.y, z = h.z - l.z;
+    return x * y + y * z + z * x;
+}
+
+// Bottom-up: triangle count, kept-interior count and SAH cost (relative to
+// the node's own area, C_trav = C_int = 1) of every subtree; a subtree of at
+// most kMaxLeafTris triangles collapses into one leaf when that is cheaper.
+struct SubtreeInfo {
+    uint32_t tris;
+    uint32_t interior;  // kept interior nodes (0 when collapsed)
+    float cost;
+    uint32_t collapsed;
+};
+
+__device__ __forceinline__ void child_info(int c, const SubtreeInfo* info, uint32_t* tris, uint32_t* interior,
+                                           float* cost) {
+    if (c < 0) {
+        *tris = 1u;
+        *interior = 0u;
+        *cost = 1.0f;
+    } else {
+        const volatile SubtreeInfo* v = info + c;  // written by the sibling's thread
+        *tris = v->tris;
+        *interior = v->interior;
+        *cost = v->cost;
+    }
+}
+
+__global__ void k_subtree(uint32_t n, const int2* __restrict__ children, const int* __restrict__ node_parent,
+                          const int* __restrict__ leaf_parent, const float4* __restrict__ leaf_lo,
+                          const float4* __restrict__ leaf_hi, const float4* __restrict__ node_lo,
+                          const float4* __restrict__ node_hi, SubtreeInfo* info, uint32_t* __restrict__ arrivals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = leaf_parent[i];
+    while (p >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0u) return;
+        const int2 ch = children[p];
+        uint32_t ta, ia, tb, ib;
+        float ca, cb;
+        child_info(ch.x, info, &ta, &ia, &ca);
+        child_info(ch.y, info, &tb, &ib, &cb);
+        const float ap = fmaxf(half_area4(node_lo[p], node_hi[p]), 1e-30f);
+        const float aa = ch.x < 0 ? half_area4(leaf_lo[~ch.x], leaf_hi[~ch.x]) : half_area4(node_lo[ch.x], node_hi[ch.x]);
+        const float ab = ch.y < 0 ? half_area4(leaf_lo[~ch.y], leaf_hi[~ch.y]) : half_area4(node_lo[ch.y], node_hi[ch.y]);
+        const float split = 1.0f + (aa * ca + ab * cb) / ap;
+        const uint32_t tris = ta + tb;
+        SubtreeInfo v;
+        v.tris = tris;
+        if (tris <= (uint32_t)kMaxLeafTris && (float)tris <= split) {
+            v.cost = (float)tris;
+            v.interior = 0u;
+            v.collapsed = 1u;
+        } else {
+            v.cost = split;
+            v.interior = 1u + ia + ib;
+            v.collapsed = 0u;
+        }
+        volatile SubtreeInfo* dst = info + p;
+        dst->tris = v.tris;
+        dst->interior = v.interior;
+        dst->cost = v.cost;
+        dst->collapsed = v.collapsed;
+        p = node_parent[p];
+    }
+}
+
+// Depth-first placement: walking up from a node or triangle to the root,
+// every step from a right child skips the left sibling's interior nodes (for
+// the node index) or triangles (for the triangle position). Nodes below a
+// collapsed ancestor are not emitted (dfs = -1).
+__global__ void k_dfs_nodes(uint32_t interior, const int2* __restrict__ children, const int* __restrict__ node_parent,
+                            const SubtreeInfo* __restrict__ info, int* __restrict__ dfs, uint32_t* __restrict__ tri_off) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= interior) return;
+    int node = (int)x;
+    int index = 0;
+    uint32_t toff = 0u;
+    bool hidden = false;
+    int p = node_parent[node];
+    while (p >= 0) {
+        const SubtreeInfo pi = info[p];
+        if (pi.collapsed) hidden = true;
+        const int2 ch = children[p];
+        index += 1;
+        if (ch.y == node) {
+            if (ch.x >= 0) {
+                const SubtreeInfo li = info[ch.x];
+                index += (int)li.interior;
+                toff += li.tris;
+            } else {
+                toff += 1u;
+            }
+        }
+        node = p;
+        p = node_parent[p];
+    }
+    dfs[x] = hidden ? -1 : index;
+    tri_off[x] = toff;
+}
+
+__global__ void k_dfs_leaves(uint32_t n, const int2* __restrict__ children, const int* __restrict__ node_parent,
+                             const int* __restrict__ leaf_parent, const SubtreeInfo* __restrict__ info,
+                             uint32_t* __restrict__ tri_pos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int node = ~(int)i;
+    uint32_t toff = 0u;
+    int p = leaf_parent[i];
+    while (p >= 0) {
+        const int2 ch = children[p];
+        if (ch.y == node) toff += ch.x >= 0 ? info[ch.x].tris : 1u;
+        node = p;
+        p = node_parent[p];
+    }
+    tri_pos[i] = toff;
+}
+
+__global__ void k_scatter_tris(uint32_t n, const uint32_t* __restrict__ tri_pos, const float4* __restrict__ src,
+                               float4* __restrict__ dst) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = tri_pos[i];
+    dst[3u * p] = src[3u * i];
+    dst[3u * p + 1] = src[3u * i + 1];
+    dst[3u * p + 2] = src[3u * i + 2];
+}
+
+__device__ __forceinline__ int child_ref(int c, const int* dfs, const uint32_t* tri_off, const uint32_t* tri_pos,
+                                         const SubtreeInfo* info) {
+    if (c < 0) return ~(int)(tri_pos[~c] << 3);
+    const SubtreeInfo v = info[c];
+    if (v.collapsed) return ~(int)((tri_off[c] << 3) | (v.tris - 1u));
+    return dfs[c];
+}
+
+__global__ void k_emit_dfs(uint32_t interior, const int2* __restrict__ children, const float4* __restrict__ node_lo,
+                           const float4* __restrict__ node_hi, const float4* __restrict__ leaf_lo,
+                           const float4* __restrict__ leaf_hi, const Bounds* __restrict__ bounds,
+                           const SubtreeInfo* __restrict__ info, const int* __restrict__ dfs,
+                           const uint32_t* __restrict__ tri_off, const uint32_t* __restrict__ tri_pos, int root,
+                           float4* __restrict__ nodes, double* __restrict__ sah) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= interior) return;
+    const int slot = dfs[x];
+    if (slot < 0 || info[x].collapsed) return;
+    const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;
+    const int2 ch = children[x];
+    float4 al, ah, bl, bh;
+    child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
+    child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
+    nodes[4u * slot + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
+    nodes[4u * slot + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
+    nodes[4u * slot + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
+    const int ra = child_ref(ch.x, dfs, tri_off, tri_pos, info);
+    const int rb = child_ref(ch.y, dfs, tri_off, tri_pos, info);
+    nodes[4u * slot + 3] = make_float4(__int_as_float(ra), __int_as_float(rb), 0.0f, 0.0f);
+    const float root_area = fmaxf(half_area4(node_lo[root], node_hi[root]), 1e-30f);
+    double cost = (double)(half_area4(node_lo[x], node_hi[x]) / root_area);
+    if (ra < 0) cost += (double)(half_area4(al, ah) / root_area) * (double)(((~ra) & 7) + 1);
+    if (rb < 0) cost += (double)(half_area4(bl, bh) / root_area) * (double)(((~rb) & 7) + 1);
     atomicAdd(sah, cost);
 }
 
@@ -296,6 +565,104 @@ void free_scene(NanContext* ctx) {
     ctx->has_scene = false;
     ctx->tri_count = ctx->node_count = ctx->leaf_count = ctx->max_depth = 0;
     ctx->device_bytes = 0;
+}
+
+
+// PLOC hierarchy over the Morton-sorted leaves, SAH leaf collapse, and a
+// depth-first emission of nodes and triangles (see the kernels above).
+int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const float4* leaf_lo, const float4* leaf_hi,
+               int2* children, int* node_parent, int* leaf_parent, float4* node_lo, float4* node_hi,
+               uint32_t* arrivals, uint32_t* depth, double* sah, const Bounds* bounds, cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    const uint32_t interior = n - 1;
+    int* idx_a = dmalloc<int>(n, s, &err);
+    int* idx_b = dmalloc<int>(n, s, &err);
+    float4* lo_a = dmalloc<float4>(n, s, &err);
+    float4* hi_a = dmalloc<float4>(n, s, &err);
+    float4* lo_b = dmalloc<float4>(n, s, &err);
+    float4* hi_b = dmalloc<float4>(n, s, &err);
+    int* nn = dmalloc<int>(n, s, &err);
+    uint32_t* valid = dmalloc<uint32_t>(n + 1, s, &err);
+    uint32_t* pos = dmalloc<uint32_t>(n + 1, s, &err);
+    uint32_t* counter = dmalloc<uint32_t>(2, s, &err);
+    SubtreeInfo* info = dmalloc<SubtreeInfo>(interior, s, &err);
+    int* dfs = dmalloc<int>(interior, s, &err);
+    uint32_t* tri_off = dmalloc<uint32_t>(interior, s, &err);
+    uint32_t* tri_pos = dmalloc<uint32_t>(n, s, &err);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, valid, pos, n + 1, s);
+    void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "PLOC scratch allocation");
+    cudaMemsetAsync(node_parent, 0xff, interior * sizeof(int), s);
+    cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), s);
+    cudaMemsetAsync(valid, 0, (n + 1) * sizeof(uint32_t), s);
+    k_ploc_init<<<blocks(n), kThreads, 0, s>>>(n, idx_a);
+    cudaMemcpyAsync(lo_a, leaf_lo, n * sizeof(float4), cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(hi_a, leaf_hi, n * sizeof(float4), cudaMemcpyDeviceToDevice, s);
+    ctx->launches++;
+    uint32_t c = n;
+    int iterations = 0;
+    while (c > 1) {
+        if (++iterations > 4096) {
+            set_error("PLOC did not converge");
+            return NAN_ERR_LIMIT;
+        }
+        const uint32_t grid = (c + kPlocBlock - 1) / kPlocBlock;
+        k_ploc_nn<<<grid, kPlocBlock, 0, s>>>((int)c, lo_a, hi_a, nn);
+        k_ploc_merge<<<blocks(c), kThreads, 0, s>>>((int)c, nn, idx_a, lo_a, hi_a, idx_b, lo_b, hi_b, valid, children,
+                                                    node_parent, leaf_parent, node_lo, node_hi, counter);
+        cudaMemsetAsync(valid + c, 0, sizeof(uint32_t), s);
+        cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, valid, pos, c + 1, s);
+        k_ploc_compact<<<blocks(c), kThreads, 0, s>>>((int)c, valid, pos, idx_b, lo_b, hi_b, idx_a, lo_a, hi_a);
+        ctx->launches += 4;
+        uint32_t next = 0;
+        err = cudaMemcpyAsync(&next, pos + c, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_fail(err, "PLOC iteration");
+        if (next >= c) {
+            set_error("PLOC made no progress");
+            return NAN_ERR_LIMIT;
+        }
+        c = next;
+    }
+    int root = 0;
+    cudaMemcpyAsync(&root, idx_a, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemsetAsync(arrivals, 0, interior * sizeof(uint32_t), s);
+    k_subtree<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, leaf_lo, leaf_hi, node_lo, node_hi,
+                                            info, arrivals);
+    k_dfs_nodes<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_parent, info, dfs, tri_off);
+    k_dfs_leaves<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, info, tri_pos);
+    k_scatter_tris<<<blocks(n), kThreads, 0, s>>>(n, tri_pos, tris_sorted, ctx->tris);
+    err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "PLOC collapse");
+    k_emit_dfs<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_lo, node_hi, leaf_lo, leaf_hi, bounds,
+                                                     info, dfs, tri_off, tri_pos, root, ctx->nodes, sah);
+    k_depth<<<blocks(n), kThreads, 0, s>>>(n, node_parent, leaf_parent, depth);
+    ctx->launches += 6;
+    SubtreeInfo root_info;
+    uint32_t max_depth = 0;
+    double sah_host = 0.0;
+    cudaMemcpyAsync(&root_info, info + root, sizeof(SubtreeInfo), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+    err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "PLOC emit");
+    for (void* p : {(void*)idx_a, (void*)idx_b, (void*)lo_a, (void*)hi_a, (void*)lo_b, (void*)hi_b, (void*)nn,
+                    (void*)valid, (void*)pos, (void*)counter, (void*)info, (void*)dfs, (void*)tri_off, (void*)tri_pos,
+                    scan_tmp})
+        cudaFreeAsync(p, s);
+    if (root_info.collapsed) {  // the whole scene is one leaf
+        ctx->root = ~(int)(n - 1u);
+        ctx->node_count = 0;
+        ctx->sah_cost = (double)n;
+    } else {
+        ctx->root = 0;
+        ctx->node_count = root_info.interior;
+        ctx->sah_cost = sah_host;
+    }
+    ctx->leaf_count = n;
+    ctx->max_depth = max_depth;
+    return NAN_OK;
 }
 
 int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
@@ -398,7 +765,10 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
     void* sort_tmp = dmalloc<uint8_t>(sort_bytes, s, &err);
     if (err != cudaSuccess) return cuda_fail(err, "scene build sort allocation");
     cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
-    k_gather_leaves<<<blocks(n), kThreads, 0, s>>>(order, n, tris_flat, lo_flat, hi_flat, ctx->tris, leaf_lo, leaf_hi);
+    const bool use_ploc = ctx->tuning.bvh_builder == 0 && n > 1;
+    float4* tris_sorted = use_ploc ? dmalloc<float4>(3ull * n, s, &err) : ctx->tris;
+    if (err != cudaSuccess) return cuda_fail(err, "scene build scratch allocation");
+    k_gather_leaves<<<blocks(n), kThreads, 0, s>>>(order, n, tris_flat, lo_flat, hi_flat, tris_sorted, leaf_lo, leaf_hi);
     ctx->launches += 4;
     if (n == 1) {
         ctx->root = ~0;
@@ -406,6 +776,11 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
         ctx->leaf_count = 1;
         ctx->max_depth = 1;
         ctx->sah_cost = 1.0;
+    } else if (use_ploc) {
+        int rc = build_ploc(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent, node_lo, node_hi,
+                            arrivals, depth, sah, bounds, s);
+        cudaFreeAsync(tris_sorted, s);
+        if (rc != NAN_OK) return rc;
     } else {
         // 5-7. hierarchy, refit, depth, emit
         k_hierarchy<<<blocks(interior), kThreads, 0, s>>>(keys_sorted, (int)n, children, node_parent, leaf_parent);

@@ -17,8 +17,9 @@ constexpr uint32_t kStatusStackOverflow = 1u;
 //   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
 //   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
 //   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
-//   d = (child0, child1, -, -): child >= 0 is an interior node, child < 0 a
-//       leaf holding the single triangle ~child (leaf order).
+//   d = (child0, child1, -, -): child >= 0 is an interior node; child < 0 a
+//       leaf of triangles [first, first + count) in leaf order, encoded as
+//       ~(first << 3 | (count - 1)) (1..8 triangles).
 // Triangles in leaf order: 3 float4 each, (v0, flat index bits), (v1, 0),
 // (v2, 0), world space.
 struct SceneView {
@@ -198,16 +199,19 @@ __device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d,
             if (h0) { node = nd.x; continue; }
             if (h1) { node = nd.y; continue; }
         } else {
-            const int tri = ~node;
-            f3 v0, v1, v2;
-            uint32_t flat;
-            load_tri(s, tri, &v0, &v1, &v2, &flat);
-            float t, V, W, det;
-            if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin &&
-                (t < best_t || (t == best_t && flat < best_key))) {
-                best_t = t;
-                best_key = flat;
-                best_tri = tri;
+            const int leaf = ~node;
+            const int first = leaf >> 3, last = first + (leaf & 7);
+            for (int tri = first; tri <= last; ++tri) {
+                f3 v0, v1, v2;
+                uint32_t flat;
+                load_tri(s, tri, &v0, &v1, &v2, &flat);
+                float t, V, W, det;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin &&
+                    (t < best_t || (t == best_t && flat < best_key))) {
+                    best_t = t;
+                    best_key = flat;
+                    best_tri = tri;
+                }
             }
         }
         if (sp == 0) break;
@@ -255,11 +259,15 @@ __device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float 
             if (h0) { node = nd.x; continue; }
             if (h1) { node = nd.y; continue; }
         } else {
-            f3 v0, v1, v2;
-            uint32_t flat;
-            load_tri(s, ~node, &v0, &v1, &v2, &flat);
-            float t, V, W, det;
-            if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) return true;
+            const int leaf = ~node;
+            const int first = leaf >> 3, last = first + (leaf & 7);
+            for (int tri = first; tri <= last; ++tri) {
+                f3 v0, v1, v2;
+                uint32_t flat;
+                load_tri(s, tri, &v0, &v1, &v2, &flat);
+                float t, V, W, det;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) return true;
+            }
         }
         if (sp == 0) break;
         node = stack[--sp];

@@ -107,7 +107,8 @@ class Lighting:
 class Scene:
     """Scene buffers on the GPU + BVH (replaces Scene.__init__/bind)."""
 
-    def __init__(self, device: Device, scene_node: SceneNode, lighting: Lighting | None = None, stream=None):
+    def __init__(self, device: Device, scene_node: SceneNode, lighting: Lighting | None = None, stream=None,
+                 bvh_builder: str = "ploc"):
         import torch
 
         self.device = device
@@ -115,6 +116,7 @@ class Scene:
         self.camera = scene_node.camera
         self.lighting = lighting or scene_node.lighting or Lighting()
         self.frame_index = 0
+        self.bvh_builder = bvh_builder
         packed = scene_node.pack()
         self.host = packed
         td = device.torch_device
@@ -141,6 +143,7 @@ class Scene:
         desc.material_count = packed["materials"].shape[0]
         self._desc = desc
         self._context = device.new_context()
+        self._context.configure(bvh_builder=bvh_builder)
         check(lib().nan_scene_build(self._context.handle, ctypes.byref(desc), stream_handle(stream)))
 
     @property
@@ -152,7 +155,7 @@ class Scene:
                   max_paths_in_flight: int = 0) -> None:
         """Integrator form for passes on this scene: "wavefront" (default) or
         "megakernel" (one thread per pixel/texel/probe), plus launch shapes."""
-        self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight)
+        self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder)
 
     def info(self) -> dict:
         info = NanSceneInfo()

@@ -11,10 +11,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _build(device, node):
+def _build(device, node, bvh_builder="ploc"):
     import nan_b200
 
-    scene = nan_b200.Scene(device, node)
+    scene = nan_b200.Scene(device, node, bvh_builder=bvh_builder)
     from oracle.oracle import OracleScene
 
     return scene, OracleScene(**scene.host)
@@ -56,16 +56,25 @@ def terrain(device):
     return _build(device, scenes.terrain_boxes(seed=1, grid=129, boxes=120))
 
 
-@pytest.mark.parametrize("which", ["cornell", "terrain"])
+@pytest.fixture(scope="module")
+def terrain_lbvh(device):
+    from nan_b200 import scenes
+
+    return _build(device, scenes.terrain_boxes(seed=1, grid=129, boxes=120), bvh_builder="lbvh")
+
+
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
 def test_bvh_world_triangles_match_oracle(which, request):
     scene, orc = request.getfixturevalue(which)
     np.testing.assert_array_equal(scene.world_triangles().cpu().numpy(), orc.world_triangles())
     info = scene.info()
     assert info["triangle_count"] == orc.triangle_count
     assert info["max_depth"] <= 96
+    if scene.bvh_builder == "ploc":  # SAH quality close to the binned-SAH reference
+        assert info["sah_cost"] <= 1.25 * orc.bvh_stats()["sah_cost"], (info["sah_cost"], orc.bvh_stats())
 
 
-@pytest.mark.parametrize("which", ["cornell", "terrain"])
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
 def test_closest_hit_bit_exact_vs_oracle(which, request):
     import torch
 
@@ -105,7 +114,7 @@ def test_closest_hit_vs_fp64_bruteforce(which, request):
     assert np.median(rel_t) <= 1e-6 and np.quantile(rel_t, 0.99) <= 1e-5, np.quantile(rel_t, [0.5, 0.99, 1])
 
 
-@pytest.mark.parametrize("which", ["cornell", "terrain"])
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
 def test_any_hit_bit_exact_vs_oracle(which, request):
     import torch
 
