@@ -110,6 +110,7 @@ class NanTuning(ctypes.Structure):
         ("trace_blocks_per_sm", ctypes.c_uint32),
         ("max_paths_in_flight", ctypes.c_uint32),
         ("bvh_builder", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 4),
     ]
 
 

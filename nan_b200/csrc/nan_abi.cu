@@ -156,6 +156,7 @@ NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
     if (!ctx || !tuning) return invalid("null argument");
     if (tuning->integrator > 1) return invalid("integrator must be 0 (wavefront) or 1 (one thread per unit)");
     if (tuning->trace_blocks_per_sm > 64) return invalid("trace_blocks_per_sm above 64");
+    if (tuning->bvh_builder > 1) return invalid("bvh_builder must be 0 (PLOC) or 1 (LBVH)");
     ctx->tuning = *tuning;
     return NAN_OK;
 }
