@@ -52,6 +52,7 @@ def parse_args():
     ap.add_argument("--integrator", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent traversal blocks per SM (0 = auto)")
     ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
+    ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
@@ -283,7 +284,7 @@ def run_nan(args):
     scene = nan_b200.Scene(device, node, bvh_builder=args.bvh)
     layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
-    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm)
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
     total = layout.total_surface_texels
     begin, end = total * rank // world, total * (rank + 1) // world
     slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
@@ -372,6 +373,7 @@ def run_nan(args):
             "parallelism": f"texel-range shards x{world}" if world > 1 else "single GPU",
             "integrator": args.integrator,
             "bvh": args.bvh,
+            "bvh_width": args.width,
             "l2": f"slot buffer {layout.total_payload_count * 16 / 1e6:.0f} MB read-modify-written per step "
                   "(> 126 MB L2)",
         },

@@ -117,7 +117,8 @@ typedef struct NanTuning {
     uint32_t trace_blocks_per_sm;  /* persistent traversal blocks per SM, 0 = occupancy limit */
     uint32_t max_paths_in_flight;  /* wavefront chunk size, 0 = as many as the scratch holds */
     uint32_t bvh_builder;          /* nan_scene_build: 0 = PLOC + SAH leaf collapse, 1 = LBVH */
-    uint32_t reserved[4];
+    uint32_t bvh_width;            /* traversed nodes: 0 or 2 = binary, 8 = compressed 8-wide (PLOC builds) */
+    uint32_t reserved[3];
 } NanTuning;
 
 /* Device-side counters accumulated by the trace calls. */

@@ -110,7 +110,8 @@ class NanTuning(ctypes.Structure):
         ("trace_blocks_per_sm", ctypes.c_uint32),
         ("max_paths_in_flight", ctypes.c_uint32),
         ("bvh_builder", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("bvh_width", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -249,9 +250,10 @@ class Context:
         self.reserve(int(paths) * per + (1 << 22))
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc") -> None:
+                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc", bvh_width: int = 2) -> None:
         t = NanTuning()
         t.bvh_builder = BVH_BUILDERS[bvh_builder]
+        t.bvh_width = 8 if int(bvh_width) == 8 else 2
         t.integrator = INTEGRATORS[integrator]
         t.trace_blocks_per_sm = int(trace_blocks_per_sm)
         t.max_paths_in_flight = int(max_paths_in_flight)

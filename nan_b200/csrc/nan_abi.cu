@@ -157,6 +157,8 @@ NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
     if (tuning->integrator > 1) return invalid("integrator must be 0 (wavefront) or 1 (one thread per unit)");
     if (tuning->trace_blocks_per_sm > 64) return invalid("trace_blocks_per_sm above 64");
     if (tuning->bvh_builder > 1) return invalid("bvh_builder must be 0 (PLOC) or 1 (LBVH)");
+    if (tuning->bvh_width != 0 && tuning->bvh_width != 2 && tuning->bvh_width != 8)
+        return invalid("bvh_width must be 0 or 2 (binary) or 8 (compressed wide)");
     ctx->tuning = *tuning;
     return NAN_OK;
 }

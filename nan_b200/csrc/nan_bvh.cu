@@ -283,7 +283,7 @@ __global__ void k_emit(uint32_t interior, const int2* __restrict__ children, con
 // ---------------------------------------------------------------------------
 constexpr int kPlocRadius = 16;
 constexpr int kPlocBlock = 256;
-constexpr int kMaxLeafTris = 4;
+constexpr int kMaxLeafTris = 3;  // the wide nodes' leaf encoding holds up to 3 triangles
 
 __device__ __forceinline__ float area_union(float4 al, float4 ah, float4 bl, float4 bh) {
     const float x = fmaxf(ah.x, bh.x) - fminf(al.x, bl.x);
@@ -539,6 +539,200 @@ __global__ void k_emit_dfs(uint32_t interior, const int2* __restrict__ children,
     atomicAdd(sah, cost);
 }
 
+
+// ---------------------------------------------------------------------------
+// Compressed 8-wide BVH (after Ylitie, Karras and Laine, "Efficient Incoherent
+// Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017), converted
+// top-down from the PLOC tree: each wide node takes up to 8 subtrees by
+// repeatedly opening the largest-area interior binary node, places them in
+// slots ordered by octant direction, stores its interior children
+// contiguously (child_base) and its leaf triangles contiguously (tri_base),
+// and quantizes the children's boxes to 8 bits against the node's box.
+// Node (80 B): w0 = (p.xyz, e.x | e.y << 8 | e.z << 16 | imask << 24)
+//              w1 = (child_base, tri_base, meta[0..3], meta[4..7])
+//              w2..w4 = qlo.x, qlo.y, qlo.z, qhi.x, qhi.y, qhi.z (8 bytes each)
+// meta[slot]: 0 empty; interior slots are marked in imask; a leaf slot holds
+// (unary triangle count) << 5 | (triangle offset from tri_base).
+// ---------------------------------------------------------------------------
+struct WideItem {
+    int bnode;      // binary node (>= 0) or leaf code (~sorted leaf)
+    uint32_t wnode;
+};
+
+__device__ __forceinline__ bool expandable(int c, const SubtreeInfo* info) { return c >= 0 && !info[c].collapsed; }
+
+__device__ __forceinline__ void entry_box(int c, const float4* node_lo, const float4* node_hi, const float4* leaf_lo,
+                                          const float4* leaf_hi, float4* lo, float4* hi) {
+    if (c < 0) {
+        *lo = leaf_lo[~c];
+        *hi = leaf_hi[~c];
+    } else {
+        *lo = node_lo[c];
+        *hi = node_hi[c];
+    }
+}
+
+__global__ void k_wide_level(const WideItem* __restrict__ items, uint32_t count, WideItem* __restrict__ items_out,
+                             uint32_t* __restrict__ counters, const int2* __restrict__ children,
+                             const float4* __restrict__ node_lo, const float4* __restrict__ node_hi,
+                             const float4* __restrict__ leaf_lo, const float4* __restrict__ leaf_hi,
+                             const SubtreeInfo* __restrict__ info, const uint32_t* __restrict__ tri_off,
+                             const uint32_t* __restrict__ tri_pos, const float4* __restrict__ tris_dfs,
+                             const Bounds* __restrict__ bounds, uint4* __restrict__ wnodes,
+                             float4* __restrict__ wtris) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const WideItem it = items[k];
+    int ent[8];
+    float4 elo[8], ehi[8];
+    int m = 0;
+    if (expandable(it.bnode, info)) {
+        const int2 ch = children[it.bnode];
+        ent[0] = ch.x;
+        ent[1] = ch.y;
+        m = 2;
+    } else {
+        ent[0] = it.bnode;  // a root that is a single leaf
+        m = 1;
+    }
+    for (int i = 0; i < m; ++i) entry_box(ent[i], node_lo, node_hi, leaf_lo, leaf_hi, &elo[i], &ehi[i]);
+    while (m < 8) {
+        int best = -1;
+        float best_area = -1.0f;
+        for (int i = 0; i < m; ++i) {
+            if (!expandable(ent[i], info)) continue;
+            const float a = half_area4(elo[i], ehi[i]);
+            if (a > best_area) {
+                best_area = a;
+                best = i;
+            }
+        }
+        if (best < 0) break;
+        const int2 ch = children[ent[best]];
+        ent[best] = ch.x;
+        ent[m] = ch.y;
+        entry_box(ent[best], node_lo, node_hi, leaf_lo, leaf_hi, &elo[best], &ehi[best]);
+        entry_box(ent[m], node_lo, node_hi, leaf_lo, leaf_hi, &elo[m], &ehi[m]);
+        ++m;
+    }
+    // node box and slot assignment by octant direction of each child's centre
+    float4 plo = elo[0], phi = ehi[0];
+    for (int i = 1; i < m; ++i) {
+        plo = make_float4(fminf(plo.x, elo[i].x), fminf(plo.y, elo[i].y), fminf(plo.z, elo[i].z), 0.0f);
+        phi = make_float4(fmaxf(phi.x, ehi[i].x), fmaxf(phi.y, ehi[i].y), fmaxf(phi.z, ehi[i].z), 0.0f);
+    }
+    const float pcx = 0.5f * (plo.x + phi.x), pcy = 0.5f * (plo.y + phi.y), pcz = 0.5f * (plo.z + phi.z);
+    float score[8][8];
+    for (int i = 0; i < m; ++i) {
+        const float vx = 0.5f * (elo[i].x + ehi[i].x) - pcx;
+        const float vy = 0.5f * (elo[i].y + ehi[i].y) - pcy;
+        const float vz = 0.5f * (elo[i].z + ehi[i].z) - pcz;
+        for (int sl = 0; sl < 8; ++sl)
+            score[i][sl] = ((sl & 1) ? vx : -vx) + ((sl & 2) ? vy : -vy) + ((sl & 4) ? vz : -vz);
+    }
+    int slot_of[8];
+    uint32_t used_slots = 0u, done = 0u;
+    for (int r = 0; r < m; ++r) {
+        float best = -INFINITY;
+        int bi = -1, bs = -1;
+        for (int i = 0; i < m; ++i) {
+            if (done & (1u << i)) continue;
+            for (int sl = 0; sl < 8; ++sl) {
+                if (used_slots & (1u << sl)) continue;
+                if (score[i][sl] > best || bi < 0) {
+                    best = score[i][sl];
+                    bi = i;
+                    bs = sl;
+                }
+            }
+        }
+        slot_of[bi] = bs;
+        done |= 1u << bi;
+        used_slots |= 1u << bs;
+    }
+    int slot_ent[8];
+    for (int sl = 0; sl < 8; ++sl) slot_ent[sl] = -1;
+    for (int i = 0; i < m; ++i) slot_ent[slot_of[i]] = i;
+    // allocation: interior children and leaf triangles, both in slot order
+    uint32_t n_int = 0u, n_tri = 0u;
+    for (int sl = 0; sl < 8; ++sl) {
+        const int i = slot_ent[sl];
+        if (i < 0) continue;
+        if (expandable(ent[i], info)) ++n_int;
+        else n_tri += ent[i] < 0 ? 1u : info[ent[i]].tris;
+    }
+    const uint32_t child_base = n_int ? atomicAdd(&counters[0], n_int) : 0u;
+    const uint32_t tri_base = n_tri ? atomicAdd(&counters[1], n_tri) : 0u;
+    const uint32_t out_base = n_int ? atomicAdd(&counters[2], n_int) : 0u;
+    // quantization grid: p = node lo, scale 2^e with 255 * 2^e >= extent
+    const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;
+    const double lo3[3] = {(double)plo.x - pad, (double)plo.y - pad, (double)plo.z - pad};
+    const double hi3[3] = {(double)phi.x + pad, (double)phi.y + pad, (double)phi.z + pad};
+    float p3[3];
+    int e3[3];
+    for (int a = 0; a < 3; ++a) {
+        p3[a] = (float)lo3[a];
+        if ((double)p3[a] > lo3[a]) p3[a] = nextafterf(p3[a], -INFINITY);  // p <= lo
+        const double ext = hi3[a] - (double)p3[a];
+        int e = -126;
+        if (ext > 0.0) {
+            e = (int)ceil(log2(ext / 255.0));
+            while (ldexp(255.0, e) < ext) ++e;
+            e = max(min(e, 127), -126);
+        }
+        e3[a] = e;
+    }
+    uint32_t imask = 0u, rank = 0u, toff = 0u;
+    uint8_t meta[8], qlo[3][8], qhi[3][8];
+    for (int sl = 0; sl < 8; ++sl) {
+        meta[sl] = 0u;
+        for (int a = 0; a < 3; ++a) {
+            qlo[a][sl] = 1u;  // empty slot: an inverted box
+            qhi[a][sl] = 0u;
+        }
+        const int i = slot_ent[sl];
+        if (i < 0) continue;
+        const double clo[3] = {(double)elo[i].x - pad, (double)elo[i].y - pad, (double)elo[i].z - pad};
+        const double chi[3] = {(double)ehi[i].x + pad, (double)ehi[i].y + pad, (double)ehi[i].z + pad};
+        for (int a = 0; a < 3; ++a) {
+            const double sc = ldexp(1.0, e3[a]);
+            const double ql = floor((clo[a] - (double)p3[a]) / sc);
+            const double qh = ceil((chi[a] - (double)p3[a]) / sc);
+            qlo[a][sl] = (uint8_t)fmax(0.0, fmin(255.0, ql));
+            qhi[a][sl] = (uint8_t)fmax(0.0, fmin(255.0, qh));
+        }
+        const int c = ent[i];
+        if (expandable(c, info)) {
+            imask |= 1u << sl;
+            items_out[out_base + rank] = WideItem{c, child_base + rank};
+            ++rank;
+        } else {
+            const uint32_t cnt = c < 0 ? 1u : info[c].tris;
+            const uint32_t src = c < 0 ? tri_pos[~c] : tri_off[c];
+            for (uint32_t t = 0; t < cnt; ++t) {
+                const uint32_t d = tri_base + toff + t;
+                wtris[3u * d + 0] = tris_dfs[3u * (src + t) + 0];
+                wtris[3u * d + 1] = tris_dfs[3u * (src + t) + 1];
+                wtris[3u * d + 2] = tris_dfs[3u * (src + t) + 2];
+            }
+            const uint32_t unary = cnt == 1u ? 1u : (cnt == 2u ? 3u : 7u);
+            meta[sl] = (uint8_t)((unary << 5) | toff);
+            toff += cnt;
+        }
+    }
+    auto pack4 = [](const uint8_t* b) {
+        return (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+    };
+    const uint32_t ebits = (uint32_t)(e3[0] + 127) | ((uint32_t)(e3[1] + 127) << 8) |
+                           ((uint32_t)(e3[2] + 127) << 16) | (imask << 24);
+    uint4* w = wnodes + 5u * it.wnode;
+    w[0] = make_uint4(__float_as_uint(p3[0]), __float_as_uint(p3[1]), __float_as_uint(p3[2]), ebits);
+    w[1] = make_uint4(child_base, tri_base, pack4(meta), pack4(meta + 4));
+    w[2] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));
+    w[3] = make_uint4(pack4(qlo[2]), pack4(qlo[2] + 4), pack4(qhi[0]), pack4(qhi[0] + 4));
+    w[4] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
+}
+
 template <class T> T* dmalloc(size_t count, cudaStream_t s, cudaError_t* err) {
     void* p = nullptr;
     cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
@@ -558,6 +752,11 @@ void free_scene(NanContext* ctx) {
         cudaFree(ctx->tris);
         cudaFree(ctx->tri_refs);
     }
+    cudaFree(ctx->wnodes);
+    cudaFree(ctx->wtris);
+    ctx->wnodes = nullptr;
+    ctx->wtris = nullptr;
+    ctx->wide_count = 0;
     ctx->caller_owned_bvh = false;
     ctx->nodes = nullptr;
     ctx->tris = nullptr;
@@ -635,6 +834,50 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     k_scatter_tris<<<blocks(n), kThreads, 0, s>>>(n, tri_pos, tris_sorted, ctx->tris);
     err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) return cuda_fail(err, "PLOC collapse");
+
+    // compressed 8-wide BVH from the collapsed binary tree, level by level
+    if (cudaMalloc(&ctx->wnodes, (size_t)(interior + 1) * 5 * sizeof(uint4)) != cudaSuccess ||
+        cudaMalloc(&ctx->wtris, (size_t)n * 3 * sizeof(float4)) != cudaSuccess) {
+        set_error("out of device memory for the wide BVH");
+        return NAN_ERR_OUT_OF_MEMORY;
+    }
+    ctx->device_bytes += (uint64_t)(interior + 1) * 5 * sizeof(uint4) + (uint64_t)n * 3 * sizeof(float4);
+    WideItem* items_a = dmalloc<WideItem>(interior + 1, s, &err);
+    WideItem* items_b = dmalloc<WideItem>(interior + 1, s, &err);
+    uint32_t* wcount = dmalloc<uint32_t>(3, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "wide BVH scratch allocation");
+    {
+        int root_host = 0;
+        cudaMemcpyAsync(&root_host, idx_a, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        const WideItem first{root_host, 0u};
+        const uint32_t init[3] = {1u, 0u, 0u};
+        cudaMemcpyAsync(items_a, &first, sizeof(WideItem), cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(wcount, init, sizeof(init), cudaMemcpyHostToDevice, s);
+        uint32_t level_count = 1u;
+        int levels = 0;
+        while (level_count > 0u) {
+            if (++levels > 256) {
+                set_error("wide BVH conversion did not terminate");
+                return NAN_ERR_LIMIT;
+            }
+            cudaMemsetAsync(wcount + 2, 0, sizeof(uint32_t), s);
+            k_wide_level<<<blocks(level_count), kThreads, 0, s>>>(items_a, level_count, items_b, wcount, children,
+                                                                  node_lo, node_hi, leaf_lo, leaf_hi, info, tri_off,
+                                                                  tri_pos, ctx->tris, bounds, ctx->wnodes, ctx->wtris);
+            ctx->launches++;
+            uint32_t counts[3];
+            err = cudaMemcpyAsync(counts, wcount, sizeof(counts), cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+            if (err != cudaSuccess) return cuda_fail(err, "wide BVH level");
+            level_count = counts[2];
+            ctx->wide_count = counts[0];
+            std::swap(items_a, items_b);
+        }
+    }
+    cudaFreeAsync(items_a, s);
+    cudaFreeAsync(items_b, s);
+    cudaFreeAsync(wcount, s);
     k_emit_dfs<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_lo, node_hi, leaf_lo, leaf_hi, bounds,
                                                      info, dfs, tri_off, tri_pos, root, ctx->nodes, sah);
     k_depth<<<blocks(n), kThreads, 0, s>>>(n, node_parent, leaf_parent, depth);

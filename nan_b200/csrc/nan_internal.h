@@ -21,6 +21,9 @@ struct NanContext {
     float4* nodes = nullptr;        // 4 float4 per interior node
     float4* tris = nullptr;         // 3 float4 per triangle, leaf order
     uint2* tri_refs = nullptr;      // flat index -> (instance, primitive)
+    uint4* wnodes = nullptr;        // compressed 8-wide nodes, 5 uint4 each (PLOC builds only)
+    float4* wtris = nullptr;        // triangles in the wide nodes' leaf order
+    uint32_t wide_count = 0;
     int root = 0;
     uint32_t tri_count = 0;
     uint32_t node_count = 0;

@@ -25,6 +25,8 @@ constexpr uint32_t kStatusStackOverflow = 1u;
 struct SceneView {
     const float4* nodes;
     const float4* tris;
+    const uint4* wnodes;            // compressed 8-wide nodes (null: use the binary nodes)
+    const float4* wtris;            // triangles in the wide leaf order
     const uint2* tri_refs;          // flat index -> (instance, primitive)
     const float* vertices;          // f32[V][8]
     const uint32_t* indices;        // u32[T][3]
@@ -161,10 +163,162 @@ __device__ __forceinline__ void box2(const BoxRay& r, float4 na, float4 nb, floa
     *h1 = lo1 <= hi1;
 }
 
+
+// ---------------------------------------------------------------------------
+// Compressed 8-wide traversal (node format in nan_bvh.cu). A group is
+// (first child index, interior-slot mask, remaining children as bits at
+// position slot ^ octant); popping the lowest bit visits the children of a
+// node roughly front to back for the ray's direction octant.
+// ---------------------------------------------------------------------------
+constexpr int kWideStack = 64;
+
+struct WideRay {
+    f3 o;
+    float ix, iy, iz;
+    uint32_t oct;
+};
+
+__device__ __forceinline__ WideRay wide_setup(f3 o, f3 d) {
+    WideRay r;
+    const float e = 1e-20f;
+    r.o = o;
+    r.ix = 1.0f / (fabsf(d.x) > e ? d.x : copysignf(e, d.x));
+    r.iy = 1.0f / (fabsf(d.y) > e ? d.y : copysignf(e, d.y));
+    r.iz = 1.0f / (fabsf(d.z) > e ? d.z : copysignf(e, d.z));
+    r.oct = (r.ix < 0.0f ? 1u : 0u) | (r.iy < 0.0f ? 2u : 0u) | (r.iz < 0.0f ? 4u : 0u);
+    return r;
+}
+
+__device__ __forceinline__ uint32_t octant_permute(uint32_t m, uint32_t oct) {
+    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m & 0xaau) >> 1);
+    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m & 0xccu) >> 2);
+    if (oct & 4u) m = ((m & 0x0fu) << 4) | ((m & 0xf0u) >> 4);
+    return m;
+}
+
+// Slots of the node whose (conservatively dequantized) boxes the ray enters
+// within [tmin, tmax].
+__device__ __forceinline__ uint32_t wide_hits(const WideRay& r, uint4 w0, uint4 w2, uint4 w3, uint4 w4, float tmin,
+                                              float tmax) {
+    const uint32_t eb = w0.w;
+    const float sx = __uint_as_float((eb & 0xffu) << 23);
+    const float sy = __uint_as_float(((eb >> 8) & 0xffu) << 23);
+    const float sz = __uint_as_float(((eb >> 16) & 0xffu) << 23);
+    const float ax = sx * r.ix, ay = sy * r.iy, az = sz * r.iz;
+    const float bx = (__uint_as_float(w0.x) - r.o.x) * r.ix;
+    const float by = (__uint_as_float(w0.y) - r.o.y) * r.iy;
+    const float bz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
+    // near / far planes by direction sign: qlo.x = w2.xy, qlo.y = w2.zw,
+    // qlo.z = w3.xy, qhi.x = w3.zw, qhi.y = w4.xy, qhi.z = w4.zw
+    const bool nx = r.ix >= 0.0f, ny = r.iy >= 0.0f, nz = r.iz >= 0.0f;
+    const uint32_t nxa = nx ? w2.x : w3.z, nxb = nx ? w2.y : w3.w, fxa = nx ? w3.z : w2.x, fxb = nx ? w3.w : w2.y;
+    const uint32_t nya = ny ? w2.z : w4.x, nyb = ny ? w2.w : w4.y, fya = ny ? w4.x : w2.z, fyb = ny ? w4.y : w2.w;
+    const uint32_t nza = nz ? w3.x : w4.z, nzb = nz ? w3.y : w4.w, fza = nz ? w4.z : w3.x, fzb = nz ? w4.w : w3.y;
+    uint32_t hits = 0u;
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl) {
+        const int sh = (sl & 3) * 8;
+        const uint32_t qnx = ((sl < 4 ? nxa : nxb) >> sh) & 0xffu, qfx = ((sl < 4 ? fxa : fxb) >> sh) & 0xffu;
+        const uint32_t qny = ((sl < 4 ? nya : nyb) >> sh) & 0xffu, qfy = ((sl < 4 ? fya : fyb) >> sh) & 0xffu;
+        const uint32_t qnz = ((sl < 4 ? nza : nzb) >> sh) & 0xffu, qfz = ((sl < 4 ? fza : fzb) >> sh) & 0xffu;
+        const float tn = fmaxf(fmaxf(__fmaf_rn((float)qnx, ax, bx), __fmaf_rn((float)qny, ay, by)),
+                               fmaxf(__fmaf_rn((float)qnz, az, bz), tmin));
+        const float tf = fminf(fminf(__fmaf_rn((float)qfx, ax, bx), __fmaf_rn((float)qfy, ay, by)),
+                               fminf(__fmaf_rn((float)qfz, az, bz), tmax));
+        if (tn <= tf) hits |= 1u << sl;
+    }
+    return hits;
+}
+
+__device__ __forceinline__ void load_wtri(const SceneView& s, uint32_t i, f3* v0, f3* v1, f3* v2, uint32_t* flat) {
+    const float4 a = __ldg(s.wtris + 3u * i);
+    const float4 b = __ldg(s.wtris + 3u * i + 1u);
+    const float4 c = __ldg(s.wtris + 3u * i + 2u);
+    *v0 = mk3(a.x, a.y, a.z);
+    *v1 = mk3(b.x, b.y, b.z);
+    *v2 = mk3(c.x, c.y, c.z);
+    *flat = __float_as_uint(a.w);
+}
+
+template <bool kAnyHit>
+__device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float tmin, float tmax, HitInfo* hit) {
+    const WtRay wr = wt_setup(d);
+    const WideRay r = wide_setup(o, d);
+    uint2 stack[kWideStack];
+    int sp = 0;
+    uint32_t g_base = 0u, g_imask = 1u, g_mask = 1u << r.oct;  // the root as slot 0 of a virtual group
+    float best_t = tmax;
+    uint32_t best_key = 0xffffffffu, best_tri = 0xffffffffu;
+    for (;;) {
+        if (g_mask == 0u) {
+            if (sp == 0) break;
+            const uint2 e = stack[--sp];
+            g_base = e.x;
+            g_imask = e.y >> 8;
+            g_mask = e.y & 0xffu;
+            continue;
+        }
+        const uint32_t pos = (uint32_t)__ffs(g_mask) - 1u;
+        g_mask &= g_mask - 1u;
+        const uint32_t slot = pos ^ r.oct;
+        const uint32_t child = g_base + (uint32_t)__popc(g_imask & ((1u << slot) - 1u));
+        if (g_mask != 0u) {
+            if (sp < kWideStack) stack[sp++] = make_uint2(g_base, (g_imask << 8) | g_mask);
+            else atomicOr(s.status, kStatusStackOverflow);
+        }
+        const uint4* w = s.wnodes + 5u * child;
+        const uint4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
+        const uint32_t imask = w0.w >> 24;
+        const uint32_t hits = wide_hits(r, w0, w2, w3, w4, tmin, kAnyHit ? tmax : best_t);
+        uint32_t leaf_hits = hits & ~imask;
+        while (leaf_hits != 0u) {
+            const uint32_t sl = (uint32_t)__ffs(leaf_hits) - 1u;
+            leaf_hits &= leaf_hits - 1u;
+            const uint32_t meta = ((sl < 4u ? w1.z : w1.w) >> ((sl & 3u) * 8u)) & 0xffu;
+            if (meta == 0u) continue;
+            const uint32_t first = w1.y + (meta & 31u);
+            const uint32_t cnt = (uint32_t)__popc(meta >> 5);
+            for (uint32_t k = 0; k < cnt; ++k) {
+                f3 v0, v1, v2;
+                uint32_t flat;
+                load_wtri(s, first + k, &v0, &v1, &v2, &flat);
+                float t, V, W, det;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin) {
+                    if (kAnyHit) {
+                        if (t <= tmax) return true;
+                    } else if (t < best_t || (t == best_t && flat < best_key)) {
+                        best_t = t;
+                        best_key = flat;
+                        best_tri = first + k;
+                    }
+                }
+            }
+        }
+        g_base = w1.x;
+        g_imask = imask;
+        g_mask = octant_permute(hits & imask, r.oct);
+    }
+    if (kAnyHit) return false;
+    if (best_tri != 0xffffffffu) {
+        f3 v0, v1, v2;
+        uint32_t flat;
+        load_wtri(s, best_tri, &v0, &v1, &v2, &flat);
+        float t, V, W, det;
+        wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det);
+        hit->valid = true;
+        hit->flat = best_key;
+        hit->t = best_t;
+        hit->b1 = V / det;
+        hit->b2 = W / det;
+        return true;
+    }
+    return false;
+}
+
 // Closest hit in [tmin, tmax]; ties in t go to the lower flat triangle index
 // (lexicographic (instance, primitive)), so the result does not depend on
-// the traversal order.
-__device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+// the traversal order. Binary-node traversal.
+__device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
     HitInfo hit;
     hit.valid = false;
     hit.flat = 0xffffffffu;
@@ -232,8 +386,8 @@ __device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d,
     return hit;
 }
 
-// Any hit in [tmin, tmax].
-__device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+// Any hit in [tmin, tmax]. Binary-node traversal.
+__device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
     if (s.tri_count == 0) return false;
     const WtRay wr = wt_setup(d);
     const BoxRay br = box_setup(o, d);
@@ -273,6 +427,40 @@ __device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float 
         node = stack[--sp];
     }
     return false;
+}
+
+// Width-specialised entry points (kWidth 2: binary nodes, 8: compressed
+// wide nodes) and a run-time dispatch for kernels that are not specialised.
+template <int kWidth>
+__device__ __forceinline__ HitInfo trace_closest_w(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    if (kWidth == 8) {
+        HitInfo hit;
+        hit.valid = false;
+        hit.flat = 0xffffffffu;
+        hit.t = tmax;
+        hit.b1 = 0.0f;
+        hit.b2 = 0.0f;
+        if (s.tri_count != 0) trace_wide<false>(s, o, d, tmin, tmax, &hit);
+        return hit;
+    }
+    return trace_closest_binary(s, o, d, tmin, tmax);
+}
+
+template <int kWidth>
+__device__ __forceinline__ bool trace_any_w(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    if (kWidth == 8) {
+        HitInfo unused;
+        return s.tri_count != 0 && trace_wide<true>(s, o, d, tmin, tmax, &unused);
+    }
+    return trace_any_binary(s, o, d, tmin, tmax);
+}
+
+__device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    return s.wnodes ? trace_closest_w<8>(s, o, d, tmin, tmax) : trace_closest_w<2>(s, o, d, tmin, tmax);
+}
+
+__device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    return s.wnodes ? trace_any_w<8>(s, o, d, tmin, tmax) : trace_any_w<2>(s, o, d, tmin, tmax);
 }
 
 // ---------------------------------------------------------------------------

@@ -29,6 +29,9 @@ SceneView scene_view(const NanContext* ctx) {
     SceneView v;
     v.nodes = ctx->nodes;
     v.tris = ctx->tris;
+    const bool wide = ctx->wnodes != nullptr && ctx->tuning.bvh_width == 8;
+    v.wnodes = wide ? ctx->wnodes : nullptr;
+    v.wtris = wide ? ctx->wtris : nullptr;
     v.tri_refs = ctx->tri_refs;
     v.vertices = ctx->scene.vertices;
     v.indices = ctx->scene.indices;

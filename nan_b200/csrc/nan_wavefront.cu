@@ -86,6 +86,7 @@ __device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.
 // ---------------------------------------------------------------------------
 // Generic traversal stages.
 // ---------------------------------------------------------------------------
+template <int kWidth>
 __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* __restrict__ queue,
                                                    uint32_t* ctl, const float4* __restrict__ ro,
                                                    const float4* __restrict__ rd, const uint32_t* __restrict__ flags,
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* 
             } else {
                 const float4 o = ro[p], d = rd[p];
                 tally.extend++;
-                const HitInfo h = trace_closest(s, xyz(o), xyz(d), o.w, d.w);
+                const HitInfo h = trace_closest_w<kWidth>(s, xyz(o), xyz(d), o.w, d.w);
                 hit[p] = make_float4(__uint_as_float(h.valid ? h.flat : 0xffffffffu), h.t, h.b1, h.b2);
             }
         }
@@ -114,6 +115,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* 
     flush_tally(counters, tally, 0u, 0u);
 }
 
+template <int kWidth>
 __global__ void __launch_bounds__(128) k_wf_shadow(SceneView s, const float4* __restrict__ queue, uint32_t* ctl,
                                                    float t_max, float4* __restrict__ rad, float4* __restrict__ si,
                                                    unsigned long long* counters) {
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(SceneView s, const float4* __
         if (idx < count) {
             const float4 a = queue[3u * idx], b = queue[3u * idx + 1u], c = queue[3u * idx + 2u];
             tally.shadow++;
-            if (!trace_any(s, xyz(a), xyz(b), 0.0f, t_max)) {
+            if (!trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, t_max)) {
                 const uint32_t p = __float_as_uint(a.w);
                 float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
                 const float4 v = target[p];
@@ -316,6 +318,9 @@ SceneView scene_view(const NanContext* ctx) {
     SceneView v;
     v.nodes = ctx->nodes;
     v.tris = ctx->tris;
+    const bool wide = ctx->wnodes != nullptr && ctx->tuning.bvh_width == 8;
+    v.wnodes = wide ? ctx->wnodes : nullptr;
+    v.wtris = wide ? ctx->wtris : nullptr;
     v.tri_refs = ctx->tri_refs;
     v.vertices = ctx->scene.vertices;
     v.indices = ctx->scene.indices;
@@ -346,7 +351,7 @@ Grid grid_for(const NanContext* ctx) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wf_extend, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wf_extend<2>, 128, 0);
     Grid g;
     const int per_sm = ctx->tuning.trace_blocks_per_sm ? (int)ctx->tuning.trace_blocks_per_sm : std::max(occ, 1);
     g.persistent_blocks = sms * per_sm;
@@ -427,11 +432,19 @@ int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay,
         for (uint32_t it = 0; it < iters; ++it) {
             const int buf = (int)(it & 1u);
             uint32_t* ctl = q.ctl + 4u * it;
-            k_wf_extend<<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                            ctx->d_counters);
+            if (s.wnodes)
+                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                                   ctx->d_counters);
+            else
+                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                                   ctx->d_counters);
             k_wf_texel_shade<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl);
-            k_wf_shadow<<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, lr.ray_t_max, S.rad, S.si,
-                                                            ctx->d_counters);
+            if (s.wnodes)
+                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, lr.ray_t_max, S.rad, S.si,
+                                                                   ctx->d_counters);
+            else
+                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, lr.ray_t_max, S.rad, S.si,
+                                                                   ctx->d_counters);
             k_wf_texel_finalize<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl, ctl + 4);
             ctx->launches += 4;
         }

@@ -74,11 +74,13 @@ def test_bvh_world_triangles_match_oracle(which, request):
         assert info["sah_cost"] <= 1.25 * orc.bvh_stats()["sah_cost"], (info["sah_cost"], orc.bvh_stats())
 
 
+@pytest.mark.parametrize("width", [2, 8])
 @pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
-def test_closest_hit_bit_exact_vs_oracle(which, request):
+def test_closest_hit_bit_exact_vs_oracle(which, width, request):
     import torch
 
     scene, orc = request.getfixturevalue(which)
+    scene.configure(bvh_width=width)
     rays = _random_rays(orc.world_triangles(), 20000, seed=7)
     ids, tb = scene.intersect(torch.from_numpy(rays).cuda())
     ids = ids.cpu().numpy().view(np.uint32)
@@ -88,6 +90,7 @@ def test_closest_hit_bit_exact_vs_oracle(which, request):
     valid = ids[:, 0] == 1
     np.testing.assert_array_equal(tb[valid], o_tb[valid])
     assert valid.mean() > 0.3
+    scene.configure()
 
 
 @pytest.mark.parametrize("which", ["cornell", "terrain"])
@@ -114,17 +117,20 @@ def test_closest_hit_vs_fp64_bruteforce(which, request):
     assert np.median(rel_t) <= 1e-6 and np.quantile(rel_t, 0.99) <= 1e-5, np.quantile(rel_t, [0.5, 0.99, 1])
 
 
+@pytest.mark.parametrize("width", [2, 8])
 @pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
-def test_any_hit_bit_exact_vs_oracle(which, request):
+def test_any_hit_bit_exact_vs_oracle(which, width, request):
     import torch
 
     scene, orc = request.getfixturevalue(which)
+    scene.configure(bvh_width=width)
     rays = _random_rays(orc.world_triangles(), 20000, seed=9)
     rays[:, 7] = np.random.default_rng(1).uniform(0.01, 3.0, rays.shape[0]).astype(np.float32)
     vis = scene.occluded(torch.from_numpy(rays).cuda()).cpu().numpy()
     o_vis, _ = orc.visibility(rays, mode=0)
     np.testing.assert_array_equal(vis, o_vis)
     assert 0.05 < vis.mean() < 0.95
+    scene.configure()
 
 
 def test_screen_path_tracer_matches_oracle(cornell, device):
