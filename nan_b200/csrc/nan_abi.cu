@@ -227,6 +227,9 @@ NAN_B200_API int nan_trace_screen(NanContext* ctx, float* out_rgba, uint32_t wid
     if (!camera || !lighting) return invalid("null camera or lighting");
     if ((width || height) && (!out_rgba || !aligned16(out_rgba))) return invalid("output must be 16-byte aligned");
     if (max_vertices > 64) return invalid("max_vertices above 64");
+    if (ctx->tuning.integrator == 0)
+        return nan_host::launch_trace_screen_wavefront(ctx, out_rgba, width, height, frame, max_vertices, camera,
+                                                       lighting, as_stream(stream));
     return nan_host::launch_trace_screen(ctx, out_rgba, width, height, frame, max_vertices, camera, lighting,
                                          as_stream(stream));
 }
@@ -279,6 +282,11 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
         return invalid("probe records must be 16-byte aligned");
     if (probe_end > probe_count) return invalid("probe range beyond probe_count");
     if (max_bounces > 64) return invalid("max_bounces above 64");
+    if (ctx->tuning.integrator == 0)
+        return nan_host::launch_trace_probes_wavefront(ctx, values, sample_counts, self_hits, radial, probes,
+                                                       probe_count, probe_instances, probe_instance_count, iteration,
+                                                       samples_per_probe, max_bounces, reset, lighting, probe_begin,
+                                                       probe_end, as_stream(stream));
     return nan_host::launch_trace_probes(ctx, values, sample_counts, self_hits, radial, probes, probe_count,
                                          probe_instances, probe_instance_count, iteration, samples_per_probe,
                                          max_bounces, reset, lighting, probe_begin, probe_end, as_stream(stream));

@@ -49,6 +49,9 @@ struct WfState {
     float4* irr;
     float2* zpdf;     // |z| and pdf of the sample's first direction
     float4* hit;      // flat bits (~0 = miss), t, b1, b2
+    float4* pa;       // probes: source instance bits, source primitive bits, source offset, first-hit distance
+    uint4* pb;        // probes: self-hit suspects of the sample, of all samples, previous count, radial texel
+    uint4* pc;        // probes: 2 per path, per-radial-texel sample counts (16 x u16)
 };
 
 struct WfQueues {
@@ -57,7 +60,7 @@ struct WfQueues {
     uint32_t* ctl;   // per iteration k: [4k] ext count, [4k+1] ext fetch, [4k+2] shd count, [4k+3] shd fetch
 };
 
-constexpr size_t kBytesPerPath = 4 + 4 + 4 + 16 * 9 + 8 + 2 * 4 + 2 * 2 * 48;
+constexpr size_t kBytesPerPath = 4 + 4 + 4 + 16 * 9 + 8 + 16 + 16 + 32 + 2 * 4 + 2 * 2 * 48;
 
 // Warp-aggregated append: returns this lane's slot in the queue.
 __device__ __forceinline__ uint32_t queue_slot(uint32_t* count, bool want) {
@@ -308,6 +311,336 @@ __global__ void __launch_bounds__(128) k_wf_texel_finalize(SceneView s, Lighting
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Screen path tracer stages (path_tracer.slang:40-130, camera.slang:201-236).
+// ---------------------------------------------------------------------------
+struct CameraWf {  // layout of NanCamera
+    float position[3];
+    float jitter_x;
+    float image_u[3];
+    float jitter_y;
+    float image_v[3];
+    float near_clip;
+    float image_w[3];
+    float far_clip;
+};
+
+struct ScreenArgs {
+    CameraWf cam;
+    float4* out;
+    uint32_t width, height, frame, max_vertices;
+};
+
+__global__ void __launch_bounds__(128) k_wf_screen_generate(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
+                                                            WfQueues q, uint32_t begin, uint32_t count,
+                                                            unsigned long long* counters) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const uint32_t pixel = begin + p;
+    const uint32_t px = pixel % a.width, py = pixel / a.width;
+    Rng rng(px, py, a.frame * 1u + 0u);
+    rng.next_1d();
+    rng.next_1d();  // the unused jitter draw (path_tracer.slang:121)
+    const CameraWf& cam = a.cam;
+    float pxf = ((float)px + 0.5f) / (float)a.width;
+    float pyf = ((float)py + 0.5f) / (float)a.height;
+    pxf = pxf + (-cam.jitter_x);
+    pyf = pyf + cam.jitter_y;
+    const float nx = 2.0f * pxf + -1.0f;
+    const float ny = -2.0f * pyf + 1.0f;
+    const f3 U = mk3(cam.image_u[0], cam.image_u[1], cam.image_u[2]);
+    const f3 V = mk3(cam.image_v[0], cam.image_v[1], cam.image_v[2]);
+    const f3 W = mk3(cam.image_w[0], cam.image_w[1], cam.image_w[2]);
+    const f3 dir = normalize3((nx * U + ny * V) + W);
+    const float inv_cos = 1.0f / dot3(normalize3(W), dir);
+    st.unit[p] = pixel;
+    st.rng[p] = rng.state;
+    st.flags[p] = 0u;
+    st.ro[p] = f4(mk3(cam.position[0], cam.position[1], cam.position[2]), cam.near_clip * inv_cos);
+    st.rd[p] = f4(dir, cam.far_clip * inv_cos);
+    st.thp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    st.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const uint32_t slot = queue_slot(q.ctl + 0, true);
+    q.ext[0][slot] = p;
+    RayTally none{0u, 0u};
+    flush_tally(counters, none, 1u, 1u);
+}
+
+__global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
+                                                         WfQueues q, int buf, uint32_t* ctl) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    const LightParams L = make_light(lraw);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        uint32_t flags = st.flags[p];
+        const float4 h = st.hit[p];
+        const f3 d = xyz(st.rd[p]);
+        f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
+        const uint32_t vertex = (flags & kBounceMask) >> kBounceShift;
+        const uint32_t flat = __float_as_uint(h.x);
+        if (flat == 0xffffffffu) {
+            f3 sky = L.sky;
+            if (vertex == 0u && L.sun_disk) sky = sky + sun_disk(L, d);
+            rad = rad + thp * sky;
+            st.rad[p] = f4(rad, 0.0f);
+            st.flags[p] = flags | kFlagEnd;
+            continue;
+        }
+        Rng rng(0u, 0u, 0u);
+        rng.state = st.rng[p];
+        const uint2 ref = __ldg(s.tri_refs + flat);
+        const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
+        rad = rad + thp * sd.emissive;
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
+        const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+        const f3 f = sd.diffuse * kInvPi;
+        push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 wo = cosine_sample_hemisphere(e0, e1, &pdf);
+        pdf = maxf(pdf, 1e-6f);
+        thp = thp * ((f * fabsf(wo.z)) / pdf);
+        st.ro[p] = f4(sd.origin_front, 0.0f);
+        st.rd[p] = f4(sd.frame.to_global(wo), L.t_max);
+        const uint32_t next = vertex + 1u;
+        flags = (flags & ~kBounceMask) | (next << kBounceShift);
+        if (next >= a.max_vertices) flags |= kFlagEnd;
+        st.thp[p] = f4(thp, 0.0f);
+        st.rad[p] = f4(rad, 0.0f);
+        st.rng[p] = rng.state;
+        st.flags[p] = flags;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_wf_screen_finalize(ScreenArgs a, WfState st, WfQueues q, int buf,
+                                                            uint32_t* ctl, uint32_t* ctl_next) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        if (!(st.flags[p] & kFlagEnd)) {
+            const uint32_t slot = queue_slot(ctl_next + 0, true);
+            q.ext[buf ^ 1][slot] = p;
+            continue;
+        }
+        const float4 r = st.rad[p];
+        a.out[st.unit[p]] = make_float4(r.x, r.y, r.z, 1.0f);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Surface-probe baker stages (surface_probe_path_tracer.slang:151-315).
+// ---------------------------------------------------------------------------
+struct ProbeArgs {
+    ProbeOut out;
+    const float4* probes;
+    const float4* pinst;
+    uint32_t probe_instance_count;
+    uint32_t iteration, n, spp, max_bounces;
+    int reset;
+};
+
+// Shading of the probe's own surface point (estimate_surface_irradiance).
+__device__ __forceinline__ Shading probe_surface(const SceneView& s, const ProbeArgs& a, uint32_t probe,
+                                                 const float4& surf) {
+    const float4 nrm = __ldg(a.probes + 3u * probe + 1u);
+    const f3 view = normalize3(mk3(nrm.x, nrm.y, nrm.z));
+    return shading_data(s, __float_as_uint(surf.z), __float_as_uint(surf.w), surf.x, surf.y, view);
+}
+
+// One cosine sample around the face normal (no sun at the probe itself).
+__device__ __forceinline__ void probe_start_sample(const SceneView& s, const LightParams& L, const ProbeArgs& a,
+                                                   const WfState& st, const WfQueues& q, int buf, uint32_t* ctl_next,
+                                                   uint32_t p, uint32_t flags, Rng& rng) {
+    const float4 surf = st.surf[p];
+    const Shading sd = probe_surface(s, a, st.unit[p], surf);
+    const float kr = st.si[p].w;
+    const float e0 = rng.next_1d(), e1 = rng.next_1d();
+    float pdf;
+    const f3 dir = cosine_sample_hemisphere(e0, e1, &pdf);
+    flags &= ~(kFlagEnd | kFlagNoPath | kBounceMask);
+    if (pdf > 1e-6f) {
+        const f3 o = sd.origin_front;
+        st.ro[p] = f4(o, 0.0f);
+        st.rd[p] = f4(Frame(normalize3(sd.face_normal)).to_global(dir), L.t_max);
+        st.thp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        st.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        st.zpdf[p] = make_float2(fabsf(dir.z), pdf);
+        st.pa[p] = make_float4(surf.z, surf.w, len3(o - sd.position), 2.0f * kr);
+        uint4 b = st.pb[p];
+        b.x = 0u;
+        b.w = radial_texel(dir);
+        st.pb[p] = b;
+    } else {
+        flags |= kFlagNoPath;
+    }
+    st.flags[p] = flags;
+    const uint32_t slot = queue_slot(ctl_next + 0, true);
+    q.ext[buf][slot] = p;
+}
+
+__global__ void __launch_bounds__(128) k_wf_probe_generate(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+                                                           WfQueues q, uint32_t begin, uint32_t count,
+                                                           unsigned long long* counters) {
+    const uint32_t slot_p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot_p >= count) return;
+    const uint32_t probe = begin + slot_p;
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(a.probes) + 3u * probe + 2u);
+    const uint32_t inst = meta.w >> 8;
+    if (inst >= a.probe_instance_count || !valid_prim(s, inst, meta.x)) {
+        atomicOr(s.status, kStatusBadRecord);
+        return;
+    }
+    const float4 params = __ldg(a.pinst + 3u * inst + 2u);
+    const LightParams L = make_light(lraw);
+    const uint32_t p = slot_p;
+    st.unit[p] = probe;
+    st.surf[p] = make_float4(__uint_as_float(meta.y), __uint_as_float(meta.z), __uint_as_float(inst),
+                             __uint_as_float(meta.x));
+    st.si[p] = make_float4(0.0f, 0.0f, 0.0f, maxf(params.x, 1e-6f));
+    st.irr[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const uint32_t prev_iter = a.reset ? 0u : a.out.counts[probe];
+    st.pb[p] = make_uint4(0u, 0u, prev_iter, 0u);
+    st.pc[2u * p] = make_uint4(0u, 0u, 0u, 0u);
+    st.pc[2u * p + 1u] = make_uint4(0u, 0u, 0u, 0u);
+    if (a.reset)
+        for (int t = 0; t < 16; ++t) a.out.radial[16u * probe + (uint32_t)t] = 0u;
+    Rng rng(probe, inst, a.iteration * a.n);
+    probe_start_sample(s, L, a, st, q, 0, q.ctl, p, 0u, rng);
+    st.rng[p] = rng.state;
+    RayTally none{0u, 0u};
+    flush_tally(counters, none, 1u, a.n);
+}
+
+__global__ void __launch_bounds__(128) k_wf_probe_shade(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+                                                        WfQueues q, int buf, uint32_t* ctl) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    const LightParams L = make_light(lraw);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        uint32_t flags = st.flags[p];
+        if (flags & kFlagNoPath) {
+            st.flags[p] = flags | kFlagEnd;
+            continue;
+        }
+        const float4 h = st.hit[p];
+        const f3 d = xyz(st.rd[p]);
+        f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
+        float4 pa = st.pa[p];  // src inst, src prim, src offset, first hit
+        const uint32_t bounce = (flags & kBounceMask) >> kBounceShift;
+        const float radial_max = 2.0f * st.si[p].w;
+        const uint32_t flat = __float_as_uint(h.x);
+        if (flat == 0xffffffffu) {
+            if (bounce == 0u) pa.w = radial_max;
+            rad = rad + thp * L.sky;
+            st.pa[p] = pa;
+            st.rad[p] = f4(rad, 0.0f);
+            st.flags[p] = flags | kFlagEnd;
+            continue;
+        }
+        if (bounce == 0u) pa.w = minf(h.y, radial_max);
+        const uint2 ref = __ldg(s.tri_refs + flat);
+        const uint32_t src_inst = __float_as_uint(pa.x), src_prim = __float_as_uint(pa.y);
+        const bool same_prim = ref.x == src_inst && ref.y == src_prim;
+        const float thr = maxf(4.0f * pa.z, 1e-6f);
+        const bool adjacent = ref.x == src_inst && h.y <= thr;
+        if (same_prim || adjacent) {
+            uint4 b = st.pb[p];
+            b.x += 1u;
+            st.pb[p] = b;
+        }
+        Rng rng(0u, 0u, 0u);
+        rng.state = st.rng[p];
+        const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
+        rad = rad + thp * sd.emissive;
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
+        const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+        const f3 f = sd.diffuse * kInvPi;
+        push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 sdir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf <= 1e-6f) {
+            flags |= kFlagEnd;
+        } else {
+            thp = thp * ((f * fabsf(sdir.z)) / pdf);
+            const f3 next_origin = sd.origin_front;
+            st.ro[p] = f4(next_origin, 0.0f);
+            st.rd[p] = f4(Frame(normalize3(sd.face_normal)).to_global(sdir), L.t_max);
+            pa.x = __uint_as_float(ref.x);
+            pa.y = __uint_as_float(ref.y);
+            pa.z = len3(next_origin - sd.position);
+            const uint32_t next = bounce + 1u;
+            flags = (flags & ~kBounceMask) | (next << kBounceShift);
+            if (next >= a.max_bounces) flags |= kFlagEnd;
+        }
+        st.pa[p] = pa;
+        st.thp[p] = f4(thp, 0.0f);
+        st.rad[p] = f4(rad, 0.0f);
+        st.rng[p] = rng.state;
+        st.flags[p] = flags;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_wf_probe_finalize(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+                                                           WfQueues q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    const LightParams L = make_light(lraw);
+    const int nbuf = buf ^ 1;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        uint32_t flags = st.flags[p];
+        if (!(flags & kFlagEnd)) {
+            const uint32_t slot = queue_slot(ctl_next + 0, true);
+            q.ext[nbuf][slot] = p;
+            continue;
+        }
+        const uint32_t probe = st.unit[p];
+        f3 irr = xyz(st.irr[p]);
+        uint4 b = st.pb[p];
+        if (!(flags & kFlagNoPath)) {
+            b.y += b.x;  // self-hit suspects of this sample
+            const uint32_t texel = b.w;
+            uint4 c = st.pc[2u * p + (texel >> 3)];
+            const uint32_t word = (texel >> 1) & 3u, shift = (texel & 1u) * 16u;
+            uint32_t* cw = word == 0u ? &c.x : (word == 1u ? &c.y : (word == 2u ? &c.z : &c.w));
+            const uint32_t local = ((*cw >> shift) & 0xffffu) + 1u;
+            *cw = (*cw & ~(0xffffu << shift)) | ((local & 0xffffu) << shift);
+            st.pc[2u * p + (texel >> 3)] = c;
+            const float kr = st.si[p].w;
+            accumulate_radial_moment(a.out.radial, probe, texel, st.pa[p].w / maxf(kr, 1e-6f), b.z, local, a.spp);
+            const float2 zp = st.zpdf[p];
+            irr = irr + ((xyz(st.rad[p]) * zp.x) / zp.y);
+        }
+        st.pb[p] = b;
+        const uint32_t k = (flags >> kSampleShift) + 1u;
+        if (k < a.n) {
+            st.irr[p] = f4(irr, 0.0f);
+            Rng rng(0u, 0u, 0u);
+            rng.state = st.rng[p];
+            probe_start_sample(s, L, a, st, q, nbuf, ctl_next, p,
+                               (flags & ((1u << kSampleShift) - 1u)) | (k << kSampleShift), rng);
+            st.rng[p] = rng.state;
+            continue;
+        }
+        irr = irr / (float)a.n;
+        const uint32_t prev = a.reset ? 0u : a.out.counts[probe];
+        f3 pv = mk3(0.0f, 0.0f, 0.0f);
+        if (prev != 0u)
+            pv = mk3(a.out.values[3u * probe], a.out.values[3u * probe + 1u], a.out.values[3u * probe + 2u]);
+        const float weight = 1.0f / (float)(prev + 1u);
+        const f3 acc = pv + weight * (irr - pv);
+        a.out.values[3u * probe] = acc.x;
+        a.out.values[3u * probe + 1u] = acc.y;
+        a.out.values[3u * probe + 2u] = acc.z;
+        a.out.counts[probe] = min(prev + 1u, 65535u);
+        const uint32_t prev_self = a.reset ? 0u : a.out.self_hits[probe];
+        a.out.self_hits[probe] = prev_self + b.y;
+    }
+}
+
 LightingRaw to_raw(const NanLighting* l) {
     LightingRaw r;
     memcpy(&r, l, sizeof(r));
@@ -365,29 +698,105 @@ namespace nan_host {
 
 size_t wavefront_bytes_per_path() { return kBytesPerPath + 64; }
 
+// Scratch plan shared by the integrators: control words for `iters`
+// iterations plus as many paths as the arena holds (or the tuning cap).
+int wf_plan(NanContext* ctx, uint64_t iters64, uint32_t* iters, uint64_t* cap) {
+    if (iters64 > (1u << 20)) {
+        set_error("samples * bounces too large for the wavefront schedule");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    *iters = (uint32_t)iters64;
+    const size_t ctl_bytes = ((size_t)(*iters + 2) * 4 * sizeof(uint32_t) + 255u) / 256u * 256u;
+    if (ctx->scratch_bytes <= ctl_bytes + 8192) {
+        set_error("no wavefront scratch reserved on this context (nan_ctx_reserve)");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    *cap = (ctx->scratch_bytes - ctl_bytes - 8192) / wavefront_bytes_per_path();
+    if (ctx->tuning.max_paths_in_flight) *cap = std::min<uint64_t>(*cap, ctx->tuning.max_paths_in_flight);
+    if (*cap == 0) {
+        set_error("wavefront scratch too small for one path");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    return NAN_OK;
+}
+
+void wf_carve(NanContext* ctx, uint32_t count, uint32_t iters, WfState& S, WfQueues& q) {
+    unsigned char* cur = static_cast<unsigned char*>(ctx->scratch);
+    q.ctl = carve<uint32_t>(cur, (size_t)(iters + 2) * 4);
+    S.unit = carve<uint32_t>(cur, count);
+    S.rng = carve<uint32_t>(cur, count);
+    S.flags = carve<uint32_t>(cur, count);
+    S.surf = carve<float4>(cur, count);
+    S.ro = carve<float4>(cur, count);
+    S.rd = carve<float4>(cur, count);
+    S.thp = carve<float4>(cur, count);
+    S.rad = carve<float4>(cur, count);
+    S.si = carve<float4>(cur, count);
+    S.irr = carve<float4>(cur, count);
+    S.zpdf = carve<float2>(cur, count);
+    S.hit = carve<float4>(cur, count);
+    S.pa = carve<float4>(cur, count);
+    S.pb = carve<uint4>(cur, count);
+    S.pc = carve<uint4>(cur, 2ull * count);
+    q.ext[0] = carve<uint32_t>(cur, count);
+    q.ext[1] = carve<uint32_t>(cur, count);
+    q.shd[0] = carve<float4>(cur, 3ull * 2 * count);
+    q.shd[1] = carve<float4>(cur, 3ull * 2 * count);
+}
+
+// Runs units [begin, end) in chunks: generate, then `iters` rounds of
+// extend / shade / shadow / finalize. gen(S, q, first_unit, count),
+// shade(S, q, buf, ctl) and fin(S, q, buf, ctl, ctl_next) launch the
+// integrator's own stages.
+template <class Gen, class Shade, class Fin>
+int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint32_t iters, uint64_t cap, float t_max,
+           Gen gen, Shade shade, Fin fin) {
+    const SceneView s = scene_view(ctx);
+    const Grid g = grid_for(ctx);
+    for (uint64_t cb = begin; cb < end; cb += cap) {
+        const uint32_t count = (uint32_t)std::min<uint64_t>(cap, end - cb);
+        WfState S;
+        WfQueues q;
+        wf_carve(ctx, count, iters, S, q);
+        cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 4 * sizeof(uint32_t), st);
+        if (err != cudaSuccess) return cuda_fail(err, "wavefront control reset");
+        gen(S, q, (uint32_t)cb, count);
+        ctx->launches++;
+        for (uint32_t it = 0; it < iters; ++it) {
+            const int buf = (int)(it & 1u);
+            uint32_t* ctl = q.ctl + 4u * it;
+            if (s.wnodes)
+                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                                   ctx->d_counters);
+            else
+                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                                   ctx->d_counters);
+            shade(S, q, buf, ctl);
+            if (s.wnodes)
+                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
+                                                                   ctx->d_counters);
+            else
+                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
+                                                                   ctx->d_counters);
+            fin(S, q, buf, ctl, ctl + 4);
+            ctx->launches += 4;
+        }
+        err = cudaGetLastError();
+        if (err != cudaSuccess) return cuda_fail(err, "wavefront launch");
+    }
+    return NAN_OK;
+}
+
 int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay, uint8_t* slots,
                                   uint32_t iteration, uint32_t spt, uint32_t max_bounces, int reset,
                                   const NanLighting* light, uint32_t begin, uint32_t end, cudaStream_t st) {
     if (end <= begin) return NAN_OK;
     const uint32_t n = std::max(spt, 1u);
-    const uint32_t sides = 2u;  // a path may run its back side after its front
-    const uint64_t iters64 = (uint64_t)sides * n * std::max(max_bounces, 1u);
-    if (iters64 > (1u << 20)) {
-        set_error("samples_per_texel * max_bounces too large for the wavefront schedule");
-        return NAN_ERR_INVALID_ARGUMENT;
-    }
-    const uint32_t iters = (uint32_t)iters64;
-    const size_t ctl_bytes = ((size_t)(iters + 2) * 4 * sizeof(uint32_t) + 255u) / 256u * 256u;
-    if (ctx->scratch_bytes <= ctl_bytes + 8192) {
-        set_error("no wavefront scratch reserved on this context (nan_ctx_reserve)");
-        return NAN_ERR_INVALID_ARGUMENT;
-    }
-    uint64_t cap = (ctx->scratch_bytes - ctl_bytes - 8192) / wavefront_bytes_per_path();
-    if (ctx->tuning.max_paths_in_flight) cap = std::min<uint64_t>(cap, ctx->tuning.max_paths_in_flight);
-    if (cap == 0) {
-        set_error("wavefront scratch too small for one path");
-        return NAN_ERR_INVALID_ARGUMENT;
-    }
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    // a path may run its back side after its front: 2 sides x n samples x bounces
+    int rc = wf_plan(ctx, 2ull * n * std::max(max_bounces, 1u), &iters, &cap);
+    if (rc) return rc;
     const SceneView s = scene_view(ctx);
     const LightingRaw lr = to_raw(light);
     TexelArgs a;
@@ -403,55 +812,90 @@ int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay,
     a.max_bounces = std::max(max_bounces, 1u);
     a.reset = reset;
     const Grid g = grid_for(ctx);
-    for (uint64_t cb = begin; cb < end; cb += cap) {
-        const uint32_t count = (uint32_t)std::min<uint64_t>(cap, end - cb);
-        unsigned char* cur = static_cast<unsigned char*>(ctx->scratch);
-        WfQueues q;
-        q.ctl = carve<uint32_t>(cur, (size_t)(iters + 2) * 4);
-        WfState S;
-        S.unit = carve<uint32_t>(cur, count);
-        S.rng = carve<uint32_t>(cur, count);
-        S.flags = carve<uint32_t>(cur, count);
-        S.surf = carve<float4>(cur, count);
-        S.ro = carve<float4>(cur, count);
-        S.rd = carve<float4>(cur, count);
-        S.thp = carve<float4>(cur, count);
-        S.rad = carve<float4>(cur, count);
-        S.si = carve<float4>(cur, count);
-        S.irr = carve<float4>(cur, count);
-        S.zpdf = carve<float2>(cur, count);
-        S.hit = carve<float4>(cur, count);
-        q.ext[0] = carve<uint32_t>(cur, count);
-        q.ext[1] = carve<uint32_t>(cur, count);
-        q.shd[0] = carve<float4>(cur, 3ull * 2 * count);
-        q.shd[1] = carve<float4>(cur, 3ull * 2 * count);
-        cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 4 * sizeof(uint32_t), st);
-        if (err != cudaSuccess) return cuda_fail(err, "wavefront control reset");
-        k_wf_texel_generate<<<(count + 127) / 128, 128, 0, st>>>(s, lr, a, S, q, (uint32_t)cb, count, ctx->d_counters);
-        ctx->launches++;
-        for (uint32_t it = 0; it < iters; ++it) {
-            const int buf = (int)(it & 1u);
-            uint32_t* ctl = q.ctl + 4u * it;
-            if (s.wnodes)
-                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                                   ctx->d_counters);
-            else
-                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                                   ctx->d_counters);
+    unsigned long long* counters = ctx->d_counters;
+    return wf_run(
+        ctx, st, begin, end, iters, cap, lr.ray_t_max,
+        [&](const WfState& S, const WfQueues& q, uint32_t first, uint32_t count) {
+            k_wf_texel_generate<<<(count + 127) / 128, 128, 0, st>>>(s, lr, a, S, q, first, count, counters);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl) {
             k_wf_texel_shade<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl);
-            if (s.wnodes)
-                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, lr.ray_t_max, S.rad, S.si,
-                                                                   ctx->d_counters);
-            else
-                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, lr.ray_t_max, S.rad, S.si,
-                                                                   ctx->d_counters);
-            k_wf_texel_finalize<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl, ctl + 4);
-            ctx->launches += 4;
-        }
-        err = cudaGetLastError();
-        if (err != cudaSuccess) return cuda_fail(err, "wavefront texel launch");
-    }
-    return NAN_OK;
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
+            k_wf_texel_finalize<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl, ctl_next);
+        });
+}
+
+int launch_trace_screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame,
+                                  uint32_t max_vertices, const NanCamera* cam, const NanLighting* light,
+                                  cudaStream_t st) {
+    const uint64_t pixels = (uint64_t)w * h;
+    if (pixels == 0 || max_vertices == 0) return NAN_OK;
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    int rc = wf_plan(ctx, max_vertices, &iters, &cap);
+    if (rc) return rc;
+    const SceneView s = scene_view(ctx);
+    const LightingRaw lr = to_raw(light);
+    ScreenArgs a;
+    memcpy(&a.cam, cam, sizeof(a.cam));
+    a.out = reinterpret_cast<float4*>(out);
+    a.width = w;
+    a.height = h;
+    a.frame = frame;
+    a.max_vertices = max_vertices;
+    const Grid g = grid_for(ctx);
+    unsigned long long* counters = ctx->d_counters;
+    return wf_run(
+        ctx, st, 0, pixels, iters, cap, lr.ray_t_max,
+        [&](const WfState& S, const WfQueues& q, uint32_t first, uint32_t count) {
+            k_wf_screen_generate<<<(count + 127) / 128, 128, 0, st>>>(s, lr, a, S, q, first, count, counters);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl) {
+            k_wf_screen_shade<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
+            k_wf_screen_finalize<<<g.stream_blocks, 128, 0, st>>>(a, S, q, buf, ctl, ctl_next);
+        });
+}
+
+int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits,
+                                  uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                                  const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
+                                  uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
+                                  uint32_t begin, uint32_t end, cudaStream_t st) {
+    end = std::min(end, probe_count);
+    if (end <= begin) return NAN_OK;
+    const uint32_t n = std::max(spp, 1u);
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    int rc = wf_plan(ctx, (uint64_t)n * std::max(max_bounces, 1u), &iters, &cap);
+    if (rc) return rc;
+    const SceneView s = scene_view(ctx);
+    const LightingRaw lr = to_raw(light);
+    ProbeArgs a;
+    a.out = ProbeOut{values, counts, self_hits, radial};
+    a.probes = reinterpret_cast<const float4*>(probes);
+    a.pinst = reinterpret_cast<const float4*>(probe_instances);
+    a.probe_instance_count = probe_instance_count;
+    a.iteration = iteration;
+    a.n = n;
+    a.spp = spp;
+    a.max_bounces = std::max(max_bounces, 1u);
+    a.reset = reset;
+    const Grid g = grid_for(ctx);
+    unsigned long long* counters = ctx->d_counters;
+    return wf_run(
+        ctx, st, begin, end, iters, cap, lr.ray_t_max,
+        [&](const WfState& S, const WfQueues& q, uint32_t first, uint32_t count) {
+            k_wf_probe_generate<<<(count + 127) / 128, 128, 0, st>>>(s, lr, a, S, q, first, count, counters);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl) {
+            k_wf_probe_shade<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
+            k_wf_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl, ctl_next);
+        });
 }
 
 }  // namespace nan_host

@@ -28,6 +28,7 @@ class PathTracer:
         if output.dim() != 3 or output.shape[2] != 4 or not output.is_contiguous():
             raise ValueError("output must be a contiguous [H, W, 4] float32 tensor")
         h, w = int(output.shape[0]), int(output.shape[1])
+        self.scene.context.reserve_paths(w * h)  # wavefront scratch; grows only
         cam = self.scene.camera.to_struct()
         light = self.scene.lighting.to_struct()
         check(lib().nan_trace_screen(self.scene.context.handle, ptr(output), w, h, int(frame) & 0xFFFFFFFF,

@@ -24,6 +24,7 @@ class SurfaceProbeDiffuseIrradianceBaker:
         self.geometry = geometry
         self.samples_per_probe = max(1, int(samples_per_probe))
         self.max_bounces = max(1, int(max_bounces))
+        scene.context.reserve_paths(max(1, int(geometry.probe_count)))  # wavefront scratch
         if profile_sink is not None:
             profile_sink.append(("trace_pipeline_create", time.perf_counter() - start))
 

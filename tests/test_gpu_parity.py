@@ -248,6 +248,68 @@ def test_texel_wavefront_two_sided(cornell, device):
     device.check()
 
 
+def test_screen_wavefront_equals_megakernel(cornell, terrain, device):
+    import torch
+
+    import nan_b200
+
+    for scene, _ in (cornell, terrain):
+        cam = scene.camera
+        w, h = 96, 64
+        a = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+        b = torch.zeros_like(a)
+        tracer = nan_b200.PathTracer(device, scene)
+        for frame in (0, 7):
+            cam.begin_frame(w, h)
+            scene.configure("megakernel")
+            tracer.execute(None, a, frame)
+            scene.configure("wavefront", max_paths_in_flight=1000)
+            tracer.execute(None, b, frame)
+            torch.testing.assert_close(b, a, rtol=0, atol=0)
+        scene.configure("wavefront")
+    device.check()
+
+
+def _probe_setup(device, scene, count, spp):
+    import nan_b200
+    from nan_b200 import scenes
+
+    probes, pinst = scenes.surface_sites(scene.scene_node, count, seed=3, radius=0.3)
+    layout = type("L", (), {})()
+    layout.probes = probes
+    layout.nodes = np.zeros((1, 4), np.uint32)
+    layout.instance_gpu_data = pinst
+    layout.triangle_vertex_probes = np.zeros((1, 4), np.uint32)
+    layout.total_probe_count = probes.shape[0]
+    layout.instance_infos = list(range(pinst.shape[0]))
+    geometry = nan_b200.SurfaceProbeGpuGeometry.create(device, layout)
+    baker = nan_b200.SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=spp,
+                                                        max_bounces=3)
+    return probes, pinst, geometry, baker
+
+
+def test_probe_wavefront_equals_megakernel(terrain, device):
+    import torch
+
+    import nan_b200
+
+    scene, _ = terrain
+    probes, pinst, geometry, baker = _probe_setup(device, scene, 3000, 12)
+    runs = []
+    for integrator in ("megakernel", "wavefront"):
+        scene.configure(integrator, max_paths_in_flight=1111 if integrator == "wavefront" else 0)
+        rd = nan_b200.RenderData(device)
+        runtime = nan_b200.SurfaceProbeRuntimeBuffers.acquire(rd, probes.shape[0])
+        for it in range(3):
+            baker.execute(None, runtime.field, runtime.attachments, it, reset=(it == 0))
+        runs.append([runtime.field.values.clone(), runtime.field.sample_counts.clone(),
+                     runtime.attachments.self_hit_counts.clone(), runtime.attachments.radial_moments.clone()])
+    scene.configure("wavefront")
+    for x, y in zip(*runs):
+        torch.testing.assert_close(y, x, rtol=0, atol=0)
+    device.check()
+
+
 def test_probe_baker_matches_oracle(terrain, device):
     import torch
 
