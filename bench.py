@@ -266,6 +266,7 @@ def run_nan(args):
     import nan_b200
     from nan_b200 import scenes
     from nan_b200.mesh_colors import MeshColorsLayout
+    from nan_b200.parallel import shard_range
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -286,7 +287,7 @@ def run_nan(args):
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
     total = layout.total_surface_texels
-    begin, end = total * rank // world, total * (rank + 1) // world
+    begin, end = shard_range(total, rank, world)
     slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
     stream = torch.cuda.current_stream()
 

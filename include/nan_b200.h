@@ -107,6 +107,8 @@ typedef struct NanMeshColorsDesc {
     const uint32_t* surface_prefix;  /* u32[I+1]: exclusive prefix of texel_count */
     uint32_t total_surface_texels;
     uint32_t payload_count;          /* slots in the payload buffer */
+    float* compensation;             /* optional f32[P][4] Kahan terms of the running means;
+                                        NULL = the reference's plain lerp (bit-exact parity) */
 } NanMeshColorsDesc;
 
 /* Execution choices of a context. The defaults (all zero) are the wavefront
@@ -224,7 +226,8 @@ NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layo
  * surface_probe_path_tracer.py:49-83; surface_probe_path_tracer.slang:47-315).
  * values f32[N][3], sample_counts u32[N], self_hits u32[N],
  * radial u32[N][16] (RG16F moments), probes u8[N][48],
- * probe_instances u8[I][48]. */
+ * probe_instances u8[I][48]; compensation: optional f32[N][4] Kahan terms of
+ * the running means (NULL = the reference's plain lerp). */
 NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* sample_counts,
                                   uint32_t* self_hits, uint32_t* radial,
                                   const uint8_t* probes, uint32_t probe_count,
@@ -232,7 +235,7 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
                                   uint32_t probe_instance_count, uint32_t iteration,
                                   uint32_t samples_per_probe, uint32_t max_bounces, int reset,
                                   const NanLighting* lighting, uint32_t probe_begin,
-                                  uint32_t probe_end, void* stream);
+                                  uint32_t probe_end, float* compensation, void* stream);
 
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */

@@ -101,6 +101,7 @@ class NanMeshColorsDesc(ctypes.Structure):
         ("surface_prefix", ctypes.c_void_p),
         ("total_surface_texels", ctypes.c_uint32),
         ("payload_count", ctypes.c_uint32),
+        ("compensation", ctypes.c_void_p),
     ]
 
 
@@ -156,7 +157,7 @@ EXPORTS = {
     "nan_trace_texels": (_I, [_VP, ctypes.POINTER(NanMeshColorsDesc), _VP, _U32, _U32, _U32, _I,
                               ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
     "nan_trace_probes": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, _I,
-                              ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
+                              ctypes.POINTER(NanLighting), _U32, _U32, _VP, _VP]),
     "nan_pack_rgb9e5": (_I, [_VP, _VP, _VP, _U32, _VP]),
 }
 

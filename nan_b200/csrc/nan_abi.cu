@@ -255,8 +255,9 @@ NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layo
     if (layout->instance_count == 0) return invalid("layout has no instances");
     if (!layout->face_infos || !layout->instance_infos || !layout->side_infos || !layout->surface_prefix || !slots)
         return invalid("null layout buffer");
-    if (!aligned16(slots) || !aligned16(layout->instance_infos))
-        return invalid("slots and instance_infos must be 16-byte aligned");
+    if (!aligned16(slots) || !aligned16(layout->instance_infos) ||
+        (layout->compensation && !aligned16(layout->compensation)))
+        return invalid("slots, instance_infos and compensation must be 16-byte aligned");
     if (texel_end > layout->total_surface_texels) return invalid("texel range beyond the layout");
     if (max_bounces > 64) return invalid("max_bounces above 64");
     if (ctx->tuning.integrator == 0)
@@ -271,25 +272,27 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
                                   const uint8_t* probe_instances, uint32_t probe_instance_count,
                                   uint32_t iteration, uint32_t samples_per_probe, uint32_t max_bounces, int reset,
                                   const NanLighting* lighting, uint32_t probe_begin, uint32_t probe_end,
-                                  void* stream) {
+                                  float* compensation, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;
     if ((rc = need_scene(ctx))) return rc;
     if (!lighting) return invalid("null lighting");
     if (probe_count && (!values || !sample_counts || !self_hits || !radial || !probes || !probe_instances))
         return invalid("null probe buffer");
-    if (probe_count && (!aligned16(probes) || !aligned16(probe_instances)))
-        return invalid("probe records must be 16-byte aligned");
+    if (probe_count && (!aligned16(probes) || !aligned16(probe_instances) ||
+                        (compensation && !aligned16(compensation))))
+        return invalid("probe records and compensation must be 16-byte aligned");
     if (probe_end > probe_count) return invalid("probe range beyond probe_count");
     if (max_bounces > 64) return invalid("max_bounces above 64");
     if (ctx->tuning.integrator == 0)
         return nan_host::launch_trace_probes_wavefront(ctx, values, sample_counts, self_hits, radial, probes,
                                                        probe_count, probe_instances, probe_instance_count, iteration,
                                                        samples_per_probe, max_bounces, reset, lighting, probe_begin,
-                                                       probe_end, as_stream(stream));
+                                                       probe_end, compensation, as_stream(stream));
     return nan_host::launch_trace_probes(ctx, values, sample_counts, self_hits, radial, probes, probe_count,
                                          probe_instances, probe_instance_count, iteration, samples_per_probe,
-                                         max_bounces, reset, lighting, probe_begin, probe_end, as_stream(stream));
+                                         max_bounces, reset, lighting, probe_begin, probe_end, compensation,
+                                         as_stream(stream));
 }
 
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {

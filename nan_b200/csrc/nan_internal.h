@@ -63,7 +63,7 @@ int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32
                         uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
                         const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
                         uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
-                        uint32_t begin, uint32_t end, cudaStream_t stream);
+                        uint32_t begin, uint32_t end, float* compensation, cudaStream_t stream);
 size_t wavefront_bytes_per_path();
 int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* layout, uint8_t* slots,
                                   uint32_t iteration, uint32_t spt, uint32_t max_bounces, int reset,
@@ -75,7 +75,7 @@ int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* coun
                                   uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
                                   const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
                                   uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
-                                  uint32_t begin, uint32_t end, cudaStream_t stream);
+                                  uint32_t begin, uint32_t end, float* compensation, cudaStream_t stream);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

@@ -33,6 +33,7 @@ __device__ __forceinline__ void flush_tally(unsigned long long* counters, const 
 // Mesh Colors lattice (mesh_colors.slang:37-65, 272-363).
 // ---------------------------------------------------------------------------
 struct McView {
+    float4* compensation;  // optional Kahan terms of the running means, one per payload slot
     const uint2* face_infos;
     const uint4* instance_infos;
     const uint2* side_infos;
@@ -165,15 +166,41 @@ __device__ __forceinline__ bool texel_surface(const SceneView& s, const McView& 
 }
 
 // store_accumulated_irradiance, texture_space_path_tracer.slang:119-138.
-__device__ __forceinline__ void store_running_mean(uint4* __restrict__ slots, uint32_t texel, f3 v, int reset) {
+// One step of the running mean m' = m + (x - m)/(n + 1). Without a
+// compensation term this is the reference's lerp. With one, the increments
+// are summed with Kahan compensation (the term lives beside the slot), so the
+// mean does not drift by one rounding per sample over long accumulations.
+__device__ __forceinline__ f3 running_mean_step(f3 m, f3 x, uint32_t prev, float4* comp) {
+    if (comp == nullptr) {
+        const float weight = 1.0f / (float)(prev + 1u);
+        return m + weight * (x - m);
+    }
+    if (prev == 0u) {
+        *comp = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return x;
+    }
+    const float weight = 1.0f / (float)(prev + 1u);
+    const f3 inc = weight * (x - m);
+    const f3 c = mk3(comp->x, comp->y, comp->z);
+    const f3 y = inc - c;
+    const f3 t = m + y;
+    const f3 nc = (t - m) - y;
+    *comp = make_float4(nc.x, nc.y, nc.z, 0.0f);
+    return t;
+}
+
+__device__ __forceinline__ void store_running_mean(uint4* __restrict__ slots, uint32_t texel, f3 v, int reset,
+                                                   float4* __restrict__ comp = nullptr) {
     uint4 old = make_uint4(0u, 0u, 0u, 0u);
     if (!reset) old = slots[texel];
     const uint32_t prev = reset ? 0u : old.w;
     f3 pv = mk3(0.0f, 0.0f, 0.0f);
     if (prev != 0u) pv = mk3(__uint_as_float(old.x), __uint_as_float(old.y), __uint_as_float(old.z));
     const uint32_t next = min(prev + 1u, 65535u);
-    const float weight = 1.0f / (float)(prev + 1u);
-    const f3 acc = pv + weight * (v - pv);
+    float4 c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (comp) c = comp[texel];
+    const f3 acc = running_mean_step(pv, v, prev, comp ? &c : nullptr);
+    if (comp) comp[texel] = c;
     slots[texel] = make_uint4(__float_as_uint(acc.x), __float_as_uint(acc.y), __float_as_uint(acc.z), next);
 }
 
@@ -209,6 +236,7 @@ __device__ __forceinline__ uint32_t radial_texel(f3 d) {
 }
 
 struct ProbeOut {
+    float4* compensation;  // optional Kahan terms of the running means, one per probe
     float* values;
     uint32_t* counts;
     uint32_t* self_hits;

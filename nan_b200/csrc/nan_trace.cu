@@ -217,12 +217,12 @@ __global__ void __launch_bounds__(128) k_trace_texels(SceneView s, LightingRaw l
     const f3 fnrm = world_flat_normal(s, inst_index, prim);
     const f3 front = ts_estimate(s, L, inst_index, prim, hb1, hb2, fnrm, n, rng, max_bounces, tally);
     uint32_t paths = n;
-    if (global_texel < mc.payload_count) store_running_mean(slots, global_texel, front, reset);
+    if (global_texel < mc.payload_count) store_running_mean(slots, global_texel, front, reset, mc.compensation);
     else atomicOr(s.status, 2u);
     if (side.y & 1u) {
         const f3 back = ts_estimate(s, L, inst_index, prim, hb1, hb2, -fnrm, n, rng, max_bounces, tally);
         const uint32_t bt = side.x + (global_texel - inst.z);
-        if (bt < mc.payload_count) store_running_mean(slots, bt, back, reset);
+        if (bt < mc.payload_count) store_running_mean(slots, bt, back, reset, mc.compensation);
         else atomicOr(s.status, 2u);
         paths += n;
     }
@@ -325,8 +325,9 @@ __global__ void __launch_bounds__(128) k_trace_probes(SceneView s, LightingRaw l
     const uint32_t prev = reset ? 0u : out.counts[p];
     f3 pv = mk3(0.0f, 0.0f, 0.0f);
     if (prev != 0u) pv = mk3(out.values[3u * p], out.values[3u * p + 1u], out.values[3u * p + 2u]);
-    const float weight = 1.0f / (float)(prev + 1u);
-    const f3 acc = pv + weight * (irr - pv);
+    float4 comp = out.compensation ? out.compensation[p] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const f3 acc = running_mean_step(pv, irr, prev, out.compensation ? &comp : nullptr);
+    if (out.compensation) out.compensation[p] = comp;
     out.values[3u * p] = acc.x;
     out.values[3u * p + 1u] = acc.y;
     out.values[3u * p + 2u] = acc.z;
@@ -431,6 +432,7 @@ int launch_trace_texels(NanContext* ctx, const NanMeshColorsDesc* lay, uint8_t* 
                         uint32_t end, cudaStream_t st) {
     if (end <= begin) return NAN_OK;
     McView mc;
+    mc.compensation = reinterpret_cast<float4*>(lay->compensation);
     mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
     mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
     mc.side_infos = reinterpret_cast<const uint2*>(lay->side_infos);
@@ -447,10 +449,11 @@ int launch_trace_texels(NanContext* ctx, const NanMeshColorsDesc* lay, uint8_t* 
 int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits, uint32_t* radial,
                         const uint8_t* probes, uint32_t probe_count, const uint8_t* probe_instances,
                         uint32_t probe_instance_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces,
-                        int reset, const NanLighting* light, uint32_t begin, uint32_t end, cudaStream_t st) {
+                        int reset, const NanLighting* light, uint32_t begin, uint32_t end, float* compensation,
+                        cudaStream_t st) {
     end = std::min(end, probe_count);
     if (end <= begin) return NAN_OK;
-    ProbeOut o{values, counts, self_hits, radial};
+    ProbeOut o{reinterpret_cast<float4*>(compensation), values, counts, self_hits, radial};
     k_trace_probes<<<blocks_for(end - begin, 128), 128, 0, st>>>(
         scene_view(ctx), to_raw(light), o, reinterpret_cast<const float4*>(probes),
         reinterpret_cast<const float4*>(probe_instances), probe_count, probe_instance_count, iteration, spp,

@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(128) k_wf_texel_finalize(SceneView s, Lighting
         const uint2 side = __ldg(a.mc.side_infos + inst);
         const uint32_t global_texel = info.z + (u - __ldg(a.mc.surface_prefix + inst));
         const uint32_t slot = (flags & kFlagBack) ? side.x + (global_texel - info.z) : global_texel;
-        if (slot < a.mc.payload_count) store_running_mean(a.slots, slot, irr / (float)a.n, a.reset);
+        if (slot < a.mc.payload_count) store_running_mean(a.slots, slot, irr / (float)a.n, a.reset, a.mc.compensation);
         else atomicOr(s.status, 2u);
         if (!(flags & kFlagBack) && (flags & kFlagTwoSided)) {
             flags = (flags & ((1u << kSampleShift) - 1u)) | kFlagBack;
@@ -630,8 +630,9 @@ __global__ void __launch_bounds__(128) k_wf_probe_finalize(SceneView s, Lighting
         f3 pv = mk3(0.0f, 0.0f, 0.0f);
         if (prev != 0u)
             pv = mk3(a.out.values[3u * probe], a.out.values[3u * probe + 1u], a.out.values[3u * probe + 2u]);
-        const float weight = 1.0f / (float)(prev + 1u);
-        const f3 acc = pv + weight * (irr - pv);
+        float4 comp = a.out.compensation ? a.out.compensation[probe] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const f3 acc = running_mean_step(pv, irr, prev, a.out.compensation ? &comp : nullptr);
+        if (a.out.compensation) a.out.compensation[probe] = comp;
         a.out.values[3u * probe] = acc.x;
         a.out.values[3u * probe + 1u] = acc.y;
         a.out.values[3u * probe + 2u] = acc.z;
@@ -800,6 +801,7 @@ int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay,
     const SceneView s = scene_view(ctx);
     const LightingRaw lr = to_raw(light);
     TexelArgs a;
+    a.mc.compensation = reinterpret_cast<float4*>(lay->compensation);
     a.mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
     a.mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
     a.mc.side_infos = reinterpret_cast<const uint2*>(lay->side_infos);
@@ -863,7 +865,7 @@ int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* coun
                                   uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
                                   const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
                                   uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
-                                  uint32_t begin, uint32_t end, cudaStream_t st) {
+                                  uint32_t begin, uint32_t end, float* compensation, cudaStream_t st) {
     end = std::min(end, probe_count);
     if (end <= begin) return NAN_OK;
     const uint32_t n = std::max(spp, 1u);
@@ -874,7 +876,7 @@ int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* coun
     const SceneView s = scene_view(ctx);
     const LightingRaw lr = to_raw(light);
     ProbeArgs a;
-    a.out = ProbeOut{values, counts, self_hits, radial};
+    a.out = ProbeOut{reinterpret_cast<float4*>(compensation), values, counts, self_hits, radial};
     a.probes = reinterpret_cast<const float4*>(probes);
     a.pinst = reinterpret_cast<const float4*>(probe_instances);
     a.probe_instance_count = probe_instance_count;

@@ -17,7 +17,7 @@ class SurfaceProbeDiffuseIrradianceBaker:
     field_desc = DIFFUSE_IRRADIANCE_RGB_FIELD
 
     def __init__(self, device, scene, geometry, *, samples_per_probe: int = 1, max_bounces: int = 3,
-                 profile_sink: list | None = None):
+                 profile_sink: list | None = None, compensated: bool = False):
         start = time.perf_counter()
         self.device = device
         self.scene = scene
@@ -25,6 +25,12 @@ class SurfaceProbeDiffuseIrradianceBaker:
         self.samples_per_probe = max(1, int(samples_per_probe))
         self.max_bounces = max(1, int(max_bounces))
         scene.context.reserve_paths(max(1, int(geometry.probe_count)))  # wavefront scratch
+        import torch
+
+        # Kahan terms of the running means (compensated FP32); None keeps the
+        # reference's plain lerp update
+        self.compensation = (torch.zeros((max(1, int(geometry.probe_count)), 4), dtype=torch.float32,
+                                          device=device.torch_device) if compensated else None)
         if profile_sink is not None:
             profile_sink.append(("trace_pipeline_create", time.perf_counter() - start))
 
@@ -40,7 +46,7 @@ class SurfaceProbeDiffuseIrradianceBaker:
             ptr(attachments.radial_moments), ptr(self.geometry.probes), n, ptr(self.geometry.instances),
             int(self.geometry.instance_count), max(0, int(iteration)) & 0xFFFFFFFF, self.samples_per_probe,
             self.max_bounces, int(bool(reset)), ctypes.byref(light), int(begin), int(end),
-            stream_handle(command_encoder)))
+            ptr(self.compensation), stream_handle(command_encoder)))
 
 
 # Historical name kept by the reference for callers (surface_probe_path_tracer.py:86-89).

@@ -19,7 +19,7 @@ class TextureSpacePathTracer:
     """
 
     def __init__(self, device, scene, layout, *, samples_per_texel: int = 1, max_bounces: int = 3,
-                 max_paths_in_flight: int | None = None):
+                 max_paths_in_flight: int | None = None, compensated: bool = False):
         self.device = device
         self.scene = scene
         self.layout = layout
@@ -36,6 +36,13 @@ class TextureSpacePathTracer:
         d.surface_prefix = ptr(self.surface_prefix_buffer)
         d.total_surface_texels = layout.total_surface_texels
         d.payload_count = layout.total_payload_count
+        # Kahan terms of the running means (compensated FP32); None keeps the
+        # reference's plain lerp update
+        import torch
+
+        self.compensation = (torch.zeros((layout.total_payload_count, 4), dtype=torch.float32,
+                                          device=device.torch_device) if compensated else None)
+        d.compensation = ptr(self.compensation)
         self._desc = d
         # wavefront scratch: one path per surface texel in flight (or the cap)
         paths = layout.total_surface_texels if max_paths_in_flight is None else int(max_paths_in_flight)
