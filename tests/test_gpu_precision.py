@@ -1,12 +1,13 @@
 """Precision of the accumulated results (GPU required).
 
-* Compensated running means: over hundreds of iterations the Kahan-compensated
-  slot means stay within a few float ulps of the FP64 mean of the same
-  per-iteration samples, and closer than the reference's plain lerp.
-* FP64 oracle: converged texel caches and screen images from the FP32 CUDA
-  path against the oracle evaluated in double precision on the same RNG
-  streams. Stated bound: relative RMSE <= 1e-4 (most samples agree to ~1e-6;
-  the rest is paths that diverge at a grazing FP32/FP64 decision).
+* Compensated running means: over 300-400 iterations the Kahan-compensated
+  means stay within 5e-7 (relative) of the FP64 mean of the same per-iteration
+  samples and are at least 4x closer on average than the reference's plain
+  lerp (measured on B200: 1.3e-7 max vs 1.5e-6 for lerp).
+* FP64 oracle: converged texel caches (24 iterations) and a 16-frame screen
+  image from the FP32 CUDA path against the oracle evaluated in double
+  precision on the same RNG streams. Stated bound: relative RMSE <= 1e-5 and
+  >= 99.9 % of values within 1e-4 (measured: 1.2e-7 and 2.5e-8 RMSE).
 """
 
 import numpy as np
@@ -53,8 +54,8 @@ def test_compensated_texel_means_track_fp64(device):
     err_a = np.abs(a - mean64) / scale
     err_b = np.abs(b - mean64) / scale
     print("texel means: plain max/mean", err_a.max(), err_a.mean(), "compensated", err_b.max(), err_b.mean())
-    assert err_b.max() <= 1e-5, err_b.max()
-    assert err_b.mean() <= err_a.mean(), (err_b.mean(), err_a.mean())
+    assert err_b.max() <= 5e-7, err_b.max()
+    assert err_b.mean() <= 0.25 * err_a.mean(), (err_b.mean(), err_a.mean())
     device.check()
 
 
@@ -90,8 +91,8 @@ def test_compensated_probe_means_track_fp64(device):
     err_a = np.abs(a - mean64) / scale
     err_b = np.abs(b - mean64) / scale
     print("probe means: plain max/mean", err_a.max(), err_a.mean(), "compensated", err_b.max(), err_b.mean())
-    assert err_b.max() <= 1e-5, err_b.max()
-    assert err_b.mean() <= err_a.mean()
+    assert err_b.max() <= 5e-7, err_b.max()
+    assert err_b.mean() <= 0.25 * err_a.mean()
     device.check()
 
 
@@ -120,7 +121,7 @@ def test_converged_texels_and_image_vs_fp64_oracle(device):
     rel_rmse = np.sqrt(np.mean((g - o) ** 2)) / max(np.sqrt(np.mean(o**2)), 1e-12)
     close = np.all(np.abs(g - o) <= 1e-4 * np.maximum(np.abs(o), 1e-2), axis=1).mean()
     print("texels vs FP64 oracle: rel RMSE", rel_rmse, "within 1e-4:", close)
-    assert close >= 0.999 and rel_rmse <= 1e-2, (close, rel_rmse)
+    assert close >= 0.999 and rel_rmse <= 1e-5, (close, rel_rmse)
 
     # screen: 16 accumulated frames of the path tracer vs the FP64 oracle
     w = h = 48
@@ -143,5 +144,5 @@ def test_converged_texels_and_image_vs_fp64_oracle(device):
     rel_rmse = np.sqrt(np.mean((img - ref) ** 2)) / max(np.sqrt(np.mean(ref**2)), 1e-12)
     close = np.all(np.abs(img - ref) <= 1e-4 * np.maximum(np.abs(ref), 1e-2), axis=1).mean()
     print("image vs FP64 oracle: rel RMSE", rel_rmse, "within 1e-4:", close)
-    assert close >= 0.999 and rel_rmse <= 1e-2, (close, rel_rmse)
+    assert close >= 0.999 and rel_rmse <= 1e-5, (close, rel_rmse)
     device.check()
