@@ -6,8 +6,11 @@ seeded 200,688-triangle scene (313x313-vertex displaced terrain + 500 boxes
 with sides U[0.2, 3] and random yaw, albedo U[0.1, 0.9]); 16 texels/unit,
 per-triangle lattice resolution 4..64, 1 hemisphere sample per texel, 3
 bounces, sun at 45 deg with irradiance 3, constant sky 0.5. One step = one
-iteration (one kernel launch). Metric: Mrays/s, every closest-hit (extend)
-and any-hit (shadow) ray counted on the device.
+iteration (the wavefront integrator's generate/extend/shade/shadow/finalize
+launches). Metric: Mrays/s, every closest-hit (extend) and any-hit (shadow)
+ray counted on the device. The roofline is that of the traversal kernels
+(k_wf_extend + k_wf_shadow), timed by CUDA events the library records on the
+launching stream inside the timed region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nan|reference]
 
@@ -53,6 +56,7 @@ def parse_args():
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent traversal blocks per SM (0 = auto)")
     ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
     ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
+    ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
@@ -216,10 +220,13 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
+def ncu_traffic(integrator: str):
+    """DRAM bytes (read + write) per step of the kernels the roofline covers,
+    from the committed ncu summary."""
     try:
         data = json.loads((ROOT / "profiles" / "traffic.json").read_text())
-        return data.get("k_trace_texels_bytes_per_launch")
+        key = "traversal_bytes_per_step" if integrator == "wavefront" else "k_trace_texels_bytes_per_launch"
+        return data.get(key)
     except Exception:
         return None
 
@@ -284,7 +291,8 @@ def run_nan(args):
     node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
     scene = nan_b200.Scene(device, node, bvh_builder=args.bvh)
     layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
-    tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3)
+    tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3,
+                                             max_paths_in_flight=args.paths or None)
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
     total = layout.total_surface_texels
     begin, end = shard_range(total, rank, world)
@@ -299,6 +307,11 @@ def run_nan(args):
     device.check()
     scene.context.read_counters(reset=True)
     launches0 = scene.context.launch_count
+    # stage timing on inside the timed region: an event pair around each
+    # wavefront launch, on the launching stream
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
+                    kernel_timing=True)
+    scene.context.read_kernel_times(reset=True)
 
     clocks = ClockSampler(local)
     events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -321,6 +334,8 @@ def run_nan(args):
     launch_ms = [a.elapsed_time(b) for a, b in events]
     launches = scene.context.launch_count - launches0
     counters = scene.context.read_counters(reset=True)
+    ktimes = scene.context.read_kernel_times(reset=True)
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
     device.check()
     rays_local = counters["extend_rays"] + counters["shadow_rays"]
 
@@ -345,12 +360,13 @@ def run_nan(args):
     e2e_counters = scene.context.read_counters(reset=True)
     e2e_rays_local = e2e_counters["extend_rays"] + e2e_counters["shadow_rays"]
 
-    stats = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device=device.torch_device)
+    trav_ms = ktimes["extend_ms"] + ktimes["shadow_ms"]
+    stats = torch.tensor([elapsed_ms, e2e_ms, trav_ms], dtype=torch.float64, device=device.torch_device)
     sums = torch.tensor([float(rays_local), float(e2e_rays_local)], dtype=torch.float64, device=device.torch_device)
     if world > 1:
         dist.all_reduce(stats, op=dist.ReduceOp.MAX)
         dist.all_reduce(sums, op=dist.ReduceOp.SUM)
-    elapsed_ms, e2e_ms = float(stats[0]), float(stats[1])
+    elapsed_ms, e2e_ms, trav_ms = float(stats[0]), float(stats[1]), float(stats[2])
     rays_total, e2e_rays = float(sums[0]), float(sums[1])
     if world > 1:
         dist.destroy_process_group()
@@ -359,11 +375,18 @@ def run_nan(args):
 
     value = rays_total / (elapsed_ms * 1e3)
     bytes_per_ray, n_node, n_tri = roofline_bytes_per_ray(node, layout, scene.lighting)
-    avg_launch_s = statistics.mean(launch_ms) * 1e-3
-    rays_per_launch = rays_local / args.steps
-    achieved = rays_per_launch * bytes_per_ray / avg_launch_s / 1e9
+    avg_step_s = statistics.mean(launch_ms) * 1e-3
+    rays_per_step = rays_local / args.steps
+    step_achieved = rays_per_step * bytes_per_ray / avg_step_s / 1e9
+    if trav_ms > 0.0:
+        # traversal kernels: all rays' algorithmic bytes over their own device time
+        scope = "k_wf_extend + k_wf_shadow (per step: all extend and shadow launches)"
+        achieved = rays_per_step * bytes_per_ray / (trav_ms / args.steps * 1e-3) / 1e9
+    else:
+        scope = "k_trace_texels (one launch per step)"
+        achieved = step_achieved
     peak, peak_kind = measured_peak_gbs()
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(args.integrator)
     line = {
         "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -385,9 +408,13 @@ def run_nan(args):
         "bvh_sah_cost": scene.info()["sah_cost"],
         "reference_sah_cost": getattr(roofline_bytes_per_ray, "sah_cost", None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
+                     "frac": achieved / peak, "traffic": traffic, "scope": scope,
                      "bytes_per_ray": bytes_per_ray, "nodes_per_ray": n_node, "tris_per_ray": n_tri,
-                     "peak_source": peak_kind},
+                     "step_achieved": step_achieved, "step_frac": step_achieved / peak,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else peak_kind},
+        "kernel_ms_per_step": {"extend": ktimes["extend_ms"] / args.steps, "shadow": ktimes["shadow_ms"] / args.steps,
+                               "generate_shade_finalize": ktimes["stage_ms"] / args.steps},
         "e2e": {"value": e2e_rays / (e2e_ms * 1e3), "unit": "Mrays/s",
                 "h2d_bytes_per_step": int(slots.numel() * 4), "d2h_bytes_per_step": int(slots.numel() * 4)},
         "gpu_launches": int(launches),

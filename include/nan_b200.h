@@ -120,8 +120,22 @@ typedef struct NanTuning {
     uint32_t max_paths_in_flight;  /* wavefront chunk size, 0 = as many as the scratch holds */
     uint32_t bvh_builder;          /* nan_scene_build: 0 = PLOC + SAH leaf collapse, 1 = LBVH */
     uint32_t bvh_width;            /* traversed nodes: 0 or 2 = binary, 8 = compressed 8-wide (PLOC builds) */
-    uint32_t reserved[3];
+    uint32_t kernel_timing;        /* 1: record CUDA events around each wavefront stage launch on the
+                                      launching stream (read with nan_ctx_read_kernel_times); not for
+                                      use under stream capture */
+    uint32_t reserved[2];
 } NanTuning;
+
+/* Device time of the wavefront stages since the last reset, from CUDA events
+ * recorded on the launching stream while NanTuning.kernel_timing is 1. */
+typedef struct NanKernelTimes {
+    double extend_ms;          /* k_wf_extend: closest-hit traversal */
+    double shadow_ms;          /* k_wf_shadow: any-hit traversal */
+    double stage_ms;           /* generate / shade / finalize kernels */
+    uint64_t extend_launches;
+    uint64_t shadow_launches;
+    uint64_t stage_launches;
+} NanKernelTimes;
 
 /* Device-side counters accumulated by the trace calls. */
 typedef struct NanCounters {
@@ -152,6 +166,9 @@ NAN_B200_API uint64_t nan_wavefront_bytes_per_path(void);
 NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning);
 /* Number of kernels this context has launched. */
 NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx);
+/* Waits for the recorded stage events and sums their durations into `out`;
+ * reset = 1 clears the sums. No counterpart in the reference (measurement). */
+NAN_B200_API int nan_ctx_read_kernel_times(NanContext* ctx, NanKernelTimes* out, int reset);
 
 /* Flatten the instances to world space and build the BVH on the GPU.
  * Replaces Scene.__init__'s buffer packing + build_blas/build_tlas

@@ -112,8 +112,23 @@ class NanTuning(ctypes.Structure):
         ("max_paths_in_flight", ctypes.c_uint32),
         ("bvh_builder", ctypes.c_uint32),
         ("bvh_width", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32 * 3),
+        ("kernel_timing", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 2),
     ]
+
+
+class NanKernelTimes(ctypes.Structure):
+    _fields_ = [
+        ("extend_ms", ctypes.c_double),
+        ("shadow_ms", ctypes.c_double),
+        ("stage_ms", ctypes.c_double),
+        ("extend_launches", ctypes.c_uint64),
+        ("shadow_launches", ctypes.c_uint64),
+        ("stage_launches", ctypes.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
@@ -144,6 +159,7 @@ EXPORTS = {
     "nan_ctx_launch_count": (_U64, [_VP]),
     "nan_ctx_reserve": (_I, [_VP, _U64]),
     "nan_wavefront_bytes_per_path": (_U64, []),
+    "nan_ctx_read_kernel_times": (_I, [_VP, ctypes.POINTER(NanKernelTimes), _I]),
     "nan_ctx_configure": (_I, [_VP, ctypes.POINTER(NanTuning)]),
     "nan_scene_build": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP]),
     "nan_scene_build_noalloc": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP, _U64, _VP, _U64, _VP, _U64, _VP]),
@@ -250,9 +266,18 @@ class Context:
         per = int(lib().nan_wavefront_bytes_per_path())
         self.reserve(int(paths) * per + (1 << 22))
 
+    def read_kernel_times(self, reset: bool = False) -> dict:
+        """Device milliseconds of the wavefront stages recorded while
+        kernel_timing is on (waits for their events)."""
+        t = NanKernelTimes()
+        check(lib().nan_ctx_read_kernel_times(self.handle, ctypes.byref(t), int(reset)))
+        return t.as_dict()
+
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc", bvh_width: int = 2) -> None:
+                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc", bvh_width: int = 2,
+                  kernel_timing: bool = False) -> None:
         t = NanTuning()
+        t.kernel_timing = int(bool(kernel_timing))
         t.bvh_builder = BVH_BUILDERS[bvh_builder]
         t.bvh_width = 8 if int(bvh_width) == 8 else 2
         t.integrator = INTEGRATORS[integrator]

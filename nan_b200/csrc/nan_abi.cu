@@ -87,6 +87,7 @@ NAN_B200_API int nan_ctx_destroy(NanContext* ctx) {
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     nan_host::free_scene(ctx);
+    nan_host::release_timing(ctx);
     cudaFree(ctx->scratch);
     cudaFree(ctx->d_status);
     cudaFree(ctx->d_counters);
@@ -132,6 +133,12 @@ NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int re
 
 NAN_B200_API uint64_t nan_ctx_launch_count(NanContext* ctx) { return ctx ? ctx->launches : 0; }
 
+NAN_B200_API int nan_ctx_read_kernel_times(NanContext* ctx, NanKernelTimes* out, int reset) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    return nan_host::read_kernel_times(ctx, out, reset);
+}
+
 NAN_B200_API uint64_t nan_wavefront_bytes_per_path(void) { return nan_host::wavefront_bytes_per_path(); }
 
 NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes) {
@@ -159,6 +166,7 @@ NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
     if (tuning->bvh_builder > 1) return invalid("bvh_builder must be 0 (PLOC) or 1 (LBVH)");
     if (tuning->bvh_width != 0 && tuning->bvh_width != 2 && tuning->bvh_width != 8)
         return invalid("bvh_width must be 0 or 2 (binary) or 8 (compressed wide)");
+    if (tuning->kernel_timing > 1) return invalid("kernel_timing must be 0 or 1");
     ctx->tuning = *tuning;
     return NAN_OK;
 }

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/nan_b200.h"
 
@@ -37,6 +38,16 @@ struct NanContext {
     void* scratch = nullptr;
     uint64_t scratch_bytes = 0;
     NanTuning tuning{};
+    // Stage timing (NanTuning.kernel_timing): events pending a read, a pool
+    // of free events, and the sums per stage kind (0 extend, 1 shadow, 2 other).
+    struct TimedLaunch {
+        int kind;
+        cudaEvent_t start, stop;
+    };
+    std::vector<TimedLaunch> timed;
+    std::vector<cudaEvent_t> event_pool;
+    double stage_ms[3] = {0.0, 0.0, 0.0};
+    uint64_t stage_launches[3] = {0, 0, 0};
 };
 
 namespace nan_host {
@@ -45,6 +56,12 @@ void set_error(const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
 
 void free_scene(NanContext* ctx);
+// Stage timing: begin returns the start event (or nullptr when timing is
+// off); end records the stop event and queues the pair.
+cudaEvent_t timing_begin(NanContext* ctx, cudaStream_t stream);
+void timing_end(NanContext* ctx, int kind, cudaEvent_t start, cudaStream_t stream);
+int read_kernel_times(NanContext* ctx, NanKernelTimes* out, int reset);
+void release_timing(NanContext* ctx);
 int build_scene(NanContext* ctx, const NanSceneDesc* desc, cudaStream_t stream);
 int world_triangles(NanContext* ctx, float* out, cudaStream_t stream);
 

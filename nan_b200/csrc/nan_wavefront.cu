@@ -699,6 +699,83 @@ namespace nan_host {
 
 size_t wavefront_bytes_per_path() { return kBytesPerPath + 64; }
 
+namespace {
+cudaEvent_t pooled_event(NanContext* ctx) {
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+}  // namespace
+
+cudaEvent_t timing_begin(NanContext* ctx, cudaStream_t stream) {
+    if (!ctx->tuning.kernel_timing) return nullptr;
+    cudaEvent_t e = pooled_event(ctx);
+    if (e && cudaEventRecord(e, stream) != cudaSuccess) {
+        ctx->event_pool.push_back(e);
+        return nullptr;
+    }
+    return e;
+}
+
+void timing_end(NanContext* ctx, int kind, cudaEvent_t start, cudaStream_t stream) {
+    if (!start) return;
+    cudaEvent_t e = pooled_event(ctx);
+    if (!e || cudaEventRecord(e, stream) != cudaSuccess) {
+        ctx->event_pool.push_back(start);
+        if (e) ctx->event_pool.push_back(e);
+        return;
+    }
+    ctx->timed.push_back({kind, start, e});
+}
+
+int read_kernel_times(NanContext* ctx, NanKernelTimes* out, int reset) {
+    cudaError_t first = cudaSuccess;
+    for (const NanContext::TimedLaunch& t : ctx->timed) {
+        float ms = 0.0f;
+        cudaError_t err = cudaEventSynchronize(t.stop);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, t.start, t.stop);
+        if (err == cudaSuccess) {
+            ctx->stage_ms[t.kind] += ms;
+            ctx->stage_launches[t.kind]++;
+        } else if (first == cudaSuccess) {
+            first = err;
+        }
+        ctx->event_pool.push_back(t.start);
+        ctx->event_pool.push_back(t.stop);
+    }
+    ctx->timed.clear();
+    if (out) {
+        out->extend_ms = ctx->stage_ms[0];
+        out->shadow_ms = ctx->stage_ms[1];
+        out->stage_ms = ctx->stage_ms[2];
+        out->extend_launches = ctx->stage_launches[0];
+        out->shadow_launches = ctx->stage_launches[1];
+        out->stage_launches = ctx->stage_launches[2];
+    }
+    if (reset) {
+        for (int k = 0; k < 3; ++k) {
+            ctx->stage_ms[k] = 0.0;
+            ctx->stage_launches[k] = 0;
+        }
+    }
+    return cuda_fail(first, "kernel timing events");
+}
+
+void release_timing(NanContext* ctx) {
+    for (const NanContext::TimedLaunch& t : ctx->timed) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    ctx->timed.clear();
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    ctx->event_pool.clear();
+}
+
 // Scratch plan shared by the integrators: control words for `iters`
 // iterations plus as many paths as the arena holds (or the tuning cap).
 int wf_plan(NanContext* ctx, uint64_t iters64, uint32_t* iters, uint64_t* cap) {
@@ -761,25 +838,35 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
         wf_carve(ctx, count, iters, S, q);
         cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 4 * sizeof(uint32_t), st);
         if (err != cudaSuccess) return cuda_fail(err, "wavefront control reset");
+        cudaEvent_t ev = timing_begin(ctx, st);
         gen(S, q, (uint32_t)cb, count);
+        timing_end(ctx, 2, ev, st);
         ctx->launches++;
         for (uint32_t it = 0; it < iters; ++it) {
             const int buf = (int)(it & 1u);
             uint32_t* ctl = q.ctl + 4u * it;
+            ev = timing_begin(ctx, st);
             if (s.wnodes)
                 k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
                                                                    ctx->d_counters);
             else
                 k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
                                                                    ctx->d_counters);
+            timing_end(ctx, 0, ev, st);
+            ev = timing_begin(ctx, st);
             shade(S, q, buf, ctl);
+            timing_end(ctx, 2, ev, st);
+            ev = timing_begin(ctx, st);
             if (s.wnodes)
                 k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
                                                                    ctx->d_counters);
             else
                 k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
                                                                    ctx->d_counters);
+            timing_end(ctx, 1, ev, st);
+            ev = timing_begin(ctx, st);
             fin(S, q, buf, ctl, ctl + 4);
+            timing_end(ctx, 2, ev, st);
             ctx->launches += 4;
         }
         err = cudaGetLastError();

@@ -152,11 +152,13 @@ class Scene:
         return self._context
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0, bvh_width: int = 2) -> None:
+                  max_paths_in_flight: int = 0, bvh_width: int = 2, kernel_timing: bool = False) -> None:
         """Integrator form for passes on this scene: "wavefront" (default) or
-        "megakernel" (one thread per pixel/texel/probe), launch shapes, and
-        the traversed node width (2: binary, the default; 8: compressed wide nodes)."""
-        self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width)
+        "megakernel" (one thread per pixel/texel/probe), launch shapes, the
+        traversed node width (2: binary, the default; 8: compressed wide nodes),
+        and per-stage CUDA-event timing (read with context.read_kernel_times)."""
+        self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width,
+                                kernel_timing)
 
     def info(self) -> dict:
         info = NanSceneInfo()

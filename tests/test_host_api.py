@@ -51,6 +51,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.NanCamera) == 64
     assert ctypes.sizeof(_native.NanCounters) == 32
     assert ctypes.sizeof(_native.NanTuning) == 32
+    assert ctypes.sizeof(_native.NanKernelTimes) == 48
 
 
 def test_null_arguments_are_rejected_without_a_device():
