@@ -259,6 +259,57 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out,
                                  uint32_t count, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned radiance cache. No counterpart in the reference: an online-trained
+ * irradiance cache (multiresolution hash encoding, 16 levels x 2 FP16
+ * features x 2^log2_table entries, feeding a 48-64-64-64-64-16 ReLU MLP whose
+ * first 3 outputs are irradiance RGB) with BF16 tcgen05 forward and backward
+ * kernels, a relative L2 loss and Adam.
+ * Queries are f32[N][8]: position xyz, pad, shading normal xyz, pad.
+ * Targets are f32[N][4]: irradiance rgb, pad. All pointers are device memory.
+ * ------------------------------------------------------------------------ */
+typedef struct NanCache NanCache;
+
+typedef struct NanCacheConfig {
+    float bounds_min[3];       /* positions are normalised to this box */
+    float bounds_max[3];
+    uint32_t log2_table;       /* entries per level, 2^10 .. 2^24 */
+    uint32_t base_resolution;  /* coarsest grid resolution */
+    uint32_t max_resolution;   /* finest grid resolution */
+    float learning_rate;       /* Adam */
+    float beta1;
+    float beta2;
+    float epsilon;
+    float loss_epsilon;        /* relative L2: (o - y)^2 / (o^2 + loss_epsilon) */
+    uint32_t reserved[4];
+} NanCacheConfig;
+
+/* Parameter counts: MLP weights (row-major per layer: 64x48, 3 x 64x64,
+ * 16x64) and hash-table floats (levels x 2^log2_table x 2). */
+NAN_B200_API int nan_cache_sizes(const NanCacheConfig* config, uint64_t* mlp_params,
+                                 uint64_t* table_params);
+NAN_B200_API int nan_cache_create(NanContext* ctx, const NanCacheConfig* config, NanCache** out);
+NAN_B200_API int nan_cache_destroy(NanCache* cache);
+/* Upload parameters (device f32 arrays) and reset the optimizer state. */
+NAN_B200_API int nan_cache_set_params(NanCache* cache, const float* mlp, const float* table,
+                                      void* stream);
+/* Copy parameters, accumulated gradients and the accumulated loss into
+ * device arrays; any output may be NULL. */
+NAN_B200_API int nan_cache_get_params(NanCache* cache, float* mlp, float* table, float* mlp_grad,
+                                      float* table_grad, float* loss, void* stream);
+/* out f32[N][4] = network(queries). */
+NAN_B200_API int nan_cache_infer(NanCache* cache, const float* queries, uint32_t count, float* out,
+                                 void* stream);
+/* Forward + backward of the loss averaged over `batch` samples; adds into
+ * the gradients and the loss (no parameter change). */
+NAN_B200_API int nan_cache_backward(NanCache* cache, const float* queries, const float* targets,
+                                    uint32_t count, uint32_t batch, void* stream);
+/* One Adam step from the accumulated gradients, which it then clears. */
+NAN_B200_API int nan_cache_step(NanCache* cache, void* stream);
+/* Train on `count` samples in batches of `batch`: backward + step each. */
+NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const float* targets,
+                                 uint32_t count, uint32_t batch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -131,6 +131,22 @@ class NanKernelTimes(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class NanCacheConfig(ctypes.Structure):
+    _fields_ = [
+        ("bounds_min", ctypes.c_float * 3),
+        ("bounds_max", ctypes.c_float * 3),
+        ("log2_table", ctypes.c_uint32),
+        ("base_resolution", ctypes.c_uint32),
+        ("max_resolution", ctypes.c_uint32),
+        ("learning_rate", ctypes.c_float),
+        ("beta1", ctypes.c_float),
+        ("beta2", ctypes.c_float),
+        ("epsilon", ctypes.c_float),
+        ("loss_epsilon", ctypes.c_float),
+        ("reserved", ctypes.c_uint32 * 4),
+    ]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -175,6 +191,15 @@ EXPORTS = {
     "nan_trace_probes": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, _I,
                               ctypes.POINTER(NanLighting), _U32, _U32, _VP, _VP]),
     "nan_pack_rgb9e5": (_I, [_VP, _VP, _VP, _U32, _VP]),
+    "nan_cache_sizes": (_I, [ctypes.POINTER(NanCacheConfig), ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "nan_cache_create": (_I, [_VP, ctypes.POINTER(NanCacheConfig), ctypes.POINTER(_VP)]),
+    "nan_cache_destroy": (_I, [_VP]),
+    "nan_cache_set_params": (_I, [_VP, _VP, _VP, _VP]),
+    "nan_cache_get_params": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "nan_cache_infer": (_I, [_VP, _VP, _U32, _VP, _VP]),
+    "nan_cache_backward": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
+    "nan_cache_step": (_I, [_VP, _VP]),
+    "nan_cache_train": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
 }
 
 _lib: ctypes.CDLL | None = None

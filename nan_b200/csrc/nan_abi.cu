@@ -1,4 +1,5 @@
 // nan_abi.cu -- the extern "C" entry points declared in include/nan_b200.h.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -47,6 +48,26 @@ int need_scene(NanContext* ctx) {
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
 
+}  // namespace
+
+
+namespace {
+int cache_enter(NanCache* k) {
+    if (!k) return invalid("null cache");
+    return enter(k->ctx);
+}
+int check_config(const NanCacheConfig* c) {
+    if (!c) return invalid("null cache config");
+    if (c->log2_table < 10 || c->log2_table > 24) return invalid("log2_table must be in [10, 24]");
+    if (c->base_resolution < 2 || c->max_resolution < c->base_resolution || c->max_resolution > (1u << 20))
+        return invalid("resolutions must satisfy 2 <= base <= max <= 2^20");
+    for (int i = 0; i < 3; ++i)
+        if (!(c->bounds_max[i] > c->bounds_min[i])) return invalid("cache bounds are empty");
+    if (!(c->learning_rate > 0.0f) || !(c->beta1 >= 0.0f && c->beta1 < 1.0f) || !(c->beta2 >= 0.0f && c->beta2 < 1.0f) ||
+        !(c->epsilon >= 0.0f) || !(c->loss_epsilon > 0.0f))
+        return invalid("bad optimizer or loss parameter");
+    return NAN_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -115,6 +136,10 @@ NAN_B200_API int nan_ctx_check(NanContext* ctx, void* stream) {
     if (status & 4u) {
         set_error("a texel or probe record names a triangle outside the scene (device status 4)");
         return NAN_ERR_INVALID_ARGUMENT;
+    }
+    if (status & 8u) {
+        set_error("a tensor-core completion wait hit its iteration limit (device status 8)");
+        return NAN_ERR_LIMIT;
     }
     return NAN_OK;
 }
@@ -311,4 +336,85 @@ NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t
     return nan_host::launch_pack_rgb9e5(ctx, slots, out, count, as_stream(stream));
 }
 
+
+NAN_B200_API int nan_cache_sizes(const NanCacheConfig* config, uint64_t* mlp_params, uint64_t* table_params) {
+    int rc = check_config(config);
+    if (rc) return rc;
+    if (mlp_params) *mlp_params = nan_host::cache_mlp_params();
+    if (table_params) *table_params = nan_host::cache_table_params(config);
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_cache_create(NanContext* ctx, const NanCacheConfig* config, NanCache** out) {
+    if (!out) return invalid("null output pointer");
+    *out = nullptr;
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = check_config(config);
+    if (rc) return rc;
+    return nan_host::cache_create(ctx, config, out);
+}
+
+NAN_B200_API int nan_cache_destroy(NanCache* cache) {
+    if (!cache) return NAN_OK;
+    cudaSetDevice(cache->ctx->device);
+    cudaDeviceSynchronize();
+    nan_host::cache_destroy(cache);
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_cache_set_params(NanCache* cache, const float* mlp, const float* table, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    if (!mlp || !table) return invalid("null parameter array");
+    return nan_host::cache_set_params(cache, mlp, table, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_get_params(NanCache* cache, float* mlp, float* table, float* mlp_grad, float* table_grad,
+                                      float* loss, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    return nan_host::cache_get_params(cache, mlp, table, mlp_grad, table_grad, loss, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_infer(NanCache* cache, const float* queries, uint32_t count, float* out, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    if (count && (!queries || !out)) return invalid("null query or output buffer");
+    if (!aligned16(queries) || !aligned16(out)) return invalid("queries and out must be 16-byte aligned");
+    return nan_host::launch_cache_infer(cache, queries, count, nullptr, out, nullptr, nullptr, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_backward(NanCache* cache, const float* queries, const float* targets, uint32_t count,
+                                    uint32_t batch, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    if (count && (!queries || !targets)) return invalid("null query or target buffer");
+    if (!aligned16(queries) || !aligned16(targets)) return invalid("queries and targets must be 16-byte aligned");
+    if (batch == 0) return invalid("batch must be positive");
+    return nan_host::launch_cache_backward(cache, queries, targets, count, batch, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_step(NanCache* cache, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    return nan_host::launch_cache_step(cache, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const float* targets, uint32_t count,
+                                 uint32_t batch, void* stream) {
+    int rc = cache_enter(cache);
+    if (rc) return rc;
+    if (batch == 0) return invalid("batch must be positive");
+    if (count && (!queries || !targets)) return invalid("null query or target buffer");
+    if (!aligned16(queries) || !aligned16(targets)) return invalid("queries and targets must be 16-byte aligned");
+    for (uint32_t b = 0; b < count; b += batch) {
+        const uint32_t n = std::min(batch, count - b);
+        rc = nan_host::launch_cache_backward(cache, queries + 8ull * b, targets + 4ull * b, n, n, as_stream(stream));
+        if (rc) return rc;
+        rc = nan_host::launch_cache_step(cache, as_stream(stream));
+        if (rc) return rc;
+    }
+    return NAN_OK;
+}
 }  // extern "C"

@@ -50,6 +50,22 @@ struct NanContext {
     uint64_t stage_launches[3] = {0, 0, 0};
 };
 
+// Learned radiance cache (nan_cache.cu): parameters, Adam moments and
+// gradients in one block each: mlp = [p | m | v | g] x 16384 floats,
+// table = [p | m | v | g] x table_params floats.
+struct NanCache {
+    NanContext* ctx = nullptr;
+    NanCacheConfig cfg{};
+    uint32_t resolutions[16] = {};
+    size_t table_params = 0;
+    uint64_t step = 0;
+    float* mlp = nullptr;
+    unsigned char* img = nullptr;  // bf16 weight images, interleaved tile layout
+    float* table = nullptr;
+    void* table16 = nullptr;       // fp16 feature pairs read by the encoding
+    float* loss = nullptr;
+};
+
 namespace nan_host {
 
 void set_error(const std::string& msg);
@@ -93,6 +109,18 @@ int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* coun
                                   const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
                                   uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light,
                                   uint32_t begin, uint32_t end, float* compensation, cudaStream_t stream);
+size_t cache_table_params(const NanCacheConfig* cfg);
+size_t cache_mlp_params();
+int cache_create(NanContext* ctx, const NanCacheConfig* cfg, NanCache** out);
+void cache_destroy(NanCache* k);
+int cache_set_params(NanCache* k, const float* mlp, const float* table, cudaStream_t st);
+int cache_get_params(NanCache* k, float* mlp, float* table, float* mlp_grad, float* table_grad, float* loss,
+                     cudaStream_t st);
+int launch_cache_infer(NanCache* k, const float* queries, uint32_t count, const uint32_t* count_dev, float* out,
+                       const float* weights, float* image, cudaStream_t st);
+int launch_cache_backward(NanCache* k, const float* queries, const float* targets, uint32_t count, uint32_t batch,
+                          cudaStream_t st);
+int launch_cache_step(NanCache* k, cudaStream_t st);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 
