@@ -266,7 +266,8 @@ NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t
  * first 3 outputs are irradiance RGB) with BF16 tcgen05 forward and backward
  * kernels, a relative L2 loss and Adam.
  * Queries are f32[N][8]: position xyz, pad, shading normal xyz, pad.
- * Targets are f32[N][4]: irradiance rgb, pad. All pointers are device memory.
+ * Targets are f32[N][4]: irradiance rgb, w (w < 0: no sample, skipped).
+ * All pointers are device memory.
  * ------------------------------------------------------------------------ */
 typedef struct NanCache NanCache;
 
@@ -283,6 +284,25 @@ typedef struct NanCacheConfig {
     float loss_epsilon;        /* relative L2: (o - y)^2 / (o^2 + loss_epsilon) */
     uint32_t reserved[4];
 } NanCacheConfig;
+
+/* Scratch and outputs of one cached frame (nan_trace_screen_cached). */
+typedef struct NanCachedFrame {
+    float* queries;          /* f32[W*H][8] scratch: the frame's cache queries
+                                (position, pixel bits; shading normal, 0) */
+    float* query_weights;    /* f32[W*H][4] scratch: throughput * albedo / pi */
+    uint32_t* query_count;   /* u32[1] scratch */
+    float* train_points;     /* f32[T][4] out: (b1, b2, instance bits, primitive bits |
+                                back << 31) of the training pixels' cache points,
+                                instance ~0 where the path ended earlier */
+    float* train_queries;    /* f32[T][8] out: their cache queries */
+    uint32_t train_count;    /* T */
+    uint32_t train_offset;   /* training pixel i is (offset + i * stride) mod (W*H) */
+    uint32_t train_stride;   /* coprime with W*H */
+    uint32_t train_stride_inverse;  /* stride^-1 mod (W*H) */
+    uint32_t cache_vertex;   /* path vertex answered by the cache: 1 = the second hit (the
+                                cache holds irradiance); 0 = the first hit, after its sun
+                                NEE (the cache holds indirect irradiance) */
+} NanCachedFrame;
 
 /* Parameter counts: MLP weights (row-major per layer: 64x48, 3 x 64x64,
  * 16x64) and hash-table floats (levels x 2^log2_table x 2). */
@@ -309,6 +329,26 @@ NAN_B200_API int nan_cache_step(NanCache* cache, void* stream);
 /* Train on `count` samples in batches of `batch`: backward + step each. */
 NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const float* targets,
                                  uint32_t count, uint32_t batch, void* stream);
+
+/* Irradiance at surface points f32[N][4] (b1, b2, instance bits, primitive
+ * bits | back << 31): the texel estimator (texture_space_path_tracer.slang:
+ * 86-117) with RNG(index, 0xFFFFFFFF, iteration * samples) and view = the
+ * flat normal (negated for back). out f32[N][4] = (E rgb, 0), or
+ * (0, 0, 0, -1) where the instance is ~0. Produces the cache's training
+ * targets; no counterpart in the reference's API. */
+enum { NAN_POINTS_INDIRECT_ONLY = 1 }; /* leave out the direct sun irradiance term */
+NAN_B200_API int nan_trace_points(NanContext* ctx, const float* points, uint32_t count, float* out,
+                                  uint32_t iteration, uint32_t samples, uint32_t max_bounces,
+                                  uint32_t flags, const NanLighting* lighting, void* stream);
+
+/* A cached frame of the screen path tracer: the reference's path
+ * (path_tracer.slang:40-84) up to vertex cache_vertex, whose remaining path
+ * is replaced by throughput * albedo / pi * max(cache irradiance, 0).
+ * Writes out f32[H][W][4] and the frame's training points. */
+NAN_B200_API int nan_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t width,
+                                         uint32_t height, uint32_t frame, const NanCamera* camera,
+                                         const NanLighting* lighting, const NanCachedFrame* frame_desc,
+                                         void* stream);
 
 #ifdef __cplusplus
 }

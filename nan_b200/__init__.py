@@ -15,6 +15,7 @@ PyTorch tensors serve as device buffers; ``command_encoder`` is a CUDA stream.
 """
 
 from .accumulator import Accumulator
+from .cached_path_tracer import CachedPathTracer
 from .camera import Camera, HaltonSamplePattern, halton
 from .mesh_colors import (MESH_COLORS_INVALID_OFFSET, MESH_COLORS_PAYLOAD_SIZE, MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED,
                           MeshColorsLayout, address_to_ij, barycentric_at, colors_per_patch, ij_to_address)
@@ -31,7 +32,7 @@ from .surface_probe_resources import SurfaceProbeGpuGeometry
 from .texture_space_path_tracer import TextureSpacePathTracer
 
 __all__ = [
-    "Accumulator", "Camera", "Device", "HaltonSamplePattern", "Lighting", "Material", "Mesh", "MeshColorsLayout",
+    "Accumulator", "CachedPathTracer", "Camera", "Device", "HaltonSamplePattern", "Lighting", "Material", "Mesh", "MeshColorsLayout",
     "MeshColorsRGB9E5Packer", "PathTracer", "RadianceCache", "RenderData", "Scene", "SceneNode", "SurfaceProbeAttachments",
     "SurfaceProbeDiffuseIrradianceBaker", "SurfaceProbeFieldBuffers", "SurfaceProbeGpuGeometry",
     "SurfaceProbePathTracer", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "address_to_ij",

@@ -147,6 +147,21 @@ class NanCacheConfig(ctypes.Structure):
     ]
 
 
+class NanCachedFrame(ctypes.Structure):
+    _fields_ = [
+        ("queries", ctypes.c_void_p),
+        ("query_weights", ctypes.c_void_p),
+        ("query_count", ctypes.c_void_p),
+        ("train_points", ctypes.c_void_p),
+        ("train_queries", ctypes.c_void_p),
+        ("train_count", ctypes.c_uint32),
+        ("train_offset", ctypes.c_uint32),
+        ("train_stride", ctypes.c_uint32),
+        ("train_stride_inverse", ctypes.c_uint32),
+        ("cache_vertex", ctypes.c_uint32),
+    ]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -200,6 +215,9 @@ EXPORTS = {
     "nan_cache_backward": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
     "nan_cache_step": (_I, [_VP, _VP]),
     "nan_cache_train": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
+    "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),
+    "nan_trace_screen_cached": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
+                                     ctypes.POINTER(NanLighting), ctypes.POINTER(NanCachedFrame), _VP]),
 }
 
 _lib: ctypes.CDLL | None = None

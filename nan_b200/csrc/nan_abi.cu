@@ -417,4 +417,45 @@ NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const fl
     }
     return NAN_OK;
 }
+
+NAN_B200_API int nan_trace_points(NanContext* ctx, const float* points, uint32_t count, float* out,
+                                  uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags,
+                                  const NanLighting* lighting, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = need_scene(ctx);
+    if (rc) return rc;
+    if (count && (!points || !out || !lighting)) return invalid("null argument");
+    if (!aligned16(points) || !aligned16(out)) return invalid("points and out must be 16-byte aligned");
+    if (flags & ~(uint32_t)NAN_POINTS_INDIRECT_ONLY) return invalid("unknown points flag");
+    return nan_host::launch_trace_points_wavefront(ctx, points, count, out, iteration, samples, max_bounces, flags,
+                                                   lighting, as_stream(stream));
+}
+
+NAN_B200_API int nan_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t width,
+                                         uint32_t height, uint32_t frame, const NanCamera* camera,
+                                         const NanLighting* lighting, const NanCachedFrame* fd, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = need_scene(ctx);
+    if (rc) return rc;
+    if (!cache || !out || !camera || !lighting || !fd) return invalid("null argument");
+    if (cache->ctx->device != ctx->device) return invalid("cache and context are on different devices");
+    const uint64_t P = (uint64_t)width * height;
+    if (P == 0) return NAN_OK;
+    if (P > 0x7fffffffull) return invalid("image too large");
+    if (!fd->queries || !fd->query_weights || !fd->query_count) return invalid("null cached-frame scratch");
+    if (fd->train_count && (!fd->train_points || !fd->train_queries)) return invalid("null training buffers");
+    if (fd->train_count > P) return invalid("more training samples than pixels");
+    if (fd->cache_vertex > 1) return invalid("cache_vertex must be 0 or 1");
+    if (fd->train_offset >= P || fd->train_stride == 0 || fd->train_stride >= P + (P == 1 ? 1 : 0))
+        return invalid("training offset and stride must lie in [0, W*H)");
+    if ((uint64_t)fd->train_stride * fd->train_stride_inverse % P != 1 % P)
+        return invalid("train_stride_inverse is not the inverse of train_stride modulo W*H");
+    if (!aligned16(out) || !aligned16(fd->queries) || !aligned16(fd->query_weights) ||
+        !aligned16(fd->train_points) || !aligned16(fd->train_queries))
+        return invalid("image, query and training buffers must be 16-byte aligned");
+    return nan_host::launch_trace_screen_cached(ctx, cache, out, width, height, frame, camera, lighting, fd,
+                                                as_stream(stream));
+}
 }  // extern "C"

@@ -289,12 +289,12 @@ __global__ void __launch_bounds__(kTile) k_cache_infer(CacheView c, const uint4*
 // ---------------------------------------------------------------------------
 struct TrainArgs {
     const float4* queries;  // 2 float4 per sample
-    const float4* targets;  // 1 float4 per sample (rgb)
+    const float4* targets;  // 1 float4 per sample (rgb, w < 0: no sample)
     uint32_t count;
     float batch;            // samples the loss is averaged over
     float inv_batch;        // 1 / batch
     float loss_eps;
-    float* grad;            // [16384]
+    float* partials;        // [gridDim.x][16384] per-CTA weight gradients
     float2* table_grad;     // [L * T]
     float* loss;            // [1] sum of per-sample losses * inv_batch
 };
@@ -356,7 +356,13 @@ __global__ void __launch_bounds__(kTile, 1) k_cache_train(CacheView c, const uin
 
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t q = tile * kTile + r;
-        const bool valid = q < a.count;
+        // a negative target .w marks a sample without a point; samples with
+        // a non-finite target are skipped too
+        bool valid = q < a.count;
+        if (valid) {
+            const float4 y = a.targets[q];
+            valid = !(y.w < 0.0f) && isfinite(y.x) && isfinite(y.y) && isfinite(y.z);
+        }
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f), q1 = q0;
         {
             float x[kInputs];
@@ -471,18 +477,20 @@ __global__ void __launch_bounds__(kTile, 1) k_cache_train(CacheView c, const uin
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (ok && !first) {
-        for (int layer = 0; layer < 5; ++layer) {
-            const int n_out = rows_of(layer), n_in = cols_of(layer);
-            const int m = 16 * (int)warp + (int)lane;  // valid for lanes 0-15
-            for (int c0 = 0; c0 < n_in; c0 += 16) {
-                float v[16];
-                tc::tmem_load16(my_lane + dw_col(layer) + c0, v);
-                if (lane < 16 && m < n_out) {
-                    float* gp = a.grad + off_of(layer) + m * n_in + c0;
+    // into this CTA's partial (summed by k_cache_reduce); zeros if it had no tile
+    float* part = a.partials + (size_t)blockIdx.x * kMlpParams;
+    for (int layer = 0; layer < 5; ++layer) {
+        const int n_out = rows_of(layer), n_in = cols_of(layer);
+        const int m = 16 * (int)warp + (int)lane;  // valid for lanes 0-15
+        for (int c0 = 0; c0 < n_in; c0 += 16) {
+            float v[16];
+            tc::tmem_load16(my_lane + dw_col(layer) + c0, v);
+            if (lane < 16 && m < n_out) {
+                float4* gp = reinterpret_cast<float4*>(part + off_of(layer) + m * n_in + c0);
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) atomicAdd(gp + i, v[i]);
-                }
+                for (int i = 0; i < 4; ++i)
+                    gp[i] = (ok && !first) ? make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3])
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
             }
         }
     }
@@ -495,6 +503,15 @@ __global__ void __launch_bounds__(kTile, 1) k_cache_train(CacheView c, const uin
     __syncthreads();
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_dealloc(tmem, kTrainTmemCols);
+}
+
+// grad[i] += sum over CTAs of partials[c][i] (fixed order: deterministic).
+__global__ void k_cache_reduce(const float* __restrict__ partials, int parts, float* __restrict__ grad) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kMlpParams) return;
+    float acc = 0.0f;
+    for (int c = 0; c < parts; ++c) acc += partials[(size_t)c * kMlpParams + i];
+    grad[i] += acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -623,6 +640,7 @@ int cache_create(NanContext* ctx, const NanCacheConfig* cfg, NanCache** out) {
     grab(reinterpret_cast<void**>(&k->table), 4 * nt * sizeof(float));  // p, m, v, g
     grab(reinterpret_cast<void**>(&k->table16), nt * sizeof(__half));
     grab(reinterpret_cast<void**>(&k->loss), 16);
+    grab(reinterpret_cast<void**>(&k->partials), (size_t)sm_count(ctx->device) * kMlpParams * sizeof(float));
     if (err == cudaSuccess) err = cudaFuncSetAttribute(k_cache_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                        kTrainSmem);
     if (err == cudaSuccess) err = cudaFuncSetAttribute(k_cache_infer, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -642,6 +660,7 @@ void cache_destroy(NanCache* k) {
     cudaFree(k->table);
     cudaFree(k->table16);
     cudaFree(k->loss);
+    cudaFree(k->partials);
     delete k;
 }
 
@@ -705,14 +724,15 @@ int launch_cache_backward(NanCache* k, const float* queries, const float* target
     a.batch = (float)batch;
     a.inv_batch = (float)(1.0 / (double)batch);
     a.loss_eps = k->cfg.loss_epsilon;
-    a.grad = k->mlp + 3 * kMlpParams;
+    a.partials = k->partials;
     a.table_grad = reinterpret_cast<float2*>(k->table + 3 * k->table_params);
     a.loss = k->loss;
     const uint32_t tiles = (count + kTile - 1) / kTile;
     // one CTA per SM: 512 TMEM columns and 124 KB shared memory each
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)sm_count(k->ctx->device));
     k_cache_train<<<grid, kTile, kTrainSmem, st>>>(cache_view(k), reinterpret_cast<const uint4*>(k->img), a);
-    k->ctx->launches++;
+    k_cache_reduce<<<kMlpParams / 256, 256, 0, st>>>(k->partials, (int)grid, k->mlp + 3 * kMlpParams);
+    k->ctx->launches += 2;
     return cuda_fail(cudaGetLastError(), "cache training");
 }
 

@@ -64,6 +64,7 @@ struct NanCache {
     float* table = nullptr;
     void* table16 = nullptr;       // fp16 feature pairs read by the encoding
     float* loss = nullptr;
+    float* partials = nullptr;     // per-CTA weight gradients of one training launch
 };
 
 namespace nan_host {
@@ -121,6 +122,12 @@ int launch_cache_infer(NanCache* k, const float* queries, uint32_t count, const 
 int launch_cache_backward(NanCache* k, const float* queries, const float* targets, uint32_t count, uint32_t batch,
                           cudaStream_t st);
 int launch_cache_step(NanCache* k, cudaStream_t st);
+int launch_trace_points_wavefront(NanContext* ctx, const float* points, uint32_t count, float* out,
+                                  uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags,
+                                  const NanLighting* light, cudaStream_t st);
+int launch_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t w, uint32_t h,
+                               uint32_t frame, const NanCamera* cam, const NanLighting* light,
+                               const NanCachedFrame* fd, cudaStream_t st);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

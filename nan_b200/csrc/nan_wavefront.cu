@@ -155,13 +155,17 @@ struct TexelArgs {
     uint32_t n;  // samples per texel
     uint32_t max_bounces;
     int reset;
+    // points mode (irradiance at given surface points instead of texels)
+    const float4* points;  // (b1, b2, instance bits, primitive bits | back << 31)
+    float4* point_out;     // (E rgb, 0), or (0, 0, 0, -1) for no point
+    int indirect_only;     // points mode: leave out the direct sun irradiance term
 };
 
 // Start sample k of the current side: sun irradiance shadow ray, first
 // direction (estimate_surface_irradiance, texture_space_path_tracer.slang:95-113).
 __device__ __forceinline__ void texel_start_sample(const SceneView& s, const LightParams& L, const WfState& st,
                                                    const WfQueues& q, int buf, uint32_t* ctl_next, uint32_t p,
-                                                   uint32_t flags, Rng& rng) {
+                                                   uint32_t flags, Rng& rng, bool direct = true) {
     const float4 sf = st.surf[p];
     const uint32_t inst = __float_as_uint(sf.z), prim = __float_as_uint(sf.w);
     f3 view = world_flat_normal(s, inst, prim);
@@ -170,7 +174,8 @@ __device__ __forceinline__ void texel_start_sample(const SceneView& s, const Lig
     const float u0 = rng.next_1d(), u1 = rng.next_1d();
     const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
     const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
-    push_shadow(q, buf, ctl_next + 2, p, sd.origin_front, l, L.illum * ndl, kKindSun);
+    // the two draws are taken either way, so the RNG streams stay aligned
+    if (direct) push_shadow(q, buf, ctl_next + 2, p, sd.origin_front, l, L.illum * ndl, kKindSun);
     st.si[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     st.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     st.thp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -207,6 +212,34 @@ __global__ void __launch_bounds__(128) k_wf_texel_generate(SceneView s, Lighting
     st.rng[p] = rng.state;
     RayTally none{0u, 0u};
     flush_tally(counters, none, 1u, (ts.side.y & 1u) ? 2u * a.n : a.n);
+}
+
+// Surface points instead of texels: the same estimator at the listed points,
+// with RNG(index, 0xFFFFFFFF, iteration * n) and view = the flat normal,
+// negated for the back side.
+__global__ void __launch_bounds__(128) k_wf_point_generate(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+                                                           WfQueues q, uint32_t begin, uint32_t count,
+                                                           unsigned long long* counters) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const uint32_t u = begin + p;
+    const float4 pt = a.points[u];
+    const uint32_t inst = __float_as_uint(pt.z), primw = __float_as_uint(pt.w);
+    const uint32_t prim = primw & 0x7fffffffu;
+    if (inst == 0xffffffffu || !valid_prim(s, inst, prim)) {
+        if (inst != 0xffffffffu) atomicOr(s.status, kStatusBadRecord);
+        a.point_out[u] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        return;
+    }
+    const LightParams L = make_light(lraw);
+    Rng rng(u, 0xffffffffu, a.iteration * a.n);
+    st.unit[p] = u;
+    st.surf[p] = make_float4(pt.x, pt.y, __uint_as_float(inst), __uint_as_float(prim));
+    st.irr[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    texel_start_sample(s, L, st, q, 0, q.ctl, p, (primw >> 31) ? kFlagBack : 0u, rng, !a.indirect_only);
+    st.rng[p] = rng.state;
+    RayTally none{0u, 0u};
+    flush_tally(counters, none, 1u, a.n);
 }
 
 // One bounce of trace_radiance (texture_space_path_tracer.slang:60-83) after
@@ -289,12 +322,16 @@ __global__ void __launch_bounds__(128) k_wf_texel_finalize(SceneView s, Lighting
         if (k < a.n) {
             flags = (flags & ((1u << kSampleShift) - 1u)) | (k << kSampleShift);
             st.irr[p] = f4(irr, 0.0f);
-            texel_start_sample(s, L, st, q, nbuf, ctl_next, p, flags, rng);
+            texel_start_sample(s, L, st, q, nbuf, ctl_next, p, flags, rng, !a.indirect_only);
             st.rng[p] = rng.state;
             continue;
         }
-        // side complete: running mean into its slot
         const uint32_t u = st.unit[p];
+        if (a.point_out) {
+            a.point_out[u] = f4(irr / (float)a.n, 0.0f);
+            continue;
+        }
+        // side complete: running mean into its slot
         const uint32_t inst = __float_as_uint(st.surf[p].z);
         const uint4 info = __ldg(a.mc.instance_infos + inst);
         const uint2 side = __ldg(a.mc.side_infos + inst);
@@ -326,10 +363,26 @@ struct CameraWf {  // layout of NanCamera
     float far_clip;
 };
 
+// Cached frames: paths end at their second hit, which becomes a cache query
+// (position and pixel, shading normal, weight = throughput * albedo / pi).
+// Pixels (offset + i * stride) mod P for i < train_count also record the
+// hit as training point i.
+struct CachedArgs {
+    float4* queries;  // 2 per query
+    float4* weights;
+    uint32_t* query_count;
+    float4* train_points;
+    float4* train_queries;  // 2 per training point
+    uint32_t train_count, train_offset, train_inverse;
+    uint32_t vertex;  // path vertex that queries the cache: 0 (indirect) or 1
+};
+
 struct ScreenArgs {
     CameraWf cam;
     float4* out;
     uint32_t width, height, frame, max_vertices;
+    int cached;
+    CachedArgs cache;
 };
 
 __global__ void __launch_bounds__(128) k_wf_screen_generate(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
@@ -392,10 +445,44 @@ __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRa
         const uint2 ref = __ldg(s.tri_refs + flat);
         const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
         rad = rad + thp * sd.emissive;
+        const f3 f = sd.diffuse * kInvPi;
+        if (a.cached && vertex == a.cache.vertex) {
+            // the rest of the path is the cache's irradiance at this point;
+            // at vertex 0 the sun is still sampled (NEE) and the cache holds
+            // the indirect irradiance only
+            if (vertex == 0u) {
+                const float u0 = rng.next_1d(), u1 = rng.next_1d();
+                const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
+                const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+                push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
+            }
+            const uint32_t pixel = st.unit[p];
+            const uint32_t qi = queue_slot(a.cache.query_count, true);
+            const float4 q0 = make_float4(sd.position.x, sd.position.y, sd.position.z, __uint_as_float(pixel));
+            const float4 q1 = f4(sd.frame.n, 0.0f);
+            a.cache.queries[2u * qi] = q0;
+            a.cache.queries[2u * qi + 1u] = q1;
+            a.cache.weights[qi] = f4(thp * f, 0.0f);
+            const uint32_t P = a.width * a.height;
+            const uint32_t rel = pixel >= a.cache.train_offset ? pixel - a.cache.train_offset
+                                                               : pixel + (P - a.cache.train_offset);
+            const uint32_t ti = (uint32_t)(((uint64_t)rel * a.cache.train_inverse) % P);
+            if (ti < a.cache.train_count) {
+                // a back side exists for double-sided materials only (as texel back slots)
+                const bool two = (__float_as_uint(__ldg(tri_refs(s, ref.x, ref.y).mat + 3)) & 1u) != 0u;
+                const bool back = two && dot3(world_flat_normal(s, ref.x, ref.y), -d) < 0.0f;
+                a.cache.train_points[ti] = make_float4(h.z, h.w, __uint_as_float(ref.x),
+                                                       __uint_as_float(ref.y | (back ? 0x80000000u : 0u)));
+                a.cache.train_queries[2u * ti] = q0;
+                a.cache.train_queries[2u * ti + 1u] = q1;
+            }
+            st.rad[p] = f4(rad, 0.0f);
+            st.flags[p] = flags | kFlagEnd;
+            continue;
+        }
         const float u0 = rng.next_1d(), u1 = rng.next_1d();
         const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
         const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
-        const f3 f = sd.diffuse * kInvPi;
         push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
         const float e0 = rng.next_1d(), e1 = rng.next_1d();
         float pdf;
@@ -888,6 +975,7 @@ int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay,
     const SceneView s = scene_view(ctx);
     const LightingRaw lr = to_raw(light);
     TexelArgs a;
+    memset(&a, 0, sizeof(a));
     a.mc.compensation = reinterpret_cast<float4*>(lay->compensation);
     a.mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
     a.mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
@@ -915,9 +1003,76 @@ int launch_trace_texels_wavefront(NanContext* ctx, const NanMeshColorsDesc* lay,
         });
 }
 
+namespace {
+int screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame, uint32_t max_vertices,
+                     const NanCamera* cam, const NanLighting* light, const CachedArgs* cached, cudaStream_t st);
+}  // namespace
+
 int launch_trace_screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame,
                                   uint32_t max_vertices, const NanCamera* cam, const NanLighting* light,
                                   cudaStream_t st) {
+    return screen_wavefront(ctx, out, w, h, frame, max_vertices, cam, light, nullptr, st);
+}
+
+int launch_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t w, uint32_t h,
+                               uint32_t frame, const NanCamera* cam, const NanLighting* light,
+                               const NanCachedFrame* fd, cudaStream_t st) {
+    CachedArgs c;
+    c.queries = reinterpret_cast<float4*>(fd->queries);
+    c.weights = reinterpret_cast<float4*>(fd->query_weights);
+    c.query_count = fd->query_count;
+    c.train_points = reinterpret_cast<float4*>(fd->train_points);
+    c.train_queries = reinterpret_cast<float4*>(fd->train_queries);
+    c.train_count = fd->train_count;
+    c.train_offset = fd->train_offset;
+    c.train_inverse = fd->train_stride_inverse;
+    c.vertex = fd->cache_vertex;
+    cudaError_t err = cudaMemsetAsync(fd->query_count, 0, sizeof(uint32_t), st);
+    if (err == cudaSuccess && fd->train_count)
+        err = cudaMemsetAsync(fd->train_points, 0xff, (size_t)fd->train_count * 16u, st);
+    if (err != cudaSuccess) return cuda_fail(err, "cached frame reset");
+    int rc = screen_wavefront(ctx, out, w, h, frame, fd->cache_vertex + 1u, cam, light, &c, st);
+    if (rc) return rc;
+    return launch_cache_infer(cache, fd->queries, w * h, fd->query_count, nullptr, fd->query_weights, out, st);
+}
+
+int launch_trace_points_wavefront(NanContext* ctx, const float* points, uint32_t count, float* out,
+                                  uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags,
+                                  const NanLighting* light, cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    const uint32_t n = std::max(samples, 1u);
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    int rc = wf_plan(ctx, (uint64_t)n * std::max(max_bounces, 1u), &iters, &cap);
+    if (rc) return rc;
+    const SceneView s = scene_view(ctx);
+    const LightingRaw lr = to_raw(light);
+    TexelArgs a;
+    memset(&a, 0, sizeof(a));
+    a.iteration = iteration;
+    a.n = n;
+    a.max_bounces = std::max(max_bounces, 1u);
+    a.points = reinterpret_cast<const float4*>(points);
+    a.point_out = reinterpret_cast<float4*>(out);
+    a.indirect_only = (flags & NAN_POINTS_INDIRECT_ONLY) != 0u;
+    const Grid g = grid_for(ctx);
+    unsigned long long* counters = ctx->d_counters;
+    return wf_run(
+        ctx, st, 0, count, iters, cap, lr.ray_t_max,
+        [&](const WfState& S, const WfQueues& q, uint32_t first, uint32_t cnt) {
+            k_wf_point_generate<<<(cnt + 127) / 128, 128, 0, st>>>(s, lr, a, S, q, first, cnt, counters);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl) {
+            k_wf_texel_shade<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl);
+        },
+        [&](const WfState& S, const WfQueues& q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
+            k_wf_texel_finalize<<<g.stream_blocks, 128, 0, st>>>(s, lr, a, S, q, buf, ctl, ctl_next);
+        });
+}
+
+namespace {
+int screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame, uint32_t max_vertices,
+                     const NanCamera* cam, const NanLighting* light, const CachedArgs* cached, cudaStream_t st) {
     const uint64_t pixels = (uint64_t)w * h;
     if (pixels == 0 || max_vertices == 0) return NAN_OK;
     uint32_t iters = 0;
@@ -933,6 +1088,9 @@ int launch_trace_screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint3
     a.height = h;
     a.frame = frame;
     a.max_vertices = max_vertices;
+    a.cached = cached != nullptr;
+    if (cached) a.cache = *cached;
+    else memset(&a.cache, 0, sizeof(a.cache));
     const Grid g = grid_for(ctx);
     unsigned long long* counters = ctx->d_counters;
     return wf_run(
@@ -947,6 +1105,7 @@ int launch_trace_screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint3
             k_wf_screen_finalize<<<g.stream_blocks, 128, 0, st>>>(a, S, q, buf, ctl, ctl_next);
         });
 }
+}  // namespace
 
 int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits,
                                   uint32_t* radial, const uint8_t* probes, uint32_t probe_count,

@@ -1,0 +1,128 @@
+"""Time to a target RMSE: the plain screen path tracer against the same path
+tracer with the learned radiance cache, on one scene.
+
+The reference image is the plain path tracer (max_vertices path vertices)
+accumulated over many frames in float64 on the GPU (FP64 is used only for
+this reduction). Both integrators start cold and accumulate 1 spp frames;
+the learned one first renders `warmup_frames` frames that only train the
+cache (their time counts, their images are not accumulated). Every frame is
+timed with CUDA events on the launching stream (render, plus the cache's
+training for the learned integrator). The error of an accumulated image is
+its relative RMSE against the reference over all pixels and channels.
+"""
+
+from __future__ import annotations
+
+
+def _rel_rmse(img, ref) -> float:
+    import torch
+
+    d = img - ref
+    return float(torch.sqrt(torch.mean(d * d)) / torch.sqrt(torch.mean(ref * ref)))
+
+
+def scene_bounds(scene, margin: float = 1e-3):
+    tris = scene.world_triangles().reshape(-1, 3)
+    lo = tris.min(dim=0).values.cpu().numpy()
+    hi = tris.max(dim=0).values.cpu().numpy()
+    pad = margin * float((hi - lo).max())
+    return tuple(float(x) - pad for x in lo), tuple(float(x) + pad for x in hi)
+
+
+def compare(device, scene, width: int, height: int, *, reference_frames: int = 512, frames: int = 64,
+            max_vertices: int = 5, train_samples: int = 65536, train_batch: int = 65536, log2_table: int = 19,
+            base_resolution: int = 16, max_resolution: int = 2048, learning_rate: float = 1e-2,
+            checkpoints=None, seed: int = 0, cache_vertex: int = 1, warmup_frames: int = 0) -> dict:
+    """Curves (frames, cumulative ms, relative RMSE) of the plain and the
+    cached integrator, and the time each needs to reach the plain
+    integrator's RMSE after `frames` frames (within 1.1x for the cached one)."""
+    import torch
+
+    from .cached_path_tracer import CachedPathTracer
+    from .path_tracer import PathTracer
+    from .radiance_cache import RadianceCache
+
+    stream = torch.cuda.current_stream()
+    cam = scene.camera
+    out = torch.zeros((height, width, 4), dtype=torch.float32, device=device.torch_device)
+    plain = PathTracer(device, scene, max_vertices=max_vertices)
+
+    ref = torch.zeros((height, width, 3), dtype=torch.float64, device=device.torch_device)
+    for f in range(reference_frames):
+        cam.begin_frame(width, height)
+        plain.execute(stream, out, 1_000_000 + f)
+        ref += out[..., :3].double()
+    ref /= reference_frames
+
+    checkpoints = sorted(set(checkpoints or [1, 2, 4, 8, 16, 32, 64, 128, 256]))
+    checkpoints = [c for c in checkpoints if c <= frames] or [frames]
+    if checkpoints[-1] != frames:
+        checkpoints.append(frames)
+
+    def run(tracer, warmup=0) -> list[tuple[int, float, float]]:
+        acc = torch.zeros((height, width, 3), dtype=torch.float64, device=device.torch_device)
+        curve, total_ms = [], 0.0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for f in range(warmup):
+            cam.begin_frame(width, height)
+            e0.record(stream)
+            tracer.execute(stream, out, frames + f)
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+        for f in range(frames):
+            cam.begin_frame(width, height)
+            e0.record(stream)
+            tracer.execute(stream, out, f)
+            e1.record(stream)
+            acc += out[..., :3].double()
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            if f + 1 in checkpoints:
+                curve.append((f + 1, total_ms, _rel_rmse(acc / (f + 1), ref)))
+        return curve
+
+    plain_curve = run(plain)
+    lo, hi = scene_bounds(scene)
+    cache = RadianceCache(device, lo, hi, log2_table=log2_table, base_resolution=base_resolution,
+                          max_resolution=max_resolution, learning_rate=learning_rate, seed=seed)
+    cached = CachedPathTracer(device, scene, cache, cache_vertex=cache_vertex, max_vertices=max_vertices,
+                              train_samples=train_samples, train_batch=train_batch)
+    cached_curve = run(cached, warmup_frames)
+    # the same cached integrator with the cache left untrained: what training gains
+    cold = RadianceCache(device, lo, hi, log2_table=log2_table, base_resolution=base_resolution,
+                         max_resolution=max_resolution, seed=seed)
+    untrained_curve = run(CachedPathTracer(device, scene, cold, cache_vertex=cache_vertex, max_vertices=max_vertices,
+                                           train=False))
+
+    target = plain_curve[-1][2]
+    t_plain = plain_curve[-1][1]
+    t_cached = next((ms for (_, ms, e) in cached_curve if e <= 1.1 * target), None)
+    device.check()
+    return {
+        "width": width, "height": height, "frames": frames, "reference_frames": reference_frames,
+        "max_vertices": max_vertices, "train_samples": train_samples, "train_batch": train_batch,
+        "cache_vertex": cache_vertex, "warmup_frames": warmup_frames,
+        "plain": plain_curve, "cached": cached_curve, "untrained": untrained_curve,
+        "target_rmse": target, "plain_ms_to_target": t_plain, "cached_ms_to_target": t_cached,
+        "speedup": (t_plain / t_cached) if t_cached else None,
+        "plain_ms_per_frame": plain_curve[-1][1] / frames, "cached_ms_per_frame": cached_curve[-1][1] / frames,
+        "rmse_per_frame_count": {"plain": plain_curve[-1][2], "cached": cached_curve[-1][2],
+                                 "untrained": untrained_curve[-1][2]},
+    }
+
+
+def summary(r: dict) -> str:
+    lines = [f"{r['width']}x{r['height']}, cache vertex {r['cache_vertex']}, warm-up {r['warmup_frames']}, reference "
+             f"{r['reference_frames']} frames, target = plain RMSE after {r['frames']} frames = {r['target_rmse']:.4f}"]
+    for name in ("plain", "cached", "untrained"):
+        lines.append(name + ": " + ", ".join(f"{n}f {ms:.0f}ms {e:.4f}" for n, ms, e in r[name]))
+    sp = r["speedup"]
+    lines.append(f"time to target: plain {r['plain_ms_to_target']:.0f} ms, cached "
+                 f"{r['cached_ms_to_target'] if r['cached_ms_to_target'] is None else round(r['cached_ms_to_target'])}"
+                 f" ms, speed-up {'n/a' if sp is None else f'{sp:.2f}x'}")
+    return "\n".join(lines)
+
+
+__all__ = ["compare", "summary", "scene_bounds"]

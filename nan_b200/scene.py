@@ -160,6 +160,23 @@ class Scene:
         self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width,
                                 kernel_timing)
 
+    def trace_points(self, points, iteration: int, samples: int = 1, max_bounces: int = 3, out=None, stream=None,
+                     indirect_only: bool = False):
+        """Irradiance at surface points f32[N, 4] (b1, b2, instance bits,
+        primitive bits | back << 31): f32[N, 4] (E rgb, 0; w = -1 where the
+        instance is ~0). The estimator of TextureSpacePathTracer at given points."""
+        import torch
+
+        n = int(points.shape[0])
+        if out is None:
+            out = torch.empty((n, 4), dtype=torch.float32, device=points.device)
+        self.context.reserve_paths(max(n, 1))
+        light = self.lighting.to_struct()
+        check(lib().nan_trace_points(self.context.handle, ptr(points), n, ptr(out), int(iteration) & 0xFFFFFFFF,
+                                     int(samples), int(max_bounces), int(bool(indirect_only)), ctypes.byref(light),
+                                     stream_handle(stream)))
+        return out
+
     def info(self) -> dict:
         info = NanSceneInfo()
         check(lib().nan_scene_info(self.context.handle, ctypes.byref(info)))

@@ -1020,12 +1020,12 @@ V3<T> ts_trace_radiance(Tracer<T>& tr, V3<T> o, V3<T> d, Rng& rng, uint32_t max_
 
 template <class T>
 V3<T> ts_estimate(Tracer<T>& tr, uint32_t inst, uint32_t prim, T bx, T by, V3<T> view, uint32_t n,
-                  Rng& rng, uint32_t max_bounces) {
+                  Rng& rng, uint32_t max_bounces, bool direct = true) {
     Shading<T> sd = shading_data<T>(tr.s, inst, prim, bx, by, view);
     V3<T> irr = mk<T>(0, 0, 0);
     for (uint32_t k = 0; k < n; ++k) {
         T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
-        V3<T> si = tr.sun_irradiance(sd, u0, u1);
+        V3<T> si = direct ? tr.sun_irradiance(sd, u0, u1) : mk<T>(0, 0, 0);
         T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
         V3<T> dir;
         T pdf;
@@ -1481,6 +1481,46 @@ int oracle_trace_texels(void* sp, const OracleLighting* lighting, uint8_t* slots
     });
     for (auto& c : unit_counts) add_counts(counts, c);
     if (bad) { g_error = "texel index out of range"; return 1; }
+    return 0;
+}
+
+int oracle_trace_points(void* sp, const OracleLighting* lighting, const float* points, int count,
+                        uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags, float* out,
+                        int precision, int threads, OracleRayCounts* counts) {
+    Scene* s = static_cast<Scene*>(sp);
+    std::vector<OracleRayCounts> unit_counts((size_t)count);
+    std::atomic<int> bad{0};
+    parallel_for(count, threads, [&](int u, int) {
+        float* o = out + 4 * (size_t)u;
+        uint32_t inst, primw;
+        std::memcpy(&inst, points + 4 * (size_t)u + 2, 4);
+        std::memcpy(&primw, points + 4 * (size_t)u + 3, 4);
+        o[0] = o[1] = o[2] = 0.0f;
+        o[3] = -1.0f;
+        if (inst == 0xffffffffu) return;
+        const uint32_t prim = primw & 0x7fffffffu;
+        const bool back = (primw >> 31) != 0;
+        if ((size_t)inst * 4 >= s->instance_descs.size() ||
+            prim >= s->mesh_descs[4 * (size_t)s->instance_descs[4 * (size_t)inst] + 1] / 3u) {
+            bad = 1;
+            return;
+        }
+        const float b1 = points[4 * (size_t)u], b2 = points[4 * (size_t)u + 1];
+        const uint32_t n = std::max(samples, 1u);
+        Rng rng((uint32_t)u, 0xffffffffu, iteration * n);
+        auto run = [&](auto tag) {
+            using T = decltype(tag);
+            Tracer<T> tr(*s, *lighting);
+            V3<T> view = world_flat_normal<T>(*s, inst, prim);
+            if (back) view = -view;
+            V3<T> e = ts_estimate<T>(tr, inst, prim, T(b1), T(b2), view, n, rng, max_bounces, (flags & 1u) == 0u);
+            o[0] = (float)e.x; o[1] = (float)e.y; o[2] = (float)e.z; o[3] = 0.0f;
+            unit_counts[u] = tr.cnt;
+        };
+        if (precision == ORACLE_F64) run(double(0)); else run(float(0));
+    });
+    for (auto& c : unit_counts) add_counts(counts, c);
+    if (bad) { g_error = "point names a triangle outside the scene"; return 1; }
     return 0;
 }
 

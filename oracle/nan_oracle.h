@@ -130,6 +130,18 @@ int oracle_trace_texels(void* scene, const OracleLighting* lighting,
                         uint32_t max_bounces, int reset, int precision,
                         int threads, OracleRayCounts* counts);
 
+/* Irradiance at surface points: the texel estimator
+ * (estimate_surface_irradiance, texture_space_path_tracer.slang:86-117) at
+ * points f32[N][4] = (b1, b2, instance bits, primitive bits | back << 31),
+ * with view = the flat normal (negated for back), RNG(index, 0xFFFFFFFF,
+ * iteration * n). out f32[N][4] = (E rgb, 0), or (0, 0, 0, -1) where the
+ * instance is ~0 (no point). flags bit 0: leave out the direct sun
+ * irradiance term (its two RNG draws are still taken). The points pass of
+ * the learned cache's training, checked bit for bit. */
+int oracle_trace_points(void* scene, const OracleLighting* lighting, const float* points, int count,
+                        uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags,
+                        float* out, int precision, int threads, OracleRayCounts* counts);
+
 /* Surface-probe irradiance baker (surface_probe_path_tracer.slang:280-315)
  * for the listed probe indices. Buffers are updated in place. */
 int oracle_trace_probes(void* scene, const OracleLighting* lighting,

@@ -108,6 +108,7 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, vp, u32, vp, i,
                                       u32, u32, u32, i, i, i, vp]
+    l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
 
 
 # ---- scalar helpers --------------------------------------------------------
@@ -304,6 +305,19 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
         return counts.as_dict()
+
+    def trace_points(self, lighting, points, iteration, samples, max_bounces, flags=0, precision=F32, threads=0):
+        """Irradiance at surface points f32[N, 4] (b1, b2, instance bits,
+        primitive bits | back << 31); returns f32[N, 4] and the ray counts."""
+        pts = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 4)
+        out = np.zeros_like(pts)
+        counts = OracleRayCounts()
+        L = lighting_struct(lighting)
+        rc = lib().oracle_trace_points(self.handle, ctypes.byref(L), _p(pts), pts.shape[0], iteration, samples,
+                                       max_bounces, flags, _p(out), precision, threads, ctypes.byref(counts))
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return out, counts.as_dict()
 
     def trace_probes(self, lighting, values, sample_counts, self_hits, radial, probes,
                      probe_instances, units, iteration, samples_per_probe, max_bounces,

@@ -1,0 +1,128 @@
+"""Learned-cache integrator on the GPU.
+
+* The points pass (training targets) equals the oracle's texel estimator at
+  the same surface points bit for bit (>= 99.9 % of points exact, all within
+  1e-4 relative), as the texel tracer does.
+* A cached frame writes one cache query per path that reached its second hit
+  and records the training pixels' points.
+* What the trained network gains: on the same frames, the cached integrator
+  with online training ends far closer to the plain integrator's converged
+  image than the same integrator with the cache left untrained (at these
+  small image sizes the fixed training cost per frame exceeds the traversal
+  it saves; frame costs at 1920x1080 are measured by bench.py).
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_points(node, n, seed):
+    h = node.pack()
+    rng = np.random.default_rng(seed)
+    inst = rng.integers(0, h["instance_descs"].shape[0], n)
+    mesh = h["instance_descs"][inst, 0]
+    prims = h["mesh_descs"][mesh, 1] // 3
+    prim = (rng.random(n) * prims).astype(np.uint32)
+    b = rng.random((n, 2)).astype(np.float32)
+    flip = b.sum(axis=1) > 1.0
+    b[flip] = 1.0 - b[flip]
+    # back sides exist for double-sided materials only (as texel back slots)
+    double_sided = (h["materials"][h["instance_descs"][inst, 1], 3].view(np.uint32) & 1) != 0
+    back = (rng.random(n) < 0.25) & double_sided
+    pts = np.zeros((n, 4), np.float32)
+    pts[:, 0:2] = b
+    pts[:, 2] = inst.astype(np.uint32).view(np.float32)
+    pts[:, 3] = (prim | np.where(back, 0x80000000, 0).astype(np.uint32)).view(np.float32)
+    pts[::97, 2] = np.uint32(0xFFFFFFFF).view(np.float32)  # a few entries without a point
+    return pts
+
+
+@pytest.mark.parametrize("which", ["cornell", "terrain"])
+def test_points_pass_matches_oracle(which, device):
+    import torch
+
+    import nan_b200
+    from nan_b200 import scenes
+    from oracle.oracle import OracleScene
+
+    node = scenes.cornell_box(64, 64) if which == "cornell" else scenes.terrain_boxes(seed=1, grid=129, boxes=120)
+    scene = nan_b200.Scene(device, node)
+    orc = OracleScene(**scene.host)
+    pts = _random_points(node, 3000, seed=5)
+    for it in (0, 7):
+        gpu = scene.trace_points(torch.from_numpy(pts).cuda(), it, samples=2, max_bounces=3).cpu().numpy()
+        ref, _ = orc.trace_points(scene.lighting, pts, it, 2, 3)
+        exact = np.all(gpu == ref, axis=1)
+        rel = np.max(np.abs(gpu - ref) / np.maximum(np.abs(ref), 1e-3), axis=1)
+        print(which, it, "exact", exact.mean())
+        assert exact.mean() >= 0.999, exact.mean()
+        assert np.all(rel <= 1e-4)
+        assert np.all(gpu[::97, 3] == -1.0)
+    device.check()
+
+
+def test_cached_frame_records_queries_and_training_points(device):
+    import torch
+
+    import nan_b200
+    from nan_b200 import scenes
+    from nan_b200.learned_eval import scene_bounds
+
+    node = scenes.terrain_boxes(seed=1, grid=129, boxes=120)
+    scene = nan_b200.Scene(device, node)
+    lo, hi = scene_bounds(scene)
+    cache = nan_b200.RadianceCache(device, lo, hi, log2_table=16)
+    w, h = 96, 64
+    tracer = nan_b200.CachedPathTracer(device, scene, cache, train_samples=1000, train_batch=512)
+    out = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+    node.camera.begin_frame(w, h)
+    tracer.execute(None, out, 3)
+    torch.cuda.synchronize()
+    nq = int(tracer.query_count[0])
+    assert 0 < nq <= w * h
+    pts = tracer.train_points.cpu().numpy()
+    valid = pts[:, 2].view(np.uint32) != 0xFFFFFFFF
+    assert valid.mean() > 0.1
+    # each training point's query is one of the frame's queries
+    tq = tracer.train_queries.cpu().numpy()[valid]
+    allq = tracer.queries.cpu().numpy()[:nq]
+    pix = allq[:, 3].view(np.uint32)
+    lookup = {int(p): i for i, p in enumerate(pix)}
+    for row in tq[:50]:
+        j = lookup[int(row[3:4].view(np.uint32)[0])]
+        np.testing.assert_array_equal(allq[j], row)
+    # training pixel i is (offset + i * stride) mod P
+    i = np.nonzero(valid)[0][:50]
+    expect = (tracer_offset(3, w * h) + i * tracer._stride) % (w * h)
+    np.testing.assert_array_equal(tq[:50, 3].view(np.uint32), expect.astype(np.uint32))
+    assert torch.isfinite(out).all()
+    device.check()
+
+
+def tracer_offset(frame, p):
+    return (frame * 2654435761) % p
+
+
+@pytest.mark.parametrize("which", ["cornell", "terrain"])
+def test_trained_cache_gains_over_untrained(which, device):
+    import nan_b200
+    from nan_b200 import learned_eval, scenes
+
+    if which == "cornell":
+        node, w, h = scenes.cornell_box(64, 64), 64, 64
+    else:
+        node, w, h = scenes.terrain_boxes(seed=1, grid=129, boxes=120), 128, 96
+    scene = nan_b200.Scene(device, node)
+    r = learned_eval.compare(device, scene, w, h, reference_frames=512, frames=64, train_samples=w * h,
+                             train_batch=4096, log2_table=16, base_resolution=8, max_resolution=512)
+    print(which, learned_eval.summary(r))
+    e = r["rmse_per_frame_count"]
+    if which == "terrain":
+        # open scene: an untrained cache drops the indirect light after the second hit
+        assert e["cached"] <= 0.5 * e["untrained"], e
+    else:
+        # closed box lit by an emitter found only by BSDF sampling: noise dominates
+        # at 64 frames, and the trained cache still lowers the error
+        assert e["cached"] < e["untrained"] and e["cached"] < e["plain"], e
