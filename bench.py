@@ -58,6 +58,7 @@ def parse_args():
     ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache time-to-RMSE measurement")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
 
@@ -422,7 +423,42 @@ def run_nan(args):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
+    if world == 1 and not args.no_learned:
+        line["learned_cache"] = learned_cache_line(device)
     print(json.dumps(line))
+
+
+def learned_cache_line(device) -> dict:
+    """Time to RMSE of the learned-cache path tracer against the plain one on
+    the seeded 998,408-triangle scene (699x699 terrain + 2000 boxes) at
+    1920x1080, 1 spp per frame, against a 256-frame plain reference
+    accumulated in float64."""
+    import torch
+
+    import nan_b200
+    from nan_b200 import learned_eval, scenes
+
+    node = scenes.terrain_boxes(seed=1, grid=699, boxes=2000)
+    scene = nan_b200.Scene(device, node)
+    out = {"scene": f"terrain 699x699 + 2000 boxes, {scene.triangle_count} triangles, sun 45 deg + sky 0.5",
+           "image": "1920x1080, 1 spp per frame, 5 path vertices", "runs": []}
+    for cv, batch in ((1, 16384), (0, 8192)):
+        r = learned_eval.compare(device, scene, 1920, 1080, reference_frames=256, frames=64, cache_vertex=cv,
+                                 warmup_frames=32, train_batch=batch)
+        out["runs"].append({
+            "cache_vertex": cv, "warmup_frames": 32, "train_samples_per_frame": 65536, "train_batch": batch,
+            "target_rmse": r["target_rmse"], "plain_ms_to_target": r["plain_ms_to_target"],
+            "cached_ms_to_target": r["cached_ms_to_target"], "speedup": r["speedup"],
+            "rmse_after_64_frames": r["rmse_per_frame_count"],
+            "ms_per_frame": {"plain": r["plain_ms_per_frame"], "cached": r["cached_ms_per_frame"],
+                             "cached_without_training": r["untrained_ms_per_frame"]},
+            "cached_warmup_ms": r["cached_warmup_ms"],
+            "cached_curve": [[n, round(ms, 2), round(e, 5)] for n, ms, e in r["cached"]],
+            "plain_curve": [[n, round(ms, 2), round(e, 5)] for n, ms, e in r["plain"]],
+        })
+        del r
+    torch.cuda.synchronize()
+    return out
 
 
 def main():

@@ -59,6 +59,8 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
     if checkpoints[-1] != frames:
         checkpoints.append(frames)
 
+    warm_ms = {}
+
     def run(tracer, warmup=0) -> list[tuple[int, float, float]]:
         acc = torch.zeros((height, width, 3), dtype=torch.float64, device=device.torch_device)
         curve, total_ms = [], 0.0
@@ -71,6 +73,7 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
             e1.record(stream)
             e1.synchronize()
             total_ms += e0.elapsed_time(e1)
+        warm_ms[id(tracer)] = total_ms
         for f in range(frames):
             cam.begin_frame(width, height)
             e0.record(stream)
@@ -90,6 +93,7 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
     cached = CachedPathTracer(device, scene, cache, cache_vertex=cache_vertex, max_vertices=max_vertices,
                               train_samples=train_samples, train_batch=train_batch)
     cached_curve = run(cached, warmup_frames)
+    cached_warm_ms = warm_ms[id(cached)]
     # the same cached integrator with the cache left untrained: what training gains
     cold = RadianceCache(device, lo, hi, log2_table=log2_table, base_resolution=base_resolution,
                          max_resolution=max_resolution, seed=seed)
@@ -107,7 +111,9 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
         "plain": plain_curve, "cached": cached_curve, "untrained": untrained_curve,
         "target_rmse": target, "plain_ms_to_target": t_plain, "cached_ms_to_target": t_cached,
         "speedup": (t_plain / t_cached) if t_cached else None,
-        "plain_ms_per_frame": plain_curve[-1][1] / frames, "cached_ms_per_frame": cached_curve[-1][1] / frames,
+        "plain_ms_per_frame": plain_curve[-1][1] / frames,
+        "cached_ms_per_frame": (cached_curve[-1][1] - cached_warm_ms) / frames, "cached_warmup_ms": cached_warm_ms,
+        "untrained_ms_per_frame": untrained_curve[-1][1] / frames,
         "rmse_per_frame_count": {"plain": plain_curve[-1][2], "cached": cached_curve[-1][2],
                                  "untrained": untrained_curve[-1][2]},
     }
