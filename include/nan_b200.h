@@ -260,6 +260,58 @@ NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t
                                  uint32_t count, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Multi-scene probe batches. No counterpart in the reference (one dispatch
+ * per scene, surface_probe_path_tracer.py:49-83): the probe sets of many
+ * scenes are baked by one persistent launch that balances (scene, probe)
+ * units across the GPU, optionally replayed from a captured CUDA graph.
+ * Each set has the buffers of nan_trace_probes. The batch keeps a snapshot of
+ * every scene's BVH: rebuild the batch after rebuilding a scene.
+ * ------------------------------------------------------------------------ */
+typedef struct NanBatch NanBatch;
+
+typedef struct NanProbeSet {
+    NanContext* scene;               /* context whose scene (BVH) the probes sit in */
+    const uint8_t* probes;           /* u8[N][48] */
+    uint32_t probe_count;
+    const uint8_t* probe_instances;  /* u8[I][48] */
+    uint32_t probe_instance_count;
+    float* values;                   /* f32[N][3] */
+    uint32_t* sample_counts;         /* u32[N] */
+    uint32_t* self_hits;             /* u32[N] */
+    uint32_t* radial;                /* u32[N][16] */
+    float* compensation;             /* optional f32[N][4] */
+    NanLighting lighting;
+} NanProbeSet;
+
+typedef struct NanBatchTuning {
+    uint32_t stack_depth;     /* traversal stack entries: 32, 48, 64 or 96 (>= every BVH's need) */
+    uint32_t blocks_per_sm;   /* persistent 128-thread blocks per SM */
+    uint32_t units_per_grab;  /* probes per lane taken from the work counter at once */
+    uint32_t reserved;
+} NanBatchTuning;
+
+NAN_B200_API int nan_batch_create(NanContext* ctx, const NanProbeSet* sets, uint32_t set_count,
+                                  NanBatch** out);
+NAN_B200_API int nan_batch_destroy(NanBatch* batch);
+/* Smallest admissible stack depth, the total probe count, the current tuning. */
+NAN_B200_API int nan_batch_info(NanBatch* batch, uint32_t* min_stack_depth, uint32_t* total_probes,
+                                NanBatchTuning* tuning);
+NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tuning);
+/* One iteration of every set (nan_trace_probes semantics per set). */
+NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,
+                                        uint32_t max_bounces, int reset, void* stream);
+/* Time each admissible launch shape on one frame (reset, iteration 0) and
+ * keep the fastest; the outputs then hold that frame. */
+NAN_B200_API int nan_batch_autotune(NanBatch* batch, uint32_t samples_per_probe, uint32_t max_bounces,
+                                    void* stream, NanBatchTuning* chosen, float* frame_ms);
+/* Capture one frame into a CUDA graph. The next replayed frame has
+ * iteration first_iteration (reset if reset_first); each replay advances the
+ * iteration on the device. Synchronises `stream` once. */
+NAN_B200_API int nan_batch_capture(NanBatch* batch, uint32_t first_iteration, int reset_first,
+                                   uint32_t samples_per_probe, uint32_t max_bounces, void* stream);
+NAN_B200_API int nan_batch_replay(NanBatch* batch, uint32_t frames, void* stream);
+
+/* ------------------------------------------------------------------------
  * Learned radiance cache. No counterpart in the reference: an online-trained
  * irradiance cache (multiresolution hash encoding, 16 levels x 2 FP16
  * features x 2^log2_table entries, feeding a 48-64-64-64-64-16 ReLU MLP whose

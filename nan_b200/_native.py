@@ -162,6 +162,31 @@ class NanCachedFrame(ctypes.Structure):
     ]
 
 
+class NanProbeSet(ctypes.Structure):
+    _fields_ = [
+        ("scene", ctypes.c_void_p),
+        ("probes", ctypes.c_void_p),
+        ("probe_count", ctypes.c_uint32),
+        ("probe_instances", ctypes.c_void_p),
+        ("probe_instance_count", ctypes.c_uint32),
+        ("values", ctypes.c_void_p),
+        ("sample_counts", ctypes.c_void_p),
+        ("self_hits", ctypes.c_void_p),
+        ("radial", ctypes.c_void_p),
+        ("compensation", ctypes.c_void_p),
+        ("lighting", NanLighting),
+    ]
+
+
+class NanBatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("stack_depth", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("units_per_grab", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -215,6 +240,14 @@ EXPORTS = {
     "nan_cache_backward": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
     "nan_cache_step": (_I, [_VP, _VP]),
     "nan_cache_train": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
+    "nan_batch_create": (_I, [_VP, _VP, _U32, ctypes.POINTER(_VP)]),
+    "nan_batch_destroy": (_I, [_VP]),
+    "nan_batch_info": (_I, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(NanBatchTuning)]),
+    "nan_batch_set_tuning": (_I, [_VP, ctypes.POINTER(NanBatchTuning)]),
+    "nan_batch_trace_probes": (_I, [_VP, _U32, _U32, _U32, _I, _VP]),
+    "nan_batch_autotune": (_I, [_VP, _U32, _U32, _VP, ctypes.POINTER(NanBatchTuning), ctypes.POINTER(ctypes.c_float)]),
+    "nan_batch_capture": (_I, [_VP, _U32, _I, _U32, _U32, _VP]),
+    "nan_batch_replay": (_I, [_VP, _U32, _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),
     "nan_trace_screen_cached": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
                                      ctypes.POINTER(NanLighting), ctypes.POINTER(NanCachedFrame), _VP]),

@@ -458,4 +458,79 @@ NAN_B200_API int nan_trace_screen_cached(NanContext* ctx, NanCache* cache, float
     return nan_host::launch_trace_screen_cached(ctx, cache, out, width, height, frame, camera, lighting, fd,
                                                 as_stream(stream));
 }
+
+NAN_B200_API int nan_batch_create(NanContext* ctx, const NanProbeSet* sets, uint32_t set_count, NanBatch** out) {
+    if (!out) return invalid("null output pointer");
+    *out = nullptr;
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (set_count && !sets) return invalid("null probe sets");
+    for (uint32_t i = 0; i < set_count; ++i) {
+        const NanProbeSet& p = sets[i];
+        if (!p.scene || p.scene->device != ctx->device) return invalid("probe set scene is null or on another device");
+        if (!p.scene->has_scene) return invalid("probe set scene has no BVH");
+        if (p.probe_count && (!p.probes || !p.probe_instances || !p.values || !p.sample_counts || !p.self_hits ||
+                              !p.radial))
+            return invalid("null probe buffer");
+        if (!aligned16(p.probes) || !aligned16(p.probe_instances) || !aligned16(p.compensation))
+            return invalid("probe records, instances and compensation must be 16-byte aligned");
+    }
+    return nan_host::batch_create(ctx, sets, set_count, out);
+}
+
+NAN_B200_API int nan_batch_destroy(NanBatch* batch) {
+    if (!batch) return NAN_OK;
+    cudaSetDevice(batch->ctx->device);
+    cudaDeviceSynchronize();
+    nan_host::batch_destroy(batch);
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_batch_info(NanBatch* batch, uint32_t* min_stack_depth, uint32_t* total_probes,
+                                NanBatchTuning* tuning) {
+    if (!batch) return invalid("null batch");
+    if (min_stack_depth) *min_stack_depth = nan_host::batch_min_depth(batch);
+    if (total_probes) *total_probes = nan_host::batch_total(batch);
+    if (tuning) *tuning = batch->tuning;
+    return NAN_OK;
+}
+
+NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tuning) {
+    if (!batch || !tuning) return invalid("null argument");
+    return nan_host::batch_set_tuning(batch, tuning);
+}
+
+NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,
+                                        uint32_t max_bounces, int reset, void* stream) {
+    if (!batch) return invalid("null batch");
+    int rc = enter(batch->ctx);
+    if (rc) return rc;
+    return nan_host::batch_frame(batch, iteration, samples_per_probe, max_bounces, reset, as_stream(stream));
+}
+
+NAN_B200_API int nan_batch_autotune(NanBatch* batch, uint32_t samples_per_probe, uint32_t max_bounces, void* stream,
+                                    NanBatchTuning* chosen, float* frame_ms) {
+    if (!batch) return invalid("null batch");
+    int rc = enter(batch->ctx);
+    if (rc) return rc;
+    rc = nan_host::batch_autotune(batch, samples_per_probe, max_bounces, as_stream(stream), chosen);
+    if (frame_ms) *frame_ms = batch->tuned_ms;
+    return rc;
+}
+
+NAN_B200_API int nan_batch_capture(NanBatch* batch, uint32_t first_iteration, int reset_first,
+                                   uint32_t samples_per_probe, uint32_t max_bounces, void* stream) {
+    if (!batch) return invalid("null batch");
+    int rc = enter(batch->ctx);
+    if (rc) return rc;
+    return nan_host::batch_capture(batch, first_iteration, reset_first, samples_per_probe, max_bounces,
+                                   as_stream(stream));
+}
+
+NAN_B200_API int nan_batch_replay(NanBatch* batch, uint32_t frames, void* stream) {
+    if (!batch) return invalid("null batch");
+    int rc = enter(batch->ctx);
+    if (rc) return rc;
+    return nan_host::batch_replay(batch, frames, as_stream(stream));
+}
 }  // extern "C"

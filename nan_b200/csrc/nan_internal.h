@@ -68,6 +68,18 @@ struct NanCache {
 };
 
 namespace nan_host {
+struct BatchImpl;
+}
+
+// Multi-scene probe batch (nan_batch.cu).
+struct NanBatch {
+    NanContext* ctx = nullptr;  // device, counters and status of the batched launches
+    nan_host::BatchImpl* impl = nullptr;
+    NanBatchTuning tuning{};
+    float tuned_ms = -1.0f;
+};
+
+namespace nan_host {
 
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
@@ -128,6 +140,16 @@ int launch_trace_points_wavefront(NanContext* ctx, const float* points, uint32_t
 int launch_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t w, uint32_t h,
                                uint32_t frame, const NanCamera* cam, const NanLighting* light,
                                const NanCachedFrame* fd, cudaStream_t st);
+int batch_create(NanContext* ctx, const NanProbeSet* sets, uint32_t count, NanBatch** out);
+void batch_destroy(NanBatch* b);
+uint32_t batch_min_depth(const NanBatch* b);
+uint32_t batch_total(const NanBatch* b);
+int batch_set_tuning(NanBatch* b, const NanBatchTuning* t);
+int batch_frame(NanBatch* b, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset, cudaStream_t st);
+int batch_capture(NanBatch* b, uint32_t first_iteration, int reset_first, uint32_t spp, uint32_t max_bounces,
+                  cudaStream_t st);
+int batch_replay(NanBatch* b, uint32_t frames, cudaStream_t st);
+int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t st, NanBatchTuning* chosen);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

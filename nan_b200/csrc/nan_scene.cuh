@@ -318,6 +318,7 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
 // Closest hit in [tmin, tmax]; ties in t go to the lower flat triangle index
 // (lexicographic (instance, primitive)), so the result does not depend on
 // the traversal order. Binary-node traversal.
+template <int kDepth = kTraversalStack>
 __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
     HitInfo hit;
     hit.valid = false;
@@ -328,7 +329,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
     if (s.tri_count == 0) return hit;
     const WtRay wr = wt_setup(d);
     const BoxRay br = box_setup(o, d);
-    int stack[kTraversalStack];
+    int stack[kDepth];
     int sp = 0;
     int node = s.root;
     float best_t = tmax;
@@ -345,7 +346,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
             if (h0 && h1) {
                 int near_child = nd.x, far_child = nd.y;
                 if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kTraversalStack) stack[sp++] = far_child;
+                if (sp < kDepth) stack[sp++] = far_child;
                 else atomicOr(s.status, kStatusStackOverflow);
                 node = near_child;
                 continue;
@@ -387,11 +388,12 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
 }
 
 // Any hit in [tmin, tmax]. Binary-node traversal.
+template <int kDepth = kTraversalStack>
 __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
     if (s.tri_count == 0) return false;
     const WtRay wr = wt_setup(d);
     const BoxRay br = box_setup(o, d);
-    int stack[kTraversalStack];
+    int stack[kDepth];
     int sp = 0;
     int node = s.root;
     for (;;) {
@@ -405,7 +407,7 @@ __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d,
             if (h0 && h1) {
                 int near_child = nd.x, far_child = nd.y;
                 if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kTraversalStack) stack[sp++] = far_child;
+                if (sp < kDepth) stack[sp++] = far_child;
                 else atomicOr(s.status, kStatusStackOverflow);
                 node = near_child;
                 continue;
@@ -462,6 +464,28 @@ __device__ __forceinline__ HitInfo trace_closest(const SceneView& s, f3 o, f3 d,
 __device__ __forceinline__ bool trace_any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
     return s.wnodes ? trace_any_w<8>(s, o, d, tmin, tmax) : trace_any_w<2>(s, o, d, tmin, tmax);
 }
+
+// Traversal policies for code templated on the tracer: the run-time
+// dispatch, or binary nodes with a fixed stack depth (a depth below the
+// BVH's must not be chosen: the overflow is flagged and the push dropped).
+struct DefaultTracer {
+    __device__ static HitInfo closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+        return trace_closest(s, o, d, tmin, tmax);
+    }
+    __device__ static bool any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+        return trace_any(s, o, d, tmin, tmax);
+    }
+};
+
+template <int kDepth>
+struct BinaryTracer {
+    __device__ static HitInfo closest(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+        return trace_closest_binary<kDepth>(s, o, d, tmin, tmax);
+    }
+    __device__ static bool any(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+        return trace_any_binary<kDepth>(s, o, d, tmin, tmax);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // Shading (scene.slang:178-406, opaque and untextured materials).
@@ -665,11 +689,12 @@ struct RayTally {
 };
 
 // sample_directional_light_with_visibility(sd, u, 1, 0), scene.slang:954-990.
+template <class Tr = DefaultTracer>
 __device__ __forceinline__ f3 sun_nee(const SceneView& s, const LightParams& L, const Shading& sd, float ux,
                                       float uy, RayTally& tally) {
     const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, ux, uy);
     tally.shadow++;
-    const float vis = trace_any(s, sd.origin_front, l, 0.0f, L.t_max) ? 0.0f : 1.0f;
+    const float vis = Tr::any(s, sd.origin_front, l, 0.0f, L.t_max) ? 0.0f : 1.0f;
     const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
     const f3 f = sd.diffuse * kInvPi;
     return ((vis * f) * L.illum) * ndl;

@@ -1,0 +1,123 @@
+"""Multi-scene probe batches: one persistent launch over the probe sets of
+several scenes of uneven size equals baking each scene on its own, bit for
+bit. That holds for direct frames, for frames replayed from the captured CUDA
+graph, and after the autotuner has changed the launch shape."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _probe_set(device, node, count, seed, compensated=False):
+    import nan_b200
+    from nan_b200 import scenes
+
+    scene = nan_b200.Scene(device, node)
+    probes, pinst = scenes.surface_sites(node, count, seed=seed, radius=0.2)
+    layout = type("L", (), {})()
+    layout.probes, layout.instance_gpu_data = probes, pinst
+    layout.nodes = np.zeros((1, 4), np.uint32)
+    layout.triangle_vertex_probes = np.zeros((1, 4), np.uint32)
+    layout.total_probe_count = probes.shape[0]
+    layout.instance_infos = list(range(pinst.shape[0]))
+    geometry = nan_b200.SurfaceProbeGpuGeometry.create(device, layout)
+    baker = nan_b200.SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=4,
+                                                        compensated=compensated)
+    return scene, baker
+
+
+def _buffers(device, baker):
+    import nan_b200
+
+    rt = nan_b200.SurfaceProbeRuntimeBuffers.acquire(nan_b200.RenderData(device), baker.geometry.probe_count)
+    return rt.field, rt.attachments
+
+
+def _snapshot(field, attachments, baker):
+    out = [field.values.cpu().numpy().copy(), field.sample_counts.cpu().numpy().copy(),
+           attachments.self_hit_counts.cpu().numpy().copy(), attachments.radial_moments.cpu().numpy().copy()]
+    if baker.compensation is not None:
+        out.append(baker.compensation.cpu().numpy().copy())
+    return out
+
+
+@pytest.fixture(scope="module")
+def sets(device):
+    from nan_b200 import scenes
+
+    items = [
+        _probe_set(device, scenes.cornell_box(32, 32), 300, seed=3),
+        _probe_set(device, scenes.terrain_boxes(seed=2, grid=65, boxes=30), 1000, seed=4, compensated=True),
+        _probe_set(device, scenes.terrain_boxes(seed=3, grid=97, boxes=60), 517, seed=5),
+    ]
+    for scene, _ in items:
+        scene.configure("megakernel")
+    return items
+
+
+def _reference(device, sets, frames):
+    refs = []
+    for scene, baker in sets:
+        field, att = _buffers(device, baker)
+        if baker.compensation is not None:
+            baker.compensation.zero_()
+        for it in range(frames):
+            baker.execute(None, field, att, it, reset=(it == 0))
+        refs.append(_snapshot(field, att, baker))
+    return refs
+
+
+def _bake_batch(device, sets, run):
+    import nan_b200
+
+    bufs = [_buffers(device, b) for _, b in sets]
+    for _, b in sets:
+        if b.compensation is not None:
+            b.compensation.zero_()
+    batch = nan_b200.ProbeBatch(device, [(b, f, a) for (_, b), (f, a) in zip(sets, bufs)])
+    run(batch)
+    return batch, [_snapshot(f, a, b) for (_, b), (f, a) in zip(sets, bufs)]
+
+
+def test_batch_equals_per_scene_bakes(device, sets):
+    refs = _reference(device, sets, 3)
+
+    def run(batch):
+        # double-sided walls carry a back record per site as well
+        assert batch.info()["total_probes"] == sum(int(b.geometry.probe_count) for _, b in sets)
+        for it in range(3):
+            batch.execute(None, it, 4, 3, reset=(it == 0))
+
+    _, got = _bake_batch(device, sets, run)
+    for g, ref in zip(got, refs):
+        for a, b in zip(g, ref):
+            np.testing.assert_array_equal(a, b)
+    device.check()
+
+
+def test_batch_graph_replay_and_autotune(device, sets):
+    from nan_b200._native import NanError
+
+    refs = _reference(device, sets, 3)
+    state = {}
+
+    def run(batch):
+        tuned = batch.autotune(4, 3)
+        print("autotune", tuned, batch.info())
+        assert tuned["stack_depth"] >= batch.info()["min_stack_depth"] and tuned["frame_ms"] > 0.0
+        for _, b in sets:
+            if b.compensation is not None:
+                b.compensation.zero_()
+        batch.capture(0, True, 4, 3)
+        batch.replay(3)
+        state["batch"] = batch
+
+    batch, got = _bake_batch(device, sets, run)
+    for g, ref in zip(got, refs):
+        for a, b in zip(g, ref):
+            np.testing.assert_array_equal(a, b)
+    # a shallower stack than the BVHs need is refused
+    with pytest.raises(NanError):
+        batch.set_tuning(16, 4, 1)
+    device.check()

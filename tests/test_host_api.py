@@ -52,6 +52,10 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.NanCounters) == 32
     assert ctypes.sizeof(_native.NanTuning) == 32
     assert ctypes.sizeof(_native.NanKernelTimes) == 48
+    assert ctypes.sizeof(_native.NanCacheConfig) == 72
+    assert ctypes.sizeof(_native.NanCachedFrame) == 64
+    assert ctypes.sizeof(_native.NanProbeSet) == 144
+    assert ctypes.sizeof(_native.NanBatchTuning) == 16
 
 
 def test_null_arguments_are_rejected_without_a_device():
