@@ -59,6 +59,7 @@ def parse_args():
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache time-to-RMSE measurement")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batched probe measurement")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
 
@@ -425,6 +426,14 @@ def run_nan(args):
         line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
     if world == 1 and not args.no_learned:
         line["learned_cache"] = learned_cache_line(device)
+    if world == 1 and not args.no_batched:
+        from nan_b200 import batch_eval
+
+        line["batched_probes"] = dict(batch_eval.measure(device, count=64, seed=1, samples_per_probe=64,
+                                                         max_bounces=3, frames=2),
+                                      workload="64 seeded terrain+box scenes, triangles log-uniform 1e3-5e5, "
+                                               "sites U{512..20480} (area-weighted random), 64 spp, 3 bounces, "
+                                               "compensated running means")
     print(json.dumps(line))
 
 

@@ -1,0 +1,103 @@
+"""Multi-scene surface-probe baking: one batched persistent launch (direct
+and replayed from a CUDA graph) against one baker dispatch per scene.
+
+Every frame bakes every site of every scene (samples_per_probe cosine
+samples, max_bounces bounces, compensated running means). Frames are timed
+with CUDA events on the launching stream after one warm-up frame; rays are
+counted on the device.
+"""
+
+from __future__ import annotations
+
+import time
+
+
+def _sites_layout(probes, pinst):
+    import numpy as np
+
+    layout = type("SiteLayout", (), {})()
+    layout.probes, layout.instance_gpu_data = probes, pinst
+    layout.nodes = np.zeros((1, 4), np.uint32)
+    layout.triangle_vertex_probes = np.zeros((1, 4), np.uint32)
+    layout.total_probe_count = probes.shape[0]
+    layout.instance_infos = list(range(pinst.shape[0]))
+    return layout
+
+
+def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64, max_bounces: int = 3,
+            frames: int = 3, tri_max: float = 5e5) -> dict:
+    import torch
+
+    from . import scenes as sc
+    from .probe_batch import ProbeBatch
+    from .render_data import RenderData
+    from .scene import Scene
+    from .surface_probe_fields import SurfaceProbeRuntimeBuffers
+    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from .surface_probe_resources import SurfaceProbeGpuGeometry
+
+    t0 = time.perf_counter()
+    items, tris, sites = [], [], []
+    for i, (node, n_sites) in enumerate(sc.batch_scenes(count, seed, tri_max=tri_max)):
+        scene = Scene(device, node)
+        probes, pinst = sc.surface_sites(node, n_sites, seed=seed + i, radius=0.25)
+        geometry = SurfaceProbeGpuGeometry.create(device, _sites_layout(probes, pinst))
+        baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=samples_per_probe,
+                                                   max_bounces=max_bounces, compensated=True)
+        rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)
+        items.append((scene, baker, rt.field, rt.attachments))
+        tris.append(scene.triangle_count)
+        sites.append(int(geometry.probe_count))
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn) -> float:
+        fn(0)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for f in range(1, frames + 1):
+            fn(f)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / frames
+
+    # one baker dispatch per scene (the reference's shape), wavefront integrator
+    def per_scene(f):
+        for scene, baker, field, att in items:
+            baker.execute(stream, field, att, f, reset=(f == 0))
+
+    for scene, *_ in items:
+        scene.context.read_counters(reset=True)
+    per_scene_ms = timed(per_scene)
+    per_scene_rays = sum(sum(v for k, v in s.context.read_counters(reset=True).items()
+                             if k in ("extend_rays", "shadow_rays")) for s, *_ in items) / (frames + 1)
+    # the same, one thread per probe (the kernel the batch runs, one launch per scene)
+    for scene, *_ in items:
+        scene.configure("megakernel")
+    per_scene_mk_ms = timed(per_scene)
+    for scene, *_ in items:
+        scene.configure("wavefront")
+        scene.context.read_counters(reset=True)
+
+    batch = ProbeBatch(device, [(b, f, a) for _, b, f, a in items])
+    tuned = batch.autotune(samples_per_probe, max_bounces)
+    batch.context.read_counters(reset=True)
+    batch_ms = timed(lambda f: batch.execute(stream, f, samples_per_probe, max_bounces, reset=(f == 0)))
+    c = batch.context.read_counters(reset=True)
+    batch_rays = (c["extend_rays"] + c["shadow_rays"]) / (frames + 1)
+    batch.capture(0, True, samples_per_probe, max_bounces)
+    graph_ms = timed(lambda f: batch.replay(1, stream))
+    device.check()
+    return {
+        "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
+        "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
+        "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
+        "setup_s": setup_s, "autotune": tuned,
+        "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
+                         "batched": batch_ms, "batched_graph": graph_ms},
+        "rays_per_frame": batch_rays, "per_scene_rays_per_frame": per_scene_rays,
+        "mrays_per_s": {"per_scene_wavefront": per_scene_rays / (per_scene_ms * 1e3),
+                        "per_scene_megakernel": per_scene_rays / (per_scene_mk_ms * 1e3),
+                        "batched": batch_rays / (batch_ms * 1e3), "batched_graph": batch_rays / (graph_ms * 1e3)},
+    }

@@ -14,6 +14,9 @@ distributions of the workload it stands for.
   noise) plus 500 boxes with sides U[0.2, 3] and random yaw; albedo
   U[0.1, 0.9]; sun at 45 deg elevation with irradiance 3, sky 0.5. The
   default 313x313 grid gives 194,688 + 6,000 = 200,688 triangles.
+* ``batch_scenes()``     -- many terrain_boxes scenes with triangle counts
+  log-uniform in [1e3, 5e5] and a site count U{512..20480} each (the
+  multi-scene probe workload).
 """
 
 from __future__ import annotations
@@ -164,6 +167,22 @@ def terrain_boxes(seed: int = 1, grid: int = 313, cell: float = 0.15, boxes: int
     s.lighting = Lighting.sun_elevation(45.0, azimuth_deg=30.0, irradiance=3.0, sky=0.5)
     s.terrain_cell = cell
     return s
+
+
+def batch_scenes(count: int = 64, seed: int = 1, tri_min: float = 1e3, tri_max: float = 5e5,
+                 sites_min: int = 512, sites_max: int = 20480) -> list[tuple[SceneNode, int]]:
+    """(scene, site count) pairs. Each scene is a terrain_boxes scene of about
+    T triangles, T log-uniform in [tri_min, tri_max]: 95 % terrain grid and
+    5 % boxes (12 triangles each)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        t = math.exp(rng.uniform(math.log(tri_min), math.log(tri_max)))
+        boxes = max(1, int(0.05 * t / 12.0))
+        grid = max(3, int(round(math.sqrt(0.95 * t / 2.0))) + 1)
+        node = terrain_boxes(seed=seed * 1000 + i, grid=grid, boxes=boxes)
+        out.append((node, int(rng.integers(sites_min, sites_max + 1))))
+    return out
 
 
 def surface_sites(scene_node: SceneNode, count: int, seed: int = 1, radius: float = 0.25,
