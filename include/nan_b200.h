@@ -54,7 +54,9 @@ typedef struct NanLighting {
     float sun_transmittance[3]; /* ground-level factor (LUT stand-in) */
     float ray_t_max;            /* t_max of bounce and shadow rays (Ray default 1000) */
     float sky_radiance[3];      /* constant sky radiance on misses */
-    uint32_t flags;             /* bit 0: add the sun disk on primary misses */
+    uint32_t flags;             /* bit 0: add the sun disk on primary misses; bit 1: screen
+                                   tracer NEE toward the context's area lights with MIS
+                                   (nan_ctx_set_area_lights; not in the reference) */
 } NanLighting;
 
 /* Pinhole camera: the fields compute_ray_pinhole reads (camera.slang:173-236,
@@ -162,6 +164,14 @@ NAN_B200_API int nan_ctx_read_counters(NanContext* ctx, NanCounters* out, int re
  * only; never inside a trace call). Synchronises the device. */
 NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes);
 NAN_B200_API uint64_t nan_wavefront_bytes_per_path(void);
+/* Emissive triangles for area-light NEE (lighting flag bit 1). lights is a
+ * caller-owned device table f32[count][16]: v0 xyz, cdf (inclusive, last =
+ * 1); e1 = v1 - v0, area; e2 = v2 - v0, luminance (0.2126 r + 0.7152 g +
+ * 0.0722 b); emission rgb, 0. power = sum of area * luminance. It must list
+ * every emissive triangle of the scene and stay alive while traced. No
+ * counterpart in the reference (its path tracer reaches emitters by BSDF
+ * sampling only). count 0 clears the table. */
+NAN_B200_API int nan_ctx_set_area_lights(NanContext* ctx, const float* lights, uint32_t count, float power);
 /* Select the integrator form and its launch shapes (see NanTuning). */
 NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning);
 /* Number of kernels this context has launched. */

@@ -216,6 +216,7 @@ EXPORTS = {
     "nan_ctx_reserve": (_I, [_VP, _U64]),
     "nan_wavefront_bytes_per_path": (_U64, []),
     "nan_ctx_read_kernel_times": (_I, [_VP, ctypes.POINTER(NanKernelTimes), _I]),
+    "nan_ctx_set_area_lights": (_I, [_VP, _VP, _U32, ctypes.c_float]),
     "nan_ctx_configure": (_I, [_VP, ctypes.POINTER(NanTuning)]),
     "nan_scene_build": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP]),
     "nan_scene_build_noalloc": (_I, [_VP, ctypes.POINTER(NanSceneDesc), _VP, _U64, _VP, _U64, _VP, _U64, _VP]),

@@ -184,6 +184,16 @@ NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes) {
     return NAN_OK;
 }
 
+NAN_B200_API int nan_ctx_set_area_lights(NanContext* ctx, const float* lights, uint32_t count, float power) {
+    if (!ctx) return invalid("null context");
+    if (count && (!lights || !aligned16(lights))) return invalid("area lights must be a 16-byte aligned table");
+    if (count && !(power > 0.0f)) return invalid("area light power must be positive");
+    ctx->lights = count ? lights : nullptr;
+    ctx->light_count = count;
+    ctx->light_power = count ? power : 0.0f;
+    return NAN_OK;
+}
+
 NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
     if (!ctx || !tuning) return invalid("null argument");
     if (tuning->integrator > 1) return invalid("integrator must be 0 (wavefront) or 1 (one thread per unit)");

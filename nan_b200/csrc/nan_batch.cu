@@ -122,6 +122,9 @@ SceneView scene_view_for_batch(const NanContext* ctx) {
     v.tri_count = ctx->tri_count;
     v.instance_count = ctx->scene.instance_count;
     v.status = ctx->d_status;
+    v.lights = reinterpret_cast<const float4*>(ctx->lights);
+    v.light_count = ctx->lights ? ctx->light_count : 0u;
+    v.light_power = ctx->light_power;
     return v;
 }
 

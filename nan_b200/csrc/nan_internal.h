@@ -38,6 +38,10 @@ struct NanContext {
     void* scratch = nullptr;
     uint64_t scratch_bytes = 0;
     NanTuning tuning{};
+    // Area lights (nan_ctx_set_area_lights): caller-owned table.
+    const float* lights = nullptr;
+    uint32_t light_count = 0;
+    float light_power = 0.0f;
     // Stage timing (NanTuning.kernel_timing): events pending a read, a pool
     // of free events, and the sums per stage kind (0 extend, 1 shadow, 2 other).
     struct TimedLaunch {

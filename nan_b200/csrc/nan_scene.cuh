@@ -39,6 +39,11 @@ struct SceneView {
     uint32_t tri_count;
     uint32_t instance_count;
     uint32_t* status;               // device status word
+    // emissive triangles for area-light NEE (4 float4 each: v0 + cdf, e1 + area,
+    // e2 + luminance, emission); null when none were given
+    const float4* lights;
+    uint32_t light_count;
+    float light_power;              // sum of area * luminance
 };
 
 constexpr uint32_t kStatusBadRecord = 4u;
@@ -633,6 +638,7 @@ struct LightParams {
     f3 sky;
     float t_max;
     bool sun_disk;
+    bool area_nee;  // screen tracer: NEE toward the emissive triangles, MIS with the BSDF
 };
 
 struct LightingRaw {  // layout of NanLighting
@@ -656,7 +662,68 @@ __device__ __forceinline__ LightParams make_light(const LightingRaw& p) {
     L.sky = mk3(p.sky_radiance[0], p.sky_radiance[1], p.sky_radiance[2]);
     L.t_max = p.ray_t_max;
     L.sun_disk = (p.flags & 1u) != 0u;
+    L.area_nee = (p.flags & 2u) != 0u;
     return L;
+}
+
+// Area-light next-event estimation (no counterpart in the reference, whose
+// path tracer reaches emitters by BSDF sampling only). A triangle is chosen
+// with probability area * luminance / power, a point uniformly on it, and
+// the estimate is weighted against the cosine BSDF pdf by the power
+// heuristic (Veach 1997, ch. 9). Emitters count from both sides.
+struct AreaSample {
+    f3 dir;
+    float tmax;
+    f3 contrib;  // to be multiplied by the path throughput when visible
+    bool valid;
+};
+
+__device__ __forceinline__ AreaSample area_nee_sample(const SceneView& s, const Shading& sd, float usel, float u0,
+                                                      float u1) {
+    AreaSample r;
+    r.valid = false;
+    if (s.light_count == 0u) return r;
+    uint32_t lo = 0u, hi = s.light_count - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (usel < __ldg(s.lights + 4u * mid).w) hi = mid; else lo = mid + 1u;
+    }
+    const float4 a = __ldg(s.lights + 4u * lo), b = __ldg(s.lights + 4u * lo + 1u);
+    const float4 c = __ldg(s.lights + 4u * lo + 2u), e = __ldg(s.lights + 4u * lo + 3u);
+    const float su = sqrtf(u0);
+    const float wa = su * (1.0f - u1), wb = su * u1;
+    const f3 p = mk3((a.x + b.x * wa) + c.x * wb, (a.y + b.y * wa) + c.y * wb, (a.z + b.z * wa) + c.z * wb);
+    const f3 v = p - sd.origin_front;
+    const float d2 = dot3(v, v);
+    if (!(d2 > 0.0f)) return r;
+    const float dist = sqrtf(d2);
+    const f3 l = v * (1.0f / dist);
+    const float cx = dot3(sd.frame.n, l);
+    if (!(cx > 0.0f)) return r;
+    const f3 nl = normalize3(cross3(mk3(b.x, b.y, b.z), mk3(c.x, c.y, c.z)));
+    const float cl = fabsf(dot3(nl, l));
+    if (!(cl > 1e-6f)) return r;
+    const float pl = ((c.w / s.light_power) * d2) / cl;
+    const float pb = cx * kInvPi;
+    const float w = (pl * pl) / (pl * pl + pb * pb);
+    const f3 f = sd.diffuse * kInvPi;
+    r.contrib = (f * mk3(e.x, e.y, e.z)) * ((cx / pl) * w);
+    r.dir = l;
+    r.tmax = dist * 0.999f;
+    r.valid = true;
+    return r;
+}
+
+// Power-heuristic weight of emission reached by a cosine BSDF sample with
+// pdf pdf_bsdf, at distance t along dir, on a triangle with face normal fn.
+__device__ __forceinline__ float area_mis_weight(const SceneView& s, f3 emissive, f3 fn, f3 dir, float t,
+                                                 float pdf_bsdf) {
+    const float lum = (0.2126f * emissive.x + 0.7152f * emissive.y) + 0.0722f * emissive.z;
+    if (!(lum > 0.0f) || s.light_count == 0u) return 1.0f;
+    const float cl = fabsf(dot3(normalize3(fn), dir));
+    if (!(cl > 1e-6f)) return 0.0f;
+    const float pl = ((lum / s.light_power) * (t * t)) / cl;
+    return (pdf_bsdf * pdf_bsdf) / (pdf_bsdf * pdf_bsdf + pl * pl);
 }
 
 // get_sun_disk_luminance, scene.slang:408-465.

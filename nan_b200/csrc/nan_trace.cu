@@ -45,6 +45,9 @@ SceneView scene_view(const NanContext* ctx) {
     v.tri_count = ctx->tri_count;
     v.instance_count = ctx->scene.instance_count;
     v.status = ctx->d_status;
+    v.lights = reinterpret_cast<const float4*>(ctx->lights);
+    v.light_count = ctx->lights ? ctx->light_count : 0u;
+    v.light_power = ctx->light_power;
     return v;
 }
 
@@ -109,6 +112,7 @@ __global__ void __launch_bounds__(128) k_trace_screen(SceneView s, LightingRaw l
     float tmax = cam.far_clip * inv_cos;
     f3 o = mk3(cam.position[0], cam.position[1], cam.position[2]);
     f3 thp = mk3(1.0f, 1.0f, 1.0f), Lr = mk3(0.0f, 0.0f, 0.0f);
+    float prev_pdf = 1.0f;
     for (uint32_t vi = 0; vi < max_vertices; ++vi) {
         const HitInfo hit = closest(s, o, dir, tmin, tmax, tally);
         if (!hit.valid) {
@@ -119,13 +123,27 @@ __global__ void __launch_bounds__(128) k_trace_screen(SceneView s, LightingRaw l
         }
         const uint2 ref = __ldg(s.tri_refs + hit.flat);
         const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
-        Lr = Lr + thp * sd.emissive;
+        if (L.area_nee && vi > 0u)
+            Lr = Lr + thp * (sd.emissive * area_mis_weight(s, sd.emissive, sd.face_normal, dir, hit.t, prev_pdf));
+        else
+            Lr = Lr + thp * sd.emissive;
         const float u0 = rng.next_1d(), u1 = rng.next_1d();
         Lr = Lr + thp * sun_nee(s, L, sd, u0, u1, tally);
+        // light reached from vertex vi lies on vertex vi + 1: sampled only where
+        // that vertex exists, so both strategies cover the same path lengths
+        if (L.area_nee && vi + 1u < max_vertices) {
+            const float us = rng.next_1d(), a0 = rng.next_1d(), a1 = rng.next_1d();
+            const AreaSample as = area_nee_sample(s, sd, us, a0, a1);
+            if (as.valid) {
+                tally.shadow++;
+                if (!trace_any(s, sd.origin_front, as.dir, 0.0f, as.tmax)) Lr = Lr + thp * as.contrib;
+            }
+        }
         const float e0 = rng.next_1d(), e1 = rng.next_1d();
         float pdf;
         const f3 wo = cosine_sample_hemisphere(e0, e1, &pdf);
         pdf = maxf(pdf, 1e-6f);
+        prev_pdf = pdf;
         const f3 f = sd.diffuse * kInvPi;
         thp = thp * ((f * fabsf(wo.z)) / pdf);
         o = sd.origin_front;

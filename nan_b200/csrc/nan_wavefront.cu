@@ -34,7 +34,7 @@ constexpr uint32_t kBounceMask = 0xffu << kBounceShift;
 constexpr uint32_t kSampleShift = 12;
 
 constexpr uint32_t kKindNee = 0u;  // shadow contribution goes to rad
-constexpr uint32_t kKindSun = 1u;  // shadow contribution goes to si
+constexpr uint32_t kKindSun = 1u;  // shadow contribution goes to si (screen: the area-light term)
 
 struct WfState {
     uint32_t* unit;   // surface texel / probe index
@@ -74,13 +74,14 @@ __device__ __forceinline__ uint32_t queue_slot(uint32_t* count, bool want) {
     return base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
 }
 
+// tmax 0: the ray runs to the scene's t_max
 __device__ __forceinline__ void push_shadow(const WfQueues& q, int buf, uint32_t* count, uint32_t p, f3 o, f3 d,
-                                            f3 c, uint32_t kind) {
+                                            f3 c, uint32_t kind, float tmax = 0.0f) {
     const uint32_t slot = queue_slot(count, true);
     float4* e = q.shd[buf] + 3u * slot;
     e[0] = make_float4(o.x, o.y, o.z, __uint_as_float(p));
     e[1] = make_float4(d.x, d.y, d.z, __uint_as_float(kind));
-    e[2] = make_float4(c.x, c.y, c.z, 0.0f);
+    e[2] = make_float4(c.x, c.y, c.z, tmax);
 }
 
 __device__ __forceinline__ f3 xyz(float4 v) { return mk3(v.x, v.y, v.z); }
@@ -134,7 +135,7 @@ __global__ void __launch_bounds__(128) k_wf_shadow(SceneView s, const float4* __
         if (idx < count) {
             const float4 a = queue[3u * idx], b = queue[3u * idx + 1u], c = queue[3u * idx + 2u];
             tally.shadow++;
-            if (!trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, t_max)) {
+            if (!trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max)) {
                 const uint32_t p = __float_as_uint(a.w);
                 float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
                 const float4 v = target[p];
@@ -382,6 +383,7 @@ struct ScreenArgs {
     float4* out;
     uint32_t width, height, frame, max_vertices;
     int cached;
+    int area_nee;  // lighting flag bit 1 (the finalize stage has no lighting)
     CachedArgs cache;
 };
 
@@ -414,10 +416,20 @@ __global__ void __launch_bounds__(128) k_wf_screen_generate(SceneView s, Lightin
     st.rd[p] = f4(dir, cam.far_clip * inv_cos);
     st.thp[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     st.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    st.si[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    st.zpdf[p] = make_float2(0.0f, 1.0f);
     const uint32_t slot = queue_slot(q.ctl + 0, true);
     q.ext[0][slot] = p;
     RayTally none{0u, 0u};
     flush_tally(counters, none, 1u, 1u);
+}
+
+// The area-light term of the previous vertex (kept apart by the shadow stage)
+// joins the radiance after that vertex's sun term, as in the loop's order.
+__device__ __forceinline__ f3 fold_area_term(const WfState& st, uint32_t p, f3 rad) {
+    const float4 a = st.si[p];
+    st.si[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return rad + xyz(a);
 }
 
 __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
@@ -430,6 +442,7 @@ __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRa
         const float4 h = st.hit[p];
         const f3 d = xyz(st.rd[p]);
         f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
+        if (L.area_nee) rad = fold_area_term(st, p, rad);
         const uint32_t vertex = (flags & kBounceMask) >> kBounceShift;
         const uint32_t flat = __float_as_uint(h.x);
         if (flat == 0xffffffffu) {
@@ -444,7 +457,10 @@ __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRa
         rng.state = st.rng[p];
         const uint2 ref = __ldg(s.tri_refs + flat);
         const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
-        rad = rad + thp * sd.emissive;
+        if (L.area_nee && vertex > 0u)
+            rad = rad + thp * (sd.emissive * area_mis_weight(s, sd.emissive, sd.face_normal, d, h.y, st.zpdf[p].y));
+        else
+            rad = rad + thp * sd.emissive;
         const f3 f = sd.diffuse * kInvPi;
         if (a.cached && vertex == a.cache.vertex) {
             // the rest of the path is the cache's irradiance at this point;
@@ -484,10 +500,18 @@ __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRa
         const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
         const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
         push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
+        // light reached from this vertex lies on the next one: sampled only
+        // where that vertex exists, so both strategies cover the same paths
+        if (L.area_nee && vertex + 1u < a.max_vertices) {
+            const float us = rng.next_1d(), a0 = rng.next_1d(), a1 = rng.next_1d();
+            const AreaSample as = area_nee_sample(s, sd, us, a0, a1);
+            if (as.valid) push_shadow(q, buf, ctl + 2, p, sd.origin_front, as.dir, thp * as.contrib, kKindSun, as.tmax);
+        }
         const float e0 = rng.next_1d(), e1 = rng.next_1d();
         float pdf;
         const f3 wo = cosine_sample_hemisphere(e0, e1, &pdf);
         pdf = maxf(pdf, 1e-6f);
+        st.zpdf[p] = make_float2(0.0f, pdf);
         thp = thp * ((f * fabsf(wo.z)) / pdf);
         st.ro[p] = f4(sd.origin_front, 0.0f);
         st.rd[p] = f4(sd.frame.to_global(wo), L.t_max);
@@ -511,7 +535,11 @@ __global__ void __launch_bounds__(128) k_wf_screen_finalize(ScreenArgs a, WfStat
             q.ext[buf ^ 1][slot] = p;
             continue;
         }
-        const float4 r = st.rad[p];
+        float4 r = st.rad[p];
+        if (a.area_nee) {
+            const float4 t = st.si[p];
+            r = make_float4(r.x + t.x, r.y + t.y, r.z + t.z, r.w);
+        }
         a.out[st.unit[p]] = make_float4(r.x, r.y, r.z, 1.0f);
     }
 }
@@ -754,6 +782,9 @@ SceneView scene_view(const NanContext* ctx) {
     v.tri_count = ctx->tri_count;
     v.instance_count = ctx->scene.instance_count;
     v.status = ctx->d_status;
+    v.lights = reinterpret_cast<const float4*>(ctx->lights);
+    v.light_count = ctx->lights ? ctx->light_count : 0u;
+    v.light_power = ctx->light_power;
     return v;
 }
 
@@ -1089,6 +1120,7 @@ int screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32
     a.frame = frame;
     a.max_vertices = max_vertices;
     a.cached = cached != nullptr;
+    a.area_nee = (light->flags & 2u) != 0u;
     if (cached) a.cache = *cached;
     else memset(&a.cache, 0, sizeof(a.cache));
     const Grid g = grid_for(ctx);

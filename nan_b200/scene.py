@@ -73,6 +73,9 @@ class Lighting:
     ray_t_max: float = 1000.0
     sky_radiance: tuple = (0.0, 0.0, 0.0)
     sun_disk: bool = True
+    # screen tracer only, not in the reference: NEE toward the scene's emissive
+    # triangles with MIS (Scene.enable_area_lights builds the table)
+    area_nee: bool = False
 
     def __post_init__(self):
         d = np.asarray(self.sun_direction, dtype=np.float64)
@@ -81,7 +84,7 @@ class Lighting:
 
     @property
     def flags(self) -> int:
-        return 1 if self.sun_disk else 0
+        return (1 if self.sun_disk else 0) | (2 if self.area_nee else 0)
 
     def to_struct(self) -> NanLighting:
         s = NanLighting()
@@ -159,6 +162,57 @@ class Scene:
         and per-stage CUDA-event timing (read with context.read_kernel_times)."""
         self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width,
                                 kernel_timing)
+
+    def area_light_table(self):
+        """(f32[L, 16], power): every emissive triangle of the scene in world
+        space -- v0, inclusive cdf; v1 - v0, area; v2 - v0, luminance;
+        emission -- with selection weights area * luminance."""
+        node = self.scene_node
+        rows = []
+        for mesh_id, mat_id, transform_id in node.instances:
+            mat = node.materials[mat_id]
+            e = np.asarray(mat.emissive, dtype=np.float32)
+            lum = (np.float32(0.2126) * e[0] + np.float32(0.7152) * e[1]) + np.float32(0.0722) * e[2]
+            if not lum > 0:
+                continue
+            mesh = node.meshes[mesh_id]
+            m = node.transforms[transform_id].astype(np.float32)
+            p = (mesh.vertices[:, 0:3].astype(np.float32) @ m[:3, :3].T + m[:3, 3]).astype(np.float32)
+            tri = p[mesh.indices.astype(np.int64)]
+            e1 = (tri[:, 1] - tri[:, 0]).astype(np.float32)
+            e2 = (tri[:, 2] - tri[:, 0]).astype(np.float32)
+            area = (0.5 * np.linalg.norm(np.cross(e1.astype(np.float64), e2.astype(np.float64)), axis=1))
+            r = np.zeros((tri.shape[0], 16), np.float32)
+            r[:, 0:3], r[:, 4:7], r[:, 8:11] = tri[:, 0], e1, e2
+            r[:, 7] = area
+            r[:, 11] = lum
+            r[:, 12:15] = e
+            rows.append(r)
+        if not rows:
+            return np.zeros((0, 16), np.float32), 0.0
+        t = np.concatenate(rows)
+        w = t[:, 7].astype(np.float64) * t[:, 11].astype(np.float64)
+        power = float(np.float32(w.sum()))
+        cdf = np.cumsum(w) / w.sum()
+        cdf[-1] = 1.0
+        t[:, 3] = cdf.astype(np.float32)
+        return t, power
+
+    def enable_area_lights(self, enabled: bool = True) -> None:
+        """Screen tracer: NEE toward the emissive triangles with MIS (an option
+        beyond the reference, whose path tracer reaches emitters by BSDF
+        sampling only). Sets lighting.area_nee."""
+        import torch
+
+        if enabled:
+            table, power = self.area_light_table()
+            self._area_lights = torch.from_numpy(table).to(self.device.torch_device)
+            self._area_power = power
+            check(lib().nan_ctx_set_area_lights(self.context.handle, ptr(self._area_lights), table.shape[0],
+                                                ctypes.c_float(power)))
+        else:
+            check(lib().nan_ctx_set_area_lights(self.context.handle, None, 0, ctypes.c_float(0.0)))
+        self.lighting.area_nee = bool(enabled)
 
     def trace_points(self, points, iteration: int, samples: int = 1, max_bounces: int = 3, out=None, stream=None,
                      indirect_only: bool = False):

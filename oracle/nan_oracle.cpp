@@ -420,6 +420,8 @@ struct Scene {
     std::vector<double> world_d;  // [T][9] double world triangles
     std::vector<BvhNode> nodes;
     std::vector<uint32_t> prim_order;
+    std::vector<float> lights;  // area lights f32[L][16] (oracle_scene_set_area_lights)
+    float light_power = 0.0f;
     float pad = 0.0f;
     uint32_t tri_count() const { return (uint32_t)flat_instance.size(); }
 };
@@ -859,7 +861,7 @@ template <class T> V3<T> world_flat_normal(const Scene& s, uint32_t inst, uint32
 template <class T> struct LightCtx {
     V3<T> sun_dir, outer, trans, illum, sky;
     T cos_half, t_max;
-    bool sun_disk;
+    bool sun_disk, area_nee;
     explicit LightCtx(const OracleLighting& p) {
         sun_dir = mk<T>(T(p.sun_direction[0]), T(p.sun_direction[1]), T(p.sun_direction[2]));
         V3<T> color = mk<T>(T(p.sun_color[0]), T(p.sun_color[1]), T(p.sun_color[2]));
@@ -870,6 +872,7 @@ template <class T> struct LightCtx {
         cos_half = T(p.sun_cos_half_angle);
         t_max = T(p.ray_t_max);
         sun_disk = (p.flags & 1u) != 0;
+        area_nee = (p.flags & 2u) != 0;
     }
 };
 
@@ -897,6 +900,49 @@ template <class T> struct Tracer {
         T ndl = vmax(T(0), dot(sd.shading_frame.n, l));
         V3<T> f = sd.diffuse * Consts<T>::INV_PI;
         return ((vis * f) * L.illum) * ndl;
+    }
+    // Area-light NEE of the screen tracer (an option beyond the reference):
+    // triangle by area * luminance, uniform point, power-heuristic MIS weight
+    // against the cosine BSDF pdf; emitters count from both sides.
+    V3<T> area_nee(const Shading<T>& sd, T usel, T u0, T u1) {
+        const size_t n = s.lights.size() / 16;
+        if (n == 0) return mk<T>(0, 0, 0);
+        size_t lo = 0, hi = n - 1;
+        while (lo < hi) {
+            size_t mid = (lo + hi) >> 1;
+            if (usel < T(s.lights[16 * mid + 3])) hi = mid; else lo = mid + 1;
+        }
+        const float* r = &s.lights[16 * lo];
+        T su = Ops<T>::sqrt(u0);
+        T wa = su * (T(1) - u1), wb = su * u1;
+        V3<T> p = mk<T>((T(r[0]) + T(r[4]) * wa) + T(r[8]) * wb, (T(r[1]) + T(r[5]) * wa) + T(r[9]) * wb,
+                        (T(r[2]) + T(r[6]) * wa) + T(r[10]) * wb);
+        V3<T> v = p - sd.origin_front;
+        T d2 = dot(v, v);
+        if (!(d2 > T(0))) return mk<T>(0, 0, 0);
+        T dist = Ops<T>::sqrt(d2);
+        V3<T> l = v * (T(1) / dist);
+        T cx = dot(sd.shading_frame.n, l);
+        if (!(cx > T(0))) return mk<T>(0, 0, 0);
+        V3<T> nl = normalize(cross(mk<T>(T(r[4]), T(r[5]), T(r[6])), mk<T>(T(r[8]), T(r[9]), T(r[10]))));
+        T cl = std::fabs(dot(nl, l));
+        if (!(cl > T(1e-6f))) return mk<T>(0, 0, 0);
+        T pl = ((T(r[11]) / T(s.light_power)) * d2) / cl;
+        T pb = cx * Consts<T>::INV_PI;
+        T w = (pl * pl) / (pl * pl + pb * pb);
+        V3<T> f = sd.diffuse * Consts<T>::INV_PI;
+        V3<T> c = (f * mk<T>(T(r[12]), T(r[13]), T(r[14]))) * ((cx / pl) * w);
+        cnt.shadow_rays++;
+        RayPre<T> ray = make_ray<T>(sd.origin_front, l, T(0), dist * T(0.999f));
+        return trace<T>(s, ray, true, use_bvh, &cnt).valid ? mk<T>(0, 0, 0) : c;
+    }
+    T area_mis_weight(V3<T> emissive, V3<T> fn, V3<T> dir, T t, T pdf_bsdf) {
+        T lum = (T(0.2126f) * emissive.x + T(0.7152f) * emissive.y) + T(0.0722f) * emissive.z;
+        if (!(lum > T(0)) || s.lights.empty()) return T(1);
+        T cl = std::fabs(dot(normalize(fn), dir));
+        if (!(cl > T(1e-6f))) return T(0);
+        T pl = ((lum / T(s.light_power)) * (t * t)) / cl;
+        return (pdf_bsdf * pdf_bsdf) / (pdf_bsdf * pdf_bsdf + pl * pl);
     }
     // scene.slang:940-952
     V3<T> sun_irradiance(const Shading<T>& sd, T ux, T uy) {
@@ -955,6 +1001,7 @@ void screen_pixel(Tracer<T>& tr, const OracleLighting& lp, const OracleCamera& c
     T tmax = T(cam.far_clip) * inv_cos;
     V3<T> o = load3<T>(cam.position);
     V3<T> thp = mk<T>(1, 1, 1), Lr = mk<T>(0, 0, 0);
+    T prev_pdf = T(1);
     (void)lp;
     for (uint32_t vi = 0; vi < max_vertices; ++vi) {
         HitRec hit = tr.closest(o, dir, tmin, tmax);
@@ -966,15 +1013,26 @@ void screen_pixel(Tracer<T>& tr, const OracleLighting& lp, const OracleCamera& c
         }
         uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
         Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(hit.b1), T(hit.b2), -dir);
-        Lr = Lr + thp * sd.emissive;
+        if (tr.L.area_nee && vi > 0)
+            Lr = Lr + thp * (sd.emissive * tr.area_mis_weight(sd.emissive, sd.face_normal, dir, T(hit.t), prev_pdf));
+        else
+            Lr = Lr + thp * sd.emissive;
         T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
         V3<T> nee = tr.sun_nee(sd, u0, u1);
         Lr = Lr + thp * nee;
+        // light reached from vertex vi lies on vertex vi + 1: sampled only where
+        // that vertex exists, so both strategies cover the same path lengths
+        if (tr.L.area_nee && vi + 1 < max_vertices) {
+            T us = T(rng.next_1d()), a0 = T(rng.next_1d()), a1 = T(rng.next_1d());
+            V3<T> an = tr.area_nee(sd, us, a0, a1);
+            Lr = Lr + thp * an;
+        }
         T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
         V3<T> wo;
         T pdf;
         cosine_sample_hemisphere<T>(e0, e1, &wo, &pdf);
         pdf = vmax(pdf, T(1e-6f));
+        prev_pdf = pdf;
         V3<T> f = sd.diffuse * Consts<T>::INV_PI;
         thp = thp * ((f * std::fabs(wo.z)) / pdf);
         o = sd.origin_front;
@@ -1482,6 +1540,12 @@ int oracle_trace_texels(void* sp, const OracleLighting* lighting, uint8_t* slots
     for (auto& c : unit_counts) add_counts(counts, c);
     if (bad) { g_error = "texel index out of range"; return 1; }
     return 0;
+}
+
+void oracle_scene_set_area_lights(void* sp, const float* lights, int count, float power) {
+    Scene* s = static_cast<Scene*>(sp);
+    s->lights.assign(lights, lights + 16 * (size_t)std::max(count, 0));
+    s->light_power = power;
 }
 
 int oracle_trace_points(void* sp, const OracleLighting* lighting, const float* points, int count,

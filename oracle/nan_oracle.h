@@ -130,6 +130,10 @@ int oracle_trace_texels(void* scene, const OracleLighting* lighting,
                         uint32_t max_bounces, int reset, int precision,
                         int threads, OracleRayCounts* counts);
 
+/* Area-light table of the screen tracer's NEE option (lighting flag bit 1),
+ * the layout of nan_ctx_set_area_lights. */
+void oracle_scene_set_area_lights(void* scene, const float* lights, int count, float power);
+
 /* Irradiance at surface points: the texel estimator
  * (estimate_surface_irradiance, texture_space_path_tracer.slang:86-117) at
  * points f32[N][4] = (b1, b2, instance bits, primitive bits | back << 31),

@@ -108,6 +108,7 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, vp, u32, vp, i,
                                       u32, u32, u32, i, i, i, vp]
+    l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
     l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
 
 
@@ -305,6 +306,11 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
         return counts.as_dict()
+
+    def set_area_lights(self, lights, power):
+        """Area-light table f32[L, 16] and total power (nan_ctx_set_area_lights layout)."""
+        self._lights = np.ascontiguousarray(lights, dtype=np.float32).reshape(-1, 16)
+        lib().oracle_scene_set_area_lights(self.handle, _p(self._lights), self._lights.shape[0], float(power))
 
     def trace_points(self, lighting, points, iteration, samples, max_bounces, flags=0, precision=F32, threads=0):
         """Irradiance at surface points f32[N, 4] (b1, b2, instance bits,
