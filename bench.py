@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache time-to-RMSE measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batched probe measurement")
+    ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box (area light) measurement")
+    ap.add_argument("--no-city", action="store_true", help="skip the 4M-triangle city frame measurement")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
 
@@ -426,6 +428,12 @@ def run_nan(args):
         line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
     if world == 1 and not args.no_learned:
         line["learned_cache"] = learned_cache_line(device)
+    if world == 1 and not args.no_cornell:
+        line["cornell_area_light"] = cornell_line(device)
+    if world == 1 and not args.no_city:
+        from nan_b200 import city_eval
+
+        line["city_frame"] = city_eval.measure(device, frames=2)
     if world == 1 and not args.no_batched:
         from nan_b200 import batch_eval
 
@@ -435,6 +443,52 @@ def run_nan(args):
                                                "sites U{512..20480} (area-weighted random), 64 spp, 3 bounces, "
                                                "compensated running means")
     print(json.dumps(line))
+
+
+def cornell_line(device) -> dict:
+    """The 36-triangle Cornell box at 256x256, 16 frames of 1 spp, 3 bounces
+    (4 path vertices): the reference's BSDF-only path tracer against the
+    area-light NEE + MIS option, each scored by relative RMSE against 4096
+    BSDF-only frames accumulated in float64."""
+    import torch
+
+    import nan_b200
+    from nan_b200 import scenes
+
+    node = scenes.cornell_box(256, 256)
+    scene = nan_b200.Scene(device, node)
+    scene.enable_area_lights()
+    tracer = nan_b200.PathTracer(device, scene, max_vertices=4)
+    w = h = 256
+    out = torch.zeros((h, w, 4), dtype=torch.float32, device=device.torch_device)
+    stream = torch.cuda.current_stream()
+
+    def run(area, frames, base, timed=False):
+        scene.lighting.area_nee = area
+        acc = torch.zeros((h, w, 3), dtype=torch.float64, device=device.torch_device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = 0.0
+        for f in range(frames):
+            node.camera.begin_frame(w, h)
+            e0.record(stream)
+            tracer.execute(stream, out, base + f)
+            e1.record(stream)
+            acc += out[..., :3].double()
+            if timed:
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+        return acc / frames, ms
+
+    ref, _ = run(False, 4096, 1_000_000)
+    res = {"scene": "Cornell box, 36 triangles, light quad emission (17, 12, 4)", "image": "256x256",
+           "frames": 16, "max_vertices": 4, "reference_frames": 4096}
+    for name, area in (("bsdf_only", False), ("area_nee_mis", True)):
+        run(area, 4, 50_000)  # warm-up
+        img, ms = run(area, 16, 0, timed=True)
+        rmse = float(torch.sqrt(torch.mean((img - ref) ** 2)) / torch.sqrt(torch.mean(ref ** 2)))
+        res[name] = {"ms_per_frame": ms / 16, "relative_rmse": rmse}
+    scene.lighting.area_nee = False
+    return res
 
 
 def learned_cache_line(device) -> dict:

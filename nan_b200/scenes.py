@@ -14,6 +14,9 @@ distributions of the workload it stands for.
   noise) plus 500 boxes with sides U[0.2, 3] and random yaw; albedo
   U[0.1, 0.9]; sun at 45 deg elevation with irradiance 3, sky 0.5. The
   default 313x313 grid gives 194,688 + 6,000 = 200,688 triangles.
+* ``city()``             -- 20k boxes (one tessellated box mesh, instanced)
+  with heights log-normal (mu 2, sigma 0.7) on a 2 km grid plus a
+  tessellated ground plane: about 4.16 M triangles; sun at 30 deg and sky.
 * ``batch_scenes()``     -- many terrain_boxes scenes with triangle counts
   log-uniform in [1e3, 5e5] and a site count U{512..20480} each (the
   multi-scene probe workload).
@@ -166,6 +169,73 @@ def terrain_boxes(seed: int = 1, grid: int = 313, cell: float = 0.15, boxes: int
     s.camera = _camera((0.0, amplitude + 0.25 * extent, 0.6 * extent), (0.0, 0.0, 0.0), 60.0)
     s.lighting = Lighting.sun_elevation(45.0, azimuth_deg=30.0, irradiance=3.0, sky=0.5)
     s.terrain_cell = cell
+    return s
+
+
+def tessellated_box(n: int) -> Mesh:
+    """Unit box (centred, outward faces) with every face split into n x n
+    quads: 12 n^2 triangles."""
+    faces = [((0, -1, 0), (0, 0, 1), (1, 0, 0)), ((0, 1, 0), (1, 0, 0), (0, 0, 1)),
+             ((0, 0, -1), (1, 0, 0), (0, 1, 0)), ((0, 0, 1), (0, 1, 0), (1, 0, 0)),
+             ((-1, 0, 0), (0, 1, 0), (0, 0, 1)), ((1, 0, 0), (0, 0, 1), (0, 1, 0))]
+    verts, tris = [], []
+    t = np.linspace(-0.5, 0.5, n + 1)
+    for nrm, u, w in faces:
+        nrm, u, w = np.array(nrm, float), np.array(u, float), np.array(w, float)
+        base = sum(len(v) for v in verts)
+        su, sw = np.meshgrid(t, t, indexing="xy")
+        p = 0.5 * nrm + su.reshape(-1, 1) * u + sw.reshape(-1, 1) * w
+        v = np.zeros((p.shape[0], 8), np.float32)
+        v[:, 0:3] = p
+        v[:, 3:6] = nrm
+        v[:, 6] = su.reshape(-1) + 0.5
+        v[:, 7] = sw.reshape(-1) + 0.5
+        verts.append(v)
+        i = np.arange(n)
+        a = (i[:, None] * (n + 1) + i[None, :]).reshape(-1) + base
+        b, c, d = a + 1, a + n + 1, a + n + 2
+        q = np.concatenate([np.stack([a, b, d], 1), np.stack([a, d, c], 1)])
+        # wind so that cross(p1 - p0, p2 - p0) points along the face normal
+        allv = np.concatenate(verts)
+        p0, p1, p2 = allv[q[0, 0] - 0, :3], allv[q[0, 1], :3], allv[q[0, 2], :3]
+        if np.dot(np.cross(p1 - p0, p2 - p0), nrm) < 0:
+            q = q[:, [0, 2, 1]]
+        tris.append(q)
+    return Mesh(np.concatenate(verts), np.concatenate(tris).astype(np.uint32))
+
+
+def city(seed: int = 1, boxes: int = 20000, extent: float = 2000.0, box_tessellation: int = 4,
+         ground_cells: int = 400, width: int = 3840, height: int = 2160) -> SceneNode:
+    """Seeded synthetic city: `boxes` buildings on a square grid of lots over
+    extent x extent metres, footprints U[6, 12] m with random yaw, heights
+    log-normal (mu 2, sigma 0.7) m, albedo U[0.2, 0.8] grey-tinted; one
+    tessellated box mesh (12 n^2 triangles) instanced for all of them, and a
+    ground plane of 2 x ground_cells^2 triangles."""
+    rng = np.random.default_rng(seed)
+    s = SceneNode(name=f"city_{boxes}_seed{seed}")
+    cell = extent / ground_cells
+    ground = s.add_mesh(grid_mesh(np.zeros((ground_cells + 1, ground_cells + 1)), cell))
+    s.add_instance(ground, s.add_material(Material((0.35, 0.35, 0.33))), s.add_transform(np.eye(4, dtype=np.float32)))
+    box = s.add_mesh(tessellated_box(box_tessellation))
+    lots = int(math.ceil(math.sqrt(boxes)))
+    spacing = extent / lots
+    palette = [s.add_material(Material(tuple(float(x) for x in rng.uniform(0.2, 0.8) * rng.uniform(0.9, 1.1, 3))))
+               for _ in range(64)]
+    k = 0
+    for iz in range(lots):
+        for ix in range(lots):
+            if k >= boxes:
+                break
+            fx, fz = rng.uniform(6.0, 12.0, 2)
+            hgt = float(np.exp(rng.normal(2.0, 0.7)))
+            x = -0.5 * extent + (ix + 0.5) * spacing + rng.uniform(-0.15, 0.15) * spacing
+            z = -0.5 * extent + (iz + 0.5) * spacing + rng.uniform(-0.15, 0.15) * spacing
+            yaw = rng.uniform(0.0, 2.0 * math.pi)
+            s.add_instance(box, palette[int(rng.integers(0, len(palette)))],
+                           s.add_transform(make_transform((x, 0.5 * hgt, z), (0.0, yaw, 0.0), (fx, hgt, fz))))
+            k += 1
+    s.camera = _camera((0.0, 180.0, 0.55 * extent), (0.0, 0.0, 0.1 * extent), 55.0, width, height)
+    s.lighting = Lighting.sun_elevation(30.0, azimuth_deg=40.0, irradiance=3.0, sky=0.5)
     return s
 
 
