@@ -294,10 +294,10 @@ typedef struct NanProbeSet {
 } NanProbeSet;
 
 typedef struct NanBatchTuning {
-    uint32_t stack_depth;     /* traversal stack entries: 32, 48, 64 or 96 (>= every BVH's need) */
-    uint32_t blocks_per_sm;   /* persistent 128-thread blocks per SM */
-    uint32_t units_per_grab;  /* probes per lane taken from the work counter at once */
-    uint32_t reserved;
+    uint32_t stack_depth;        /* traversal stack entries: 48 or 96 (>= every BVH's need) */
+    uint32_t blocks_per_sm;      /* persistent 128-thread blocks per SM */
+    uint32_t units_per_grab;     /* probes per lane taken from the work counter at once */
+    uint32_t min_blocks_per_sm;  /* register cap of the kernel variant: 0 (compiler's), 4 or 6 */
 } NanBatchTuning;
 
 NAN_B200_API int nan_batch_create(NanContext* ctx, const NanProbeSet* sets, uint32_t set_count,
@@ -307,6 +307,15 @@ NAN_B200_API int nan_batch_destroy(NanBatch* batch);
 NAN_B200_API int nan_batch_info(NanBatch* batch, uint32_t* min_stack_depth, uint32_t* total_probes,
                                 NanBatchTuning* tuning);
 NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tuning);
+/* How a probe's samples draw random numbers. SEQUENTIAL (the default): one
+ * stream per probe, samples in sequence, as the reference's baker
+ * (surface_probe_path_tracer.slang:206-278) -- bit-exact with
+ * nan_trace_probes. INDEPENDENT: sample k draws from RNG(probe, instance,
+ * iteration * samples + k), so a warp traces 32 samples of one probe at once;
+ * the per-probe sums are still formed in sample order. Resets the launch
+ * shape to the new kernel's defaults. */
+enum { NAN_BATCH_SEQUENTIAL_SAMPLES = 0, NAN_BATCH_INDEPENDENT_SAMPLES = 1 };
+NAN_B200_API int nan_batch_set_mode(NanBatch* batch, uint32_t mode);
 /* One iteration of every set (nan_trace_probes semantics per set). */
 NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,
                                         uint32_t max_bounces, int reset, void* stream);

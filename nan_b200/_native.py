@@ -183,7 +183,7 @@ class NanBatchTuning(ctypes.Structure):
         ("stack_depth", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_uint32),
         ("units_per_grab", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("min_blocks_per_sm", ctypes.c_uint32),
     ]
 
 
@@ -245,6 +245,7 @@ EXPORTS = {
     "nan_batch_destroy": (_I, [_VP]),
     "nan_batch_info": (_I, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32), ctypes.POINTER(NanBatchTuning)]),
     "nan_batch_set_tuning": (_I, [_VP, ctypes.POINTER(NanBatchTuning)]),
+    "nan_batch_set_mode": (_I, [_VP, _U32]),
     "nan_batch_trace_probes": (_I, [_VP, _U32, _U32, _U32, _I, _VP]),
     "nan_batch_autotune": (_I, [_VP, _U32, _U32, _VP, ctypes.POINTER(NanBatchTuning), ctypes.POINTER(ctypes.c_float)]),
     "nan_batch_capture": (_I, [_VP, _U32, _I, _U32, _U32, _VP]),

@@ -2,7 +2,10 @@
 and replayed from a CUDA graph) against one baker dispatch per scene.
 
 Every frame bakes every site of every scene (samples_per_probe cosine
-samples, max_bounces bounces, compensated running means). Frames are timed
+samples, max_bounces bounces, compensated running means). The batched
+launch runs in both sample modes: one RNG stream per probe (the reference's,
+bit-exact with the per-scene baker) and one stream per sample (a warp per
+probe). Frames are timed
 with CUDA events on the launching stream after one warm-up frame; rays are
 counted on the device.
 """
@@ -88,16 +91,28 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     batch_rays = (c["extend_rays"] + c["shadow_rays"]) / (frames + 1)
     batch.capture(0, True, samples_per_probe, max_bounces)
     graph_ms = timed(lambda f: batch.replay(1, stream))
+    batch.close()
+    # one RNG stream per sample: a warp traces 32 samples of one probe at once
+    ind = ProbeBatch(device, [(b, f, a) for _, b, f, a in items], independent_samples=True)
+    tuned_ind = ind.autotune(samples_per_probe, max_bounces)
+    ind.capture(0, True, samples_per_probe, max_bounces)
+    ind.context.read_counters(reset=True)
+    ind_ms = timed(lambda f: ind.replay(1, stream))
+    c = ind.context.read_counters(reset=True)
+    ind_rays = (c["extend_rays"] + c["shadow_rays"]) / (frames + 1)
+    ind.close()
     device.check()
     return {
         "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
         "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
         "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
-        "setup_s": setup_s, "autotune": tuned,
+        "setup_s": setup_s, "autotune": tuned, "autotune_independent_samples": tuned_ind,
         "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
-                         "batched": batch_ms, "batched_graph": graph_ms},
+                         "batched": batch_ms, "batched_graph": graph_ms,
+                         "batched_graph_independent_samples": ind_ms},
         "rays_per_frame": batch_rays, "per_scene_rays_per_frame": per_scene_rays,
         "mrays_per_s": {"per_scene_wavefront": per_scene_rays / (per_scene_ms * 1e3),
                         "per_scene_megakernel": per_scene_rays / (per_scene_mk_ms * 1e3),
-                        "batched": batch_rays / (batch_ms * 1e3), "batched_graph": batch_rays / (graph_ms * 1e3)},
+                        "batched": batch_rays / (batch_ms * 1e3), "batched_graph": batch_rays / (graph_ms * 1e3),
+                        "batched_graph_independent_samples": ind_rays / (ind_ms * 1e3)},
     }

@@ -1,7 +1,8 @@
 """One frame of the large workload on the seeded 4.16 M-triangle city
 (scenes.city): the screen at 3840x2160 with 4 spp and 5 path vertices (the
 learned-cache path tracer, and the plain one for comparison), a 20,480-site
-surface-probe pass (64 spp, 3 bounces, compensated sums, batched launch) and
+surface-probe pass (64 spp, 3 bounces, compensated sums, batched launch with
+one RNG stream per sample) and
 a Mesh Colors texel pass over the whole city (about 12.6 M texels, 1 sample,
 3 bounces). Every pass is timed with CUDA events on the launching stream
 after one warm-up frame; rays are counted on the device.
@@ -87,7 +88,7 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
                                                compensated=True)
     rt = SurfaceProbeRuntimeBuffers.acquire(rd, geometry.probe_count)
-    batch = ProbeBatch(device, [(baker, rt.field, rt.attachments)])
+    batch = ProbeBatch(device, [(baker, rt.field, rt.attachments)], independent_samples=True)
     tuned = batch.autotune(64, 3)
     res["probes"] = timed(lambda f: batch.execute(stream, f, 64, 3, reset=(f == 0)), batch.context)
     res["probes"]["autotune"] = tuned

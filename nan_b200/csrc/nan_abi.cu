@@ -510,6 +510,11 @@ NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tun
     return nan_host::batch_set_tuning(batch, tuning);
 }
 
+NAN_B200_API int nan_batch_set_mode(NanBatch* batch, uint32_t mode) {
+    if (!batch) return invalid("null batch");
+    return nan_host::batch_set_mode(batch, mode);
+}
+
 NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,
                                         uint32_t max_bounces, int reset, void* stream) {
     if (!batch) return invalid("null batch");

@@ -41,8 +41,10 @@ struct BatchCtl {
     uint32_t pad;
 };
 
-template <int kDepth>
-__global__ void __launch_bounds__(128) k_batch_probes(const BatchSet* __restrict__ sets,
+// kMinBlocks: the launch-bounds occupancy target that caps registers
+// (0: the compiler's choice), one of the autotuned dimensions.
+template <int kDepth, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) k_batch_probes(const BatchSet* __restrict__ sets,
                                                       const uint32_t* __restrict__ prefix, uint32_t set_count,
                                                       uint32_t total, BatchCtl* ctl, uint32_t spp,
                                                       uint32_t max_bounces, uint32_t grab,
@@ -76,6 +78,76 @@ __global__ void __launch_bounds__(128) k_batch_probes(const BatchSet* __restrict
     flush_tally(counters, tally, units, units * max(spp, 1u));
 }
 
+// Independent-sample mode: sample k of probe p draws from its own stream
+// RNG(p, instance, iteration * n + k), so one warp traces 32 samples of one
+// probe at once. Lane 0 then folds them in sample order, forming every sum
+// exactly as the sequential loop does with those per-sample values.
+template <int kDepth, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks) k_batch_probes_ws(const BatchSet* __restrict__ sets,
+                                                         const uint32_t* __restrict__ prefix, uint32_t set_count,
+                                                         uint32_t total, BatchCtl* ctl, uint32_t spp,
+                                                         uint32_t max_bounces, uint32_t grab,
+                                                         unsigned long long* counters) {
+    (void)grab;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t iteration = ctl->iteration;
+    const int reset = (int)ctl->reset;
+    const uint32_t n = max(spp, 1u);
+    RayTally tally{0u, 0u};
+    uint32_t units = 0u;
+    for (;;) {
+        uint32_t u = 0u;
+        if (lane == 0u) u = atomicAdd(&ctl->next, 1u);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= total) break;
+        uint32_t lo = 0u, hi = set_count - 1u;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (__ldg(prefix + mid) <= u) lo = mid; else hi = mid - 1u;
+        }
+        const BatchSet& b = sets[lo];
+        const uint32_t p = u - __ldg(prefix + lo);
+        const LightParams L = make_light(b.light);
+        ProbeSite site;
+        if (!probe_site(b.s, b.probes, b.pinst, b.probe_instance_count, p, &site)) continue;
+        const uint32_t prev_iter = reset ? 0u : b.out.counts[p];
+        if (reset && lane < 16u) b.out.radial[16u * p + lane] = 0u;
+        __syncwarp();
+        ProbeAcc acc;
+        probe_acc_init(acc);
+        for (uint32_t k0 = 0; k0 < n; k0 += 32u) {
+            const uint32_t k = k0 + lane;
+            ProbeSample smp;
+            smp.si = mk3(0.0f, 0.0f, 0.0f);
+            smp.self_hits = 0u;
+            smp.texel = 0u;
+            smp.nd = 0.0f;
+            smp.has_path = false;
+            if (k < n) {
+                Rng rng(p, site.inst, iteration * n + k);
+                smp = probe_sample<BinaryTracer<kDepth>>(b.s, L, site, rng, max_bounces, tally);
+            }
+            const uint32_t cnt = min(32u, n - k0);
+            for (uint32_t j = 0; j < cnt; ++j) {
+                ProbeSample q;
+                q.si = mk3(__shfl_sync(0xffffffffu, smp.si.x, j), __shfl_sync(0xffffffffu, smp.si.y, j),
+                           __shfl_sync(0xffffffffu, smp.si.z, j));
+                q.self_hits = __shfl_sync(0xffffffffu, smp.self_hits, j);
+                q.texel = __shfl_sync(0xffffffffu, smp.texel, j);
+                q.nd = __shfl_sync(0xffffffffu, smp.nd, j);
+                q.has_path = __shfl_sync(0xffffffffu, (int)smp.has_path, j) != 0;
+                if (lane == 0u) probe_fold(acc, b.out, p, q, prev_iter, spp);
+            }
+        }
+        if (lane == 0u) {
+            probe_store(b.out, p, acc, n, reset);
+            units++;
+        }
+        __syncwarp();
+    }
+    flush_tally(counters, tally, units, units * n);
+}
+
 __global__ void k_batch_begin(BatchCtl* ctl, uint32_t iteration, uint32_t reset) {
     ctl->next = 0u;
     ctl->iteration = iteration;
@@ -89,15 +161,26 @@ __global__ void k_batch_advance(BatchCtl* ctl) {
     ctl->reset = 0u;
 }
 
-constexpr uint32_t kDepths[] = {32u, 48u, 64u, 96u};
+constexpr uint32_t kDepths[] = {48u, 96u};
+constexpr uint32_t kRegCaps[] = {0u, 4u, 6u};
 
-const void* kernel_for(uint32_t depth) {
-    switch (depth) {
-        case 32: return reinterpret_cast<const void*>(k_batch_probes<32>);
-        case 48: return reinterpret_cast<const void*>(k_batch_probes<48>);
-        case 64: return reinterpret_cast<const void*>(k_batch_probes<64>);
-        default: return reinterpret_cast<const void*>(k_batch_probes<96>);
+template <int kDepth, int kMinBlocks>
+const void* pick(uint32_t mode) {
+    return mode == NAN_BATCH_INDEPENDENT_SAMPLES ? reinterpret_cast<const void*>(k_batch_probes_ws<kDepth, kMinBlocks>)
+                                                 : reinterpret_cast<const void*>(k_batch_probes<kDepth, kMinBlocks>);
+}
+
+template <int kDepth>
+const void* pick_caps(uint32_t mode, uint32_t cap) {
+    switch (cap) {
+        case 4: return pick<kDepth, 4>(mode);
+        case 6: return pick<kDepth, 6>(mode);
+        default: return pick<kDepth, 0>(mode);
     }
+}
+
+const void* kernel_for(uint32_t depth, uint32_t mode, uint32_t cap) {
+    return depth <= 48u ? pick_caps<48>(mode, cap) : pick_caps<96>(mode, cap);
 }
 
 }  // namespace
@@ -155,7 +238,8 @@ int launch_frame_kernel(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStr
     const uint32_t* prefix = m->prefix;
     unsigned long long* counters = b->ctx->d_counters;
     void* args[] = {(void*)&sets, (void*)&prefix, &sc, &total, &ctl, &spp, &max_bounces, &grab, &counters};
-    cudaError_t err = cudaLaunchKernel(kernel_for(t.stack_depth), dim3(grid), dim3(128), args, 0, st);
+    cudaError_t err = cudaLaunchKernel(kernel_for(t.stack_depth, b->mode, t.min_blocks_per_sm), dim3(grid), dim3(128),
+                                       args, 0, st);
     b->ctx->launches++;
     return cuda_fail(err, "batched probe launch");
 }
@@ -197,12 +281,7 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
     BatchImpl* m = b->impl;
     m->set_count = count;
     m->total = prefix[count];
-    m->min_depth = 96u;
-    for (uint32_t d : kDepths)
-        if (d >= max_depth + 2u) {
-            m->min_depth = d;
-            break;
-        }
+    m->min_depth = max_depth + 2u <= 48u ? 48u : 96u;
     if (max_depth + 2u > 96u) {
         delete m;
         delete b;
@@ -210,8 +289,9 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
         return NAN_ERR_LIMIT;
     }
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_probes<96>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch_probes<96, 0>, 128, 0);
     b->tuning.stack_depth = 96u;
+    b->tuning.min_blocks_per_sm = 0u;
     b->tuning.blocks_per_sm = (uint32_t)std::max(occ, 1);
     b->tuning.units_per_grab = 1u;
     cudaError_t err = cudaMalloc(&m->sets, sizeof(BatchSet) * std::max(count, 1u));
@@ -245,11 +325,32 @@ void batch_destroy(NanBatch* b) {
 }
 
 uint32_t batch_min_depth(const NanBatch* b) { return b->impl->min_depth; }
+
+int batch_set_mode(NanBatch* b, uint32_t mode) {
+    if (mode != NAN_BATCH_SEQUENTIAL_SAMPLES && mode != NAN_BATCH_INDEPENDENT_SAMPLES) {
+        set_error("mode must be NAN_BATCH_SEQUENTIAL_SAMPLES or NAN_BATCH_INDEPENDENT_SAMPLES");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    if (mode != b->mode) {
+        b->mode = mode;
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &occ, kernel_for(b->tuning.stack_depth, mode, b->tuning.min_blocks_per_sm), 128, 0);
+        b->tuning.blocks_per_sm = (uint32_t)std::max(occ, 1);
+        b->tuning.units_per_grab = 1u;
+        drop_graph(b->impl);
+    }
+    return NAN_OK;
+}
 uint32_t batch_total(const NanBatch* b) { return b->impl->total; }
 
 int batch_set_tuning(NanBatch* b, const NanBatchTuning* t) {
-    if (t->stack_depth != 32 && t->stack_depth != 48 && t->stack_depth != 64 && t->stack_depth != 96) {
-        set_error("stack_depth must be 32, 48, 64 or 96");
+    if (t->stack_depth != 48 && t->stack_depth != 96) {
+        set_error("stack_depth must be 48 or 96");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    if (t->min_blocks_per_sm != 0 && t->min_blocks_per_sm != 4 && t->min_blocks_per_sm != 6) {
+        set_error("min_blocks_per_sm must be 0, 4 or 6");
         return NAN_ERR_INVALID_ARGUMENT;
     }
     if (t->stack_depth < b->impl->min_depth) {
@@ -332,34 +433,39 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
     for (uint32_t depth : kDepths) {
         if (rc) break;
         if (depth < m->min_depth) continue;
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_for(depth), 128, 0);
-        occ = std::max(occ, 1);
-        const uint32_t blocks[] = {(uint32_t)std::max(occ / 4, 1), (uint32_t)std::max(occ / 2, 1), (uint32_t)occ};
-        for (uint32_t bps : blocks) {
-            for (uint32_t grab : {1u, 4u}) {
-                NanBatchTuning t = b->tuning;
-                t.stack_depth = depth;
-                t.blocks_per_sm = bps;
-                t.units_per_grab = grab;
-                b->tuning = t;
-                cudaEventRecord(e0, st);
-                rc = batch_frame(b, 0u, spp, max_bounces, 1, st);
-                cudaEventRecord(e1, st);
-                if (rc) break;
-                err = cudaEventSynchronize(e1);
-                float ms = 0.0f;
-                if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
-                if (err != cudaSuccess) {
-                    rc = cuda_fail(err, "autotune timing");
-                    break;
-                }
-                if (best_ms < 0.0f || ms < best_ms) {
-                    best_ms = ms;
-                    best = t;
-                }
-            }
+        for (uint32_t cap : kRegCaps) {
             if (rc) break;
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel_for(depth, b->mode, cap), 128, 0);
+            occ = std::max(occ, 1);
+            const uint32_t blocks[] = {(uint32_t)std::max(occ / 2, 1), (uint32_t)occ};
+            for (uint32_t bps : blocks) {
+                for (uint32_t grab : {1u, 4u}) {
+                    if (b->mode == NAN_BATCH_INDEPENDENT_SAMPLES && grab != 1u) continue;  // one probe per warp
+                    NanBatchTuning t = b->tuning;
+                    t.stack_depth = depth;
+                    t.min_blocks_per_sm = cap;
+                    t.blocks_per_sm = bps;
+                    t.units_per_grab = grab;
+                    b->tuning = t;
+                    cudaEventRecord(e0, st);
+                    rc = batch_frame(b, 0u, spp, max_bounces, 1, st);
+                    cudaEventRecord(e1, st);
+                    if (rc) break;
+                    err = cudaEventSynchronize(e1);
+                    float ms = 0.0f;
+                    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+                    if (err != cudaSuccess) {
+                        rc = cuda_fail(err, "autotune timing");
+                        break;
+                    }
+                    if (best_ms < 0.0f || ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                    }
+                }
+                if (rc) break;
+            }
         }
     }
     cudaEventDestroy(e0);

@@ -81,6 +81,7 @@ struct NanBatch {
     nan_host::BatchImpl* impl = nullptr;
     NanBatchTuning tuning{};
     float tuned_ms = -1.0f;
+    uint32_t mode = 0;  // NAN_BATCH_SEQUENTIAL_SAMPLES or NAN_BATCH_INDEPENDENT_SAMPLES
 };
 
 namespace nan_host {
@@ -147,6 +148,7 @@ int launch_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uin
 int batch_create(NanContext* ctx, const NanProbeSet* sets, uint32_t count, NanBatch** out);
 void batch_destroy(NanBatch* b);
 uint32_t batch_min_depth(const NanBatch* b);
+int batch_set_mode(NanBatch* b, uint32_t mode);
 uint32_t batch_total(const NanBatch* b);
 int batch_set_tuning(NanBatch* b, const NanBatchTuning* t);
 int batch_frame(NanBatch* b, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset, cudaStream_t st);

@@ -9,7 +9,9 @@ surface_probe_path_tracer.py:49-83).
 
 Each item is a SurfaceProbeDiffuseIrradianceBaker with the field and
 attachments it would be executed with; the results equal those of
-baker.execute(...) per scene, bit for bit.
+baker.execute(...) per scene, bit for bit. With independent_samples=True
+each sample of a probe draws from its own RNG stream and a warp traces 32
+samples of one probe at once (a different, equally valid sample set).
 """
 
 from __future__ import annotations
@@ -20,7 +22,7 @@ from ._native import NanBatchTuning, NanProbeSet, check, lib, ptr, stream_handle
 
 
 class ProbeBatch:
-    def __init__(self, device, items):
+    def __init__(self, device, items, *, independent_samples: bool = False):
         self.device = device
         self._keep = []
         sets = (NanProbeSet * max(len(items), 1))()
@@ -43,6 +45,8 @@ class ProbeBatch:
         handle = ctypes.c_void_p()
         check(lib().nan_batch_create(self._context.handle, sets, len(items), ctypes.byref(handle)))
         self.handle = handle
+        if independent_samples:
+            check(lib().nan_batch_set_mode(self.handle, 1))
 
     @property
     def context(self):
@@ -64,11 +68,13 @@ class ProbeBatch:
         t = NanBatchTuning()
         check(lib().nan_batch_info(self.handle, ctypes.byref(depth), ctypes.byref(total), ctypes.byref(t)))
         return {"min_stack_depth": depth.value, "total_probes": total.value, "stack_depth": t.stack_depth,
-                "blocks_per_sm": t.blocks_per_sm, "units_per_grab": t.units_per_grab}
+                "blocks_per_sm": t.blocks_per_sm, "units_per_grab": t.units_per_grab,
+                "min_blocks_per_sm": t.min_blocks_per_sm}
 
-    def set_tuning(self, stack_depth: int, blocks_per_sm: int, units_per_grab: int) -> None:
+    def set_tuning(self, stack_depth: int, blocks_per_sm: int, units_per_grab: int, min_blocks_per_sm: int = 0) -> None:
         t = NanBatchTuning()
         t.stack_depth, t.blocks_per_sm, t.units_per_grab = int(stack_depth), int(blocks_per_sm), int(units_per_grab)
+        t.min_blocks_per_sm = int(min_blocks_per_sm)
         check(lib().nan_batch_set_tuning(self.handle, ctypes.byref(t)))
 
     def autotune(self, samples_per_probe: int, max_bounces: int = 3, stream=None) -> dict:
@@ -77,7 +83,7 @@ class ProbeBatch:
         check(lib().nan_batch_autotune(self.handle, int(samples_per_probe), int(max_bounces), stream_handle(stream),
                                        ctypes.byref(t), ctypes.byref(ms)))
         return {"stack_depth": t.stack_depth, "blocks_per_sm": t.blocks_per_sm, "units_per_grab": t.units_per_grab,
-                "frame_ms": ms.value}
+                "min_blocks_per_sm": t.min_blocks_per_sm, "frame_ms": ms.value}
 
     def execute(self, command_encoder, iteration: int, samples_per_probe: int, max_bounces: int = 3, *,
                 reset: bool = False) -> None:

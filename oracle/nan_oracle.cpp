@@ -1192,7 +1192,7 @@ void accumulate_radial_moment(ProbeBuffers& b, uint32_t probe, uint32_t texel, T
 
 template <class T>
 void probe_unit(Tracer<T>& tr, ProbeBuffers& b, const uint8_t* probes, const uint8_t* pinst, uint32_t probe,
-                uint32_t iteration, uint32_t spp, uint32_t max_bounces, bool reset) {
+                uint32_t iteration, uint32_t spp, uint32_t max_bounces, bool reset, bool independent = false) {
     const uint8_t* rec = probes + 48 * (size_t)probe;
     float nrm[4];
     uint32_t meta[4];
@@ -1218,8 +1218,12 @@ void probe_unit(Tracer<T>& tr, ProbeBuffers& b, const uint8_t* probes, const uin
     if (reset)
         for (int t = 0; t < 16; ++t) b.radial[16 * (size_t)probe + t] = 0u;
     for (uint32_t k = 0; k < n; ++k) {
+        // independent-sample mode (batched baker option): sample k has its own
+        // stream RNG(probe, instance, iteration * n + k)
+        Rng own(probe, inst, iteration * n + k);
+        Rng& r = independent ? own : rng;
         V3<T> si = mk<T>(0, 0, 0);
-        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        T e0 = T(r.next_1d()), e1 = T(r.next_1d());
         V3<T> dir;
         T pdf;
         cosine_sample_hemisphere<T>(e0, e1, &dir, &pdf);
@@ -1236,7 +1240,7 @@ void probe_unit(Tracer<T>& tr, ProbeBuffers& b, const uint8_t* probes, const uin
             p.self_hits = 0;
             p.first_hit = T(2) * kr;
             p.radial_max = T(2) * kr;
-            probe_trace_radiance<T>(tr, p, rng, max_bounces);
+            probe_trace_radiance<T>(tr, p, r, max_bounces);
             self_total += p.self_hits;
             float u, v;
             hemi_oct_encode((float)dir.x, (float)dir.y, (float)dir.z, &u, &v);
@@ -1588,13 +1592,12 @@ int oracle_trace_points(void* sp, const OracleLighting* lighting, const float* p
     return 0;
 }
 
-int oracle_trace_probes(void* sp, const OracleLighting* lighting, float* values, uint32_t* sample_counts,
-                        uint32_t* self_hits, uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
-                        const uint8_t* probe_instances, uint32_t probe_instance_count, const uint32_t* units,
-                        int unit_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset,
-                        int precision, int threads, OracleRayCounts* counts) {
+static int trace_probes_impl(void* sp, const OracleLighting* lighting, float* values, uint32_t* sample_counts,
+                             uint32_t* self_hits, uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                             const uint8_t* probe_instances, const uint32_t* units, int unit_count,
+                             uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset, int precision,
+                             int threads, OracleRayCounts* counts, bool independent) {
     Scene* s = static_cast<Scene*>(sp);
-    (void)probe_instance_count;
     ProbeBuffers b{values, sample_counts, self_hits, radial};
     std::vector<OracleRayCounts> unit_counts((size_t)unit_count);
     parallel_for(unit_count, threads, [&](int u, int) {
@@ -1602,16 +1605,41 @@ int oracle_trace_probes(void* sp, const OracleLighting* lighting, float* values,
         if (p >= probe_count) return;
         if (precision == ORACLE_F64) {
             Tracer<double> tr(*s, *lighting);
-            probe_unit<double>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0);
+            probe_unit<double>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0,
+                               independent);
             unit_counts[u] = tr.cnt;
         } else {
             Tracer<float> tr(*s, *lighting);
-            probe_unit<float>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0);
+            probe_unit<float>(tr, b, probes, probe_instances, p, iteration, spp, max_bounces, reset != 0,
+                              independent);
             unit_counts[u] = tr.cnt;
         }
     });
     for (auto& c : unit_counts) add_counts(counts, c);
     return 0;
+}
+
+int oracle_trace_probes(void* sp, const OracleLighting* lighting, float* values, uint32_t* sample_counts,
+                        uint32_t* self_hits, uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
+                        const uint8_t* probe_instances, uint32_t probe_instance_count, const uint32_t* units,
+                        int unit_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset,
+                        int precision, int threads, OracleRayCounts* counts) {
+    (void)probe_instance_count;
+    return trace_probes_impl(sp, lighting, values, sample_counts, self_hits, radial, probes, probe_count,
+                             probe_instances, units, unit_count, iteration, spp, max_bounces, reset, precision,
+                             threads, counts, false);
+}
+
+int oracle_trace_probes_independent(void* sp, const OracleLighting* lighting, float* values,
+                                    uint32_t* sample_counts, uint32_t* self_hits, uint32_t* radial,
+                                    const uint8_t* probes, uint32_t probe_count, const uint8_t* probe_instances,
+                                    uint32_t probe_instance_count, const uint32_t* units, int unit_count,
+                                    uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset,
+                                    int precision, int threads, OracleRayCounts* counts) {
+    (void)probe_instance_count;
+    return trace_probes_impl(sp, lighting, values, sample_counts, self_hits, radial, probes, probe_count,
+                             probe_instances, units, unit_count, iteration, spp, max_bounces, reset, precision,
+                             threads, counts, true);
 }
 
 }  // extern "C"

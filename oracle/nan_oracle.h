@@ -159,6 +159,19 @@ int oracle_trace_probes(void* scene, const OracleLighting* lighting,
                         uint32_t max_bounces, int reset, int precision,
                         int threads, OracleRayCounts* counts);
 
+/* The same with one RNG stream per sample, RNG(probe, instance, iteration * n
+ * + k): the batched baker's independent-sample mode. */
+int oracle_trace_probes_independent(void* scene, const OracleLighting* lighting,
+                                    float* values, uint32_t* sample_counts,
+                                    uint32_t* self_hits, uint32_t* radial,
+                                    const uint8_t* probes, uint32_t probe_count,
+                                    const uint8_t* probe_instances,
+                                    uint32_t probe_instance_count,
+                                    const uint32_t* units, int unit_count,
+                                    uint32_t iteration, uint32_t samples_per_probe,
+                                    uint32_t max_bounces, int reset, int precision,
+                                    int threads, OracleRayCounts* counts);
+
 #ifdef __cplusplus
 }
 #endif

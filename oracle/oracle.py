@@ -108,6 +108,7 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes.argtypes = [vp, vp, vp, vp, vp, vp, vp, u32, vp, u32, vp, i,
                                       u32, u32, u32, i, i, i, vp]
+    l.oracle_trace_probes_independent.argtypes = l.oracle_trace_probes.argtypes
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
     l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
 
@@ -327,7 +328,7 @@ class OracleScene:
 
     def trace_probes(self, lighting, values, sample_counts, self_hits, radial, probes,
                      probe_instances, units, iteration, samples_per_probe, max_bounces,
-                     reset, precision=F32, threads=0):
+                     reset, precision=F32, threads=0, independent_samples=False):
         """Updates values/sample_counts/self_hits/radial in place."""
         for buf in (values, sample_counts, self_hits, radial):
             assert buf.flags["C_CONTIGUOUS"]
@@ -336,7 +337,8 @@ class OracleScene:
         un = np.ascontiguousarray(units, dtype=np.uint32).reshape(-1)
         counts = OracleRayCounts()
         L = lighting_struct(lighting)
-        rc = lib().oracle_trace_probes(self.handle, ctypes.byref(L), _p(values),
+        fn = lib().oracle_trace_probes_independent if independent_samples else lib().oracle_trace_probes
+        rc = fn(self.handle, ctypes.byref(L), _p(values),
                                        _p(sample_counts), _p(self_hits), _p(radial), _p(pr),
                                        pr.size // 48, _p(pi), pi.size // 48, _p(un), un.size,
                                        iteration, samples_per_probe, max_bounces,
