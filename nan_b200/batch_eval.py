@@ -116,3 +116,45 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
                         "batched": batch_rays / (batch_ms * 1e3), "batched_graph": batch_rays / (graph_ms * 1e3),
                         "batched_graph_independent_samples": ind_rays / (ind_ms * 1e3)},
     }
+
+
+def main() -> None:
+    """`--frames` batched frames over `--count` seeded scenes (no per-scene
+    comparison); a small, self-contained workload for profiling."""
+    import argparse
+
+    import torch
+
+    from . import scenes as sc
+    from .probe_batch import ProbeBatch
+    from .render_data import RenderData
+    from .scene import Device, Scene
+    from .surface_probe_fields import SurfaceProbeRuntimeBuffers
+    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from .surface_probe_resources import SurfaceProbeGpuGeometry
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--count", type=int, default=16)
+    ap.add_argument("--frames", type=int, default=2)
+    ap.add_argument("--independent-samples", action="store_true")
+    a = ap.parse_args()
+    device = Device(0)
+    items = []
+    for i, (node, n_sites) in enumerate(sc.batch_scenes(a.count, 1)):
+        scene = Scene(device, node)
+        probes, pinst = sc.surface_sites(node, n_sites, seed=1 + i, radius=0.25)
+        geometry = SurfaceProbeGpuGeometry.create(device, _sites_layout(probes, pinst))
+        baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
+                                                   compensated=True)
+        rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)
+        items.append((scene, baker, rt.field, rt.attachments))
+    batch = ProbeBatch(device, [(b, f, at) for _, b, f, at in items], independent_samples=a.independent_samples)
+    for f in range(a.frames):
+        batch.execute(None, f, 64, 3, reset=(f == 0))
+    torch.cuda.synchronize()
+    device.check()
+    print("ok", a.frames, "batched frames over", a.count, "scenes")
+
+
+if __name__ == "__main__":
+    main()

@@ -132,3 +132,40 @@ def summary(r: dict) -> str:
 
 
 __all__ = ["compare", "summary", "scene_bounds"]
+
+
+def main() -> None:
+    """Run `--frames` cached frames (render + online training) on the seeded
+    998,408-triangle scene; a small, self-contained workload for profiling."""
+    import argparse
+
+    import torch
+
+    from . import scenes
+    from .cached_path_tracer import CachedPathTracer
+    from .radiance_cache import RadianceCache
+    from .scene import Device, Scene
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--frames", type=int, default=6)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--cache-vertex", type=int, default=1)
+    a = ap.parse_args()
+    device = Device(0)
+    node = scenes.terrain_boxes(seed=1, grid=699, boxes=2000)
+    scene = Scene(device, node)
+    lo, hi = scene_bounds(scene)
+    tracer = CachedPathTracer(device, scene, RadianceCache(device, lo, hi), cache_vertex=a.cache_vertex,
+                              train_batch=16384)
+    out = torch.zeros((a.height, a.width, 4), dtype=torch.float32, device=device.torch_device)
+    for f in range(a.frames):
+        node.camera.begin_frame(a.width, a.height)
+        tracer.execute(None, out, f)
+    torch.cuda.synchronize()
+    device.check()
+    print("ok", a.frames, "cached frames")
+
+
+if __name__ == "__main__":
+    main()
