@@ -264,6 +264,18 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
                                   const NanLighting* lighting, uint32_t probe_begin,
                                   uint32_t probe_end, float* compensation, void* stream);
 
+/* MeshColorsResolve.execute / execute_frozen (mesh_colors_resolve.py:8-73;
+ * mesh_colors_resolve.slang:29-73, mesh_colors_frozen_resolve.slang:93-135):
+ * one primary ray per pixel, the hit triangle's lattice colours interpolated
+ * (mesh_colors.slang:365-426) and shaded as emissive + albedo / pi *
+ * irradiance into out f32[H][W][4]. colors is the 16-byte slot buffer
+ * (packed = 0) or the RGB9E5 words of nan_pack_rgb9e5 (packed = 1); the
+ * layout's face, instance and side buffers are read. */
+NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout,
+                                         const void* colors, int packed, float* out, uint32_t width,
+                                         uint32_t height, const NanCamera* camera,
+                                         const NanLighting* lighting, void* stream);
+
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out,

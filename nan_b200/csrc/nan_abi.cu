@@ -338,6 +338,22 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
                                          as_stream(stream));
 }
 
+NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const void* colors,
+                                         int packed, float* out, uint32_t width, uint32_t height,
+                                         const NanCamera* camera, const NanLighting* lighting, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = need_scene(ctx);
+    if (rc) return rc;
+    if (!layout || !colors || !out || !camera || !lighting) return invalid("null argument");
+    if (!layout->face_infos || !layout->instance_infos || !layout->side_infos) return invalid("null layout buffer");
+    if (layout->instance_count < ctx->scene.instance_count)
+        return invalid("the layout covers fewer instances than the scene");
+    if (!aligned16(out) || (!packed && !aligned16(colors))) return invalid("out and slot colors must be 16-byte aligned");
+    return nan_host::launch_resolve_mesh_colors(ctx, layout, colors, packed, out, width, height, camera, lighting,
+                                                as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -156,6 +156,9 @@ int batch_capture(NanBatch* b, uint32_t first_iteration, int reset_first, uint32
                   cudaStream_t st);
 int batch_replay(NanBatch* b, uint32_t frames, cudaStream_t st);
 int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t st, NanBatchTuning* chosen);
+int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const void* colors, int packed,
+                               float* out, uint32_t w, uint32_t h, const NanCamera* cam, const NanLighting* light,
+                               cudaStream_t st);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

@@ -155,6 +155,109 @@ __global__ void __launch_bounds__(128) k_trace_screen(SceneView s, LightingRaw l
     flush_tally(counters, tally, 1u, 1u);
 }
 
+// ---------------------------------------------------------------------------
+// Mesh Colors resolve (mesh_colors_resolve.slang:29-73) and frozen RGB9E5
+// resolve (mesh_colors_frozen_resolve.slang:93-135): one primary ray per
+// pixel, the hit triangle's lattice colours interpolated
+// (mesh_colors_sample_irradiance, mesh_colors.slang:365-426), shaded as
+// emissive + albedo / pi * irradiance.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ f3 mc_load(const void* colors, bool packed, uint32_t texel) {
+    if (packed) {
+        const uint32_t p = __ldg(reinterpret_cast<const uint32_t*>(colors) + texel);
+        // exp2(e - 24) for the 5-bit exponent e, built exactly
+        const float scale = __int_as_float((int)(((p >> 27) - 24u + 127u) << 23));
+        return mk3((float)(p & 0x1ffu) * scale, (float)((p >> 9) & 0x1ffu) * scale,
+                   (float)((p >> 18) & 0x1ffu) * scale);
+    }
+    const float4 v = __ldg(reinterpret_cast<const float4*>(colors) + texel);
+    return mk3(v.x, v.y, v.z);
+}
+
+__device__ __forceinline__ uint32_t mc_side_texel(uint32_t front, uint4 inst, uint2 side, bool back) {
+    return back ? side.x + (front - inst.z) : front;
+}
+
+template <bool kPacked>
+__global__ void __launch_bounds__(128) k_resolve_mesh_colors(SceneView s, LightingRaw lraw, CameraRaw cam, McView mc,
+                                                             const void* __restrict__ colors,
+                                                             float4* __restrict__ out, uint32_t w, uint32_t h) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= w || py >= h) return;
+    const LightParams L = make_light(lraw);
+    // compute_ray_pinhole (camera.slang:223-236), as in the path tracer
+    float pxf = ((float)px + 0.5f) / (float)w;
+    float pyf = ((float)py + 0.5f) / (float)h;
+    pxf = pxf + (-cam.jitter_x);
+    pyf = pyf + cam.jitter_y;
+    const float nx = 2.0f * pxf + -1.0f;
+    const float ny = -2.0f * pyf + 1.0f;
+    const f3 U = mk3(cam.image_u[0], cam.image_u[1], cam.image_u[2]);
+    const f3 V = mk3(cam.image_v[0], cam.image_v[1], cam.image_v[2]);
+    const f3 W = mk3(cam.image_w[0], cam.image_w[1], cam.image_w[2]);
+    const f3 dir = normalize3((nx * U + ny * V) + W);
+    const float inv_cos = 1.0f / dot3(normalize3(W), dir);
+    const f3 o = mk3(cam.position[0], cam.position[1], cam.position[2]);
+    const HitInfo hit = trace_closest(s, o, dir, cam.near_clip * inv_cos, cam.far_clip * inv_cos);
+    const size_t pix = (size_t)py * w + px;
+    if (!hit.valid) {
+        f3 sky = L.sky;
+        if (L.sun_disk) sky = sky + sun_disk(L, dir);
+        out[pix] = make_float4(sky.x, sky.y, sky.z, 1.0f);
+        return;
+    }
+    const uint2 ref = __ldg(s.tri_refs + hit.flat);
+    const bool back = dot3(world_flat_normal(s, ref.x, ref.y), -dir) <= 0.0f;
+    if (ref.x >= mc.instance_count) {
+        atomicOr(s.status, kStatusBadRecord);
+        return;
+    }
+    const uint4 inst = __ldg(mc.instance_infos + ref.x);
+    const uint2 side = __ldg(mc.side_infos + ref.x);
+    if (back && !(side.y & 1u)) {
+        out[pix] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+        return;
+    }
+    const uint2 face = __ldg(mc.face_infos + inst.x + ref.y);
+    const float b0 = (1.0f - hit.b1) - hit.b2, b1 = hit.b1, b2 = hit.b2;
+    const uint32_t R = face.y;
+    const float rf = (float)R;
+    const float s0 = sat(b0) * rf, s1 = sat(b1) * rf, s2 = sat(b2) * rf;
+    uint32_t i = min((uint32_t)s0, R);
+    uint32_t j = min((uint32_t)s1, R - i);
+    float w0 = s0 - floorf(s0), w1 = s1 - floorf(s1), w2 = s2 - floorf(s2);
+    const bool upper = fabsf(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
+    if (upper) {
+        w0 = 1.0f - w0;
+        w1 = 1.0f - w1;
+        w2 = 1.0f - w2;
+    }
+    f3 irr;
+    if ((w0 + w1) + w2 <= 1e-6f || i >= R || j >= R - i) {
+        irr = mc_load(colors, kPacked, mc_side_texel(mc_address(i, j, inst.z, face), inst, side, back));
+    } else {
+        uint32_t ta, tb, tc;
+        if (upper) {
+            ta = mc_address(i, j + 1u, inst.z, face);
+            tb = mc_address(i + 1u, j, inst.z, face);
+            tc = mc_address(i + 1u, j + 1u, inst.z, face);
+        } else {
+            ta = mc_address(i + 1u, j, inst.z, face);
+            tb = mc_address(i, j + 1u, inst.z, face);
+            tc = mc_address(i, j, inst.z, face);
+        }
+        const f3 ca = mc_load(colors, kPacked, mc_side_texel(ta, inst, side, back));
+        const f3 cb = mc_load(colors, kPacked, mc_side_texel(tb, inst, side, back));
+        const f3 cc = mc_load(colors, kPacked, mc_side_texel(tc, inst, side, back));
+        irr = (w0 * ca + w1 * cb) + w2 * cc;
+    }
+    const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
+    const f3 c = sd.emissive + (sd.diffuse * kInvPi) * irr;
+    out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+
 // accumulator.slang:9-19
 __global__ void k_accumulate(const float4* __restrict__ input, float4* __restrict__ output,
                              float4* __restrict__ history, uint32_t n, int reset) {
@@ -342,6 +445,30 @@ int launch_trace_screen(NanContext* ctx, float* out, uint32_t w, uint32_t h, uin
                                          max_vertices, ctx->d_counters);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "trace_screen launch");
+}
+
+int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* lay, const void* colors, int packed,
+                               float* out, uint32_t w, uint32_t h, const NanCamera* cam, const NanLighting* light,
+                               cudaStream_t st) {
+    if (w == 0 || h == 0) return NAN_OK;
+    CameraRaw c;
+    memcpy(&c, cam, sizeof(c));
+    McView mc;
+    memset(&mc, 0, sizeof(mc));
+    mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
+    mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
+    mc.side_infos = reinterpret_cast<const uint2*>(lay->side_infos);
+    mc.instance_count = lay->instance_count;
+    mc.payload_count = lay->payload_count;
+    dim3 grid(blocks_for(w, 16), blocks_for(h, 8));
+    if (packed)
+        k_resolve_mesh_colors<true><<<grid, 128, 0, st>>>(scene_view(ctx), to_raw(light), c, mc, colors,
+                                                          reinterpret_cast<float4*>(out), w, h);
+    else
+        k_resolve_mesh_colors<false><<<grid, 128, 0, st>>>(scene_view(ctx), to_raw(light), c, mc, colors,
+                                                           reinterpret_cast<float4*>(out), w, h);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "resolve_mesh_colors launch");
 }
 
 int launch_accumulate(NanContext* ctx, const float* input, float* output, float* history, uint32_t w, uint32_t h,

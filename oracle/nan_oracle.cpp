@@ -1267,6 +1267,79 @@ void probe_unit(Tracer<T>& tr, ProbeBuffers& b, const uint8_t* probes, const uin
     b.self_hits[probe] = prev_self + self_total;
 }
 
+// Mesh Colors resolve (mesh_colors_resolve.slang:29-73) and the frozen RGB9E5
+// variant (mesh_colors_frozen_resolve.slang:93-135), one pixel.
+template <class T>
+void resolve_pixel(Tracer<T>& tr, const OracleCamera& cam, uint32_t w, uint32_t h, uint32_t px, uint32_t py,
+                   const uint32_t* face_infos, const uint32_t* instance_infos, const uint32_t* side_infos,
+                   uint32_t instance_count, const void* colors, bool packed, float* out) {
+    // compute_ray_pinhole (camera.slang:223-236)
+    T pxf = (T((float)px) + T(0.5)) / T((float)w);
+    T pyf = (T((float)py) + T(0.5)) / T((float)h);
+    pxf = pxf + (-T(cam.jitter_x));
+    pyf = pyf + T(cam.jitter_y);
+    T nx = T(2) * pxf + T(-1);
+    T ny = T(-2) * pyf + T(1);
+    V3<T> U = load3<T>(cam.image_u), Vv = load3<T>(cam.image_v), W = load3<T>(cam.image_w);
+    V3<T> dir = normalize((nx * U + ny * Vv) + W);
+    T inv_cos = T(1) / dot(normalize(W), dir);
+    V3<T> o = load3<T>(cam.position);
+    HitRec hit = tr.closest(o, dir, T(cam.near_clip) * inv_cos, T(cam.far_clip) * inv_cos);
+    out[3] = 1.0f;
+    if (!hit.valid) {
+        V3<T> sky = tr.L.sky;
+        if (tr.L.sun_disk) sky = sky + tr.sun_disk(dir);
+        out[0] = (float)sky.x; out[1] = (float)sky.y; out[2] = (float)sky.z;
+        return;
+    }
+    uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
+    bool back = dot(world_flat_normal<T>(tr.s, inst, prim), -dir) <= T(0);
+    out[0] = out[1] = out[2] = 0.0f;
+    if (inst >= instance_count) return;
+    InstInfo ii{instance_infos[4 * inst], instance_infos[4 * inst + 1], instance_infos[4 * inst + 2],
+                instance_infos[4 * inst + 3]};
+    uint32_t side_back = side_infos[2 * inst], side_flags = side_infos[2 * inst + 1];
+    if (back && !(side_flags & 1u)) return;
+    FaceInfo f{face_infos[2 * (ii.face_offset + prim)], face_infos[2 * (ii.face_offset + prim) + 1]};
+    auto load = [&](uint32_t front) {
+        uint32_t t = back ? side_back + (front - ii.texel_offset) : front;
+        float c[3];
+        if (packed) {
+            unpack_rgb9e5(static_cast<const uint32_t*>(colors)[t], c);
+        } else {
+            std::memcpy(c, static_cast<const uint8_t*>(colors) + 16 * (size_t)t, 12);
+        }
+        return mk<T>(T(c[0]), T(c[1]), T(c[2]));
+    };
+    T b1 = T(hit.b1), b2 = T(hit.b2);
+    T b0 = (T(1) - b1) - b2;
+    uint32_t R = f.resolution;
+    T rf = T((float)R);
+    T s0 = saturate(b0) * rf, s1 = saturate(b1) * rf, s2 = saturate(b2) * rf;
+    uint32_t i = std::min((uint32_t)s0, R);
+    uint32_t j = std::min((uint32_t)s1, R - i);
+    T w0 = s0 - std::floor(s0), w1 = s1 - std::floor(s1), w2 = s2 - std::floor(s2);
+    bool upper = std::fabs(((w0 + w1) + w2) - T(2)) <= T(1e-3f);
+    if (upper) {
+        w0 = T(1) - w0;
+        w1 = T(1) - w1;
+        w2 = T(1) - w2;
+    }
+    V3<T> irr;
+    if ((w0 + w1) + w2 <= T(1e-6f) || i >= R || j >= R - i) {
+        irr = load(mc_address(i, j, ii, f));
+    } else if (upper) {
+        irr = (w0 * load(mc_address(i, j + 1, ii, f)) + w1 * load(mc_address(i + 1, j, ii, f))) +
+              w2 * load(mc_address(i + 1, j + 1, ii, f));
+    } else {
+        irr = (w0 * load(mc_address(i + 1, j, ii, f)) + w1 * load(mc_address(i, j + 1, ii, f))) +
+              w2 * load(mc_address(i, j, ii, f));
+    }
+    Shading<T> sd = shading_data<T>(tr.s, inst, prim, b1, b2, -dir);
+    V3<T> c = sd.emissive + (sd.diffuse * Consts<T>::INV_PI) * irr;
+    out[0] = (float)c.x; out[1] = (float)c.y; out[2] = (float)c.z;
+}
+
 template <class F> void parallel_for(int count, int threads, F&& fn) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::max(1, std::min(threads, count));
@@ -1543,6 +1616,26 @@ int oracle_trace_texels(void* sp, const OracleLighting* lighting, uint8_t* slots
     });
     for (auto& c : unit_counts) add_counts(counts, c);
     if (bad) { g_error = "texel index out of range"; return 1; }
+    return 0;
+}
+
+int oracle_resolve_mesh_colors(void* sp, const OracleLighting* lighting, const OracleCamera* camera, uint32_t width,
+                               uint32_t height, const uint32_t* pixels, int pixel_count, const uint32_t* face_infos,
+                               const uint32_t* instance_infos, const uint32_t* side_infos, uint32_t instance_count,
+                               const void* colors, int packed, int precision, int threads, float* out) {
+    Scene* s = static_cast<Scene*>(sp);
+    parallel_for(pixel_count, threads, [&](int i, int) {
+        uint32_t px = pixels[2 * i], py = pixels[2 * i + 1];
+        if (precision == ORACLE_F64) {
+            Tracer<double> tr(*s, *lighting);
+            resolve_pixel<double>(tr, *camera, width, height, px, py, face_infos, instance_infos, side_infos,
+                                  instance_count, colors, packed != 0, out + 4 * (size_t)i);
+        } else {
+            Tracer<float> tr(*s, *lighting);
+            resolve_pixel<float>(tr, *camera, width, height, px, py, face_infos, instance_infos, side_infos,
+                                 instance_count, colors, packed != 0, out + 4 * (size_t)i);
+        }
+    });
     return 0;
 }
 

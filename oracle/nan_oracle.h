@@ -130,6 +130,17 @@ int oracle_trace_texels(void* scene, const OracleLighting* lighting,
                         uint32_t max_bounces, int reset, int precision,
                         int threads, OracleRayCounts* counts);
 
+/* Mesh Colors resolve of the listed pixels (mesh_colors_resolve.slang:29-73;
+ * packed = 1: the frozen RGB9E5 resolve, mesh_colors_frozen_resolve.slang:
+ * 93-135). colors: 16-byte slots or RGB9E5 words. out f32[N][4]. */
+int oracle_resolve_mesh_colors(void* scene, const OracleLighting* lighting,
+                               const OracleCamera* camera, uint32_t width, uint32_t height,
+                               const uint32_t* pixels, int pixel_count,
+                               const uint32_t* face_infos, const uint32_t* instance_infos,
+                               const uint32_t* side_infos, uint32_t instance_count,
+                               const void* colors, int packed, int precision, int threads,
+                               float* out);
+
 /* Area-light table of the screen tracer's NEE option (lighting flag bit 1),
  * the layout of nan_ctx_set_area_lights. */
 void oracle_scene_set_area_lights(void* scene, const float* lights, int count, float power);

@@ -110,6 +110,7 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes_independent.argtypes = l.oracle_trace_probes.argtypes
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
+    l.oracle_resolve_mesh_colors.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, vp, vp, u32, vp, i, i, i, vp]
     l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
 
 
@@ -307,6 +308,24 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
         return counts.as_dict()
+
+    def resolve_mesh_colors(self, lighting, camera, width, height, pixels, face_infos, instance_infos, side_infos,
+                            colors, packed=False, precision=F32, threads=0):
+        """Mesh Colors resolve of pixels u32[N, 2]; colors are slots (uint32 [P, 4])
+        or RGB9E5 words (uint32 [P]). Returns f32[N, 4]."""
+        px = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+        fi = np.ascontiguousarray(face_infos, dtype=np.uint32).reshape(-1, 2)
+        ii = np.ascontiguousarray(instance_infos, dtype=np.uint32).reshape(-1, 4)
+        si = np.ascontiguousarray(side_infos, dtype=np.uint32).reshape(-1, 2)
+        col = np.ascontiguousarray(colors, dtype=np.uint32)
+        out = np.zeros((px.shape[0], 4), np.float32)
+        L, C = lighting_struct(lighting), camera_struct(camera)
+        rc = lib().oracle_resolve_mesh_colors(self.handle, ctypes.byref(L), ctypes.byref(C), width, height, _p(px),
+                                              px.shape[0], _p(fi), _p(ii), _p(si), ii.shape[0], _p(col),
+                                              int(bool(packed)), precision, threads, _p(out))
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
+        return out
 
     def set_area_lights(self, lights, power):
         """Area-light table f32[L, 16] and total power (nan_ctx_set_area_lights layout)."""
