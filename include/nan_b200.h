@@ -276,6 +276,20 @@ NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDes
                                          uint32_t height, const NanCamera* camera,
                                          const NanLighting* lighting, void* stream);
 
+/* MeshColorsSurfaceFilter.execute (mesh_colors_surface_filter.py:95-130;
+ * mesh_colors_surface_filter.slang:1-253): one pass of the one-ring,
+ * normal-aware filter from source slots to destination slots (distinct
+ * buffers; counts are copied). adjacency u32[F][4]: per face the packed edges
+ * 0..2 ((mesh-local adjacent face << 3) | adjacent edge | flip << 2, ~0 for
+ * none); face_normals f32[F][4] in world space; neighbor_weight =
+ * exp(-0.5 / spatial_sigma^2); normal_sigma in radians. All instances in one
+ * launch. */
+NAN_B200_API int nan_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout,
+                                        const uint32_t* adjacency, const float* face_normals,
+                                        const uint8_t* source, uint8_t* destination,
+                                        float neighbor_weight, float normal_sigma_radians,
+                                        void* stream);
+
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out,

@@ -20,6 +20,7 @@ from .camera import Camera, HaltonSamplePattern, halton
 from .mesh_colors import (MESH_COLORS_INVALID_OFFSET, MESH_COLORS_PAYLOAD_SIZE, MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED,
                           MeshColorsLayout, address_to_ij, barycentric_at, colors_per_patch, ij_to_address)
 from .mesh_colors_resolve import MeshColorsResolve
+from .mesh_colors_surface_filter import MeshColorsSurfaceFilter
 from .mesh_colors_rgb9e5 import MeshColorsRGB9E5Packer
 from .path_tracer import PathTracer
 from .probe_batch import ProbeBatch
@@ -35,7 +36,7 @@ from .texture_space_path_tracer import TextureSpacePathTracer
 
 __all__ = [
     "Accumulator", "CachedPathTracer", "Camera", "Device", "HaltonSamplePattern", "Lighting", "Material", "Mesh", "MeshColorsLayout",
-    "MeshColorsRGB9E5Packer", "MeshColorsResolve", "PathTracer", "ProbeBatch", "RadianceCache", "RenderData", "Scene", "SceneNode", "SurfaceProbeAttachments",
+    "MeshColorsRGB9E5Packer", "MeshColorsResolve", "MeshColorsSurfaceFilter", "PathTracer", "ProbeBatch", "RadianceCache", "RenderData", "Scene", "SceneNode", "SurfaceProbeAttachments",
     "SurfaceProbeDiffuseIrradianceBaker", "SurfaceProbeFieldBuffers", "SurfaceProbeGpuGeometry",
     "SurfaceProbePathTracer", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "address_to_ij",
     "barycentric_at", "colors_per_patch", "halton", "ij_to_address", "make_transform",

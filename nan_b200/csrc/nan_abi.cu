@@ -354,6 +354,22 @@ NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDes
                                                 as_stream(stream));
 }
 
+NAN_B200_API int nan_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const uint32_t* adjacency,
+                                        const float* face_normals, const uint8_t* source, uint8_t* destination,
+                                        float neighbor_weight, float normal_sigma_radians, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!layout || !adjacency || !face_normals || !source || !destination) return invalid("null argument");
+    if (!layout->face_infos || !layout->instance_infos || !layout->side_infos || !layout->surface_prefix)
+        return invalid("null layout buffer");
+    if (source == destination) return invalid("the surface filter needs distinct source and destination buffers");
+    if (!aligned16(adjacency) || !aligned16(face_normals) || !aligned16(source) || !aligned16(destination))
+        return invalid("adjacency, normals and slot buffers must be 16-byte aligned");
+    if (!(neighbor_weight >= 0.0f) || !(normal_sigma_radians >= 0.0f)) return invalid("negative filter weight or sigma");
+    return nan_host::launch_filter_mesh_colors(ctx, layout, adjacency, face_normals, source, destination,
+                                               neighbor_weight, normal_sigma_radians, as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -178,6 +178,40 @@ __device__ __forceinline__ uint32_t mc_side_texel(uint32_t front, uint4 inst, ui
     return back ? side.x + (front - inst.z) : front;
 }
 
+// mesh_colors_sample_irradiance (mesh_colors.slang:365-426) at barycentrics
+// (b0, b1, b2) of a face, front or back side.
+__device__ __forceinline__ f3 mc_sample(const void* colors, bool packed, float b0, float b1, float b2, uint4 inst,
+                                        uint2 face, uint2 side, bool back) {
+    const uint32_t R = face.y;
+    const float rf = (float)R;
+    const float s0 = sat(b0) * rf, s1 = sat(b1) * rf, s2 = sat(b2) * rf;
+    uint32_t i = min((uint32_t)s0, R);
+    uint32_t j = min((uint32_t)s1, R - i);
+    float w0 = s0 - floorf(s0), w1 = s1 - floorf(s1), w2 = s2 - floorf(s2);
+    const bool upper = fabsf(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
+    if (upper) {
+        w0 = 1.0f - w0;
+        w1 = 1.0f - w1;
+        w2 = 1.0f - w2;
+    }
+    if ((w0 + w1) + w2 <= 1e-6f || i >= R || j >= R - i)
+        return mc_load(colors, packed, mc_side_texel(mc_address(i, j, inst.z, face), inst, side, back));
+    uint32_t ta, tb, tc;
+    if (upper) {
+        ta = mc_address(i, j + 1u, inst.z, face);
+        tb = mc_address(i + 1u, j, inst.z, face);
+        tc = mc_address(i + 1u, j + 1u, inst.z, face);
+    } else {
+        ta = mc_address(i + 1u, j, inst.z, face);
+        tb = mc_address(i, j + 1u, inst.z, face);
+        tc = mc_address(i, j, inst.z, face);
+    }
+    const f3 ca = mc_load(colors, packed, mc_side_texel(ta, inst, side, back));
+    const f3 cb = mc_load(colors, packed, mc_side_texel(tb, inst, side, back));
+    const f3 cc = mc_load(colors, packed, mc_side_texel(tc, inst, side, back));
+    return (w0 * ca + w1 * cb) + w2 * cc;
+}
+
 template <bool kPacked>
 __global__ void __launch_bounds__(128) k_resolve_mesh_colors(SceneView s, LightingRaw lraw, CameraRaw cam, McView mc,
                                                              const void* __restrict__ colors,
@@ -221,41 +255,138 @@ __global__ void __launch_bounds__(128) k_resolve_mesh_colors(SceneView s, Lighti
         return;
     }
     const uint2 face = __ldg(mc.face_infos + inst.x + ref.y);
-    const float b0 = (1.0f - hit.b1) - hit.b2, b1 = hit.b1, b2 = hit.b2;
-    const uint32_t R = face.y;
-    const float rf = (float)R;
-    const float s0 = sat(b0) * rf, s1 = sat(b1) * rf, s2 = sat(b2) * rf;
-    uint32_t i = min((uint32_t)s0, R);
-    uint32_t j = min((uint32_t)s1, R - i);
-    float w0 = s0 - floorf(s0), w1 = s1 - floorf(s1), w2 = s2 - floorf(s2);
-    const bool upper = fabsf(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
-    if (upper) {
-        w0 = 1.0f - w0;
-        w1 = 1.0f - w1;
-        w2 = 1.0f - w2;
-    }
-    f3 irr;
-    if ((w0 + w1) + w2 <= 1e-6f || i >= R || j >= R - i) {
-        irr = mc_load(colors, kPacked, mc_side_texel(mc_address(i, j, inst.z, face), inst, side, back));
-    } else {
-        uint32_t ta, tb, tc;
-        if (upper) {
-            ta = mc_address(i, j + 1u, inst.z, face);
-            tb = mc_address(i + 1u, j, inst.z, face);
-            tc = mc_address(i + 1u, j + 1u, inst.z, face);
-        } else {
-            ta = mc_address(i + 1u, j, inst.z, face);
-            tb = mc_address(i, j + 1u, inst.z, face);
-            tc = mc_address(i, j, inst.z, face);
-        }
-        const f3 ca = mc_load(colors, kPacked, mc_side_texel(ta, inst, side, back));
-        const f3 cb = mc_load(colors, kPacked, mc_side_texel(tb, inst, side, back));
-        const f3 cc = mc_load(colors, kPacked, mc_side_texel(tc, inst, side, back));
-        irr = (w0 * ca + w1 * cb) + w2 * cc;
-    }
+    const float b0 = (1.0f - hit.b1) - hit.b2;
+    const f3 irr = mc_sample(colors, kPacked, b0, hit.b1, hit.b2, inst, face, side, back);
     const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
     const f3 c = sd.emissive + (sd.diffuse * kInvPi) * irr;
     out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Mesh Colors one-ring surface filter (mesh_colors_surface_filter.slang:
+// 1-253): each texel's colour becomes the weighted mean of itself and its six
+// lattice neighbours; neighbours across an edge are mapped into the adjacent
+// face (mesh_colors_map_one_edge_tap, mesh_colors.slang:156-203), sampled
+// there and weighted by the Gaussian in the angle between face normals. All
+// instances in one launch (the reference dispatches per instance).
+// ---------------------------------------------------------------------------
+struct FilterArgs {
+    McView mc;
+    const uint4* adjacency;  // per face: packed edges 0..2
+    const float4* normals;   // per face
+    const float4* src;
+    float4* dst;
+    float neighbor_weight;
+    float sigma;
+    uint32_t total_texels;
+};
+
+__device__ __forceinline__ float normal_filter_weight(f3 c, f3 n, float sigma) {
+    const float cosine = minf(maxf(dot3(c, n), 0.0f), 1.0f);
+    if (sigma <= 1e-6f) return cosine >= 1.0f - 1e-6f ? 1.0f : 0.0f;
+    const float angle = acosf(cosine);
+    const float na = angle / sigma;
+    return expf(-0.5f * na * na);
+}
+
+// Lattice point candidate (x, y) outside the face, across `edge`: its
+// barycentrics in the adjacent face, or false.
+__device__ __forceinline__ bool map_edge_tap(int x, int y, uint32_t R, uint32_t adj_edge, bool flip, uint32_t edge,
+                                             float nb[3]) {
+    const float inv = 1.0f / (float)R;
+    const float sb[3] = {(float)x * inv, (float)y * inv, 1.0f - (float)(x + y) * inv};
+    const uint32_t s_start = edge, s_end = (edge + 1u) % 3u, s_opp = (edge + 2u) % 3u;
+    const uint32_t n_start = adj_edge, n_end = (adj_edge + 1u) % 3u, n_opp = (adj_edge + 2u) % 3u;
+    const float outside = sb[s_opp];
+    const uint32_t m_start = flip ? n_end : n_start, m_end = flip ? n_start : n_end;
+    nb[0] = nb[1] = nb[2] = 0.0f;
+    nb[m_start] = sb[s_start] + outside;
+    nb[m_end] = sb[s_end] + outside;
+    nb[n_opp] = -outside;
+    for (int k = 0; k < 3; ++k)
+        if (nb[k] < -1e-5f || nb[k] > 1.0f + 1e-5f) return false;
+    for (int k = 0; k < 3; ++k) nb[k] = maxf(nb[k], 0.0f);
+    const float sum = maxf((nb[0] + nb[1]) + nb[2], 1e-6f);
+    for (int k = 0; k < 3; ++k) nb[k] = nb[k] / sum;
+    return true;
+}
+
+__device__ __forceinline__ void filter_side(const FilterArgs& a, uint32_t front, int ci, int cj, uint4 inst,
+                                            uint2 side, uint2 face, uint32_t prim, f3 cn, bool back) {
+    const uint32_t center = mc_side_texel(front, inst, side, back);
+    const float4 c = __ldg(a.src + center);
+    f3 acc = mk3(c.x, c.y, c.z);
+    float wsum = 1.0f;
+    const int R = (int)face.y;
+    const int off[6][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, -1}, {-1, 1}};
+    for (int t = 0; t < 6; ++t) {
+        const int x = ci + off[t][0], y = cj + off[t][1];
+        if (x >= 0 && y >= 0 && x + y <= R) {
+            const uint32_t ft = mc_address((uint32_t)x, (uint32_t)y, inst.z, face);
+            const f3 v = mc_load(a.src, false, mc_side_texel(ft, inst, side, back));
+            acc = acc + a.neighbor_weight * v;
+            wsum = wsum + a.neighbor_weight;
+            continue;
+        }
+        const uint32_t edge = x < 0 ? 1u : (y < 0 ? 2u : 0u);
+        const uint4 adj4 = __ldg(a.adjacency + inst.x + prim);
+        const uint32_t packed = edge == 0u ? adj4.x : (edge == 1u ? adj4.y : adj4.z);
+        if (packed == 0xffffffffu) continue;
+        const uint32_t adj_face = inst.x + (packed >> 3);
+        float nb[3];
+        if (!map_edge_tap(x, y, face.y, packed & 3u, (packed & 4u) != 0u, edge, nb)) continue;
+        const float4 nn = __ldg(a.normals + adj_face);
+        const float w = a.neighbor_weight * normal_filter_weight(cn, mk3(nn.x, nn.y, nn.z), a.sigma);
+        const uint2 nface = __ldg(a.mc.face_infos + adj_face);
+        const f3 v = mc_sample(a.src, false, nb[0], nb[1], nb[2], inst, nface, side, back);
+        if (w > 0.0f) {
+            acc = acc + w * v;
+            wsum = wsum + w;
+        }
+    }
+    const f3 r = acc / maxf(wsum, 1e-6f);
+    a.dst[center] = make_float4(r.x, r.y, r.z, c.w);
+}
+
+__global__ void __launch_bounds__(128) k_filter_mesh_colors(FilterArgs a) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= a.total_texels) return;
+    const McView& mc = a.mc;
+    uint32_t lo = 0u, hi = mc.instance_count - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(mc.surface_prefix + mid) <= u) lo = mid; else hi = mid - 1u;
+    }
+    const uint32_t local = u - __ldg(mc.surface_prefix + lo);
+    const uint4 inst = __ldg(mc.instance_infos + lo);
+    if (local >= inst.w) return;
+    // mesh_colors_find_face (mesh_colors.slang:272-305)
+    int left = (int)inst.x, right = (int)(inst.x + inst.y) - 1;
+    uint2 face = make_uint2(0u, 1u);
+    uint32_t prim = 0u;
+    bool found = false;
+    while (left <= right) {
+        const int mid = (left + right) / 2;
+        face = __ldg(mc.face_infos + mid);
+        const int loc = (int)local - (int)face.x;
+        const int count = (int)((face.y + 1u) * (face.y + 2u) / 2u);
+        if (loc < 0) right = mid - 1;
+        else if (loc >= count) left = mid + 1;
+        else {
+            prim = (uint32_t)mid - inst.x;
+            found = true;
+            break;
+        }
+    }
+    if (!found) return;
+    const uint2 side = __ldg(mc.side_infos + lo);
+    uint32_t ti, tj;
+    mc_address_to_ij(local - face.x, face.y, &ti, &tj);
+    const float4 n4 = __ldg(a.normals + inst.x + prim);
+    const f3 cn = mk3(n4.x, n4.y, n4.z);
+    const uint32_t front = inst.z + local;
+    filter_side(a, front, (int)ti, (int)tj, inst, side, face, prim, cn, false);
+    if (side.y & 1u) filter_side(a, front, (int)ti, (int)tj, inst, side, face, prim, cn, true);
 }
 
 // accumulator.slang:9-19
@@ -469,6 +600,30 @@ int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* lay, co
                                                            reinterpret_cast<float4*>(out), w, h);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "resolve_mesh_colors launch");
+}
+
+int launch_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* lay, const uint32_t* adjacency,
+                              const float* face_normals, const uint8_t* src, uint8_t* dst, float neighbor_weight,
+                              float sigma, cudaStream_t st) {
+    if (lay->total_surface_texels == 0 || lay->instance_count == 0) return NAN_OK;
+    FilterArgs a;
+    memset(&a, 0, sizeof(a));
+    a.mc.face_infos = reinterpret_cast<const uint2*>(lay->face_infos);
+    a.mc.instance_infos = reinterpret_cast<const uint4*>(lay->instance_infos);
+    a.mc.side_infos = reinterpret_cast<const uint2*>(lay->side_infos);
+    a.mc.surface_prefix = lay->surface_prefix;
+    a.mc.instance_count = lay->instance_count;
+    a.mc.payload_count = lay->payload_count;
+    a.adjacency = reinterpret_cast<const uint4*>(adjacency);
+    a.normals = reinterpret_cast<const float4*>(face_normals);
+    a.src = reinterpret_cast<const float4*>(src);
+    a.dst = reinterpret_cast<float4*>(dst);
+    a.neighbor_weight = neighbor_weight;
+    a.sigma = sigma;
+    a.total_texels = lay->total_surface_texels;
+    k_filter_mesh_colors<<<blocks_for(a.total_texels, 128), 128, 0, st>>>(a);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "filter_mesh_colors launch");
 }
 
 int launch_accumulate(NanContext* ctx, const float* input, float* output, float* history, uint32_t w, uint32_t h,

@@ -229,3 +229,70 @@ class MeshColorsLayout:
         local = np.arange(int(counts.sum()), dtype=np.int64) - np.repeat(self.surface_prefix[:-1].astype(np.int64),
                                                                          counts)
         return np.stack([inst, local.astype(np.uint32)], axis=1)
+
+
+# Edge adjacency of a triangle mesh (mesh_colors_adjacency.py:164-246 of the
+# reference): edge e of a face runs from vertex e to vertex (e + 1) % 3; a
+# manifold edge (used by exactly two faces) links each face to the other as
+# (adjacent face << 3) | adjacent edge | flip << 2, where flip means the two
+# faces traverse the edge in opposite directions; other edges stay ~0.
+ADJACENCY_INVALID = 0xFFFFFFFF
+
+
+def build_triangle_adjacency(indices) -> np.ndarray:
+    """u32[F][4]: packed adjacency of edges 0..2, then ~0."""
+    tri = np.asarray(indices, dtype=np.int64).reshape(-1, 3)
+    n = tri.shape[0]
+    out = np.full((n, 4), ADJACENCY_INVALID, dtype=np.uint32)
+    if n == 0:
+        return out
+    good = (tri[:, 0] != tri[:, 1]) & (tri[:, 1] != tri[:, 2]) & (tri[:, 0] != tri[:, 2])
+    f = np.repeat(np.arange(n), 3)
+    e = np.tile(np.arange(3), n)
+    a = tri[f, e]
+    b = tri[f, (e + 1) % 3]
+    keep = good[f]
+    f, e, a, b = f[keep], e[keep], a[keep], b[keep]
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    order = np.lexsort((e, f, hi, lo))  # by edge key, then in insertion order (face, edge)
+    f, e, a, b, lo, hi = f[order], e[order], a[order], b[order], lo[order], hi[order]
+    starts = np.flatnonzero(np.r_[True, (lo[1:] != lo[:-1]) | (hi[1:] != hi[:-1])])
+    sizes = np.diff(np.r_[starts, lo.size])
+    pair = starts[sizes == 2]
+    first, second = pair, pair + 1
+    ok = f[first] != f[second]
+    first, second = first[ok], second[ok]
+    flip = (a[first] == b[second]) & (b[first] == a[second])
+    fl = np.where(flip, 4, 0).astype(np.int64)
+    out[f[first], e[first]] = ((f[second] << 3) | e[second] | fl).astype(np.uint32)
+    out[f[second], e[second]] = ((f[first] << 3) | e[first] | fl).astype(np.uint32)
+    return out
+
+
+def layout_adjacency(scene_node) -> np.ndarray:
+    """u32[F][4] for every face of the layout (instances in order, mesh-local
+    adjacent face indices), as the filter reads it."""
+    per_mesh = {}
+    rows = []
+    for mesh_id, _, _ in scene_node.instances:
+        if mesh_id not in per_mesh:
+            per_mesh[mesh_id] = build_triangle_adjacency(scene_node.meshes[mesh_id].indices)
+        rows.append(per_mesh[mesh_id])
+    return np.concatenate(rows) if rows else np.zeros((0, 4), np.uint32)
+
+
+def layout_face_normals(scene_node) -> np.ndarray:
+    """f32[F][4]: unit world-space face normals (0 for degenerate faces)."""
+    rows = []
+    for mesh_id, _, transform_id in scene_node.instances:
+        mesh = scene_node.meshes[mesh_id]
+        m = np.asarray(scene_node.transforms[transform_id], dtype=np.float64)
+        p = mesh.vertices[:, 0:3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
+        tri = p[mesh.indices.astype(np.int64)]
+        nrm = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+        length = np.linalg.norm(nrm, axis=1, keepdims=True)
+        nrm = np.where(length > 1e-20, nrm / np.maximum(length, 1e-300), 0.0)
+        r = np.zeros((tri.shape[0], 4), np.float32)
+        r[:, :3] = nrm
+        rows.append(r)
+    return np.concatenate(rows) if rows else np.zeros((0, 4), np.float32)

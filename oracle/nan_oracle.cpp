@@ -1340,6 +1340,117 @@ void resolve_pixel(Tracer<T>& tr, const OracleCamera& cam, uint32_t w, uint32_t 
     out[0] = (float)c.x; out[1] = (float)c.y; out[2] = (float)c.z;
 }
 
+// mesh_colors_sample_irradiance (mesh_colors.slang:365-426) on float32 slots.
+V3<float> mc_sample_slots(const uint8_t* slots, float b0, float b1, float b2, const InstInfo& ii, const FaceInfo& f,
+                          uint32_t side_back, bool back) {
+    auto load = [&](uint32_t front) {
+        uint32_t t = back ? side_back + (front - ii.texel_offset) : front;
+        float c[3];
+        std::memcpy(c, slots + 16 * (size_t)t, 12);
+        return mk<float>(c[0], c[1], c[2]);
+    };
+    uint32_t R = f.resolution;
+    float rf = (float)R;
+    float s0 = saturate(b0) * rf, s1 = saturate(b1) * rf, s2 = saturate(b2) * rf;
+    uint32_t i = std::min((uint32_t)s0, R);
+    uint32_t j = std::min((uint32_t)s1, R - i);
+    float w0 = s0 - std::floor(s0), w1 = s1 - std::floor(s1), w2 = s2 - std::floor(s2);
+    bool upper = std::fabs(((w0 + w1) + w2) - 2.0f) <= 1e-3f;
+    if (upper) {
+        w0 = 1.0f - w0;
+        w1 = 1.0f - w1;
+        w2 = 1.0f - w2;
+    }
+    if ((w0 + w1) + w2 <= 1e-6f || i >= R || j >= R - i) return load(mc_address(i, j, ii, f));
+    if (upper)
+        return (w0 * load(mc_address(i, j + 1, ii, f)) + w1 * load(mc_address(i + 1, j, ii, f))) +
+               w2 * load(mc_address(i + 1, j + 1, ii, f));
+    return (w0 * load(mc_address(i + 1, j, ii, f)) + w1 * load(mc_address(i, j + 1, ii, f))) +
+           w2 * load(mc_address(i, j, ii, f));
+}
+
+// One pass of the one-ring surface filter, mesh_colors_surface_filter.slang:
+// 1-253 (float32 like the shader; acos and exp from the C library).
+void surface_filter_texel(const uint32_t* face_infos, const InstInfo& ii, uint32_t side_back, uint32_t side_flags,
+                          const uint32_t* adjacency, const float* normals, const uint8_t* src, uint8_t* dst,
+                          uint32_t local, float neighbor_weight, float sigma) {
+    FaceInfo f;
+    uint32_t prim;
+    if (!find_face(face_infos, ii, local, &f, &prim)) return;
+    uint32_t ti, tj;
+    address_to_ij(local - f.address, f.resolution, &ti, &tj);
+    const float* cnp = normals + 4 * (size_t)(ii.face_offset + prim);
+    V3<float> cn = mk<float>(cnp[0], cnp[1], cnp[2]);
+    uint32_t front = ii.texel_offset + local;
+    const int off[6][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, -1}, {-1, 1}};
+    for (int side = 0; side < ((side_flags & 1u) ? 2 : 1); ++side) {
+        bool back = side == 1;
+        uint32_t center = back ? side_back + (front - ii.texel_offset) : front;
+        float c[4];
+        std::memcpy(c, src + 16 * (size_t)center, 16);
+        V3<float> acc = mk<float>(c[0], c[1], c[2]);
+        float wsum = 1.0f;
+        int R = (int)f.resolution;
+        for (int t = 0; t < 6; ++t) {
+            int x = (int)ti + off[t][0], y = (int)tj + off[t][1];
+            if (x >= 0 && y >= 0 && x + y <= R) {
+                uint32_t ft = mc_address((uint32_t)x, (uint32_t)y, ii, f);
+                uint32_t tt = back ? side_back + (ft - ii.texel_offset) : ft;
+                float v[3];
+                std::memcpy(v, src + 16 * (size_t)tt, 12);
+                acc = acc + neighbor_weight * mk<float>(v[0], v[1], v[2]);
+                wsum = wsum + neighbor_weight;
+                continue;
+            }
+            uint32_t edge = x < 0 ? 1u : (y < 0 ? 2u : 0u);
+            uint32_t packed = adjacency[4 * (size_t)(ii.face_offset + prim) + edge];
+            if (packed == 0xffffffffu) continue;
+            uint32_t adj_face = ii.face_offset + (packed >> 3);
+            uint32_t adj_edge = packed & 3u;
+            bool flip = (packed & 4u) != 0;
+            // mesh_colors_map_one_edge_tap (mesh_colors.slang:156-203)
+            float inv = 1.0f / (float)f.resolution;
+            float sb[3] = {(float)x * inv, (float)y * inv, 1.0f - (float)(x + y) * inv};
+            uint32_t s_start = edge, s_end = (edge + 1) % 3, s_opp = (edge + 2) % 3;
+            uint32_t n_start = adj_edge, n_end = (adj_edge + 1) % 3, n_opp = (adj_edge + 2) % 3;
+            float outside = sb[s_opp];
+            uint32_t m_start = flip ? n_end : n_start, m_end = flip ? n_start : n_end;
+            float nb[3] = {0.0f, 0.0f, 0.0f};
+            nb[m_start] = sb[s_start] + outside;
+            nb[m_end] = sb[s_end] + outside;
+            nb[n_opp] = -outside;
+            bool ok = true;
+            for (int k = 0; k < 3; ++k)
+                if (nb[k] < -1e-5f || nb[k] > 1.0f + 1e-5f) ok = false;
+            if (!ok) continue;
+            for (int k = 0; k < 3; ++k) nb[k] = std::max(nb[k], 0.0f);
+            float sum = std::max((nb[0] + nb[1]) + nb[2], 1e-6f);
+            for (int k = 0; k < 3; ++k) nb[k] = nb[k] / sum;
+            // mesh_colors_normal_filter_weight (mesh_colors.slang:205-216)
+            const float* np_ = normals + 4 * (size_t)adj_face;
+            float cosine = std::min(std::max(dot(cn, mk<float>(np_[0], np_[1], np_[2])), 0.0f), 1.0f);
+            float nw;
+            if (sigma <= 1e-6f) {
+                nw = cosine >= 1.0f - 1e-6f ? 1.0f : 0.0f;
+            } else {
+                float na = std::acos(cosine) / sigma;
+                nw = std::exp(-0.5f * na * na);
+            }
+            float w = neighbor_weight * nw;
+            FaceInfo nf{face_infos[2 * adj_face], face_infos[2 * adj_face + 1]};
+            V3<float> v = mc_sample_slots(src, nb[0], nb[1], nb[2], ii, nf, side_back, back);
+            if (w > 0.0f) {
+                acc = acc + w * v;
+                wsum = wsum + w;
+            }
+        }
+        V3<float> r = acc / std::max(wsum, 1e-6f);
+        float outv[3] = {r.x, r.y, r.z};
+        std::memcpy(dst + 16 * (size_t)center, outv, 12);
+        std::memcpy(dst + 16 * (size_t)center + 12, &c[3], 4);
+    }
+}
+
 template <class F> void parallel_for(int count, int threads, F&& fn) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::max(1, std::min(threads, count));
@@ -1635,6 +1746,23 @@ int oracle_resolve_mesh_colors(void* sp, const OracleLighting* lighting, const O
             resolve_pixel<float>(tr, *camera, width, height, px, py, face_infos, instance_infos, side_infos,
                                  instance_count, colors, packed != 0, out + 4 * (size_t)i);
         }
+    });
+    return 0;
+}
+
+int oracle_filter_mesh_colors(const uint32_t* face_infos, const uint32_t* instance_infos, const uint32_t* side_infos,
+                              uint32_t instance_count, const uint32_t* adjacency, const float* face_normals,
+                              const uint8_t* source, uint8_t* destination, float neighbor_weight, float sigma,
+                              int threads) {
+    std::vector<std::pair<uint32_t, uint32_t>> units;
+    for (uint32_t k = 0; k < instance_count; ++k)
+        for (uint32_t t = 0; t < instance_infos[4 * k + 3]; ++t) units.emplace_back(k, t);
+    parallel_for((int)units.size(), threads, [&](int u, int) {
+        uint32_t k = units[u].first;
+        InstInfo ii{instance_infos[4 * k], instance_infos[4 * k + 1], instance_infos[4 * k + 2],
+                    instance_infos[4 * k + 3]};
+        surface_filter_texel(face_infos, ii, side_infos[2 * k], side_infos[2 * k + 1], adjacency, face_normals,
+                             source, destination, units[u].second, neighbor_weight, sigma);
     });
     return 0;
 }

@@ -141,6 +141,15 @@ int oracle_resolve_mesh_colors(void* scene, const OracleLighting* lighting,
                                const void* colors, int packed, int precision, int threads,
                                float* out);
 
+/* One pass of the Mesh Colors one-ring surface filter over every texel of
+ * every instance (mesh_colors_surface_filter.slang:1-253): source and
+ * destination are 16-byte slot buffers. */
+int oracle_filter_mesh_colors(const uint32_t* face_infos, const uint32_t* instance_infos,
+                              const uint32_t* side_infos, uint32_t instance_count,
+                              const uint32_t* adjacency, const float* face_normals,
+                              const uint8_t* source, uint8_t* destination,
+                              float neighbor_weight, float normal_sigma_radians, int threads);
+
 /* Area-light table of the screen tracer's NEE option (lighting flag bit 1),
  * the layout of nan_ctx_set_area_lights. */
 void oracle_scene_set_area_lights(void* scene, const float* lights, int count, float power);

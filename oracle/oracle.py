@@ -110,11 +110,27 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes_independent.argtypes = l.oracle_trace_probes.argtypes
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
+    l.oracle_filter_mesh_colors.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, i]
     l.oracle_resolve_mesh_colors.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, vp, vp, u32, vp, i, i, i, vp]
     l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
 
 
 # ---- scalar helpers --------------------------------------------------------
+def filter_mesh_colors(face_infos, instance_infos, side_infos, adjacency, face_normals, source, neighbor_weight,
+                       normal_sigma_radians, threads=0):
+    """One surface-filter pass; source and the returned slots are uint32 [P, 4]."""
+    fi = np.ascontiguousarray(face_infos, dtype=np.uint32).reshape(-1, 2)
+    ii = np.ascontiguousarray(instance_infos, dtype=np.uint32).reshape(-1, 4)
+    si = np.ascontiguousarray(side_infos, dtype=np.uint32).reshape(-1, 2)
+    adj = np.ascontiguousarray(adjacency, dtype=np.uint32).reshape(-1, 4)
+    nrm = np.ascontiguousarray(face_normals, dtype=np.float32).reshape(-1, 4)
+    src = np.ascontiguousarray(source).view(np.uint32).reshape(-1, 4)
+    dst = src.copy()
+    lib().oracle_filter_mesh_colors(_p(fi), _p(ii), _p(si), ii.shape[0], _p(adj), _p(nrm), _p(src), _p(dst),
+                                    float(neighbor_weight), float(normal_sigma_radians), threads)
+    return dst
+
+
 
 def rng_sequence(x: int, y: int, sample_index: int, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.float32)
