@@ -290,6 +290,32 @@ NAN_B200_API int nan_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc
                                         float neighbor_weight, float normal_sigma_radians,
                                         void* stream);
 
+/* SurfaceProbePrtBaker.execute (surface_probe_prt.py:62-128;
+ * surface_probe_prt_baker.slang:169-371): one iteration of the PRT L2 field
+ * baker over probes [probe_begin, probe_end). values f32[N][9][3] (SH L2
+ * transport), static_source f32[N][3] (emission and sun along the paths),
+ * sample_counts u32[N], self_hits u32[N], radial u32[N][16]. */
+NAN_B200_API int nan_trace_probes_prt(NanContext* ctx, float* values, uint32_t* sample_counts,
+                                      uint32_t* self_hits, uint32_t* radial, float* static_source,
+                                      const uint8_t* probes, uint32_t probe_count,
+                                      const uint8_t* probe_instances, uint32_t probe_instance_count,
+                                      uint32_t iteration, uint32_t samples_per_probe,
+                                      uint32_t max_bounces, int reset, const NanLighting* lighting,
+                                      uint32_t probe_begin, uint32_t probe_end, void* stream);
+
+/* SurfaceProbePrtEvaluator.execute (surface_probe_prt.py:131-248;
+ * surface_probe_prt_evaluate.slang:20-103), first pass: the lighting's escape
+ * radiance projected on SH L2 with sample_count quasi-random sphere
+ * directions; lighting_sh f32[9][4] (rgb, 0), 16-byte aligned. */
+NAN_B200_API int nan_prt_project_lighting(NanContext* ctx, float* lighting_sh, uint32_t sample_count,
+                                          const NanLighting* lighting, void* stream);
+/* Second pass: out_values f32[N][3] = max(static_source + sum_c values[c] *
+ * lighting_sh[c], 0) (static only where sample_counts is 0); out_sample_counts
+ * copies sample_counts. */
+NAN_B200_API int nan_prt_evaluate(NanContext* ctx, const float* values, const uint32_t* sample_counts,
+                                  const float* static_source, const float* lighting_sh, float* out_values,
+                                  uint32_t* out_sample_counts, uint32_t probe_count, void* stream);
+
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out,

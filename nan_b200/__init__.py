@@ -30,6 +30,8 @@ from .scene import Device, Lighting, Scene
 from .scene_node import Material, Mesh, SceneNode, make_transform
 from .surface_probe_fields import (DIFFUSE_IRRADIANCE_ATTACHMENTS, DIFFUSE_IRRADIANCE_RGB_FIELD,
                                    SurfaceProbeAttachments, SurfaceProbeFieldBuffers, SurfaceProbeRuntimeBuffers)
+from .surface_probe_prt import (SurfaceProbePrtBaker, SurfaceProbePrtEvaluator, evaluate_prt_l2_rgb,
+                               surface_probe_sh_l2_basis)
 from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker, SurfaceProbePathTracer
 from .surface_probe_resources import SurfaceProbeGpuGeometry
 from .texture_space_path_tracer import TextureSpacePathTracer
@@ -38,7 +40,7 @@ __all__ = [
     "Accumulator", "CachedPathTracer", "Camera", "Device", "HaltonSamplePattern", "Lighting", "Material", "Mesh", "MeshColorsLayout",
     "MeshColorsRGB9E5Packer", "MeshColorsResolve", "MeshColorsSurfaceFilter", "PathTracer", "ProbeBatch", "RadianceCache", "RenderData", "Scene", "SceneNode", "SurfaceProbeAttachments",
     "SurfaceProbeDiffuseIrradianceBaker", "SurfaceProbeFieldBuffers", "SurfaceProbeGpuGeometry",
-    "SurfaceProbePathTracer", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "address_to_ij",
+    "SurfaceProbePathTracer", "SurfaceProbePrtBaker", "SurfaceProbePrtEvaluator", "evaluate_prt_l2_rgb", "surface_probe_sh_l2_basis", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "address_to_ij",
     "barycentric_at", "colors_per_patch", "halton", "ij_to_address", "make_transform",
     "DIFFUSE_IRRADIANCE_ATTACHMENTS", "DIFFUSE_IRRADIANCE_RGB_FIELD", "MESH_COLORS_INVALID_OFFSET",
     "MESH_COLORS_PAYLOAD_SIZE", "MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED",

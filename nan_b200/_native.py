@@ -254,6 +254,10 @@ EXPORTS = {
                                      ctypes.POINTER(NanCamera), ctypes.POINTER(NanLighting), _VP]),
     "nan_filter_mesh_colors": (_I, [_VP, ctypes.POINTER(NanMeshColorsDesc), _VP, _VP, _VP, _VP, ctypes.c_float,
                                     ctypes.c_float, _VP]),
+    "nan_trace_probes_prt": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, _I,
+                                  ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
+    "nan_prt_project_lighting": (_I, [_VP, _VP, _U32, ctypes.POINTER(NanLighting), _VP]),
+    "nan_prt_evaluate": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),
     "nan_trace_screen_cached": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
                                      ctypes.POINTER(NanLighting), ctypes.POINTER(NanCachedFrame), _VP]),

@@ -370,6 +370,48 @@ NAN_B200_API int nan_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc
                                                neighbor_weight, normal_sigma_radians, as_stream(stream));
 }
 
+NAN_B200_API int nan_trace_probes_prt(NanContext* ctx, float* values, uint32_t* sample_counts, uint32_t* self_hits,
+                                      uint32_t* radial, float* static_source, const uint8_t* probes,
+                                      uint32_t probe_count, const uint8_t* probe_instances,
+                                      uint32_t probe_instance_count, uint32_t iteration, uint32_t samples_per_probe,
+                                      uint32_t max_bounces, int reset, const NanLighting* lighting,
+                                      uint32_t probe_begin, uint32_t probe_end, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = need_scene(ctx);
+    if (rc) return rc;
+    if (probe_count && (!values || !sample_counts || !self_hits || !radial || !static_source || !probes ||
+                        !probe_instances || !lighting))
+        return invalid("null argument");
+    if (!aligned16(probes) || !aligned16(probe_instances)) return invalid("probe records must be 16-byte aligned");
+    return nan_host::launch_trace_probes_prt(ctx, values, sample_counts, self_hits, radial, static_source, probes,
+                                             probe_count, probe_instances, probe_instance_count, iteration,
+                                             samples_per_probe, max_bounces, reset, lighting, probe_begin,
+                                             probe_end, as_stream(stream));
+}
+
+NAN_B200_API int nan_prt_project_lighting(NanContext* ctx, float* lighting_sh, uint32_t sample_count,
+                                          const NanLighting* lighting, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!lighting_sh || !lighting) return invalid("null argument");
+    if (!aligned16(lighting_sh)) return invalid("lighting_sh must be 16-byte aligned");
+    return nan_host::launch_prt_project_lighting(ctx, lighting_sh, sample_count, lighting, as_stream(stream));
+}
+
+NAN_B200_API int nan_prt_evaluate(NanContext* ctx, const float* values, const uint32_t* sample_counts,
+                                  const float* static_source, const float* lighting_sh, float* out_values,
+                                  uint32_t* out_sample_counts, uint32_t probe_count, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (probe_count && (!values || !sample_counts || !static_source || !lighting_sh || !out_values ||
+                        !out_sample_counts))
+        return invalid("null argument");
+    if (!aligned16(lighting_sh)) return invalid("lighting_sh must be 16-byte aligned");
+    return nan_host::launch_prt_evaluate(ctx, values, sample_counts, static_source, lighting_sh, out_values,
+                                         out_sample_counts, probe_count, as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -162,6 +162,15 @@ int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout,
 int launch_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const uint32_t* adjacency,
                               const float* face_normals, const uint8_t* src, uint8_t* dst, float neighbor_weight,
                               float sigma, cudaStream_t st);
+int launch_trace_probes_prt(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits, uint32_t* radial,
+                            float* static_source, const uint8_t* probes, uint32_t probe_count,
+                            const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
+                            uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light, uint32_t begin,
+                            uint32_t end, cudaStream_t st);
+int launch_prt_project_lighting(NanContext* ctx, float* sh, uint32_t samples, const NanLighting* light,
+                                cudaStream_t st);
+int launch_prt_evaluate(NanContext* ctx, const float* values, const uint32_t* counts, const float* static_source,
+                        const float* sh, float* out, uint32_t* out_counts, uint32_t n, cudaStream_t st);
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count,
                        cudaStream_t stream);
 

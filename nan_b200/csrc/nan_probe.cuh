@@ -180,4 +180,145 @@ __device__ __forceinline__ bool probe_unit(const SceneView& s, const LightParams
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// PRT L2 field baker (surface_probe_prt_baker.slang:169-371): per probe, the
+// transport of escaping light projected on the real SH L2 basis
+// (surface_probe_sh.slang:5-21), and an RGB static source (emission and sun
+// NEE along the paths), kept as running means; self-hit and radial moments as
+// in the irradiance baker. One RNG stream per probe, samples in sequence.
+// ---------------------------------------------------------------------------
+struct PrtOut {
+    float* values;         // f32[N][9][3]
+    uint32_t* counts;
+    uint32_t* self_hits;
+    uint32_t* radial;
+    float* static_source;  // f32[N][3]
+};
+
+__device__ __forceinline__ float sh_l2_basis(uint32_t c, f3 dir) {
+    const f3 d = normalize3(dir);
+    const float x = d.x, y = d.y, z = d.z;
+    switch (c) {
+        case 0: return 0.2820947918f;
+        case 1: return 0.4886025119f * y;
+        case 2: return 0.4886025119f * z;
+        case 3: return 0.4886025119f * x;
+        case 4: return 1.0925484306f * x * y;
+        case 5: return 1.0925484306f * y * z;
+        case 6: return 0.3153915653f * (3.0f * y * y - 1.0f);
+        case 7: return 1.0925484306f * x * z;
+        default: return 0.5462742153f * (x * x - z * z);
+    }
+}
+
+template <class Tr>
+__device__ __forceinline__ bool probe_prt_unit(const SceneView& s, const LightParams& L, const PrtOut& out,
+                                               const float4* __restrict__ probes, const float4* __restrict__ pinst,
+                                               uint32_t probe_instance_count, uint32_t iteration, uint32_t spp,
+                                               uint32_t max_bounces, int reset, uint32_t p, RayTally& tally) {
+    ProbeSite site;
+    if (!probe_site(s, probes, pinst, probe_instance_count, p, &site)) return false;
+    const uint32_t n = max(spp, 1u);
+    Rng rng(p, site.inst, iteration * n);
+    const Shading& sd = site.sd;
+    const float kr = site.kr;
+    const uint32_t prev_iter = reset ? 0u : out.counts[p];
+    if (reset)
+        for (int t = 0; t < 16; ++t) out.radial[16u * p + (uint32_t)t] = 0u;
+    f3 transport[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) transport[c] = mk3(0.0f, 0.0f, 0.0f);
+    f3 stat = mk3(0.0f, 0.0f, 0.0f);
+    uint32_t self_total = 0u;
+    uint32_t local_counts[16];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) local_counts[t] = 0u;
+    for (uint32_t k = 0; k < n; ++k) {
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 dir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf <= 1e-6f) continue;
+        f3 lt[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) lt[c] = mk3(0.0f, 0.0f, 0.0f);
+        f3 o = sd.origin_front;
+        f3 d = Frame(site.normal).to_global(dir);
+        f3 thp = mk3(1.0f, 1.0f, 1.0f), st = mk3(0.0f, 0.0f, 0.0f);
+        uint32_t src_inst = site.inst, src_prim = site.prim;
+        float src_off = len3(o - sd.position);
+        uint32_t self_hits = 0u;
+        const float radial_max = 2.0f * kr;
+        float first_hit = 2.0f * kr;
+        // trace_prt_transport (surface_probe_prt_baker.slang:164-230)
+        for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+            tally.extend++;
+            const HitInfo hit = Tr::closest(s, o, d, 0.0f, L.t_max);
+            if (!hit.valid) {
+                if (bounce == 0u) first_hit = radial_max;
+#pragma unroll
+                for (uint32_t c = 0; c < 9; ++c) lt[c] = lt[c] + thp * sh_l2_basis(c, d);
+                break;
+            }
+            if (bounce == 0u) first_hit = minf(hit.t, radial_max);
+            const uint2 ref = __ldg(s.tri_refs + hit.flat);
+            const bool same_prim = ref.x == src_inst && ref.y == src_prim;
+            const float thr = maxf(4.0f * src_off, 1e-6f);
+            const bool adjacent = ref.x == src_inst && hit.t <= thr;
+            if (same_prim || adjacent) self_hits += 1u;
+            const Shading hs = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -d);
+            st = st + thp * hs.emissive;
+            const float u0 = rng.next_1d(), u1 = rng.next_1d();
+            st = st + thp * sun_nee<Tr>(s, L, hs, u0, u1, tally);
+            const float f0 = rng.next_1d(), f1 = rng.next_1d();
+            float spdf;
+            const f3 sdir = cosine_sample_hemisphere(f0, f1, &spdf);
+            if (spdf <= 1e-6f) break;
+            const f3 f = hs.diffuse * kInvPi;
+            thp = thp * ((f * fabsf(sdir.z)) / spdf);
+            const f3 next_origin = hs.origin_front;
+            d = Frame(normalize3(hs.face_normal)).to_global(sdir);
+            o = next_origin;
+            src_inst = ref.x;
+            src_prim = ref.y;
+            src_off = len3(next_origin - hs.position);
+        }
+        self_total += self_hits;
+        const float w = fabsf(dir.z) / pdf;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) transport[c] = transport[c] + w * lt[c];
+        stat = stat + w * st;
+        const uint32_t texel = radial_texel(dir);
+        local_counts[texel] += 1u;
+        accumulate_radial_moment(out.radial, p, texel, first_hit / maxf(kr, 1e-6f), prev_iter, local_counts[texel],
+                                 spp);
+    }
+    const float inv = 1.0f / (float)n;
+    // store_accumulated_prt (surface_probe_prt_baker.slang:43-74)
+    const uint32_t prev = reset ? 0u : out.counts[p];
+    const float weight = 1.0f / (float)(prev + 1u);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        const f3 t = transport[c] * inv;
+        float* v = out.values + 27u * p + 3u * (uint32_t)c;
+        const f3 pv = prev == 0u ? mk3(0.0f, 0.0f, 0.0f) : mk3(v[0], v[1], v[2]);
+        const f3 r = pv + weight * (t - pv);
+        v[0] = r.x;
+        v[1] = r.y;
+        v[2] = r.z;
+    }
+    {
+        const f3 t = stat * inv;
+        float* v = out.static_source + 3u * p;
+        const f3 pv = prev == 0u ? mk3(0.0f, 0.0f, 0.0f) : mk3(v[0], v[1], v[2]);
+        const f3 r = pv + weight * (t - pv);
+        v[0] = r.x;
+        v[1] = r.y;
+        v[2] = r.z;
+    }
+    out.counts[p] = min(prev + 1u, 65535u);
+    const uint32_t prev_self = reset ? 0u : out.self_hits[p];
+    out.self_hits[p] = prev_self + self_total;
+    return true;
+}
+
 }  // namespace nbd

@@ -500,6 +500,68 @@ __global__ void __launch_bounds__(128) k_trace_probes(SceneView s, LightingRaw l
         flush_tally(counters, tally, 1u, max(spp, 1u));
 }
 
+__global__ void __launch_bounds__(128) k_trace_probes_prt(SceneView s, LightingRaw lraw, PrtOut out,
+                                                          const float4* __restrict__ probes,
+                                                          const float4* __restrict__ pinst, uint32_t probe_count,
+                                                          uint32_t probe_instance_count, uint32_t iteration,
+                                                          uint32_t spp, uint32_t max_bounces, int reset,
+                                                          uint32_t begin, uint32_t end, unsigned long long* counters) {
+    const uint32_t p = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= end || p >= probe_count) return;
+    const LightParams L = make_light(lraw);
+    RayTally tally{0u, 0u};
+    if (probe_prt_unit<DefaultTracer>(s, L, out, probes, pinst, probe_instance_count, iteration, spp, max_bounces,
+                                      reset, p, tally))
+        flush_tally(counters, tally, 1u, max(spp, 1u));
+}
+
+// ---------------------------------------------------------------------------
+// PRT evaluation (surface_probe_prt_evaluate.slang:20-103). The lighting is
+// projected on the SH L2 basis by a quasi-random sphere rule: sample i of n at
+// y = 1 - 2 (i + 0.5) / n and phi = 2 pi radical_inverse(i); the radiance a
+// path that escapes meets is the sky term. One thread per coefficient, the
+// samples summed in order. Evaluation is static + sum_c T_c * L_c, clamped
+// at 0, for probes with at least one sample.
+// ---------------------------------------------------------------------------
+__global__ void k_prt_project_lighting(LightingRaw lraw, float4* __restrict__ sh, uint32_t n) {
+    const uint32_t c = threadIdx.x;
+    if (c >= 9u) return;
+    const LightParams L = make_light(lraw);
+    n = max(n, 1u);
+    f3 acc = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float u = (static_cast<float>(i) + 0.5f) / static_cast<float>(n);
+        const float v = static_cast<float>(__brev(i)) * 2.3283064365386963e-10f;
+        const float y = 1.0f - 2.0f * u;
+        const float r = sqrtf(fmaxf(1.0f - y * y, 0.0f));
+        float sn, cs;
+        nan_sincos(kTwoPi * v, &sn, &cs);
+        acc = acc + L.sky * sh_l2_basis(c, mk3(r * cs, y, r * sn));
+    }
+    acc = acc * ((4.0f * kPi) / static_cast<float>(n));
+    sh[c] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+}
+
+__global__ void k_prt_evaluate(const float* __restrict__ values, const uint32_t* __restrict__ counts,
+                               const float* __restrict__ static_source, const float4* __restrict__ sh,
+                               float* __restrict__ out, uint32_t* __restrict__ out_counts, uint32_t n) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t count = counts[p];
+    f3 e = mk3(static_source[3 * p], static_source[3 * p + 1], static_source[3 * p + 2]);
+    if (count > 0u) {
+        const float* t = values + 27ull * p;
+        for (int c = 0; c < 9; ++c) {
+            const float4 l = sh[c];
+            e = e + mk3(t[3 * c] * l.x, t[3 * c + 1] * l.y, t[3 * c + 2] * l.z);
+        }
+    }
+    out[3 * p] = fmaxf(e.x, 0.0f);
+    out[3 * p + 1] = fmaxf(e.y, 0.0f);
+    out[3 * p + 2] = fmaxf(e.z, 0.0f);
+    out_counts[p] = count;
+}
+
 // ---------------------------------------------------------------------------
 // RGB9E5: mesh_colors.slang:218-253 and mesh_colors_rgb9e5_pack.slang:7-16.
 // floor(log2(max)) is taken exactly from the binary exponent.
@@ -671,6 +733,38 @@ int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32
         ctx->d_counters);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "trace_probes launch");
+}
+
+int launch_trace_probes_prt(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits, uint32_t* radial,
+                            float* static_source, const uint8_t* probes, uint32_t probe_count,
+                            const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,
+                            uint32_t spp, uint32_t max_bounces, int reset, const NanLighting* light, uint32_t begin,
+                            uint32_t end, cudaStream_t st) {
+    end = std::min(end, probe_count);
+    if (end <= begin) return NAN_OK;
+    PrtOut o{values, counts, self_hits, radial, static_source};
+    k_trace_probes_prt<<<blocks_for(end - begin, 128), 128, 0, st>>>(
+        scene_view(ctx), to_raw(light), o, reinterpret_cast<const float4*>(probes),
+        reinterpret_cast<const float4*>(probe_instances), probe_count, probe_instance_count, iteration, spp,
+        max_bounces, reset, begin, end, ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "trace_probes_prt launch");
+}
+
+int launch_prt_project_lighting(NanContext* ctx, float* sh, uint32_t samples, const NanLighting* light,
+                                cudaStream_t st) {
+    k_prt_project_lighting<<<1, 32, 0, st>>>(to_raw(light), reinterpret_cast<float4*>(sh), samples);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "prt_project_lighting launch");
+}
+
+int launch_prt_evaluate(NanContext* ctx, const float* values, const uint32_t* counts, const float* static_source,
+                        const float* sh, float* out, uint32_t* out_counts, uint32_t n, cudaStream_t st) {
+    if (n == 0) return NAN_OK;
+    k_prt_evaluate<<<blocks_for(n, 256), 256, 0, st>>>(values, counts, static_source,
+                                                       reinterpret_cast<const float4*>(sh), out, out_counts, n);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "prt_evaluate launch");
 }
 
 int launch_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, cudaStream_t st) {

@@ -1451,6 +1451,142 @@ void surface_filter_texel(const uint32_t* face_infos, const InstInfo& ii, uint32
     }
 }
 
+// PRT L2 field baker, surface_probe_prt_baker.slang:169-371, with the real
+// SH L2 basis of surface_probe_sh.slang:5-21.
+template <class T> T sh_l2_basis(uint32_t c, V3<T> dir) {
+    V3<T> d = normalize(dir);
+    T x = d.x, y = d.y, z = d.z;
+    switch (c) {
+        case 0: return T(0.2820947918f);
+        case 1: return T(0.4886025119f) * y;
+        case 2: return T(0.4886025119f) * z;
+        case 3: return T(0.4886025119f) * x;
+        case 4: return T(1.0925484306f) * x * y;
+        case 5: return T(1.0925484306f) * y * z;
+        case 6: return T(0.3153915653f) * (T(3) * y * y - T(1));
+        case 7: return T(1.0925484306f) * x * z;
+        default: return T(0.5462742153f) * (x * x - z * z);
+    }
+}
+
+template <class T>
+void probe_prt_unit(Tracer<T>& tr, ProbeBuffers& b, float* static_source, const uint8_t* probes,
+                    const uint8_t* pinst, uint32_t probe, uint32_t iteration, uint32_t spp, uint32_t max_bounces,
+                    bool reset) {
+    const uint8_t* rec = probes + 48 * (size_t)probe;
+    float nrm[4];
+    uint32_t meta[4];
+    std::memcpy(nrm, rec + 16, 16);
+    std::memcpy(meta, rec + 32, 16);
+    uint32_t inst = meta[3] >> 8;
+    float params[4];
+    std::memcpy(params, pinst + 48 * (size_t)inst + 32, 16);
+    float bx, by;
+    std::memcpy(&bx, &meta[1], 4);
+    std::memcpy(&by, &meta[2], 4);
+    uint32_t prim = meta[0];
+    uint32_t n = std::max(spp, 1u);
+    Rng rng(probe, inst, iteration * n);
+    V3<T> view = normalize(mk<T>(T(nrm[0]), T(nrm[1]), T(nrm[2])));
+    T kr = vmax(T(params[0]), T(1e-6f));
+    Shading<T> sd = shading_data<T>(tr.s, inst, prim, T(bx), T(by), view);
+    V3<T> transport[9];
+    for (auto& t : transport) t = mk<T>(0, 0, 0);
+    V3<T> stat = mk<T>(0, 0, 0);
+    uint32_t self_total = 0;
+    uint32_t prev_iter = reset ? 0u : b.counts[probe];
+    uint32_t local_counts[16] = {0};
+    if (reset)
+        for (int t = 0; t < 16; ++t) b.radial[16 * (size_t)probe + t] = 0u;
+    for (uint32_t k = 0; k < n; ++k) {
+        T e0 = T(rng.next_1d()), e1 = T(rng.next_1d());
+        V3<T> dir;
+        T pdf;
+        cosine_sample_hemisphere<T>(e0, e1, &dir, &pdf);
+        if (pdf <= T(1e-6f)) continue;
+        V3<T> lt[9];
+        for (auto& t : lt) t = mk<T>(0, 0, 0);
+        ProbePath<T> p;
+        V3<T> origin = sd.origin_front;
+        p.o = origin;
+        p.d = Frame<T>(normalize(sd.face_normal)).to_global(dir);
+        p.thp = mk<T>(1, 1, 1);
+        p.rad = mk<T>(0, 0, 0);  // the static source of this path
+        p.src_inst = inst;
+        p.src_prim = prim;
+        p.src_off = length(origin - sd.position);
+        p.self_hits = 0;
+        p.first_hit = T(2) * kr;
+        p.radial_max = T(2) * kr;
+        for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
+            HitRec hit = tr.closest(p.o, p.d, T(0), tr.L.t_max);
+            if (!hit.valid) {
+                if (bounce == 0u) p.first_hit = p.radial_max;
+                for (uint32_t c = 0; c < 9; ++c) lt[c] = lt[c] + p.thp * sh_l2_basis<T>(c, p.d);
+                break;
+            }
+            T ht = T(hit.t);
+            if (bounce == 0u) p.first_hit = vmin(ht, p.radial_max);
+            uint32_t hi = tr.s.flat_instance[hit.flat], hp = tr.s.flat_prim[hit.flat];
+            bool same_prim = hi == p.src_inst && hp == p.src_prim;
+            T thr = vmax(T(4) * p.src_off, T(1e-6f));
+            bool adjacent = hi == p.src_inst && ht <= thr;
+            if (same_prim || adjacent) p.self_hits += 1u;
+            Shading<T> hs = shading_data<T>(tr.s, hi, hp, T(hit.b1), T(hit.b2), -p.d);
+            p.rad = p.rad + p.thp * hs.emissive;
+            T u0 = T(rng.next_1d()), u1 = T(rng.next_1d());
+            p.rad = p.rad + p.thp * tr.sun_nee(hs, u0, u1);
+            T f0 = T(rng.next_1d()), f1 = T(rng.next_1d());
+            V3<T> sdir;
+            T spdf;
+            cosine_sample_hemisphere<T>(f0, f1, &sdir, &spdf);
+            if (spdf <= T(1e-6f)) break;
+            V3<T> f = hs.diffuse * Consts<T>::INV_PI;
+            p.thp = p.thp * ((f * std::fabs(sdir.z)) / spdf);
+            V3<T> next_origin = hs.origin_front;
+            p.d = Frame<T>(normalize(hs.face_normal)).to_global(sdir);
+            p.o = next_origin;
+            p.src_inst = hi;
+            p.src_prim = hp;
+            p.src_off = length(next_origin - hs.position);
+        }
+        self_total += p.self_hits;
+        T w = std::fabs(dir.z) / pdf;
+        for (int c = 0; c < 9; ++c) transport[c] = transport[c] + w * lt[c];
+        stat = stat + w * p.rad;
+        float u, v;
+        hemi_oct_encode((float)dir.x, (float)dir.y, (float)dir.z, &u, &v);
+        uint32_t texel = radial_texel_index(u, v);
+        local_counts[texel] += 1u;
+        accumulate_radial_moment<T>(b, probe, texel, p.first_hit / vmax(kr, T(1e-6f)), prev_iter,
+                                    local_counts[texel], spp);
+    }
+    T inv = T(1) / T((float)n);
+    uint32_t prev = reset ? 0u : b.counts[probe];
+    float weight = 1.0f / (float)(prev + 1u);
+    for (int c = 0; c < 9; ++c) {
+        V3<T> t = transport[c] * inv;
+        float* v = b.values + 27 * (size_t)probe + 3 * c;
+        float tv[3] = {(float)t.x, (float)t.y, (float)t.z};
+        for (int ch = 0; ch < 3; ++ch) {
+            float pv = prev == 0u ? 0.0f : v[ch];
+            v[ch] = pv + weight * (tv[ch] - pv);
+        }
+    }
+    {
+        V3<T> t = stat * inv;
+        float* v = static_source + 3 * (size_t)probe;
+        float tv[3] = {(float)t.x, (float)t.y, (float)t.z};
+        for (int ch = 0; ch < 3; ++ch) {
+            float pv = prev == 0u ? 0.0f : v[ch];
+            v[ch] = pv + weight * (tv[ch] - pv);
+        }
+    }
+    b.counts[probe] = std::min(prev + 1u, 65535u);
+    uint32_t prev_self = reset ? 0u : b.self_hits[probe];
+    b.self_hits[probe] = prev_self + self_total;
+}
+
 template <class F> void parallel_for(int count, int threads, F&& fn) {
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     threads = std::max(1, std::min(threads, count));
@@ -1765,6 +1901,76 @@ int oracle_filter_mesh_colors(const uint32_t* face_infos, const uint32_t* instan
                              source, destination, units[u].second, neighbor_weight, sigma);
     });
     return 0;
+}
+
+int oracle_trace_probes_prt(void* sp, const OracleLighting* lighting, float* values, uint32_t* sample_counts,
+                            uint32_t* self_hits, uint32_t* radial, float* static_source, const uint8_t* probes,
+                            uint32_t probe_count, const uint8_t* probe_instances, const uint32_t* units,
+                            int unit_count, uint32_t iteration, uint32_t spp, uint32_t max_bounces, int reset,
+                            int precision, int threads) {
+    Scene* s = static_cast<Scene*>(sp);
+    ProbeBuffers b{values, sample_counts, self_hits, radial};
+    parallel_for(unit_count, threads, [&](int u, int) {
+        uint32_t p = units[u];
+        if (p >= probe_count) return;
+        if (precision == ORACLE_F64) {
+            Tracer<double> tr(*s, *lighting);
+            probe_prt_unit<double>(tr, b, static_source, probes, probe_instances, p, iteration, spp, max_bounces,
+                                   reset != 0);
+        } else {
+            Tracer<float> tr(*s, *lighting);
+            probe_prt_unit<float>(tr, b, static_source, probes, probe_instances, p, iteration, spp, max_bounces,
+                                  reset != 0);
+        }
+    });
+    return 0;
+}
+
+// PRT evaluation, surface_probe_prt_evaluate.slang:20-103: SH L2 projection
+// of the escape radiance (the sky term) by the quasi-random sphere rule
+// y = 1 - 2 (i + 0.5) / n, phi = 2 pi radical_inverse(i), summed in order;
+// then static + sum_c T_c L_c clamped at 0 per probe.
+static uint32_t reverse_bits32(uint32_t b) {
+    b = (b << 16u) | (b >> 16u);
+    b = ((b & 0x55555555u) << 1u) | ((b & 0xAAAAAAAAu) >> 1u);
+    b = ((b & 0x33333333u) << 2u) | ((b & 0xCCCCCCCCu) >> 2u);
+    b = ((b & 0x0F0F0F0Fu) << 4u) | ((b & 0xF0F0F0F0u) >> 4u);
+    b = ((b & 0x00FF00FFu) << 8u) | ((b & 0xFF00FF00u) >> 8u);
+    return b;
+}
+
+void oracle_prt_project_lighting(const OracleLighting* lighting, uint32_t sample_count, float* sh) {
+    LightCtx<float> L(*lighting);
+    const uint32_t n = std::max(sample_count, 1u);
+    for (uint32_t c = 0; c < 9; ++c) {
+        V3<float> acc = mk<float>(0.0f, 0.0f, 0.0f);
+        for (uint32_t i = 0; i < n; ++i) {
+            const float u = ((float)i + 0.5f) / (float)n;
+            const float v = (float)reverse_bits32(i) * 2.3283064365386963e-10f;
+            const float y = 1.0f - 2.0f * u;
+            const float r = std::sqrt(std::fmax(1.0f - y * y, 0.0f));
+            float sn, cs;
+            own_sincos(6.28318530717958647692f * v, &sn, &cs);
+            acc = acc + L.sky * sh_l2_basis<float>(c, mk<float>(r * cs, y, r * sn));
+        }
+        acc = acc * ((4.0f * 3.14159265358979323846f) / (float)n);
+        sh[4 * c] = acc.x;
+        sh[4 * c + 1] = acc.y;
+        sh[4 * c + 2] = acc.z;
+        sh[4 * c + 3] = 0.0f;
+    }
+}
+
+void oracle_prt_evaluate(const float* values, const uint32_t* sample_counts, const float* static_source,
+                         const float* sh, float* out, uint32_t* out_counts, uint32_t probe_count) {
+    for (uint32_t p = 0; p < probe_count; ++p) {
+        float e[3] = {static_source[3 * p], static_source[3 * p + 1], static_source[3 * p + 2]};
+        if (sample_counts[p] > 0u)
+            for (int c = 0; c < 9; ++c)
+                for (int k = 0; k < 3; ++k) e[k] = e[k] + values[27 * (size_t)p + 3 * c + k] * sh[4 * c + k];
+        for (int k = 0; k < 3; ++k) out[3 * p + k] = std::fmax(e[k], 0.0f);
+        out_counts[p] = sample_counts[p];
+    }
 }
 
 void oracle_scene_set_area_lights(void* sp, const float* lights, int count, float power) {

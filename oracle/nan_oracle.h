@@ -150,6 +150,23 @@ int oracle_filter_mesh_colors(const uint32_t* face_infos, const uint32_t* instan
                               const uint8_t* source, uint8_t* destination,
                               float neighbor_weight, float normal_sigma_radians, int threads);
 
+/* PRT L2 field baker (surface_probe_prt_baker.slang:169-371) for the listed
+ * probe indices: values f32[N][9][3], static_source f32[N][3] and the
+ * baker's counts, self hits and radial moments, updated in place. */
+int oracle_trace_probes_prt(void* scene, const OracleLighting* lighting, float* values,
+                            uint32_t* sample_counts, uint32_t* self_hits, uint32_t* radial,
+                            float* static_source, const uint8_t* probes, uint32_t probe_count,
+                            const uint8_t* probe_instances, const uint32_t* units, int unit_count,
+                            uint32_t iteration, uint32_t samples_per_probe, uint32_t max_bounces,
+                            int reset, int precision, int threads);
+
+/* PRT evaluation (surface_probe_prt_evaluate.slang:20-103): the SH L2
+ * projection of the escape radiance, sh f32[9][4], and the per-probe
+ * evaluation max(static + sum_c values[c] * sh[c], 0) into out f32[N][3]. */
+void oracle_prt_project_lighting(const OracleLighting* lighting, uint32_t sample_count, float* sh);
+void oracle_prt_evaluate(const float* values, const uint32_t* sample_counts, const float* static_source,
+                         const float* sh, float* out, uint32_t* out_counts, uint32_t probe_count);
+
 /* Area-light table of the screen tracer's NEE option (lighting flag bit 1),
  * the layout of nan_ctx_set_area_lights. */
 void oracle_scene_set_area_lights(void* scene, const float* lights, int count, float power);

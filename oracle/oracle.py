@@ -110,6 +110,11 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes_independent.argtypes = l.oracle_trace_probes.argtypes
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
+    l.oracle_prt_project_lighting.argtypes = [vp, u32, vp]
+    l.oracle_prt_project_lighting.restype = None
+    l.oracle_prt_evaluate.argtypes = [vp, vp, vp, vp, vp, vp, u32]
+    l.oracle_prt_evaluate.restype = None
+    l.oracle_trace_probes_prt.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, u32, vp, vp, i, u32, u32, u32, i, i, i]
     l.oracle_filter_mesh_colors.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, i]
     l.oracle_resolve_mesh_colors.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, vp, vp, u32, vp, i, i, i, vp]
     l.oracle_trace_points.argtypes = [vp, vp, vp, i, u32, u32, u32, u32, vp, i, i, vp]
@@ -129,6 +134,26 @@ def filter_mesh_colors(face_infos, instance_infos, side_infos, adjacency, face_n
     lib().oracle_filter_mesh_colors(_p(fi), _p(ii), _p(si), ii.shape[0], _p(adj), _p(nrm), _p(src), _p(dst),
                                     float(neighbor_weight), float(normal_sigma_radians), threads)
     return dst
+
+
+def prt_project_lighting(lighting, sample_count=2048):
+    """SH L2 projection of the escape radiance, f32[9, 4]."""
+    sh = np.zeros((9, 4), np.float32)
+    L = lighting_struct(lighting)
+    lib().oracle_prt_project_lighting(ctypes.byref(L), int(sample_count), _p(sh))
+    return sh
+
+
+def prt_evaluate(values, sample_counts, static_source, sh):
+    """Evaluated irradiance f32[N, 3] and the copied counts u32[N]."""
+    v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1, 27)
+    c = np.ascontiguousarray(sample_counts).view(np.uint32).reshape(-1)
+    st = np.ascontiguousarray(static_source, dtype=np.float32).reshape(-1, 3)
+    s = np.ascontiguousarray(sh, dtype=np.float32).reshape(9, 4)
+    out = np.zeros((v.shape[0], 3), np.float32)
+    counts = np.zeros(v.shape[0], np.uint32)
+    lib().oracle_prt_evaluate(_p(v), _p(c), _p(st), _p(s), _p(out), _p(counts), v.shape[0])
+    return out, counts
 
 
 
@@ -342,6 +367,23 @@ class OracleScene:
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
         return out
+
+    def trace_probes_prt(self, lighting, values, sample_counts, self_hits, radial, static_source, probes,
+                         probe_instances, units, iteration, samples_per_probe, max_bounces, reset, precision=F32,
+                         threads=0):
+        """PRT L2 baker; values f32[N, 27], static_source f32[N, 3] and the rest updated in place."""
+        for buf in (values, sample_counts, self_hits, radial, static_source):
+            assert buf.flags["C_CONTIGUOUS"]
+        pr = np.ascontiguousarray(probes).view(np.uint8).reshape(-1)
+        pi = np.ascontiguousarray(probe_instances).view(np.uint8).reshape(-1)
+        un = np.ascontiguousarray(units, dtype=np.uint32).reshape(-1)
+        L = lighting_struct(lighting)
+        rc = lib().oracle_trace_probes_prt(self.handle, ctypes.byref(L), _p(values), _p(sample_counts),
+                                           _p(self_hits), _p(radial), _p(static_source), _p(pr), pr.size // 48,
+                                           _p(pi), _p(un), un.size, iteration, samples_per_probe, max_bounces,
+                                           int(bool(reset)), precision, threads)
+        if rc != 0:
+            raise RuntimeError(lib().oracle_last_error().decode())
 
     def set_area_lights(self, lights, power):
         """Area-light table f32[L, 16] and total power (nan_ctx_set_area_lights layout)."""
