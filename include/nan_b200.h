@@ -113,6 +113,50 @@ typedef struct NanMeshColorsDesc {
                                         NULL = the reference's plain lerp (bit-exact parity) */
 } NanMeshColorsDesc;
 
+/* Surface-probe layout (SurfaceProbeLayout, surface_probes.py:1490-1535, as
+ * uploaded by surface_probe_resources.py:24-89): probe records 48 B
+ * {position_radius, normal_side (xyz normal, w support), meta u32x4}; octree
+ * nodes u32[M][4] (child_base, child_mask, probe_start, probe_count);
+ * instance records 48 B {root_center_extent, offsets u32x4 (node offset, node
+ * count, probe offset, probe count), params (kernel radius, normal cosine
+ * threshold, plane sigma, triangle-map offset bits)}, one per scene instance;
+ * triangle -> vertex-anchor probe map u32[R][4] (two records per triangle,
+ * front and back; bit 0 of w marks a valid record). */
+typedef struct NanProbeLayoutDesc {
+    const uint8_t* probes;
+    uint32_t probe_count;
+    uint32_t node_count;
+    const uint32_t* nodes;
+    const uint8_t* instances;
+    uint32_t instance_count;
+    uint32_t triangle_vertex_probe_count;
+    const uint32_t* triangle_vertex_probes;
+} NanProbeLayoutDesc;
+
+/* SurfaceProbeResolve.execute options (surface_probe_resolve.py:46-112).
+ * Vertex lighting (SurfaceProbeVertexLighting's outputs) is optional:
+ * vertex_lighting_rgbm = NULL means not built; otherwise rgbm u32[V], target
+ * f32[V][4], triangle map u32[R][4] (xyz vertices, w valid) and instance
+ * offsets u32[I][2] with one entry per probe-layout instance. */
+typedef struct NanProbeResolveOptions {
+    uint32_t debug_view;             /* 0 beauty, 1 gather count, 2 support, 3 density,
+                                        4 reconstruction confidence, 5 self-hit rate,
+                                        6 vertex lighting, 7 vertex-lighting confidence */
+    uint32_t min_gather_count;       /* clamped to 1..32 */
+    uint32_t use_vertex_fallback;
+    uint32_t use_vertex_lighting;
+    uint32_t use_radial_visibility;
+    uint32_t frame_index;            /* RNG(pixel, frame) of the real-time sun sample */
+    float max_density_multiplier;
+    float vertex_lighting_rgbm_range;
+    const uint32_t* vertex_lighting_rgbm;
+    const float* vertex_lighting_target;
+    const uint32_t* vertex_lighting_triangle_map;
+    const uint32_t* vertex_lighting_instance_offsets;
+    uint32_t vertex_lighting_vertex_count;
+    uint32_t vertex_lighting_triangle_record_count;
+} NanProbeResolveOptions;
+
 /* Execution choices of a context. The defaults (all zero) are the wavefront
  * integrator with occupancy-sized persistent traversal grids, as many paths
  * in flight as the reserved scratch holds, and the PLOC BVH builder. */
@@ -275,6 +319,20 @@ NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDes
                                          const void* colors, int packed, float* out, uint32_t width,
                                          uint32_t height, const NanCamera* camera,
                                          const NanLighting* lighting, void* stream);
+
+/* SurfaceProbeResolve.execute (surface_probe_resolve.py:16-112;
+ * surface_probe_resolve.slang:325-472): one primary ray per pixel; the hit
+ * instance's probes are gathered from its point octree (up to 96 candidates
+ * weighted by distance, plane distance and normal, times the radial
+ * Chebyshev visibility prior, the 32 strongest kept, a 2R fallback merged
+ * when the gather's effective sample size is below min_gather_count) and
+ * reconstructed from the irradiance field values f32[N][3] with its
+ * sample_counts, self_hits and radial moments; out f32[H][W][4]. */
+NAN_B200_API int nan_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* layout, const float* values,
+                                    const uint32_t* sample_counts, const uint32_t* self_hits,
+                                    const uint32_t* radial, const NanProbeResolveOptions* options, float* out,
+                                    uint32_t width, uint32_t height, const NanCamera* camera,
+                                    const NanLighting* lighting, void* stream);
 
 /* MeshColorsSurfaceFilter.execute (mesh_colors_surface_filter.py:95-130;
  * mesh_colors_surface_filter.slang:1-253): one pass of the one-ring,

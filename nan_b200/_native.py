@@ -187,6 +187,38 @@ class NanBatchTuning(ctypes.Structure):
     ]
 
 
+class NanProbeLayoutDesc(ctypes.Structure):
+    _fields_ = [
+        ("probes", ctypes.c_void_p),
+        ("probe_count", ctypes.c_uint32),
+        ("node_count", ctypes.c_uint32),
+        ("nodes", ctypes.c_void_p),
+        ("instances", ctypes.c_void_p),
+        ("instance_count", ctypes.c_uint32),
+        ("triangle_vertex_probe_count", ctypes.c_uint32),
+        ("triangle_vertex_probes", ctypes.c_void_p),
+    ]
+
+
+class NanProbeResolveOptions(ctypes.Structure):
+    _fields_ = [
+        ("debug_view", ctypes.c_uint32),
+        ("min_gather_count", ctypes.c_uint32),
+        ("use_vertex_fallback", ctypes.c_uint32),
+        ("use_vertex_lighting", ctypes.c_uint32),
+        ("use_radial_visibility", ctypes.c_uint32),
+        ("frame_index", ctypes.c_uint32),
+        ("max_density_multiplier", ctypes.c_float),
+        ("vertex_lighting_rgbm_range", ctypes.c_float),
+        ("vertex_lighting_rgbm", ctypes.c_void_p),
+        ("vertex_lighting_target", ctypes.c_void_p),
+        ("vertex_lighting_triangle_map", ctypes.c_void_p),
+        ("vertex_lighting_instance_offsets", ctypes.c_void_p),
+        ("vertex_lighting_vertex_count", ctypes.c_uint32),
+        ("vertex_lighting_triangle_record_count", ctypes.c_uint32),
+    ]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -258,6 +290,9 @@ EXPORTS = {
                                   ctypes.POINTER(NanLighting), _U32, _U32, _VP]),
     "nan_prt_project_lighting": (_I, [_VP, _VP, _U32, ctypes.POINTER(NanLighting), _VP]),
     "nan_prt_evaluate": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP]),
+    "nan_resolve_probes": (_I, [_VP, ctypes.POINTER(NanProbeLayoutDesc), _VP, _VP, _VP, _VP,
+                                ctypes.POINTER(NanProbeResolveOptions), _VP, _U32, _U32, ctypes.POINTER(NanCamera),
+                                ctypes.POINTER(NanLighting), _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),
     "nan_trace_screen_cached": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
                                      ctypes.POINTER(NanLighting), ctypes.POINTER(NanCachedFrame), _VP]),

@@ -412,6 +412,35 @@ NAN_B200_API int nan_prt_evaluate(NanContext* ctx, const float* values, const ui
                                          out_sample_counts, probe_count, as_stream(stream));
 }
 
+NAN_B200_API int nan_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* layout, const float* values,
+                                    const uint32_t* sample_counts, const uint32_t* self_hits,
+                                    const uint32_t* radial, const NanProbeResolveOptions* options, float* out,
+                                    uint32_t width, uint32_t height, const NanCamera* camera,
+                                    const NanLighting* lighting, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    rc = need_scene(ctx);
+    if (rc) return rc;
+    if (!layout || !options || !camera || !lighting) return invalid("null argument");
+    if ((uint64_t)width * height == 0) return NAN_OK;
+    if (!out || !layout->instances || (layout->probe_count && (!layout->probes || !values || !sample_counts ||
+                                                               !self_hits || !radial)) ||
+        (layout->node_count && !layout->nodes) ||
+        (layout->triangle_vertex_probe_count && !layout->triangle_vertex_probes))
+        return invalid("null buffer");
+    if (!aligned16(out) || !aligned16(layout->probes) || !aligned16(layout->nodes) ||
+        !aligned16(layout->instances) || !aligned16(layout->triangle_vertex_probes))
+        return invalid("probe layout buffers and out must be 16-byte aligned");
+    if (options->vertex_lighting_rgbm &&
+        (!options->vertex_lighting_target || !options->vertex_lighting_triangle_map ||
+         !options->vertex_lighting_instance_offsets || !aligned16(options->vertex_lighting_target) ||
+         !aligned16(options->vertex_lighting_triangle_map) ||
+         (reinterpret_cast<uintptr_t>(options->vertex_lighting_instance_offsets) & 7u)))
+        return invalid("vertex lighting needs target, triangle map and instance offsets (aligned)");
+    return nan_host::launch_resolve_probes(ctx, layout, values, sample_counts, self_hits, radial, options, out, width,
+                                           height, camera, lighting, as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

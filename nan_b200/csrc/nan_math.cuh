@@ -7,7 +7,8 @@
 // Slang expressions (common.slang, scene.slang) in a fixed order:
 //   dot(a,b) = (a.x*b.x + a.y*b.y) + a.z*b.z, vector sums left to right,
 //   normalize(v) = v * (1/sqrt(dot(v,v))), lerp(a,b,s) = a + s*(b-a),
-//   sin/cos from nan_sincos() (own Cody-Waite + Taylor, no libdevice).
+//   sin/cos from nan_sincos(), exp from nan_exp(), log2 from nan_log2() (own
+//   Cody-Waite reductions and series, no libdevice).
 #pragma once
 
 #include <cstdint>
@@ -69,6 +70,59 @@ __device__ __forceinline__ void nan_sincos(float a, float* s, float* c) {
     }
 }
 
+// e^x: Cody-Waite reduction x = k ln2 + r with |r| <= ln2/2 (ln2 split in a
+// 16-bit head and a tail, fused steps), e^r by its Taylor series to degree 7
+// (truncation below 6e-9 relative) in Horner form, then 2^k applied as two
+// exact power-of-two factors. Below -87.3 the result is 0, above 88.7 inf.
+__device__ __forceinline__ float nan_exp(float x) {
+    if (x != x) return x;
+    if (x > 88.7f) return __int_as_float(0x7f800000);
+    if (x < -87.3f) return 0.0f;
+    const float kf = rintf(x * 1.44269504088896341f);
+    const int k = (int)kf;
+    float r = __fmaf_rn(-kf, 0.693145751953125f, x);
+    r = __fmaf_rn(-kf, 1.428606820309417232e-6f, r);
+    float p = __fmaf_rn(r, 1.98412698412698413e-4f, 1.38888888888888889e-3f);
+    p = __fmaf_rn(r, p, 8.33333333333333333e-3f);
+    p = __fmaf_rn(r, p, 4.16666666666666667e-2f);
+    p = __fmaf_rn(r, p, 1.66666666666666667e-1f);
+    p = __fmaf_rn(r, p, 0.5f);
+    p = __fmaf_rn(r, p, 1.0f);
+    p = __fmaf_rn(r, p, 1.0f);
+    const int k1 = k >> 1, k2 = k - k1;
+    return (p * __int_as_float((k1 + 127) << 23)) * __int_as_float((k2 + 127) << 23);
+}
+
+// log2(x): x = m 2^e with m in [sqrt(1/2), sqrt(2)], ln m = 2 atanh(s),
+// s = (m-1)/(m+1), |s| <= 0.1716, by the odd series to s^11 (truncation below
+// 1e-10), then e + ln m * log2(e). Subnormals are scaled by 2^23 first.
+__device__ __forceinline__ float nan_log2(float x) {
+    if (x != x || x < 0.0f) return __int_as_float(0x7fc00000);
+    if (x == 0.0f) return __int_as_float(0xff800000);
+    if (x > 3.40282347e38f) return x;
+    int e = 0;
+    if (x < 1.17549435e-38f) {
+        x = x * 8388608.0f;
+        e = -23;
+    }
+    const uint32_t bits = __float_as_uint(x);
+    e += (int)((bits >> 23) & 0xffu) - 127;
+    float m = __uint_as_float((bits & 0x7fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    const float s = (m - 1.0f) / (m + 1.0f);
+    const float s2 = s * s;
+    float p = __fmaf_rn(s2, 9.09090909090909091e-2f, 1.11111111111111111e-1f);
+    p = __fmaf_rn(s2, p, 1.42857142857142857e-1f);
+    p = __fmaf_rn(s2, p, 2.0e-1f);
+    p = __fmaf_rn(s2, p, 3.33333333333333333e-1f);
+    p = __fmaf_rn(s2, p, 1.0f);
+    const float ln_m = (2.0f * s) * p;
+    return (float)e + ln_m * 1.44269504088896341f;
+}
+
 // LCG of common.slang:164-210.
 struct Rng {
     uint32_t state;
@@ -90,6 +144,7 @@ struct Frame {
         b = cross3(nn, t);
     }
     __device__ __forceinline__ f3 to_global(f3 w) const { return (w.x * t + w.y * b) + w.z * n; }
+    __device__ __forceinline__ f3 to_local(f3 w) const { return mk3(dot3(t, w), dot3(b, w), dot3(n, w)); }
 };
 
 // common.slang:54-68; returns direction, writes pdf.

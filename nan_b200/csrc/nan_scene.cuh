@@ -502,7 +502,8 @@ struct Shading {
     f3 face_normal;
     f3 diffuse;
     f3 emissive;
-    Frame frame;  // shading frame
+    Frame frame;     // shading frame
+    bool back_side;  // double-sided material seen from its back
 };
 
 struct TriRefs {
@@ -609,6 +610,7 @@ __device__ __forceinline__ Shading shading_data(const SceneView& s, uint32_t ins
     sd.frame = Frame(sn);
     sd.diffuse = ld3(r.mat);
     sd.emissive = ld3(r.mat + 4);
+    sd.back_side = double_sided && !front;
     return sd;
 }
 

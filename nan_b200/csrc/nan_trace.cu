@@ -8,6 +8,7 @@
 #include "nan_scene.cuh"
 #include "nan_sinks.cuh"
 #include "nan_probe.cuh"
+#include "nan_probe_gather.cuh"
 
 namespace {
 
@@ -259,6 +260,174 @@ __global__ void __launch_bounds__(128) k_resolve_mesh_colors(SceneView s, Lighti
     const f3 irr = mc_sample(colors, kPacked, b0, hit.b1, hit.b2, inst, face, side, back);
     const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
     const f3 c = sd.emissive + (sd.diffuse * kInvPi) * irr;
+    out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
+}
+
+// ---------------------------------------------------------------------------
+// Surface-probe resolve (surface_probe_resolve.slang:325-472): per pixel one
+// primary ray; at the hit the probes of the hit instance are gathered from its
+// point octree and reconstructed (nan_probe_gather.cuh), optionally blended
+// with the triangle's vertex-anchor probes and replaced by baked vertex
+// lighting; shaded as emissive + real-time sun + albedo / pi * irradiance, or
+// one of the seven debug views.
+// ---------------------------------------------------------------------------
+struct ProbeResolveArgs {
+    ProbeLayoutView layout;
+    ProbeFieldView field;
+    const uint32_t* vl_rgbm;
+    const float4* vl_target;
+    const uint4* vl_tri_map;
+    const uint2* vl_inst;
+    uint32_t vl_vertex_count, vl_tri_map_count;
+    uint32_t debug_view, min_gather, use_vertex_fallback, use_vertex_lighting, use_radial, frame;
+    float max_density, vl_range;
+};
+
+__device__ __forceinline__ f3 decode_rgbm(uint32_t packed, float range) {
+    const float x = (float)(packed & 255u) / 255.0f, y = (float)((packed >> 8) & 255u) / 255.0f;
+    const float z = (float)((packed >> 16) & 255u) / 255.0f, w = (float)((packed >> 24) & 255u) / 255.0f;
+    return (mk3(x, y, z) * w) * range;
+}
+
+__global__ void __launch_bounds__(128) k_resolve_probes(SceneView s, LightingRaw lraw, CameraRaw cam,
+                                                        ProbeResolveArgs a, float4* __restrict__ out, uint32_t w,
+                                                        uint32_t h) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= w || py >= h) return;
+    const LightParams L = make_light(lraw);
+    float pxf = ((float)px + 0.5f) / (float)w;
+    float pyf = ((float)py + 0.5f) / (float)h;
+    pxf = pxf + (-cam.jitter_x);
+    pyf = pyf + cam.jitter_y;
+    const float nx = 2.0f * pxf + -1.0f;
+    const float ny = -2.0f * pyf + 1.0f;
+    const f3 U = mk3(cam.image_u[0], cam.image_u[1], cam.image_u[2]);
+    const f3 V = mk3(cam.image_v[0], cam.image_v[1], cam.image_v[2]);
+    const f3 W = mk3(cam.image_w[0], cam.image_w[1], cam.image_w[2]);
+    const f3 dir = normalize3((nx * U + ny * V) + W);
+    const float inv_cos = 1.0f / dot3(normalize3(W), dir);
+    const f3 o = mk3(cam.position[0], cam.position[1], cam.position[2]);
+    const HitInfo hit = trace_closest(s, o, dir, cam.near_clip * inv_cos, cam.far_clip * inv_cos);
+    const size_t pix = (size_t)py * w + px;
+    const bool beauty = a.debug_view == 0u || a.debug_view == 6u;
+    if (!hit.valid) {
+        f3 c = mk3(0.02f, 0.02f, 0.02f);
+        if (beauty) {
+            c = L.sky;
+            if (L.sun_disk) c = c + sun_disk(L, dir);
+        }
+        out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
+        return;
+    }
+    const uint2 ref = __ldg(s.tri_refs + hit.flat);
+    const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -dir);
+    f3 sun = mk3(0.0f, 0.0f, 0.0f);
+    if (beauty) {
+        Rng rng(px, py, a.frame);
+        const float ux = rng.next_1d();
+        const float uy = rng.next_1d();
+        RayTally tally{0u, 0u};
+        sun = sun_nee<DefaultTracer>(s, L, sd, ux, uy, tally);
+    }
+    if (ref.x >= a.layout.instance_count) {
+        atomicOr(s.status, kStatusBadRecord);
+        return;
+    }
+    const ProbeInstance ins = load_probe_instance(a.layout, ref.x);
+    if (ins.offsets.w == 0u) {
+        const f3 c = beauty ? sd.emissive + sun : gather_count_color(0u);
+        out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
+        return;
+    }
+    Candidates cand;
+    const ProbeReconstruction r = probe_reconstruct(a.layout, a.field, ins, sd.position, normalize3(sd.face_normal),
+                                                    a.min_gather, a.use_radial != 0u, cand, s.status);
+    const uint32_t side = sd.back_side ? 1u : 0u;
+    const float b0 = (1.0f - hit.b1) - hit.b2;
+    const float bary[3] = {b0, hit.b1, hit.b2};
+    // surface_probe_sample_vertex_fallback
+    f3 vertex_irr = mk3(0.0f, 0.0f, 0.0f);
+    bool has_fallback = false;
+    if (a.use_vertex_fallback != 0u) {
+        const uint32_t rec = ins.tri_map_offset + ref.y * 2u + side;
+        if (rec >= a.layout.tri_map_count) {
+            atomicOr(s.status, kStatusBadRecord);
+        } else {
+            const uint4 anchors = __ldg(a.layout.tri_vertex_probes + rec);
+            if (anchors.w & 1u) {
+                const uint32_t idx[3] = {anchors.x, anchors.y, anchors.z};
+                f3 acc = mk3(0.0f, 0.0f, 0.0f);
+                float avail = 0.0f;
+                for (int c = 0; c < 3; ++c) {
+                    if (idx[c] >= a.layout.probe_count) {
+                        atomicOr(s.status, kStatusBadRecord);
+                        continue;
+                    }
+                    if (__ldg(a.field.counts + idx[c]) == 0u) continue;
+                    acc = acc + bary[c] * probe_irradiance(a.field, idx[c]);
+                    avail = avail + bary[c];
+                }
+                if (avail > 1e-6f) {
+                    vertex_irr = acc / avail;
+                    has_fallback = true;
+                }
+            }
+        }
+    }
+    const float target = (float)min(max(a.min_gather, 1u), 32u);
+    float conf = minf(sat((float)r.gathered / target), sat(r.ess / target));
+    if (r.weight_sum <= 1e-6f) conf = 0.0f;
+    if (!has_fallback) conf = 1.0f;
+    const float fallback_weight = 1.0f - conf;
+    f3 irr = lerp3(vertex_irr, r.irradiance, conf);
+    f3 c;
+    if (a.debug_view == 1u) {
+        c = gather_count_color(r.gathered);
+    } else if (a.debug_view == 2u) {
+        c = support_color(r.support);
+    } else if (a.debug_view == 3u) {
+        c = density_color(r.support, a.max_density);
+    } else if (a.debug_view == 4u) {
+        c = support_color(1.0f - fallback_weight);
+    } else if (a.debug_view == 5u) {
+        c = self_hit_color(r.self_hit_rate);
+    } else {
+        // surface_probe_sample_vertex_lighting
+        bool has_vl = false;
+        f3 vl = mk3(0.0f, 0.0f, 0.0f);
+        float vl_conf = 0.0f;
+        if (a.vl_rgbm != nullptr) {
+            const uint2 io = __ldg(a.vl_inst + ref.x);
+            const uint32_t rec = io.x + ref.y * 2u + side;
+            if (rec >= a.vl_tri_map_count) {
+                atomicOr(s.status, kStatusBadRecord);
+            } else {
+                const uint4 vv = __ldg(a.vl_tri_map + rec);
+                if (vv.w != 0u) {
+                    if (vv.x >= a.vl_vertex_count || vv.y >= a.vl_vertex_count || vv.z >= a.vl_vertex_count) {
+                        atomicOr(s.status, kStatusBadRecord);
+                    } else {
+                        vl = (b0 * decode_rgbm(__ldg(a.vl_rgbm + vv.x), a.vl_range) +
+                              hit.b1 * decode_rgbm(__ldg(a.vl_rgbm + vv.y), a.vl_range)) +
+                             hit.b2 * decode_rgbm(__ldg(a.vl_rgbm + vv.z), a.vl_range);
+                        vl_conf = (b0 * __ldg(a.vl_target + vv.x).w + hit.b1 * __ldg(a.vl_target + vv.y).w) +
+                                  hit.b2 * __ldg(a.vl_target + vv.z).w;
+                        has_vl = true;
+                    }
+                }
+            }
+        }
+        if (a.debug_view == 6u) {
+            c = has_vl ? (sd.emissive + sun) + (sd.diffuse * kInvPi) * vl : mk3(1.0f, 0.0f, 1.0f);
+        } else if (a.debug_view == 7u) {
+            c = has_vl ? support_color(vl_conf) : mk3(1.0f, 0.0f, 1.0f);
+        } else {
+            if (a.use_vertex_lighting != 0u && has_vl) irr = vl;
+            c = (sd.emissive + sun) + (sd.diffuse * kInvPi) * irr;
+        }
+    }
     out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
 }
 
@@ -662,6 +831,45 @@ int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* lay, co
                                                            reinterpret_cast<float4*>(out), w, h);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "resolve_mesh_colors launch");
+}
+
+int launch_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* lay, const float* values,
+                          const uint32_t* counts, const uint32_t* self_hits, const uint32_t* radial,
+                          const NanProbeResolveOptions* opt, float* out, uint32_t w, uint32_t h,
+                          const NanCamera* cam, const NanLighting* light, cudaStream_t st) {
+    if (w == 0 || h == 0) return NAN_OK;
+    CameraRaw c;
+    memcpy(&c, cam, sizeof(c));
+    ProbeResolveArgs a;
+    memset(&a, 0, sizeof(a));
+    a.layout.probes = reinterpret_cast<const float4*>(lay->probes);
+    a.layout.nodes = reinterpret_cast<const uint4*>(lay->nodes);
+    a.layout.instances = reinterpret_cast<const float4*>(lay->instances);
+    a.layout.tri_vertex_probes = reinterpret_cast<const uint4*>(lay->triangle_vertex_probes);
+    a.layout.probe_count = lay->probe_count;
+    a.layout.node_count = lay->node_count;
+    a.layout.instance_count = lay->instance_count;
+    a.layout.tri_map_count = lay->triangle_vertex_probe_count;
+    a.field = ProbeFieldView{values, counts, self_hits, radial};
+    a.vl_rgbm = opt->vertex_lighting_rgbm;
+    a.vl_target = reinterpret_cast<const float4*>(opt->vertex_lighting_target);
+    a.vl_tri_map = reinterpret_cast<const uint4*>(opt->vertex_lighting_triangle_map);
+    a.vl_inst = reinterpret_cast<const uint2*>(opt->vertex_lighting_instance_offsets);
+    a.vl_vertex_count = opt->vertex_lighting_vertex_count;
+    a.vl_tri_map_count = opt->vertex_lighting_triangle_record_count;
+    a.debug_view = std::min(opt->debug_view, 7u);
+    a.min_gather = opt->min_gather_count;
+    a.use_vertex_fallback = opt->use_vertex_fallback;
+    a.use_vertex_lighting = opt->use_vertex_lighting;
+    a.use_radial = opt->use_radial_visibility;
+    a.frame = opt->frame_index;
+    a.max_density = opt->max_density_multiplier;
+    a.vl_range = std::max(opt->vertex_lighting_rgbm_range, 1.0f);
+    dim3 grid(blocks_for(w, 16), blocks_for(h, 8));
+    k_resolve_probes<<<grid, 128, 0, st>>>(scene_view(ctx), to_raw(light), c, a, reinterpret_cast<float4*>(out), w,
+                                           h);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "resolve_probes launch");
 }
 
 int launch_filter_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* lay, const uint32_t* adjacency,

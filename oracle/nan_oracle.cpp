@@ -68,6 +68,69 @@ void own_sincos(float a, float* s, float* c) {
     }
 }
 
+static float bits_float(uint32_t b) {
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+
+static uint32_t float_bits(float f) {
+    uint32_t b;
+    std::memcpy(&b, &f, 4);
+    return b;
+}
+
+// e^x by Cody-Waite reduction x = k ln2 + r (ln2 split in a 16-bit head and a
+// tail), the Taylor series of e^r to degree 7 in Horner form, and 2^k as two
+// exact power-of-two factors; 0 below -87.3, inf above 88.7.
+float spec_exp(float x) {
+    if (x != x) return x;
+    if (x > 88.7f) return bits_float(0x7f800000u);
+    if (x < -87.3f) return 0.0f;
+    float kf = std::rint(x * 1.44269504088896341f);
+    int k = (int)kf;
+    float r = std::fmaf(-kf, 0.693145751953125f, x);
+    r = std::fmaf(-kf, 1.428606820309417232e-6f, r);
+    float p = std::fmaf(r, 1.98412698412698413e-4f, 1.38888888888888889e-3f);
+    p = std::fmaf(r, p, 8.33333333333333333e-3f);
+    p = std::fmaf(r, p, 4.16666666666666667e-2f);
+    p = std::fmaf(r, p, 1.66666666666666667e-1f);
+    p = std::fmaf(r, p, 0.5f);
+    p = std::fmaf(r, p, 1.0f);
+    p = std::fmaf(r, p, 1.0f);
+    int k1 = k >> 1, k2 = k - k1;
+    return (p * bits_float((uint32_t)(k1 + 127) << 23)) * bits_float((uint32_t)(k2 + 127) << 23);
+}
+
+// log2 x: x = m 2^e, m in [sqrt(1/2), sqrt(2)], ln m = 2 atanh((m-1)/(m+1)) by
+// its odd series to s^11; subnormals scaled by 2^23 first.
+float spec_log2(float x) {
+    if (x != x || x < 0.0f) return bits_float(0x7fc00000u);
+    if (x == 0.0f) return bits_float(0xff800000u);
+    if (x > 3.40282347e38f) return x;
+    int e = 0;
+    if (x < 1.17549435e-38f) {
+        x = x * 8388608.0f;
+        e = -23;
+    }
+    uint32_t bits = float_bits(x);
+    e += (int)((bits >> 23) & 0xffu) - 127;
+    float m = bits_float((bits & 0x7fffffu) | 0x3f800000u);
+    if (m > 1.41421356f) {
+        m = m * 0.5f;
+        e += 1;
+    }
+    float sv = (m - 1.0f) / (m + 1.0f);
+    float s2 = sv * sv;
+    float p = std::fmaf(s2, 9.09090909090909091e-2f, 1.11111111111111111e-1f);
+    p = std::fmaf(s2, p, 1.42857142857142857e-1f);
+    p = std::fmaf(s2, p, 2.0e-1f);
+    p = std::fmaf(s2, p, 3.33333333333333333e-1f);
+    p = std::fmaf(s2, p, 1.0f);
+    float ln_m = (2.0f * sv) * p;
+    return (float)e + ln_m * 1.44269504088896341f;
+}
+
 template <class T> struct Ops;
 template <> struct Ops<float> {
     static float fma(float a, float b, float c) { return std::fmaf(a, b, c); }
@@ -728,6 +791,7 @@ template <class T> struct Shading {
     T offset;
     V3<T> view_direction, face_normal, diffuse, emissive;
     Frame<T> shading_frame{mk<T>(0, 0, 1)};
+    bool back_side = false;  // double-sided material seen from its back
 };
 
 template <class T> V3<T> load3(const float* p) { return mk<T>(T(p[0]), T(p[1]), T(p[2])); }
@@ -838,6 +902,7 @@ Shading<T> shading_data(const Scene& s, uint32_t inst, uint32_t prim, T bx, T by
     sd.shading_frame = Frame<T>(sn);
     sd.diffuse = load3<T>(r.mat);
     sd.emissive = load3<T>(r.mat + 4);
+    sd.back_side = double_sided && !front;
     return sd;
 }
 
@@ -1884,6 +1949,552 @@ int oracle_resolve_mesh_colors(void* sp, const OracleLighting* lighting, const O
         }
     });
     return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Surface-probe resolve, surface_probe_resolve.slang:29-472 with the gather
+// of surface_probes.slang:272-535 and surface_probe_irradiance_field.slang:
+// 28-81, in float. lerp(a, b, t) = a + t (b - a); exp and log2 are spec_exp
+// and spec_log2.
+// ---------------------------------------------------------------------------
+namespace probe_resolve {
+
+constexpr uint32_t kMaxGather = 32, kMaxCandidates = 96, kStack = 64;
+constexpr float kHardCos = 0.17364818f;
+using F3 = V3<float>;
+
+struct Layout {
+    const float* probes;     // 12 floats per probe
+    const uint32_t* nodes;   // 4 per node
+    const float* instances;  // 12 floats per instance
+    const uint32_t* tri_map; // 4 per record
+    uint32_t probe_count, node_count, instance_count, tri_map_count;
+    const float* values;
+    const uint32_t* counts;
+    const uint32_t* self_hits;
+    const uint32_t* radial;
+};
+
+struct Instance {
+    F3 center;
+    float extent;
+    uint32_t offsets[4];
+    float kr, ncos, sigma;
+    uint32_t map_offset;
+};
+
+struct Cands {
+    uint32_t count = 0;
+    uint32_t index[kMaxCandidates];
+    float weight[kMaxCandidates];
+};
+
+struct Gath {
+    uint32_t count = 0;
+    uint32_t index[kMaxGather];
+    float weight[kMaxGather];
+};
+
+float sat(float a) { return std::fmin(std::fmax(a, 0.0f), 1.0f); }
+float lerpf(float a, float b, float t) { return a + t * (b - a); }
+F3 lerp3(F3 a, F3 b, float t) { return a + t * (b - a); }
+float smooth(float e0, float e1, float x) {
+    float t = sat((x - e0) / (e1 - e0));
+    return (t * t) * (3.0f - 2.0f * t);
+}
+F3 ppos(const Layout& l, uint32_t p) { return mk<float>(l.probes[12 * (size_t)p], l.probes[12 * (size_t)p + 1],
+                                                        l.probes[12 * (size_t)p + 2]); }
+F3 pnormal(const Layout& l, uint32_t p) { return mk<float>(l.probes[12 * (size_t)p + 4], l.probes[12 * (size_t)p + 5],
+                                                           l.probes[12 * (size_t)p + 6]); }
+float psupport(const Layout& l, uint32_t p) { return l.probes[12 * (size_t)p + 7]; }
+F3 pirr(const Layout& l, uint32_t p) { return mk<float>(l.values[3 * (size_t)p], l.values[3 * (size_t)p + 1],
+                                                        l.values[3 * (size_t)p + 2]); }
+
+Instance load_instance(const Layout& l, uint32_t i) {
+    const float* r = l.instances + 12 * (size_t)i;
+    Instance v;
+    v.center = mk<float>(r[0], r[1], r[2]);
+    v.extent = r[3];
+    std::memcpy(v.offsets, r + 4, 16);
+    v.kr = r[8];
+    v.ncos = r[9];
+    v.sigma = r[10];
+    std::memcpy(&v.map_offset, r + 11, 4);
+    return v;
+}
+
+bool sphere_cube(F3 p, float r, F3 c, float e) {
+    F3 a = mk<float>(std::fabs(p.x - c.x), std::fabs(p.y - c.y), std::fabs(p.z - c.z));
+    F3 d = mk<float>(std::fmax(a.x - e, 0.0f), std::fmax(a.y - e, 0.0f), std::fmax(a.z - e, 0.0f));
+    return dot(d, d) <= r * r;
+}
+
+float soft_normal(float nc, float full) {
+    float end = std::fmax(full, kHardCos + 1e-3f);
+    return smooth(kHardCos, end, nc) * std::fmax(nc, 0.0f);
+}
+
+// surface_probes.slang:272-392
+void gather(const Layout& l, const Instance& ins, F3 q, F3 qn, float scale, Cands& out, bool* bad) {
+    out.count = 0;
+    float kr = std::fmax(ins.kr * std::fmax(scale, 1.0f), 1e-6f);
+    float ps = std::fmax(ins.sigma, 1e-6f);
+    float kr2 = kr * kr;
+    uint32_t sn[kStack];
+    F3 sc[kStack];
+    float se[kStack];
+    uint32_t n = 1;
+    sn[0] = ins.offsets[0];
+    sc[0] = ins.center;
+    se[0] = ins.extent;
+    while (n > 0) {
+        n -= 1;
+        uint32_t ni = sn[n];
+        F3 c = sc[n];
+        float e = se[n];
+        if (!sphere_cube(q, kr, c, e)) continue;
+        if (ni >= l.node_count) {
+            *bad = true;
+            continue;
+        }
+        const uint32_t* node = l.nodes + 4 * (size_t)ni;
+        if (node[1] == 0) {
+            if (node[2] > l.probe_count || node[3] > l.probe_count - node[2]) {
+                *bad = true;
+                continue;
+            }
+            for (uint32_t k = 0; k < node[3]; ++k) {
+                uint32_t p = node[2] + k;
+                F3 delta = ppos(l, p) - q;
+                float d2 = dot(delta, delta);
+                if (d2 > kr2) continue;
+                float nc = dot(qn, normalize(pnormal(l, p)));
+                if (nc < kHardCos) continue;
+                float pd = std::fabs(dot(delta, qn));
+                float pw = spec_exp((-0.5f * (pd / ps)) * (pd / ps));
+                float sp = std::fmax(1.0f - d2 / kr2, 0.0f);
+                float w = ((sp * sp) * pw) * soft_normal(nc, ins.ncos);
+                if (w <= 1e-6f) continue;
+                if (out.count < kMaxCandidates) {
+                    out.index[out.count] = p;
+                    out.weight[out.count] = w;
+                    out.count += 1;
+                } else {
+                    uint32_t weakest = 0;
+                    for (uint32_t i = 1; i < kMaxCandidates; ++i)
+                        if (out.weight[i] < out.weight[weakest]) weakest = i;
+                    if (w > out.weight[weakest]) {
+                        out.index[weakest] = p;
+                        out.weight[weakest] = w;
+                    }
+                }
+            }
+            continue;
+        }
+        float ce = e * 0.5f;
+        uint32_t compact = 0;
+        for (uint32_t o = 0; o < 8; ++o) {
+            if (!(node[1] & (1u << o))) continue;
+            F3 off = mk<float>((o & 1) ? 1.0f : -1.0f, (o & 2) ? 1.0f : -1.0f, (o & 4) ? 1.0f : -1.0f);
+            F3 cc = c + off * ce;
+            if (sphere_cube(q, kr, cc, ce) && n < kStack) {
+                sn[n] = node[0] + compact;
+                sc[n] = cc;
+                se[n] = ce;
+                n += 1;
+            }
+            compact += 1;
+        }
+    }
+}
+
+float half_bits_to_float(uint32_t h) { return f16_to_f32((uint16_t)h); }
+
+// surface_probes.slang:134-155, 201-244, 462-535
+void hemi_oct(F3 d, float* u, float* v) {
+    F3 h = mk<float>(d.x, d.y, std::fmax(d.z, 0.0f));
+    float l2 = dot(h, h);
+    if (l2 <= 1e-12f) {
+        *u = *v = 0.5f;
+        return;
+    }
+    h = h * (1.0f / std::sqrt(l2));
+    float inv_l1 = 1.0f / std::fmax((std::fabs(h.x) + std::fabs(h.y)) + h.z, 1e-6f);
+    float ox = h.x * inv_l1, oy = h.y * inv_l1;
+    *u = sat((ox + oy) * 0.5f + 0.5f);
+    *v = sat((ox - oy) * 0.5f + 0.5f);
+}
+
+float visibility(const Layout& l, uint32_t p, F3 q, float kr, uint32_t sample_count, bool enabled) {
+    if (!enabled) return 1.0f;
+    F3 delta = q - ppos(l, p);
+    float dist = std::sqrt(dot(delta, delta));
+    if (dist <= 1e-6f) return 1.0f;
+    F3 dl = mk<float>(delta.x / dist, delta.y / dist, delta.z / dist);
+    F3 local = Frame<float>(normalize(pnormal(l, p))).to_local(dl);
+    float nd = std::fmin(dist / std::fmax(kr, 1e-6f), 2.0f);
+    float u, v;
+    hemi_oct(local, &u, &v);
+    float tx = sat(u) * 4.0f - 0.5f, ty = sat(v) * 4.0f - 0.5f;
+    float fx = std::floor(tx), fy = std::floor(ty);
+    int bx = (int)fx, by = (int)fy;
+    float ax = tx - fx, ay = ty - fy;
+    auto cl = [](int a) { return std::max(std::min(a, 3), 0); };
+    int x0 = cl(bx), x1 = cl(bx + 1), y0 = cl(by), y1 = cl(by + 1);
+    float w[4] = {(1.0f - ax) * (1.0f - ay), ax * (1.0f - ay), (1.0f - ax) * ay, ax * ay};
+    int t[4] = {y0 * 4 + x0, y0 * 4 + x1, y1 * 4 + x0, y1 * 4 + x1};
+    float mx = 0.0f, my = 0.0f, vw = 0.0f;
+    for (int i = 0; i < 4; ++i) {
+        uint32_t packed = l.radial[16 * (size_t)p + t[i]];
+        float sx = half_bits_to_float(packed & 0xffffu), sy = half_bits_to_float(packed >> 16);
+        if (sy > 0.0f) {
+            mx = mx + sx * w[i];
+            my = my + sy * w[i];
+            vw = vw + w[i];
+        }
+    }
+    if (vw <= 1e-6f) return 1.0f;
+    mx = mx / vw;
+    my = my / vw;
+    float vis = 1.0f;
+    if (my > 0.0f) {
+        float mean = std::fmax(mx, 0.0f);
+        if (!(nd <= mean + 0.035f)) {
+            float var = std::fmax(my - mean * mean, 2.5e-3f);
+            float diff = nd - mean;
+            float prob = var / (var + diff * diff);
+            vis = std::fmax(sat((prob - 0.2f) / 0.8f), 0.05f);
+        }
+    }
+    float tc = sat((float)sample_count / 32.0f);
+    return lerpf(1.0f, vis, 0.75f * tc);
+}
+
+void select(const Cands& c, Gath& out) {
+    out.count = 0;
+    uint32_t used[3] = {0, 0, 0};
+    for (uint32_t sel = 0; sel < c.count && out.count < kMaxGather; ++sel) {
+        uint32_t best = 0;
+        float bw = -1.0f;
+        for (uint32_t i = 0; i < c.count; ++i) {
+            bool consumed = (used[i >> 5] >> (i & 31u)) & 1u;
+            if (!consumed && c.weight[i] > bw) {
+                best = i;
+                bw = c.weight[i];
+            }
+        }
+        used[best >> 5] |= 1u << (best & 31u);
+        out.index[out.count] = c.index[best];
+        out.weight[out.count] = bw;
+        out.count += 1;
+    }
+}
+
+void merge(const Gath& fb, float scale, Gath& g) {
+    for (uint32_t k = 0; k < fb.count; ++k) {
+        bool dup = false;
+        for (uint32_t i = 0; i < g.count; ++i)
+            if (g.index[i] == fb.index[k]) {
+                dup = true;
+                break;
+            }
+        if (dup) continue;
+        float w = fb.weight[k] * scale;
+        if (w <= 1e-8f) continue;
+        if (g.count < kMaxGather) {
+            g.index[g.count] = fb.index[k];
+            g.weight[g.count] = w;
+            g.count += 1;
+        } else {
+            uint32_t weakest = 0;
+            for (uint32_t i = 1; i < g.count; ++i)
+                if (g.weight[i] < g.weight[weakest]) weakest = i;
+            if (w > g.weight[weakest]) {
+                g.index[weakest] = fb.index[k];
+                g.weight[weakest] = w;
+            }
+        }
+    }
+}
+
+float ess(const Gath& g) {
+    float s = 0.0f, s2 = 0.0f;
+    for (uint32_t i = 0; i < g.count; ++i) {
+        float w = std::fmax(g.weight[i], 0.0f);
+        s = s + w;
+        s2 = s2 + w * w;
+    }
+    return s2 > 1e-12f ? (s * s) / s2 : 0.0f;
+}
+
+struct Recon {
+    F3 irradiance;
+    uint32_t gathered;
+    float support, weight_sum, ess, self_hit_rate;
+};
+
+void weigh(const Layout& l, Cands& c, F3 q, float kr, bool radial) {
+    for (uint32_t i = 0; i < c.count; ++i)
+        c.weight[i] = c.weight[i] * visibility(l, c.index[i], q, kr, l.counts[c.index[i]], radial);
+}
+
+Recon reconstruct(const Layout& l, const Instance& ins, F3 q, F3 qn, uint32_t min_gather, bool radial, bool* bad) {
+    Cands cand;
+    Gath g;
+    gather(l, ins, q, qn, 1.0f, cand, bad);
+    weigh(l, cand, q, ins.kr, radial);
+    select(cand, g);
+    uint32_t mg = std::min(std::max(min_gather, 1u), 32u);
+    float e0 = ess(g);
+    float fs = smooth(0.0f, 1.0f, sat(((float)mg - e0) / (float)mg));
+    if (fs > 1e-4f) {
+        Gath fb;
+        gather(l, ins, q, qn, 2.0f, cand, bad);
+        weigh(l, cand, q, ins.kr, radial);
+        select(cand, fb);
+        merge(fb, 0.25f * fs, g);
+    }
+    Recon r;
+    float shs = 0.0f, shw = 0.0f;
+    for (uint32_t i = 0; i < g.count; ++i) {
+        uint32_t p = g.index[i];
+        uint32_t sc = l.counts[p];
+        if (sc == 0) continue;
+        float rate = (float)l.self_hits[p] / (float)sc;
+        shs = shs + g.weight[i] * rate;
+        shw = shw + g.weight[i];
+    }
+    r.self_hit_rate = shw > 1e-6f ? shs / shw : 0.0f;
+    F3 acc = mk<float>(0, 0, 0), best = mk<float>(0, 0, 0);
+    float ws = 0.0f, wss = 0.0f, ss = 0.0f, ssw = 0.0f, best_w = -1.0f;
+    for (uint32_t i = 0; i < g.count; ++i) {
+        uint32_t p = g.index[i];
+        ss = ss + g.weight[i] * sat(psupport(l, p));
+        ssw = ssw + g.weight[i];
+        F3 irr = pirr(l, p);
+        float conf = l.counts[p] > 0 ? 1.0f : 0.0f;
+        float w = g.weight[i] * conf;
+        acc = acc + w * irr;
+        ws = ws + w;
+        wss = wss + w * w;
+        if (w > best_w) {
+            best_w = w;
+            best = irr;
+        }
+    }
+    r.gathered = g.count;
+    r.support = ssw > 1e-6f ? sat(ss / ssw) : 0.0f;
+    r.weight_sum = ws;
+    r.ess = wss > 1e-12f ? (ws * ws) / wss : 0.0f;
+    if (ws > 1e-6f)
+        r.irradiance = mk<float>(acc.x / ws, acc.y / ws, acc.z / ws);
+    else if (best_w >= 0.0f)
+        r.irradiance = best;
+    else
+        r.irradiance = mk<float>(0, 0, 0);
+    return r;
+}
+
+F3 count_color(uint32_t n) {
+    if (n == 0) return mk<float>(1, 0, 1);
+    if (n < 4) return lerp3(mk<float>(1, 0, 0), mk<float>(1, 0.5f, 0), (float)(n - 1) / 3.0f);
+    if (n < 8) return lerp3(mk<float>(1, 1, 0), mk<float>(0, 1, 0), (float)(n - 4) / 4.0f);
+    if (n < 16) return lerp3(mk<float>(0, 1, 0), mk<float>(0, 1, 1), (float)(n - 8) / 8.0f);
+    if (n < 24) return lerp3(mk<float>(0, 1, 1), mk<float>(0, 0, 1), (float)(n - 16) / 8.0f);
+    return lerp3(mk<float>(0, 0, 1), mk<float>(1, 1, 1), (float)(std::min(n, 32u) - 24) / 8.0f);
+}
+
+F3 support_color(float s) {
+    float v = sat(s);
+    if (v < 0.25f) return lerp3(mk<float>(1, 0, 1), mk<float>(1, 0, 0), v * 4.0f);
+    if (v < 0.5f) return lerp3(mk<float>(1, 0, 0), mk<float>(1, 1, 0), (v - 0.25f) * 4.0f);
+    if (v < 0.75f) return lerp3(mk<float>(1, 1, 0), mk<float>(0, 1, 0), (v - 0.5f) * 4.0f);
+    return lerp3(mk<float>(0, 1, 0), mk<float>(0, 0.25f, 1), (v - 0.75f) * 4.0f);
+}
+
+F3 density_color(float s, float maxd) {
+    float mx = std::fmax(maxd, 1.0f);
+    float density = std::fmin(mx, 1.0f / std::fmax(sat(s), 1.0f / mx));
+    float normalized = mx > 1.0f ? spec_log2(density) / spec_log2(mx) : 0.0f;
+    return support_color(1.0f - sat(normalized));
+}
+
+F3 self_hit_color(float rate) {
+    if (rate <= 0.0f) return mk<float>(0, 0, 0.25f);
+    float lr = spec_log2(std::fmax(rate, 1e-6f)) / spec_log2(10.0f);
+    float v = sat((lr + 6.0f) / 5.0f);
+    if (v < 1.0f / 3.0f) return lerp3(mk<float>(0, 0, 0.25f), mk<float>(0, 1, 1), v * 3.0f);
+    if (v < 2.0f / 3.0f) return lerp3(mk<float>(0, 1, 1), mk<float>(1, 1, 0), (v - 1.0f / 3.0f) * 3.0f);
+    return lerp3(mk<float>(1, 1, 0), mk<float>(1, 0, 0), (v - 2.0f / 3.0f) * 3.0f);
+}
+
+F3 decode_rgbm(uint32_t packed, float range) {
+    float x = (float)(packed & 255u) / 255.0f, y = (float)((packed >> 8) & 255u) / 255.0f;
+    float z = (float)((packed >> 16) & 255u) / 255.0f, w = (float)((packed >> 24) & 255u) / 255.0f;
+    return (mk<float>(x, y, z) * w) * range;
+}
+
+}  // namespace probe_resolve
+
+void resolve_probe_pixel(Tracer<float>& tr, const OracleCamera& cam, uint32_t w, uint32_t h, uint32_t px,
+                         uint32_t py, const probe_resolve::Layout& l, const OracleProbeResolveOptions& o, float* out,
+                         bool* bad) {
+    using namespace probe_resolve;
+    float pxf = ((float)px + 0.5f) / (float)w;
+    float pyf = ((float)py + 0.5f) / (float)h;
+    pxf = pxf + (-cam.jitter_x);
+    pyf = pyf + cam.jitter_y;
+    float nx = 2.0f * pxf + -1.0f;
+    float ny = -2.0f * pyf + 1.0f;
+    F3 U = load3<float>(cam.image_u), Vv = load3<float>(cam.image_v), W = load3<float>(cam.image_w);
+    F3 dir = normalize((nx * U + ny * Vv) + W);
+    float inv_cos = 1.0f / dot(normalize(W), dir);
+    F3 org = load3<float>(cam.position);
+    HitRec hit = tr.closest(org, dir, cam.near_clip * inv_cos, cam.far_clip * inv_cos);
+    uint32_t view = std::min(o.debug_view, 7u);
+    bool beauty = view == 0 || view == 6;
+    auto put = [&](F3 c) {
+        out[0] = c.x;
+        out[1] = c.y;
+        out[2] = c.z;
+        out[3] = 1.0f;
+    };
+    if (!hit.valid) {
+        F3 c = mk<float>(0.02f, 0.02f, 0.02f);
+        if (beauty) {
+            c = tr.L.sky;
+            if (tr.L.sun_disk) c = c + tr.sun_disk(dir);
+        }
+        put(c);
+        return;
+    }
+    uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
+    float b1 = hit.b1, b2 = hit.b2;
+    Shading<float> sd = shading_data<float>(tr.s, inst, prim, b1, b2, -dir);
+    F3 sun = mk<float>(0, 0, 0);
+    if (beauty) {
+        Rng rng(px, py, o.frame_index);
+        float ux = rng.next_1d();
+        float uy = rng.next_1d();
+        sun = tr.sun_nee(sd, ux, uy);
+    }
+    if (inst >= l.instance_count) {
+        *bad = true;
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+        return;
+    }
+    Instance ins = load_instance(l, inst);
+    if (ins.offsets[3] == 0) {
+        put(beauty ? sd.emissive + sun : count_color(0));
+        return;
+    }
+    Recon r = reconstruct(l, ins, sd.position, normalize(sd.face_normal), o.min_gather_count,
+                          o.use_radial_visibility != 0, bad);
+    uint32_t side = sd.back_side ? 1u : 0u;
+    float b0 = (1.0f - b1) - b2;
+    float bary[3] = {b0, b1, b2};
+    F3 vertex_irr = mk<float>(0, 0, 0);
+    bool has_fallback = false;
+    if (o.use_vertex_fallback) {
+        uint32_t rec = ins.map_offset + prim * 2u + side;
+        if (rec >= l.tri_map_count) {
+            *bad = true;
+        } else {
+            const uint32_t* a = l.tri_map + 4 * (size_t)rec;
+            if (a[3] & 1u) {
+                F3 acc = mk<float>(0, 0, 0);
+                float avail = 0.0f;
+                for (int c = 0; c < 3; ++c) {
+                    if (a[c] >= l.probe_count) {
+                        *bad = true;
+                        continue;
+                    }
+                    if (l.counts[a[c]] == 0) continue;
+                    acc = acc + bary[c] * pirr(l, a[c]);
+                    avail = avail + bary[c];
+                }
+                if (avail > 1e-6f) {
+                    vertex_irr = mk<float>(acc.x / avail, acc.y / avail, acc.z / avail);
+                    has_fallback = true;
+                }
+            }
+        }
+    }
+    float target = (float)std::min(std::max(o.min_gather_count, 1u), 32u);
+    float conf = std::fmin(sat((float)r.gathered / target), sat(r.ess / target));
+    if (r.weight_sum <= 1e-6f) conf = 0.0f;
+    if (!has_fallback) conf = 1.0f;
+    float fallback_weight = 1.0f - conf;
+    F3 irr = lerp3(vertex_irr, r.irradiance, conf);
+    if (view == 1) return put(count_color(r.gathered));
+    if (view == 2) return put(support_color(r.support));
+    if (view == 3) return put(density_color(r.support, o.max_density_multiplier));
+    if (view == 4) return put(support_color(1.0f - fallback_weight));
+    if (view == 5) return put(self_hit_color(r.self_hit_rate));
+    bool has_vl = false;
+    F3 vl = mk<float>(0, 0, 0);
+    float vl_conf = 0.0f;
+    float range = std::fmax(o.vertex_lighting_rgbm_range, 1.0f);
+    if (o.vertex_lighting_rgbm) {
+        uint32_t io = o.vertex_lighting_instance_offsets[2 * (size_t)inst];
+        uint32_t rec = io + prim * 2u + side;
+        if (rec >= o.vertex_lighting_triangle_record_count) {
+            *bad = true;
+        } else {
+            const uint32_t* vv = o.vertex_lighting_triangle_map + 4 * (size_t)rec;
+            if (vv[3] != 0) {
+                uint32_t nv = o.vertex_lighting_vertex_count;
+                if (vv[0] >= nv || vv[1] >= nv || vv[2] >= nv) {
+                    *bad = true;
+                } else {
+                    const float* t = o.vertex_lighting_target;
+                    vl = (b0 * decode_rgbm(o.vertex_lighting_rgbm[vv[0]], range) +
+                          b1 * decode_rgbm(o.vertex_lighting_rgbm[vv[1]], range)) +
+                         b2 * decode_rgbm(o.vertex_lighting_rgbm[vv[2]], range);
+                    vl_conf = (b0 * t[4 * (size_t)vv[0] + 3] + b1 * t[4 * (size_t)vv[1] + 3]) +
+                              b2 * t[4 * (size_t)vv[2] + 3];
+                    has_vl = true;
+                }
+            }
+        }
+    }
+    if (view == 6)
+        return put(has_vl ? (sd.emissive + sun) + (sd.diffuse * Consts<float>::INV_PI) * vl : mk<float>(1, 0, 1));
+    if (view == 7) return put(has_vl ? support_color(vl_conf) : mk<float>(1, 0, 1));
+    if (o.use_vertex_lighting && has_vl) irr = vl;
+    put((sd.emissive + sun) + (sd.diffuse * Consts<float>::INV_PI) * irr);
+}
+
+}  // namespace
+
+extern "C" {
+
+float own_exp(float x) { return spec_exp(x); }
+float own_log2(float x) { return spec_log2(x); }
+
+int oracle_resolve_probes(void* sp, const OracleLighting* lighting, const OracleCamera* camera, uint32_t width,
+                          uint32_t height, const uint32_t* pixels, int pixel_count, const float* probes,
+                          uint32_t probe_count, const uint32_t* nodes, uint32_t node_count, const float* instances,
+                          uint32_t instance_count, const uint32_t* triangle_vertex_probes,
+                          uint32_t triangle_vertex_probe_count, const float* values, const uint32_t* sample_counts,
+                          const uint32_t* self_hits, const uint32_t* radial, const OracleProbeResolveOptions* options,
+                          int threads, float* out) {
+    Scene* s = static_cast<Scene*>(sp);
+    probe_resolve::Layout l{probes, nodes, instances, triangle_vertex_probes, probe_count, node_count,
+                            instance_count, triangle_vertex_probe_count, values, sample_counts, self_hits, radial};
+    std::atomic<int> bad{0};
+    parallel_for(pixel_count, threads, [&](int i, int) {
+        Tracer<float> tr(*s, *lighting);
+        bool b = false;
+        resolve_probe_pixel(tr, *camera, width, height, pixels[2 * i], pixels[2 * i + 1], l, *options,
+                            out + 4 * (size_t)i, &b);
+        if (b) bad = 1;
+    });
+    return bad.load() ? 4 : 0;
 }
 
 int oracle_filter_mesh_colors(const uint32_t* face_infos, const uint32_t* instance_infos, const uint32_t* side_infos,

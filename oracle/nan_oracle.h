@@ -141,6 +141,42 @@ int oracle_resolve_mesh_colors(void* scene, const OracleLighting* lighting,
                                const void* colors, int packed, int precision, int threads,
                                float* out);
 
+/* Options of the surface-probe resolve (the layout of NanProbeResolveOptions,
+ * host pointers). */
+typedef struct OracleProbeResolveOptions {
+    uint32_t debug_view;
+    uint32_t min_gather_count;
+    uint32_t use_vertex_fallback;
+    uint32_t use_vertex_lighting;
+    uint32_t use_radial_visibility;
+    uint32_t frame_index;
+    float max_density_multiplier;
+    float vertex_lighting_rgbm_range;
+    const uint32_t* vertex_lighting_rgbm;
+    const float* vertex_lighting_target;
+    const uint32_t* vertex_lighting_triangle_map;
+    const uint32_t* vertex_lighting_instance_offsets;
+    uint32_t vertex_lighting_vertex_count;
+    uint32_t vertex_lighting_triangle_record_count;
+} OracleProbeResolveOptions;
+
+/* Surface-probe resolve (surface_probe_resolve.slang:325-472) of the listed
+ * pixels u32[N][2] into out f32[N][4]; returns 4 when a layout index was out
+ * of range (that access skipped), else 0. */
+int oracle_resolve_probes(void* scene, const OracleLighting* lighting, const OracleCamera* camera,
+                          uint32_t width, uint32_t height, const uint32_t* pixels, int pixel_count,
+                          const float* probes, uint32_t probe_count, const uint32_t* nodes,
+                          uint32_t node_count, const float* instances, uint32_t instance_count,
+                          const uint32_t* triangle_vertex_probes, uint32_t triangle_vertex_probe_count,
+                          const float* values, const uint32_t* sample_counts, const uint32_t* self_hits,
+                          const uint32_t* radial, const OracleProbeResolveOptions* options, int threads,
+                          float* out);
+
+/* e^x and log2 x of the kernels' own float implementations (nan_exp,
+ * nan_log2), for tests against the C library. */
+float own_exp(float x);
+float own_log2(float x);
+
 /* One pass of the Mesh Colors one-ring surface filter over every texel of
  * every instance (mesh_colors_surface_filter.slang:1-253): source and
  * destination are 16-byte slot buffers. */

@@ -35,6 +35,25 @@ class OracleLighting(ctypes.Structure):
     ]
 
 
+class OracleProbeResolveOptions(ctypes.Structure):
+    _fields_ = [
+        ("debug_view", ctypes.c_uint32),
+        ("min_gather_count", ctypes.c_uint32),
+        ("use_vertex_fallback", ctypes.c_uint32),
+        ("use_vertex_lighting", ctypes.c_uint32),
+        ("use_radial_visibility", ctypes.c_uint32),
+        ("frame_index", ctypes.c_uint32),
+        ("max_density_multiplier", ctypes.c_float),
+        ("vertex_lighting_rgbm_range", ctypes.c_float),
+        ("vertex_lighting_rgbm", ctypes.c_void_p),
+        ("vertex_lighting_target", ctypes.c_void_p),
+        ("vertex_lighting_triangle_map", ctypes.c_void_p),
+        ("vertex_lighting_instance_offsets", ctypes.c_void_p),
+        ("vertex_lighting_vertex_count", ctypes.c_uint32),
+        ("vertex_lighting_triangle_record_count", ctypes.c_uint32),
+    ]
+
+
 class OracleCamera(ctypes.Structure):
     _fields_ = [
         ("position", ctypes.c_float * 3),
@@ -110,6 +129,12 @@ def _declare(l: ctypes.CDLL) -> None:
                                       u32, u32, u32, i, i, i, vp]
     l.oracle_trace_probes_independent.argtypes = l.oracle_trace_probes.argtypes
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
+    l.oracle_resolve_probes.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
+                                        vp, vp, i, vp]
+    l.own_exp.argtypes = [ctypes.c_float]
+    l.own_exp.restype = ctypes.c_float
+    l.own_log2.argtypes = [ctypes.c_float]
+    l.own_log2.restype = ctypes.c_float
     l.oracle_prt_project_lighting.argtypes = [vp, u32, vp]
     l.oracle_prt_project_lighting.restype = None
     l.oracle_prt_evaluate.argtypes = [vp, vp, vp, vp, vp, vp, u32]
@@ -134,6 +159,16 @@ def filter_mesh_colors(face_infos, instance_infos, side_infos, adjacency, face_n
     lib().oracle_filter_mesh_colors(_p(fi), _p(ii), _p(si), ii.shape[0], _p(adj), _p(nrm), _p(src), _p(dst),
                                     float(neighbor_weight), float(normal_sigma_radians), threads)
     return dst
+
+
+def own_exp(x: float) -> float:
+    """The kernels' own float e^x (nan_exp)."""
+    return float(lib().own_exp(float(x)))
+
+
+def own_log2(x: float) -> float:
+    """The kernels' own float log2 (nan_log2)."""
+    return float(lib().own_log2(float(x)))
 
 
 def prt_project_lighting(lighting, sample_count=2048):
@@ -366,6 +401,37 @@ class OracleScene:
                                               int(bool(packed)), precision, threads, _p(out))
         if rc != 0:
             raise RuntimeError(lib().oracle_last_error().decode())
+        return out
+
+    def resolve_probes(self, lighting, camera, width, height, pixels, layout, values, sample_counts, self_hits,
+                       radial, *, debug_view=0, min_gather_count=4, use_radial_visibility=True,
+                       use_vertex_fallback=False, frame_index=0, max_density_multiplier=8.0, threads=0):
+        """Surface-probe resolve of pixels u32[N, 2] against a probe layout
+        (probes, nodes, instance_gpu_data, triangle_vertex_probes) and an
+        irradiance field; returns f32[N, 4]. Raises on an out-of-range index."""
+        px = np.ascontiguousarray(pixels, dtype=np.uint32).reshape(-1, 2)
+        pr = np.ascontiguousarray(layout.probes).view(np.float32).reshape(-1, 12)
+        nd = np.ascontiguousarray(layout.nodes, dtype=np.uint32).reshape(-1, 4)
+        ins = np.ascontiguousarray(layout.instance_gpu_data).view(np.float32).reshape(-1, 12)
+        tm = np.ascontiguousarray(layout.triangle_vertex_probes, dtype=np.uint32).reshape(-1, 4)
+        v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1, 3)
+        c = np.ascontiguousarray(sample_counts).view(np.uint32).reshape(-1)
+        sh = np.ascontiguousarray(self_hits).view(np.uint32).reshape(-1)
+        rm = np.ascontiguousarray(radial).view(np.uint32).reshape(-1, 16)
+        opt = OracleProbeResolveOptions(debug_view=int(debug_view), min_gather_count=int(min_gather_count),
+                                        use_vertex_fallback=int(bool(use_vertex_fallback)),
+                                        use_radial_visibility=int(bool(use_radial_visibility)),
+                                        frame_index=int(frame_index) & 0xFFFFFFFF,
+                                        max_density_multiplier=float(max_density_multiplier),
+                                        vertex_lighting_rgbm_range=1.0)
+        out = np.zeros((px.shape[0], 4), np.float32)
+        L, C = lighting_struct(lighting), camera_struct(camera)
+        rc = lib().oracle_resolve_probes(self.handle, ctypes.byref(L), ctypes.byref(C), width, height, _p(px),
+                                         px.shape[0], _p(pr), pr.shape[0], _p(nd), nd.shape[0], _p(ins),
+                                         ins.shape[0], _p(tm), tm.shape[0], _p(v), _p(c), _p(sh), _p(rm),
+                                         ctypes.byref(opt), threads, _p(out))
+        if rc != 0:
+            raise RuntimeError("probe resolve: a layout index is out of range")
         return out
 
     def trace_probes_prt(self, lighting, values, sample_counts, self_hits, radial, static_source, probes,

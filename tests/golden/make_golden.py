@@ -8,8 +8,9 @@ Run in a container that holds the reference project (default root
 It imports the reference's numpy reference functions -- the RGB9E5 pack/unpack
 of ``test_mesh_colors_rgb9e5.py:15-50``, the hemi-oct encode/decode of
 ``surface_probes.py:45-110``, the Mesh Colors lattice math of
-``mesh_colors.py:24-79`` and the FP64 brute-force any-hit caster of
-``vertex_baker/visibility_baker.py:348-402`` -- with the graphics-only modules
+``mesh_colors.py:24-79``, the FP64 brute-force any-hit caster of
+``vertex_baker/visibility_baker.py:348-402``, and the point octree builder and
+query of ``surface_probes.py:1348-1438, 3007-3099`` -- with the graphics-only modules
 (slangpy, trimesh, pygltflib, PIL) replaced by inert stand-ins, evaluates them
 on seeded inputs, and writes ``reference_vectors.npz`` next to this file.
 The GPU box never runs this script; tests read the committed ``.npz`` only.
@@ -137,6 +138,62 @@ def main() -> None:
     out["vis_directions"] = directions
     out["vis_max_distance"] = np.asarray([1.25], dtype=np.float32)
     out["vis_occluded"] = occluded.astype(np.uint8)
+
+    # Point octree: the two cases of test_surface_probes.py:133-190 (boundary
+    # points on the float32 centre; a degenerate single-octant chain), and
+    # clustered sites on two facing sheets with the layout defaults, plus
+    # radius queries with and without the normal gate on the last one. Each
+    # case has its own generator so the vectors above stay as they were.
+    cases = []
+    a = np.random.default_rng(1234).uniform(-2.0, 3.0, size=(4097, 3)).astype(np.float32)
+    a[:8] = np.array([[0.5, 0.5, 0.5], [0.5, 0.5, -2.0], [0.5, -2.0, 0.5], [0.5, -2.0, -2.0],
+                      [-2.0, 0.5, 0.5], [-2.0, 0.5, -2.0], [-2.0, -2.0, 0.5], [-2.0, -2.0, -2.0]], np.float32)
+    cases.append((a, 8, 12))
+    cases.append((np.zeros((33, 3), np.float32), 1, 5))
+    crng = np.random.default_rng(77)
+    sheet = crng.uniform(0.0, 4.0, size=(3000, 2))
+    c = np.zeros((6000, 3), np.float32)
+    c[:3000, 0], c[:3000, 2] = sheet[:, 0], sheet[:, 1]
+    c[3000:, 0], c[3000:, 2] = sheet[:, 0], sheet[:, 1]
+    c[3000:, 1] = 0.05
+    c[100:140] = c[99]  # exact duplicates fill one leaf past capacity
+    cases.append((c, 8, 16))
+    for k, (pos, leaf, depth) in enumerate(cases):
+        nodes, order, center, extent = surface_probes._build_point_octree_python(
+            pos, leaf_capacity=leaf, max_depth=depth)
+        out[f"octree{k}_positions"] = pos
+        out[f"octree{k}_params"] = np.asarray([leaf, depth], np.uint32)
+        out[f"octree{k}_nodes"] = np.asarray(nodes, np.uint32)
+        out[f"octree{k}_order"] = np.asarray(order, np.int64)
+        out[f"octree{k}_root"] = np.asarray([*center, extent], np.float64)
+    pos = cases[2][0]
+    nodes, order, center, extent = surface_probes._build_point_octree_python(pos, leaf_capacity=8, max_depth=16)
+    probes = np.zeros(pos.shape[0], dtype=surface_probes.SURFACE_PROBE_DTYPE)
+    probes["position_radius"][:, :3] = pos[order]
+    normals = np.zeros((pos.shape[0], 3), np.float32)
+    normals[:3000, 1] = 1.0
+    normals[3000:, 1] = -1.0
+    probes["normal_side"][:, :3] = normals[order]
+    info = types.SimpleNamespace(node_offset=0, root_center=center, root_extent=extent, kernel_radius=0.3)
+    layout = types.SimpleNamespace(instance_infos=[info], nodes=nodes, probes=probes,
+                                   _sphere_intersects_cube=surface_probes.SurfaceProbeLayout._sphere_intersects_cube)
+    qrng = np.random.default_rng(91)
+    queries = np.concatenate([qrng.uniform(-0.2, 4.2, size=(200, 1)), qrng.uniform(-0.1, 0.15, size=(200, 1)),
+                              qrng.uniform(-0.2, 4.2, size=(200, 1))], axis=1)
+    radii = qrng.uniform(0.0, 0.6, size=200)
+    found, offsets, qnormals = [], [0], []
+    for i in range(200):
+        qn = None if i % 2 == 0 else (0.0, 1.0 if i % 4 == 1 else -1.0, 0.0)
+        r = None if i % 10 == 3 else float(radii[i])
+        idx = surface_probes.SurfaceProbeLayout.query_probe_indices(layout, 0, queries[i], radius=r, normal=qn)
+        found.append(np.asarray(idx, np.int64))
+        offsets.append(offsets[-1] + len(idx))
+        qnormals.append((0.0, 0.0, 0.0) if qn is None else qn)
+    out["octree_query_positions"] = queries
+    out["octree_query_radii"] = np.where(np.arange(200) % 10 == 3, -1.0, radii)
+    out["octree_query_normals"] = np.asarray(qnormals, np.float64)
+    out["octree_query_found"] = np.concatenate(found)
+    out["octree_query_offsets"] = np.asarray(offsets, np.int64)
 
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})
