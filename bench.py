@@ -62,6 +62,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batched probe measurement")
     ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box (area light) measurement")
     ap.add_argument("--no-city", action="store_true", help="skip the 4M-triangle city frame measurement")
+    ap.add_argument("--no-consumers", action="store_true",
+                    help="skip the resolve / filter / PRT / probe-resolve pass timings")
     ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
 
@@ -428,6 +430,10 @@ def run_nan(args):
         line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
     if world == 1 and not args.no_learned:
         line["learned_cache"] = learned_cache_line(device)
+    if world == 1 and not args.no_consumers:
+        from nan_b200 import consumers_eval
+
+        line["consumers"] = consumers_eval.measure(device, scene, node, layout, slots, frames=5)
     if world == 1 and not args.no_cornell:
         line["cornell_area_light"] = cornell_line(device)
     if world == 1 and not args.no_city:

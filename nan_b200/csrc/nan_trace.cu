@@ -692,23 +692,43 @@ __global__ void __launch_bounds__(128) k_trace_probes_prt(SceneView s, LightingR
 // samples summed in order. Evaluation is static + sum_c T_c * L_c, clamped
 // at 0, for probes with at least one sample.
 // ---------------------------------------------------------------------------
-__global__ void k_prt_project_lighting(LightingRaw lraw, float4* __restrict__ sh, uint32_t n) {
-    const uint32_t c = threadIdx.x;
-    if (c >= 9u) return;
+// 256 threads: each chunk of 256 sample directions is evaluated in parallel
+// into shared memory (sky * Y_c per coefficient and channel), then 27 threads
+// each add their own (coefficient, channel) column in sample order, so every
+// sum is the same sequential float sum as one loop over the samples.
+__global__ void __launch_bounds__(256) k_prt_project_lighting(LightingRaw lraw, float4* __restrict__ sh,
+                                                               uint32_t n) {
+    __shared__ float terms[27][256];
+    const uint32_t tid = threadIdx.x;
     const LightParams L = make_light(lraw);
     n = max(n, 1u);
-    f3 acc = mk3(0.0f, 0.0f, 0.0f);
-    for (uint32_t i = 0; i < n; ++i) {
-        const float u = (static_cast<float>(i) + 0.5f) / static_cast<float>(n);
-        const float v = static_cast<float>(__brev(i)) * 2.3283064365386963e-10f;
-        const float y = 1.0f - 2.0f * u;
-        const float r = sqrtf(fmaxf(1.0f - y * y, 0.0f));
-        float sn, cs;
-        nan_sincos(kTwoPi * v, &sn, &cs);
-        acc = acc + L.sky * sh_l2_basis(c, mk3(r * cs, y, r * sn));
+    float acc = 0.0f;
+    for (uint32_t base = 0; base < n; base += 256u) {
+        const uint32_t i = base + tid;
+        if (i < n) {
+            const float u = (static_cast<float>(i) + 0.5f) / static_cast<float>(n);
+            const float v = static_cast<float>(__brev(i)) * 2.3283064365386963e-10f;
+            const float y = 1.0f - 2.0f * u;
+            const float r = sqrtf(fmaxf(1.0f - y * y, 0.0f));
+            float sn, cs;
+            nan_sincos(kTwoPi * v, &sn, &cs);
+            const f3 d = mk3(r * cs, y, r * sn);
+            for (uint32_t c = 0; c < 9u; ++c) {
+                const f3 t = L.sky * sh_l2_basis(c, d);
+                terms[3 * c][tid] = t.x;
+                terms[3 * c + 1][tid] = t.y;
+                terms[3 * c + 2][tid] = t.z;
+            }
+        }
+        __syncthreads();
+        if (tid < 27u) {
+            const uint32_t m = min(256u, n - base);
+            for (uint32_t k = 0; k < m; ++k) acc = acc + terms[tid][k];
+        }
+        __syncthreads();
     }
-    acc = acc * ((4.0f * kPi) / static_cast<float>(n));
-    sh[c] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+    if (tid < 27u) reinterpret_cast<float*>(sh)[4u * (tid / 3u) + tid % 3u] = acc * ((4.0f * kPi) / static_cast<float>(n));
+    if (tid < 9u) reinterpret_cast<float*>(sh)[4u * tid + 3u] = 0.0f;
 }
 
 __global__ void k_prt_evaluate(const float* __restrict__ values, const uint32_t* __restrict__ counts,
@@ -961,7 +981,7 @@ int launch_trace_probes_prt(NanContext* ctx, float* values, uint32_t* counts, ui
 
 int launch_prt_project_lighting(NanContext* ctx, float* sh, uint32_t samples, const NanLighting* light,
                                 cudaStream_t st) {
-    k_prt_project_lighting<<<1, 32, 0, st>>>(to_raw(light), reinterpret_cast<float4*>(sh), samples);
+    k_prt_project_lighting<<<1, 256, 0, st>>>(to_raw(light), reinterpret_cast<float4*>(sh), samples);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "prt_project_lighting launch");
 }
