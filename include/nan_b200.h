@@ -157,6 +157,13 @@ typedef struct NanProbeResolveOptions {
     uint32_t vertex_lighting_triangle_record_count;
 } NanProbeResolveOptions;
 
+/* Options of the weighted sample elimination (SurfaceProbeWSEOptions,
+ * surface_probe_sampler.h:15-20, less the surface area, which is per set). */
+typedef struct NanWseOptions {
+    float normal_cosine_threshold;  /* 0.5 in the reference */
+    float plane_distance_scale;     /* 0.35 in the reference */
+} NanWseOptions;
+
 /* Execution choices of a context. The defaults (all zero) are the wavefront
  * integrator with occupancy-sized persistent traversal grids, as many paths
  * in flight as the reserved scratch holds, and the PLOC BVH builder. */
@@ -373,6 +380,25 @@ NAN_B200_API int nan_prt_project_lighting(NanContext* ctx, float* lighting_sh, u
 NAN_B200_API int nan_prt_evaluate(NanContext* ctx, const float* values, const uint32_t* sample_counts,
                                   const float* static_source, const float* lighting_sh, float* out_values,
                                   uint32_t* out_sample_counts, uint32_t probe_count, void* stream);
+
+/* Weighted sample elimination of surface-probe candidates
+ * (weighted_sample_elimination, surface_probes.py:897-985 and 1091-1123;
+ * surface_probe_wse_eliminate, surface_probe_sampler.h:120-130) for
+ * set_count candidate sets in one call. positions and normals are device
+ * f32[N][3] with the sets contiguous: set k is [set_offsets[k],
+ * set_offsets[k+1]). set_offsets (S+1), output_counts and surface_areas (S)
+ * are host arrays. keep (device u8[N]) gets 1 for the survivors: per set the
+ * output_count candidates (clamped to 1..count) that remain when, one at a
+ * time, the candidate of largest weight (lowest index on ties) is removed.
+ * poisson_radii (host f32[S], optional) gets d_max / 2 per set (the spacing
+ * sqrt(area / count) when nothing is eliminated); rounds (optional) the
+ * number of parallel elimination rounds. Contribution weights are rounded to
+ * units of 2^-50 so the sums are exact (NAN_ERR_LIMIT past 8000 neighbours). Allocates scratch on the stream and
+ * synchronizes it. */
+NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, const float* normals,
+                                   const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                                   const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
+                                   float* poisson_radii, uint32_t* rounds, void* stream);
 
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */

@@ -39,12 +39,20 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
     from .surface_probe_resources import SurfaceProbeGpuGeometry
 
+    from .surface_probe_layout import SurfaceProbeSiteLayout
+    from .surface_probe_sampler import SurfaceProbeSampler
+
     t0 = time.perf_counter()
     items, tris, sites = [], [], []
+    sampler = SurfaceProbeSampler(device)
+    placement = {"candidates": 0, "elimination_s": 0.0, "candidates_s": 0.0, "packing_s": 0.0}
     for i, (node, n_sites) in enumerate(sc.batch_scenes(count, seed, tri_max=tri_max)):
         scene = Scene(device, node)
-        probes, pinst = sc.surface_sites(node, n_sites, seed=seed + i, radius=0.25)
-        geometry = SurfaceProbeGpuGeometry.create(device, _sites_layout(probes, pinst))
+        prof: dict = {}
+        layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=seed + i, profile=prof)
+        for k in placement:
+            placement[k] += prof[k]
+        geometry = SurfaceProbeGpuGeometry.create(device, layout)
         baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=samples_per_probe,
                                                    max_bounces=max_bounces, compensated=True)
         rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)
@@ -106,7 +114,9 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
         "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
         "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
         "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
-        "setup_s": setup_s, "autotune": tuned, "autotune_independent_samples": tuned_ind,
+        "setup_s": setup_s, "site_placement": dict(placement, method="weighted sample elimination on the GPU, "
+                                                                   "5x oversampled area-weighted candidates"),
+        "autotune": tuned, "autotune_independent_samples": tuned_ind,
         "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
                          "batched": batch_ms, "batched_graph": graph_ms,
                          "batched_graph_independent_samples": ind_ms},
@@ -140,10 +150,14 @@ def main() -> None:
     a = ap.parse_args()
     device = Device(0)
     items = []
+    from .surface_probe_layout import SurfaceProbeSiteLayout
+    from .surface_probe_sampler import SurfaceProbeSampler
+
+    sampler = SurfaceProbeSampler(device)
     for i, (node, n_sites) in enumerate(sc.batch_scenes(a.count, 1)):
         scene = Scene(device, node)
-        probes, pinst = sc.surface_sites(node, n_sites, seed=1 + i, radius=0.25)
-        geometry = SurfaceProbeGpuGeometry.create(device, _sites_layout(probes, pinst))
+        geometry = SurfaceProbeGpuGeometry.create(
+            device, SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=1 + i))
         baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
                                                    compensated=True)
         rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)

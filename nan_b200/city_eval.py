@@ -1,8 +1,9 @@
 """One frame of the large workload on the seeded 4.16 M-triangle city
 (scenes.city): the screen at 3840x2160 with 4 spp and 5 path vertices (the
 learned-cache path tracer, and the plain one for comparison), a 20,480-site
-surface-probe pass (64 spp, 3 bounces, compensated sums, batched launch with
-one RNG stream per sample) and
+surface-probe pass (sites by weighted sample elimination of 5x oversampled
+candidates on the GPU; 64 spp, 3 bounces, compensated sums, batched launch
+with one RNG stream per sample) and
 a Mesh Colors texel pass over the whole city (about 12.6 M texels, 1 sample,
 3 bounces). Every pass is timed with CUDA events on the launching stream
 after one warm-up frame; rays are counted on the device.
@@ -18,7 +19,6 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
 
     from . import scenes as sc
     from .accumulator import Accumulator
-    from .batch_eval import _sites_layout
     from .cached_path_tracer import CachedPathTracer
     from .learned_eval import scene_bounds
     from .mesh_colors import MeshColorsLayout
@@ -29,7 +29,9 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     from .scene import Scene
     from .surface_probe_fields import SurfaceProbeRuntimeBuffers
     from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from .surface_probe_layout import SurfaceProbeSiteLayout
     from .surface_probe_resources import SurfaceProbeGpuGeometry
+    from .surface_probe_sampler import SurfaceProbeSampler
     from .texture_space_path_tracer import TextureSpacePathTracer
 
     t0 = time.perf_counter()
@@ -37,8 +39,12 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     node.lighting.ray_t_max = 5000.0  # the city's diagonal exceeds the reference's 1000
     scene = Scene(device, node)
     layout = MeshColorsLayout.build(node, texels_per_unit=0.1, min_resolution=1, max_resolution=64)
-    probes, pinst = sc.surface_sites(node, 20480, seed=1, radius=2.0)
     host_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    placement: dict = {}
+    sites = SurfaceProbeSiteLayout.build_wse(node, 20480, sampler=SurfaceProbeSampler(device), seed=1,
+                                             profile=placement)
+    placement["total_s"] = time.perf_counter() - t1
     info = scene.info()
     rd = RenderData(device)
     dev = device.torch_device
@@ -84,7 +90,7 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     res = {"screen_plain": timed(screen_plain, scene.context)}
     res["screen_learned_cache"] = timed(screen_cached, scene.context)
 
-    geometry = SurfaceProbeGpuGeometry.create(device, _sites_layout(probes, pinst))
+    geometry = SurfaceProbeGpuGeometry.create(device, sites)
     baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
                                                compensated=True)
     rt = SurfaceProbeRuntimeBuffers.acquire(rd, geometry.probe_count)
@@ -101,7 +107,7 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     return {
         "scene": f"seeded city: 20,000 boxes (log-normal heights mu 2, sigma 0.7) on a 2 km grid + ground, "
                  f"{info['triangle_count']} triangles, sun 30 deg + sky 0.5, t_max 5000",
-        "bvh_build_ms": info["build_ms"], "host_setup_s": host_s,
+        "bvh_build_ms": info["build_ms"], "host_setup_s": host_s, "site_placement": placement,
         "screen": f"{width}x{height}, {spp} spp, 5 path vertices", "probe_sites": int(geometry.probe_count),
         "texels": int(layout.total_surface_texels), "passes": res,
         "frame_ms_learned_screen_probes_texels": frame_ms,

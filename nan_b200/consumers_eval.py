@@ -1,7 +1,8 @@
 """Timing of the passes that consume the accumulated caches, on the
 texel-tracer workload's scene and slots: Mesh Colors resolve (16-byte slots
 and RGB9E5), the RGB9E5 pack, one surface-filter pass over every slot, and
-on 20,480 probe sites placed on the same scene: the irradiance and PRT L2
+on 20,480 probe sites placed on the same scene by weighted sample
+elimination of 5x oversampled candidates: the irradiance and PRT L2
 bakers (16 spp, 3 bounces), the PRT evaluation and the probe resolve. Every
 pass runs once untimed, then `frames` times between CUDA events on the
 launching stream; rates are per second of that device time.
@@ -67,8 +68,9 @@ def measure(device, scene, node, layout, slots, *, frames: int = 5, width: int =
     del dst, packed
 
     t0 = time.perf_counter()
-    sites = SurfaceProbeSiteLayout.build(node, probe_sites, seed=1)
-    res["probe_layout_host_s"] = time.perf_counter() - t0
+    placement: dict = {}
+    sites = SurfaceProbeSiteLayout.build_wse(node, probe_sites, device=device, seed=1, profile=placement)
+    res["probe_site_placement"] = dict(placement, total_s=time.perf_counter() - t0)
     geometry = SurfaceProbeGpuGeometry.create(device, sites)
     n = sites.total_probe_count
     rd = RenderData(device)

@@ -1,6 +1,7 @@
 // nan_abi.cu -- the extern "C" entry points declared in include/nan_b200.h.
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -439,6 +440,30 @@ NAN_B200_API int nan_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* l
         return invalid("vertex lighting needs target, triangle map and instance offsets (aligned)");
     return nan_host::launch_resolve_probes(ctx, layout, values, sample_counts, self_hits, radial, options, out, width,
                                            height, camera, lighting, as_stream(stream));
+}
+
+NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, const float* normals,
+                                   const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                                   const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
+                                   float* poisson_radii, uint32_t* rounds, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!set_offsets || !options || (set_count && (!output_counts || !surface_areas)))
+        return invalid("null argument");
+    if (set_count > 65536u) return invalid("at most 65536 candidate sets per call");
+    if (set_offsets[0] != 0u) return invalid("set_offsets[0] must be 0");
+    for (uint32_t k = 0; k < set_count; ++k) {
+        if (set_offsets[k + 1] < set_offsets[k]) return invalid("set_offsets must be non-decreasing");
+        if (!(surface_areas[k] > 0.0f) || !std::isfinite(surface_areas[k]))
+            return invalid("surface areas must be positive and finite");
+    }
+    if (!(options->normal_cosine_threshold >= -1.0f && options->normal_cosine_threshold <= 1.0f) ||
+        !(options->plane_distance_scale > 0.0f) || !std::isfinite(options->plane_distance_scale))
+        return invalid("normal cosine threshold must be in [-1, 1] and plane distance scale positive");
+    const uint32_t n = set_offsets[set_count];
+    if (n && (!positions || !normals || !keep)) return invalid("null buffer");
+    return nan_host::launch_wse_eliminate(ctx, positions, normals, set_offsets, set_count, output_counts,
+                                          surface_areas, options, keep, poisson_radii, rounds, as_stream(stream));
 }
 
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {

@@ -159,6 +159,10 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
 int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const void* colors, int packed,
                                float* out, uint32_t w, uint32_t h, const NanCamera* cam, const NanLighting* light,
                                cudaStream_t st);
+int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* normals, const uint32_t* set_offsets,
+                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
+                         const NanWseOptions* opt, uint8_t* keep, float* poisson_radii, uint32_t* rounds_out,
+                         cudaStream_t st);
 int launch_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* lay, const float* values,
                           const uint32_t* counts, const uint32_t* self_hits, const uint32_t* radial,
                           const NanProbeResolveOptions* opt, float* out, uint32_t w, uint32_t h,

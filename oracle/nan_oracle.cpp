@@ -27,6 +27,9 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <queue>
+#include <tuple>
+#include <unordered_map>
 #include <string>
 #include <thread>
 #include <vector>
@@ -2469,9 +2472,126 @@ void resolve_probe_pixel(Tracer<float>& tr, const OracleCamera& cam, uint32_t w,
     put((sd.emissive + sun) + (sd.diffuse * Consts<float>::INV_PI) * irr);
 }
 
+// ---------------------------------------------------------------------------
+// Weighted sample elimination, surface_probes.py:897-985, run as the
+// reference runs it: one candidate at a time, the largest weight first
+// (lowest index on ties), with a max-heap and stale-entry versions. The
+// neighbour test and contribution (1 - d/d_max)^8 are evaluated in float64 in
+// the reference's order; each contribution is rounded to units of 2^-50 and
+// the weights are integer sums of those units.
+// ---------------------------------------------------------------------------
+long long wse_contribution(const float* pos, const float* nrm, uint32_t i, uint32_t j, double d_max,
+                           double plane_limit, double ncos) {
+    const double dx = (double)pos[3 * j] - (double)pos[3 * i];
+    const double dy = (double)pos[3 * j + 1] - (double)pos[3 * i + 1];
+    const double dz = (double)pos[3 * j + 2] - (double)pos[3 * i + 2];
+    const double d2 = (dx * dx + dy * dy) + dz * dz;
+    if (!(d2 > 1e-20) || !(d2 < d_max * d_max)) return 0;
+    const double nix = nrm[3 * i], niy = nrm[3 * i + 1], niz = nrm[3 * i + 2];
+    const double njx = nrm[3 * j], njy = nrm[3 * j + 1], njz = nrm[3 * j + 2];
+    const double ndot = (njx * nix + njy * niy) + njz * niz;
+    if (!(ndot >= ncos)) return 0;
+    const double pa = std::fabs((dx * nix + dy * niy) + dz * niz);
+    const double pb = std::fabs((dx * njx + dy * njy) + dz * njz);
+    if (!(pa <= plane_limit) || !(pb <= plane_limit)) return 0;
+    const double base = std::fmax(1.0 - std::sqrt(d2) / d_max, 0.0);
+    const double b2 = base * base;
+    const double b4 = b2 * b2;
+    return std::llrint((b4 * b4) * 1125899906842624.0);
+}
+
+bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, uint32_t out, double d_max,
+             double plane_limit, double ncos, uint8_t* keep, uint32_t* order) {
+    const uint32_t n = end - begin;
+    struct Key {
+        long long x, y, z;
+        bool operator==(const Key& o) const { return x == o.x && y == o.y && z == o.z; }
+    };
+    struct KeyHash {
+        size_t operator()(const Key& k) const {
+            return (size_t)(k.x * 73856093LL) ^ (size_t)(k.y * 19349663LL) ^ (size_t)(k.z * 83492791LL);
+        }
+    };
+    const double inv = 1.0 / std::max(d_max, 1e-8);
+    std::unordered_map<Key, std::vector<uint32_t>, KeyHash> grid;
+    std::vector<Key> cell(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t i = begin + k;
+        cell[k] = {(long long)std::floor((double)pos[3 * i] * inv), (long long)std::floor((double)pos[3 * i + 1] * inv),
+                   (long long)std::floor((double)pos[3 * i + 2] * inv)};
+        grid[cell[k]].push_back(i);
+    }
+    std::vector<std::vector<std::pair<uint32_t, long long>>> adj(n);
+    std::vector<long long> w(n, 0);
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t i = begin + k;
+        for (long long dz = -1; dz <= 1; ++dz)
+            for (long long dy = -1; dy <= 1; ++dy)
+                for (long long dx = -1; dx <= 1; ++dx) {
+                    auto it = grid.find({cell[k].x + dx, cell[k].y + dy, cell[k].z + dz});
+                    if (it == grid.end()) continue;
+                    for (uint32_t j : it->second) {
+                        if (j == i) continue;
+                        const long long q = wse_contribution(pos, nrm, i, j, d_max, plane_limit, ncos);
+                        if (q <= 0) continue;
+                        adj[k].push_back({j - begin, q});
+                        w[k] += q;
+                    }
+                }
+    }
+    for (uint32_t k = 0; k < n; ++k)
+        if (adj[k].size() > 8000) return false;  // the GPU's bound on integer weights
+    std::vector<uint8_t> active(n, 1);
+    std::vector<uint32_t> version(n, 0);
+    // max-heap on (weight, -index); stale entries are skipped by version
+    std::priority_queue<std::tuple<long long, long long, uint32_t>> heap;
+    for (uint32_t k = 0; k < n; ++k) heap.push({w[k], -(long long)k, 0u});
+    uint32_t remaining = n, step = 0;
+    while (remaining > out && !heap.empty()) {
+        auto [wk, neg, ver] = heap.top();
+        heap.pop();
+        const uint32_t k = (uint32_t)(-neg);
+        if (!active[k] || version[k] != ver) continue;
+        active[k] = 0;
+        --remaining;
+        if (order) order[begin + step] = begin + k;
+        ++step;
+        for (auto [j, q] : adj[k]) {
+            if (!active[j]) continue;
+            w[j] = std::max<long long>(0, w[j] - q);
+            version[j] += 1;
+            heap.push({w[j], -(long long)j, version[j]});
+        }
+        (void)wk;
+    }
+    for (uint32_t k = 0; k < n; ++k) keep[begin + k] = active[k];
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
+
+int oracle_wse_eliminate(const float* positions, const float* normals, const uint32_t* set_offsets,
+                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
+                         float normal_cosine_threshold, float plane_distance_scale, uint8_t* keep,
+                         float* poisson_radii, uint32_t* order, int threads) {
+    std::atomic<int> bad{0};
+    parallel_for((int)set_count, threads, [&](int k, int) {
+        const uint32_t b = set_offsets[k], e = set_offsets[k + 1];
+        const uint32_t count = e - b;
+        const uint32_t out = std::max(1u, std::min(output_counts[k], std::max(count, 1u)));
+        const double area = std::max((double)surface_areas[k], 1e-20);
+        const double r = std::sqrt(area / (2.0 * std::sqrt(3.0) * (double)out));
+        const double d_max = std::max(2.0 * r, 1e-6);
+        const double plane_limit = std::max(d_max * (double)plane_distance_scale, 1e-8);
+        if (poisson_radii) poisson_radii[k] = count == out ? (float)std::sqrt(area / out) : (float)(d_max * 0.5);
+        if (!wse_set(positions, normals, b, e, out, d_max, plane_limit, (double)normal_cosine_threshold, keep,
+                     order))
+            bad = 1;
+    });
+    return bad.load() ? 3 : 0;
+}
 
 float own_exp(float x) { return spec_exp(x); }
 float own_log2(float x) { return spec_log2(x); }

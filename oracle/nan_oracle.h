@@ -172,6 +172,17 @@ int oracle_resolve_probes(void* scene, const OracleLighting* lighting, const Ora
                           const uint32_t* radial, const OracleProbeResolveOptions* options, int threads,
                           float* out);
 
+/* Weighted sample elimination (surface_probes.py:897-985), one candidate at
+ * a time with a heap, for each contiguous candidate set: keep u8[N] marks
+ * the survivors, poisson_radii f32[S] gets d_max / 2, order (optional
+ * u32[N]) the eliminated candidates of each set in removal order from the
+ * set's first slot. Contributions are rounded to 2^-50 units as in
+ * nan_wse_eliminate. */
+int oracle_wse_eliminate(const float* positions, const float* normals, const uint32_t* set_offsets,
+                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
+                         float normal_cosine_threshold, float plane_distance_scale, uint8_t* keep,
+                         float* poisson_radii, uint32_t* order, int threads);
+
 /* e^x and log2 x of the kernels' own float implementations (nan_exp,
  * nan_log2), for tests against the C library. */
 float own_exp(float x);

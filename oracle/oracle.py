@@ -131,6 +131,7 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
     l.oracle_resolve_probes.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
                                         vp, vp, i, vp]
+    l.oracle_wse_eliminate.argtypes = [vp, vp, vp, u32, vp, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, i]
     l.own_exp.argtypes = [ctypes.c_float]
     l.own_exp.restype = ctypes.c_float
     l.own_log2.argtypes = [ctypes.c_float]
@@ -159,6 +160,27 @@ def filter_mesh_colors(face_infos, instance_infos, side_infos, adjacency, face_n
     lib().oracle_filter_mesh_colors(_p(fi), _p(ii), _p(si), ii.shape[0], _p(adj), _p(nrm), _p(src), _p(dst),
                                     float(neighbor_weight), float(normal_sigma_radians), threads)
     return dst
+
+
+def wse_eliminate(positions, normals, set_offsets, output_counts, surface_areas, normal_cosine_threshold=0.5,
+                  plane_distance_scale=0.35, threads=0):
+    """Sequential weighted sample elimination per contiguous set; returns
+    (keep u8[N], poisson radii f32[S], removal order u32[N] per set from its
+    first slot, ~0 past the eliminated ones)."""
+    p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    nrm = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    off = np.ascontiguousarray(set_offsets, dtype=np.uint32).reshape(-1)
+    outs = np.ascontiguousarray(output_counts, dtype=np.uint32).reshape(-1)
+    areas = np.ascontiguousarray(surface_areas, dtype=np.float32).reshape(-1)
+    keep = np.zeros(p.shape[0], np.uint8)
+    radii = np.zeros(outs.shape[0], np.float32)
+    order = np.full(p.shape[0], 0xFFFFFFFF, np.uint32)
+    rc = lib().oracle_wse_eliminate(_p(p), _p(nrm), _p(off), outs.shape[0], _p(outs), _p(areas),
+                                    float(normal_cosine_threshold), float(plane_distance_scale), _p(keep),
+                                    _p(radii), _p(order), threads)
+    if rc != 0:
+        raise RuntimeError("weighted sample elimination: a candidate has more than 8000 neighbours")
+    return keep, radii, order
 
 
 def own_exp(x: float) -> float:

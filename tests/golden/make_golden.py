@@ -9,8 +9,9 @@ It imports the reference's numpy reference functions -- the RGB9E5 pack/unpack
 of ``test_mesh_colors_rgb9e5.py:15-50``, the hemi-oct encode/decode of
 ``surface_probes.py:45-110``, the Mesh Colors lattice math of
 ``mesh_colors.py:24-79``, the FP64 brute-force any-hit caster of
-``vertex_baker/visibility_baker.py:348-402``, and the point octree builder and
-query of ``surface_probes.py:1348-1438, 3007-3099`` -- with the graphics-only modules
+``vertex_baker/visibility_baker.py:348-402``, the point octree builder and
+query of ``surface_probes.py:1348-1438, 3007-3099``, and the Python weighted
+sample elimination of ``surface_probes.py:897-985`` -- with the graphics-only modules
 (slangpy, trimesh, pygltflib, PIL) replaced by inert stand-ins, evaluates them
 on seeded inputs, and writes ``reference_vectors.npz`` next to this file.
 The GPU box never runs this script; tests read the committed ``.npz`` only.
@@ -194,6 +195,36 @@ def main() -> None:
     out["octree_query_normals"] = np.asarray(qnormals, np.float64)
     out["octree_query_found"] = np.concatenate(found)
     out["octree_query_offsets"] = np.asarray(offsets, np.int64)
+
+    # Weighted sample elimination (the reference's Python backend): random
+    # candidates on a plane, on two facing sheets plus a wall, and the
+    # regular grid of test_surface_probes.py:194-230.
+    wrng = np.random.default_rng(4242)
+    wse_cases = []
+    p = np.zeros((2000, 3), np.float32)
+    p[:, 0], p[:, 2] = wrng.uniform(0.0, 1.0, 2000), wrng.uniform(0.0, 1.0, 2000)
+    n = np.tile(np.float32([0.0, 1.0, 0.0]), (2000, 1))
+    wse_cases.append((p, n, 400, 1.0))
+    m = 3000
+    p = np.zeros((m, 3), np.float32)
+    n = np.zeros((m, 3), np.float32)
+    u = wrng.uniform(0.0, 1.0, (m, 2)).astype(np.float32)
+    p[:1000, 0], p[:1000, 2], n[:1000, 1] = u[:1000, 0], u[:1000, 1], 1.0
+    p[1000:2000, 0], p[1000:2000, 2], p[1000:2000, 1], n[1000:2000, 1] = u[1000:2000, 0], u[1000:2000, 1], 0.05, -1.0
+    p[2000:, 1], p[2000:, 2], n[2000:, 0] = u[2000:, 0], u[2000:, 1], 1.0
+    wse_cases.append((p, n, 600, 3.0))
+    c = np.linspace(0.0, 1.0, 20, dtype=np.float32)
+    gx, gz = np.meshgrid(c, c, indexing="xy")
+    p = np.stack((gx.reshape(-1), np.zeros(gx.size, np.float32), gz.reshape(-1)), axis=1).astype(np.float32)
+    n = np.tile(np.float32([0.0, 1.0, 0.0]), (p.shape[0], 1))
+    wse_cases.append((p, n, 64, 1.0))
+    for k, (pos, nrm, count, area) in enumerate(wse_cases):
+        sel, radius = surface_probes._weighted_sample_elimination_python(pos, nrm, count, surface_area=area)
+        out[f"wse{k}_positions"] = pos
+        out[f"wse{k}_normals"] = nrm
+        out[f"wse{k}_params"] = np.asarray([count, area], np.float64)
+        out[f"wse{k}_selected"] = np.asarray(sel, np.int64)
+        out[f"wse{k}_radius"] = np.asarray([radius], np.float64)
 
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})
