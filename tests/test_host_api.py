@@ -58,6 +58,39 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_native.NanBatchTuning) == 16
 
 
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """sizeof and every field offset of the ABI structs, as gcc lays them out
+    from include/nan_b200.h, equal the ctypes mirrors."""
+    import shutil
+    import subprocess
+
+    from nan_b200 import _native
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    structs = ["NanLighting", "NanCamera", "NanCounters", "NanTuning", "NanKernelTimes", "NanCacheConfig",
+               "NanCachedFrame", "NanProbeSet", "NanBatchTuning", "NanProbeLayoutDesc", "NanProbeResolveOptions",
+               "NanWseOptions", "NanSceneDesc", "NanMeshColorsDesc", "NanSceneInfo"]
+    structs = [s for s in structs if hasattr(_native, s)]
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "nan_b200.h"', "int main(void) {"]
+    expect = []
+    for name in structs:
+        cls = getattr(_native, name)
+        lines.append(f'printf("%zu\\n", sizeof({name}));')
+        expect.append(ctypes.sizeof(cls))
+        for field, *_ in cls._fields_:
+            lines.append(f'printf("%zu\\n", offsetof({name}, {field}));')
+            expect.append(getattr(cls, field).offset)
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    include = Path(_native.__file__).resolve().parents[1] / "include"
+    subprocess.run(["gcc", "-std=c11", "-I", str(include), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == expect
+
+
 def test_null_arguments_are_rejected_without_a_device():
     from nan_b200 import _native
 
