@@ -122,7 +122,7 @@ __device__ __forceinline__ long long wse_contribution(const WseArgs& a, const Ws
     return __double2ll_rn((b4 * b4) * kWseUnit);
 }
 
-// Walks the 27 cells around candidate i; kFill = false counts neighbours,
+// Walks the 3x3x3 cells around candidate i; kFill = false counts neighbours,
 // kFill = true writes them and the initial weight.
 template <bool kFill>
 __global__ void k_wse_neighbors(WseArgs a, const unsigned long long* keys, const uint32_t* sorted_idx,
@@ -137,28 +137,31 @@ __global__ void k_wse_neighbors(WseArgs a, const unsigned long long* keys, const
     uint32_t count = 0;
     uint32_t out = kFill ? offsets[i] : 0u;
     long long w = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int r0 = c[0] + dx - s.cmin[0], r1 = c[1] + dy - s.cmin[1], r2 = c[2] + dz - s.cmin[2];
-                if (r0 < 0 || r1 < 0 || r2 < 0) continue;
-                const unsigned long long key = ((unsigned long long)si << 48) | ((unsigned long long)r0 << 32) |
-                                               ((unsigned long long)r1 << 16) | (unsigned long long)r2;
-                for (uint32_t k = lower_bound_key(keys, a.n, key); k < a.n && keys[k] == key; ++k) {
-                    const uint32_t j = sorted_idx[k];
-                    if (j == i) continue;
-                    const long long q = wse_contribution(a, s, i, j);
-                    if (q <= 0) continue;
-                    if (kFill) {
-                        nbr[out] = j;
-                        contrib[out] = q;
-                        ++out;
-                        w += q;
-                    } else {
-                        ++count;
-                    }
+    // keys order cells by (set, x, y, z): the three z-neighbours of one (x, y)
+    // column are one contiguous key range, found by one search
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int r0 = c[0] + dx - s.cmin[0], r1 = c[1] + dy - s.cmin[1], rz = c[2] - s.cmin[2];
+            if (r0 < 0 || r1 < 0) continue;
+            const unsigned long long column = ((unsigned long long)si << 48) | ((unsigned long long)r0 << 32) |
+                                              ((unsigned long long)r1 << 16);
+            const unsigned long long lo = column | (unsigned long long)max(rz - 1, 0);
+            const unsigned long long hi = column | (unsigned long long)(rz + 1);
+            for (uint32_t k = lower_bound_key(keys, a.n, lo); k < a.n && keys[k] <= hi; ++k) {
+                const uint32_t j = sorted_idx[k];
+                if (j == i) continue;
+                const long long q = wse_contribution(a, s, i, j);
+                if (q <= 0) continue;
+                if (kFill) {
+                    nbr[out] = j;
+                    contrib[out] = q;
+                    ++out;
+                    w += q;
+                } else {
+                    ++count;
                 }
             }
+        }
     if (kFill) {
         weight[i] = w;
     } else {
