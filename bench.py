@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
     ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
+    ap.add_argument("--ray-order", type=int, choices=[0, 1], default=0,
+                    help="wavefront extend queue: 0 path order, 1 regrouped by direction octant")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-cache time-to-RMSE measurement")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batched probe measurement")
@@ -300,7 +302,8 @@ def run_nan(args):
     layout = MeshColorsLayout.build(node, texels_per_unit=16.0, min_resolution=4, max_resolution=64)
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3,
                                              max_paths_in_flight=args.paths or None)
-    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
+                    ray_order=args.ray_order)
     total = layout.total_surface_texels
     begin, end = shard_range(total, rank, world)
     slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
@@ -317,7 +320,7 @@ def run_nan(args):
     # stage timing on inside the timed region: an event pair around each
     # wavefront launch, on the launching stream
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
-                    kernel_timing=True)
+                    kernel_timing=True, ray_order=args.ray_order)
     scene.context.read_kernel_times(reset=True)
 
     clocks = ClockSampler(local)
@@ -342,7 +345,8 @@ def run_nan(args):
     launches = scene.context.launch_count - launches0
     counters = scene.context.read_counters(reset=True)
     ktimes = scene.context.read_kernel_times(reset=True)
-    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width)
+    scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
+                    ray_order=args.ray_order)
     device.check()
     rays_local = counters["extend_rays"] + counters["shadow_rays"]
 

@@ -176,7 +176,9 @@ typedef struct NanTuning {
     uint32_t kernel_timing;        /* 1: record CUDA events around each wavefront stage launch on the
                                       launching stream (read with nan_ctx_read_kernel_times); not for
                                       use under stream capture */
-    uint32_t reserved[2];
+    uint32_t ray_order;            /* wavefront extend queue: 0 = path order, 1 = regrouped by ray
+                                      direction octant before each extend launch */
+    uint32_t reserved;
 } NanTuning;
 
 /* Device time of the wavefront stages since the last reset, from CUDA events

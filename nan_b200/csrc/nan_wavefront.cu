@@ -56,11 +56,13 @@ struct WfState {
 
 struct WfQueues {
     uint32_t* ext[2];
-    float4* shd[2];  // 3 float4 per entry: (o, path bits), (d, kind bits), (c, 0)
-    uint32_t* ctl;   // per iteration k: [4k] ext count, [4k+1] ext fetch, [4k+2] shd count, [4k+3] shd fetch
+    uint32_t* ext_sorted;  // the extend queue regrouped by direction octant (NanTuning ray_order 1)
+    float4* shd[2];        // 3 float4 per entry: (o, path bits), (d, kind bits), (c, 0)
+    uint32_t* ctl;         // per iteration k: [4k] ext count, [4k+1] ext fetch, [4k+2] shd count, [4k+3] shd fetch
+    uint32_t* oct;         // per iteration k: [16k..16k+7] paths per octant, [16k+8..16k+15] placement cursors
 };
 
-constexpr size_t kBytesPerPath = 4 + 4 + 4 + 16 * 9 + 8 + 16 + 16 + 32 + 2 * 4 + 2 * 2 * 48;
+constexpr size_t kBytesPerPath = 4 + 4 + 4 + 16 * 9 + 8 + 16 + 16 + 32 + 3 * 4 + 2 * 2 * 48;
 
 // Warp-aggregated append: returns this lane's slot in the queue.
 __device__ __forceinline__ uint32_t queue_slot(uint32_t* count, bool want) {
@@ -90,6 +92,48 @@ __device__ __forceinline__ float4 f4(f3 v, float w) { return make_float4(v.x, v.
 // ---------------------------------------------------------------------------
 // Generic traversal stages.
 // ---------------------------------------------------------------------------
+// Extend-queue regrouping by ray direction octant (x < 0 | y < 0 << 1 |
+// z < 0 << 2): neighbouring lanes of the traversal then follow rays of one
+// octant, in their previous order within it. Two passes over the queue:
+// a histogram, then a placement with warp-aggregated cursors.
+__device__ __forceinline__ uint32_t dir_octant(float4 d) {
+    return (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+}
+
+__global__ void __launch_bounds__(256) k_wf_octant_count(const uint32_t* __restrict__ queue, const uint32_t* ctl,
+                                                         const float4* __restrict__ rd, uint32_t* oct) {
+    const uint32_t count = *(volatile const uint32_t*)(ctl + 0);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t o = dir_octant(rd[queue[idx]]);
+        const unsigned group = __match_any_sync(__activemask(), o);
+        if ((threadIdx.x & 31u) == (uint32_t)(__ffs(group) - 1)) atomicAdd(oct + o, (uint32_t)__popc(group));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_wf_octant_place(const uint32_t* __restrict__ queue, const uint32_t* ctl,
+                                                         const float4* __restrict__ rd, uint32_t* oct,
+                                                         uint32_t* __restrict__ out) {
+    const uint32_t count = *(volatile const uint32_t*)(ctl + 0);
+    uint32_t base[8];
+    uint32_t sum = 0u;
+    for (int o = 0; o < 8; ++o) {
+        base[o] = sum;
+        sum += oct[o];
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = queue[idx];
+        const uint32_t o = dir_octant(rd[p]);
+        const unsigned active = __activemask();
+        const unsigned group = __match_any_sync(active, o);
+        const int leader = __ffs(group) - 1;
+        uint32_t first = 0u;
+        if ((int)lane == leader) first = atomicAdd(oct + 8 + o, (uint32_t)__popc(group));
+        first = __shfl_sync(active, first, leader);
+        out[base[o] + first + (uint32_t)__popc(group & ((1u << lane) - 1u))] = p;
+    }
+}
+
 template <int kWidth>
 __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* __restrict__ queue,
                                                    uint32_t* ctl, const float4* __restrict__ ro,
@@ -902,7 +946,7 @@ int wf_plan(NanContext* ctx, uint64_t iters64, uint32_t* iters, uint64_t* cap) {
         return NAN_ERR_INVALID_ARGUMENT;
     }
     *iters = (uint32_t)iters64;
-    const size_t ctl_bytes = ((size_t)(*iters + 2) * 4 * sizeof(uint32_t) + 255u) / 256u * 256u;
+    const size_t ctl_bytes = ((size_t)(*iters + 2) * 20 * sizeof(uint32_t) + 255u) / 256u * 256u;
     if (ctx->scratch_bytes <= ctl_bytes + 8192) {
         set_error("no wavefront scratch reserved on this context (nan_ctx_reserve)");
         return NAN_ERR_INVALID_ARGUMENT;
@@ -918,7 +962,8 @@ int wf_plan(NanContext* ctx, uint64_t iters64, uint32_t* iters, uint64_t* cap) {
 
 void wf_carve(NanContext* ctx, uint32_t count, uint32_t iters, WfState& S, WfQueues& q) {
     unsigned char* cur = static_cast<unsigned char*>(ctx->scratch);
-    q.ctl = carve<uint32_t>(cur, (size_t)(iters + 2) * 4);
+    q.ctl = carve<uint32_t>(cur, (size_t)(iters + 2) * 20);
+    q.oct = q.ctl + (size_t)(iters + 2) * 4;
     S.unit = carve<uint32_t>(cur, count);
     S.rng = carve<uint32_t>(cur, count);
     S.flags = carve<uint32_t>(cur, count);
@@ -936,6 +981,7 @@ void wf_carve(NanContext* ctx, uint32_t count, uint32_t iters, WfState& S, WfQue
     S.pc = carve<uint4>(cur, 2ull * count);
     q.ext[0] = carve<uint32_t>(cur, count);
     q.ext[1] = carve<uint32_t>(cur, count);
+    q.ext_sorted = carve<uint32_t>(cur, count);
     q.shd[0] = carve<float4>(cur, 3ull * 2 * count);
     q.shd[1] = carve<float4>(cur, 3ull * 2 * count);
 }
@@ -954,7 +1000,7 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
         WfState S;
         WfQueues q;
         wf_carve(ctx, count, iters, S, q);
-        cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 4 * sizeof(uint32_t), st);
+        cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 20 * sizeof(uint32_t), st);
         if (err != cudaSuccess) return cuda_fail(err, "wavefront control reset");
         cudaEvent_t ev = timing_begin(ctx, st);
         gen(S, q, (uint32_t)cb, count);
@@ -963,6 +1009,15 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
         for (uint32_t it = 0; it < iters; ++it) {
             const int buf = (int)(it & 1u);
             uint32_t* ctl = q.ctl + 4u * it;
+            if (ctx->tuning.ray_order == 1u) {
+                ev = timing_begin(ctx, st);
+                uint32_t* oct = q.oct + 16u * it;
+                k_wf_octant_count<<<g.stream_blocks, 256, 0, st>>>(q.ext[buf], ctl, S.rd, oct);
+                k_wf_octant_place<<<g.stream_blocks, 256, 0, st>>>(q.ext[buf], ctl, S.rd, oct, q.ext_sorted);
+                timing_end(ctx, 2, ev, st);
+                std::swap(q.ext[buf], q.ext_sorted);
+                ctx->launches += 2;
+            }
             ev = timing_begin(ctx, st);
             if (s.wnodes)
                 k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,

@@ -155,13 +155,16 @@ class Scene:
         return self._context
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0, bvh_width: int = 2, kernel_timing: bool = False) -> None:
+                  max_paths_in_flight: int = 0, bvh_width: int = 2, kernel_timing: bool = False,
+                  ray_order: int = 0) -> None:
         """Integrator form for passes on this scene: "wavefront" (default) or
         "megakernel" (one thread per pixel/texel/probe), launch shapes, the
         traversed node width (2: binary, the default; 8: compressed wide nodes),
-        and per-stage CUDA-event timing (read with context.read_kernel_times)."""
+        per-stage CUDA-event timing (read with context.read_kernel_times) and
+        the wavefront's ray order (1: extend queue regrouped by direction
+        octant)."""
         self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width,
-                                kernel_timing)
+                                kernel_timing, ray_order)
 
     def area_light_table(self):
         """(f32[L, 16], power): every emissive triangle of the scene in world
