@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
     ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
+    ap.add_argument("--e2e-chunks", type=int, default=2,
+                    help="texel chunks per e2e step (copies of one chunk overlap the tracing of the others)")
     ap.add_argument("--ray-order", type=int, choices=[0, 1], default=0,
                     help="wavefront extend queue: 0 path order, 1 regrouped by direction octant")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -350,20 +352,26 @@ def run_nan(args):
     device.check()
     rays_local = counters["extend_rays"] + counters["shadow_rays"]
 
-    # e2e through the public API with host buffers: pinned H2D of the slot
-    # buffer, the iteration, D2H of the updated slots, every step.
+    # e2e through the public API with host buffers: every step the slot
+    # buffer goes H2D from pinned memory, the iteration runs, and the updated
+    # slots come back D2H (TextureSpacePathTracer.execute_host: per texel
+    # chunk, so the copies of one chunk overlap the tracing of the others and
+    # of the neighbouring steps; the timed region ends after the last copy).
     host_slots = torch.zeros_like(slots, device="cpu").pin_memory()
     host_slots.copy_(slots)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    tracer.execute_host(host_slots, slots, it, texel_range=(begin, end), chunks=args.e2e_chunks, stream=stream)
+    tracer.host_ready(stream)
+    it += 1
     barrier()
     torch.cuda.synchronize()
+    scene.context.read_counters(reset=True)
     e0.record(stream)
     for k in range(args.steps):
-        slots.copy_(host_slots, non_blocking=True)
-        tracer.execute(stream, slots, it, texel_range=(begin, end))
-        host_slots.copy_(slots, non_blocking=True)
+        tracer.execute_host(host_slots, slots, it, texel_range=(begin, end), chunks=args.e2e_chunks, stream=stream)
         it += 1
+    tracer.host_ready(stream)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
