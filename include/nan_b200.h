@@ -164,6 +164,15 @@ typedef struct NanWseOptions {
     float plane_distance_scale;     /* 0.35 in the reference */
 } NanWseOptions;
 
+/* Options of the deficit repair (SurfaceProbeRepairOptions,
+ * surface_probe_sampler.h:50-56). */
+typedef struct NanRepairOptions {
+    uint32_t min_gather_count;     /* 1..32; 4 in the reference */
+    uint32_t max_repair_count;     /* budget of chosen candidates */
+    float normal_cosine_threshold; /* full-confidence cosine of the soft normal gate */
+    float weight_epsilon;          /* 1e-6 in the reference */
+} NanRepairOptions;
+
 /* Execution choices of a context. The defaults (all zero) are the wavefront
  * integrator with occupancy-sized persistent traversal grids, as many paths
  * in flight as the reserved scratch holds, and the PLOC BVH builder. */
@@ -401,6 +410,34 @@ NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, cons
                                    const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
                                    const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
                                    float* poisson_radii, uint32_t* rounds, void* stream);
+
+/* Deficit repair (deficit_repair, surface_probes.py:1201-1253;
+ * surface_probe_deficit_repair, surface_probe_sampler.h:120-223; the Python
+ * form deficit_repair_python, surface_probe_sampler.py:990-1103). Each audit
+ * point gathers the base probes of its own instance within that instance's
+ * kernel radius (weights (1 - d^2/R^2)^2 x exp(-(plane distance / (R/4))^2 / 2)
+ * x the soft normal gate, above weight_epsilon, the 32 largest); its deficit
+ * is min_gather_count - count. Repair candidates are then chosen one at a
+ * time by score sum (2 deficit - 1) over the deficient audits they reach,
+ * highest first (lowest index on ties), each lowering those deficits by one,
+ * until max_repair_count or no positive score. Positions and normals are
+ * device f32[N][3], instances device u32[N]; instance_radii is a host
+ * f32[instance_count]. selected (device u32[max_repair_count]) gets the
+ * chosen candidates in choice order and *repair_count (host) their number;
+ * counts, weight sums and effective sample sizes of every audit before and
+ * after (device, audit_count each). Allocates scratch on the stream and
+ * synchronizes it. */
+NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions, const float* base_normals,
+                                    const uint32_t* base_instances, uint32_t base_count,
+                                    const float* candidate_positions, const float* candidate_normals,
+                                    const uint32_t* candidate_instances, uint32_t candidate_count,
+                                    const float* audit_positions, const float* audit_normals,
+                                    const uint32_t* audit_instances, uint32_t audit_count,
+                                    const float* instance_radii, uint32_t instance_count,
+                                    const NanRepairOptions* options, uint32_t* selected, uint32_t* repair_count,
+                                    uint32_t* counts_before, uint32_t* counts_after, float* weight_sums_before,
+                                    float* weight_sums_after, float* ess_before, float* ess_after,
+                                    uint32_t* rounds, void* stream);
 
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */

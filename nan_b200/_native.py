@@ -224,6 +224,11 @@ class NanWseOptions(ctypes.Structure):
     _fields_ = [("normal_cosine_threshold", ctypes.c_float), ("plane_distance_scale", ctypes.c_float)]
 
 
+class NanRepairOptions(ctypes.Structure):
+    _fields_ = [("min_gather_count", ctypes.c_uint32), ("max_repair_count", ctypes.c_uint32),
+                ("normal_cosine_threshold", ctypes.c_float), ("weight_epsilon", ctypes.c_float)]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -298,6 +303,9 @@ EXPORTS = {
     "nan_resolve_probes": (_I, [_VP, ctypes.POINTER(NanProbeLayoutDesc), _VP, _VP, _VP, _VP,
                                 ctypes.POINTER(NanProbeResolveOptions), _VP, _U32, _U32, ctypes.POINTER(NanCamera),
                                 ctypes.POINTER(NanLighting), _VP]),
+    "nan_deficit_repair": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _U32,
+                                ctypes.POINTER(NanRepairOptions), _VP, ctypes.POINTER(_U32), _VP, _VP, _VP, _VP, _VP,
+                                _VP, ctypes.POINTER(_U32), _VP]),
     "nan_wse_eliminate": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, ctypes.POINTER(NanWseOptions), _VP, _VP,
                                ctypes.POINTER(_U32), _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),

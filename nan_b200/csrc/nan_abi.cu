@@ -467,6 +467,50 @@ NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, cons
                                           surface_areas, options, keep, poisson_radii, rounds, as_stream(stream));
 }
 
+NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions, const float* base_normals,
+                                    const uint32_t* base_instances, uint32_t base_count,
+                                    const float* candidate_positions, const float* candidate_normals,
+                                    const uint32_t* candidate_instances, uint32_t candidate_count,
+                                    const float* audit_positions, const float* audit_normals,
+                                    const uint32_t* audit_instances, uint32_t audit_count,
+                                    const float* instance_radii, uint32_t instance_count,
+                                    const NanRepairOptions* options, uint32_t* selected, uint32_t* repair_count,
+                                    uint32_t* counts_before, uint32_t* counts_after, float* weight_sums_before,
+                                    float* weight_sums_after, float* ess_before, float* ess_after,
+                                    uint32_t* rounds, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!options || !repair_count || !instance_radii) return invalid("null argument");
+    if (base_count == 0 || audit_count == 0 || instance_count == 0)
+        return invalid("base_count, audit_count and instance_count must be positive");
+    if (instance_count > 65535u) return invalid("at most 65535 instances");
+    if (!base_positions || !base_normals || !base_instances || !audit_positions || !audit_normals ||
+        !audit_instances || !counts_before || !counts_after || !weight_sums_before || !weight_sums_after ||
+        !ess_before || !ess_after)
+        return invalid("null buffer");
+    if (candidate_count && (!candidate_positions || !candidate_normals || !candidate_instances))
+        return invalid("non-empty repair candidates need their buffers");
+    if (options->min_gather_count == 0 || options->min_gather_count > 32)
+        return invalid("min_gather_count must be within [1, 32]");
+    if (!std::isfinite(options->normal_cosine_threshold) || options->normal_cosine_threshold < -1.0f ||
+        options->normal_cosine_threshold > 1.0f || !std::isfinite(options->weight_epsilon) ||
+        options->weight_epsilon < 0.0f)
+        return invalid("invalid deficit repair thresholds");
+    if (std::min(options->max_repair_count, candidate_count) > 0 && !selected)
+        return invalid("selected cannot be null when repairs are enabled");
+    for (uint32_t k = 0; k < instance_count; ++k)
+        if (!std::isfinite(instance_radii[k]) || !(instance_radii[k] > 0.0f))
+            return invalid("instance radii must be positive and finite");
+    const float* base[2] = {base_positions, base_normals};
+    const float* cand[2] = {candidate_positions, candidate_normals};
+    const float* audit[2] = {audit_positions, audit_normals};
+    return nan_host::launch_deficit_repair(ctx, base, base_instances, base_count, cand, candidate_instances,
+                                           candidate_count, audit, audit_instances, audit_count, instance_radii,
+                                           instance_count, options, selected, repair_count, counts_before,
+                                           counts_after, weight_sums_before, weight_sums_after, ess_before,
+                                           ess_after, rounds, as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

@@ -163,6 +163,13 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
                          uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
                          const NanWseOptions* opt, uint8_t* keep, float* poisson_radii, uint32_t* rounds_out,
                          cudaStream_t st);
+int launch_deficit_repair(NanContext* ctx, const float* const* base, const uint32_t* base_instances, uint32_t base_count,
+                          const float* const* cand, const uint32_t* cand_instances, uint32_t cand_count,
+                          const float* const* audit, const uint32_t* audit_instances, uint32_t audit_count,
+                          const float* radii, uint32_t instance_count, const NanRepairOptions* opt, uint32_t* selected,
+                          uint32_t* repair_count, uint32_t* counts_before, uint32_t* counts_after,
+                          float* sums_before, float* sums_after, float* ess_before, float* ess_after,
+                          uint32_t* rounds_out, cudaStream_t st);
 int launch_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* lay, const float* values,
                           const uint32_t* counts, const uint32_t* self_hits, const uint32_t* radial,
                           const NanProbeResolveOptions* opt, float* out, uint32_t w, uint32_t h,

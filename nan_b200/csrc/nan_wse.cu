@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "nan_internal.h"
+#include "nan_math.cuh"
 
 namespace {
 
@@ -242,6 +243,319 @@ cudaError_t alloc(T** p, size_t count, cudaStream_t s) {
 
 uint32_t blocks(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 
+// ---------------------------------------------------------------------------
+// Deficit repair (deficit_repair_python, surface_probe_sampler.py:990-1103;
+// C ABI surface_probe_deficit_repair, surface_probe_sampler.h:120-223).
+// An audit point gathers probes of its own instance as the resolve does
+// (_gather_weights_reference, :949-987: weight (1 - d^2/R^2)^2 x plane
+// Gaussian x soft normal gate, kept above epsilon, the 32 largest); its
+// deficit is min_gather - count. Repair candidates are then chosen one at a
+// time by score = sum over the deficient audits a candidate reaches of
+// (2 deficit - 1), highest first (lowest index on ties), each choice
+// lowering the deficits it reaches by one, until the budget is spent or no
+// score is positive. A score only falls when a candidate sharing one of its
+// audits is chosen, so the same parallel rounds as the elimination give the
+// sequential choices: every candidate whose (score, -index) tops those of
+// all candidates sharing an audit with it is chosen at once.
+// ---------------------------------------------------------------------------
+constexpr float kRepairHardCos = 0.17364818f;
+
+struct RepairSet {
+    const float* pos;
+    const float* nrm;
+    const uint32_t* inst;
+    uint32_t n;
+};
+
+struct RepairInst {
+    double inv_cell;
+    float r2;           // float32(R * R)
+    float plane_sigma;  // float32(max(R / 4, 1e-6))
+    int cmin[3];
+};
+
+struct RepairParams {
+    const RepairInst* inst;
+    uint32_t inst_count;
+    float ncos_span;  // float32(max(threshold, hard + 1e-3) - hard)
+    float eps;
+    uint32_t min_gather;
+};
+
+__device__ __forceinline__ float rep_weight(const RepairParams& rp, const RepairInst& ri, const float* q,
+                                            const float* qn, const float* p, const float* pn) {
+    const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+    const float d2 = (dx * dx + dy * dy) + dz * dz;
+    const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
+    if (!(d2 <= ri.r2) || !(nc >= kRepairHardCos)) return 0.0f;
+    const float pd = fabsf((dx * qn[0] + dy * qn[1]) + dz * qn[2]);
+    const float t = pd / ri.plane_sigma;
+    const float pw = nbd::nan_exp(-0.5f * (t * t));
+    const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
+    const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
+    const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
+    const float w = ((sp * sp) * pw) * soft;
+    return w > rp.eps ? w : 0.0f;
+}
+
+// numpy's float64 pairwise sum of float32 values (n <= 128: eight running
+// partial sums, combined pairwise, then the remainder in order).
+__device__ __forceinline__ double pairwise_sum(const float* v, uint32_t n, bool square) {
+    auto at = [&](uint32_t i) { return square ? (double)(v[i] * v[i]) : (double)v[i]; };
+    if (n < 8u) {
+        double r = 0.0;
+        for (uint32_t i = 0; i < n; ++i) r += at(i);
+        return r;
+    }
+    double r[8];
+    for (int j = 0; j < 8; ++j) r[j] = at(j);
+    uint32_t i = 8;
+    for (; i < n - (n % 8u); i += 8)
+        for (int j = 0; j < 8; ++j) r[j] += at(i + j);
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += at(i);
+    return res;
+}
+
+__global__ void k_rep_cmin(RepairSet set, RepairInst* inst, uint32_t inst_count, int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= set.n) return;
+    const uint32_t k = set.inst[i];
+    if (k >= inst_count) {
+        atomicOr(status, 8);
+        return;
+    }
+    const double inv = inst[k].inv_cell;
+    const unsigned group = __match_any_sync(__activemask(), k);
+    const bool leader = (threadIdx.x & 31u) == (uint32_t)(__ffs(group) - 1);
+    for (int a = 0; a < 3; ++a) {
+        const double f = floor((double)set.pos[3 * i + a] * inv);
+        int v = 0x7fffffff;
+        if (f > -1.0e9 && f < 1.0e9) v = (int)f;
+        else atomicOr(status, 1);
+        const int m = __reduce_min_sync(group, v);
+        if (leader) atomicMin(&inst[k].cmin[a], m);
+    }
+}
+
+__device__ __forceinline__ bool rep_cell(const RepairInst& ri, const float* p, int r[3]) {
+    for (int a = 0; a < 3; ++a) {
+        r[a] = (int)floor((double)p[a] * ri.inv_cell) - ri.cmin[a];
+        if (r[a] < 0 || r[a] >= kCellLimit - 1) return false;
+    }
+    return true;
+}
+
+__global__ void k_rep_keys(RepairSet set, const RepairInst* inst, uint32_t inst_count, unsigned long long* keys,
+                           uint32_t* idx, int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= set.n) return;
+    const uint32_t k = set.inst[i];
+    if (k >= inst_count) {
+        atomicOr(status, 8);
+        keys[i] = ~0ull;
+        idx[i] = i;
+        return;
+    }
+    int r[3];
+    if (!rep_cell(inst[k], set.pos + 3 * i, r)) {
+        atomicOr(status, 2);
+        keys[i] = ~0ull;
+        idx[i] = i;
+        return;
+    }
+    keys[i] = ((unsigned long long)k << 48) | ((unsigned long long)r[0] << 32) | ((unsigned long long)r[1] << 16) |
+              (unsigned long long)r[2];
+    idx[i] = i;
+}
+
+struct RepairGrid {
+    const unsigned long long* keys;  // sorted
+    const uint32_t* idx;
+    uint32_t n;
+};
+
+// Calls f(j) for every point of `g` in the 3x3x3 cells around the cell `c`
+// of instance k.
+template <class F>
+__device__ __forceinline__ void rep_neighbourhood(const RepairGrid& g, uint32_t k, const int c[3], F f) {
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int r0 = c[0] + dx, r1 = c[1] + dy;
+            if (r0 < 0 || r1 < 0) continue;
+            const unsigned long long column = ((unsigned long long)k << 48) | ((unsigned long long)r0 << 32) |
+                                              ((unsigned long long)r1 << 16);
+            const unsigned long long lo = column | (unsigned long long)max(c[2] - 1, 0);
+            const unsigned long long hi = column | (unsigned long long)(c[2] + 1);
+            for (uint32_t q = lower_bound_key(g.keys, g.n, lo); q < g.n && g.keys[q] <= hi; ++q) f(g.idx[q]);
+        }
+}
+
+// Per audit: the 32 largest weights over the base probes and, when given,
+// the chosen repair candidates; count, float64 pairwise sum and ESS.
+__global__ void k_rep_gather(RepairParams rp, RepairSet audits, RepairSet base, RepairGrid base_grid,
+                             RepairSet extra, RepairGrid extra_grid, const uint8_t* extra_on, uint32_t* counts,
+                             float* sums, float* ess) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= audits.n) return;
+    const uint32_t k = audits.inst[a];
+    const RepairInst ri = rp.inst[k];
+    int c[3];
+    float top[32];
+    uint32_t n = 0;
+    const float* q = audits.pos + 3 * a;
+    const float* qn = audits.nrm + 3 * a;
+    auto offer = [&](float w) {
+        if (w <= 0.0f) return;
+        if (n < 32u) {
+            uint32_t j = n++;
+            while (j > 0 && top[j - 1] < w) {
+                top[j] = top[j - 1];
+                --j;
+            }
+            top[j] = w;
+        } else if (w > top[31]) {
+            uint32_t j = 31;
+            while (j > 0 && top[j - 1] < w) {
+                top[j] = top[j - 1];
+                --j;
+            }
+            top[j] = w;
+        }
+    };
+    if (rep_cell(ri, q, c)) {
+        rep_neighbourhood(base_grid, k, c, [&](uint32_t j) {
+            offer(rep_weight(rp, ri, q, qn, base.pos + 3 * j, base.nrm + 3 * j));
+        });
+        if (extra_on != nullptr)
+            rep_neighbourhood(extra_grid, k, c, [&](uint32_t j) {
+                if (extra_on[j]) offer(rep_weight(rp, ri, q, qn, extra.pos + 3 * j, extra.nrm + 3 * j));
+            });
+    }
+    counts[a] = n;
+    const float s32 = (float)pairwise_sum(top, n, false);
+    const double sq = pairwise_sum(top, n, true);
+    sums[a] = s32;
+    ess[a] = sq > 0.0 ? (float)(((double)s32 * (double)s32) / sq) : 0.0f;
+}
+
+// Candidate -> deficient audits it reaches (weight above epsilon).
+template <bool kFill>
+__global__ void k_rep_cover(RepairParams rp, RepairSet cand, RepairSet audits, RepairGrid audit_grid,
+                            const int* deficit, const uint32_t* offsets, uint32_t* degree, uint32_t* list,
+                            uint32_t* audit_degree) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= cand.n) return;
+    const uint32_t k = cand.inst[i];
+    if (k >= rp.inst_count) {
+        if (!kFill) degree[i] = 0;
+        return;
+    }
+    const RepairInst ri = rp.inst[k];
+    int c[3];
+    uint32_t count = 0, out = kFill ? offsets[i] : 0u;
+    if (rep_cell(ri, cand.pos + 3 * i, c)) {
+        rep_neighbourhood(audit_grid, k, c, [&](uint32_t a) {
+            if (deficit[a] <= 0) return;
+            if (rep_weight(rp, ri, audits.pos + 3 * a, audits.nrm + 3 * a, cand.pos + 3 * i, cand.nrm + 3 * i) <=
+                0.0f)
+                return;
+            if (kFill) {
+                list[out++] = a;
+            } else {
+                ++count;
+                atomicAdd(audit_degree + a, 1u);
+            }
+        });
+    }
+    if (!kFill) degree[i] = count;
+}
+
+__global__ void k_rep_transpose(uint32_t n, const uint32_t* offsets, const uint32_t* list,
+                                const uint32_t* audit_offsets, uint32_t* audit_cursor, uint32_t* audit_list) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
+        const uint32_t a = list[e];
+        audit_list[audit_offsets[a] + atomicAdd(audit_cursor + a, 1u)] = i;
+    }
+}
+
+__global__ void k_rep_score(uint32_t n, const uint32_t* offsets, const uint32_t* list, const int* deficit,
+                            const uint8_t* chosen, long long* score, unsigned int* positive) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long s = 0;
+    if (!chosen[i])
+        for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
+            const int d = deficit[list[e]];
+            if (d > 0) s += 2 * d - 1;
+        }
+    score[i] = s;
+    if (s > 0) atomicAdd(positive, 1u);
+}
+
+__global__ void k_rep_mark(uint32_t n, const uint32_t* offsets, const uint32_t* list, const uint32_t* audit_offsets,
+                           const uint32_t* audit_list, const long long* score, uint8_t* mark) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const long long si = score[i];
+    bool top = si > 0;
+    for (uint32_t e = offsets[i]; top && e < offsets[i + 1]; ++e) {
+        const uint32_t a = list[e];
+        for (uint32_t f = audit_offsets[a]; f < audit_offsets[a + 1]; ++f) {
+            const uint32_t j = audit_list[f];
+            if (j == i) continue;
+            const long long sj = score[j];
+            if (sj > 0 && !(si > sj || (si == sj && i < j))) {
+                top = false;
+                break;
+            }
+        }
+    }
+    mark[i] = top ? 1 : 0;
+}
+
+__global__ void k_rep_choose(uint32_t n, const uint32_t* offsets, const uint32_t* list, const long long* score,
+                             const uint8_t* mark, int* deficit, uint8_t* chosen, long long* key) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !mark[i]) return;
+    chosen[i] = 1;
+    key[i] = score[i];
+    // no two candidates chosen in one round share an audit
+    for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
+        const uint32_t a = list[e];
+        deficit[a] = max(deficit[a] - 1, 0);
+    }
+}
+
+__global__ void k_rep_order_keys(uint32_t n, const uint8_t* chosen, const long long* key, unsigned long long* okey,
+                                 uint32_t* idx) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    okey[i] = chosen[i] ? (unsigned long long)(0x7fffffffffffffffLL - key[i]) : 0xffffffffffffffffull;
+    idx[i] = i;
+}
+
+__global__ void k_rep_take(uint32_t take, const uint32_t* order, uint32_t* selected, uint8_t* on) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= take) return;
+    selected[r] = order[r];
+    on[order[r]] = 1;
+}
+
+__global__ void k_rep_count_chosen(uint32_t n, const uint8_t* chosen, unsigned int* total) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool c = i < n && chosen[i];
+    const unsigned b = __ballot_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31u) == 0u && b) atomicAdd(total, (unsigned int)__popc(b));
+}
+
+__global__ void k_rep_deficit(uint32_t n, const uint32_t* counts, uint32_t min_gather, int* deficit) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < n) deficit[a] = max((int)min_gather - (int)counts[a], 0);
+}
+
 }  // namespace
 
 namespace nan_host {
@@ -402,6 +716,189 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     release();
     if (rounds_out) *rounds_out = rounds;
     return e == cudaSuccess ? NAN_OK : cuda_fail(e, "wse");
+}
+
+int launch_deficit_repair(NanContext* ctx, const float* const* base, const uint32_t* base_instances, uint32_t base_count,
+                          const float* const* cand, const uint32_t* cand_instances, uint32_t cand_count,
+                          const float* const* audit, const uint32_t* audit_instances, uint32_t audit_count,
+                          const float* radii, uint32_t instance_count, const NanRepairOptions* opt, uint32_t* selected,
+                          uint32_t* repair_count, uint32_t* counts_before, uint32_t* counts_after,
+                          float* sums_before, float* sums_after, float* ess_before, float* ess_after,
+                          uint32_t* rounds_out, cudaStream_t st) {
+    std::vector<RepairInst> host_inst(instance_count);
+    for (uint32_t k = 0; k < instance_count; ++k) {
+        const double r = (double)radii[k];
+        host_inst[k].inv_cell = 1.0 / std::max(r, 1e-8);
+        host_inst[k].r2 = radii[k] * radii[k];
+        host_inst[k].plane_sigma = (float)std::max(r * 0.25, 1e-6);
+        host_inst[k].cmin[0] = host_inst[k].cmin[1] = host_inst[k].cmin[2] = 0x7fffffff;
+    }
+    const double hard = 0.17364817766693041;  // cos(80 degrees)
+    const uint32_t limit = std::min(opt->max_repair_count, cand_count);
+    RepairSet B{base[0], base[1], base_instances, base_count};
+    RepairSet C{cand[0], cand[1], cand_instances, cand_count};
+    RepairSet A{audit[0], audit[1], audit_instances, audit_count};
+    std::vector<void*> owned;
+    cudaError_t e = cudaSuccess;
+    auto get = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) owned.push_back(p);
+        return p;
+    };
+    auto release = [&]() {
+        for (void* p : owned) cudaFreeAsync(p, st);
+        owned.clear();
+    };
+    RepairInst* inst = (RepairInst*)get(instance_count * sizeof(RepairInst));
+    int* status = (int*)get(sizeof(int));
+    unsigned long long* keys_in = (unsigned long long*)get(std::max({base_count, cand_count, audit_count}) * 8ull);
+    uint32_t* idx_in = (uint32_t*)get(std::max({base_count, cand_count, audit_count}) * 4ull);
+    unsigned long long* bkeys = (unsigned long long*)get(base_count * 8ull);
+    uint32_t* bidx = (uint32_t*)get(base_count * 4ull);
+    unsigned long long* ckeys = (unsigned long long*)get(cand_count * 8ull);
+    uint32_t* cidx = (uint32_t*)get(cand_count * 4ull);
+    unsigned long long* akeys = (unsigned long long*)get(audit_count * 8ull);
+    uint32_t* aidx = (uint32_t*)get(audit_count * 4ull);
+    int* deficit = (int*)get(audit_count * 4ull);
+    uint32_t* cdeg = (uint32_t*)get((cand_count + 1) * 4ull);
+    uint32_t* coff = (uint32_t*)get((cand_count + 1) * 4ull);
+    uint32_t* adeg = (uint32_t*)get((audit_count + 1) * 4ull);
+    uint32_t* aoff = (uint32_t*)get((audit_count + 1) * 4ull);
+    uint32_t* acur = (uint32_t*)get(audit_count * 4ull);
+    long long* score = (long long*)get(cand_count * 8ull);
+    long long* key = (long long*)get(cand_count * 8ull);
+    uint8_t* mark = (uint8_t*)get(cand_count);
+    uint8_t* chosen = (uint8_t*)get(cand_count);
+    uint8_t* on = (uint8_t*)get(cand_count);
+    unsigned int* positive = (unsigned int*)get(64 * sizeof(unsigned int));
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "deficit repair scratch");
+    }
+    cudaMemcpyAsync(inst, host_inst.data(), instance_count * sizeof(RepairInst), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(status, 0, sizeof(int), st);
+    for (const RepairSet* set : {&B, &C, &A})
+        if (set->n) k_rep_cmin<<<blocks(set->n, 256), 256, 0, st>>>(*set, inst, instance_count, status);
+    // sorted cell keys of each set
+    size_t tmp_bytes = 0;
+    const uint32_t nmax = std::max({base_count, cand_count, audit_count, 1u});
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_in, bkeys, idx_in, bidx, (int)nmax, 0, 64, st);
+    size_t need = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, cdeg, coff, (int)(nmax + 1), st);
+    tmp_bytes = std::max(tmp_bytes, need);
+    void* tmp = get(tmp_bytes);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "deficit repair sort scratch");
+    }
+    const std::pair<const RepairSet*, std::pair<unsigned long long*, uint32_t*>> sets[3] = {
+        {&B, {bkeys, bidx}}, {&C, {ckeys, cidx}}, {&A, {akeys, aidx}}};
+    for (const auto& item : sets) {
+        const RepairSet& set = *item.first;
+        if (!set.n) continue;
+        k_rep_keys<<<blocks(set.n, 256), 256, 0, st>>>(set, inst, instance_count, keys_in, idx_in, status);
+        cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, item.second.first, idx_in, item.second.second,
+                                        (int)set.n, 0, 64, st);
+    }
+    int host_status = 0;
+    cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || host_status) {
+        release();
+        if (e != cudaSuccess) return cuda_fail(e, "deficit repair grids");
+        set_error(host_status & 8 ? "an instance index is out of range"
+                  : host_status & 2 ? "an instance spans more than 65535 kernel radii on an axis"
+                                    : "positions must be finite");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    RepairParams rp{inst, instance_count,
+                    (float)(std::max((double)opt->normal_cosine_threshold, hard + 1e-3) - hard), opt->weight_epsilon,
+                    opt->min_gather_count};
+    const RepairGrid BG{bkeys, bidx, base_count}, CG{ckeys, cidx, cand_count}, AG{akeys, aidx, audit_count};
+    const uint32_t ga = blocks(audit_count, 128), gc = blocks(std::max(cand_count, 1u), 256);
+    k_rep_gather<<<ga, 128, 0, st>>>(rp, A, B, BG, C, CG, nullptr, counts_before, sums_before, ess_before);
+    k_rep_deficit<<<blocks(audit_count, 256), 256, 0, st>>>(audit_count, counts_before, opt->min_gather_count,
+                                                             deficit);
+    uint32_t rounds = 0, take = 0;
+    if (cand_count && limit) {
+        cudaMemsetAsync(adeg, 0, (audit_count + 1) * 4ull, st);
+        cudaMemsetAsync(cdeg + cand_count, 0, 4, st);
+        k_rep_cover<false><<<gc, 256, 0, st>>>(rp, C, A, AG, deficit, nullptr, cdeg, nullptr, adeg);
+        cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, cdeg, coff, (int)(cand_count + 1), st);
+        cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, adeg, aoff, (int)(audit_count + 1), st);
+        uint32_t pairs = 0;
+        cudaMemcpyAsync(&pairs, coff + cand_count, 4, cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+        uint32_t* list = (uint32_t*)get(pairs * 4ull);
+        uint32_t* alist = (uint32_t*)get(pairs * 4ull);
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(e, "deficit repair coverage");
+        }
+        k_rep_cover<true><<<gc, 256, 0, st>>>(rp, C, A, AG, deficit, coff, nullptr, list, nullptr);
+        cudaMemsetAsync(acur, 0, audit_count * 4ull, st);
+        k_rep_transpose<<<gc, 256, 0, st>>>(cand_count, coff, list, aoff, acur, alist);
+        cudaMemsetAsync(chosen, 0, cand_count, st);
+        cudaMemsetAsync(positive, 0, 64 * sizeof(unsigned int), st);
+        // rounds, four at a time, until no candidate has a positive score
+        for (;;) {
+            for (int r = 0; r < 4; ++r) {
+                k_rep_score<<<gc, 256, 0, st>>>(cand_count, coff, list, deficit, chosen, score,
+                                                positive + ((rounds + r) & 63u));
+                k_rep_mark<<<gc, 256, 0, st>>>(cand_count, coff, list, aoff, alist, score, mark);
+                k_rep_choose<<<gc, 256, 0, st>>>(cand_count, coff, list, score, mark, deficit, chosen, key);
+                ctx->launches += 3;
+            }
+            rounds += 4;
+            unsigned int pos = 0;
+            cudaMemcpyAsync(&pos, positive + ((rounds - 1) & 63u), sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+            cudaMemsetAsync(positive + (rounds & 63u), 0, 4 * sizeof(unsigned int), st);
+            e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess || pos == 0u) break;
+            if (rounds > cand_count + 8u) {
+                release();
+                set_error("deficit repair did not finish");
+                return NAN_ERR_LIMIT;
+            }
+        }
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(e, "deficit repair rounds");
+        }
+        // choices in sequential order: score at choice descending, index ascending
+        unsigned long long* okey = keys_in;
+        uint32_t* oidx = (uint32_t*)get(cand_count * 4ull);
+        unsigned long long* okey_sorted = (unsigned long long*)get(cand_count * 8ull);
+        uint32_t* oidx_sorted = (uint32_t*)get(cand_count * 4ull);
+        if (e != cudaSuccess) {
+            release();
+            return cuda_fail(e, "deficit repair order");
+        }
+        k_rep_order_keys<<<gc, 256, 0, st>>>(cand_count, chosen, key, okey, oidx);
+        cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, okey, okey_sorted, oidx, oidx_sorted, (int)cand_count, 0, 64,
+                                        st);
+        // how many were chosen
+        unsigned int chosen_total = 0;
+        {
+            unsigned int* cnt = (unsigned int*)get(sizeof(unsigned int));
+            cudaMemsetAsync(cnt, 0, sizeof(unsigned int), st);
+            k_rep_count_chosen<<<gc, 256, 0, st>>>(cand_count, chosen, cnt);
+            cudaMemcpyAsync(&chosen_total, cnt, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+            e = cudaStreamSynchronize(st);
+        }
+        take = std::min<uint32_t>(chosen_total, limit);
+        cudaMemsetAsync(on, 0, cand_count, st);
+        if (take) k_rep_take<<<blocks(take, 256), 256, 0, st>>>(take, oidx_sorted, selected, on);
+    }
+    k_rep_gather<<<ga, 128, 0, st>>>(rp, A, B, BG, C, CG, take ? on : nullptr, counts_after, sums_after, ess_after);
+    ctx->launches += 12;
+    e = cudaGetLastError();
+    release();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    *repair_count = take;
+    if (rounds_out) *rounds_out = rounds;
+    return e == cudaSuccess ? NAN_OK : cuda_fail(e, "deficit repair");
 }
 
 }  // namespace nan_host

@@ -1,6 +1,13 @@
-"""Weighted sample elimination of surface-probe candidates on the GPU
+"""Surface-probe site selection on the GPU: weighted sample elimination
 (surface_probe_sampler.py / surface_probe_sampler.h:120-130 and
-weighted_sample_elimination, surface_probes.py:1091-1123 of the reference).
+weighted_sample_elimination, surface_probes.py:1091-1123 of the reference)
+and deficit repair (deficit_repair, surface_probes.py:1201-1253;
+deficit_repair_python, surface_probe_sampler.py:990-1103).
+
+SurfaceProbeSampler.deficit_repair adds repair candidates where audit
+points gather fewer than min_gather_count probes: candidates are chosen one
+at a time by their summed deficit score (highest first, lowest index on
+ties), computed as parallel rounds that give the same choices.
 
 SurfaceProbeSampler.eliminate thins many candidate sets in one call (one
 persistent set of launches for all instances of a scene);
@@ -14,17 +21,45 @@ rounds that remove every local maximum at once and give the same survivors.
 from __future__ import annotations
 
 import ctypes
+from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import Context, NanWseOptions, check, lib, ptr, stream_handle
+from ._native import Context, NanRepairOptions, NanWseOptions, check, lib, ptr, stream_handle
 
 WSE_NORMAL_COSINE_THRESHOLD = 0.5
 WSE_PLANE_DISTANCE_SCALE = 0.35
 
 
+def _points(dev, positions, normals, instances, name):
+    import torch
+
+    p = torch.as_tensor(np.asarray(positions, dtype=np.float32).reshape(-1, 3) if not hasattr(positions, "device")
+                        else positions, dtype=torch.float32, device=dev).reshape(-1, 3).contiguous()
+    n = torch.as_tensor(np.asarray(normals, dtype=np.float32).reshape(-1, 3) if not hasattr(normals, "device")
+                        else normals, dtype=torch.float32, device=dev).reshape(-1, 3).contiguous()
+    i = torch.as_tensor(np.asarray(instances, dtype=np.int64).astype(np.uint32).view(np.int32)
+                        if not hasattr(instances, "device") else instances, device=dev).reshape(-1).contiguous()
+    if p.shape[0] != n.shape[0] or p.shape[0] != i.shape[0]:
+        raise ValueError(f"{name} positions, normals and instances must have the same length")
+    return p, n, i
+
+
+@dataclass(frozen=True)
+class DeficitRepairResult:
+    """As the reference's DeficitRepairResult (surface_probe_sampler.py:219-229)."""
+    selected_candidate_indices: np.ndarray
+    counts_before: np.ndarray
+    counts_after: np.ndarray
+    weight_sums_before: np.ndarray
+    weight_sums_after: np.ndarray
+    ess_before: np.ndarray
+    ess_after: np.ndarray
+    rounds: int = 0
+
+
 class SurfaceProbeSampler:
-    """Owns the context the elimination runs in."""
+    """Owns the context the elimination and the repair run in."""
 
     def __init__(self, device):
         self.device = device
@@ -59,6 +94,38 @@ class SurfaceProbeSampler:
         self.last_rounds = int(rounds.value)
         return keep, radii[:sets]
 
+    def deficit_repair(self, base_positions, base_normals, base_instances, candidate_positions, candidate_normals,
+                       candidate_instances, audit_positions, audit_normals, audit_instances, instance_radii, *,
+                       min_gather_count: int = 4, max_repair_count: int, normal_cosine_threshold: float = 0.5,
+                       weight_epsilon: float = 1e-6, stream=None) -> DeficitRepairResult:
+        """The reference's deficit_repair on the GPU (arrays or CUDA tensors;
+        instance_radii per instance). Result arrays are on the host."""
+        import torch
+
+        dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
+        bp, bn, bi = _points(dev, base_positions, base_normals, base_instances, "base")
+        cp, cn, ci = _points(dev, candidate_positions, candidate_normals, candidate_instances, "candidate")
+        ap, an, ai = _points(dev, audit_positions, audit_normals, audit_instances, "audit")
+        radii = np.ascontiguousarray(instance_radii, dtype=np.float32).reshape(-1)
+        na = ap.shape[0]
+        budget = max(0, min(int(max_repair_count), cp.shape[0]))
+        selected = torch.zeros(max(budget, 1), dtype=torch.int32, device=dev)
+        counts = [torch.zeros(na, dtype=torch.int32, device=dev) for _ in range(2)]
+        floats = [torch.zeros(na, dtype=torch.float32, device=dev) for _ in range(4)]
+        opt = NanRepairOptions(max(1, min(32, int(min_gather_count))), budget, float(normal_cosine_threshold),
+                               float(weight_epsilon))
+        count = ctypes.c_uint32(0)
+        rounds = ctypes.c_uint32(0)
+        check(lib().nan_deficit_repair(self.context.handle, ptr(bp), ptr(bn), ptr(bi), bp.shape[0], ptr(cp), ptr(cn),
+                                       ptr(ci), cp.shape[0], ptr(ap), ptr(an), ptr(ai), na, radii.ctypes.data,
+                                       radii.shape[0], ctypes.byref(opt), ptr(selected), ctypes.byref(count),
+                                       ptr(counts[0]), ptr(counts[1]), ptr(floats[0]), ptr(floats[1]), ptr(floats[2]),
+                                       ptr(floats[3]), ctypes.byref(rounds), stream_handle(stream)))
+        host = lambda t: t.cpu().numpy()
+        return DeficitRepairResult(host(selected)[:count.value].astype(np.int64), host(counts[0]).view(np.uint32),
+                                   host(counts[1]).view(np.uint32), host(floats[0]), host(floats[1]), host(floats[2]),
+                                   host(floats[3]), int(rounds.value))
+
 
 def weighted_sample_elimination(positions, normals, output_count: int, *, surface_area: float,
                                 normal_cosine_threshold: float = WSE_NORMAL_COSINE_THRESHOLD,
@@ -75,3 +142,4 @@ def weighted_sample_elimination(positions, normals, output_count: int, *, surfac
                                     [float(surface_area)], normal_cosine_threshold=normal_cosine_threshold,
                                     plane_distance_scale=plane_distance_scale)
     return np.flatnonzero(keep.cpu().numpy()).astype(np.int64), float(radii[0])
+

@@ -2568,9 +2568,126 @@ bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, u
     return true;
 }
 
+// Deficit repair, deficit_repair_python (surface_probe_sampler.py:990-1103)
+// with the gather weights of _gather_weights_reference (:949-987) in float32,
+// exp from spec_exp, and numpy's float64 pairwise sums for the diagnostics.
+float repair_weight(const float* q, const float* qn, const float* p, const float* pn, float r2, float plane_sigma,
+                    float span, float eps) {
+    const float hard = 0.17364818f;
+    const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+    const float d2 = (dx * dx + dy * dy) + dz * dz;
+    const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
+    if (!(d2 <= r2) || !(nc >= hard)) return 0.0f;
+    const float pd = std::fabs((dx * qn[0] + dy * qn[1]) + dz * qn[2]);
+    const float t = pd / plane_sigma;
+    const float pw = spec_exp(-0.5f * (t * t));
+    const float sp = std::fmax(1.0f - d2 / r2, 0.0f);
+    const float g = std::fmin(std::fmax((nc - hard) / span, 0.0f), 1.0f);
+    const float soft = ((g * g) * (3.0f - 2.0f * g)) * std::fmax(nc, 0.0f);
+    const float w = ((sp * sp) * pw) * soft;
+    return w > eps ? w : 0.0f;
+}
+
+double numpy_pairwise_sum(const float* v, uint32_t n, bool square) {
+    auto at = [&](uint32_t i) { return square ? (double)(v[i] * v[i]) : (double)v[i]; };
+    if (n < 8u) {
+        double r = 0.0;
+        for (uint32_t i = 0; i < n; ++i) r += at(i);
+        return r;
+    }
+    double r[8];
+    for (int j = 0; j < 8; ++j) r[j] = at(j);
+    uint32_t i = 8;
+    for (; i < n - (n % 8u); i += 8)
+        for (int j = 0; j < 8; ++j) r[j] += at(i + j);
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += at(i);
+    return res;
+}
+
 }  // namespace
 
 extern "C" {
+
+int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32_t* base_i, uint32_t base_count,
+                          const float* cand_p, const float* cand_n, const uint32_t* cand_i, uint32_t cand_count,
+                          const float* audit_p, const float* audit_n, const uint32_t* audit_i, uint32_t audit_count,
+                          const float* radii, uint32_t instance_count, uint32_t min_gather, uint32_t max_repair,
+                          float normal_cosine_threshold, float eps, uint32_t* selected, uint32_t* repair_count,
+                          uint32_t* counts_before, uint32_t* counts_after, float* sums_before, float* sums_after,
+                          float* ess_before, float* ess_after) {
+    const double hard = 0.17364817766693041;  // cos(80 degrees)
+    const float span = (float)(std::max((double)normal_cosine_threshold, hard + 1e-3) - hard);
+    auto params = [&](uint32_t k, float* r2, float* sigma) {
+        *r2 = radii[k] * radii[k];
+        *sigma = (float)std::max((double)radii[k] * 0.25, 1e-6);
+    };
+    for (uint32_t a = 0; a < audit_count; ++a)
+        if (audit_i[a] >= instance_count) return 8;
+    auto summarize = [&](const std::vector<uint32_t>& extra, uint32_t* counts, float* sums, float* ess) {
+        for (uint32_t a = 0; a < audit_count; ++a) {
+            const uint32_t k = audit_i[a];
+            float r2, sigma;
+            params(k, &r2, &sigma);
+            std::vector<float> w;
+            auto take = [&](const float* p, const float* n, const uint32_t* inst, uint32_t j) {
+                if (inst[j] != k) return;
+                const float v = repair_weight(audit_p + 3 * (size_t)a, audit_n + 3 * (size_t)a, p + 3 * (size_t)j,
+                                              n + 3 * (size_t)j, r2, sigma, span, eps);
+                if (v > 0.0f) w.push_back(v);
+            };
+            for (uint32_t j = 0; j < base_count; ++j) take(base_p, base_n, base_i, j);
+            for (uint32_t j : extra) take(cand_p, cand_n, cand_i, j);
+            std::stable_sort(w.begin(), w.end(), [](float x, float y) { return x > y; });
+            const uint32_t n = (uint32_t)std::min<size_t>(w.size(), 32);
+            counts[a] = n;
+            const float s32 = (float)numpy_pairwise_sum(w.data(), n, false);
+            const double sq = numpy_pairwise_sum(w.data(), n, true);
+            sums[a] = s32;
+            ess[a] = sq > 0.0 ? (float)(((double)s32 * (double)s32) / sq) : 0.0f;
+        }
+    };
+    summarize({}, counts_before, sums_before, ess_before);
+    std::vector<long long> deficit(audit_count);
+    for (uint32_t a = 0; a < audit_count; ++a) deficit[a] = std::max<long long>((long long)min_gather - counts_before[a], 0);
+    std::vector<std::vector<uint32_t>> coverage(cand_count);
+    for (uint32_t c = 0; c < cand_count; ++c) {
+        if (cand_i[c] >= instance_count) continue;
+        for (uint32_t a = 0; a < audit_count; ++a) {
+            if (deficit[a] <= 0 || audit_i[a] != cand_i[c]) continue;
+            float r2, sigma;
+            params(audit_i[a], &r2, &sigma);
+            if (repair_weight(audit_p + 3 * (size_t)a, audit_n + 3 * (size_t)a, cand_p + 3 * (size_t)c,
+                              cand_n + 3 * (size_t)c, r2, sigma, span, eps) > 0.0f)
+                coverage[c].push_back(a);
+        }
+    }
+    const uint32_t limit = std::min(max_repair, cand_count);
+    std::vector<uint8_t> active(cand_count, 1);
+    std::vector<uint32_t> chosen;
+    while (chosen.size() < limit) {
+        long long best_score = 0;
+        int best = -1;
+        for (uint32_t c = 0; c < cand_count; ++c) {
+            if (!active[c]) continue;
+            long long score = 0;
+            for (uint32_t a : coverage[c])
+                if (deficit[a] > 0) score += 2 * deficit[a] - 1;
+            if (score > best_score) {
+                best_score = score;
+                best = (int)c;
+            }
+        }
+        if (best < 0) break;
+        active[best] = 0;
+        chosen.push_back((uint32_t)best);
+        for (uint32_t a : coverage[best]) deficit[a] = std::max<long long>(deficit[a] - 1, 0);
+    }
+    for (size_t r = 0; r < chosen.size(); ++r) selected[r] = chosen[r];
+    *repair_count = (uint32_t)chosen.size();
+    summarize(chosen, counts_after, sums_after, ess_after);
+    return 0;
+}
 
 int oracle_wse_eliminate(const float* positions, const float* normals, const uint32_t* set_offsets,
                          uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,

@@ -183,6 +183,18 @@ int oracle_wse_eliminate(const float* positions, const float* normals, const uin
                          float normal_cosine_threshold, float plane_distance_scale, uint8_t* keep,
                          float* poisson_radii, uint32_t* order, int threads);
 
+/* Deficit repair (deficit_repair_python, surface_probe_sampler.py:990-1103),
+ * one candidate at a time, with the float32 gather weights of the GPU
+ * version. selected gets the chosen candidates in choice order. Returns 8
+ * when an audit names an instance out of range. */
+int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32_t* base_i, uint32_t base_count,
+                          const float* cand_p, const float* cand_n, const uint32_t* cand_i, uint32_t cand_count,
+                          const float* audit_p, const float* audit_n, const uint32_t* audit_i, uint32_t audit_count,
+                          const float* radii, uint32_t instance_count, uint32_t min_gather, uint32_t max_repair,
+                          float normal_cosine_threshold, float eps, uint32_t* selected, uint32_t* repair_count,
+                          uint32_t* counts_before, uint32_t* counts_after, float* sums_before, float* sums_after,
+                          float* ess_before, float* ess_after);
+
 /* e^x and log2 x of the kernels' own float implementations (nan_exp,
  * nan_log2), for tests against the C library. */
 float own_exp(float x);

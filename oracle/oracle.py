@@ -132,6 +132,8 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_resolve_probes.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
                                         vp, vp, i, vp]
     l.oracle_wse_eliminate.argtypes = [vp, vp, vp, u32, vp, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, i]
+    l.oracle_deficit_repair.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, u32, u32,
+                                        ctypes.c_float, ctypes.c_float, vp, vp, vp, vp, vp, vp, vp, vp]
     l.own_exp.argtypes = [ctypes.c_float]
     l.own_exp.restype = ctypes.c_float
     l.own_log2.argtypes = [ctypes.c_float]
@@ -181,6 +183,37 @@ def wse_eliminate(positions, normals, set_offsets, output_counts, surface_areas,
     if rc != 0:
         raise RuntimeError("weighted sample elimination: a candidate has more than 8000 neighbours")
     return keep, radii, order
+
+
+def deficit_repair(base_positions, base_normals, base_instances, candidate_positions, candidate_normals,
+                   candidate_instances, audit_positions, audit_normals, audit_instances, instance_radii, *,
+                   min_gather_count=4, max_repair_count=0, normal_cosine_threshold=0.5, weight_epsilon=1e-6):
+    """One-at-a-time deficit repair; returns a dict with selected (choice
+    order), counts/weight sums/ess before and after."""
+    def arrays(p, n, i):
+        return (np.ascontiguousarray(p, dtype=np.float32).reshape(-1, 3),
+                np.ascontiguousarray(n, dtype=np.float32).reshape(-1, 3),
+                np.ascontiguousarray(i, dtype=np.uint32).reshape(-1))
+    bp, bn, bi = arrays(base_positions, base_normals, base_instances)
+    cp, cn, ci = arrays(candidate_positions, candidate_normals, candidate_instances)
+    ap, an, ai = arrays(audit_positions, audit_normals, audit_instances)
+    radii = np.ascontiguousarray(instance_radii, dtype=np.float32).reshape(-1)
+    na = ap.shape[0]
+    sel = np.zeros(max(1, min(int(max_repair_count), cp.shape[0])), np.uint32)
+    count = ctypes.c_uint32(0)
+    out = {k: np.zeros(na, np.uint32) for k in ("counts_before", "counts_after")}
+    out.update({k: np.zeros(na, np.float32) for k in ("weight_sums_before", "weight_sums_after", "ess_before",
+                                                        "ess_after")})
+    rc = lib().oracle_deficit_repair(_p(bp), _p(bn), _p(bi), bp.shape[0], _p(cp), _p(cn), _p(ci), cp.shape[0],
+                                     _p(ap), _p(an), _p(ai), na, _p(radii), radii.shape[0], int(min_gather_count),
+                                     int(max_repair_count), float(normal_cosine_threshold), float(weight_epsilon),
+                                     _p(sel), ctypes.byref(count), _p(out["counts_before"]), _p(out["counts_after"]),
+                                     _p(out["weight_sums_before"]), _p(out["weight_sums_after"]),
+                                     _p(out["ess_before"]), _p(out["ess_after"]))
+    if rc != 0:
+        raise RuntimeError("deficit repair: an audit names an instance out of range")
+    out["selected"] = sel[:count.value].astype(np.int64)
+    return out
 
 
 def own_exp(x: float) -> float:

@@ -10,8 +10,9 @@ of ``test_mesh_colors_rgb9e5.py:15-50``, the hemi-oct encode/decode of
 ``surface_probes.py:45-110``, the Mesh Colors lattice math of
 ``mesh_colors.py:24-79``, the FP64 brute-force any-hit caster of
 ``vertex_baker/visibility_baker.py:348-402``, the point octree builder and
-query of ``surface_probes.py:1348-1438, 3007-3099``, and the Python weighted
-sample elimination of ``surface_probes.py:897-985`` -- with the graphics-only modules
+query of ``surface_probes.py:1348-1438, 3007-3099``, the Python weighted
+sample elimination of ``surface_probes.py:897-985`` and the Python deficit
+repair of ``surface_probe_sampler.py:990-1103`` -- with the graphics-only modules
 (slangpy, trimesh, pygltflib, PIL) replaced by inert stand-ins, evaluates them
 on seeded inputs, and writes ``reference_vectors.npz`` next to this file.
 The GPU box never runs this script; tests read the committed ``.npz`` only.
@@ -225,6 +226,51 @@ def main() -> None:
         out[f"wse{k}_params"] = np.asarray([count, area], np.float64)
         out[f"wse{k}_selected"] = np.asarray(sel, np.int64)
         out[f"wse{k}_radius"] = np.asarray([radius], np.float64)
+
+    # Deficit repair (the reference's Python form): the cases of
+    # test_surface_probes.py:436-600 and a seeded two-instance case.
+    import surface_probe_sampler
+
+    up = np.float32([0.0, 1.0, 0.0])
+    rep_cases = []
+    bp = np.float32([[0, 0, 0], [1, 0, 0]])
+    cp = np.float32([[0.1, 0, 0], [0.2, 0, 0], [0.9, 0, 0]])
+    rep_cases.append((bp, np.tile(up, (2, 1)), np.zeros(2, np.uint32), cp, np.tile(up, (3, 1)),
+                      np.zeros(3, np.uint32), bp.copy(), np.tile(up, (2, 1)), np.zeros(2, np.uint32),
+                      np.float32([0.5]), 3, 3))
+    bp = np.float32([[9.9, 0, 0], [10.0, 0, 0], [10.1, 0, 0]])
+    cp = np.float32([[0.0, 0, 0], [0.02, 0, 0], [0.04, 0, 0], [0.06, 0, 0], [0.08, 0, 0], [10.2, 0, 0]])
+    rep_cases.append((bp, np.tile(up, (3, 1)), np.zeros(3, np.uint32), cp, np.tile(up, (6, 1)),
+                      np.zeros(6, np.uint32), np.float32([[0, 0, 0], [10, 0, 0]]), np.tile(up, (2, 1)),
+                      np.zeros(2, np.uint32), np.float32([0.5]), 4, 6))
+    rrng = np.random.default_rng(31)
+
+    def sheet(n, inst, normal, offset):
+        p = np.zeros((n, 3), np.float32)
+        u = rrng.uniform(0.0, 2.0, (n, 2)).astype(np.float32)
+        if normal[1] != 0:
+            p[:, 0], p[:, 2], p[:, 1] = u[:, 0], u[:, 1], offset
+        else:
+            p[:, 1], p[:, 2], p[:, 0] = u[:, 0], u[:, 1], offset
+        return p, np.tile(np.float32(normal), (n, 1)), np.full(n, inst, np.uint32)
+
+    b0, b1 = sheet(60, 0, [0, 1, 0], 0.0), sheet(25, 1, [1, 0, 0], 3.0)
+    c0, c1 = sheet(400, 0, [0, 1, 0], 0.0), sheet(300, 1, [1, 0, 0], 3.0)
+    a0, a1 = sheet(500, 0, [0, 1, 0], 0.0), sheet(400, 1, [1, 0, 0], 3.0)
+    cat = lambda x, y: tuple(np.concatenate([x[k], y[k]]) for k in range(3))
+    rep_cases.append((*cat(b0, b1), *cat(c0, c1), *cat(a0, a1), np.float32([0.35, 0.5]), 4, 120))
+    for k, (bp, bn, bi, cp, cn, ci, ap, an, ai, radii, mg, budget) in enumerate(rep_cases):
+        res = surface_probe_sampler.deficit_repair_python(bp, bn, bi, cp, cn, ci, ap, an, ai, radii,
+                                                          min_gather_count=mg, max_repair_count=budget,
+                                                          normal_cosine_threshold=0.5)
+        for name, value in (("bp", bp), ("bn", bn), ("bi", bi), ("cp", cp), ("cn", cn), ("ci", ci), ("ap", ap),
+                            ("an", an), ("ai", ai), ("radii", radii)):
+            out[f"rep{k}_{name}"] = np.asarray(value)
+        out[f"rep{k}_params"] = np.asarray([mg, budget], np.uint32)
+        out[f"rep{k}_selected"] = np.asarray(res.selected_candidate_indices, np.int64)
+        for name in ("counts_before", "counts_after", "weight_sums_before", "weight_sums_after", "ess_before",
+                     "ess_after"):
+            out[f"rep{k}_{name}"] = np.asarray(getattr(res, name))
 
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})

@@ -1,0 +1,39 @@
+"""Deficit repair on the oracle (CPU) against the reference's own Python
+deficit_repair_python run on the same inputs (tests/golden): the cases of
+test_surface_probes.py:436-600 (the budget, the zero-score skip) and a
+seeded two-instance case give the same choices, counts, weight sums and
+effective sample sizes."""
+
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_repair_oracle_matches_reference(golden, case):
+    from oracle.oracle import deficit_repair
+
+    g = lambda name: golden[f"rep{case}_{name}"]
+    mg, budget = (int(x) for x in g("params"))
+    r = deficit_repair(g("bp"), g("bn"), g("bi"), g("cp"), g("cn"), g("ci"), g("ap"), g("an"), g("ai"), g("radii"),
+                       min_gather_count=mg, max_repair_count=budget)
+    np.testing.assert_array_equal(r["selected"], g("selected"))
+    for name in ("counts_before", "counts_after", "weight_sums_before", "weight_sums_after", "ess_before",
+                 "ess_after"):
+        np.testing.assert_array_equal(r[name], g(name))
+    if case == 1:  # the zero-score candidate is skipped, the repair goes on
+        np.testing.assert_array_equal(r["counts_after"], [4, 4])
+        assert r["selected"].shape[0] == 5
+
+
+def test_repair_oracle_no_deficit_and_budget_cap(golden):
+    from oracle.oracle import deficit_repair
+
+    up = np.tile(np.float32([0, 1, 0]), (4, 1))
+    pos = np.float32([[-0.15, 0, 0], [-0.05, 0, 0], [0.05, 0, 0], [0.15, 0, 0]])
+    r = deficit_repair(pos, up, np.zeros(4), np.float32([[0.3, 0, 0]]), up[:1], np.zeros(1),
+                       np.float32([[0, 0, 0]]), up[:1], np.zeros(1), [0.5], min_gather_count=4, max_repair_count=1)
+    assert r["selected"].shape[0] == 0
+    g = lambda name: golden[f"rep0_{name}"]
+    r = deficit_repair(g("bp"), g("bn"), g("bi"), g("cp"), g("cn"), g("ci"), g("ap"), g("an"), g("ai"), g("radii"),
+                       min_gather_count=4, max_repair_count=1)
+    assert r["selected"].shape[0] == 1 and np.any(r["counts_after"] < 4)
