@@ -10,16 +10,18 @@ triangle-map offset bits). The triangle -> vertex-anchor map has two
 records (front, back) per triangle; without anchors every record is
 invalid (w = 0).
 
-Sites: build_wse places them as the reference's layout build does before
-its repair stages (surface_probes.py:1536-2030): the site budget is split
+Sites: build_wse places them as the reference's layout build does
+(surface_probes.py:1536-2420): the site budget is split
 over instances by area (_allocate_counts, surface_probes.py:265-293), each
 instance draws oversample x its count area-weighted candidates
 (_sample_instance_surface, :445-497) and weighted sample elimination on the
 GPU (all instances in one call, SurfaceProbeSampler) keeps its count.
 from_sites takes any sites (e.g. scenes.surface_sites). The kernel radius
 follows the reference's rule max(2.5 * sqrt(area / sites), 2.5 * Poisson
-radius, 2.5 * sqrt(total area / total sites), 1e-5). Deficit repair, the
-protected closure and support estimation are not applied (support 1).
+radius, 2.5 * sqrt(total area / total sites), 1e-5), fixed before the
+deficit repair adds up to 30 % more sites where audit points gather fewer
+than 4 (surface_probes.py:2380-2420). The protected closure and support
+estimation are not applied (support 1).
 """
 
 from __future__ import annotations
@@ -58,6 +60,62 @@ def allocate_counts(weights, total: int, *, minimum_per_entry: int = 1) -> np.nd
     return out
 
 
+def _surface_points(t, areas, k, rng):
+    """k area-weighted points on triangles t (_sample_instance_surface,
+    surface_probes.py:445-497): (positions, face normals, triangle, b1, b2)."""
+    cdf = np.cumsum(areas, dtype=np.float64)
+    cdf /= cdf[-1]
+    cdf[-1] = 1.0
+    choice = np.minimum(np.searchsorted(cdf, rng.random(k), side="right"), t.shape[0] - 1)
+    uv = rng.random((k, 2), dtype=np.float32)
+    su = np.sqrt(uv[:, 0])
+    b1 = (su * (1.0 - uv[:, 1])).astype(np.float32)
+    b2 = (su * uv[:, 1]).astype(np.float32)
+    ea = t[choice, 1] - t[choice, 0]
+    eb = t[choice, 2] - t[choice, 0]
+    pos = (t[choice, 0] + ea * b1[:, None] + eb * b2[:, None]).astype(np.float32)
+    return pos, _face_normals(t)[choice], choice.astype(np.uint32), b1, b2
+
+
+def _face_normals(t):
+    cr = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]).astype(np.float64)
+    return (cr / np.maximum(np.linalg.norm(cr, axis=1, keepdims=True), 1e-30)).astype(np.float32)
+
+
+def _limit(n, k, rng):
+    return np.arange(n) if n <= k else np.sort(rng.choice(n, size=k, replace=False))
+
+
+def _centroids(t, k, rng):
+    """Triangle centroids (_triangle_centroid_candidates, :593-611), at most k."""
+    idx = _limit(t.shape[0], k, rng)
+    third = np.full(idx.shape[0], 1.0 / 3.0, np.float32)
+    return (t[idx].mean(axis=1, dtype=np.float32), _face_normals(t)[idx], idx.astype(np.uint32), third, third)
+
+
+def _inset_corners(t, inset_distance, k, rng):
+    """Corners pulled inside their face (_triangle_inset_corner_candidates,
+    :614-655), at most k."""
+    edges = np.stack([np.linalg.norm(t[:, 1] - t[:, 0], axis=1), np.linalg.norm(t[:, 2] - t[:, 1], axis=1),
+                      np.linalg.norm(t[:, 0] - t[:, 2], axis=1)], axis=1)
+    inset = np.clip(float(inset_distance) / np.maximum(edges.max(axis=1), 1e-8), 1e-4, 0.1).astype(np.float32)
+    bary = np.repeat(inset[:, None], 9, axis=1).reshape(-1, 3)
+    for corner in range(3):
+        bary[corner::3, corner] = 1.0 - 2.0 * inset
+    tri = np.repeat(np.arange(t.shape[0]), 3)
+    pos = np.einsum("ni,nij->nj", bary, t[tri]).astype(np.float32)
+    idx = _limit(pos.shape[0], k, rng)
+    return pos[idx], _face_normals(t)[tri[idx]], tri[idx].astype(np.uint32), bary[idx, 1], bary[idx, 2]
+
+
+def _take(points, idx):
+    return tuple(x[idx] for x in points)
+
+
+def _concat(sets):
+    return tuple(np.concatenate([s[j] for s in sets]) for j in range(5))
+
+
 @dataclass(frozen=True)
 class SurfaceProbeSiteInstance:
     root_center: tuple[float, float, float]
@@ -87,7 +145,8 @@ class SurfaceProbeSiteLayout:
     @classmethod
     def from_sites(cls, scene_node, probes, *, leaf_capacity: int = 8, max_depth: int = 16,
                    kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
-                   max_density_multiplier: float = 8.0, poisson_radii=None) -> "SurfaceProbeSiteLayout":
+                   max_density_multiplier: float = 8.0, poisson_radii=None,
+                   kernel_radii=None) -> "SurfaceProbeSiteLayout":
         probes = np.asarray(probes, dtype=SURFACE_PROBE_DTYPE)
         instance_of = probes["meta"][:, 3] >> SURFACE_PROBE_INSTANCE_SHIFT
         n_inst = len(scene_node.instances)
@@ -115,8 +174,12 @@ class SurfaceProbeSiteLayout:
         for i in range(n_inst):
             rec = probes[by_instance[bounds[i]:bounds[i + 1]]].copy()
             sites = int(fronts[i])
-            kernel = max(global_kernel, math.sqrt(areas[i] / sites) * kernel_radius_scale if sites else 0.0,
-                         float(poisson_radii[i]) * kernel_radius_scale if poisson_radii is not None else 0.0, 1e-5)
+            if kernel_radii is not None:
+                kernel = float(kernel_radii[i])
+            else:
+                kernel = max(global_kernel, math.sqrt(areas[i] / sites) * kernel_radius_scale if sites else 0.0,
+                             float(poisson_radii[i]) * kernel_radius_scale if poisson_radii is not None else 0.0,
+                             1e-5)
             maps = np.full((int(tri_counts[i]) * 2, 4), 0xFFFFFFFF, np.uint32)
             maps[:, 3] = 0
             if rec.shape[0]:
@@ -153,9 +216,15 @@ class SurfaceProbeSiteLayout:
 
     @classmethod
     def build_wse(cls, scene_node, target_probe_count: int, *, device=None, oversample_factor: int = 5,
-                  seed: int = 1, minimum_per_instance: int = 4, sampler=None, profile: dict | None = None,
-                  **kwargs) -> "SurfaceProbeSiteLayout":
-        """Sites by weighted sample elimination of oversampled candidates."""
+                  seed: int = 1, minimum_per_instance: int = 4, repair_budget_ratio: float = 0.30,
+                  repair_min_gather: int = 4, kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
+                  sampler=None, profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
+        """Sites by weighted sample elimination of oversampled candidates, then
+        deficit repair: audit points (a second surface sample, triangle
+        centroids and inset corners per instance) that gather fewer than
+        repair_min_gather sites get repair sites from the eliminated candidates
+        and the audit points, up to repair_budget_ratio x the target
+        (0 turns the repair off)."""
         import time
 
         from .surface_probe_sampler import SurfaceProbeSampler
@@ -172,56 +241,76 @@ class SurfaceProbeSiteLayout:
             areas.append(0.5 * np.linalg.norm(e, axis=1))
             double_sided.append(bool(scene_node.materials[mat_id].double_sided))
         totals = np.array([a.sum() for a in areas])
-        counts = allocate_counts(totals, int(target_probe_count),
-                                 minimum_per_entry=min(minimum_per_instance,
-                                                       max(1, int(target_probe_count) // max(len(totals), 1))))
-        cand_pos, cand_nrm, cand_tri, cand_bary, offsets = [], [], [], [], [0]
-        for i, (t, a) in enumerate(zip(tris, areas)):
-            k = int(counts[i]) * max(1, int(oversample_factor))
-            rng = np.random.default_rng([int(seed), i])
-            cdf = np.cumsum(a, dtype=np.float64)
-            cdf /= cdf[-1]
-            cdf[-1] = 1.0
-            choice = np.minimum(np.searchsorted(cdf, rng.random(k), side="right"), t.shape[0] - 1)
-            uv = rng.random((k, 2), dtype=np.float32)
-            su = np.sqrt(uv[:, 0])
-            b1 = su * (1.0 - uv[:, 1])
-            b2 = su * uv[:, 1]
-            ea = t[choice, 1] - t[choice, 0]
-            eb = t[choice, 2] - t[choice, 0]
-            cand_pos.append((t[choice, 0] + ea * b1[:, None] + eb * b2[:, None]).astype(np.float32))
-            cr = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]).astype(np.float64)
-            fn = cr / np.maximum(np.linalg.norm(cr, axis=1, keepdims=True), 1e-30)
-            cand_nrm.append(fn[choice].astype(np.float32))
-            cand_tri.append(choice.astype(np.uint32))
-            cand_bary.append(np.stack((b1, b2), axis=1).astype(np.float32))
-            offsets.append(offsets[-1] + k)
+        target = int(target_probe_count)
+        counts = allocate_counts(totals, target, minimum_per_entry=min(minimum_per_instance,
+                                                                      max(1, target // max(len(totals), 1))))
+        cands = [_surface_points(t, a, int(counts[i]) * max(1, int(oversample_factor)),
+                                 np.random.default_rng([int(seed), i])) for i, (t, a) in enumerate(zip(tris, areas))]
+        offsets = np.concatenate([[0], np.cumsum([c[0].shape[0] for c in cands])]).astype(np.int64)
         t1 = time.perf_counter()
         if sampler is None:
             from .scene import Device
 
             sampler = SurfaceProbeSampler(device if device is not None else Device(0))
-        keep, radii = sampler.eliminate(np.concatenate(cand_pos), np.concatenate(cand_nrm), offsets, counts, totals)
+        keep, radii = sampler.eliminate(np.concatenate([c[0] for c in cands]), np.concatenate([c[1] for c in cands]),
+                                        offsets, counts, totals)
         keep = keep.cpu().numpy().astype(bool)
         t2 = time.perf_counter()
+        sites = [_take(c, np.flatnonzero(keep[offsets[i]:offsets[i + 1]])) for i, c in enumerate(cands)]
+        repaired = 0
+        budget = int(math.floor(target * float(repair_budget_ratio)))
+        # kernel radius per instance, fixed before the repair as the reference does
+        global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale, 1e-5)
+        kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
+                                float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
+        if budget > 0:
+            audits, repairs = [], []
+            for i, (t, a) in enumerate(zip(tris, areas)):
+                rng = np.random.default_rng([int(seed), i, 7919])
+                k = int(counts[i])
+                audit = _concat([_surface_points(t, a, k, rng), _centroids(t, max(16, k), rng),
+                                 _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng)])
+                audits.append(audit)
+                rest = _take(cands[i], np.flatnonzero(~keep[offsets[i]:offsets[i + 1]]))
+                repairs.append(_concat([rest, audit]))
+            flat = lambda sets, j: np.concatenate([x[j] for x in sets])
+            inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
+            result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
+                                            flat(repairs, 1), inst_of(repairs), flat(audits, 0), flat(audits, 1),
+                                            inst_of(audits), kernels, min_gather_count=repair_min_gather,
+                                            max_repair_count=budget,
+                                            normal_cosine_threshold=math.cos(math.radians(normal_angle_degrees)))
+            chosen = np.sort(result.selected_candidate_indices)
+            repair_inst = inst_of(repairs)[chosen]
+            repair_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in repairs])])
+            for i in np.unique(repair_inst):
+                local = chosen[repair_inst == i] - repair_starts[i]
+                sites[i] = _concat([sites[i], _take(repairs[i], local)])
+            repaired = int(chosen.shape[0])
+            if profile is not None:
+                profile.update(repair_sites=repaired, audits=int(result.counts_before.shape[0]),
+                               audits_below_min_before=int((result.counts_before < repair_min_gather).sum()),
+                               audits_below_min_after=int((result.counts_after < repair_min_gather).sum()),
+                               repair_rounds=int(result.rounds))
+        t3 = time.perf_counter()
         records = []
-        for i in range(len(tris)):
-            sel = np.flatnonzero(keep[offsets[i]:offsets[i + 1]])
-            pos = cand_pos[i][sel]
+        for i, (pos, nrm, tri, b1, b2) in enumerate(sites):
             for side in range(2 if double_sided[i] else 1):
-                r = np.zeros(sel.shape[0], dtype=SURFACE_PROBE_DTYPE)
+                r = np.zeros(pos.shape[0], dtype=SURFACE_PROBE_DTYPE)
                 r["position_radius"][:, :3] = pos
-                r["normal_side"][:, :3] = cand_nrm[i][sel] * (-1.0 if side else 1.0)
+                r["normal_side"][:, :3] = nrm * (-1.0 if side else 1.0)
                 r["normal_side"][:, 3] = 1.0
-                r["meta"][:, 0] = cand_tri[i][sel]
-                r["meta"][:, 1] = cand_bary[i][sel, 0].view(np.uint32)
-                r["meta"][:, 2] = cand_bary[i][sel, 1].view(np.uint32)
+                r["meta"][:, 0] = tri
+                r["meta"][:, 1] = b1.view(np.uint32)
+                r["meta"][:, 2] = b2.view(np.uint32)
                 r["meta"][:, 3] = (1 if side else 0) | (i << SURFACE_PROBE_INSTANCE_SHIFT)
                 records.append(r)
-        layout = cls.from_sites(scene_node, np.concatenate(records), poisson_radii=radii, **kwargs)
+        layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
+                                normal_angle_degrees=normal_angle_degrees, **kwargs)
         if profile is not None:
-            profile.update(candidates_s=t1 - t0, elimination_s=t2 - t1, packing_s=time.perf_counter() - t2,
-                           candidates=int(offsets[-1]), rounds=int(sampler.last_rounds))
+            profile.update(candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2,
+                           packing_s=time.perf_counter() - t3, candidates=int(offsets[-1]),
+                           rounds=int(sampler.last_rounds), base_sites=int(sum(counts)), repair_sites=repaired)
         return layout
 
     @classmethod

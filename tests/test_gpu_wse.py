@@ -81,7 +81,7 @@ def test_wse_layout_spaces_sites_wider_than_random(device):
 
     node = scenes.terrain_boxes(seed=1, grid=129, boxes=0)
     prof = {}
-    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof)
+    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof, repair_budget_ratio=0.0)
     rnd = SurfaceProbeSiteLayout.build(node, 4000, seed=3)
     print("wse layout", prof)
 
@@ -99,3 +99,24 @@ def test_wse_layout_spaces_sites_wider_than_random(device):
     info = wse.instance_infos[0]
     found = wse.query_probe_indices(0, info.root_center, radius=info.root_extent * 4.0)
     np.testing.assert_array_equal(np.sort(found), np.arange(info.probe_offset, info.probe_offset + info.probe_count))
+
+
+def test_wse_layout_repair_fills_gather_deficits(device):
+    """With boxes on the terrain, the repair adds sites where audit points
+    gather fewer than 4 (box faces, seams) and every audit deficit it can
+    reach is closed."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+
+    node = scenes.terrain_boxes(seed=2, grid=97, boxes=40)
+    prof = {}
+    layout = SurfaceProbeSiteLayout.build_wse(node, 3000, device=device, seed=5, profile=prof)
+    print("repair", prof)
+    assert 0 < prof["repair_sites"] <= 900
+    assert prof["audits_below_min_after"] < prof["audits_below_min_before"]
+    fronts = int(((layout.probes["meta"][:, 3] & 1) == 0).sum())
+    assert fronts == prof["base_sites"] + prof["repair_sites"]
+    for k, info in enumerate(layout.instance_infos):
+        if info.probe_count:
+            found = layout.query_probe_indices(k, info.root_center, radius=info.root_extent * 4.0)
+            assert found.shape[0] == info.probe_count
