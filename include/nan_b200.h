@@ -487,9 +487,13 @@ NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tun
  * (surface_probe_path_tracer.slang:206-278) -- bit-exact with
  * nan_trace_probes. INDEPENDENT: sample k draws from RNG(probe, instance,
  * iteration * samples + k), so a warp traces 32 samples of one probe at once;
- * the per-probe sums are still formed in sample order. Resets the launch
- * shape to the new kernel's defaults. */
-enum { NAN_BATCH_SEQUENTIAL_SAMPLES = 0, NAN_BATCH_INDEPENDENT_SAMPLES = 1 };
+ * the per-probe sums are still formed in sample order. WAVEFRONT: the
+ * sequential sample streams, run as one multi-scene wavefront (every probe of
+ * every set one path in flight; extend / shade / shadow / finalize rounds
+ * over all sets; bit-exact with SEQUENTIAL); allocates one path of scratch
+ * per probe on the batch's context; the tuning's blocks_per_sm is the
+ * traversal grid. Resets the launch shape to the new kernel's defaults. */
+enum { NAN_BATCH_SEQUENTIAL_SAMPLES = 0, NAN_BATCH_INDEPENDENT_SAMPLES = 1, NAN_BATCH_WAVEFRONT = 2 };
 NAN_B200_API int nan_batch_set_mode(NanBatch* batch, uint32_t mode);
 /* One iteration of every set (nan_trace_probes semantics per set). */
 NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,

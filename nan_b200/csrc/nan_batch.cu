@@ -7,7 +7,9 @@
 // 32 * grab (scene, probe) units per atomic from one counter, so scenes of
 // very different size share the GPU without a launch per scene, and each
 // unit runs the per-probe baker of nan_probe.cuh with the binary BVH at a
-// fixed stack depth. A frame is [reset counter, bake]; frames can be
+// fixed stack depth, or (NAN_BATCH_WAVEFRONT) every (scene, probe) unit
+// becomes one path of a multi-scene wavefront (nan_wavefront.cu) with the
+// same per-probe sample sequence. A frame is [reset counter, bake]; frames can be
 // captured once into a CUDA graph whose last node advances the iteration
 // on the device, and replayed. The autotuner times the launch shapes
 // (stack depth, warps per SM, units per grab) on the batch itself.
@@ -24,22 +26,6 @@ using namespace nbd;
 using nan_host::cuda_fail;
 using nan_host::set_error;
 
-struct BatchSet {
-    SceneView s;
-    LightingRaw light;
-    ProbeOut out;
-    const float4* probes;
-    const float4* pinst;
-    uint32_t probe_count;
-    uint32_t probe_instance_count;
-};
-
-struct BatchCtl {
-    uint32_t next;
-    uint32_t iteration;
-    uint32_t reset;
-    uint32_t pad;
-};
 
 // kMinBlocks: the launch-bounds occupancy target that caps registers
 // (0: the compiler's choice), one of the autotuned dimensions.
@@ -215,6 +201,8 @@ struct BatchImpl {
     BatchSet* sets = nullptr;
     uint32_t* prefix = nullptr;
     BatchCtl* ctl = nullptr;
+    uint32_t* set_of = nullptr;  // wavefront mode: probe set of each path
+    float t_max = 0.0f;          // largest ray t_max of the sets
     uint32_t set_count = 0;
     uint32_t total = 0;
     uint32_t min_depth = 32;  // smallest stack depth that covers every scene's BVH
@@ -227,6 +215,12 @@ namespace {
 
 int launch_frame_kernel(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t st) {
     BatchImpl* m = b->impl;
+    if (b->mode == NAN_BATCH_WAVEFRONT) {
+        NanTuning& tt = b->ctx->tuning;
+        tt.trace_blocks_per_sm = b->tuning.blocks_per_sm;
+        return nan_host::launch_batch_wavefront(b->ctx, m->sets, m->prefix, m->ctl, m->set_count, m->total, m->set_of,
+                                                spp, max_bounces, m->t_max, st);
+    }
     const NanBatchTuning& t = b->tuning;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ctx->device);
@@ -257,6 +251,7 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
     std::vector<BatchSet> sets(count);
     std::vector<uint32_t> prefix(count + 1u, 0u);
     uint32_t max_depth = 0;
+    float t_max = 0.0f;
     for (uint32_t i = 0; i < count; ++i) {
         const NanProbeSet& p = in[i];
         BatchSet& b = sets[i];
@@ -274,6 +269,7 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
         }
         prefix[i + 1] = (uint32_t)next;
         max_depth = std::max(max_depth, p.scene->max_depth);
+        t_max = std::max(t_max, p.lighting.ray_t_max);
     }
     NanBatch* b = new NanBatch();
     b->ctx = ctx;
@@ -281,6 +277,7 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
     BatchImpl* m = b->impl;
     m->set_count = count;
     m->total = prefix[count];
+    m->t_max = t_max;
     m->min_depth = max_depth + 2u <= 48u ? 48u : 96u;
     if (max_depth + 2u > 96u) {
         delete m;
@@ -319,6 +316,7 @@ void batch_destroy(NanBatch* b) {
         cudaFree(m->sets);
         cudaFree(m->prefix);
         cudaFree(m->ctl);
+        cudaFree(m->set_of);
         delete m;
     }
     delete b;
@@ -327,9 +325,33 @@ void batch_destroy(NanBatch* b) {
 uint32_t batch_min_depth(const NanBatch* b) { return b->impl->min_depth; }
 
 int batch_set_mode(NanBatch* b, uint32_t mode) {
-    if (mode != NAN_BATCH_SEQUENTIAL_SAMPLES && mode != NAN_BATCH_INDEPENDENT_SAMPLES) {
-        set_error("mode must be NAN_BATCH_SEQUENTIAL_SAMPLES or NAN_BATCH_INDEPENDENT_SAMPLES");
+    if (mode != NAN_BATCH_SEQUENTIAL_SAMPLES && mode != NAN_BATCH_INDEPENDENT_SAMPLES &&
+        mode != NAN_BATCH_WAVEFRONT) {
+        set_error("mode must be NAN_BATCH_SEQUENTIAL_SAMPLES, NAN_BATCH_INDEPENDENT_SAMPLES or NAN_BATCH_WAVEFRONT");
         return NAN_ERR_INVALID_ARGUMENT;
+    }
+    if (mode == NAN_BATCH_WAVEFRONT && mode != b->mode) {
+        BatchImpl* m = b->impl;
+        NanContext* ctx = b->ctx;
+        // one path per probe in flight, plus room for the control words
+        const uint64_t need = (uint64_t)std::max(m->total, 1u) * nan_host::wavefront_bytes_per_path() + (1ull << 22);
+        cudaError_t err = cudaDeviceSynchronize();
+        if (err == cudaSuccess && !m->set_of) err = cudaMalloc(&m->set_of, sizeof(uint32_t) * std::max(m->total, 1u));
+        if (err == cudaSuccess && ctx->scratch_bytes < need) {
+            cudaFree(ctx->scratch);
+            ctx->scratch = nullptr;
+            ctx->scratch_bytes = 0;
+            err = cudaMalloc(&ctx->scratch, need);
+            if (err == cudaSuccess) ctx->scratch_bytes = need;
+        }
+        if (err != cudaSuccess) return cuda_fail(err, "batch wavefront scratch");
+        b->mode = mode;
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, nan_host::wavefront_extend_kernel(), 128, 0);
+        b->tuning.blocks_per_sm = (uint32_t)std::max(occ, 1);
+        b->tuning.units_per_grab = 1u;
+        drop_graph(m);
+        return NAN_OK;
     }
     if (mode != b->mode) {
         b->mode = mode;
@@ -430,7 +452,35 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
     float best_ms = -1.0f;
     // one untimed frame first (first touch of the scenes' data)
     int rc = batch_frame(b, 0u, spp, max_bounces, 1, st);
+    if (b->mode == NAN_BATCH_WAVEFRONT) {
+        // the traversal grid of the wavefront: persistent blocks per SM
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, nan_host::wavefront_extend_kernel(), 128, 0);
+        occ = std::max(occ, 1);
+        for (uint32_t bps : {(uint32_t)std::max(occ / 2, 1), (uint32_t)std::max(3 * occ / 4, 1), (uint32_t)occ}) {
+            if (rc) break;
+            NanBatchTuning t = b->tuning;
+            t.blocks_per_sm = bps;
+            b->tuning = t;
+            cudaEventRecord(e0, st);
+            rc = batch_frame(b, 0u, spp, max_bounces, 1, st);
+            cudaEventRecord(e1, st);
+            if (rc) break;
+            float ms = 0.0f;
+            err = cudaEventSynchronize(e1);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+            if (err != cudaSuccess) {
+                rc = cuda_fail(err, "autotune timing");
+                break;
+            }
+            if (best_ms < 0.0f || ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        }
+    }
     for (uint32_t depth : kDepths) {
+        if (b->mode == NAN_BATCH_WAVEFRONT) break;
         if (rc) break;
         if (depth < m->min_depth) continue;
         for (uint32_t cap : kRegCaps) {

@@ -9,6 +9,27 @@
 
 namespace nbd {
 
+// One probe set of a multi-scene batch (nan_batch.cu): the scene, its
+// lighting, the probe records and the outputs.
+struct BatchSet {
+    SceneView s;
+    LightingRaw light;
+    ProbeOut out;
+    const float4* probes;
+    const float4* pinst;
+    uint32_t probe_count;
+    uint32_t probe_instance_count;
+};
+
+// Device-side frame control of a batch: the work counter of the persistent
+// launch, the iteration and the reset flag of the current frame.
+struct BatchCtl {
+    uint32_t next;
+    uint32_t iteration;
+    uint32_t reset;
+    uint32_t pad;
+};
+
 // The probe's own surface point (estimate_surface_irradiance setup,
 // surface_probe_path_tracer.slang:206-236).
 struct ProbeSite {

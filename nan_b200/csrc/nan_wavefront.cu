@@ -18,6 +18,7 @@
 #include "nan_internal.h"
 #include "nan_scene.cuh"
 #include "nan_sinks.cuh"
+#include "nan_probe.cuh"
 
 namespace {
 
@@ -134,8 +135,21 @@ __global__ void __launch_bounds__(256) k_wf_octant_place(const uint32_t* __restr
     }
 }
 
-template <int kWidth>
-__global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* __restrict__ queue,
+// Scene of a path: one scene for the per-scene passes, the path's probe set
+// for the multi-scene batch (set index per path).
+struct OneScene {
+    SceneView s;
+    __device__ __forceinline__ const SceneView& of(uint32_t) const { return s; }
+};
+
+struct ManyScenes {
+    const BatchSet* sets;
+    const uint32_t* set_of;
+    __device__ __forceinline__ const SceneView& of(uint32_t p) const { return sets[set_of[p]].s; }
+};
+
+template <int kWidth, class Src>
+__global__ void __launch_bounds__(128) k_wf_extend(Src src, const uint32_t* __restrict__ queue,
                                                    uint32_t* ctl, const float4* __restrict__ ro,
                                                    const float4* __restrict__ rd, const uint32_t* __restrict__ flags,
                                                    float4* __restrict__ hit, unsigned long long* counters) {
@@ -153,6 +167,7 @@ __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* 
             if (flags[p] & kFlagNoPath) {
                 hit[p] = make_float4(__uint_as_float(0xffffffffu), 0.0f, 0.0f, 0.0f);
             } else {
+                const SceneView s = src.of(p);
                 const float4 o = ro[p], d = rd[p];
                 tally.extend++;
                 const HitInfo h = trace_closest_w<kWidth>(s, xyz(o), xyz(d), o.w, d.w);
@@ -163,8 +178,8 @@ __global__ void __launch_bounds__(128) k_wf_extend(SceneView s, const uint32_t* 
     flush_tally(counters, tally, 0u, 0u);
 }
 
-template <int kWidth>
-__global__ void __launch_bounds__(128) k_wf_shadow(SceneView s, const float4* __restrict__ queue, uint32_t* ctl,
+template <int kWidth, class Src>
+__global__ void __launch_bounds__(128) k_wf_shadow(Src src, const float4* __restrict__ queue, uint32_t* ctl,
                                                    float t_max, float4* __restrict__ rad, float4* __restrict__ si,
                                                    unsigned long long* counters) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 2);
@@ -179,8 +194,9 @@ __global__ void __launch_bounds__(128) k_wf_shadow(SceneView s, const float4* __
         if (idx < count) {
             const float4 a = queue[3u * idx], b = queue[3u * idx + 1u], c = queue[3u * idx + 2u];
             tally.shadow++;
+            const uint32_t p = __float_as_uint(a.w);
+            const SceneView s = src.of(p);
             if (!trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max)) {
-                const uint32_t p = __float_as_uint(a.w);
                 float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
                 const float4 v = target[p];
                 target[p] = make_float4(v.x + c.x, v.y + c.y, v.z + c.z, v.w);
@@ -639,21 +655,17 @@ __device__ __forceinline__ void probe_start_sample(const SceneView& s, const Lig
     q.ext[buf][slot] = p;
 }
 
-__global__ void __launch_bounds__(128) k_wf_probe_generate(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
-                                                           WfQueues q, uint32_t begin, uint32_t count,
-                                                           unsigned long long* counters) {
-    const uint32_t slot_p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot_p >= count) return;
-    const uint32_t probe = begin + slot_p;
+// Per-path bodies of the probe stages, shared by the one-scene kernels and the
+// multi-scene batch kernels (which look up the path's probe set first).
+__device__ __forceinline__ bool probe_generate_path(const SceneView& s, const LightParams& L, const ProbeArgs& a,
+                                                    const WfState& st, const WfQueues& q, uint32_t probe, uint32_t p) {
     const uint4 meta = __ldg(reinterpret_cast<const uint4*>(a.probes) + 3u * probe + 2u);
     const uint32_t inst = meta.w >> 8;
     if (inst >= a.probe_instance_count || !valid_prim(s, inst, meta.x)) {
         atomicOr(s.status, kStatusBadRecord);
-        return;
+        return false;
     }
     const float4 params = __ldg(a.pinst + 3u * inst + 2u);
-    const LightParams L = make_light(lraw);
-    const uint32_t p = slot_p;
     st.unit[p] = probe;
     st.surf[p] = make_float4(__uint_as_float(meta.y), __uint_as_float(meta.z), __uint_as_float(inst),
                              __uint_as_float(meta.x));
@@ -668,6 +680,137 @@ __global__ void __launch_bounds__(128) k_wf_probe_generate(SceneView s, Lighting
     Rng rng(probe, inst, a.iteration * a.n);
     probe_start_sample(s, L, a, st, q, 0, q.ctl, p, 0u, rng);
     st.rng[p] = rng.state;
+    return true;
+}
+
+__device__ __forceinline__ void probe_shade_path(const SceneView& s, const LightParams& L, const ProbeArgs& a,
+                                                 const WfState& st, const WfQueues& q, int buf, uint32_t* ctl,
+                                                 uint32_t p) {
+    uint32_t flags = st.flags[p];
+    if (flags & kFlagNoPath) {
+        st.flags[p] = flags | kFlagEnd;
+        return;
+    }
+    const float4 h = st.hit[p];
+    const f3 d = xyz(st.rd[p]);
+    f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
+    float4 pa = st.pa[p];  // src inst, src prim, src offset, first hit
+    const uint32_t bounce = (flags & kBounceMask) >> kBounceShift;
+    const float radial_max = 2.0f * st.si[p].w;
+    const uint32_t flat = __float_as_uint(h.x);
+    if (flat == 0xffffffffu) {
+        if (bounce == 0u) pa.w = radial_max;
+        rad = rad + thp * L.sky;
+        st.pa[p] = pa;
+        st.rad[p] = f4(rad, 0.0f);
+        st.flags[p] = flags | kFlagEnd;
+        return;
+    }
+    if (bounce == 0u) pa.w = minf(h.y, radial_max);
+    const uint2 ref = __ldg(s.tri_refs + flat);
+    const uint32_t src_inst = __float_as_uint(pa.x), src_prim = __float_as_uint(pa.y);
+    const bool same_prim = ref.x == src_inst && ref.y == src_prim;
+    const float thr = maxf(4.0f * pa.z, 1e-6f);
+    const bool adjacent = ref.x == src_inst && h.y <= thr;
+    if (same_prim || adjacent) {
+        uint4 b = st.pb[p];
+        b.x += 1u;
+        st.pb[p] = b;
+    }
+    Rng rng(0u, 0u, 0u);
+    rng.state = st.rng[p];
+    const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
+    rad = rad + thp * sd.emissive;
+    const float u0 = rng.next_1d(), u1 = rng.next_1d();
+    const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
+    const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
+    const f3 f = sd.diffuse * kInvPi;
+    // the set's own t_max travels with the shadow ray (the batch mixes scenes)
+    push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee, L.t_max);
+    const float e0 = rng.next_1d(), e1 = rng.next_1d();
+    float pdf;
+    const f3 sdir = cosine_sample_hemisphere(e0, e1, &pdf);
+    if (pdf <= 1e-6f) {
+        flags |= kFlagEnd;
+    } else {
+        thp = thp * ((f * fabsf(sdir.z)) / pdf);
+        const f3 next_origin = sd.origin_front;
+        st.ro[p] = f4(next_origin, 0.0f);
+        st.rd[p] = f4(Frame(normalize3(sd.face_normal)).to_global(sdir), L.t_max);
+        pa.x = __uint_as_float(ref.x);
+        pa.y = __uint_as_float(ref.y);
+        pa.z = len3(next_origin - sd.position);
+        const uint32_t next = bounce + 1u;
+        flags = (flags & ~kBounceMask) | (next << kBounceShift);
+        if (next >= a.max_bounces) flags |= kFlagEnd;
+    }
+    st.pa[p] = pa;
+    st.thp[p] = f4(thp, 0.0f);
+    st.rad[p] = f4(rad, 0.0f);
+    st.rng[p] = rng.state;
+    st.flags[p] = flags;
+}
+
+__device__ __forceinline__ void probe_finalize_path(const SceneView& s, const LightParams& L, const ProbeArgs& a,
+                                                    const WfState& st, const WfQueues& q, int buf,
+                                                    uint32_t* ctl_next, uint32_t p) {
+    const int nbuf = buf ^ 1;
+    uint32_t flags = st.flags[p];
+    if (!(flags & kFlagEnd)) {
+        const uint32_t slot = queue_slot(ctl_next + 0, true);
+        q.ext[nbuf][slot] = p;
+        return;
+    }
+    const uint32_t probe = st.unit[p];
+    f3 irr = xyz(st.irr[p]);
+    uint4 b = st.pb[p];
+    if (!(flags & kFlagNoPath)) {
+        b.y += b.x;  // self-hit suspects of this sample
+        const uint32_t texel = b.w;
+        uint4 c = st.pc[2u * p + (texel >> 3)];
+        const uint32_t word = (texel >> 1) & 3u, shift = (texel & 1u) * 16u;
+        uint32_t* cw = word == 0u ? &c.x : (word == 1u ? &c.y : (word == 2u ? &c.z : &c.w));
+        const uint32_t local = ((*cw >> shift) & 0xffffu) + 1u;
+        *cw = (*cw & ~(0xffffu << shift)) | ((local & 0xffffu) << shift);
+        st.pc[2u * p + (texel >> 3)] = c;
+        const float kr = st.si[p].w;
+        accumulate_radial_moment(a.out.radial, probe, texel, st.pa[p].w / maxf(kr, 1e-6f), b.z, local, a.spp);
+        const float2 zp = st.zpdf[p];
+        irr = irr + ((xyz(st.rad[p]) * zp.x) / zp.y);
+    }
+    st.pb[p] = b;
+    const uint32_t k = (flags >> kSampleShift) + 1u;
+    if (k < a.n) {
+        st.irr[p] = f4(irr, 0.0f);
+        Rng rng(0u, 0u, 0u);
+        rng.state = st.rng[p];
+        probe_start_sample(s, L, a, st, q, nbuf, ctl_next, p,
+                           (flags & ((1u << kSampleShift) - 1u)) | (k << kSampleShift), rng);
+        st.rng[p] = rng.state;
+        return;
+    }
+    irr = irr / (float)a.n;
+    const uint32_t prev = a.reset ? 0u : a.out.counts[probe];
+    f3 pv = mk3(0.0f, 0.0f, 0.0f);
+    if (prev != 0u)
+        pv = mk3(a.out.values[3u * probe], a.out.values[3u * probe + 1u], a.out.values[3u * probe + 2u]);
+    float4 comp = a.out.compensation ? a.out.compensation[probe] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const f3 acc = running_mean_step(pv, irr, prev, a.out.compensation ? &comp : nullptr);
+    if (a.out.compensation) a.out.compensation[probe] = comp;
+    a.out.values[3u * probe] = acc.x;
+    a.out.values[3u * probe + 1u] = acc.y;
+    a.out.values[3u * probe + 2u] = acc.z;
+    a.out.counts[probe] = min(prev + 1u, 65535u);
+    const uint32_t prev_self = a.reset ? 0u : a.out.self_hits[probe];
+    a.out.self_hits[probe] = prev_self + b.y;
+}
+
+__global__ void __launch_bounds__(128) k_wf_probe_generate(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+                                                           WfQueues q, uint32_t begin, uint32_t count,
+                                                           unsigned long long* counters) {
+    const uint32_t slot_p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot_p >= count) return;
+    if (!probe_generate_path(s, make_light(lraw), a, st, q, begin + slot_p, slot_p)) return;
     RayTally none{0u, 0u};
     flush_tally(counters, none, 1u, a.n);
 }
@@ -676,128 +819,81 @@ __global__ void __launch_bounds__(128) k_wf_probe_shade(SceneView s, LightingRaw
                                                         WfQueues q, int buf, uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
-    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
-        const uint32_t p = q.ext[buf][idx];
-        uint32_t flags = st.flags[p];
-        if (flags & kFlagNoPath) {
-            st.flags[p] = flags | kFlagEnd;
-            continue;
-        }
-        const float4 h = st.hit[p];
-        const f3 d = xyz(st.rd[p]);
-        f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
-        float4 pa = st.pa[p];  // src inst, src prim, src offset, first hit
-        const uint32_t bounce = (flags & kBounceMask) >> kBounceShift;
-        const float radial_max = 2.0f * st.si[p].w;
-        const uint32_t flat = __float_as_uint(h.x);
-        if (flat == 0xffffffffu) {
-            if (bounce == 0u) pa.w = radial_max;
-            rad = rad + thp * L.sky;
-            st.pa[p] = pa;
-            st.rad[p] = f4(rad, 0.0f);
-            st.flags[p] = flags | kFlagEnd;
-            continue;
-        }
-        if (bounce == 0u) pa.w = minf(h.y, radial_max);
-        const uint2 ref = __ldg(s.tri_refs + flat);
-        const uint32_t src_inst = __float_as_uint(pa.x), src_prim = __float_as_uint(pa.y);
-        const bool same_prim = ref.x == src_inst && ref.y == src_prim;
-        const float thr = maxf(4.0f * pa.z, 1e-6f);
-        const bool adjacent = ref.x == src_inst && h.y <= thr;
-        if (same_prim || adjacent) {
-            uint4 b = st.pb[p];
-            b.x += 1u;
-            st.pb[p] = b;
-        }
-        Rng rng(0u, 0u, 0u);
-        rng.state = st.rng[p];
-        const Shading sd = shading_data(s, ref.x, ref.y, h.z, h.w, -d);
-        rad = rad + thp * sd.emissive;
-        const float u0 = rng.next_1d(), u1 = rng.next_1d();
-        const f3 l = sample_cone_direction(L.sun_dir, L.cos_half, u0, u1);
-        const float ndl = maxf(0.0f, dot3(sd.frame.n, l));
-        const f3 f = sd.diffuse * kInvPi;
-        push_shadow(q, buf, ctl + 2, p, sd.origin_front, l, thp * ((f * L.illum) * ndl), kKindNee);
-        const float e0 = rng.next_1d(), e1 = rng.next_1d();
-        float pdf;
-        const f3 sdir = cosine_sample_hemisphere(e0, e1, &pdf);
-        if (pdf <= 1e-6f) {
-            flags |= kFlagEnd;
-        } else {
-            thp = thp * ((f * fabsf(sdir.z)) / pdf);
-            const f3 next_origin = sd.origin_front;
-            st.ro[p] = f4(next_origin, 0.0f);
-            st.rd[p] = f4(Frame(normalize3(sd.face_normal)).to_global(sdir), L.t_max);
-            pa.x = __uint_as_float(ref.x);
-            pa.y = __uint_as_float(ref.y);
-            pa.z = len3(next_origin - sd.position);
-            const uint32_t next = bounce + 1u;
-            flags = (flags & ~kBounceMask) | (next << kBounceShift);
-            if (next >= a.max_bounces) flags |= kFlagEnd;
-        }
-        st.pa[p] = pa;
-        st.thp[p] = f4(thp, 0.0f);
-        st.rad[p] = f4(rad, 0.0f);
-        st.rng[p] = rng.state;
-        st.flags[p] = flags;
-    }
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+        probe_shade_path(s, L, a, st, q, buf, ctl, q.ext[buf][idx]);
 }
 
 __global__ void __launch_bounds__(128) k_wf_probe_finalize(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
                                                            WfQueues q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
-    const int nbuf = buf ^ 1;
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+        probe_finalize_path(s, L, a, st, q, buf, ctl_next, q.ext[buf][idx]);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-scene probe batch on the wavefront: every (set, probe) unit of the
+// batch is one path in flight; each stage looks up the path's set (scene,
+// lighting, records, outputs). The iteration and reset come from the batch's
+// device control block, so a captured frame replays with the next iteration.
+// ---------------------------------------------------------------------------
+struct BatchWfArgs {
+    const BatchSet* sets;
+    const uint32_t* prefix;
+    const BatchCtl* ctl;
+    uint32_t* set_of;
+    uint32_t set_count, total, n, spp, max_bounces;
+};
+
+__device__ __forceinline__ ProbeArgs batch_probe_args(const BatchWfArgs& m, const BatchSet& b) {
+    ProbeArgs a;
+    a.out = b.out;
+    a.probes = b.probes;
+    a.pinst = b.pinst;
+    a.probe_instance_count = b.probe_instance_count;
+    a.iteration = m.ctl->iteration;
+    a.n = m.n;
+    a.spp = m.spp;
+    a.max_bounces = m.max_bounces;
+    a.reset = m.ctl->reset ? 1 : 0;
+    return a;
+}
+
+__global__ void __launch_bounds__(128) k_wfb_probe_generate(BatchWfArgs m, WfState st, WfQueues q,
+                                                            unsigned long long* counters) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= m.total) return;
+    uint32_t lo = 0u, hi = m.set_count - 1u;  // set = last s with prefix[s] <= u
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(m.prefix + mid) <= u) lo = mid;
+        else hi = mid - 1u;
+    }
+    m.set_of[u] = lo;
+    const BatchSet& b = m.sets[lo];
+    const ProbeArgs a = batch_probe_args(m, b);
+    if (!probe_generate_path(b.s, make_light(b.light), a, st, q, u - __ldg(m.prefix + lo), u)) return;
+    RayTally none{0u, 0u};
+    flush_tally(counters, none, 1u, a.n);
+}
+
+__global__ void __launch_bounds__(128) k_wfb_probe_shade(BatchWfArgs m, WfState st, WfQueues q, int buf,
+                                                         uint32_t* ctl) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
         const uint32_t p = q.ext[buf][idx];
-        uint32_t flags = st.flags[p];
-        if (!(flags & kFlagEnd)) {
-            const uint32_t slot = queue_slot(ctl_next + 0, true);
-            q.ext[nbuf][slot] = p;
-            continue;
-        }
-        const uint32_t probe = st.unit[p];
-        f3 irr = xyz(st.irr[p]);
-        uint4 b = st.pb[p];
-        if (!(flags & kFlagNoPath)) {
-            b.y += b.x;  // self-hit suspects of this sample
-            const uint32_t texel = b.w;
-            uint4 c = st.pc[2u * p + (texel >> 3)];
-            const uint32_t word = (texel >> 1) & 3u, shift = (texel & 1u) * 16u;
-            uint32_t* cw = word == 0u ? &c.x : (word == 1u ? &c.y : (word == 2u ? &c.z : &c.w));
-            const uint32_t local = ((*cw >> shift) & 0xffffu) + 1u;
-            *cw = (*cw & ~(0xffffu << shift)) | ((local & 0xffffu) << shift);
-            st.pc[2u * p + (texel >> 3)] = c;
-            const float kr = st.si[p].w;
-            accumulate_radial_moment(a.out.radial, probe, texel, st.pa[p].w / maxf(kr, 1e-6f), b.z, local, a.spp);
-            const float2 zp = st.zpdf[p];
-            irr = irr + ((xyz(st.rad[p]) * zp.x) / zp.y);
-        }
-        st.pb[p] = b;
-        const uint32_t k = (flags >> kSampleShift) + 1u;
-        if (k < a.n) {
-            st.irr[p] = f4(irr, 0.0f);
-            Rng rng(0u, 0u, 0u);
-            rng.state = st.rng[p];
-            probe_start_sample(s, L, a, st, q, nbuf, ctl_next, p,
-                               (flags & ((1u << kSampleShift) - 1u)) | (k << kSampleShift), rng);
-            st.rng[p] = rng.state;
-            continue;
-        }
-        irr = irr / (float)a.n;
-        const uint32_t prev = a.reset ? 0u : a.out.counts[probe];
-        f3 pv = mk3(0.0f, 0.0f, 0.0f);
-        if (prev != 0u)
-            pv = mk3(a.out.values[3u * probe], a.out.values[3u * probe + 1u], a.out.values[3u * probe + 2u]);
-        float4 comp = a.out.compensation ? a.out.compensation[probe] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        const f3 acc = running_mean_step(pv, irr, prev, a.out.compensation ? &comp : nullptr);
-        if (a.out.compensation) a.out.compensation[probe] = comp;
-        a.out.values[3u * probe] = acc.x;
-        a.out.values[3u * probe + 1u] = acc.y;
-        a.out.values[3u * probe + 2u] = acc.z;
-        a.out.counts[probe] = min(prev + 1u, 65535u);
-        const uint32_t prev_self = a.reset ? 0u : a.out.self_hits[probe];
-        a.out.self_hits[probe] = prev_self + b.y;
+        const BatchSet& b = m.sets[m.set_of[p]];
+        probe_shade_path(b.s, make_light(b.light), batch_probe_args(m, b), st, q, buf, ctl, p);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_wfb_probe_finalize(BatchWfArgs m, WfState st, WfQueues q, int buf,
+                                                            uint32_t* ctl, uint32_t* ctl_next) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        const BatchSet& b = m.sets[m.set_of[p]];
+        probe_finalize_path(b.s, make_light(b.light), batch_probe_args(m, b), st, q, buf, ctl_next, p);
     }
 }
 
@@ -847,7 +943,7 @@ Grid grid_for(const NanContext* ctx) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wf_extend<2>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_wf_extend<2, OneScene>, 128, 0);
     Grid g;
     const int per_sm = ctx->tuning.trace_blocks_per_sm ? (int)ctx->tuning.trace_blocks_per_sm : std::max(occ, 1);
     g.persistent_blocks = sms * per_sm;
@@ -1020,10 +1116,10 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
             }
             ev = timing_begin(ctx, st);
             if (s.wnodes)
-                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
                                                                    ctx->d_counters);
             else
-                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
                                                                    ctx->d_counters);
             timing_end(ctx, 0, ev, st);
             ev = timing_begin(ctx, st);
@@ -1031,10 +1127,10 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
             timing_end(ctx, 2, ev, st);
             ev = timing_begin(ctx, st);
             if (s.wnodes)
-                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
+                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.shd[buf], ctl, t_max, S.rad, S.si,
                                                                    ctx->d_counters);
             else
-                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(s, q.shd[buf], ctl, t_max, S.rad, S.si,
+                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.shd[buf], ctl, t_max, S.rad, S.si,
                                                                    ctx->d_counters);
             timing_end(ctx, 1, ev, st);
             ev = timing_begin(ctx, st);
@@ -1193,6 +1289,58 @@ int screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32
         });
 }
 }  // namespace
+
+const void* wavefront_extend_kernel() { return reinterpret_cast<const void*>(&k_wf_extend<2, ManyScenes>); }
+
+// The multi-scene probe batch on the wavefront: generate every (set, probe)
+// unit as one path, then n * max_bounces rounds of extend / shade / shadow /
+// finalize over all sets, with no host synchronisation (capturable). The
+// context's scratch must hold `total` paths.
+int launch_batch_wavefront(NanContext* ctx, const void* sets, const uint32_t* prefix, const void* batch_ctl,
+                           uint32_t set_count, uint32_t total, uint32_t* set_of, uint32_t spp, uint32_t max_bounces,
+                           float t_max, cudaStream_t st) {
+    if (total == 0) return NAN_OK;
+    const uint32_t n = std::max(spp, 1u);
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    int rc = wf_plan(ctx, (uint64_t)n * std::max(max_bounces, 1u), &iters, &cap);
+    if (rc) return rc;
+    if (cap < total) {
+        set_error("batch wavefront scratch holds fewer paths than the batch has probes");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    BatchWfArgs m;
+    m.sets = static_cast<const BatchSet*>(sets);
+    m.prefix = prefix;
+    m.ctl = static_cast<const BatchCtl*>(batch_ctl);
+    m.set_of = set_of;
+    m.set_count = set_count;
+    m.total = total;
+    m.n = n;
+    m.spp = spp;
+    m.max_bounces = std::max(max_bounces, 1u);
+    const ManyScenes src{m.sets, set_of};
+    const Grid g = grid_for(ctx);
+    WfState S;
+    WfQueues q;
+    wf_carve(ctx, total, iters, S, q);
+    cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 20 * sizeof(uint32_t), st);
+    if (err != cudaSuccess) return cuda_fail(err, "batch wavefront control reset");
+    k_wfb_probe_generate<<<(total + 127) / 128, 128, 0, st>>>(m, S, q, ctx->d_counters);
+    ctx->launches++;
+    for (uint32_t it = 0; it < iters; ++it) {
+        const int buf = (int)(it & 1u);
+        uint32_t* ctl = q.ctl + 4u * it;
+        k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                           ctx->d_counters);
+        k_wfb_probe_shade<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl);
+        k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.shd[buf], ctl, t_max, S.rad, S.si,
+                                                           ctx->d_counters);
+        k_wfb_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl, ctl + 4);
+        ctx->launches += 4;
+    }
+    return cuda_fail(cudaGetLastError(), "batch wavefront launch");
+}
 
 int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits,
                                   uint32_t* radial, const uint8_t* probes, uint32_t probe_count,

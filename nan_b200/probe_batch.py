@@ -11,7 +11,11 @@ Each item is a SurfaceProbeDiffuseIrradianceBaker with the field and
 attachments it would be executed with; the results equal those of
 baker.execute(...) per scene, bit for bit. With independent_samples=True
 each sample of a probe draws from its own RNG stream and a warp traces 32
-samples of one probe at once (a different, equally valid sample set).
+samples of one probe at once (a different, equally valid sample set). With
+wavefront=True the reference's sample sequence runs as one multi-scene
+wavefront: every probe of every scene is a path in flight and each
+extend / shade / shadow / finalize round covers all scenes (results equal
+the per-scene bakes bit for bit).
 """
 
 from __future__ import annotations
@@ -22,7 +26,9 @@ from ._native import NanBatchTuning, NanProbeSet, check, lib, ptr, stream_handle
 
 
 class ProbeBatch:
-    def __init__(self, device, items, *, independent_samples: bool = False):
+    def __init__(self, device, items, *, independent_samples: bool = False, wavefront: bool = False):
+        if independent_samples and wavefront:
+            raise ValueError("independent_samples and wavefront are exclusive")
         self.device = device
         self._keep = []
         sets = (NanProbeSet * max(len(items), 1))()
@@ -47,6 +53,8 @@ class ProbeBatch:
         self.handle = handle
         if independent_samples:
             check(lib().nan_batch_set_mode(self.handle, 1))
+        elif wavefront:
+            check(lib().nan_batch_set_mode(self.handle, 2))
 
     @property
     def context(self):

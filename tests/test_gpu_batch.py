@@ -1,7 +1,8 @@
 """Multi-scene probe batches: one persistent launch over the probe sets of
 several scenes of uneven size equals baking each scene on its own, bit for
 bit. That holds for direct frames, for frames replayed from the captured CUDA
-graph, and after the autotuner has changed the launch shape."""
+graph, and after the autotuner has changed the launch shape; and the same
+for the multi-scene wavefront mode."""
 
 import numpy as np
 import pytest
@@ -68,14 +69,14 @@ def _reference(device, sets, frames):
     return refs
 
 
-def _bake_batch(device, sets, run):
+def _bake_batch(device, sets, run, **mode):
     import nan_b200
 
     bufs = [_buffers(device, b) for _, b in sets]
     for _, b in sets:
         if b.compensation is not None:
             b.compensation.zero_()
-    batch = nan_b200.ProbeBatch(device, [(b, f, a) for (_, b), (f, a) in zip(sets, bufs)])
+    batch = nan_b200.ProbeBatch(device, [(b, f, a) for (_, b), (f, a) in zip(sets, bufs)], **mode)
     run(batch)
     return batch, [_snapshot(f, a, b) for (_, b), (f, a) in zip(sets, bufs)]
 
@@ -159,4 +160,35 @@ def test_batch_independent_samples_match_oracle(device):
         exact = np.all(g_values == values, axis=1) & (g_self == self_hits) & np.all(g_radial == radial, axis=1)
         print("independent samples vs oracle exact", exact.mean())
         assert exact.mean() >= 0.999, exact.mean()
+    device.check()
+
+
+def test_batch_wavefront_equals_per_scene_bakes(device, sets):
+    """The multi-scene wavefront (every probe of every scene a path in
+    flight) keeps the reference's sample sequence: direct frames, autotuned
+    and graph-replayed frames equal the per-scene bakes bit for bit."""
+    refs = _reference(device, sets, 3)
+
+    def direct(batch):
+        for it in range(3):
+            batch.execute(None, it, 4, 3, reset=(it == 0))
+
+    _, got = _bake_batch(device, sets, direct, wavefront=True)
+    for g, ref in zip(got, refs):
+        for a, b in zip(g, ref):
+            np.testing.assert_array_equal(a, b)
+
+    def tuned_graph(batch):
+        tuned = batch.autotune(4, 3)
+        print("wavefront autotune", tuned)
+        for _, b in sets:
+            if b.compensation is not None:
+                b.compensation.zero_()
+        batch.capture(0, True, 4, 3)
+        batch.replay(3)
+
+    _, got = _bake_batch(device, sets, tuned_graph, wavefront=True)
+    for g, ref in zip(got, refs):
+        for a, b in zip(g, ref):
+            np.testing.assert_array_equal(a, b)
     device.check()
