@@ -158,6 +158,7 @@ def main() -> None:
     ap.add_argument("--count", type=int, default=16)
     ap.add_argument("--frames", type=int, default=2)
     ap.add_argument("--independent-samples", action="store_true")
+    ap.add_argument("--wavefront", action="store_true")
     a = ap.parse_args()
     device = Device(0)
     items = []
@@ -173,7 +174,8 @@ def main() -> None:
                                                    compensated=True)
         rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)
         items.append((scene, baker, rt.field, rt.attachments))
-    batch = ProbeBatch(device, [(b, f, at) for _, b, f, at in items], independent_samples=a.independent_samples)
+    batch = ProbeBatch(device, [(b, f, at) for _, b, f, at in items], independent_samples=a.independent_samples,
+                       wavefront=a.wavefront)
     for f in range(a.frames):
         batch.execute(None, f, 64, 3, reset=(f == 0))
     torch.cuda.synchronize()
