@@ -492,8 +492,17 @@ NAN_B200_API int nan_batch_set_tuning(NanBatch* batch, const NanBatchTuning* tun
  * every set one path in flight; extend / shade / shadow / finalize rounds
  * over all sets; bit-exact with SEQUENTIAL); allocates one path of scratch
  * per probe on the batch's context; the tuning's blocks_per_sm is the
- * traversal grid. Resets the launch shape to the new kernel's defaults. */
-enum { NAN_BATCH_SEQUENTIAL_SAMPLES = 0, NAN_BATCH_INDEPENDENT_SAMPLES = 1, NAN_BATCH_WAVEFRONT = 2 };
+ * traversal grid. WAVEFRONT_INDEPENDENT: the INDEPENDENT sample streams on
+ * the wavefront, one path per (probe, sample), in chunks of up to 2^24 paths,
+ * each finished sample stored and every probe's samples folded in sample
+ * order (bit-exact with INDEPENDENT). Resets the launch shape to the new
+ * kernel's defaults. */
+enum {
+    NAN_BATCH_SEQUENTIAL_SAMPLES = 0,
+    NAN_BATCH_INDEPENDENT_SAMPLES = 1,
+    NAN_BATCH_WAVEFRONT = 2,
+    NAN_BATCH_WAVEFRONT_INDEPENDENT = 3
+};
 NAN_B200_API int nan_batch_set_mode(NanBatch* batch, uint32_t mode);
 /* One iteration of every set (nan_trace_probes semantics per set). */
 NAN_B200_API int nan_batch_trace_probes(NanBatch* batch, uint32_t iteration, uint32_t samples_per_probe,

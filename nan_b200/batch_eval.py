@@ -109,6 +109,15 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     c = wf.context.read_counters(reset=True)
     wf_rays = (c["extend_rays"] + c["shadow_rays"]) / (frames + 1)
     wf.close()
+    # independent samples on the wavefront: one path per (probe, sample)
+    wfi = ProbeBatch(device, [(b, f, a) for _, b, f, a in items], independent_samples=True, wavefront=True)
+    tuned_wfi = wfi.autotune(samples_per_probe, max_bounces)
+    wfi.capture(0, True, samples_per_probe, max_bounces)
+    wfi.context.read_counters(reset=True)
+    wfi_ms = timed(lambda f: wfi.replay(1, stream))
+    c = wfi.context.read_counters(reset=True)
+    wfi_rays = (c["extend_rays"] + c["shadow_rays"]) / (frames + 1)
+    wfi.close()
     # one RNG stream per sample: a warp traces 32 samples of one probe at once
     ind = ProbeBatch(device, [(b, f, a) for _, b, f, a in items], independent_samples=True)
     tuned_ind = ind.autotune(samples_per_probe, max_bounces)
@@ -126,15 +135,18 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
         "setup_s": setup_s, "site_placement": dict(placement, method="weighted sample elimination on the GPU, "
                                                                    "5x oversampled area-weighted candidates"),
         "autotune": tuned, "autotune_independent_samples": tuned_ind, "autotune_wavefront": tuned_wf,
+        "autotune_wavefront_independent_samples": tuned_wfi,
         "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
                          "batched": batch_ms, "batched_graph": graph_ms,
                          "batched_graph_wavefront": wf_ms,
+                         "batched_graph_wavefront_independent_samples": wfi_ms,
                          "batched_graph_independent_samples": ind_ms},
         "rays_per_frame": batch_rays, "per_scene_rays_per_frame": per_scene_rays,
         "mrays_per_s": {"per_scene_wavefront": per_scene_rays / (per_scene_ms * 1e3),
                         "per_scene_megakernel": per_scene_rays / (per_scene_mk_ms * 1e3),
                         "batched": batch_rays / (batch_ms * 1e3), "batched_graph": batch_rays / (graph_ms * 1e3),
                         "batched_graph_wavefront": wf_rays / (wf_ms * 1e3),
+                        "batched_graph_wavefront_independent_samples": wfi_rays / (wfi_ms * 1e3),
                         "batched_graph_independent_samples": ind_rays / (ind_ms * 1e3)},
     }
 

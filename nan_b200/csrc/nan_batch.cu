@@ -201,8 +201,11 @@ struct BatchImpl {
     BatchSet* sets = nullptr;
     uint32_t* prefix = nullptr;
     BatchCtl* ctl = nullptr;
-    uint32_t* set_of = nullptr;  // wavefront mode: probe set of each path
-    float t_max = 0.0f;          // largest ray t_max of the sets
+    uint32_t* set_of = nullptr;      // wavefront modes: probe set of each path
+    uint64_t set_of_paths = 0;       // entries of set_of
+    void* samples = nullptr;         // independent wavefront: one sample record per path
+    uint64_t sample_paths = 0;       // paths the sample records and the scratch hold
+    float t_max = 0.0f;              // largest ray t_max of the sets
     uint32_t set_count = 0;
     uint32_t total = 0;
     uint32_t min_depth = 32;  // smallest stack depth that covers every scene's BVH
@@ -215,9 +218,13 @@ namespace {
 
 int launch_frame_kernel(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t st) {
     BatchImpl* m = b->impl;
-    if (b->mode == NAN_BATCH_WAVEFRONT) {
+    if (b->mode == NAN_BATCH_WAVEFRONT || b->mode == NAN_BATCH_WAVEFRONT_INDEPENDENT) {
         NanTuning& tt = b->ctx->tuning;
         tt.trace_blocks_per_sm = b->tuning.blocks_per_sm;
+        if (b->mode == NAN_BATCH_WAVEFRONT_INDEPENDENT)
+            return nan_host::launch_batch_wavefront_independent(b->ctx, m->sets, m->prefix, m->ctl, m->set_count,
+                                                                m->total, m->set_of, m->samples, m->sample_paths,
+                                                                spp, max_bounces, m->t_max, st);
         return nan_host::launch_batch_wavefront(b->ctx, m->sets, m->prefix, m->ctl, m->set_count, m->total, m->set_of,
                                                 spp, max_bounces, m->t_max, st);
     }
@@ -317,6 +324,7 @@ void batch_destroy(NanBatch* b) {
         cudaFree(m->prefix);
         cudaFree(m->ctl);
         cudaFree(m->set_of);
+        cudaFree(m->samples);
         delete m;
     }
     delete b;
@@ -326,17 +334,37 @@ uint32_t batch_min_depth(const NanBatch* b) { return b->impl->min_depth; }
 
 int batch_set_mode(NanBatch* b, uint32_t mode) {
     if (mode != NAN_BATCH_SEQUENTIAL_SAMPLES && mode != NAN_BATCH_INDEPENDENT_SAMPLES &&
-        mode != NAN_BATCH_WAVEFRONT) {
-        set_error("mode must be NAN_BATCH_SEQUENTIAL_SAMPLES, NAN_BATCH_INDEPENDENT_SAMPLES or NAN_BATCH_WAVEFRONT");
+        mode != NAN_BATCH_WAVEFRONT && mode != NAN_BATCH_WAVEFRONT_INDEPENDENT) {
+        set_error("mode must be NAN_BATCH_SEQUENTIAL_SAMPLES, NAN_BATCH_INDEPENDENT_SAMPLES, NAN_BATCH_WAVEFRONT or "
+                  "NAN_BATCH_WAVEFRONT_INDEPENDENT");
         return NAN_ERR_INVALID_ARGUMENT;
     }
-    if (mode == NAN_BATCH_WAVEFRONT && mode != b->mode) {
+    if ((mode == NAN_BATCH_WAVEFRONT || mode == NAN_BATCH_WAVEFRONT_INDEPENDENT) && mode != b->mode) {
         BatchImpl* m = b->impl;
         NanContext* ctx = b->ctx;
-        // one path per probe in flight, plus room for the control words
-        const uint64_t need = (uint64_t)std::max(m->total, 1u) * nan_host::wavefront_bytes_per_path() + (1ull << 22);
+        // WAVEFRONT: one path per probe; INDEPENDENT: one path per (probe,
+        // sample), in chunks of at most 2^24 paths (64 samples of every probe
+        // when the batch is smaller)
+        const bool ind = mode == NAN_BATCH_WAVEFRONT_INDEPENDENT;
+        const uint64_t paths = ind ? std::min<uint64_t>(std::max<uint64_t>((uint64_t)m->total * 64ull, 1ull << 15),
+                                                        1ull << 24)
+                                   : std::max<uint64_t>(m->total, 1u);
+        const uint64_t need = paths * nan_host::wavefront_bytes_per_path() + (1ull << 22);
         cudaError_t err = cudaDeviceSynchronize();
-        if (err == cudaSuccess && !m->set_of) err = cudaMalloc(&m->set_of, sizeof(uint32_t) * std::max(m->total, 1u));
+        if (err == cudaSuccess && m->set_of_paths < paths) {
+            cudaFree(m->set_of);
+            m->set_of = nullptr;
+            m->set_of_paths = 0;
+            err = cudaMalloc(&m->set_of, sizeof(uint32_t) * paths);
+            if (err == cudaSuccess) m->set_of_paths = paths;
+        }
+        if (err == cudaSuccess && ind && m->sample_paths < paths) {
+            cudaFree(m->samples);
+            m->samples = nullptr;
+            m->sample_paths = 0;
+            err = cudaMalloc(&m->samples, nan_host::probe_sample_bytes() * paths);
+            if (err == cudaSuccess) m->sample_paths = paths;
+        }
         if (err == cudaSuccess && ctx->scratch_bytes < need) {
             cudaFree(ctx->scratch);
             ctx->scratch = nullptr;
@@ -452,7 +480,7 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
     float best_ms = -1.0f;
     // one untimed frame first (first touch of the scenes' data)
     int rc = batch_frame(b, 0u, spp, max_bounces, 1, st);
-    if (b->mode == NAN_BATCH_WAVEFRONT) {
+    if (b->mode == NAN_BATCH_WAVEFRONT || b->mode == NAN_BATCH_WAVEFRONT_INDEPENDENT) {
         // the traversal grid of the wavefront: persistent blocks per SM
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, nan_host::wavefront_extend_kernel(), 128, 0);
@@ -480,7 +508,7 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
         }
     }
     for (uint32_t depth : kDepths) {
-        if (b->mode == NAN_BATCH_WAVEFRONT) break;
+        if (b->mode == NAN_BATCH_WAVEFRONT || b->mode == NAN_BATCH_WAVEFRONT_INDEPENDENT) break;
         if (rc) break;
         if (depth < m->min_depth) continue;
         for (uint32_t cap : kRegCaps) {

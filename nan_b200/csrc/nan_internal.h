@@ -126,6 +126,11 @@ const void* wavefront_extend_kernel();  // for occupancy queries
 int launch_batch_wavefront(NanContext* ctx, const void* sets, const uint32_t* prefix, const void* batch_ctl,
                            uint32_t set_count, uint32_t total, uint32_t* set_of, uint32_t spp, uint32_t max_bounces,
                            float t_max, cudaStream_t st);
+int launch_batch_wavefront_independent(NanContext* ctx, const void* sets, const uint32_t* prefix,
+                                       const void* batch_ctl, uint32_t set_count, uint32_t total, uint32_t* set_of,
+                                       void* samples, uint64_t path_capacity, uint32_t spp, uint32_t max_bounces,
+                                       float t_max, cudaStream_t st);
+size_t probe_sample_bytes();
 int launch_trace_probes_wavefront(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits,
                                   uint32_t* radial, const uint8_t* probes, uint32_t probe_count,
                                   const uint8_t* probe_instances, uint32_t probe_instance_count, uint32_t iteration,

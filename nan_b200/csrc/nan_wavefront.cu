@@ -843,7 +843,21 @@ struct BatchWfArgs {
     const BatchCtl* ctl;
     uint32_t* set_of;
     uint32_t set_count, total, n, spp, max_bounces;
+    // independent samples: units [unit_begin, unit_begin + units) of this
+    // chunk, one path per (unit, sample), and the per-sample results
+    uint32_t unit_begin, units;
+    ProbeSample* samples;
 };
+
+__device__ __forceinline__ uint32_t batch_set_of_unit(const BatchWfArgs& m, uint32_t u) {
+    uint32_t lo = 0u, hi = m.set_count - 1u;  // set = last s with prefix[s] <= u
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(m.prefix + mid) <= u) lo = mid;
+        else hi = mid - 1u;
+    }
+    return lo;
+}
 
 __device__ __forceinline__ ProbeArgs batch_probe_args(const BatchWfArgs& m, const BatchSet& b) {
     ProbeArgs a;
@@ -875,6 +889,96 @@ __global__ void __launch_bounds__(128) k_wfb_probe_generate(BatchWfArgs m, WfSta
     if (!probe_generate_path(b.s, make_light(b.light), a, st, q, u - __ldg(m.prefix + lo), u)) return;
     RayTally none{0u, 0u};
     flush_tally(counters, none, 1u, a.n);
+}
+
+// Independent samples (NAN_BATCH_WAVEFRONT_INDEPENDENT): sample k of a probe
+// draws from RNG(probe, instance, iteration * n + k) and is its own path, so a
+// frame is max_bounces rounds; every finished path stores its sample, and a
+// last pass folds each probe's samples in sample order, as the
+// independent-sample persistent kernel does.
+__global__ void __launch_bounds__(128) k_wfi_probe_generate(BatchWfArgs m, WfState st, WfQueues q) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= m.units * m.n) return;
+    const uint32_t uoff = p / m.n, k = p - uoff * m.n;
+    const uint32_t u = m.unit_begin + uoff;
+    const uint32_t set = batch_set_of_unit(m, u);
+    m.set_of[p] = set;
+    const BatchSet& b = m.sets[set];
+    const uint32_t probe = u - __ldg(m.prefix + set);
+    const ProbeArgs a = batch_probe_args(m, b);
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(a.probes) + 3u * probe + 2u);
+    const uint32_t inst = meta.w >> 8;
+    if (inst >= a.probe_instance_count || !valid_prim(b.s, inst, meta.x)) {
+        atomicOr(b.s.status, kStatusBadRecord);
+        ProbeSample none;
+        none.si = mk3(0.0f, 0.0f, 0.0f);
+        none.self_hits = 0u;
+        none.texel = 0u;
+        none.nd = 0.0f;
+        none.has_path = false;
+        m.samples[p] = none;
+        return;
+    }
+    const float4 params = __ldg(a.pinst + 3u * inst + 2u);
+    st.unit[p] = probe;
+    st.surf[p] = make_float4(__uint_as_float(meta.y), __uint_as_float(meta.z), __uint_as_float(inst),
+                             __uint_as_float(meta.x));
+    st.si[p] = make_float4(0.0f, 0.0f, 0.0f, maxf(params.x, 1e-6f));
+    st.pb[p] = make_uint4(0u, 0u, 0u, 0u);
+    Rng rng(probe, inst, a.iteration * m.n + k);
+    probe_start_sample(b.s, make_light(b.light), a, st, q, 0, q.ctl, p, 0u, rng);
+    st.rng[p] = rng.state;
+}
+
+__global__ void __launch_bounds__(128) k_wfi_probe_finalize(BatchWfArgs m, WfState st, WfQueues q, int buf,
+                                                            uint32_t* ctl, uint32_t* ctl_next) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+        const uint32_t p = q.ext[buf][idx];
+        const uint32_t flags = st.flags[p];
+        if (!(flags & kFlagEnd)) {
+            const uint32_t slot = queue_slot(ctl_next + 0, true);
+            q.ext[buf ^ 1][slot] = p;
+            continue;
+        }
+        ProbeSample r;
+        r.si = mk3(0.0f, 0.0f, 0.0f);
+        r.self_hits = 0u;
+        r.texel = 0u;
+        r.nd = 0.0f;
+        r.has_path = !(flags & kFlagNoPath);
+        if (r.has_path) {
+            const uint4 b = st.pb[p];
+            const float2 zp = st.zpdf[p];
+            r.si = r.si + ((xyz(st.rad[p]) * zp.x) / zp.y);
+            r.self_hits = b.x;
+            r.texel = b.w;
+            r.nd = st.pa[p].w / maxf(st.si[p].w, 1e-6f);
+        }
+        m.samples[p] = r;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_wfi_probe_fold(BatchWfArgs m, unsigned long long* counters) {
+    const uint32_t uoff = blockIdx.x * blockDim.x + threadIdx.x;
+    if (uoff >= m.units) return;
+    const uint32_t u = m.unit_begin + uoff;
+    const uint32_t set = batch_set_of_unit(m, u);
+    const BatchSet& b = m.sets[set];
+    const uint32_t probe = u - __ldg(m.prefix + set);
+    const uint4 meta = __ldg(reinterpret_cast<const uint4*>(b.probes) + 3u * probe + 2u);
+    const uint32_t inst = meta.w >> 8;
+    if (inst >= b.probe_instance_count || !valid_prim(b.s, inst, meta.x)) return;
+    const int reset = m.ctl->reset ? 1 : 0;
+    const uint32_t prev_iter = reset ? 0u : b.out.counts[probe];
+    if (reset)
+        for (int t = 0; t < 16; ++t) b.out.radial[16u * probe + (uint32_t)t] = 0u;
+    ProbeAcc acc;
+    probe_acc_init(acc);
+    for (uint32_t k = 0; k < m.n; ++k) probe_fold(acc, b.out, probe, m.samples[uoff * m.n + k], prev_iter, m.spp);
+    probe_store(b.out, probe, acc, m.n, reset);
+    RayTally none{0u, 0u};
+    flush_tally(counters, none, 1u, m.n);
 }
 
 __global__ void __launch_bounds__(128) k_wfb_probe_shade(BatchWfArgs m, WfState st, WfQueues q, int buf,
@@ -1290,6 +1394,8 @@ int screen_wavefront(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32
 }
 }  // namespace
 
+size_t probe_sample_bytes() { return sizeof(ProbeSample); }
+
 const void* wavefront_extend_kernel() { return reinterpret_cast<const void*>(&k_wf_extend<2, ManyScenes>); }
 
 // The multi-scene probe batch on the wavefront: generate every (set, probe)
@@ -1319,6 +1425,9 @@ int launch_batch_wavefront(NanContext* ctx, const void* sets, const uint32_t* pr
     m.n = n;
     m.spp = spp;
     m.max_bounces = std::max(max_bounces, 1u);
+    m.unit_begin = 0u;
+    m.units = total;
+    m.samples = nullptr;
     const ManyScenes src{m.sets, set_of};
     const Grid g = grid_for(ctx);
     WfState S;
@@ -1338,6 +1447,61 @@ int launch_batch_wavefront(NanContext* ctx, const void* sets, const uint32_t* pr
                                                            ctx->d_counters);
         k_wfb_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl, ctl + 4);
         ctx->launches += 4;
+    }
+    return cuda_fail(cudaGetLastError(), "batch wavefront launch");
+}
+
+int launch_batch_wavefront_independent(NanContext* ctx, const void* sets, const uint32_t* prefix,
+                                       const void* batch_ctl, uint32_t set_count, uint32_t total, uint32_t* set_of,
+                                       void* samples, uint64_t path_capacity, uint32_t spp, uint32_t max_bounces,
+                                       float t_max, cudaStream_t st) {
+    if (total == 0) return NAN_OK;
+    const uint32_t n = std::max(spp, 1u);
+    uint32_t iters = 0;
+    uint64_t cap = 0;
+    int rc = wf_plan(ctx, std::max(max_bounces, 1u), &iters, &cap);
+    if (rc) return rc;
+    cap = std::min(cap, path_capacity);
+    const uint64_t chunk_units = cap / n;
+    if (chunk_units == 0) {
+        set_error("batch wavefront scratch holds fewer paths than one probe's samples");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    BatchWfArgs m;
+    m.sets = static_cast<const BatchSet*>(sets);
+    m.prefix = prefix;
+    m.ctl = static_cast<const BatchCtl*>(batch_ctl);
+    m.set_of = set_of;
+    m.set_count = set_count;
+    m.total = total;
+    m.n = n;
+    m.spp = spp;
+    m.max_bounces = std::max(max_bounces, 1u);
+    m.samples = static_cast<ProbeSample*>(samples);
+    const ManyScenes src{m.sets, set_of};
+    const Grid g = grid_for(ctx);
+    for (uint64_t ub = 0; ub < total; ub += chunk_units) {
+        m.unit_begin = (uint32_t)ub;
+        m.units = (uint32_t)std::min<uint64_t>(chunk_units, total - ub);
+        const uint32_t paths = m.units * n;
+        WfState S;
+        WfQueues q;
+        wf_carve(ctx, paths, iters, S, q);
+        cudaError_t err = cudaMemsetAsync(q.ctl, 0, (size_t)(iters + 2) * 20 * sizeof(uint32_t), st);
+        if (err != cudaSuccess) return cuda_fail(err, "batch wavefront control reset");
+        k_wfi_probe_generate<<<(paths + 127) / 128, 128, 0, st>>>(m, S, q);
+        for (uint32_t it = 0; it < iters; ++it) {
+            const int buf = (int)(it & 1u);
+            uint32_t* ctl = q.ctl + 4u * it;
+            k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
+                                                               ctx->d_counters);
+            k_wfb_probe_shade<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl);
+            k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.shd[buf], ctl, t_max, S.rad, S.si,
+                                                               ctx->d_counters);
+            k_wfi_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl, ctl + 4);
+        }
+        k_wfi_probe_fold<<<(m.units + 127) / 128, 128, 0, st>>>(m, ctx->d_counters);
+        ctx->launches += 2 + 4ull * iters;
     }
     return cuda_fail(cudaGetLastError(), "batch wavefront launch");
 }

@@ -15,7 +15,9 @@ samples of one probe at once (a different, equally valid sample set). With
 wavefront=True the reference's sample sequence runs as one multi-scene
 wavefront: every probe of every scene is a path in flight and each
 extend / shade / shadow / finalize round covers all scenes (results equal
-the per-scene bakes bit for bit).
+the per-scene bakes bit for bit); with both flags every (probe, sample) is
+a path and the samples are folded in order afterwards (results equal the
+independent-sample persistent kernel's).
 """
 
 from __future__ import annotations
@@ -27,8 +29,7 @@ from ._native import NanBatchTuning, NanProbeSet, check, lib, ptr, stream_handle
 
 class ProbeBatch:
     def __init__(self, device, items, *, independent_samples: bool = False, wavefront: bool = False):
-        if independent_samples and wavefront:
-            raise ValueError("independent_samples and wavefront are exclusive")
+
         self.device = device
         self._keep = []
         sets = (NanProbeSet * max(len(items), 1))()
@@ -51,10 +52,9 @@ class ProbeBatch:
         handle = ctypes.c_void_p()
         check(lib().nan_batch_create(self._context.handle, sets, len(items), ctypes.byref(handle)))
         self.handle = handle
-        if independent_samples:
-            check(lib().nan_batch_set_mode(self.handle, 1))
-        elif wavefront:
-            check(lib().nan_batch_set_mode(self.handle, 2))
+        mode = (3 if wavefront else 1) if independent_samples else (2 if wavefront else 0)
+        if mode:
+            check(lib().nan_batch_set_mode(self.handle, mode))
 
     @property
     def context(self):

@@ -192,3 +192,32 @@ def test_batch_wavefront_equals_per_scene_bakes(device, sets):
         for a, b in zip(g, ref):
             np.testing.assert_array_equal(a, b)
     device.check()
+
+
+def test_batch_wavefront_independent_equals_persistent_independent(device):
+    """Independent samples on the wavefront (one path per probe and sample,
+    samples folded in order afterwards) equal the persistent independent
+    kernel bit for bit; with 2 spp x 3 bounces and 70 spp (more than one warp
+    of samples per probe)."""
+    import nan_b200
+    from nan_b200 import scenes
+
+    sets = [_probe_set(device, scenes.cornell_box(32, 32), 300, seed=7),
+            _probe_set(device, scenes.terrain_boxes(seed=3, grid=97, boxes=60), 700, seed=8, compensated=True)]
+    for spp in (2, 70):
+        results = []
+        for wavefront in (False, True):
+            bufs = [_buffers(device, b) for _, b in sets]
+            for _, b in sets:
+                if b.compensation is not None:
+                    b.compensation.zero_()
+            batch = nan_b200.ProbeBatch(device, [(b, f, a) for (_, b), (f, a) in zip(sets, bufs)],
+                                        independent_samples=True, wavefront=wavefront)
+            for it in range(3):
+                batch.execute(None, it, spp, 3, reset=(it == 0))
+            results.append([_snapshot(f, a, b) for (_, b), (f, a) in zip(sets, bufs)])
+            batch.close()
+        for g, ref in zip(*results):
+            for a, b in zip(g, ref):
+                np.testing.assert_array_equal(a, b)
+    device.check()
