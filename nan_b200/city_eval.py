@@ -3,7 +3,7 @@
 learned-cache path tracer, and the plain one for comparison), a 20,480-site
 surface-probe pass (sites by weighted sample elimination of 5x oversampled
 candidates on the GPU; 64 spp, 3 bounces, compensated sums, batched launch
-with one RNG stream per sample) and
+with one RNG stream per sample, one wavefront path per probe and sample) and
 a Mesh Colors texel pass over the whole city (about 12.6 M texels, 1 sample,
 3 bounces). Every pass is timed with CUDA events on the launching stream
 after one warm-up frame; rays are counted on the device.
@@ -94,7 +94,7 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
                                                compensated=True)
     rt = SurfaceProbeRuntimeBuffers.acquire(rd, geometry.probe_count)
-    batch = ProbeBatch(device, [(baker, rt.field, rt.attachments)], independent_samples=True)
+    batch = ProbeBatch(device, [(baker, rt.field, rt.attachments)], independent_samples=True, wavefront=True)
     tuned = batch.autotune(64, 3)
     res["probes"] = timed(lambda f: batch.execute(stream, f, 64, 3, reset=(f == 0)), batch.context)
     res["probes"]["autotune"] = tuned
