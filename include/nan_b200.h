@@ -173,6 +173,15 @@ typedef struct NanRepairOptions {
     float weight_epsilon;          /* 1e-6 in the reference */
 } NanRepairOptions;
 
+/* Options of the support estimate (SurfaceProbeSupportOptions,
+ * surface_probe_sampler.h:87-92). */
+typedef struct NanSupportOptions {
+    float normal_cosine_threshold; /* full-confidence cosine of the soft normal gate (0.5) */
+    float weight_epsilon;          /* kernel values at or below are 0 (1e-6) */
+    float max_density_multiplier;  /* M (8) */
+    float reserved;
+} NanSupportOptions;
+
 /* Execution choices of a context. The defaults (all zero) are the wavefront
  * integrator with occupancy-sized persistent traversal grids, as many paths
  * in flight as the reserved scratch holds, and the PLOC BVH builder. */
@@ -438,6 +447,25 @@ NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions
                                     uint32_t* counts_before, uint32_t* counts_after, float* weight_sums_before,
                                     float* weight_sums_after, float* ess_before, float* ess_after,
                                     uint32_t* rounds, void* stream);
+
+/* Support estimate (estimate_surface_support, surface_probes.py:1256-1299;
+ * surface_probe_estimate_support, surface_probe_sampler.h:120-223; the
+ * Python form estimate_support_python, surface_probe_sampler.py:1179-1260):
+ * per query site, support = the float64 sum (ascending reference index,
+ * numpy's pairwise scheme) of kernel x area weight over the reference points
+ * of its instance within that instance's radius; f = clip(support / (pi R^2
+ * / 3), 0, 1) and m = min(M, 1 / max(f, 1 / M)). Reference and query arrays
+ * are device memory as in nan_deficit_repair; support_f and density_m are
+ * device f32[query_count]. NAN_ERR_LIMIT when a query reaches more than 512
+ * reference points. Allocates scratch on the stream and synchronizes it. */
+NAN_B200_API int nan_estimate_support(NanContext* ctx, const float* reference_positions,
+                                      const float* reference_normals, const uint32_t* reference_instances,
+                                      const float* reference_area_weights, uint32_t reference_count,
+                                      const float* query_positions, const float* query_normals,
+                                      const uint32_t* query_instances, uint32_t query_count,
+                                      const float* instance_radii, uint32_t instance_count,
+                                      const NanSupportOptions* options, float* support_f, float* density_m,
+                                      void* stream);
 
 /* 16-byte slots -> one RGB9E5 uint each (MeshColorsRGB9E5Packer.execute,
  * mesh_colors_rgb9e5.py:4-29; mesh_colors_rgb9e5_pack.slang:7-16). */

@@ -229,6 +229,11 @@ class NanRepairOptions(ctypes.Structure):
                 ("normal_cosine_threshold", ctypes.c_float), ("weight_epsilon", ctypes.c_float)]
 
 
+class NanSupportOptions(ctypes.Structure):
+    _fields_ = [("normal_cosine_threshold", ctypes.c_float), ("weight_epsilon", ctypes.c_float),
+                ("max_density_multiplier", ctypes.c_float), ("reserved", ctypes.c_float)]
+
+
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
 BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
 
@@ -306,6 +311,8 @@ EXPORTS = {
     "nan_deficit_repair": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _U32,
                                 ctypes.POINTER(NanRepairOptions), _VP, ctypes.POINTER(_U32), _VP, _VP, _VP, _VP, _VP,
                                 _VP, ctypes.POINTER(_U32), _VP]),
+    "nan_estimate_support": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _U32,
+                                  ctypes.POINTER(NanSupportOptions), _VP, _VP, _VP]),
     "nan_wse_eliminate": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, ctypes.POINTER(NanWseOptions), _VP, _VP,
                                ctypes.POINTER(_U32), _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),

@@ -511,6 +511,36 @@ NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions
                                            ess_after, rounds, as_stream(stream));
 }
 
+NAN_B200_API int nan_estimate_support(NanContext* ctx, const float* reference_positions,
+                                      const float* reference_normals, const uint32_t* reference_instances,
+                                      const float* reference_area_weights, uint32_t reference_count,
+                                      const float* query_positions, const float* query_normals,
+                                      const uint32_t* query_instances, uint32_t query_count,
+                                      const float* instance_radii, uint32_t instance_count,
+                                      const NanSupportOptions* options, float* support_f, float* density_m,
+                                      void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!options || !instance_radii) return invalid("null argument");
+    if (instance_count == 0 || instance_count > 65535u) return invalid("instance_count must be in [1, 65535]");
+    if (reference_count && (!reference_positions || !reference_normals || !reference_instances ||
+                            !reference_area_weights))
+        return invalid("null reference buffer");
+    if (query_count && (!query_positions || !query_normals || !query_instances || !support_f || !density_m))
+        return invalid("null query buffer");
+    if (!std::isfinite(options->normal_cosine_threshold) || options->normal_cosine_threshold < -1.0f ||
+        options->normal_cosine_threshold > 1.0f || !std::isfinite(options->weight_epsilon) ||
+        options->weight_epsilon < 0.0f || !std::isfinite(options->max_density_multiplier))
+        return invalid("invalid support options");
+    for (uint32_t k = 0; k < instance_count; ++k)
+        if (!std::isfinite(instance_radii[k]) || !(instance_radii[k] > 0.0f))
+            return invalid("instance radii must be positive and finite");
+    return nan_host::launch_estimate_support(ctx, reference_positions, reference_normals, reference_instances,
+                                             reference_area_weights, reference_count, query_positions,
+                                             query_normals, query_instances, query_count, instance_radii,
+                                             instance_count, options, support_f, density_m, as_stream(stream));
+}
+
 NAN_B200_API int nan_pack_rgb9e5(NanContext* ctx, const uint8_t* slots, uint32_t* out, uint32_t count, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;

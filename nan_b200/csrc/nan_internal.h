@@ -172,6 +172,11 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
                          uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
                          const NanWseOptions* opt, uint8_t* keep, float* poisson_radii, uint32_t* rounds_out,
                          cudaStream_t st);
+int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* ref_nrm, const uint32_t* ref_inst,
+                            const float* area_weights, uint32_t ref_count, const float* query_pos,
+                            const float* query_nrm, const uint32_t* query_inst, uint32_t query_count,
+                            const float* radii, uint32_t instance_count, const NanSupportOptions* opt,
+                            float* support_f, float* density_m, cudaStream_t st);
 int launch_deficit_repair(NanContext* ctx, const float* const* base, const uint32_t* base_instances, uint32_t base_count,
                           const float* const* cand, const uint32_t* cand_instances, uint32_t cand_count,
                           const float* const* audit, const uint32_t* audit_instances, uint32_t audit_count,

@@ -551,6 +551,81 @@ __global__ void k_rep_count_chosen(uint32_t n, const uint8_t* chosen, unsigned i
     if ((threadIdx.x & 31u) == 0u && b) atomicAdd(total, (unsigned int)__popc(b));
 }
 
+// ---------------------------------------------------------------------------
+// Support estimate (estimate_support_python, surface_probe_sampler.py:
+// 1179-1260): per query site, support = sum over the reference points of its
+// instance within R (normal past the hard gate) of kernel x area weight, the
+// kernel as the gather's with values at or below epsilon set to 0; the sum in
+// float64 over the points in ascending index order with numpy's pairwise
+// scheme; f = clip(support / (pi R^2 / 3), 0, 1), m = min(M, 1 / max(f, 1/M)).
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSupportMaxTerms = 512;
+
+// numpy's split of a pairwise sum above 128 terms, unrolled at compile time
+// (no device recursion, so the stack stays statically sized): each level at
+// least halves the terms up to 8, and four levels cover the 512 terms a query
+// may hold.
+template <int kLevels>
+__device__ __forceinline__ double pairwise_sum_terms(const float* v, uint32_t n) {
+    if (kLevels == 0 || n <= 128u) return pairwise_sum(v, n, false);
+    uint32_t n2 = n / 2u;
+    n2 -= n2 % 8u;
+    return pairwise_sum_terms<kLevels == 0 ? 0 : kLevels - 1>(v, n2) +
+           pairwise_sum_terms<kLevels == 0 ? 0 : kLevels - 1>(v + n2, n - n2);
+}
+
+__global__ void k_support(RepairParams rp, RepairSet query, RepairSet ref, RepairGrid ref_grid,
+                          const float* area_weight, const double* flat_support, double max_density, float* support_f,
+                          float* density_m, int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= query.n) return;
+    const uint32_t k = query.inst[i];
+    const RepairInst ri = rp.inst[k];
+    uint32_t idx[kSupportMaxTerms];
+    float val[kSupportMaxTerms];
+    uint32_t n = 0;
+    bool overflow = false;
+    const float* q = query.pos + 3 * i;
+    const float* qn = query.nrm + 3 * i;
+    int c[3];
+    if (rep_cell(ri, q, c)) {
+        rep_neighbourhood(ref_grid, k, c, [&](uint32_t j) {
+            const float* p = ref.pos + 3 * j;
+            const float* pn = ref.nrm + 3 * j;
+            const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+            const float d2 = (dx * dx + dy * dy) + dz * dz;
+            const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
+            if (!(d2 <= ri.r2) || !(nc >= kRepairHardCos)) return;
+            const float t = ((dx * qn[0] + dy * qn[1]) + dz * qn[2]) / ri.plane_sigma;
+            const float pw = nbd::nan_exp(-0.5f * (t * t));
+            const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
+            const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
+            const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
+            float kw = ((sp * sp) * pw) * soft;
+            kw = kw > rp.eps ? kw : 0.0f;
+            if (n == kSupportMaxTerms) {
+                overflow = true;
+                return;
+            }
+            // keep ascending reference index (insertion)
+            uint32_t at = n++;
+            while (at > 0 && idx[at - 1] > j) {
+                idx[at] = idx[at - 1];
+                val[at] = val[at - 1];
+                --at;
+            }
+            idx[at] = j;
+            val[at] = kw * area_weight[j];
+        });
+    }
+    if (overflow) atomicOr(status, 16);
+    const double support = n ? pairwise_sum_terms<4>(val, n) : 0.0;
+    const double flat = flat_support[k];
+    const double v = fmin(fmax(support / fmax(flat, 1e-30), 0.0), 1.0);
+    support_f[i] = (float)v;
+    density_m[i] = (float)fmin(max_density, 1.0 / fmax(v, 1.0 / max_density));
+}
+
 __global__ void k_rep_deficit(uint32_t n, const uint32_t* counts, uint32_t min_gather, int* deficit) {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a < n) deficit[a] = max((int)min_gather - (int)counts[a], 0);
@@ -899,6 +974,91 @@ int launch_deficit_repair(NanContext* ctx, const float* const* base, const uint3
     *repair_count = take;
     if (rounds_out) *rounds_out = rounds;
     return e == cudaSuccess ? NAN_OK : cuda_fail(e, "deficit repair");
+}
+
+int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* ref_nrm, const uint32_t* ref_inst,
+                            const float* area_weights, uint32_t ref_count, const float* query_pos,
+                            const float* query_nrm, const uint32_t* query_inst, uint32_t query_count,
+                            const float* radii, uint32_t instance_count, const NanSupportOptions* opt,
+                            float* support_f, float* density_m, cudaStream_t st) {
+    std::vector<RepairInst> host_inst(instance_count);
+    std::vector<double> flat(instance_count);
+    for (uint32_t k = 0; k < instance_count; ++k) {
+        const double r = (double)radii[k];
+        host_inst[k].inv_cell = 1.0 / std::max(r, 1e-8);
+        host_inst[k].r2 = radii[k] * radii[k];
+        host_inst[k].plane_sigma = (float)std::max(r * 0.25, 1e-6);
+        host_inst[k].cmin[0] = host_inst[k].cmin[1] = host_inst[k].cmin[2] = 0x7fffffff;
+        flat[k] = 3.141592653589793 * r * r / 3.0;
+    }
+    const double hard = 0.17364817766693041;  // cos(80 degrees)
+    RepairSet R{ref_pos, ref_nrm, ref_inst, ref_count};
+    RepairSet Q{query_pos, query_nrm, query_inst, query_count};
+    std::vector<void*> owned;
+    cudaError_t e = cudaSuccess;
+    auto get = [&](size_t bytes) -> void* {
+        void* p = nullptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) owned.push_back(p);
+        return p;
+    };
+    auto release = [&]() {
+        for (void* p : owned) cudaFreeAsync(p, st);
+        owned.clear();
+    };
+    RepairInst* inst = (RepairInst*)get(instance_count * sizeof(RepairInst));
+    double* flat_dev = (double*)get(instance_count * sizeof(double));
+    int* status = (int*)get(sizeof(int));
+    const uint32_t nmax = std::max(ref_count, 1u);
+    unsigned long long* keys_in = (unsigned long long*)get(nmax * 8ull);
+    uint32_t* idx_in = (uint32_t*)get(nmax * 4ull);
+    unsigned long long* rkeys = (unsigned long long*)get(nmax * 8ull);
+    uint32_t* ridx = (uint32_t*)get(nmax * 4ull);
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_in, rkeys, idx_in, ridx, (int)nmax, 0, 64, st);
+    void* tmp = get(tmp_bytes);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "support scratch");
+    }
+    cudaMemcpyAsync(inst, host_inst.data(), instance_count * sizeof(RepairInst), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(flat_dev, flat.data(), instance_count * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(status, 0, sizeof(int), st);
+    for (const RepairSet* set : {&R, &Q})
+        if (set->n) k_rep_cmin<<<blocks(set->n, 256), 256, 0, st>>>(*set, inst, instance_count, status);
+    if (ref_count) {
+        k_rep_keys<<<blocks(ref_count, 256), 256, 0, st>>>(R, inst, instance_count, keys_in, idx_in, status);
+        cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, rkeys, idx_in, ridx, (int)ref_count, 0, 64, st);
+    }
+    int host_status = 0;
+    cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess || host_status) {
+        release();
+        if (e != cudaSuccess) return cuda_fail(e, "support grid");
+        set_error(host_status & 8 ? "an instance index is out of range"
+                  : host_status & 2 ? "an instance spans more than 65535 kernel radii on an axis"
+                                    : "positions must be finite");
+        return NAN_ERR_INVALID_ARGUMENT;
+    }
+    RepairParams rp{inst, instance_count,
+                    (float)(std::max((double)opt->normal_cosine_threshold, hard + 1e-3) - hard), opt->weight_epsilon,
+                    1u};
+    const RepairGrid RG{rkeys, ridx, ref_count};
+    if (query_count)
+        k_support<<<blocks(query_count, 64), 64, 0, st>>>(rp, Q, R, RG, area_weights, flat_dev,
+                                                          std::max(1.0, (double)opt->max_density_multiplier),
+                                                          support_f, density_m, status);
+    ctx->launches += 4;
+    cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    release();
+    if (e != cudaSuccess) return cuda_fail(e, "support estimate");
+    if (host_status & 16) {
+        set_error("a query site reaches more than 512 reference points");
+        return NAN_ERR_LIMIT;
+    }
+    return NAN_OK;
 }
 
 }  // namespace nan_host

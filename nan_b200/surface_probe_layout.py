@@ -20,8 +20,10 @@ from_sites takes any sites (e.g. scenes.surface_sites). The kernel radius
 follows the reference's rule max(2.5 * sqrt(area / sites), 2.5 * Poisson
 radius, 2.5 * sqrt(total area / total sites), 1e-5), fixed before the
 deficit repair adds up to 30 % more sites where audit points gather fewer
-than 4 (surface_probes.py:2380-2420). The protected closure and support
-estimation are not applied (support 1).
+than 4 (surface_probes.py:2380-2420), and each site's support f
+(estimate_surface_support against the candidate population, area /
+candidates each, surface_probes.py:2586-2604) goes into its record. The
+protected closure is not applied.
 """
 
 from __future__ import annotations
@@ -263,6 +265,8 @@ class SurfaceProbeSiteLayout:
         global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale, 1e-5)
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
+        flat = lambda sets, j: np.concatenate([x[j] for x in sets])
+        inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
         if budget > 0:
             audits, repairs = [], []
             for i, (t, a) in enumerate(zip(tris, areas)):
@@ -273,8 +277,6 @@ class SurfaceProbeSiteLayout:
                 audits.append(audit)
                 rest = _take(cands[i], np.flatnonzero(~keep[offsets[i]:offsets[i + 1]]))
                 repairs.append(_concat([rest, audit]))
-            flat = lambda sets, j: np.concatenate([x[j] for x in sets])
-            inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
             result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
                                             flat(repairs, 1), inst_of(repairs), flat(audits, 0), flat(audits, 1),
                                             inst_of(audits), kernels, min_gather_count=repair_min_gather,
@@ -293,13 +295,22 @@ class SurfaceProbeSiteLayout:
                                audits_below_min_after=int((result.counts_after < repair_min_gather).sum()),
                                repair_rounds=int(result.rounds))
         t3 = time.perf_counter()
+        # support f of every site against the candidate population (area / candidates each)
+        ref_area = np.concatenate([np.full(c[0].shape[0], totals[i] / max(c[0].shape[0], 1), np.float32)
+                                   for i, c in enumerate(cands)])
+        support, density = sampler.estimate_support(flat(cands, 0), flat(cands, 1), inst_of(cands), ref_area,
+                                                    flat(sites, 0), flat(sites, 1), inst_of(sites), kernels,
+                                                    normal_cosine_threshold=math.cos(math.radians(normal_angle_degrees)),
+                                                    max_density_multiplier=kwargs.get("max_density_multiplier", 8.0))
+        starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sites])])
+        t4 = time.perf_counter()
         records = []
         for i, (pos, nrm, tri, b1, b2) in enumerate(sites):
             for side in range(2 if double_sided[i] else 1):
                 r = np.zeros(pos.shape[0], dtype=SURFACE_PROBE_DTYPE)
                 r["position_radius"][:, :3] = pos
                 r["normal_side"][:, :3] = nrm * (-1.0 if side else 1.0)
-                r["normal_side"][:, 3] = 1.0
+                r["normal_side"][:, 3] = support[starts[i]:starts[i + 1]]
                 r["meta"][:, 0] = tri
                 r["meta"][:, 1] = b1.view(np.uint32)
                 r["meta"][:, 2] = b2.view(np.uint32)
@@ -308,9 +319,12 @@ class SurfaceProbeSiteLayout:
         layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees, **kwargs)
         if profile is not None:
-            profile.update(candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2,
-                           packing_s=time.perf_counter() - t3, candidates=int(offsets[-1]),
-                           rounds=int(sampler.last_rounds), base_sites=int(sum(counts)), repair_sites=repaired)
+            profile.update(candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,
+                           packing_s=time.perf_counter() - t4, candidates=int(offsets[-1]),
+                           rounds=int(sampler.last_rounds), base_sites=int(sum(counts)), repair_sites=repaired,
+                           support_p10=float(np.percentile(support, 10)) if support.size else 0.0,
+                           support_p50=float(np.median(support)) if support.size else 0.0,
+                           density_p95=float(np.percentile(density, 95)) if density.size else 0.0)
         return layout
 
     @classmethod

@@ -9,6 +9,10 @@ points gather fewer than min_gather_count probes: candidates are chosen one
 at a time by their summed deficit score (highest first, lowest index on
 ties), computed as parallel rounds that give the same choices.
 
+SurfaceProbeSampler.estimate_support gives each site its support f (the
+area-weighted kernel mass of the surface around it, relative to a flat
+disc) and density multiplier m.
+
 SurfaceProbeSampler.eliminate thins many candidate sets in one call (one
 persistent set of launches for all instances of a scene);
 weighted_sample_elimination keeps the reference's single-set signature and
@@ -25,7 +29,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import Context, NanRepairOptions, NanWseOptions, check, lib, ptr, stream_handle
+from ._native import Context, NanRepairOptions, NanSupportOptions, NanWseOptions, check, lib, ptr, stream_handle
 
 WSE_NORMAL_COSINE_THRESHOLD = 0.5
 WSE_PLANE_DISTANCE_SCALE = 0.35
@@ -125,6 +129,33 @@ class SurfaceProbeSampler:
         return DeficitRepairResult(host(selected)[:count.value].astype(np.int64), host(counts[0]).view(np.uint32),
                                    host(counts[1]).view(np.uint32), host(floats[0]), host(floats[1]), host(floats[2]),
                                    host(floats[3]), int(rounds.value))
+
+
+    def estimate_support(self, reference_positions, reference_normals, reference_instances, reference_area_weights,
+                         query_positions, query_normals, query_instances, instance_radii, *,
+                         normal_cosine_threshold: float = 0.5, weight_epsilon: float = 1e-6,
+                         max_density_multiplier: float = 8.0, stream=None):
+        """The reference's estimate_surface_support on the GPU: (support_f,
+        density_m) per query site, host float32 arrays."""
+        import torch
+
+        dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
+        rp, rn, ri = _points(dev, reference_positions, reference_normals, reference_instances, "reference")
+        qp, qn, qi = _points(dev, query_positions, query_normals, query_instances, "query")
+        ra = torch.as_tensor(np.asarray(reference_area_weights, dtype=np.float32).reshape(-1)
+                             if not hasattr(reference_area_weights, "device") else reference_area_weights,
+                             dtype=torch.float32, device=dev).reshape(-1).contiguous()
+        if ra.shape[0] != rp.shape[0]:
+            raise ValueError("reference_area_weights must have one weight per reference point")
+        radii = np.ascontiguousarray(instance_radii, dtype=np.float32).reshape(-1)
+        f = torch.zeros(qp.shape[0], dtype=torch.float32, device=dev)
+        m = torch.zeros(qp.shape[0], dtype=torch.float32, device=dev)
+        opt = NanSupportOptions(float(normal_cosine_threshold), float(weight_epsilon), float(max_density_multiplier),
+                                0.0)
+        check(lib().nan_estimate_support(self.context.handle, ptr(rp), ptr(rn), ptr(ri), ptr(ra), rp.shape[0],
+                                         ptr(qp), ptr(qn), ptr(qi), qp.shape[0], radii.ctypes.data, radii.shape[0],
+                                         ctypes.byref(opt), ptr(f), ptr(m), stream_handle(stream)))
+        return f.cpu().numpy(), m.cpu().numpy()
 
 
 def weighted_sample_elimination(positions, normals, output_count: int, *, surface_area: float,

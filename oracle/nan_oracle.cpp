@@ -2605,9 +2605,66 @@ double numpy_pairwise_sum(const float* v, uint32_t n, bool square) {
     return res;
 }
 
+double numpy_pairwise_terms(const float* v, uint32_t n) {
+    if (n <= 128u) return numpy_pairwise_sum(v, n, false);
+    uint32_t n2 = n / 2u;
+    n2 -= n2 % 8u;
+    return numpy_pairwise_terms(v, n2) + numpy_pairwise_terms(v + n2, n - n2);
+}
+
 }  // namespace
 
 extern "C" {
+
+// Support estimate, estimate_support_python (surface_probe_sampler.py:
+// 1179-1260), brute force per query over the reference points of its
+// instance in index order.
+int oracle_estimate_support(const float* ref_p, const float* ref_n, const uint32_t* ref_i, const float* area,
+                            uint32_t ref_count, const float* q_p, const float* q_n, const uint32_t* q_i,
+                            uint32_t q_count, const float* radii, uint32_t instance_count,
+                            float normal_cosine_threshold, float eps, float max_density, float* support_f,
+                            float* density_m) {
+    const double hard = 0.17364817766693041;
+    const float hard_f = 0.17364818f;
+    const float span = (float)(std::max((double)normal_cosine_threshold, hard + 1e-3) - hard);
+    const double m = std::max(1.0, (double)max_density);
+    for (uint32_t i = 0; i < q_count; ++i)
+        if (q_i[i] >= instance_count) return 8;
+    for (uint32_t j = 0; j < ref_count; ++j)
+        if (ref_i[j] >= instance_count) return 8;
+    parallel_for((int)q_count, 0, [&](int qi, int) {
+        const uint32_t k = q_i[qi];
+        const float r2 = radii[k] * radii[k];
+        const float sigma = (float)std::max((double)radii[k] * 0.25, 1e-6);
+        const float* q = q_p + 3 * (size_t)qi;
+        const float* qn = q_n + 3 * (size_t)qi;
+        std::vector<float> terms;
+        for (uint32_t j = 0; j < ref_count; ++j) {
+            if (ref_i[j] != k) continue;
+            const float* p = ref_p + 3 * (size_t)j;
+            const float* pn = ref_n + 3 * (size_t)j;
+            const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+            const float d2 = (dx * dx + dy * dy) + dz * dz;
+            const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
+            if (!(d2 <= r2) || !(nc >= hard_f)) continue;
+            const float t = ((dx * qn[0] + dy * qn[1]) + dz * qn[2]) / sigma;
+            const float pw = spec_exp(-0.5f * (t * t));
+            const float sp = std::fmax(1.0f - d2 / r2, 0.0f);
+            const float g = std::fmin(std::fmax((nc - hard_f) / span, 0.0f), 1.0f);
+            const float soft = ((g * g) * (3.0f - 2.0f * g)) * std::fmax(nc, 0.0f);
+            float kw = ((sp * sp) * pw) * soft;
+            kw = kw > eps ? kw : 0.0f;
+            terms.push_back(kw * area[j]);
+        }
+        const double support = terms.empty() ? 0.0 : numpy_pairwise_terms(terms.data(), (uint32_t)terms.size());
+        const double rr = (double)radii[k];
+        const double flat = 3.141592653589793 * rr * rr / 3.0;
+        const double v = std::fmin(std::fmax(support / std::fmax(flat, 1e-30), 0.0), 1.0);
+        support_f[qi] = (float)v;
+        density_m[qi] = (float)std::fmin(m, 1.0 / std::fmax(v, 1.0 / m));
+    });
+    return 0;
+}
 
 int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32_t* base_i, uint32_t base_count,
                           const float* cand_p, const float* cand_n, const uint32_t* cand_i, uint32_t cand_count,

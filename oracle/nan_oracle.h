@@ -195,6 +195,15 @@ int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32
                           uint32_t* counts_before, uint32_t* counts_after, float* sums_before, float* sums_after,
                           float* ess_before, float* ess_after);
 
+/* Support estimate (estimate_support_python, surface_probe_sampler.py:
+ * 1179-1260) with the float32 kernel of the GPU version; returns 8 when an
+ * instance index is out of range. */
+int oracle_estimate_support(const float* ref_p, const float* ref_n, const uint32_t* ref_i, const float* area,
+                            uint32_t ref_count, const float* q_p, const float* q_n, const uint32_t* q_i,
+                            uint32_t q_count, const float* radii, uint32_t instance_count,
+                            float normal_cosine_threshold, float eps, float max_density, float* support_f,
+                            float* density_m);
+
 /* e^x and log2 x of the kernels' own float implementations (nan_exp,
  * nan_log2), for tests against the C library. */
 float own_exp(float x);

@@ -134,6 +134,8 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_wse_eliminate.argtypes = [vp, vp, vp, u32, vp, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, i]
     l.oracle_deficit_repair.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, u32, u32,
                                         ctypes.c_float, ctypes.c_float, vp, vp, vp, vp, vp, vp, vp, vp]
+    l.oracle_estimate_support.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, ctypes.c_float,
+                                          ctypes.c_float, ctypes.c_float, vp, vp]
     l.own_exp.argtypes = [ctypes.c_float]
     l.own_exp.restype = ctypes.c_float
     l.own_log2.argtypes = [ctypes.c_float]
@@ -214,6 +216,28 @@ def deficit_repair(base_positions, base_normals, base_instances, candidate_posit
         raise RuntimeError("deficit repair: an audit names an instance out of range")
     out["selected"] = sel[:count.value].astype(np.int64)
     return out
+
+
+def estimate_support(reference_positions, reference_normals, reference_instances, reference_area_weights,
+                     query_positions, query_normals, query_instances, instance_radii, *, normal_cosine_threshold=0.5,
+                     weight_epsilon=1e-6, max_density_multiplier=8.0):
+    """Support f and density m per query site (float32 each)."""
+    rp = np.ascontiguousarray(reference_positions, dtype=np.float32).reshape(-1, 3)
+    rn = np.ascontiguousarray(reference_normals, dtype=np.float32).reshape(-1, 3)
+    ri = np.ascontiguousarray(reference_instances, dtype=np.uint32).reshape(-1)
+    ra = np.ascontiguousarray(reference_area_weights, dtype=np.float32).reshape(-1)
+    qp = np.ascontiguousarray(query_positions, dtype=np.float32).reshape(-1, 3)
+    qn = np.ascontiguousarray(query_normals, dtype=np.float32).reshape(-1, 3)
+    qi = np.ascontiguousarray(query_instances, dtype=np.uint32).reshape(-1)
+    radii = np.ascontiguousarray(instance_radii, dtype=np.float32).reshape(-1)
+    f = np.zeros(qp.shape[0], np.float32)
+    m = np.zeros(qp.shape[0], np.float32)
+    rc = lib().oracle_estimate_support(_p(rp), _p(rn), _p(ri), _p(ra), rp.shape[0], _p(qp), _p(qn), _p(qi),
+                                       qp.shape[0], _p(radii), radii.shape[0], float(normal_cosine_threshold),
+                                       float(weight_epsilon), float(max_density_multiplier), _p(f), _p(m))
+    if rc != 0:
+        raise RuntimeError("support estimate: an instance index is out of range")
+    return f, m
 
 
 def own_exp(x: float) -> float:

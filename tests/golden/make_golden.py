@@ -11,8 +11,9 @@ of ``test_mesh_colors_rgb9e5.py:15-50``, the hemi-oct encode/decode of
 ``mesh_colors.py:24-79``, the FP64 brute-force any-hit caster of
 ``vertex_baker/visibility_baker.py:348-402``, the point octree builder and
 query of ``surface_probes.py:1348-1438, 3007-3099``, the Python weighted
-sample elimination of ``surface_probes.py:897-985`` and the Python deficit
-repair of ``surface_probe_sampler.py:990-1103`` -- with the graphics-only modules
+sample elimination of ``surface_probes.py:897-985``, and the Python deficit
+repair and support estimate of ``surface_probe_sampler.py:990-1103,
+1179-1260`` -- with the graphics-only modules
 (slangpy, trimesh, pygltflib, PIL) replaced by inert stand-ins, evaluates them
 on seeded inputs, and writes ``reference_vectors.npz`` next to this file.
 The GPU box never runs this script; tests read the committed ``.npz`` only.
@@ -271,6 +272,32 @@ def main() -> None:
         for name in ("counts_before", "counts_after", "weight_sums_before", "weight_sums_after", "ess_before",
                      "ess_after"):
             out[f"rep{k}_{name}"] = np.asarray(getattr(res, name))
+
+    # Support estimate (the reference's Python form): two instances, one a
+    # tilted sheet so the plane and normal terms are not axis aligned, and
+    # query sites in the interior and at the borders.
+    srng = np.random.default_rng(57)
+    nrm1 = np.float32([0.3, 0.9, 0.2])
+    nrm1 /= np.linalg.norm(nrm1)
+    t1 = np.cross(nrm1, [1.0, 0.0, 0.0])
+    t1 /= np.linalg.norm(t1)
+    b1 = np.cross(nrm1, t1)
+    u = srng.uniform(0.0, 3.0, (2500, 2))
+    ref1 = (5.0 + u[:, :1] * t1 + u[:, 1:] * b1).astype(np.float32)
+    ref0 = np.zeros((2000, 3), np.float32)
+    ref0[:, 0], ref0[:, 2] = srng.uniform(0, 2, 2000), srng.uniform(0, 2, 2000)
+    rp = np.concatenate([ref0, ref1])
+    rn = np.concatenate([np.tile(np.float32([0, 1, 0]), (2000, 1)), np.tile(nrm1.astype(np.float32), (2500, 1))])
+    ri = np.concatenate([np.zeros(2000, np.uint32), np.ones(2500, np.uint32)])
+    ra = np.concatenate([np.full(2000, 4.0 / 2000, np.float32), np.full(2500, 9.0 / 2500, np.float32)])
+    qp = np.concatenate([ref0[:150], ref1[:150]]).copy()
+    qn = np.concatenate([rn[:150], rn[2000:2150]])
+    qi = np.concatenate([np.zeros(150, np.uint32), np.ones(150, np.uint32)])
+    radii = np.float32([0.12, 0.2])
+    res = surface_probe_sampler.estimate_support_python(rp, rn, ri, ra, qp, qn, qi, radii, normal_cosine_threshold=0.5)
+    for name, value in (("rp", rp), ("rn", rn), ("ri", ri), ("ra", ra), ("qp", qp), ("qn", qn), ("qi", qi),
+                        ("radii", radii), ("f", res.support_f), ("m", res.density_m)):
+        out[f"sup_{name}"] = np.asarray(value)
 
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})

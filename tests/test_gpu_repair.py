@@ -73,3 +73,49 @@ def test_repair_matches_oracle_at_scale(device):
     assert gpu.selected_candidate_indices.shape[0] > 100
     _compare(gpu, ref)
     device.check()
+
+
+def test_support_matches_oracle(golden, device):
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+    from oracle.oracle import estimate_support
+
+    g = lambda name: golden[f"sup_{name}"]
+    args = (g("rp"), g("rn"), g("ri"), g("ra"), g("qp"), g("qn"), g("qi"), g("radii"))
+    f, m = SurfaceProbeSampler(device).estimate_support(*args)
+    rf, rm = estimate_support(*args)
+    np.testing.assert_array_equal(f, rf)
+    np.testing.assert_array_equal(m, rm)
+    np.testing.assert_array_equal(f, g("f"))
+
+
+def test_wse_layout_support_in_records(device):
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+
+    node = scenes.terrain_boxes(seed=2, grid=97, boxes=40)
+    prof = {}
+    layout = SurfaceProbeSiteLayout.build_wse(node, 3000, device=device, seed=5, profile=prof)
+    support = layout.probes["normal_side"][:, 3]
+    print("support p10 / p50", prof["support_p10"], prof["support_p50"], "density p95", prof["density_p95"])
+    assert support.min() > 0.0 and support.max() <= 1.0
+    assert prof["support_p10"] < prof["support_p50"]
+
+
+def test_wse_layout_support_flat_interior(device):
+    """On a flat plane a site whose kernel disc lies inside the plane sees the
+    whole flat-disc mass, so its support is near 1; sites at the border see
+    about half of it."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+
+    node = scenes.terrain_boxes(seed=3, grid=81, boxes=0, amplitude=0.0)
+    layout = SurfaceProbeSiteLayout.build_wse(node, 3000, device=device, seed=9)
+    radius = float(layout.instance_infos[0].kernel_radius)
+    pos = layout.probes["position_radius"][:, :3]
+    support = layout.probes["normal_side"][:, 3]
+    half = 0.5 * 0.15 * 80
+    inner = (np.abs(pos[:, 0]) < half - radius) & (np.abs(pos[:, 2]) < half - radius)
+    edge = (np.abs(pos[:, 0]) > half - 0.1 * radius) | (np.abs(pos[:, 2]) > half - 0.1 * radius)
+    assert inner.sum() > 1000 and edge.sum() > 10
+    assert np.median(support[inner]) > 0.9 and np.percentile(support[inner], 10) > 0.6
+    assert np.median(support[edge]) < 0.8

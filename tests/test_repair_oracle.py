@@ -1,8 +1,10 @@
-"""Deficit repair on the oracle (CPU) against the reference's own Python
-deficit_repair_python run on the same inputs (tests/golden): the cases of
+"""Deficit repair and support estimate on the oracle (CPU) against the
+reference's own Python deficit_repair_python and estimate_support_python
+run on the same inputs (tests/golden): the repair cases of
 test_surface_probes.py:436-600 (the budget, the zero-score skip) and a
 seeded two-instance case give the same choices, counts, weight sums and
-effective sample sizes."""
+effective sample sizes; the support estimate gives the same f and m on a
+flat and a tilted instance."""
 
 import numpy as np
 import pytest
@@ -37,3 +39,15 @@ def test_repair_oracle_no_deficit_and_budget_cap(golden):
     r = deficit_repair(g("bp"), g("bn"), g("bi"), g("cp"), g("cn"), g("ci"), g("ap"), g("an"), g("ai"), g("radii"),
                        min_gather_count=4, max_repair_count=1)
     assert r["selected"].shape[0] == 1 and np.any(r["counts_after"] < 4)
+
+
+def test_support_oracle_matches_reference(golden):
+    """The support estimate equals the reference's Python
+    estimate_support_python bit for bit, on a flat and a tilted instance."""
+    from oracle.oracle import estimate_support
+
+    g = lambda name: golden[f"sup_{name}"]
+    f, m = estimate_support(g("rp"), g("rn"), g("ri"), g("ra"), g("qp"), g("qn"), g("qi"), g("radii"))
+    np.testing.assert_array_equal(f, g("f"))
+    np.testing.assert_array_equal(m, g("m"))
+    assert f.min() < 0.6 and f.max() == 1.0  # border sites see less surface than interior ones
