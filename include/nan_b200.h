@@ -420,6 +420,45 @@ NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, cons
                                    const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
                                    float* poisson_radii, uint32_t* rounds, void* stream);
 
+/* The adaptive elimination (_adaptive_weighted_sample_elimination_python,
+ * surface_probes.py:988-1088 and 1126-1166; surface_probe_wse_eliminate_adaptive,
+ * surface_probe_sampler.h:120-223), same arguments plus relative_densities
+ * (device f32[N], finite and positive): candidate i is compared with its
+ * neighbours within its own d_max_i = max(d_max / sqrt(density_i), 1e-6)
+ * (plane limit max(d_max_i x plane_distance_scale, 1e-8)), so dense regions
+ * keep more candidates. poisson_radii gets the base radius
+ * sqrt(area / (2 sqrt(3) output_count)) per set. The reference's
+ * partition_masses only shape its CPU partitioning and have no counterpart. */
+NAN_B200_API int nan_wse_eliminate_adaptive(NanContext* ctx, const float* positions, const float* normals,
+                                            const float* relative_densities, const uint32_t* set_offsets,
+                                            uint32_t set_count, const uint32_t* output_counts,
+                                            const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
+                                            float* poisson_radii, uint32_t* rounds, void* stream);
+
+/* Audit/repair candidate filter (surface_probe_filter_audit_repair_candidates,
+ * surface_probe_sampler.h:120-223; the Python form _deduplicate_audit_candidates
+ * and _exclude_selected_duplicates, surface_probes.py:782-832) for set_count
+ * candidate sets in one call. Candidates (device f32[N][3] positions and
+ * normals, candidate_sets device u32[N] or null for one set) and base sites
+ * (device f32[B][3], base_sets u32[B] or null) with the selected base sites
+ * base_selected_indices (device u32[M]). audit_indices (device u32[N]) gets,
+ * ascending, the candidates kept as audit points: per set and cell
+ * floor(p / audit_cell_sizes[set]) (host f64[S]), in index order, those whose
+ * normal dot with every earlier kept one of the cell stays below
+ * normal_cosine_threshold. repair_indices (device u32[N]) gets, ascending,
+ * the candidates whose (set, position bits, normal bits) match no selected
+ * base site and no lower-indexed candidate. audit_count and repair_count are
+ * host outputs. Allocates scratch on the stream and synchronizes it. */
+NAN_B200_API int nan_filter_audit_repair(NanContext* ctx, const float* candidate_positions,
+                                         const float* candidate_normals, const uint32_t* candidate_sets,
+                                         uint32_t candidate_count, const float* base_positions,
+                                         const float* base_normals, const uint32_t* base_sets, uint32_t base_count,
+                                         const uint32_t* base_selected_indices, uint32_t base_selected_count,
+                                         uint32_t set_count, const double* audit_cell_sizes,
+                                         double normal_cosine_threshold, uint32_t* audit_indices,
+                                         uint32_t* audit_count, uint32_t* repair_indices, uint32_t* repair_count,
+                                         void* stream);
+
 /* Deficit repair (deficit_repair, surface_probes.py:1201-1253;
  * surface_probe_deficit_repair, surface_probe_sampler.h:120-223; the Python
  * form deficit_repair_python, surface_probe_sampler.py:990-1103). Each audit

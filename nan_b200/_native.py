@@ -315,6 +315,10 @@ EXPORTS = {
                                   ctypes.POINTER(NanSupportOptions), _VP, _VP, _VP]),
     "nan_wse_eliminate": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, ctypes.POINTER(NanWseOptions), _VP, _VP,
                                ctypes.POINTER(_U32), _VP]),
+    "nan_wse_eliminate_adaptive": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _VP, _VP, ctypes.POINTER(NanWseOptions), _VP,
+                                        _VP, ctypes.POINTER(_U32), _VP]),
+    "nan_filter_audit_repair": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _VP,
+                                     ctypes.c_double, _VP, ctypes.POINTER(_U32), _VP, ctypes.POINTER(_U32), _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),
     "nan_trace_screen_cached": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
                                      ctypes.POINTER(NanLighting), ctypes.POINTER(NanCachedFrame), _VP]),

@@ -443,10 +443,10 @@ NAN_B200_API int nan_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* l
                                            height, camera, lighting, as_stream(stream));
 }
 
-NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, const float* normals,
-                                   const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
-                                   const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
-                                   float* poisson_radii, uint32_t* rounds, void* stream) {
+static int wse_entry(NanContext* ctx, const float* positions, const float* normals, const float* densities,
+                     const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                     const float* surface_areas, const NanWseOptions* options, uint8_t* keep, float* poisson_radii,
+                     uint32_t* rounds, void* stream) {
     int rc = enter(ctx);
     if (rc) return rc;
     if (!set_offsets || !options || (set_count && (!output_counts || !surface_areas)))
@@ -463,8 +463,58 @@ NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, cons
         return invalid("normal cosine threshold must be in [-1, 1] and plane distance scale positive");
     const uint32_t n = set_offsets[set_count];
     if (n && (!positions || !normals || !keep)) return invalid("null buffer");
-    return nan_host::launch_wse_eliminate(ctx, positions, normals, set_offsets, set_count, output_counts,
+    return nan_host::launch_wse_eliminate(ctx, positions, normals, densities, set_offsets, set_count, output_counts,
                                           surface_areas, options, keep, poisson_radii, rounds, as_stream(stream));
+}
+
+NAN_B200_API int nan_wse_eliminate(NanContext* ctx, const float* positions, const float* normals,
+                                   const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                                   const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
+                                   float* poisson_radii, uint32_t* rounds, void* stream) {
+    return wse_entry(ctx, positions, normals, nullptr, set_offsets, set_count, output_counts, surface_areas, options,
+                     keep, poisson_radii, rounds, stream);
+}
+
+NAN_B200_API int nan_wse_eliminate_adaptive(NanContext* ctx, const float* positions, const float* normals,
+                                            const float* relative_densities, const uint32_t* set_offsets,
+                                            uint32_t set_count, const uint32_t* output_counts,
+                                            const float* surface_areas, const NanWseOptions* options, uint8_t* keep,
+                                            float* poisson_radii, uint32_t* rounds, void* stream) {
+    if (set_offsets && set_count && set_offsets[set_count] && !relative_densities)
+        return invalid("relative densities are required");
+    return wse_entry(ctx, positions, normals, relative_densities, set_offsets, set_count, output_counts,
+                     surface_areas, options, keep, poisson_radii, rounds, stream);
+}
+
+NAN_B200_API int nan_filter_audit_repair(NanContext* ctx, const float* candidate_positions,
+                                         const float* candidate_normals, const uint32_t* candidate_sets,
+                                         uint32_t candidate_count, const float* base_positions,
+                                         const float* base_normals, const uint32_t* base_sets, uint32_t base_count,
+                                         const uint32_t* base_selected_indices, uint32_t base_selected_count,
+                                         uint32_t set_count, const double* audit_cell_sizes,
+                                         double normal_cosine_threshold, uint32_t* audit_indices,
+                                         uint32_t* audit_count, uint32_t* repair_indices, uint32_t* repair_count,
+                                         void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!candidate_positions || !candidate_normals || !base_positions || !base_normals || !audit_indices ||
+        !audit_count || !repair_indices || !repair_count || !audit_cell_sizes)
+        return invalid("surface probe candidate filter received a null pointer");
+    if (candidate_count == 0 || base_count == 0) return invalid("candidate_count and base_count must be positive");
+    if (base_selected_count > 0 && !base_selected_indices)
+        return invalid("base_selected_indices cannot be null when selections exist");
+    if (set_count == 0 || set_count > 65536u) return invalid("set_count must be in 1..65536");
+    if (set_count > 1 && (!candidate_sets || !base_sets)) return invalid("several sets need candidate and base sets");
+    for (uint32_t k = 0; k < set_count; ++k)
+        if (!std::isfinite(audit_cell_sizes[k]) || !(audit_cell_sizes[k] > 0.0))
+            return invalid("invalid candidate filter cell size or normal threshold");
+    if (!std::isfinite(normal_cosine_threshold) || normal_cosine_threshold < -1.0 || normal_cosine_threshold > 1.0)
+        return invalid("invalid candidate filter cell size or normal threshold");
+    if ((uint64_t)candidate_count + base_selected_count > 0x7fffffffull) return invalid("too many entries");
+    return nan_host::launch_filter_audit_repair(
+        ctx, candidate_positions, candidate_normals, candidate_sets, candidate_count, base_positions, base_normals,
+        base_sets, base_count, base_selected_indices, base_selected_count, set_count, audit_cell_sizes,
+        normal_cosine_threshold, audit_indices, audit_count, repair_indices, repair_count, as_stream(stream));
 }
 
 NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions, const float* base_normals,

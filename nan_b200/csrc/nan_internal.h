@@ -168,10 +168,16 @@ int batch_autotune(NanBatch* b, uint32_t spp, uint32_t max_bounces, cudaStream_t
 int launch_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDesc* layout, const void* colors, int packed,
                                float* out, uint32_t w, uint32_t h, const NanCamera* cam, const NanLighting* light,
                                cudaStream_t st);
-int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* normals, const uint32_t* set_offsets,
-                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
-                         const NanWseOptions* opt, uint8_t* keep, float* poisson_radii, uint32_t* rounds_out,
-                         cudaStream_t st);
+int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* normals, const float* densities,
+                         const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                         const float* surface_areas, const NanWseOptions* opt, uint8_t* keep, float* poisson_radii,
+                         uint32_t* rounds_out, cudaStream_t st);
+int launch_filter_audit_repair(NanContext* ctx, const float* cand_pos, const float* cand_nrm, const uint32_t* cand_set,
+                               uint32_t cand_count, const float* base_pos, const float* base_nrm,
+                               const uint32_t* base_set, uint32_t base_count, const uint32_t* base_selected,
+                               uint32_t base_selected_count, uint32_t set_count, const double* cell_sizes,
+                               double ncos, uint32_t* audit_indices, uint32_t* audit_count, uint32_t* repair_indices,
+                               uint32_t* repair_count, cudaStream_t st);
 int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* ref_nrm, const uint32_t* ref_inst,
                             const float* area_weights, uint32_t ref_count, const float* query_pos,
                             const float* query_nrm, const uint32_t* query_inst, uint32_t query_count,

@@ -19,6 +19,14 @@
 // the sequential process sees; the sequential order is then (removal weight
 // descending, index ascending), so the survivors are the last n_out of that
 // order within each set.
+//
+// The adaptive elimination (_adaptive_weighted_sample_elimination_python,
+// surface_probes.py:988-1088; C ABI surface_probe_wse_eliminate_adaptive)
+// gives candidate i its own d_max_i = max(d_max / sqrt(density_i), 1e-6) and
+// plane limit; j contributes to i under i's d_max, so "j is in i's list" is
+// one-sided. The rounds then hold when a removed candidate lowers the
+// candidates whose lists hold it (its out-list, the transposed lists) and a
+// candidate is taken only when it tops both its lists.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -47,7 +55,41 @@ struct WseArgs {
     const WseSet* sets;
     double ncos;
     uint32_t n;
+    const float* density;  // f32[N] relative densities (adaptive) or null
+    double plane_scale;
 };
+
+// Candidate i's d_max and plane limit.
+__device__ __forceinline__ void wse_radius(const WseArgs& a, const WseSet& s, uint32_t i, double* d_max,
+                                           double* plane_limit) {
+    if (!a.density) {
+        *d_max = s.d_max;
+        *plane_limit = s.plane_limit;
+        return;
+    }
+    *d_max = fmax(s.d_max / sqrt((double)a.density[i]), 1e-6);
+    *plane_limit = fmax(*d_max * a.plane_scale, 1e-8);
+}
+
+// Adaptive sets: the smallest density of each set (its largest d_max sizes
+// the cells); densities must be finite and positive.
+__global__ void k_wse_density_min(WseArgs a, unsigned int* min_bits, int* status) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float d = a.density[i];
+    if (!(d > 0.0f) || !(d <= 3.4028235e38f)) {
+        atomicOr(status, 32);
+        return;
+    }
+    atomicMin(min_bits + a.set_of[i], __float_as_uint(d));  // positive floats order as their bits
+}
+
+__global__ void k_wse_set_cells(uint32_t set_count, const unsigned int* min_bits, WseSet* sets) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= set_count || min_bits[k] == 0xffffffffu) return;
+    const double cell = fmax(sets[k].d_max / sqrt((double)__uint_as_float(min_bits[k])), 1e-6);
+    sets[k].inv_cell = 1.0 / fmax(cell, 1e-8);
+}
 
 __device__ __forceinline__ void cell_of(const WseArgs& a, uint32_t i, const WseSet& s, int c[3]) {
     for (int k = 0; k < 3; ++k) c[k] = (int)floor((double)a.pos[3 * i + k] * s.inv_cell);
@@ -103,21 +145,23 @@ __device__ __forceinline__ uint32_t lower_bound_key(const unsigned long long* ke
     return lo;
 }
 
-// Contribution of candidate j to candidate i in 2^-50 units (0: not neighbours).
-__device__ __forceinline__ long long wse_contribution(const WseArgs& a, const WseSet& s, uint32_t i, uint32_t j) {
+// Contribution of candidate j to candidate i in 2^-50 units (0: not
+// neighbours), under i's d_max and plane limit.
+__device__ __forceinline__ long long wse_contribution(const WseArgs& a, double d_max, double plane_limit, uint32_t i,
+                                                      uint32_t j) {
     const double dx = (double)a.pos[3 * j] - (double)a.pos[3 * i];
     const double dy = (double)a.pos[3 * j + 1] - (double)a.pos[3 * i + 1];
     const double dz = (double)a.pos[3 * j + 2] - (double)a.pos[3 * i + 2];
     const double d2 = (dx * dx + dy * dy) + dz * dz;
-    if (!(d2 > 1e-20) || !(d2 < s.d_max * s.d_max)) return 0;
+    if (!(d2 > 1e-20) || !(d2 < d_max * d_max)) return 0;
     const double nix = a.nrm[3 * i], niy = a.nrm[3 * i + 1], niz = a.nrm[3 * i + 2];
     const double njx = a.nrm[3 * j], njy = a.nrm[3 * j + 1], njz = a.nrm[3 * j + 2];
     const double ndot = (njx * nix + njy * niy) + njz * niz;
     if (!(ndot >= a.ncos)) return 0;
     const double pa = fabs((dx * nix + dy * niy) + dz * niz);
     const double pb = fabs((dx * njx + dy * njy) + dz * njz);
-    if (!(pa <= s.plane_limit) || !(pb <= s.plane_limit)) return 0;
-    const double base = fmax(1.0 - sqrt(d2) / s.d_max, 0.0);
+    if (!(pa <= plane_limit) || !(pb <= plane_limit)) return 0;
+    const double base = fmax(1.0 - sqrt(d2) / d_max, 0.0);
     const double b2 = base * base;
     const double b4 = b2 * b2;
     return __double2ll_rn((b4 * b4) * kWseUnit);
@@ -135,6 +179,8 @@ __global__ void k_wse_neighbors(WseArgs a, const unsigned long long* keys, const
     const WseSet s = a.sets[si];
     int c[3];
     cell_of(a, i, s, c);
+    double d_max, plane_limit;
+    wse_radius(a, s, i, &d_max, &plane_limit);
     uint32_t count = 0;
     uint32_t out = kFill ? offsets[i] : 0u;
     long long w = 0;
@@ -151,7 +197,7 @@ __global__ void k_wse_neighbors(WseArgs a, const unsigned long long* keys, const
             for (uint32_t k = lower_bound_key(keys, a.n, lo); k < a.n && keys[k] <= hi; ++k) {
                 const uint32_t j = sorted_idx[k];
                 if (j == i) continue;
-                const long long q = wse_contribution(a, s, i, j);
+                const long long q = wse_contribution(a, d_max, plane_limit, i, j);
                 if (q <= 0) continue;
                 if (kFill) {
                     nbr[out] = j;
@@ -174,8 +220,21 @@ __global__ void k_wse_neighbors(WseArgs a, const unsigned long long* keys, const
     }
 }
 
-__global__ void k_wse_mark(uint32_t n, const uint32_t* offsets, const uint32_t* nbr, const long long* weight,
-                           const uint8_t* active, uint8_t* mark) {
+__device__ __forceinline__ bool wse_tops(uint32_t i, long long wi, const uint32_t* offsets, const uint32_t* nbr,
+                                         const long long* weight, const uint8_t* active) {
+    for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
+        const uint32_t j = nbr[e];
+        if (!active[j]) continue;
+        const long long wj = weight[j];
+        if (!(wi > wj || (wi == wj && i < j))) return false;
+    }
+    return true;
+}
+
+// out_offsets / out_nbr: the transposed lists of the adaptive elimination
+// (null when the relation is symmetric).
+__global__ void k_wse_mark(uint32_t n, const uint32_t* offsets, const uint32_t* nbr, const uint32_t* out_offsets,
+                           const uint32_t* out_nbr, const long long* weight, const uint8_t* active, uint8_t* mark) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!active[i]) {
@@ -183,32 +242,46 @@ __global__ void k_wse_mark(uint32_t n, const uint32_t* offsets, const uint32_t* 
         return;
     }
     const long long wi = weight[i];
-    bool top = true;
-    for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
-        const uint32_t j = nbr[e];
-        if (!active[j]) continue;
-        const long long wj = weight[j];
-        if (!(wi > wj || (wi == wj && i < j))) {
-            top = false;
-            break;
-        }
-    }
+    bool top = wse_tops(i, wi, offsets, nbr, weight, active);
+    if (top && out_offsets) top = wse_tops(i, wi, out_offsets, out_nbr, weight, active);
     mark[i] = top ? 1 : 0;
 }
 
-__global__ void k_wse_remove(uint32_t n, const uint32_t* offsets, const uint32_t* nbr, const long long* contrib,
-                             long long* weight, uint8_t* active, const uint8_t* mark, long long* key,
-                             unsigned int* removed) {
+// A removed candidate lowers every remaining candidate whose list holds it
+// (lose_offsets / lose_nbr / lose_contrib: the lists themselves when the
+// relation is symmetric, else their transpose).
+__global__ void k_wse_remove(uint32_t n, const uint32_t* lose_offsets, const uint32_t* lose_nbr,
+                             const long long* lose_contrib, long long* weight, uint8_t* active, const uint8_t* mark,
+                             long long* key, unsigned int* removed) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !mark[i]) return;
     active[i] = 0;
     key[i] = weight[i];
     atomicAdd(removed, 1u);
+    for (uint32_t e = lose_offsets[i]; e < lose_offsets[i + 1]; ++e) {
+        const uint32_t j = lose_nbr[e];
+        // a candidate related to a removed one is never removed in the same round
+        if (active[j]) atomicAdd(reinterpret_cast<unsigned long long*>(weight + j),
+                                 (unsigned long long)(-lose_contrib[e]));
+    }
+}
+
+__global__ void k_wse_out_degree(uint32_t n, const uint32_t* offsets, const uint32_t* nbr, uint32_t* out_degree) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) atomicAdd(out_degree + nbr[e], 1u);
+}
+
+__global__ void k_wse_out_fill(uint32_t n, const uint32_t* offsets, const uint32_t* nbr, const long long* contrib,
+                               const uint32_t* out_offsets, uint32_t* cursor, uint32_t* out_nbr,
+                               long long* out_contrib) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     for (uint32_t e = offsets[i]; e < offsets[i + 1]; ++e) {
         const uint32_t j = nbr[e];
-        // a neighbour of a removed candidate is never removed in the same round
-        if (active[j]) atomicAdd(reinterpret_cast<unsigned long long*>(weight + j),
-                                 (unsigned long long)(-contrib[e]));
+        const uint32_t at = out_offsets[j] + atomicAdd(cursor + j, 1u);
+        out_nbr[at] = i;
+        out_contrib[at] = contrib[e];
     }
 }
 
@@ -635,10 +708,10 @@ __global__ void k_rep_deficit(uint32_t n, const uint32_t* counts, uint32_t min_g
 
 namespace nan_host {
 
-int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* normals, const uint32_t* set_offsets,
-                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
-                         const NanWseOptions* opt, uint8_t* keep, float* poisson_radii, uint32_t* rounds_out,
-                         cudaStream_t st) {
+int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* normals, const float* densities,
+                         const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                         const float* surface_areas, const NanWseOptions* opt, uint8_t* keep, float* poisson_radii,
+                         uint32_t* rounds_out, cudaStream_t st) {
     const uint32_t n = set_offsets[set_count];
     std::vector<WseSet> host_sets(set_count);
     std::vector<uint32_t> set_of_host(n), begin_host(set_count), elim_host(set_count);
@@ -654,8 +727,9 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
         begin_host[k] = set_offsets[k];
         elim_host[k] = count > out ? count - out : 0u;
         if (poisson_radii)
-            poisson_radii[k] = count == out ? (float)std::sqrt(std::max((double)surface_areas[k], 1e-20) / out)
-                                            : (float)(s.d_max * 0.5);
+            poisson_radii[k] = densities      ? (float)r
+                               : count == out ? (float)std::sqrt(std::max((double)surface_areas[k], 1e-20) / out)
+                                              : (float)(s.d_max * 0.5);
         for (uint32_t i = set_offsets[k]; i < set_offsets[k + 1]; ++i) set_of_host[i] = k;
     }
     if (rounds_out) *rounds_out = 0;
@@ -668,13 +742,16 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     long long *contrib = nullptr, *weight = nullptr, *rkey = nullptr;
     uint8_t *active = nullptr, *mark = nullptr;
     int* status = nullptr;
-    unsigned int* removed = nullptr;
+    unsigned int *removed = nullptr, *min_bits = nullptr;
+    uint32_t *out_offsets = nullptr, *out_nbr = nullptr, *cursor = nullptr;
+    long long* out_contrib = nullptr;
     void* tmp = nullptr;
     auto release = [&]() {
         for (void* p : {(void*)sets, (void*)set_of, (void*)idx, (void*)idx_sorted, (void*)degree, (void*)offsets,
                         (void*)nbr, (void*)set_begin, (void*)set_elim, (void*)set_sorted, (void*)keys,
                         (void*)keys_sorted, (void*)contrib, (void*)weight, (void*)rkey, (void*)active, (void*)mark,
-                        (void*)status, (void*)removed, tmp})
+                        (void*)status, (void*)removed, (void*)min_bits, (void*)out_offsets, (void*)out_nbr,
+                        (void*)cursor, (void*)out_contrib, tmp})
             if (p) cudaFreeAsync(p, st);
     };
     cudaError_t e = cudaSuccess;
@@ -699,6 +776,11 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     ok(alloc(&set_begin, set_count, st));
     ok(alloc(&set_elim, set_count, st));
     ok(alloc(&set_sorted, n, st));
+    if (densities) {
+        ok(alloc(&min_bits, set_count, st));
+        ok(alloc(&out_offsets, n + 1, st));
+        ok(alloc(&cursor, n, st));
+    }
     if (e != cudaSuccess) {
         release();
         return cuda_fail(e, "wse scratch");
@@ -708,8 +790,15 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     ok(cudaMemcpyAsync(set_begin, begin_host.data(), set_count * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     ok(cudaMemcpyAsync(set_elim, elim_host.data(), set_count * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     ok(cudaMemsetAsync(status, 0, sizeof(int), st));
-    WseArgs a{positions, normals, set_of, sets, (double)opt->normal_cosine_threshold, n};
+    WseArgs a{positions, normals, set_of, sets, (double)opt->normal_cosine_threshold, n, densities,
+              (double)opt->plane_distance_scale};
     const uint32_t g = blocks(n, 256);
+    if (densities) {
+        ok(cudaMemsetAsync(min_bits, 0xff, set_count * sizeof(unsigned int), st));
+        k_wse_density_min<<<g, 256, 0, st>>>(a, min_bits, status);
+        k_wse_set_cells<<<blocks(set_count, 128), 128, 0, st>>>(set_count, min_bits, sets);
+        ctx->launches += 2;
+    }
     k_wse_cells<<<g, 256, 0, st>>>(a, sets, status);
     k_wse_keys<<<g, 256, 0, st>>>(a, keys, idx, status);
     ctx->launches += 2;
@@ -719,8 +808,9 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     if (e != cudaSuccess || host_status) {
         release();
         if (e != cudaSuccess) return cuda_fail(e, "wse cells");
-        set_error(host_status & 2 ? "a candidate set spans more than 65535 cells of d_max on an axis"
-                                  : "candidate positions must be finite");
+        set_error(host_status & 32 ? "relative densities must be finite and positive"
+                  : host_status & 2 ? "a candidate set spans more than 65535 cells of d_max on an axis"
+                                    : "candidate positions must be finite");
         return NAN_ERR_INVALID_ARGUMENT;
     }
     // sort candidates by (set, cell)
@@ -761,13 +851,31 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
                                              status);
     ok(cudaMemsetAsync(active, 1, n, st));
     ctx->launches += 2;
+    if (densities) {
+        // transposed lists: who loses weight when a candidate goes
+        ok(cudaMemsetAsync(degree, 0, (n + 1) * sizeof(uint32_t), st));
+        ok(cudaMemsetAsync(cursor, 0, n * sizeof(uint32_t), st));
+        k_wse_out_degree<<<g, 256, 0, st>>>(n, offsets, nbr, degree);
+        cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, degree, out_offsets, (int)(n + 1), st);
+        if (!ok(alloc(&out_nbr, edges, st)) || !ok(alloc(&out_contrib, edges, st))) {
+            release();
+            return cuda_fail(e, "wse transposed lists");
+        }
+        k_wse_out_fill<<<g, 256, 0, st>>>(n, offsets, nbr, contrib, out_offsets, cursor, out_nbr, out_contrib);
+        ctx->launches += 2;
+    }
+    const uint32_t* lose_offsets = densities ? out_offsets : offsets;
+    const uint32_t* lose_nbr = densities ? out_nbr : nbr;
+    const long long* lose_contrib = densities ? out_contrib : contrib;
     // elimination rounds, until every candidate has its removal weight
     uint32_t rounds = 0, done = 0;
     ok(cudaMemsetAsync(removed, 0, sizeof(unsigned int), st));
     while (e == cudaSuccess && done < n) {
         for (int k = 0; k < 8; ++k) {
-            k_wse_mark<<<g, 256, 0, st>>>(n, offsets, nbr, weight, active, mark);
-            k_wse_remove<<<g, 256, 0, st>>>(n, offsets, nbr, contrib, weight, active, mark, rkey, removed);
+            k_wse_mark<<<g, 256, 0, st>>>(n, offsets, nbr, densities ? out_offsets : nullptr,
+                                          densities ? out_nbr : nullptr, weight, active, mark);
+            k_wse_remove<<<g, 256, 0, st>>>(n, lose_offsets, lose_nbr, lose_contrib, weight, active, mark, rkey,
+                                            removed);
             ctx->launches += 2;
             ++rounds;
         }

@@ -13,8 +13,16 @@ SurfaceProbeSampler.estimate_support gives each site its support f (the
 area-weighted kernel mass of the surface around it, relative to a flat
 disc) and density multiplier m.
 
+SurfaceProbeSampler.filter_audit_repair_candidates keeps one audit point per
+cell and normal cone and drops repair candidates that duplicate a selected
+base site or an earlier candidate bit for bit
+(filter_audit_repair_candidates_cpp, surface_probe_sampler.py:721-800).
+
 SurfaceProbeSampler.eliminate thins many candidate sets in one call (one
-persistent set of launches for all instances of a scene);
+persistent set of launches for all instances of a scene); with
+relative_densities it runs the adaptive elimination
+(adaptive_weighted_sample_elimination, surface_probes.py:988-1166), each
+candidate compared within its own d_max / sqrt(density);
 weighted_sample_elimination keeps the reference's single-set signature and
 returns (selected indices ascending, Poisson radius). The elimination is the
 reference's: largest weight first (lowest index on ties), weights
@@ -50,6 +58,14 @@ def _points(dev, positions, normals, instances, name):
 
 
 @dataclass(frozen=True)
+class CandidateFilterResult:
+    """As the reference's CandidateFilterResult (surface_probe_sampler.py:211-215),
+    without its CPU timing profile."""
+    audit_indices: np.ndarray
+    repair_indices: np.ndarray
+
+
+@dataclass(frozen=True)
 class DeficitRepairResult:
     """As the reference's DeficitRepairResult (surface_probe_sampler.py:219-229)."""
     selected_candidate_indices: np.ndarray
@@ -73,15 +89,22 @@ class SurfaceProbeSampler:
 
     def eliminate(self, positions, normals, set_offsets, output_counts, surface_areas, *,
                   normal_cosine_threshold: float = WSE_NORMAL_COSINE_THRESHOLD,
-                  plane_distance_scale: float = WSE_PLANE_DISTANCE_SCALE, stream=None):
+                  plane_distance_scale: float = WSE_PLANE_DISTANCE_SCALE, relative_densities=None, stream=None):
         """positions, normals: float32 [N, 3] (CUDA tensors or arrays), the sets
         contiguous with boundaries set_offsets [S+1]. Returns (keep uint8 CUDA
-        tensor [N], Poisson radius per set)."""
+        tensor [N], Poisson radius per set). relative_densities (float32 [N],
+        finite and positive) selects the adaptive elimination; its Poisson
+        radius is the base one, sqrt(area / (2 sqrt(3) count))."""
         import torch
 
         dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
         pos = torch.as_tensor(positions, dtype=torch.float32, device=dev).reshape(-1, 3).contiguous()
         nrm = torch.as_tensor(normals, dtype=torch.float32, device=dev).reshape(-1, 3).contiguous()
+        dens = None
+        if relative_densities is not None:
+            dens = torch.as_tensor(relative_densities, dtype=torch.float32, device=dev).reshape(-1).contiguous()
+            if dens.shape[0] != pos.shape[0]:
+                raise ValueError("relative_densities must have one value per candidate")
         off = np.ascontiguousarray(set_offsets, dtype=np.uint32).reshape(-1)
         outs = np.ascontiguousarray(output_counts, dtype=np.uint32).reshape(-1)
         areas = np.ascontiguousarray(surface_areas, dtype=np.float32).reshape(-1)
@@ -92,11 +115,60 @@ class SurfaceProbeSampler:
         radii = np.zeros(max(sets, 1), np.float32)
         rounds = ctypes.c_uint32(0)
         opt = NanWseOptions(float(normal_cosine_threshold), float(plane_distance_scale))
-        check(lib().nan_wse_eliminate(self.context.handle, ptr(pos), ptr(nrm), off.ctypes.data, sets,
-                                      outs.ctypes.data, areas.ctypes.data, ctypes.byref(opt), ptr(keep),
-                                      radii.ctypes.data, ctypes.byref(rounds), stream_handle(stream)))
+        if dens is None:
+            check(lib().nan_wse_eliminate(self.context.handle, ptr(pos), ptr(nrm), off.ctypes.data, sets,
+                                          outs.ctypes.data, areas.ctypes.data, ctypes.byref(opt), ptr(keep),
+                                          radii.ctypes.data, ctypes.byref(rounds), stream_handle(stream)))
+        else:
+            check(lib().nan_wse_eliminate_adaptive(self.context.handle, ptr(pos), ptr(nrm), ptr(dens),
+                                                   off.ctypes.data, sets, outs.ctypes.data, areas.ctypes.data,
+                                                   ctypes.byref(opt), ptr(keep), radii.ctypes.data,
+                                                   ctypes.byref(rounds), stream_handle(stream)))
         self.last_rounds = int(rounds.value)
         return keep, radii[:sets]
+
+    def filter_audit_repair_candidates(self, candidate_positions, candidate_normals, base_positions, base_normals,
+                                       base_selected_indices, *, audit_cell_size, normal_cosine_threshold: float,
+                                       candidate_sets=None, base_sets=None, stream=None) -> CandidateFilterResult:
+        """The reference's audit/repair candidate filter on the GPU. One set
+        by default; with candidate_sets and base_sets (per point set
+        indices) audit_cell_size is a per-set sequence. Result indices are
+        host int64 arrays, ascending."""
+        import torch
+
+        dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
+        f3 = lambda a: torch.as_tensor(a if hasattr(a, "device") else np.asarray(a, dtype=np.float32),
+                                       dtype=torch.float32, device=dev).reshape(-1, 3).contiguous()
+        u32 = lambda a: torch.as_tensor(a if hasattr(a, "device") else np.asarray(a, dtype=np.int64).astype(
+            np.uint32).view(np.int32), device=dev).reshape(-1).contiguous()
+        cp, cn, bp, bn = f3(candidate_positions), f3(candidate_normals), f3(base_positions), f3(base_normals)
+        if cn.shape != cp.shape or bn.shape != bp.shape:
+            raise ValueError("normals must match positions")
+        if cp.shape[0] == 0 or bp.shape[0] == 0:
+            raise ValueError("candidate and base arrays must be non-empty")
+        sel = u32(base_selected_indices)
+        cells = np.ascontiguousarray(np.atleast_1d(np.asarray(audit_cell_size, dtype=np.float64)))
+        sets = int(cells.shape[0])
+        cs = bs = None
+        if candidate_sets is not None or base_sets is not None:
+            if candidate_sets is None or base_sets is None:
+                raise ValueError("candidate_sets and base_sets go together")
+            cs, bs = u32(candidate_sets), u32(base_sets)
+            if cs.shape[0] != cp.shape[0] or bs.shape[0] != bp.shape[0]:
+                raise ValueError("set indices must cover every point")
+        elif sets != 1:
+            raise ValueError("several cell sizes need candidate_sets and base_sets")
+        n = cp.shape[0]
+        audit = torch.empty(n, dtype=torch.int32, device=dev)
+        repair = torch.empty(n, dtype=torch.int32, device=dev)
+        na, nr = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        check(lib().nan_filter_audit_repair(self.context.handle, ptr(cp), ptr(cn), ptr(cs) if cs is not None else None,
+                                            n, ptr(bp), ptr(bn), ptr(bs) if bs is not None else None, bp.shape[0],
+                                            ptr(sel) if sel.numel() else None, sel.shape[0], sets, cells.ctypes.data,
+                                            float(normal_cosine_threshold), ptr(audit), ctypes.byref(na), ptr(repair),
+                                            ctypes.byref(nr), stream_handle(stream)))
+        host = lambda t, k: t[:k].cpu().numpy().view(np.uint32).astype(np.int64)
+        return CandidateFilterResult(host(audit, na.value), host(repair, nr.value))
 
     def deficit_repair(self, base_positions, base_normals, base_instances, candidate_positions, candidate_normals,
                        candidate_instances, audit_positions, audit_normals, audit_instances, instance_radii, *,
@@ -156,6 +228,28 @@ class SurfaceProbeSampler:
                                          ptr(qp), ptr(qn), ptr(qi), qp.shape[0], radii.ctypes.data, radii.shape[0],
                                          ctypes.byref(opt), ptr(f), ptr(m), stream_handle(stream)))
         return f.cpu().numpy(), m.cpu().numpy()
+
+
+def adaptive_weighted_sample_elimination(positions, normals, relative_densities, output_count: int, *,
+                                         surface_area: float, partition_masses=None,
+                                         normal_cosine_threshold: float = WSE_NORMAL_COSINE_THRESHOLD,
+                                         plane_distance_scale: float = WSE_PLANE_DISTANCE_SCALE, device=None):
+    """Single-set adaptive form: (selected candidate indices ascending, base
+    Poisson radius). partition_masses only shape the reference's CPU
+    partitioning; they are checked for shape and otherwise unused."""
+    from .scene import Device
+
+    n = int(np.asarray(positions).reshape(-1, 3).shape[0]) if not hasattr(positions, "shape") else int(
+        positions.shape[0])
+    if n == 0:
+        raise ValueError("weighted sample elimination needs at least one candidate")
+    if partition_masses is not None and np.asarray(partition_masses).reshape(-1).shape[0] != n:
+        raise ValueError("partition_masses must have one value per candidate")
+    sampler = SurfaceProbeSampler(device if device is not None else Device(0))
+    keep, radii = sampler.eliminate(positions, normals, [0, n], [max(1, min(int(output_count), n))],
+                                    [float(surface_area)], normal_cosine_threshold=normal_cosine_threshold,
+                                    plane_distance_scale=plane_distance_scale, relative_densities=relative_densities)
+    return np.flatnonzero(keep.cpu().numpy()).astype(np.int64), float(radii[0])
 
 
 def weighted_sample_elimination(positions, normals, output_count: int, *, surface_area: float,

@@ -25,9 +25,12 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <array>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <queue>
+#include <set>
 #include <tuple>
 #include <unordered_map>
 #include <string>
@@ -2500,9 +2503,23 @@ long long wse_contribution(const float* pos, const float* nrm, uint32_t i, uint3
     return std::llrint((b4 * b4) * 1125899906842624.0);
 }
 
-bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, uint32_t out, double d_max,
-             double plane_limit, double ncos, uint8_t* keep, uint32_t* order) {
+// density == nullptr: one d_max for the whole set (weighted_sample_elimination,
+// surface_probes.py:897-985). Otherwise the adaptive elimination
+// (_adaptive_weighted_sample_elimination_python, :988-1088): candidate i has
+// d_max_i = max(d_max / sqrt(density_i), 1e-6) and plane limit
+// max(d_max_i * scale, 1e-8); j contributes to i's weight under i's own d_max,
+// so the neighbour relation is one-sided and the removal of k lowers the
+// weights of the candidates whose lists hold k.
+bool wse_set(const float* pos, const float* nrm, const float* density, uint32_t begin, uint32_t end, uint32_t out,
+             double d_max, double plane_scale, double ncos, uint8_t* keep, uint32_t* order) {
     const uint32_t n = end - begin;
+    std::vector<double> dmax_of(n, d_max), plane_of(n);
+    double cell_size = d_max;
+    for (uint32_t k = 0; k < n; ++k) {
+        if (density) dmax_of[k] = std::max(d_max / std::sqrt((double)density[begin + k]), 1e-6);
+        plane_of[k] = std::max(dmax_of[k] * plane_scale, 1e-8);
+        cell_size = density ? (k ? std::max(cell_size, dmax_of[k]) : dmax_of[k]) : d_max;
+    }
     struct Key {
         long long x, y, z;
         bool operator==(const Key& o) const { return x == o.x && y == o.y && z == o.z; }
@@ -2512,7 +2529,7 @@ bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, u
             return (size_t)(k.x * 73856093LL) ^ (size_t)(k.y * 19349663LL) ^ (size_t)(k.z * 83492791LL);
         }
     };
-    const double inv = 1.0 / std::max(d_max, 1e-8);
+    const double inv = 1.0 / std::max(cell_size, 1e-8);
     std::unordered_map<Key, std::vector<uint32_t>, KeyHash> grid;
     std::vector<Key> cell(n);
     for (uint32_t k = 0; k < n; ++k) {
@@ -2532,7 +2549,7 @@ bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, u
                     if (it == grid.end()) continue;
                     for (uint32_t j : it->second) {
                         if (j == i) continue;
-                        const long long q = wse_contribution(pos, nrm, i, j, d_max, plane_limit, ncos);
+                        const long long q = wse_contribution(pos, nrm, i, j, dmax_of[k], plane_of[k], ncos);
                         if (q <= 0) continue;
                         adj[k].push_back({j - begin, q});
                         w[k] += q;
@@ -2541,6 +2558,14 @@ bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, u
     }
     for (uint32_t k = 0; k < n; ++k)
         if (adj[k].size() > 8000) return false;  // the GPU's bound on integer weights
+    // who loses weight when k goes: the candidates whose lists hold k
+    std::vector<std::vector<std::pair<uint32_t, long long>>> out_adj;
+    if (density) {
+        out_adj.resize(n);
+        for (uint32_t k = 0; k < n; ++k)
+            for (auto [j, q] : adj[k]) out_adj[j].push_back({k, q});
+    }
+    const auto& losers = density ? out_adj : adj;
     std::vector<uint8_t> active(n, 1);
     std::vector<uint32_t> version(n, 0);
     // max-heap on (weight, -index); stale entries are skipped by version
@@ -2556,7 +2581,7 @@ bool wse_set(const float* pos, const float* nrm, uint32_t begin, uint32_t end, u
         --remaining;
         if (order) order[begin + step] = begin + k;
         ++step;
-        for (auto [j, q] : adj[k]) {
+        for (auto [j, q] : losers[k]) {
             if (!active[j]) continue;
             w[j] = std::max<long long>(0, w[j] - q);
             version[j] += 1;
@@ -2615,6 +2640,58 @@ double numpy_pairwise_terms(const float* v, uint32_t n) {
 }  // namespace
 
 extern "C" {
+
+// Audit/repair candidate filter, _deduplicate_audit_candidates and
+// _exclude_selected_duplicates (surface_probes.py:782-832) as the C++ form
+// computes them (surface_probe_sampler.cpp:1736-1997: float normal dot
+// compared with the double threshold), one pass per set in index order.
+int oracle_filter_audit_repair(const float* cp, const float* cn, const uint32_t* cs, uint32_t n, const float* bp,
+                               const float* bn, const uint32_t* bs, uint32_t base_count, const uint32_t* selected,
+                               uint32_t m, uint32_t set_count, const double* cell_sizes, double ncos,
+                               uint32_t* audit, uint32_t* audit_count, uint32_t* repair, uint32_t* repair_count) {
+    using Cell = std::array<long long, 4>;
+    using Exact = std::array<uint32_t, 7>;
+    std::map<Cell, std::vector<uint32_t>> reps;
+    std::set<Exact> occupied;
+    auto exact = [](const float* p, const float* nn, uint32_t set, uint32_t i) {
+        Exact k{};
+        k[0] = set;
+        std::memcpy(k.data() + 1, p + 3 * (size_t)i, 12);
+        std::memcpy(k.data() + 4, nn + 3 * (size_t)i, 12);
+        return k;
+    };
+    for (uint32_t e = 0; e < m; ++e) {
+        if (selected[e] >= base_count) return 1;
+        occupied.insert(exact(bp, bn, bs ? bs[selected[e]] : 0u, selected[e]));
+    }
+    uint32_t na = 0, nr = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t set = cs ? cs[i] : 0u;
+        if (set >= set_count) return 2;
+        const double inv = 1.0 / std::max(cell_sizes[set], 1e-8);
+        Cell c{(long long)set, (long long)std::floor((double)cp[3 * i] * inv),
+               (long long)std::floor((double)cp[3 * i + 1] * inv), (long long)std::floor((double)cp[3 * i + 2] * inv)};
+        auto& list = reps[c];
+        const float* a = cn + 3 * (size_t)i;
+        bool dup = false;
+        for (uint32_t r : list) {
+            const float* b = cn + 3 * (size_t)r;
+            const float d = (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+            if ((double)d >= ncos) {
+                dup = true;
+                break;
+            }
+        }
+        if (!dup) {
+            list.push_back(i);
+            audit[na++] = i;
+        }
+        if (occupied.insert(exact(cp, cn, set, i)).second) repair[nr++] = i;
+    }
+    *audit_count = na;
+    *repair_count = nr;
+    return 0;
+}
 
 // Support estimate, estimate_support_python (surface_probe_sampler.py:
 // 1179-1260), brute force per query over the reference points of its
@@ -2746,10 +2823,10 @@ int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32
     return 0;
 }
 
-int oracle_wse_eliminate(const float* positions, const float* normals, const uint32_t* set_offsets,
-                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
-                         float normal_cosine_threshold, float plane_distance_scale, uint8_t* keep,
-                         float* poisson_radii, uint32_t* order, int threads) {
+int oracle_wse_eliminate(const float* positions, const float* normals, const float* relative_densities,
+                         const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                         const float* surface_areas, float normal_cosine_threshold, float plane_distance_scale,
+                         uint8_t* keep, float* poisson_radii, uint32_t* order, int threads) {
     std::atomic<int> bad{0};
     parallel_for((int)set_count, threads, [&](int k, int) {
         const uint32_t b = set_offsets[k], e = set_offsets[k + 1];
@@ -2758,10 +2835,12 @@ int oracle_wse_eliminate(const float* positions, const float* normals, const uin
         const double area = std::max((double)surface_areas[k], 1e-20);
         const double r = std::sqrt(area / (2.0 * std::sqrt(3.0) * (double)out));
         const double d_max = std::max(2.0 * r, 1e-6);
-        const double plane_limit = std::max(d_max * (double)plane_distance_scale, 1e-8);
-        if (poisson_radii) poisson_radii[k] = count == out ? (float)std::sqrt(area / out) : (float)(d_max * 0.5);
-        if (!wse_set(positions, normals, b, e, out, d_max, plane_limit, (double)normal_cosine_threshold, keep,
-                     order))
+        if (poisson_radii)
+            poisson_radii[k] = relative_densities ? (float)r
+                               : count == out     ? (float)std::sqrt(area / out)
+                                                  : (float)(d_max * 0.5);
+        if (!wse_set(positions, normals, relative_densities, b, e, out, d_max, (double)plane_distance_scale,
+                     (double)normal_cosine_threshold, keep, order))
             bad = 1;
     });
     return bad.load() ? 3 : 0;

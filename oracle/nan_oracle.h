@@ -177,11 +177,13 @@ int oracle_resolve_probes(void* scene, const OracleLighting* lighting, const Ora
  * the survivors, poisson_radii f32[S] gets d_max / 2, order (optional
  * u32[N]) the eliminated candidates of each set in removal order from the
  * set's first slot. Contributions are rounded to 2^-50 units as in
- * nan_wse_eliminate. */
-int oracle_wse_eliminate(const float* positions, const float* normals, const uint32_t* set_offsets,
-                         uint32_t set_count, const uint32_t* output_counts, const float* surface_areas,
-                         float normal_cosine_threshold, float plane_distance_scale, uint8_t* keep,
-                         float* poisson_radii, uint32_t* order, int threads);
+ * nan_wse_eliminate. relative_densities (nullable, f32[N]) selects the
+ * adaptive elimination: per-candidate d_max / sqrt(density), the Poisson
+ * radius the base one. */
+int oracle_wse_eliminate(const float* positions, const float* normals, const float* relative_densities,
+                         const uint32_t* set_offsets, uint32_t set_count, const uint32_t* output_counts,
+                         const float* surface_areas, float normal_cosine_threshold, float plane_distance_scale,
+                         uint8_t* keep, float* poisson_radii, uint32_t* order, int threads);
 
 /* Deficit repair (deficit_repair_python, surface_probe_sampler.py:990-1103),
  * one candidate at a time, with the float32 gather weights of the GPU
@@ -198,6 +200,15 @@ int oracle_deficit_repair(const float* base_p, const float* base_n, const uint32
 /* Support estimate (estimate_support_python, surface_probe_sampler.py:
  * 1179-1260) with the float32 kernel of the GPU version; returns 8 when an
  * instance index is out of range. */
+/* Audit/repair candidate filter (surface_probe_filter_audit_repair_candidates):
+ * audit (u32[N]) the kept audit points, repair (u32[N]) the kept repair
+ * candidates, both ascending. cs / bs per point set indices (nullable: one
+ * set), cell_sizes f64[set_count]. Returns 1 for a selected base index out of
+ * range, 2 for a set index out of range. */
+int oracle_filter_audit_repair(const float* cp, const float* cn, const uint32_t* cs, uint32_t n, const float* bp,
+                               const float* bn, const uint32_t* bs, uint32_t base_count, const uint32_t* selected,
+                               uint32_t m, uint32_t set_count, const double* cell_sizes, double ncos,
+                               uint32_t* audit, uint32_t* audit_count, uint32_t* repair, uint32_t* repair_count);
 int oracle_estimate_support(const float* ref_p, const float* ref_n, const uint32_t* ref_i, const float* area,
                             uint32_t ref_count, const float* q_p, const float* q_n, const uint32_t* q_i,
                             uint32_t q_count, const float* radii, uint32_t instance_count,

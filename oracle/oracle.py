@@ -131,9 +131,12 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_scene_set_area_lights.argtypes = [vp, vp, i, ctypes.c_float]
     l.oracle_resolve_probes.argtypes = [vp, vp, vp, u32, u32, vp, i, vp, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
                                         vp, vp, i, vp]
-    l.oracle_wse_eliminate.argtypes = [vp, vp, vp, u32, vp, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, i]
+    l.oracle_wse_eliminate.argtypes = [vp, vp, vp, vp, u32, vp, vp, ctypes.c_float, ctypes.c_float, vp, vp, vp, i]
     l.oracle_deficit_repair.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, u32, u32,
                                         ctypes.c_float, ctypes.c_float, vp, vp, vp, vp, vp, vp, vp, vp]
+    l.oracle_filter_audit_repair.argtypes = [vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, u32, vp, ctypes.c_double,
+                                             vp, ctypes.POINTER(ctypes.c_uint32), vp,
+                                             ctypes.POINTER(ctypes.c_uint32)]
     l.oracle_estimate_support.argtypes = [vp, vp, vp, vp, u32, vp, vp, vp, u32, vp, u32, ctypes.c_float,
                                           ctypes.c_float, ctypes.c_float, vp, vp]
     l.own_exp.argtypes = [ctypes.c_float]
@@ -167,11 +170,14 @@ def filter_mesh_colors(face_infos, instance_infos, side_infos, adjacency, face_n
 
 
 def wse_eliminate(positions, normals, set_offsets, output_counts, surface_areas, normal_cosine_threshold=0.5,
-                  plane_distance_scale=0.35, threads=0):
+                  plane_distance_scale=0.35, threads=0, relative_densities=None):
     """Sequential weighted sample elimination per contiguous set; returns
     (keep u8[N], poisson radii f32[S], removal order u32[N] per set from its
-    first slot, ~0 past the eliminated ones)."""
+    first slot, ~0 past the eliminated ones). relative_densities (f32[N])
+    selects the adaptive elimination."""
     p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    dens = None if relative_densities is None else np.ascontiguousarray(relative_densities,
+                                                                         dtype=np.float32).reshape(-1)
     nrm = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
     off = np.ascontiguousarray(set_offsets, dtype=np.uint32).reshape(-1)
     outs = np.ascontiguousarray(output_counts, dtype=np.uint32).reshape(-1)
@@ -179,7 +185,8 @@ def wse_eliminate(positions, normals, set_offsets, output_counts, surface_areas,
     keep = np.zeros(p.shape[0], np.uint8)
     radii = np.zeros(outs.shape[0], np.float32)
     order = np.full(p.shape[0], 0xFFFFFFFF, np.uint32)
-    rc = lib().oracle_wse_eliminate(_p(p), _p(nrm), _p(off), outs.shape[0], _p(outs), _p(areas),
+    rc = lib().oracle_wse_eliminate(_p(p), _p(nrm), None if dens is None else _p(dens), _p(off), outs.shape[0],
+                                    _p(outs), _p(areas),
                                     float(normal_cosine_threshold), float(plane_distance_scale), _p(keep),
                                     _p(radii), _p(order), threads)
     if rc != 0:
@@ -216,6 +223,30 @@ def deficit_repair(base_positions, base_normals, base_instances, candidate_posit
         raise RuntimeError("deficit repair: an audit names an instance out of range")
     out["selected"] = sel[:count.value].astype(np.int64)
     return out
+
+
+def filter_audit_repair(candidate_positions, candidate_normals, base_positions, base_normals, base_selected_indices,
+                        *, audit_cell_size, normal_cosine_threshold, candidate_sets=None, base_sets=None):
+    """(audit indices, repair indices), int64 ascending."""
+    cp = np.ascontiguousarray(candidate_positions, dtype=np.float32).reshape(-1, 3)
+    cn = np.ascontiguousarray(candidate_normals, dtype=np.float32).reshape(-1, 3)
+    bp = np.ascontiguousarray(base_positions, dtype=np.float32).reshape(-1, 3)
+    bn = np.ascontiguousarray(base_normals, dtype=np.float32).reshape(-1, 3)
+    sel = np.ascontiguousarray(base_selected_indices, dtype=np.uint32).reshape(-1)
+    cells = np.ascontiguousarray(np.atleast_1d(np.asarray(audit_cell_size, dtype=np.float64)))
+    cs = None if candidate_sets is None else np.ascontiguousarray(candidate_sets, dtype=np.uint32).reshape(-1)
+    bs = None if base_sets is None else np.ascontiguousarray(base_sets, dtype=np.uint32).reshape(-1)
+    audit = np.zeros(max(cp.shape[0], 1), np.uint32)
+    repair = np.zeros(max(cp.shape[0], 1), np.uint32)
+    na, nr = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    rc = lib().oracle_filter_audit_repair(_p(cp), _p(cn), None if cs is None else _p(cs), cp.shape[0], _p(bp), _p(bn),
+                                          None if bs is None else _p(bs), bp.shape[0], _p(sel), sel.shape[0],
+                                          cells.shape[0], _p(cells), float(normal_cosine_threshold), _p(audit),
+                                          ctypes.byref(na), _p(repair), ctypes.byref(nr))
+    if rc:
+        raise ValueError("base_selected_indices contains an invalid index" if rc == 1 else
+                         "a candidate set index is out of range")
+    return audit[:na.value].astype(np.int64), repair[:nr.value].astype(np.int64)
 
 
 def estimate_support(reference_positions, reference_normals, reference_instances, reference_area_weights,

@@ -299,6 +299,81 @@ def main() -> None:
                         ("radii", radii), ("f", res.support_f), ("m", res.density_m)):
         out[f"sup_{name}"] = np.asarray(value)
 
+    # Adaptive weighted sample elimination (the reference's Python form):
+    # random candidates on a plane with a 4:1 density step and jitter, two
+    # facing sheets plus a wall with smoothly varying densities, and the
+    # tie-heavy density grid of test_surface_probes.py:312-377.
+    arng = np.random.default_rng(77)
+    awse_cases = []
+    p = np.zeros((2000, 3), np.float32)
+    p[:, 0], p[:, 2] = arng.uniform(0.0, 1.0, 2000), arng.uniform(0.0, 1.0, 2000)
+    d = (np.where(p[:, 0] < 0.5, 1.6, 0.4) * arng.uniform(0.8, 1.25, 2000)).astype(np.float32)
+    awse_cases.append((p, np.tile(np.float32([0.0, 1.0, 0.0]), (2000, 1)), d, 300, 1.0))
+    m = 3000
+    p = np.zeros((m, 3), np.float32)
+    n = np.zeros((m, 3), np.float32)
+    u = arng.uniform(0.0, 1.0, (m, 2)).astype(np.float32)
+    p[:1000, 0], p[:1000, 2], n[:1000, 1] = u[:1000, 0], u[:1000, 1], 1.0
+    p[1000:2000, 0], p[1000:2000, 2], p[1000:2000, 1], n[1000:2000, 1] = u[1000:2000, 0], u[1000:2000, 1], 0.05, -1.0
+    p[2000:, 1], p[2000:, 2], n[2000:, 0] = u[2000:, 0], u[2000:, 1], 1.0
+    d = (0.5 + 1.5 * u[:, 0] * u[:, 0]).astype(np.float32)
+    awse_cases.append((p, n, d, 500, 3.0))
+    c = np.linspace(0.0, 1.0, 20, dtype=np.float32)
+    gx, gz = np.meshgrid(c, c, indexing="xy")
+    p = np.stack((gx.reshape(-1), np.zeros(gx.size, np.float32), gz.reshape(-1)), axis=1).astype(np.float32)
+    d = np.where(p[:, 0] < 0.5, 1.6, 0.4).astype(np.float32)
+    awse_cases.append((p, np.tile(np.float32([0.0, 1.0, 0.0]), (p.shape[0], 1)), d, 64, 1.0))
+    for k, (pos, nrm, dens, count, area) in enumerate(awse_cases):
+        sel, radius = surface_probes._adaptive_weighted_sample_elimination_python(pos, nrm, dens, count,
+                                                                                  surface_area=area)
+        out[f"awse{k}_positions"] = pos
+        out[f"awse{k}_normals"] = nrm
+        out[f"awse{k}_densities"] = dens
+        out[f"awse{k}_params"] = np.asarray([count, area], np.float64)
+        out[f"awse{k}_selected"] = np.asarray(sel, np.int64)
+        out[f"awse{k}_radius"] = np.asarray([radius], np.float64)
+
+    # Audit/repair candidate filter (the reference's Python form,
+    # _deduplicate_audit_candidates and _exclude_selected_duplicates): the
+    # case of test_surface_probes.py:697-730 and random candidates whose
+    # second half repeats the first, every third base site selected.
+    frng = np.random.default_rng(91)
+    flt_cases = []
+    p = np.float32([[0.0, 0, 0], [0.1, 0, 0], [0.0, 0, 0], [0.2, 0, 0], [1.1, 0, 0]])
+    n = np.float32([[0, 1, 0], [0, 1, 0], [0, 1, 0], [0, -1, 0], [0, 1, 0]])
+    flt_cases.append((p, n, np.uint32([0]), 1.0))
+    p = frng.uniform(-1.0, 1.0, (6000, 3)).astype(np.float32)
+    n = frng.normal(size=(6000, 3)).astype(np.float32)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-20)
+    p[3000:], n[3000:] = p[:3000], n[:3000]
+    flt_cases.append((p, n, np.arange(0, 3000, 3, dtype=np.uint32), 0.05))
+    for k, (pos, nrm, sel, cell) in enumerate(flt_cases):
+        cands = surface_probes._InstanceCandidates(pos, nrm, np.zeros((pos.shape[0], 2), np.float32),
+                                                   np.zeros(pos.shape[0], np.uint32), 1.0)
+        audit = surface_probes._deduplicate_audit_candidates(cands, cell, 0.5)
+        repair = surface_probes._exclude_selected_duplicates(cands, cands, sel.astype(np.int64))
+        # the subsets carry positions; map them back to candidate indices
+        index_of = {}
+        for i in range(pos.shape[0]):
+            index_of.setdefault((pos[i].tobytes(), nrm[i].tobytes()), []).append(i)
+
+        def indices(subset):
+            taken = {}
+            res = []
+            for q in range(subset.positions.shape[0]):
+                key = (subset.positions[q].tobytes(), subset.normals[q].tobytes())
+                j = taken.get(key, 0)
+                res.append(index_of[key][j])
+                taken[key] = j + 1
+            return np.asarray(res, np.int64)
+
+        out[f"flt{k}_positions"] = pos
+        out[f"flt{k}_normals"] = nrm
+        out[f"flt{k}_selected_base"] = sel
+        out[f"flt{k}_cell"] = np.asarray([cell], np.float64)
+        out[f"flt{k}_audit"] = indices(audit)
+        out[f"flt{k}_repair"] = indices(repair)
+
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})
 

@@ -1,7 +1,8 @@
 """Weighted sample elimination on the GPU (parallel rounds) against the
 oracle's one-at-a-time elimination: identical survivors on the reference's
 golden candidate sets, on a batch of 40 uneven sets in one call and on a
-200k-candidate terrain set; and the WSE site layout of the terrain (5x
+200k-candidate terrain set; the adaptive (density-driven) elimination on
+the reference's golden cases and 40 sets with varying densities; and the WSE site layout of the terrain (5x
 oversampling) spaces its sites wider than area-weighted random sites while
 keeping every octree range valid."""
 
@@ -24,6 +25,62 @@ def test_wse_matches_oracle_on_reference_cases(golden, device):
         keep, radii, _ = wse_eliminate(pos, nrm, [0, pos.shape[0]], [int(count)], [area])
         np.testing.assert_array_equal(sel, np.flatnonzero(keep))
         assert radius == float(radii[0])
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_adaptive_matches_oracle_on_reference_cases(golden, device, case):
+    """The adaptive elimination: the oracle's survivors (which are the
+    reference Python's on cases 0 and 1) and the base Poisson radius."""
+    from nan_b200.surface_probe_sampler import adaptive_weighted_sample_elimination
+    from oracle.oracle import wse_eliminate
+
+    g = lambda name: golden[f"awse{case}_{name}"]
+    pos, nrm, dens = g("positions"), g("normals"), g("densities")
+    count, area = g("params")
+    sel, radius = adaptive_weighted_sample_elimination(pos, nrm, dens, int(count), surface_area=float(area),
+                                                       partition_masses=np.ones_like(dens), device=device)
+    keep, radii, _ = wse_eliminate(pos, nrm, [0, pos.shape[0]], [int(count)], [area], relative_densities=dens)
+    np.testing.assert_array_equal(sel, np.flatnonzero(keep))
+    assert radius == float(radii[0])
+    if case < 2:
+        np.testing.assert_array_equal(sel, g("selected"))
+
+
+def test_adaptive_batches_match_oracle(device):
+    """40 uneven sets on terrain + boxes with densities varying 6:1 across
+    each set, one call."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+    from oracle.oracle import wse_eliminate
+
+    node = scenes.terrain_boxes(seed=2, grid=129, boxes=40)
+    pos, nrm, off, outs, areas = _surface_candidates(node, 40.0, seed=9)
+    rng = np.random.default_rng(4)
+    dens = (0.4 + 2.0 * (0.5 + 0.5 * np.sin(pos[:, 0] * 0.7 + pos[:, 2] * 0.3))
+            * rng.uniform(0.9, 1.1, pos.shape[0])).astype(np.float32)
+    sampler = SurfaceProbeSampler(device)
+    t0 = time.perf_counter()
+    keep, radii = sampler.eliminate(pos, nrm, off, outs, areas, relative_densities=dens)
+    keep = keep.cpu().numpy()
+    gpu_s = time.perf_counter() - t0
+    ref, ref_radii, _ = wse_eliminate(pos, nrm, off, outs, areas, relative_densities=dens)
+    print(f"adaptive sets {len(outs)} candidates {pos.shape[0]} rounds {sampler.last_rounds} "
+          f"gpu {gpu_s * 1e3:.1f} ms")
+    np.testing.assert_array_equal(keep, ref)
+    np.testing.assert_array_equal(radii, ref_radii)
+    device.check()
+
+
+def test_adaptive_rejects_bad_densities(device):
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+
+    pos = np.random.default_rng(1).uniform(0, 1, (100, 3)).astype(np.float32)
+    nrm = np.tile(np.float32([0, 1, 0]), (100, 1))
+    dens = np.ones(100, np.float32)
+    dens[17] = 0.0
+    with pytest.raises(Exception, match="densities"):
+        SurfaceProbeSampler(device).eliminate(pos, nrm, [0, 100], [20], [1.0], relative_densities=dens)
+    device.check()
 
 
 def _surface_candidates(node, per_instance_scale, seed):
