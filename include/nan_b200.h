@@ -495,8 +495,10 @@ NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions
  * of its instance within that instance's radius; f = clip(support / (pi R^2
  * / 3), 0, 1) and m = min(M, 1 / max(f, 1 / M)). Reference and query arrays
  * are device memory as in nan_deficit_repair; support_f and density_m are
- * device f32[query_count]. NAN_ERR_LIMIT when a query reaches more than 512
- * reference points. Allocates scratch on the stream and synchronizes it. */
+ * device f32[query_count]. The float64 sum is numpy's for a float32 array:
+ * buffers of 8192 terms, each summed pairwise, the buffer sums added in
+ * order; no cap on the terms of a query. Allocates scratch on the stream and
+ * synchronizes it. */
 NAN_B200_API int nan_estimate_support(NanContext* ctx, const float* reference_positions,
                                       const float* reference_normals, const uint32_t* reference_instances,
                                       const float* reference_area_weights, uint32_t reference_count,

@@ -629,22 +629,151 @@ __global__ void k_rep_count_chosen(uint32_t n, const uint8_t* chosen, unsigned i
 // 1179-1260): per query site, support = sum over the reference points of its
 // instance within R (normal past the hard gate) of kernel x area weight, the
 // kernel as the gather's with values at or below epsilon set to 0; the sum in
-// float64 over the points in ascending index order with numpy's pairwise
-// scheme; f = clip(support / (pi R^2 / 3), 0, 1), m = min(M, 1 / max(f, 1/M)).
+// float64 over the points in ascending index order as numpy forms it for a
+// float32 array summed in float64: the terms in buffers of 8192, each buffer
+// summed by the pairwise scheme, the buffer sums added in order;
+// f = clip(support / (pi R^2 / 3), 0, 1), m = min(M, 1 / max(f, 1/M)).
+//
+// A query's points are the 27 grid cells around it, each an index-sorted
+// run of the sorted grid: one pass counts the terms, a second merges the
+// runs by index and streams the terms into the summation, so no query holds
+// its terms and none is capped.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kSupportMaxTerms = 512;
+constexpr uint32_t kNumpyBuffer = 8192;  // numpy's default ufunc buffer (elements)
 
-// numpy's split of a pairwise sum above 128 terms, unrolled at compile time
-// (no device recursion, so the stack stays statically sized): each level at
-// least halves the terms up to 8, and four levels cover the 512 terms a query
-// may hold.
-template <int kLevels>
-__device__ __forceinline__ double pairwise_sum_terms(const float* v, uint32_t n) {
-    if (kLevels == 0 || n <= 128u) return pairwise_sum(v, n, false);
-    uint32_t n2 = n / 2u;
-    n2 -= n2 % 8u;
-    return pairwise_sum_terms<kLevels == 0 ? 0 : kLevels - 1>(v, n2) +
-           pairwise_sum_terms<kLevels == 0 ? 0 : kLevels - 1>(v + n2, n - n2);
+struct CellRuns {
+    uint32_t b[27], e[27];
+};
+
+__device__ __forceinline__ void support_runs(const RepairGrid& g, uint32_t k, const int c[3], CellRuns& r) {
+    int t = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz, ++t) {
+                const int r0 = c[0] + dx, r1 = c[1] + dy, r2 = c[2] + dz;
+                if (r0 < 0 || r1 < 0 || r2 < 0) {
+                    r.b[t] = r.e[t] = 0;
+                    continue;
+                }
+                const unsigned long long key = ((unsigned long long)k << 48) | ((unsigned long long)r0 << 32) |
+                                               ((unsigned long long)r1 << 16) | (unsigned long long)r2;
+                r.b[t] = lower_bound_key(g.keys, g.n, key);
+                r.e[t] = lower_bound_key(g.keys, g.n, key + 1);
+            }
+}
+
+struct SupportTerm {
+    const RepairParams& rp;
+    const RepairInst& ri;
+    const RepairSet& ref;
+    const float* q;
+    const float* qn;
+    const float* area;
+
+    __device__ __forceinline__ bool valid(uint32_t j, float* d2_out, float* nc_out, float* t_out) const {
+        const float* p = ref.pos + 3 * j;
+        const float* pn = ref.nrm + 3 * j;
+        const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+        const float d2 = (dx * dx + dy * dy) + dz * dz;
+        const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
+        *d2_out = d2;
+        *nc_out = nc;
+        *t_out = ((dx * qn[0] + dy * qn[1]) + dz * qn[2]) / ri.plane_sigma;
+        return d2 <= ri.r2 && nc >= kRepairHardCos;
+    }
+    __device__ __forceinline__ float value(uint32_t j, float d2, float nc, float t) const {
+        const float pw = nbd::nan_exp(-0.5f * (t * t));
+        const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
+        const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
+        const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
+        float kw = ((sp * sp) * pw) * soft;
+        kw = kw > rp.eps ? kw : 0.0f;
+        return kw * area[j];
+    }
+};
+
+// The valid terms of the runs in ascending reference index.
+struct TermStream {
+    const SupportTerm& term;
+    const uint32_t* idx;
+    CellRuns& runs;
+
+    __device__ __forceinline__ double next() {
+        for (;;) {
+            int best = -1;
+            uint32_t best_j = 0xffffffffu;
+            for (int t = 0; t < 27; ++t)
+                if (runs.b[t] < runs.e[t]) {
+                    const uint32_t j = idx[runs.b[t]];
+                    if (j < best_j) {
+                        best_j = j;
+                        best = t;
+                    }
+                }
+            if (best < 0) return 0.0;  // not reached: the count pass found every term
+            ++runs.b[best];
+            float d2, nc, tt;
+            if (term.valid(best_j, &d2, &nc, &tt)) return (double)term.value(best_j, d2, nc, tt);
+        }
+    }
+};
+
+// numpy's pairwise sum of n <= 128 terms: eight running sums, combined
+// pairwise, then the remainder in order (fewer than 8: in order).
+__device__ __forceinline__ double pairwise_leaf(uint32_t n, TermStream& s) {
+    if (n < 8u) {
+        double r = 0.0;
+        for (uint32_t i = 0; i < n; ++i) r += s.next();
+        return r;
+    }
+    double r[8];
+    for (int j = 0; j < 8; ++j) r[j] = s.next();
+    uint32_t i = 8;
+    for (; i < n - (n % 8u); i += 8)
+        for (int j = 0; j < 8; ++j) r[j] += s.next();
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += s.next();
+    return res;
+}
+
+// numpy's pairwise sum of n <= 8192 streamed terms: above 128 terms the left
+// part holds n/2 rounded down to a multiple of 8. Walked with an explicit
+// stack (at most 8 levels for 8192 terms).
+__device__ double pairwise_streamed(uint32_t n, TermStream& s) {
+    uint32_t len[12];
+    uint8_t stage[12];
+    double left[12];
+    int sp = 0;
+    len[0] = n;
+    stage[0] = 0;
+    for (;;) {
+        const uint32_t L = len[sp];
+        if (L > 128u && stage[sp] == 0 && sp < 11) {
+            uint32_t h = L / 2u;
+            h -= h % 8u;
+            stage[sp] = 1;
+            len[sp + 1] = h;
+            stage[sp + 1] = 0;
+            ++sp;
+            continue;
+        }
+        double v = pairwise_leaf(L, s);
+        for (;;) {
+            if (sp == 0) return v;
+            --sp;
+            if (stage[sp] == 1) {
+                uint32_t h = len[sp] / 2u;
+                h -= h % 8u;
+                left[sp] = v;
+                stage[sp] = 2;
+                len[sp + 1] = len[sp] - h;
+                stage[sp + 1] = 0;
+                ++sp;
+                break;
+            }
+            v = left[sp] + v;
+        }
+    }
 }
 
 __global__ void k_support(RepairParams rp, RepairSet query, RepairSet ref, RepairGrid ref_grid,
@@ -654,45 +783,26 @@ __global__ void k_support(RepairParams rp, RepairSet query, RepairSet ref, Repai
     if (i >= query.n) return;
     const uint32_t k = query.inst[i];
     const RepairInst ri = rp.inst[k];
-    uint32_t idx[kSupportMaxTerms];
-    float val[kSupportMaxTerms];
-    uint32_t n = 0;
-    bool overflow = false;
     const float* q = query.pos + 3 * i;
     const float* qn = query.nrm + 3 * i;
+    double support = 0.0;
     int c[3];
     if (rep_cell(ri, q, c)) {
-        rep_neighbourhood(ref_grid, k, c, [&](uint32_t j) {
-            const float* p = ref.pos + 3 * j;
-            const float* pn = ref.nrm + 3 * j;
-            const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
-            const float d2 = (dx * dx + dy * dy) + dz * dz;
-            const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
-            if (!(d2 <= ri.r2) || !(nc >= kRepairHardCos)) return;
-            const float t = ((dx * qn[0] + dy * qn[1]) + dz * qn[2]) / ri.plane_sigma;
-            const float pw = nbd::nan_exp(-0.5f * (t * t));
-            const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
-            const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
-            const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
-            float kw = ((sp * sp) * pw) * soft;
-            kw = kw > rp.eps ? kw : 0.0f;
-            if (n == kSupportMaxTerms) {
-                overflow = true;
-                return;
+        CellRuns runs;
+        support_runs(ref_grid, k, c, runs);
+        const SupportTerm term{rp, ri, ref, q, qn, area_weight};
+        uint32_t n = 0;
+        for (int t = 0; t < 27; ++t)
+            for (uint32_t r = runs.b[t]; r < runs.e[t]; ++r) {
+                float d2, nc, tt;
+                n += term.valid(ref_grid.idx[r], &d2, &nc, &tt) ? 1u : 0u;
             }
-            // keep ascending reference index (insertion)
-            uint32_t at = n++;
-            while (at > 0 && idx[at - 1] > j) {
-                idx[at] = idx[at - 1];
-                val[at] = val[at - 1];
-                --at;
-            }
-            idx[at] = j;
-            val[at] = kw * area_weight[j];
-        });
+        TermStream stream{term, ref_grid.idx, runs};
+        for (uint32_t done = 0; done < n; done += kNumpyBuffer)
+            support = support + pairwise_streamed(min(kNumpyBuffer, n - done), stream);
+    } else {
+        atomicOr(status, 2);
     }
-    if (overflow) atomicOr(status, 16);
-    const double support = n ? pairwise_sum_terms<4>(val, n) : 0.0;
     const double flat = flat_support[k];
     const double v = fmin(fmax(support / fmax(flat, 1e-30), 0.0), 1.0);
     support_f[i] = (float)v;
@@ -1162,9 +1272,9 @@ int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* 
     e = cudaStreamSynchronize(st);
     release();
     if (e != cudaSuccess) return cuda_fail(e, "support estimate");
-    if (host_status & 16) {
-        set_error("a query site reaches more than 512 reference points");
-        return NAN_ERR_LIMIT;
+    if (host_status & 2) {
+        set_error("an instance spans more than 65535 kernel radii on an axis");
+        return NAN_ERR_INVALID_ARGUMENT;
     }
     return NAN_OK;
 }

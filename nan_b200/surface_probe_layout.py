@@ -62,10 +62,12 @@ def allocate_counts(weights, total: int, *, minimum_per_entry: int = 1) -> np.nd
     return out
 
 
-def _surface_points(t, areas, k, rng):
+def _surface_points(t, areas, k, rng, densities=None):
     """k area-weighted points on triangles t (_sample_instance_surface,
-    surface_probes.py:445-497): (positions, face normals, triangle, b1, b2)."""
-    cdf = np.cumsum(areas, dtype=np.float64)
+    surface_probes.py:445-497), area x density weighted when densities are
+    given: (positions, face normals, triangle, b1, b2)."""
+    weights = areas if densities is None else areas * np.asarray(densities, dtype=np.float64)
+    cdf = np.cumsum(weights, dtype=np.float64)
     cdf /= cdf[-1]
     cdf[-1] = 1.0
     choice = np.minimum(np.searchsorted(cdf, rng.random(k), side="right"), t.shape[0] - 1)
@@ -220,13 +222,23 @@ class SurfaceProbeSiteLayout:
     def build_wse(cls, scene_node, target_probe_count: int, *, device=None, oversample_factor: int = 5,
                   seed: int = 1, minimum_per_instance: int = 4, repair_budget_ratio: float = 0.30,
                   repair_min_gather: int = 4, kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
-                  sampler=None, profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
+                  adaptive_wse: bool = True, max_density_multiplier: float = 8.0, sampler=None,
+                  profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
         """Sites by weighted sample elimination of oversampled candidates, then
         deficit repair: audit points (a second surface sample, triangle
         centroids and inset corners per instance) that gather fewer than
         repair_min_gather sites get repair sites from the eliminated candidates
         and the audit points, up to repair_budget_ratio x the target
-        (0 turns the repair off)."""
+        (0 turns the repair off).
+
+        adaptive_wse (the reference's default, surface_probes.py:1706-2000)
+        first measures each triangle's support f at its centroid against a
+        surface sample plus every centroid (radius: the global kernel
+        radius) and gives it the density m = min(M, 1 / max(f, 1/M)); the
+        instance budget then follows area x m, candidates are drawn with
+        probability proportional to area x m, and the elimination is the
+        adaptive one with each candidate's relative density
+        m / (adaptive mass / area)."""
         import time
 
         from .surface_probe_sampler import SurfaceProbeSampler
@@ -244,29 +256,58 @@ class SurfaceProbeSiteLayout:
             double_sided.append(bool(scene_node.materials[mat_id].double_sided))
         totals = np.array([a.sum() for a in areas])
         target = int(target_probe_count)
-        counts = allocate_counts(totals, target, minimum_per_entry=min(minimum_per_instance,
-                                                                      max(1, target // max(len(totals), 1))))
-        cands = [_surface_points(t, a, int(counts[i]) * max(1, int(oversample_factor)),
-                                 np.random.default_rng([int(seed), i])) for i, (t, a) in enumerate(zip(tris, areas))]
-        offsets = np.concatenate([[0], np.cumsum([c[0].shape[0] for c in cands])]).astype(np.int64)
-        t1 = time.perf_counter()
+        minimum = min(minimum_per_instance, max(1, target // max(len(totals), 1)))
+        counts = allocate_counts(totals, target, minimum_per_entry=minimum)
         if sampler is None:
             from .scene import Device
 
             sampler = SurfaceProbeSampler(device if device is not None else Device(0))
+        global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale, 1e-5)
+        ncos = math.cos(math.radians(normal_angle_degrees))
+        flat = lambda sets, j: np.concatenate([x[j] for x in sets])
+        inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
+        tri_density = [None] * len(tris)
+        t_pre = time.perf_counter()
+        if adaptive_wse:
+            refs, ref_w, queries = [], [], []
+            for i, (t, a) in enumerate(zip(tris, areas)):
+                n_ref = min(int(counts[i]) * min(max(1, int(oversample_factor)), 2), 131072)
+                rnd = _surface_points(t, a, max(1, n_ref), np.random.default_rng([int(seed), i, 17]))
+                cen = _centroids(t, t.shape[0], None)
+                refs.append(_concat([rnd, cen]))
+                ref_w.append(np.concatenate([np.full(rnd[0].shape[0], 0.5 * totals[i] / rnd[0].shape[0], np.float32),
+                                             (0.5 * a).astype(np.float32)]))
+                queries.append(cen)
+            _, m = sampler.estimate_support(flat(refs, 0), flat(refs, 1), inst_of(refs), np.concatenate(ref_w),
+                                            flat(queries, 0), flat(queries, 1), inst_of(queries),
+                                            np.full(len(tris), global_kernel, np.float32),
+                                            normal_cosine_threshold=ncos,
+                                            max_density_multiplier=max_density_multiplier)
+            starts = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])])
+            tri_density = [m[starts[i]:starts[i + 1]] for i in range(len(tris))]
+            masses = np.array([float(np.sum(a * d.astype(np.float64))) for a, d in zip(areas, tri_density)])
+            counts = allocate_counts(masses, target, minimum_per_entry=minimum)
+        t_pre_end = time.perf_counter()
+        cands = [_surface_points(t, a, int(counts[i]) * max(1, int(oversample_factor)),
+                                 np.random.default_rng([int(seed), i]), tri_density[i])
+                 for i, (t, a) in enumerate(zip(tris, areas))]
+        offsets = np.concatenate([[0], np.cumsum([c[0].shape[0] for c in cands])]).astype(np.int64)
+        cand_density = None
+        if adaptive_wse:
+            cand_density = np.concatenate([
+                (tri_density[i][c[2]] / max(masses[i] / max(totals[i], 1e-30), 1e-6)).astype(np.float32)
+                for i, c in enumerate(cands)])
+        t1 = time.perf_counter()
         keep, radii = sampler.eliminate(np.concatenate([c[0] for c in cands]), np.concatenate([c[1] for c in cands]),
-                                        offsets, counts, totals)
+                                        offsets, counts, totals, relative_densities=cand_density)
         keep = keep.cpu().numpy().astype(bool)
         t2 = time.perf_counter()
         sites = [_take(c, np.flatnonzero(keep[offsets[i]:offsets[i + 1]])) for i, c in enumerate(cands)]
         repaired = 0
         budget = int(math.floor(target * float(repair_budget_ratio)))
         # kernel radius per instance, fixed before the repair as the reference does
-        global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale, 1e-5)
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
-        flat = lambda sets, j: np.concatenate([x[j] for x in sets])
-        inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
         if budget > 0:
             audits, repairs = [], []
             for i, (t, a) in enumerate(zip(tris, areas)):
@@ -280,8 +321,7 @@ class SurfaceProbeSiteLayout:
             result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
                                             flat(repairs, 1), inst_of(repairs), flat(audits, 0), flat(audits, 1),
                                             inst_of(audits), kernels, min_gather_count=repair_min_gather,
-                                            max_repair_count=budget,
-                                            normal_cosine_threshold=math.cos(math.radians(normal_angle_degrees)))
+                                            max_repair_count=budget, normal_cosine_threshold=ncos)
             chosen = np.sort(result.selected_candidate_indices)
             repair_inst = inst_of(repairs)[chosen]
             repair_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in repairs])])
@@ -295,13 +335,20 @@ class SurfaceProbeSiteLayout:
                                audits_below_min_after=int((result.counts_after < repair_min_gather).sum()),
                                repair_rounds=int(result.rounds))
         t3 = time.perf_counter()
-        # support f of every site against the candidate population (area / candidates each)
-        ref_area = np.concatenate([np.full(c[0].shape[0], totals[i] / max(c[0].shape[0], 1), np.float32)
-                                   for i, c in enumerate(cands)])
-        support, density = sampler.estimate_support(flat(cands, 0), flat(cands, 1), inst_of(cands), ref_area,
-                                                    flat(sites, 0), flat(sites, 1), inst_of(sites), kernels,
-                                                    normal_cosine_threshold=math.cos(math.radians(normal_angle_degrees)),
-                                                    max_density_multiplier=kwargs.get("max_density_multiplier", 8.0))
+        # support f of every site against the candidate population: area /
+        # candidates each, or, for density-drawn candidates, area x
+        # (1 / density) normalised to the instance area
+        ref_area = []
+        for i, c in enumerate(cands):
+            if adaptive_wse:
+                w = 1.0 / np.maximum(tri_density[i][c[2]].astype(np.float64), 1e-12)
+                ref_area.append((w * (totals[i] / max(float(w.sum()), 1e-30))).astype(np.float32))
+            else:
+                ref_area.append(np.full(c[0].shape[0], totals[i] / max(c[0].shape[0], 1), np.float32))
+        support, density = sampler.estimate_support(flat(cands, 0), flat(cands, 1), inst_of(cands),
+                                                    np.concatenate(ref_area), flat(sites, 0), flat(sites, 1),
+                                                    inst_of(sites), kernels, normal_cosine_threshold=ncos,
+                                                    max_density_multiplier=max_density_multiplier)
         starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sites])])
         t4 = time.perf_counter()
         records = []
@@ -317,9 +364,11 @@ class SurfaceProbeSiteLayout:
                 r["meta"][:, 3] = (1 if side else 0) | (i << SURFACE_PROBE_INSTANCE_SHIFT)
                 records.append(r)
         layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
-                                normal_angle_degrees=normal_angle_degrees, **kwargs)
+                                normal_angle_degrees=normal_angle_degrees,
+                                max_density_multiplier=max_density_multiplier, **kwargs)
         if profile is not None:
-            profile.update(candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,
+            profile.update(density_prepass_s=t_pre_end - t_pre, adaptive=bool(adaptive_wse),
+                           candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,
                            packing_s=time.perf_counter() - t4, candidates=int(offsets[-1]),
                            rounds=int(sampler.last_rounds), base_sites=int(sum(counts)), repair_sites=repaired,
                            support_p10=float(np.percentile(support, 10)) if support.size else 0.0,

@@ -2637,6 +2637,15 @@ double numpy_pairwise_terms(const float* v, uint32_t n) {
     return numpy_pairwise_terms(v, n2) + numpy_pairwise_terms(v + n2, n - n2);
 }
 
+// np.sum(float32 array, dtype=float64): the cast runs through numpy's ufunc
+// buffers of 8192 elements; each buffer is summed pairwise and the buffer
+// sums are added in order.
+double numpy_f32_sum_f64(const float* v, uint32_t n) {
+    double total = 0.0;
+    for (uint32_t s = 0; s < n; s += 8192u) total = total + numpy_pairwise_terms(v + s, std::min(8192u, n - s));
+    return total;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2733,7 +2742,7 @@ int oracle_estimate_support(const float* ref_p, const float* ref_n, const uint32
             kw = kw > eps ? kw : 0.0f;
             terms.push_back(kw * area[j]);
         }
-        const double support = terms.empty() ? 0.0 : numpy_pairwise_terms(terms.data(), (uint32_t)terms.size());
+        const double support = numpy_f32_sum_f64(terms.data(), (uint32_t)terms.size());
         const double rr = (double)radii[k];
         const double flat = 3.141592653589793 * rr * rr / 3.0;
         const double v = std::fmin(std::fmax(support / std::fmax(flat, 1e-30), 0.0), 1.0);

@@ -298,6 +298,19 @@ def main() -> None:
     for name, value in (("rp", rp), ("rn", rn), ("ri", ri), ("ra", ra), ("qp", qp), ("qn", qn), ("qi", qi),
                         ("radii", radii), ("f", res.support_f), ("m", res.density_m)):
         out[f"sup_{name}"] = np.asarray(value)
+    # a dense case: 30000 reference points, radius 0.6, so each query sums
+    # 10^4 to 2.5 x 10^4 terms (several of numpy's 8192-element buffers)
+    u = srng.uniform(0.0, 1.0, (30000, 2)).astype(np.float32)
+    rp = np.stack([u[:, 0], 0.02 * np.sin(7.0 * u[:, 1]), u[:, 1]], axis=1).astype(np.float32)
+    rn = np.tile(np.float32([0, 1, 0]), (30000, 1))
+    ri = np.zeros(30000, np.uint32)
+    ra = (srng.uniform(0.5, 1.5, 30000) / 30000).astype(np.float32)
+    qp, qn, qi = rp[:24].copy(), rn[:24].copy(), ri[:24].copy()
+    radii = np.float32([0.6])
+    res = surface_probe_sampler.estimate_support_python(rp, rn, ri, ra, qp, qn, qi, radii, normal_cosine_threshold=0.5)
+    for name, value in (("rp", rp), ("rn", rn), ("ri", ri), ("ra", ra), ("qp", qp), ("qn", qn), ("qi", qi),
+                        ("radii", radii), ("f", res.support_f), ("m", res.density_m)):
+        out[f"supd_{name}"] = np.asarray(value)
 
     # Adaptive weighted sample elimination (the reference's Python form):
     # random candidates on a plane with a 4:1 density step and jitter, two

@@ -88,6 +88,19 @@ def test_support_matches_oracle(golden, device):
     np.testing.assert_array_equal(f, g("f"))
 
 
+def test_support_dense_matches_golden(golden, device):
+    """No cap on the terms of a query: 10^4 to 2.5 x 10^4 per site, summed in
+    numpy's buffered pairwise order, equal to the reference's Python form."""
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+
+    g = lambda name: golden[f"supd_{name}"]
+    args = (g("rp"), g("rn"), g("ri"), g("ra"), g("qp"), g("qn"), g("qi"), g("radii"))
+    f, m = SurfaceProbeSampler(device).estimate_support(*args)
+    np.testing.assert_array_equal(f, g("f"))
+    np.testing.assert_array_equal(m, g("m"))
+    device.check()
+
+
 def test_wse_layout_support_in_records(device):
     from nan_b200 import scenes
     from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout

@@ -138,7 +138,8 @@ def test_wse_layout_spaces_sites_wider_than_random(device):
 
     node = scenes.terrain_boxes(seed=1, grid=129, boxes=0)
     prof = {}
-    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof, repair_budget_ratio=0.0)
+    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof, repair_budget_ratio=0.0,
+                                           adaptive_wse=False)
     rnd = SurfaceProbeSiteLayout.build(node, 4000, seed=3)
     print("wse layout", prof)
 
@@ -177,3 +178,51 @@ def test_wse_layout_repair_fills_gather_deficits(device):
         if info.probe_count:
             found = layout.query_probe_indices(k, info.root_center, radius=info.root_extent * 4.0)
             assert found.shape[0] == info.probe_count
+
+
+def test_adaptive_layout_reallocates_without_changing_base_budget(device):
+    """test_surface_probes.py:1068-1090 on the reference's demo box: the
+    density prepass moves sites between instances, the base budget stays 80."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+
+    node = scenes.reference_demo()
+    pa, pu = {}, {}
+    adaptive = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_budget_ratio=0.0,
+                                                device=device, profile=pa)
+    uniform = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_budget_ratio=0.0,
+                                               adaptive_wse=False, device=device, profile=pu)
+    assert pa["adaptive"] and not pu["adaptive"]
+    assert pa["base_sites"] == 80 and pu["base_sites"] == 80
+    counts = lambda layout: [info.surface_site_count for info in layout.instance_infos]
+    print("adaptive", counts(adaptive), "uniform", counts(uniform))
+    assert counts(adaptive) != counts(uniform)
+
+
+def test_adaptive_layout_densifies_low_support_surface(device):
+    """Where the kernel disc leaves the surface (the terrain's border, the
+    boxes) support is low and the density multiplier high: the adaptive
+    layout puts a larger share of the sites there than the uniform one."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+
+    node = scenes.terrain_boxes(seed=2, grid=97, boxes=40)
+    kw = dict(device=device, seed=5, repair_budget_ratio=0.0)
+    pa = {}
+    adaptive = SurfaceProbeSiteLayout.build_wse(node, 3000, profile=pa, **kw)
+    uniform = SurfaceProbeSiteLayout.build_wse(node, 3000, adaptive_wse=False, **kw)
+    print("adaptive profile", pa)
+
+    def shares(layout):
+        front = (layout.probes["meta"][:, 3] & 1) == 0
+        inst = layout.probes["meta"][front, 3] >> 8
+        pos = layout.probes["position_radius"][front, :3]
+        half = 0.5 * 0.15 * 96
+        radius = float(layout.instance_infos[0].kernel_radius)
+        on_terrain = inst == 0
+        border = on_terrain & ((np.abs(pos[:, 0]) > half - radius) | (np.abs(pos[:, 2]) > half - radius))
+        return float((~on_terrain).mean()), float(border.sum() / max(on_terrain.sum(), 1))
+
+    (box_a, border_a), (box_u, border_u) = shares(adaptive), shares(uniform)
+    print("box share adaptive / uniform", box_a, box_u, "border share", border_a, border_u)
+    assert box_a > box_u and border_a > border_u
