@@ -34,8 +34,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from .surface_probe_octree import build_point_octree, query_probe_indices
-from .surface_probe_resources import (SURFACE_PROBE_DTYPE, SURFACE_PROBE_INSTANCE_DTYPE,
-                                      SURFACE_PROBE_INSTANCE_SHIFT)
+from .surface_probe_resources import (SURFACE_PROBE_DTYPE, SURFACE_PROBE_FLAG_PROTECTED,
+                                      SURFACE_PROBE_INSTANCE_DTYPE, SURFACE_PROBE_INSTANCE_SHIFT)
 
 
 def allocate_counts(weights, total: int, *, minimum_per_entry: int = 1) -> np.ndarray:
@@ -225,11 +225,14 @@ class SurfaceProbeSiteLayout:
                   adaptive_wse: bool = True, max_density_multiplier: float = 8.0, sampler=None,
                   profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
         """Sites by weighted sample elimination of oversampled candidates, then
-        deficit repair: audit points (a second surface sample, triangle
-        centroids and inset corners per instance) that gather fewer than
-        repair_min_gather sites get repair sites from the eliminated candidates
-        and the audit points, up to repair_budget_ratio x the target
-        (0 turns the repair off).
+        deficit repair: audit points (filtered from inset corners, centroids,
+        the candidates and a second surface sample per instance) that gather
+        fewer than repair_min_gather sites get repair sites from the filtered
+        repair candidates, up to repair_budget_ratio x the target; audit
+        points still short then get their residual deficit as colocated
+        protected sites, without a budget (the protected closure; its sites
+        carry SURFACE_PROBE_FLAG_PROTECTED). repair_min_gather = 0 turns
+        repair and closure off.
 
         adaptive_wse (the reference's default, surface_probes.py:1706-2000)
         first measures each triangle's support f at its centroid against a
@@ -303,21 +306,35 @@ class SurfaceProbeSiteLayout:
         keep = keep.cpu().numpy().astype(bool)
         t2 = time.perf_counter()
         sites = [_take(c, np.flatnonzero(keep[offsets[i]:offsets[i + 1]])) for i, c in enumerate(cands)]
-        repaired = 0
+        flags = [np.zeros(x[0].shape[0], np.uint32) for x in sites]
+        repaired = protected = 0
         budget = int(math.floor(target * float(repair_budget_ratio)))
         # kernel radius per instance, fixed before the repair as the reference does
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
-        if budget > 0:
-            audits, repairs = [], []
+        if repair_min_gather > 0:
+            # audit source per instance (surface_probes.py:2060-2180): inset
+            # corners, centroids, every base candidate and a second surface
+            # sample; the filter keeps one audit point per cell of R/2 and
+            # normal cone, and as repair candidates those that no selected
+            # base site or earlier candidate duplicates bit for bit
+            sources = []
             for i, (t, a) in enumerate(zip(tris, areas)):
                 rng = np.random.default_rng([int(seed), i, 7919])
                 k = int(counts[i])
-                audit = _concat([_surface_points(t, a, k, rng), _centroids(t, max(16, k), rng),
-                                 _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng)])
-                audits.append(audit)
-                rest = _take(cands[i], np.flatnonzero(~keep[offsets[i]:offsets[i + 1]]))
-                repairs.append(_concat([rest, audit]))
+                sources.append(_concat([_inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
+                                        _centroids(t, max(16, k), rng), cands[i], _surface_points(t, a, k, rng)]))
+            src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])
+            base_sel = np.concatenate([np.flatnonzero(keep[offsets[i]:offsets[i + 1]]) + offsets[i]
+                                       for i in range(len(cands))])
+            filt = sampler.filter_audit_repair_candidates(
+                flat(sources, 0), flat(sources, 1), flat(cands, 0), flat(cands, 1), base_sel,
+                audit_cell_size=(kernels.astype(np.float64) * 0.5), normal_cosine_threshold=ncos,
+                candidate_sets=inst_of(sources), base_sets=inst_of(cands))
+            split = lambda idx: [idx[(idx >= src_starts[i]) & (idx < src_starts[i + 1])] - src_starts[i]
+                                 for i in range(len(sources))]
+            audits = [_take(sources[i], ix) for i, ix in enumerate(split(filt.audit_indices))]
+            repairs = [_take(sources[i], ix) for i, ix in enumerate(split(filt.repair_indices))]
             result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
                                             flat(repairs, 1), inst_of(repairs), flat(audits, 0), flat(audits, 1),
                                             inst_of(audits), kernels, min_gather_count=repair_min_gather,
@@ -328,11 +345,40 @@ class SurfaceProbeSiteLayout:
             for i in np.unique(repair_inst):
                 local = chosen[repair_inst == i] - repair_starts[i]
                 sites[i] = _concat([sites[i], _take(repairs[i], local)])
+                flags[i] = np.concatenate([flags[i], np.zeros(local.shape[0], np.uint32)])
             repaired = int(chosen.shape[0])
+            # protected closure (surface_probes.py:2462-2587): every audit point
+            # still short of the gather target offers its residual deficit as
+            # colocated candidates, chosen without a budget
+            deficits = np.maximum(int(repair_min_gather) - result.counts_after.astype(np.int64), 0)
+            short = np.flatnonzero(deficits)
+            closure_after = result.counts_after.copy()
+            if short.size:
+                audit_inst = inst_of(audits)
+                offers = np.repeat(short, deficits[short])
+                prot = tuple(np.concatenate([x[j] for x in audits])[offers] for j in range(5))
+                prot_inst = audit_inst[offers]
+                closure = sampler.deficit_repair(
+                    flat(sites, 0), flat(sites, 1), inst_of(sites), prot[0], prot[1], prot_inst,
+                    flat(audits, 0)[short], flat(audits, 1)[short], audit_inst[short], kernels,
+                    min_gather_count=repair_min_gather, max_repair_count=int(offers.shape[0]),
+                    normal_cosine_threshold=ncos)
+                picked = np.sort(closure.selected_candidate_indices)
+                for i in np.unique(prot_inst[picked]):
+                    local = picked[prot_inst[picked] == i]
+                    sites[i] = _concat([sites[i], tuple(x[local] for x in prot)])
+                    flags[i] = np.concatenate([flags[i], np.full(local.shape[0], SURFACE_PROBE_FLAG_PROTECTED,
+                                                                 np.uint32)])
+                protected = int(picked.shape[0])
+                closure_after[short] = closure.counts_after
             if profile is not None:
-                profile.update(repair_sites=repaired, audits=int(result.counts_before.shape[0]),
+                profile.update(repair_sites=repaired, protected_sites=protected,
+                               audits=int(result.counts_before.shape[0]),
+                               repair_candidates=int(filt.repair_indices.shape[0]),
                                audits_below_min_before=int((result.counts_before < repair_min_gather).sum()),
-                               audits_below_min_after=int((result.counts_after < repair_min_gather).sum()),
+                               audits_below_min_after_repair=int((result.counts_after < repair_min_gather).sum()),
+                               audits_below_min_after=int((closure_after < repair_min_gather).sum()),
+                               zero_gather_after=int((closure_after == 0).sum()),
                                repair_rounds=int(result.rounds))
         t3 = time.perf_counter()
         # support f of every site against the candidate population: area /
@@ -361,7 +407,7 @@ class SurfaceProbeSiteLayout:
                 r["meta"][:, 0] = tri
                 r["meta"][:, 1] = b1.view(np.uint32)
                 r["meta"][:, 2] = b2.view(np.uint32)
-                r["meta"][:, 3] = (1 if side else 0) | (i << SURFACE_PROBE_INSTANCE_SHIFT)
+                r["meta"][:, 3] = (1 if side else 0) | flags[i] | (i << SURFACE_PROBE_INSTANCE_SHIFT)
                 records.append(r)
         layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees,
@@ -371,6 +417,7 @@ class SurfaceProbeSiteLayout:
                            candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,
                            packing_s=time.perf_counter() - t4, candidates=int(offsets[-1]),
                            rounds=int(sampler.last_rounds), base_sites=int(sum(counts)), repair_sites=repaired,
+                           protected_sites=protected,
                            support_p10=float(np.percentile(support, 10)) if support.size else 0.0,
                            support_p50=float(np.median(support)) if support.size else 0.0,
                            density_p95=float(np.percentile(density, 95)) if density.size else 0.0)

@@ -19,6 +19,8 @@ SURFACE_PROBE_INSTANCE_SIZE = 48
 SURFACE_PROBE_RADIAL_DEPTH_DIM = 4
 SURFACE_PROBE_RADIAL_MOMENT_SIZE = SURFACE_PROBE_RADIAL_DEPTH_DIM * SURFACE_PROBE_RADIAL_DEPTH_DIM * 4
 SURFACE_PROBE_FLAG_BACK_SIDE = 1 << 0
+SURFACE_PROBE_FLAG_VERTEX_ANCHOR = 1 << 1
+SURFACE_PROBE_FLAG_PROTECTED = 1 << 2
 SURFACE_PROBE_INSTANCE_SHIFT = 8
 
 SURFACE_PROBE_DTYPE = np.dtype(

@@ -138,7 +138,7 @@ def test_wse_layout_spaces_sites_wider_than_random(device):
 
     node = scenes.terrain_boxes(seed=1, grid=129, boxes=0)
     prof = {}
-    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof, repair_budget_ratio=0.0,
+    wse = SurfaceProbeSiteLayout.build_wse(node, 4000, device=device, seed=3, profile=prof, repair_min_gather=0,
                                            adaptive_wse=False)
     rnd = SurfaceProbeSiteLayout.build(node, 4000, seed=3)
     print("wse layout", prof)
@@ -171,9 +171,10 @@ def test_wse_layout_repair_fills_gather_deficits(device):
     layout = SurfaceProbeSiteLayout.build_wse(node, 3000, device=device, seed=5, profile=prof)
     print("repair", prof)
     assert 0 < prof["repair_sites"] <= 900
-    assert prof["audits_below_min_after"] < prof["audits_below_min_before"]
+    assert prof["audits_below_min_after_repair"] < prof["audits_below_min_before"]
+    assert prof["audits_below_min_after"] == 0 and prof["zero_gather_after"] == 0
     fronts = int(((layout.probes["meta"][:, 3] & 1) == 0).sum())
-    assert fronts == prof["base_sites"] + prof["repair_sites"]
+    assert fronts == prof["base_sites"] + prof["repair_sites"] + prof["protected_sites"]
     for k, info in enumerate(layout.instance_infos):
         if info.probe_count:
             found = layout.query_probe_indices(k, info.root_center, radius=info.root_extent * 4.0)
@@ -188,9 +189,9 @@ def test_adaptive_layout_reallocates_without_changing_base_budget(device):
 
     node = scenes.reference_demo()
     pa, pu = {}, {}
-    adaptive = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_budget_ratio=0.0,
+    adaptive = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_min_gather=0,
                                                 device=device, profile=pa)
-    uniform = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_budget_ratio=0.0,
+    uniform = SurfaceProbeSiteLayout.build_wse(node, 80, oversample_factor=3, seed=7, repair_min_gather=0,
                                                adaptive_wse=False, device=device, profile=pu)
     assert pa["adaptive"] and not pu["adaptive"]
     assert pa["base_sites"] == 80 and pu["base_sites"] == 80
@@ -207,7 +208,7 @@ def test_adaptive_layout_densifies_low_support_surface(device):
     from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
 
     node = scenes.terrain_boxes(seed=2, grid=97, boxes=40)
-    kw = dict(device=device, seed=5, repair_budget_ratio=0.0)
+    kw = dict(device=device, seed=5, repair_min_gather=0)
     pa = {}
     adaptive = SurfaceProbeSiteLayout.build_wse(node, 3000, profile=pa, **kw)
     uniform = SurfaceProbeSiteLayout.build_wse(node, 3000, adaptive_wse=False, **kw)
@@ -226,3 +227,28 @@ def test_adaptive_layout_densifies_low_support_surface(device):
     (box_a, border_a), (box_u, border_u) = shares(adaptive), shares(uniform)
     print("box share adaptive / uniform", box_a, box_u, "border share", border_a, border_u)
     assert box_a > box_u and border_a > border_u
+
+
+def test_protected_closure_eliminates_unbudgeted_gather_deficits(device):
+    """test_surface_probes.py:1001-1032: with no repair budget and a small
+    kernel, audit points stay short after the repair; the closure adds
+    colocated protected sites (at most 4 per short audit point) until none
+    is short, and the build repeats exactly."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_resources import SURFACE_PROBE_FLAG_PROTECTED
+
+    node = scenes.reference_demo()
+    options = dict(oversample_factor=1, seed=7, kernel_radius_scale=0.5, repair_budget_ratio=0.0, device=device)
+    prof = {}
+    layout = SurfaceProbeSiteLayout.build_wse(node, 8, profile=prof, **options)
+    print("closure", prof)
+    assert prof["repair_sites"] == 0
+    assert prof["audits_below_min_after_repair"] > 0
+    assert prof["protected_sites"] > 0
+    assert prof["audits_below_min_after"] == 0 and prof["zero_gather_after"] == 0
+    assert prof["protected_sites"] <= 4 * prof["audits_below_min_after_repair"]
+    protected = (layout.probes["meta"][:, 3] & SURFACE_PROBE_FLAG_PROTECTED) != 0
+    assert protected.any()
+    again = SurfaceProbeSiteLayout.build_wse(node, 8, **options)
+    np.testing.assert_array_equal(again.probes, layout.probes)
