@@ -464,9 +464,10 @@ def run_nan(args):
         line["batched_probes"] = dict(batch_eval.measure(device, count=64, seed=1, samples_per_probe=64,
                                                          max_bounces=3, frames=2),
                                       workload="64 seeded terrain+box scenes, triangles log-uniform 1e3-5e5, "
-                                               "sites U{512..20480} placed by weighted sample elimination of 5x "
-                                               "oversampled candidates, 64 spp, 3 bounces, compensated running "
-                                               "means")
+                                               "site targets U{512..20480} placed as the reference places "
+                                               "them (density prepass, adaptive elimination of 5x oversampled "
+                                               "candidates, 30 % repair, protected closure), 64 spp, 3 bounces, "
+                                               "compensated running means")
     print(json.dumps(line))
 
 

@@ -45,13 +45,14 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     t0 = time.perf_counter()
     items, tris, sites = [], [], []
     sampler = SurfaceProbeSampler(device)
-    placement = {"candidates": 0, "elimination_s": 0.0, "candidates_s": 0.0, "packing_s": 0.0}
+    placement = {"candidates": 0, "base_sites": 0, "repair_sites": 0, "protected_sites": 0, "density_prepass_s": 0.0,
+                 "candidates_s": 0.0, "elimination_s": 0.0, "repair_s": 0.0, "support_s": 0.0, "packing_s": 0.0}
     for i, (node, n_sites) in enumerate(sc.batch_scenes(count, seed, tri_max=tri_max)):
         scene = Scene(device, node)
         prof: dict = {}
         layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=seed + i, profile=prof)
         for k in placement:
-            placement[k] += prof[k]
+            placement[k] += prof.get(k, 0)
         geometry = SurfaceProbeGpuGeometry.create(device, layout)
         baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=samples_per_probe,
                                                    max_bounces=max_bounces, compensated=True)
@@ -132,8 +133,10 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
         "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
         "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
         "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
-        "setup_s": setup_s, "site_placement": dict(placement, method="weighted sample elimination on the GPU, "
-                                                                   "5x oversampled area-weighted candidates"),
+        "setup_s": setup_s, "site_placement": dict(placement, method="the reference's default placement on the GPU: "
+                                                                   "density prepass, adaptive weighted sample "
+                                                                   "elimination of 5x oversampled candidates, "
+                                                                   "budgeted deficit repair, protected closure"),
         "autotune": tuned, "autotune_independent_samples": tuned_ind, "autotune_wavefront": tuned_wf,
         "autotune_wavefront_independent_samples": tuned_wfi,
         "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
