@@ -112,6 +112,52 @@ def _inset_corners(t, inset_distance, k, rng):
     return pos[idx], _face_normals(t)[tri[idx]], tri[idx].astype(np.uint32), bary[idx, 1], bary[idx, 2]
 
 
+def _boundary_edges(t, mesh_indices, spacing):
+    """Points along the edges used by one triangle only
+    (_boundary_edge_candidates, surface_probes.py:658-779): ceil(length /
+    spacing) segment midpoints per edge, with the face normal."""
+    corners = np.array([[0, 1], [1, 2], [2, 0]])
+    ev = np.sort(mesh_indices.astype(np.int64)[:, corners].reshape(-1, 2), axis=1)
+    keys = ev[:, 0] * (int(ev.max(initial=0)) + 1) + ev[:, 1]
+    _, inverse, counts = np.unique(keys, return_inverse=True, return_counts=True)
+    edges = np.flatnonzero(counts[inverse] == 1)
+    empty = (np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros(0, np.uint32),
+             np.zeros(0, np.float32), np.zeros(0, np.float32))
+    if edges.size == 0:
+        return empty
+    face, local = edges // 3, edges % 3
+    a, b = corners[local, 0], corners[local, 1]
+    p0, p1 = t[face, a], t[face, b]
+    seg = np.maximum(np.ceil(np.linalg.norm(p1 - p0, axis=1) / max(float(spacing), 1e-8)).astype(np.int64), 1)
+    edge_of = np.repeat(np.arange(edges.size), seg)
+    first = np.concatenate([[0], np.cumsum(seg)[:-1]])
+    step = (np.arange(edge_of.size) - first[edge_of]).astype(np.float32)
+    u = (step + np.float32(0.5)) / seg[edge_of].astype(np.float32)
+    pos = (p0[edge_of] * (1.0 - u[:, None]) + p1[edge_of] * u[:, None]).astype(np.float32)
+    bary = np.zeros((edge_of.size, 3), np.float32)
+    rows = np.arange(edge_of.size)
+    bary[rows, a[edge_of]] = 1.0 - u
+    bary[rows, b[edge_of]] = u
+    return pos, _face_normals(t)[face[edge_of]], face[edge_of].astype(np.uint32), bary[:, 1], bary[:, 2]
+
+
+def _render_vertices(mesh, transform, k, rng):
+    """The instance's render vertices with their transformed normals, each on
+    its first incident triangle (_instance_vertex_anchors,
+    surface_probes.py:375-442), at most k."""
+    flat_idx = mesh.indices.astype(np.int64).reshape(-1)
+    verts, first = np.unique(flat_idx, return_index=True)
+    m = np.asarray(transform, dtype=np.float64)
+    pos = (mesh.vertices[verts, :3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]).astype(np.float32)
+    nrm = (mesh.vertices[verts, 3:6].astype(np.float64) @ np.linalg.inv(m[:3, :3])).astype(np.float32)
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-20)
+    tri, corner = first // 3, first % 3
+    b1 = (corner == 1).astype(np.float32)
+    b2 = (corner == 2).astype(np.float32)
+    idx = _limit(verts.shape[0], k, rng)
+    return pos[idx], nrm[idx], tri[idx].astype(np.uint32), b1[idx], b2[idx]
+
+
 def _take(points, idx):
     return tuple(x[idx] for x in points)
 
@@ -225,8 +271,9 @@ class SurfaceProbeSiteLayout:
                   adaptive_wse: bool = True, max_density_multiplier: float = 8.0, sampler=None,
                   profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
         """Sites by weighted sample elimination of oversampled candidates, then
-        deficit repair: audit points (filtered from inset corners, centroids,
-        the candidates and a second surface sample per instance) that gather
+        deficit repair: audit points (filtered from boundary-edge points, inset
+        corners, centroids, the candidates, a second surface sample and the
+        render vertices per instance) that gather
         fewer than repair_min_gather sites get repair sites from the filtered
         repair candidates, up to repair_budget_ratio x the target; audit
         points still short then get their residual deficit as colocated
@@ -313,17 +360,24 @@ class SurfaceProbeSiteLayout:
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
         if repair_min_gather > 0:
-            # audit source per instance (surface_probes.py:2060-2180): inset
-            # corners, centroids, every base candidate and a second surface
-            # sample; the filter keeps one audit point per cell of R/2 and
-            # normal cone, and as repair candidates those that no selected
-            # base site or earlier candidate duplicates bit for bit
+            # audit source per instance (surface_probes.py:2026-2180): boundary
+            # edge points, inset corners, centroids, every base candidate, a
+            # second surface sample and the render vertices; the filter keeps
+            # one audit point per cell of R/2 and normal cone, and as repair
+            # candidates those that no selected base site or earlier
+            # candidate duplicates bit for bit
             sources = []
             for i, (t, a) in enumerate(zip(tris, areas)):
                 rng = np.random.default_rng([int(seed), i, 7919])
                 k = int(counts[i])
-                sources.append(_concat([_inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
-                                        _centroids(t, max(16, k), rng), cands[i], _surface_points(t, a, k, rng)]))
+                mesh_id, _, transform_id = scene_node.instances[i]
+                mesh = scene_node.meshes[mesh_id]
+                boundary = _boundary_edges(t, mesh.indices, float(kernels[i]) * 0.5)
+                boundary = _take(boundary, _limit(boundary[0].shape[0], max(16, k), rng))
+                sources.append(_concat([boundary, _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
+                                        _centroids(t, max(16, k), rng), cands[i], _surface_points(t, a, k, rng),
+                                        _render_vertices(mesh, scene_node.transforms[transform_id], max(16, k),
+                                                         rng)]))
             src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])
             base_sel = np.concatenate([np.flatnonzero(keep[offsets[i]:offsets[i + 1]]) + offsets[i]
                                        for i in range(len(cands))])
