@@ -641,24 +641,30 @@ __global__ void k_rep_count_chosen(uint32_t n, const uint8_t* chosen, unsigned i
 // ---------------------------------------------------------------------------
 constexpr uint32_t kNumpyBuffer = 8192;  // numpy's default ufunc buffer (elements)
 
+// The non-empty cell runs around a query, with each run's head (the
+// reference index at its cursor) cached.
 struct CellRuns {
-    uint32_t b[27], e[27];
+    uint32_t b[27], e[27], head[27];
+    int n;
 };
 
 __device__ __forceinline__ void support_runs(const RepairGrid& g, uint32_t k, const int c[3], CellRuns& r) {
-    int t = 0;
+    r.n = 0;
     for (int dx = -1; dx <= 1; ++dx)
         for (int dy = -1; dy <= 1; ++dy)
-            for (int dz = -1; dz <= 1; ++dz, ++t) {
+            for (int dz = -1; dz <= 1; ++dz) {
                 const int r0 = c[0] + dx, r1 = c[1] + dy, r2 = c[2] + dz;
-                if (r0 < 0 || r1 < 0 || r2 < 0) {
-                    r.b[t] = r.e[t] = 0;
-                    continue;
-                }
+                if (r0 < 0 || r1 < 0 || r2 < 0) continue;
                 const unsigned long long key = ((unsigned long long)k << 48) | ((unsigned long long)r0 << 32) |
                                                ((unsigned long long)r1 << 16) | (unsigned long long)r2;
-                r.b[t] = lower_bound_key(g.keys, g.n, key);
-                r.e[t] = lower_bound_key(g.keys, g.n, key + 1);
+                const uint32_t b = lower_bound_key(g.keys, g.n, key);
+                const uint32_t e = lower_bound_key(g.keys, g.n, key + 1);
+                if (b < e) {
+                    r.b[r.n] = b;
+                    r.e[r.n] = e;
+                    r.head[r.n] = g.idx[b];
+                    ++r.n;
+                }
             }
 }
 
@@ -700,18 +706,23 @@ struct TermStream {
 
     __device__ __forceinline__ double next() {
         for (;;) {
-            int best = -1;
-            uint32_t best_j = 0xffffffffu;
-            for (int t = 0; t < 27; ++t)
-                if (runs.b[t] < runs.e[t]) {
-                    const uint32_t j = idx[runs.b[t]];
-                    if (j < best_j) {
-                        best_j = j;
-                        best = t;
-                    }
+            if (runs.n == 0) return 0.0;  // not reached: the count pass found every term
+            int best = 0;
+            uint32_t best_j = runs.head[0];
+            for (int t = 1; t < runs.n; ++t)
+                if (runs.head[t] < best_j) {
+                    best_j = runs.head[t];
+                    best = t;
                 }
-            if (best < 0) return 0.0;  // not reached: the count pass found every term
-            ++runs.b[best];
+            const uint32_t nb = ++runs.b[best];
+            if (nb < runs.e[best]) {
+                runs.head[best] = idx[nb];
+            } else {  // the run is spent: the last one takes its slot
+                const int last = --runs.n;
+                runs.b[best] = runs.b[last];
+                runs.e[best] = runs.e[last];
+                runs.head[best] = runs.head[last];
+            }
             float d2, nc, tt;
             if (term.valid(best_j, &d2, &nc, &tt)) return (double)term.value(best_j, d2, nc, tt);
         }
@@ -792,7 +803,7 @@ __global__ void k_support(RepairParams rp, RepairSet query, RepairSet ref, Repai
         support_runs(ref_grid, k, c, runs);
         const SupportTerm term{rp, ri, ref, q, qn, area_weight};
         uint32_t n = 0;
-        for (int t = 0; t < 27; ++t)
+        for (int t = 0; t < runs.n; ++t)
             for (uint32_t r = runs.b[t]; r < runs.e[t]; ++r) {
                 float d2, nc, tt;
                 n += term.valid(ref_grid.idx[r], &d2, &nc, &tt) ? 1u : 0u;
