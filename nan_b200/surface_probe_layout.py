@@ -35,7 +35,8 @@ import numpy as np
 
 from .surface_probe_octree import build_point_octree, query_probe_indices
 from .surface_probe_resources import (SURFACE_PROBE_DTYPE, SURFACE_PROBE_FLAG_PROTECTED,
-                                      SURFACE_PROBE_INSTANCE_DTYPE, SURFACE_PROBE_INSTANCE_SHIFT)
+                                      SURFACE_PROBE_FLAG_VERTEX_ANCHOR, SURFACE_PROBE_INSTANCE_DTYPE,
+                                      SURFACE_PROBE_INSTANCE_SHIFT)
 
 
 def allocate_counts(weights, total: int, *, minimum_per_entry: int = 1) -> np.ndarray:
@@ -196,7 +197,13 @@ class SurfaceProbeSiteLayout:
     def from_sites(cls, scene_node, probes, *, leaf_capacity: int = 8, max_depth: int = 16,
                    kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
                    max_density_multiplier: float = 8.0, poisson_radii=None,
-                   kernel_radii=None) -> "SurfaceProbeSiteLayout":
+                   kernel_radii=None, vertex_anchors=None) -> "SurfaceProbeSiteLayout":
+        """vertex_anchors (optional, per instance None or (records, map,
+        anchor site count)): anchor probe records (fronts, then backs for a
+        double-sided instance) kept after the instance's octree-ordered probes
+        and outside its octree, and map u32[T, 3] naming each triangle's three
+        vertex anchors (0xFFFFFFFF: none); the packed triangle map then points
+        each triangle side at its anchors (surface_probes.py:2712-2758)."""
         probes = np.asarray(probes, dtype=SURFACE_PROBE_DTYPE)
         instance_of = probes["meta"][:, 3] >> SURFACE_PROBE_INSTANCE_SHIFT
         n_inst = len(scene_node.instances)
@@ -244,6 +251,20 @@ class SurfaceProbeSiteLayout:
             else:
                 nodes = np.zeros((0, 4), np.uint32)
                 center, extent = (0.0, 0.0, 0.0), 0.0
+            recon = int(rec.shape[0])
+            if vertex_anchors is not None and vertex_anchors[i] is not None:
+                anchor_rec, tri_map, anchor_sites = vertex_anchors[i]
+                anchor_rec = np.asarray(anchor_rec, dtype=SURFACE_PROBE_DTYPE).copy()
+                anchor_rec["position_radius"][:, 3] = kernel
+                rec = np.concatenate([rec, anchor_rec])
+                tri_map = np.asarray(tri_map, dtype=np.uint32).reshape(-1, 3)
+                valid = np.flatnonzero(np.all(tri_map != 0xFFFFFFFF, axis=1))
+                front = tri_map[valid] + np.uint32(probe_offset + recon)
+                back = front + np.uint32(anchor_sites) if anchor_rec.shape[0] > anchor_sites else front
+                maps[2 * valid, :3] = front
+                maps[2 * valid + 1, :3] = back
+                maps[2 * valid, 3] |= 1
+                maps[2 * valid + 1, 3] |= 1
             plane_sigma = max(kernel * 0.25, 1e-6)
             gpu["root_center_extent"][i] = (*center, extent)
             gpu["offsets"][i] = (node_offset, nodes.shape[0], probe_offset, rec.shape[0])
@@ -251,7 +272,7 @@ class SurfaceProbeSiteLayout:
                                 np.asarray(map_offset, dtype=np.uint32).view(np.float32).item())
             infos.append(SurfaceProbeSiteInstance(center, extent, node_offset, int(nodes.shape[0]), probe_offset,
                                                   int(rec.shape[0]), kernel, normal_cos, plane_sigma,
-                                                  float(areas[i]), sites, int(rec.shape[0])))
+                                                  float(areas[i]), sites, recon))
             out_probes.append(rec)
             out_nodes.append(nodes)
             out_maps.append(maps)
@@ -268,7 +289,8 @@ class SurfaceProbeSiteLayout:
     def build_wse(cls, scene_node, target_probe_count: int, *, device=None, oversample_factor: int = 5,
                   seed: int = 1, minimum_per_instance: int = 4, repair_budget_ratio: float = 0.30,
                   repair_min_gather: int = 4, kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
-                  adaptive_wse: bool = True, max_density_multiplier: float = 8.0, sampler=None,
+                  adaptive_wse: bool = True, max_density_multiplier: float = 8.0,
+                  build_vertex_anchors: bool = False, sampler=None,
                   profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
         """Sites by weighted sample elimination of oversampled candidates, then
         deficit repair: audit points (filtered from boundary-edge points, inset
@@ -288,7 +310,12 @@ class SurfaceProbeSiteLayout:
         instance budget then follows area x m, candidates are drawn with
         probability proportional to area x m, and the elimination is the
         adaptive one with each candidate's relative density
-        m / (adaptive mass / area)."""
+        m / (adaptive mass / area).
+
+        build_vertex_anchors (off by default, as in the reference) adds one
+        anchor probe per render vertex of each instance, flagged
+        SURFACE_PROBE_FLAG_VERTEX_ANCHOR and kept outside the octree, and
+        the triangle map the resolve's vertex fallback reads."""
         import time
 
         from .surface_probe_sampler import SurfaceProbeSampler
@@ -463,9 +490,31 @@ class SurfaceProbeSiteLayout:
                 r["meta"][:, 2] = b2.view(np.uint32)
                 r["meta"][:, 3] = (1 if side else 0) | flags[i] | (i << SURFACE_PROBE_INSTANCE_SHIFT)
                 records.append(r)
+        anchors = None
+        if build_vertex_anchors:
+            anchors = []
+            for i, (mesh_id, _, transform_id) in enumerate(scene_node.instances):
+                mesh = scene_node.meshes[mesh_id]
+                pos, nrm, tri, b1, b2 = _render_vertices(mesh, scene_node.transforms[transform_id], 1 << 62, None)
+                verts = np.unique(mesh.indices.astype(np.int64).reshape(-1))
+                lookup = np.full(mesh.vertex_count, 0xFFFFFFFF, np.uint32)
+                lookup[verts] = np.arange(verts.shape[0], dtype=np.uint32)
+                recs = []
+                for side in range(2 if double_sided[i] else 1):
+                    r = np.zeros(pos.shape[0], dtype=SURFACE_PROBE_DTYPE)
+                    r["position_radius"][:, :3] = pos
+                    r["normal_side"][:, :3] = nrm * (-1.0 if side else 1.0)
+                    r["normal_side"][:, 3] = 1.0
+                    r["meta"][:, 0] = tri
+                    r["meta"][:, 1] = b1.view(np.uint32)
+                    r["meta"][:, 2] = b2.view(np.uint32)
+                    r["meta"][:, 3] = ((1 if side else 0) | SURFACE_PROBE_FLAG_VERTEX_ANCHOR
+                                       | (i << SURFACE_PROBE_INSTANCE_SHIFT))
+                    recs.append(r)
+                anchors.append((np.concatenate(recs), lookup[mesh.indices.astype(np.int64)], pos.shape[0]))
         layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees,
-                                max_density_multiplier=max_density_multiplier, **kwargs)
+                                max_density_multiplier=max_density_multiplier, vertex_anchors=anchors, **kwargs)
         if profile is not None:
             profile.update(density_prepass_s=t_pre_end - t_pre, adaptive=bool(adaptive_wse),
                            candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,
