@@ -459,6 +459,27 @@ NAN_B200_API int nan_filter_audit_repair(NanContext* ctx, const float* candidate
                                          uint32_t* audit_count, uint32_t* repair_indices, uint32_t* repair_count,
                                          void* stream);
 
+/* Point octrees of surface-probe sites (_build_point_octree_python,
+ * surface_probes.py:1348-1438; surface_probe_build_point_octree,
+ * surface_probe_sampler.h:120-223) for set_count point sets in one call.
+ * positions: device f32[N][3], set k = [set_offsets[k], set_offsets[k+1])
+ * (host u32[S+1]); empty sets get no nodes. Per set, nodes u32[4] =
+ * (child_base, child_mask, probe_start, probe_count), numbered as the
+ * reference's depth-first build numbers them (root 0, a split node's present
+ * octants contiguous in ascending order from child_base), local to the set;
+ * written to nodes (device u32[node_capacity][4]) from node_offsets[k] (host
+ * u32[S+1] out). order (device u32[N]) gets, per set, the set-local input
+ * index of each position in leaf order (each leaf ascending), which
+ * probe_start and probe_count index. roots (host f64[S][4]) gets each root
+ * cube's centre and half extent. leaf_capacity >= 1, max_depth 1..16.
+ * NAN_ERR_LIMIT when the nodes exceed node_capacity, with
+ * node_offsets[set_count] holding the count needed. Allocates scratch on the
+ * stream and synchronizes it. */
+NAN_B200_API int nan_build_point_octrees(NanContext* ctx, const float* positions, const uint32_t* set_offsets,
+                                         uint32_t set_count, uint32_t leaf_capacity, uint32_t max_depth,
+                                         uint32_t* nodes, uint32_t node_capacity, uint32_t* node_offsets,
+                                         uint32_t* order, double* roots, void* stream);
+
 /* Deficit repair (deficit_repair, surface_probes.py:1201-1253;
  * surface_probe_deficit_repair, surface_probe_sampler.h:120-223; the Python
  * form deficit_repair_python, surface_probe_sampler.py:990-1103). Each audit

@@ -317,6 +317,7 @@ EXPORTS = {
                                ctypes.POINTER(_U32), _VP]),
     "nan_wse_eliminate_adaptive": (_I, [_VP, _VP, _VP, _VP, _VP, _U32, _VP, _VP, ctypes.POINTER(NanWseOptions), _VP,
                                         _VP, ctypes.POINTER(_U32), _VP]),
+    "nan_build_point_octrees": (_I, [_VP, _VP, _VP, _U32, _U32, _U32, _VP, _U32, _VP, _VP, _VP, _VP]),
     "nan_filter_audit_repair": (_I, [_VP, _VP, _VP, _VP, _U32, _VP, _VP, _VP, _U32, _VP, _U32, _U32, _VP,
                                      ctypes.c_double, _VP, ctypes.POINTER(_U32), _VP, ctypes.POINTER(_U32), _VP]),
     "nan_trace_points": (_I, [_VP, _VP, _U32, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanLighting), _VP]),

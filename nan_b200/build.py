@@ -23,7 +23,7 @@ CSRC = PKG / "csrc"
 ROOT = PKG.parent
 OUT = PKG / "libnan_b200.so"
 BUILD = ROOT / "_build"
-SOURCES = ["nan_abi.cu", "nan_bvh.cu", "nan_trace.cu", "nan_wavefront.cu", "nan_cache.cu", "nan_batch.cu", "nan_wse.cu", "nan_audit_filter.cu"]
+SOURCES = ["nan_abi.cu", "nan_bvh.cu", "nan_trace.cu", "nan_wavefront.cu", "nan_cache.cu", "nan_batch.cu", "nan_wse.cu", "nan_audit_filter.cu", "nan_octree.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-fvisibility=hidden",

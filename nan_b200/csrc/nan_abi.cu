@@ -517,6 +517,26 @@ NAN_B200_API int nan_filter_audit_repair(NanContext* ctx, const float* candidate
         normal_cosine_threshold, audit_indices, audit_count, repair_indices, repair_count, as_stream(stream));
 }
 
+NAN_B200_API int nan_build_point_octrees(NanContext* ctx, const float* positions, const uint32_t* set_offsets,
+                                         uint32_t set_count, uint32_t leaf_capacity, uint32_t max_depth,
+                                         uint32_t* nodes, uint32_t node_capacity, uint32_t* node_offsets,
+                                         uint32_t* order, double* roots, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if (!set_offsets || !node_offsets || !roots) return invalid("surface probe octree received a null pointer");
+    if (set_count == 0 || set_count > 65536u) return invalid("set_count must be in 1..65536");
+    if (leaf_capacity == 0 || max_depth == 0 || max_depth > 16u)
+        return invalid("leaf_capacity must be positive and max_depth in 1..16");
+    if (set_offsets[0] != 0u) return invalid("set_offsets[0] must be 0");
+    for (uint32_t k = 0; k < set_count; ++k)
+        if (set_offsets[k + 1] < set_offsets[k]) return invalid("set_offsets must be non-decreasing");
+    const uint32_t n = set_offsets[set_count];
+    if (n == 0) return invalid("the octrees need at least one position");
+    if (!positions || !order || (node_capacity && !nodes)) return invalid("null buffer");
+    return nan_host::launch_build_point_octrees(ctx, positions, set_offsets, set_count, leaf_capacity, max_depth,
+                                                nodes, node_capacity, node_offsets, order, roots, as_stream(stream));
+}
+
 NAN_B200_API int nan_deficit_repair(NanContext* ctx, const float* base_positions, const float* base_normals,
                                     const uint32_t* base_instances, uint32_t base_count,
                                     const float* candidate_positions, const float* candidate_normals,

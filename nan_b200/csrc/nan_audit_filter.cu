@@ -17,6 +17,7 @@
 // entry's exact duplicates before it in that order sit before it in its hash
 // run; a candidate scans back through its run and is kept when it finds none.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <cmath>
@@ -219,7 +220,7 @@ int launch_filter_audit_repair(NanContext* ctx, const float* cand_pos, const flo
     size_t tmp_bytes = 0, need = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, need, keys, keys_sorted, idx, idx_sorted, (int)entries, 0, 64, st);
     tmp_bytes = std::max(tmp_bytes, need);
-    cub::DeviceSelect::Flagged(nullptr, need, cub::CountingInputIterator<uint32_t>(0), audit, audit_indices, counts,
+    cub::DeviceSelect::Flagged(nullptr, need, thrust::counting_iterator<uint32_t>(0), audit, audit_indices, counts,
                                (int)n, st);
     tmp_bytes = std::max(tmp_bytes, need);
     void* tmp = get(tmp_bytes);
@@ -247,9 +248,9 @@ int launch_filter_audit_repair(NanContext* ctx, const float* cand_pos, const flo
     k_flt_hash<<<blocks(entries, 256), 256, 0, st>>>(fe, keys, idx, status);
     cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys, keys_sorted, idx, idx_sorted, (int)entries, 0, 64, st);
     k_flt_exclude<<<blocks(entries, 256), 256, 0, st>>>(fe, keys_sorted, idx_sorted, repair);
-    cub::DeviceSelect::Flagged(tmp, tmp_bytes, cub::CountingInputIterator<uint32_t>(0), audit, audit_indices, counts,
+    cub::DeviceSelect::Flagged(tmp, tmp_bytes, thrust::counting_iterator<uint32_t>(0), audit, audit_indices, counts,
                                (int)n, st);
-    cub::DeviceSelect::Flagged(tmp, tmp_bytes, cub::CountingInputIterator<uint32_t>(0), repair, repair_indices,
+    cub::DeviceSelect::Flagged(tmp, tmp_bytes, thrust::counting_iterator<uint32_t>(0), repair, repair_indices,
                                counts + 1, (int)n, st);
     ctx->launches += 9;
     uint32_t host_counts[2] = {0, 0};

@@ -178,6 +178,10 @@ int launch_filter_audit_repair(NanContext* ctx, const float* cand_pos, const flo
                                uint32_t base_selected_count, uint32_t set_count, const double* cell_sizes,
                                double ncos, uint32_t* audit_indices, uint32_t* audit_count, uint32_t* repair_indices,
                                uint32_t* repair_count, cudaStream_t st);
+int launch_build_point_octrees(NanContext* ctx, const float* positions, const uint32_t* set_offsets,
+                               uint32_t set_count, uint32_t leaf_capacity, uint32_t max_depth, uint32_t* nodes,
+                               uint32_t node_capacity, uint32_t* node_offsets, uint32_t* order, double* roots,
+                               cudaStream_t st);
 int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* ref_nrm, const uint32_t* ref_inst,
                             const float* area_weights, uint32_t ref_count, const float* query_pos,
                             const float* query_nrm, const uint32_t* query_inst, uint32_t query_count,

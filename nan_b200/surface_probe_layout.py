@@ -197,13 +197,16 @@ class SurfaceProbeSiteLayout:
     def from_sites(cls, scene_node, probes, *, leaf_capacity: int = 8, max_depth: int = 16,
                    kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
                    max_density_multiplier: float = 8.0, poisson_radii=None,
-                   kernel_radii=None, vertex_anchors=None) -> "SurfaceProbeSiteLayout":
+                   kernel_radii=None, vertex_anchors=None, sampler=None) -> "SurfaceProbeSiteLayout":
         """vertex_anchors (optional, per instance None or (records, map,
         anchor site count)): anchor probe records (fronts, then backs for a
         double-sided instance) kept after the instance's octree-ordered probes
         and outside its octree, and map u32[T, 3] naming each triangle's three
         vertex anchors (0xFFFFFFFF: none); the packed triangle map then points
-        each triangle side at its anchors (surface_probes.py:2712-2758)."""
+        each triangle side at its anchors (surface_probes.py:2712-2758).
+        With a SurfaceProbeSampler the instances' octrees are built on its
+        GPU in one call (nan_build_point_octrees), else by
+        build_point_octree on the host; both give the same nodes and order."""
         probes = np.asarray(probes, dtype=SURFACE_PROBE_DTYPE)
         instance_of = probes["meta"][:, 3] >> SURFACE_PROBE_INSTANCE_SHIFT
         n_inst = len(scene_node.instances)
@@ -228,6 +231,11 @@ class SurfaceProbeSiteLayout:
         node_offset = probe_offset = map_offset = 0
         by_instance = np.argsort(instance_of, kind="stable")
         bounds = np.searchsorted(instance_of[by_instance], np.arange(n_inst + 1))
+        gpu_trees = None
+        if sampler is not None and probes.shape[0]:
+            gpu_trees = sampler.build_point_octrees(
+                [probes["position_radius"][by_instance[bounds[i]:bounds[i + 1]], :3] for i in range(n_inst)],
+                leaf_capacity=leaf_capacity, max_depth=max_depth)
         for i in range(n_inst):
             rec = probes[by_instance[bounds[i]:bounds[i + 1]]].copy()
             sites = int(fronts[i])
@@ -241,8 +249,12 @@ class SurfaceProbeSiteLayout:
             maps[:, 3] = 0
             if rec.shape[0]:
                 rec["position_radius"][:, 3] = kernel
-                nodes, order, center, extent = build_point_octree(rec["position_radius"][:, :3],
-                                                                  leaf_capacity=leaf_capacity, max_depth=max_depth)
+                if gpu_trees is not None:
+                    nodes, order, center, extent = gpu_trees[i]
+                else:
+                    nodes, order, center, extent = build_point_octree(rec["position_radius"][:, :3],
+                                                                      leaf_capacity=leaf_capacity,
+                                                                      max_depth=max_depth)
                 rec = rec[order]
                 nodes = nodes.copy()
                 branch = nodes[:, 1] != 0
@@ -514,7 +526,8 @@ class SurfaceProbeSiteLayout:
                 anchors.append((np.concatenate(recs), lookup[mesh.indices.astype(np.int64)], pos.shape[0]))
         layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees,
-                                max_density_multiplier=max_density_multiplier, vertex_anchors=anchors, **kwargs)
+                                max_density_multiplier=max_density_multiplier, vertex_anchors=anchors,
+                                sampler=sampler, **kwargs)
         if profile is not None:
             profile.update(density_prepass_s=t_pre_end - t_pre, adaptive=bool(adaptive_wse),
                            candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,

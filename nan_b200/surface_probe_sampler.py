@@ -170,6 +170,46 @@ class SurfaceProbeSampler:
         host = lambda t, k: t[:k].cpu().numpy().view(np.uint32).astype(np.int64)
         return CandidateFilterResult(host(audit, na.value), host(repair, nr.value))
 
+    def build_point_octrees(self, position_sets, *, leaf_capacity: int = 8, max_depth: int = 16, stream=None):
+        """Point octrees of several position sets (each f32 [n, 3]) in one
+        GPU call, as build_point_octree builds each: per set (nodes u32
+        [M, 4], order i64 [n], root centre, root half extent), or None for an
+        empty set."""
+        import torch
+
+        dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
+        sets = [np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3) for x in position_sets]
+        offsets = np.concatenate([[0], np.cumsum([x.shape[0] for x in sets])]).astype(np.uint32)
+        n = int(offsets[-1])
+        if n == 0:
+            return [None] * len(sets)
+        pos = torch.as_tensor(np.concatenate(sets), device=dev)
+        order = torch.empty(n, dtype=torch.int32, device=dev)
+        node_offsets = np.zeros(len(sets) + 1, np.uint32)
+        roots = np.zeros((len(sets), 4), np.float64)
+        capacity = max(64, n // max(int(leaf_capacity), 1) * 3 + 2 * len(sets))
+        for _ in range(2):
+            nodes = torch.empty((capacity, 4), dtype=torch.int32, device=dev)
+            rc = lib().nan_build_point_octrees(self.context.handle, ptr(pos), offsets.ctypes.data, len(sets),
+                                               int(leaf_capacity), int(max_depth), ptr(nodes), capacity,
+                                               node_offsets.ctypes.data, ptr(order), roots.ctypes.data,
+                                               stream_handle(stream))
+            if rc == 3 and int(node_offsets[-1]) > capacity:  # NAN_ERR_LIMIT: retry at the needed size
+                capacity = int(node_offsets[-1])
+                continue
+            check(rc)
+            break
+        nodes_h = nodes[:int(node_offsets[-1])].cpu().numpy().view(np.uint32)
+        order_h = order.cpu().numpy().astype(np.int64)
+        out = []
+        for k in range(len(sets)):
+            if offsets[k + 1] == offsets[k]:
+                out.append(None)
+                continue
+            out.append((nodes_h[node_offsets[k]:node_offsets[k + 1]].copy(), order_h[offsets[k]:offsets[k + 1]],
+                        tuple(float(v) for v in roots[k, :3]), float(roots[k, 3])))
+        return out
+
     def deficit_repair(self, base_positions, base_normals, base_instances, candidate_positions, candidate_normals,
                        candidate_instances, audit_positions, audit_normals, audit_instances, instance_radii, *,
                        min_gather_count: int = 4, max_repair_count: int, normal_cosine_threshold: float = 0.5,
