@@ -34,6 +34,7 @@ from __future__ import annotations
 
 import ctypes
 from dataclasses import dataclass
+from typing import NamedTuple
 
 import numpy as np
 
@@ -55,6 +56,13 @@ def _points(dev, positions, normals, instances, name):
     if p.shape[0] != n.shape[0] or p.shape[0] != i.shape[0]:
         raise ValueError(f"{name} positions, normals and instances must have the same length")
     return p, n, i
+
+
+class SupportEstimateResult(NamedTuple):
+    """As the reference's SupportEstimateResult (support_f, density_m); unpacks
+    as a pair."""
+    support_f: np.ndarray
+    density_m: np.ndarray
 
 
 @dataclass(frozen=True)
@@ -247,8 +255,9 @@ class SurfaceProbeSampler:
                          query_positions, query_normals, query_instances, instance_radii, *,
                          normal_cosine_threshold: float = 0.5, weight_epsilon: float = 1e-6,
                          max_density_multiplier: float = 8.0, stream=None):
-        """The reference's estimate_surface_support on the GPU: (support_f,
-        density_m) per query site, host float32 arrays."""
+        """The reference's estimate_surface_support on the GPU: support_f and
+        density_m per query site (host float32 arrays), as a
+        SupportEstimateResult that also unpacks as a pair."""
         import torch
 
         dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
@@ -267,7 +276,7 @@ class SurfaceProbeSampler:
         check(lib().nan_estimate_support(self.context.handle, ptr(rp), ptr(rn), ptr(ri), ptr(ra), rp.shape[0],
                                          ptr(qp), ptr(qn), ptr(qi), qp.shape[0], radii.ctypes.data, radii.shape[0],
                                          ctypes.byref(opt), ptr(f), ptr(m), stream_handle(stream)))
-        return f.cpu().numpy(), m.cpu().numpy()
+        return SupportEstimateResult(f.cpu().numpy(), m.cpu().numpy())
 
 
 def adaptive_weighted_sample_elimination(positions, normals, relative_densities, output_count: int, *,
