@@ -172,3 +172,29 @@ def estimate_support(reference_positions, reference_normals, reference_instances
     _call("surface_probe_estimate_support", _p(rp), _p(rn), _p(ri), _p(ra), u(rp.shape[0]), _p(qp), _p(qn), _p(qi),
           u(qp.shape[0]), _p(radii), u(radii.shape[0]), ctypes.byref(opt), _p(f), _p(m))
     return f, m
+
+
+class PointOctreeResult(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.POINTER(ctypes.c_uint32)), ("node_count", ctypes.c_uint32),
+                ("probe_order", ctypes.POINTER(ctypes.c_uint32)), ("probe_count", ctypes.c_uint32),
+                ("root_center", ctypes.c_double * 3), ("root_extent", ctypes.c_double)]
+
+
+def build_point_octree(positions, *, leaf_capacity=8, max_depth=16):
+    """surface_probe_build_point_octree: (nodes u32[M, 4], order i64[N],
+    root centre, root half extent); the library's buffers are released."""
+    p = _f3(positions)
+    res = PointOctreeResult()
+    u = lambda v: ctypes.c_uint32(int(v))
+    _call("surface_probe_build_point_octree", _p(p), u(p.shape[0]), u(leaf_capacity), u(max_depth),
+          ctypes.byref(res), ctypes.c_void_p(0))
+    try:
+        nodes = np.ctypeslib.as_array(res.nodes, shape=(res.node_count * 4,)).reshape(-1, 4).copy()
+        order = np.ctypeslib.as_array(res.probe_order, shape=(res.probe_count,)).astype(np.int64)
+        center = tuple(float(v) for v in res.root_center)
+        extent = float(res.root_extent)
+    finally:
+        free = lib().surface_probe_free_point_octree
+        free.restype = None
+        free(ctypes.byref(res))
+    return nodes, order, center, extent

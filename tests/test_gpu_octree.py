@@ -1,6 +1,7 @@
 """Point octrees on the GPU (nan_build_point_octrees) against the
 reference's builder: the golden vectors made by its own Python builder
-(nodes, order, root), and the host restatement (build_point_octree) on many
+(nodes, order, root), its C++ builder compiled from its sources, and the
+host restatement (build_point_octree) on many
 sets in one call, with clustered and coincident points and depth limits; a
 site layout packed with the GPU octrees equals the host-packed one."""
 
@@ -46,6 +47,24 @@ def test_gpu_octrees_match_host_builder(device, leaf, depth):
         np.testing.assert_array_equal(tree[0], nodes)
         np.testing.assert_array_equal(tree[1], order)
         assert tree[2] == center and tree[3] == extent
+    device.check()
+
+
+def test_gpu_octrees_match_reference_cpp_builder(device):
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+    from oracle import ref_sampler
+
+    if not ref_sampler.available():
+        pytest.skip("reference sampler library not built")
+    rng = np.random.default_rng(17)
+    sets = [rng.normal(size=(int(n), 3)).astype(np.float32) * 3.0 for n in rng.integers(1, 20000, 6)]
+    for leaf, depth in ((8, 16), (2, 9)):
+        trees = SurfaceProbeSampler(device).build_point_octrees(sets, leaf_capacity=leaf, max_depth=depth)
+        for p, tree in zip(sets, trees):
+            ref = ref_sampler.build_point_octree(p, leaf_capacity=leaf, max_depth=depth)
+            np.testing.assert_array_equal(tree[0], ref[0])
+            np.testing.assert_array_equal(tree[1], ref[1])
+            assert tree[2] == ref[2] and tree[3] == ref[3]
     device.check()
 
 

@@ -105,3 +105,23 @@ def test_own_exp_and_log2_within_two_ulp():
         got = own_log2(float(y))
         assert abs(got - want) <= 2.5 * abs(float(np.spacing(np.float32(want)))) + 1e-7, (y, got, want)
     assert own_exp(-100.0) == 0.0 and math.isinf(own_exp(100.0)) and own_log2(8.0) == 3.0
+
+
+@pytest.mark.parametrize("leaf,depth", [(8, 16), (1, 16), (3, 5)])
+def test_octree_matches_reference_cpp_builder(leaf, depth):
+    """The reference's default (C++) builder, compiled from its sources,
+    gives the same nodes, order and root as the host builder."""
+    from nan_b200.surface_probe_octree import build_point_octree
+    from oracle import ref_sampler
+
+    if not ref_sampler.available():
+        pytest.skip("reference sampler library not built")
+    rng = np.random.default_rng(leaf * 10 + depth)
+    p = rng.normal(size=(3000, 3)).astype(np.float32)
+    p[:600] = p[0]
+    p[600:1000, 1] = 0.0
+    ref = ref_sampler.build_point_octree(p, leaf_capacity=leaf, max_depth=depth)
+    mine = build_point_octree(p, leaf_capacity=leaf, max_depth=depth)
+    np.testing.assert_array_equal(mine[0], ref[0])
+    np.testing.assert_array_equal(mine[1], ref[1])
+    assert mine[2] == ref[2] and mine[3] == ref[3]

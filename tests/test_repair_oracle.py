@@ -79,3 +79,24 @@ def test_support_oracle_against_reference_cpp(golden, case):
     cf, cm = ref_sampler.estimate_support(*args)
     np.testing.assert_allclose(f, cf, atol=1e-6)
     np.testing.assert_allclose(m, cm, atol=1e-5)
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_repair_oracle_against_reference_cpp(golden, case):
+    """The reference's default (C++) repair, compiled from its sources: the
+    same choices and counts; weight sums and ESS within the reference's own
+    cross-backend bar (rtol 1e-6, test_surface_probes.py:469-495)."""
+    from oracle import ref_sampler
+    from oracle.oracle import deficit_repair
+
+    if not ref_sampler.available():
+        pytest.skip("reference sampler library not built")
+    args = [golden[f"rep{case}_{n}"] for n in ("bp", "bn", "bi", "cp", "cn", "ci", "ap", "an", "ai", "radii")]
+    mg, budget = (int(v) for v in golden[f"rep{case}_params"])
+    mine = deficit_repair(*args, min_gather_count=mg, max_repair_count=budget)
+    ref = ref_sampler.deficit_repair(*args, min_gather_count=mg, max_repair_count=budget)
+    np.testing.assert_array_equal(mine["selected"], ref["selected"])
+    for name in ("counts_before", "counts_after"):
+        np.testing.assert_array_equal(mine[name], ref[name])
+    for name in ("weight_sums_before", "weight_sums_after", "ess_before", "ess_after"):
+        np.testing.assert_allclose(mine[name], ref[name], rtol=1e-6)
