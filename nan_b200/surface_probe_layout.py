@@ -100,37 +100,46 @@ def _centroids(t, k, rng):
 
 def _inset_corners(t, inset_distance, k, rng):
     """Corners pulled inside their face (_triangle_inset_corner_candidates,
-    :614-655), at most k."""
-    edges = np.stack([np.linalg.norm(t[:, 1] - t[:, 0], axis=1), np.linalg.norm(t[:, 2] - t[:, 1], axis=1),
-                      np.linalg.norm(t[:, 0] - t[:, 2], axis=1)], axis=1)
+    :614-655), at most k (the subset drawn first, then only it computed)."""
+    idx = _limit(3 * t.shape[0], k, rng)
+    tri, corner = idx // 3, idx % 3
+    ts = t[tri]
+    edges = np.stack([np.linalg.norm(ts[:, 1] - ts[:, 0], axis=1), np.linalg.norm(ts[:, 2] - ts[:, 1], axis=1),
+                      np.linalg.norm(ts[:, 0] - ts[:, 2], axis=1)], axis=1)
     inset = np.clip(float(inset_distance) / np.maximum(edges.max(axis=1), 1e-8), 1e-4, 0.1).astype(np.float32)
-    bary = np.repeat(inset[:, None], 9, axis=1).reshape(-1, 3)
-    for corner in range(3):
-        bary[corner::3, corner] = 1.0 - 2.0 * inset
-    tri = np.repeat(np.arange(t.shape[0]), 3)
-    pos = np.einsum("ni,nij->nj", bary, t[tri]).astype(np.float32)
-    idx = _limit(pos.shape[0], k, rng)
-    return pos[idx], _face_normals(t)[tri[idx]], tri[idx].astype(np.uint32), bary[idx, 1], bary[idx, 2]
+    bary = np.repeat(inset[:, None], 3, axis=1)
+    bary[np.arange(idx.shape[0]), corner] = 1.0 - 2.0 * inset
+    pos = np.einsum("ni,nij->nj", bary, ts).astype(np.float32)
+    return pos, _face_normals(ts), tri.astype(np.uint32), bary[:, 1], bary[:, 2]
 
 
-def _boundary_edges(t, mesh_indices, spacing):
-    """Points along the edges used by one triangle only
-    (_boundary_edge_candidates, surface_probes.py:658-779): ceil(length /
-    spacing) segment midpoints per edge, with the face normal."""
+def _boundary_edge_list(mesh_indices):
+    """(face, local edge) of every edge used by one triangle only, keyed by
+    vertex index (_boundary_edge_topology, surface_probes.py:658-688); a
+    property of the mesh, shared by its instances."""
     corners = np.array([[0, 1], [1, 2], [2, 0]])
     ev = np.sort(mesh_indices.astype(np.int64)[:, corners].reshape(-1, 2), axis=1)
     keys = ev[:, 0] * (int(ev.max(initial=0)) + 1) + ev[:, 1]
     _, inverse, counts = np.unique(keys, return_inverse=True, return_counts=True)
     edges = np.flatnonzero(counts[inverse] == 1)
+    return edges // 3, edges % 3
+
+
+def _boundary_edges(t, mesh_indices, spacing, edge_list=None):
+    """Points along the edges used by one triangle only
+    (_boundary_edge_candidates, surface_probes.py:690-779): ceil(length /
+    spacing) segment midpoints per edge, with the face normal. edge_list:
+    the mesh's _boundary_edge_list, when already known."""
+    corners = np.array([[0, 1], [1, 2], [2, 0]])
+    face, local = _boundary_edge_list(mesh_indices) if edge_list is None else edge_list
     empty = (np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros(0, np.uint32),
              np.zeros(0, np.float32), np.zeros(0, np.float32))
-    if edges.size == 0:
+    if face.size == 0:
         return empty
-    face, local = edges // 3, edges % 3
     a, b = corners[local, 0], corners[local, 1]
     p0, p1 = t[face, a], t[face, b]
     seg = np.maximum(np.ceil(np.linalg.norm(p1 - p0, axis=1) / max(float(spacing), 1e-8)).astype(np.int64), 1)
-    edge_of = np.repeat(np.arange(edges.size), seg)
+    edge_of = np.repeat(np.arange(face.size), seg)
     first = np.concatenate([[0], np.cumsum(seg)[:-1]])
     step = (np.arange(edge_of.size) - first[edge_of]).astype(np.float32)
     u = (step + np.float32(0.5)) / seg[edge_of].astype(np.float32)
@@ -139,24 +148,29 @@ def _boundary_edges(t, mesh_indices, spacing):
     rows = np.arange(edge_of.size)
     bary[rows, a[edge_of]] = 1.0 - u
     bary[rows, b[edge_of]] = u
-    return pos, _face_normals(t)[face[edge_of]], face[edge_of].astype(np.uint32), bary[:, 1], bary[:, 2]
+    return pos, _face_normals(t[face])[edge_of], face[edge_of].astype(np.uint32), bary[:, 1], bary[:, 2]
 
 
-def _render_vertices(mesh, transform, k, rng):
+def _vertex_list(mesh):
+    """The mesh's used vertices and, for each, the first index slot naming
+    it (a property of the mesh, shared by its instances)."""
+    flat_idx = mesh.indices.astype(np.int64).reshape(-1)
+    return np.unique(flat_idx, return_index=True)
+
+
+def _render_vertices(mesh, transform, k, rng, vertex_list=None):
     """The instance's render vertices with their transformed normals, each on
     its first incident triangle (_instance_vertex_anchors,
     surface_probes.py:375-442), at most k."""
-    flat_idx = mesh.indices.astype(np.int64).reshape(-1)
-    verts, first = np.unique(flat_idx, return_index=True)
+    verts, first = _vertex_list(mesh) if vertex_list is None else vertex_list
+    idx = _limit(verts.shape[0], k, rng)
+    verts, first = verts[idx], first[idx]
     m = np.asarray(transform, dtype=np.float64)
     pos = (mesh.vertices[verts, :3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]).astype(np.float32)
     nrm = (mesh.vertices[verts, 3:6].astype(np.float64) @ np.linalg.inv(m[:3, :3])).astype(np.float32)
     nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-20)
     tri, corner = first // 3, first % 3
-    b1 = (corner == 1).astype(np.float32)
-    b2 = (corner == 2).astype(np.float32)
-    idx = _limit(verts.shape[0], k, rng)
-    return pos[idx], nrm[idx], tri[idx].astype(np.uint32), b1[idx], b2[idx]
+    return pos, nrm, tri.astype(np.uint32), (corner == 1).astype(np.float32), (corner == 2).astype(np.float32)
 
 
 def _take(points, idx):
@@ -333,16 +347,25 @@ class SurfaceProbeSiteLayout:
         from .surface_probe_sampler import SurfaceProbeSampler
 
         t0 = time.perf_counter()
-        tris, areas, double_sided = [], [], []
-        for mesh_id, mat_id, transform_id in scene_node.instances:
+        # world triangles and areas, the instances of one mesh transformed together
+        n_inst = len(scene_node.instances)
+        tris, areas = [None] * n_inst, [None] * n_inst
+        double_sided = [bool(scene_node.materials[mat_id].double_sided) for _, mat_id, _ in scene_node.instances]
+        by_mesh: dict = {}
+        for i, (mesh_id, _, _) in enumerate(scene_node.instances):
+            by_mesh.setdefault(mesh_id, []).append(i)
+        for mesh_id, members in by_mesh.items():
             mesh = scene_node.meshes[mesh_id]
-            m = scene_node.transforms[transform_id].astype(np.float64)
-            p = mesh.vertices[:, :3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
-            t = p[mesh.indices.astype(np.int64).reshape(-1, 3)].astype(np.float32)
-            tris.append(t)
-            e = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]).astype(np.float64)
-            areas.append(0.5 * np.linalg.norm(e, axis=1))
-            double_sided.append(bool(scene_node.materials[mat_id].double_sided))
+            mats = np.stack([np.asarray(scene_node.transforms[scene_node.instances[i][2]], dtype=np.float64)
+                             for i in members])
+            p = np.einsum("vk,gjk->gvj", mesh.vertices[:, :3].astype(np.float64), mats[:, :3, :3]) + \
+                mats[:, None, :3, 3]
+            t = p[:, mesh.indices.astype(np.int64)].astype(np.float32)  # [g, T, 3, 3]
+            e = np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0]).astype(np.float64)
+            a = 0.5 * np.linalg.norm(e, axis=2)
+            for j, i in enumerate(members):
+                tris[i], areas[i] = t[j], a[j]
+        mesh_lists: dict = {}  # per mesh: boundary edges and used vertices, shared by its instances
         totals = np.array([a.sum() for a in areas])
         target = int(target_probe_count)
         minimum = min(minimum_per_instance, max(1, target // max(len(totals), 1)))
@@ -411,12 +434,15 @@ class SurfaceProbeSiteLayout:
                 k = int(counts[i])
                 mesh_id, _, transform_id = scene_node.instances[i]
                 mesh = scene_node.meshes[mesh_id]
-                boundary = _boundary_edges(t, mesh.indices, float(kernels[i]) * 0.5)
+                if mesh_id not in mesh_lists:
+                    mesh_lists[mesh_id] = (_boundary_edge_list(mesh.indices), _vertex_list(mesh))
+                edge_list, vertex_list = mesh_lists[mesh_id]
+                boundary = _boundary_edges(t, mesh.indices, float(kernels[i]) * 0.5, edge_list)
                 boundary = _take(boundary, _limit(boundary[0].shape[0], max(16, k), rng))
                 sources.append(_concat([boundary, _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
                                         _centroids(t, max(16, k), rng), cands[i], _surface_points(t, a, k, rng),
                                         _render_vertices(mesh, scene_node.transforms[transform_id], max(16, k),
-                                                         rng)]))
+                                                         rng, vertex_list)]))
             src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])
             base_sel = np.concatenate([np.flatnonzero(keep[offsets[i]:offsets[i + 1]]) + offsets[i]
                                        for i in range(len(cands))])
