@@ -82,6 +82,33 @@ def _surface_points(t, areas, k, rng, densities=None):
     return pos, _face_normals(t)[choice], choice.astype(np.uint32), b1, b2
 
 
+def _surface_points_group(t, areas, counts, rng, densities=None):
+    """_surface_points for the g instances of one mesh at once: t f32[g, T,
+    3, 3], areas [g, T], counts[g] points per instance, densities [g, T] or
+    None; one random stream for the group. Returns one tuple per instance."""
+    g, n = areas.shape
+    w = areas if densities is None else areas * np.asarray(densities, dtype=np.float64)
+    cdf = np.cumsum(w, axis=1, dtype=np.float64)
+    cdf /= cdf[:, -1:]
+    cdf[:, -1] = 1.0
+    counts = np.asarray(counts, dtype=np.int64)
+    rows = np.repeat(np.arange(g), counts)
+    # row r's distribution shifted to [r, r + 1]: one search for every row
+    flat = (cdf + np.arange(g, dtype=np.float64)[:, None]).reshape(-1)
+    choice = np.searchsorted(flat, rng.random(rows.size) + rows, side="right") - rows * n
+    choice = np.clip(choice, 0, n - 1)
+    uv = rng.random((rows.size, 2), dtype=np.float32)
+    su = np.sqrt(uv[:, 0])
+    b1 = (su * (1.0 - uv[:, 1])).astype(np.float32)
+    b2 = (su * uv[:, 1]).astype(np.float32)
+    tt = t[rows, choice]
+    pos = (tt[:, 0] + (tt[:, 1] - tt[:, 0]) * b1[:, None] + (tt[:, 2] - tt[:, 0]) * b2[:, None]).astype(np.float32)
+    parts = np.cumsum(counts)[:-1]
+    cols = (np.split(pos, parts), np.split(_face_normals(tt), parts), np.split(choice.astype(np.uint32), parts),
+            np.split(b1, parts), np.split(b2, parts))
+    return [tuple(c[j] for c in cols) for j in range(g)]
+
+
 def _face_normals(t):
     cr = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]).astype(np.float64)
     return (cr / np.maximum(np.linalg.norm(cr, axis=1, keepdims=True), 1e-30)).astype(np.float32)
@@ -352,6 +379,7 @@ class SurfaceProbeSiteLayout:
         tris, areas = [None] * n_inst, [None] * n_inst
         double_sided = [bool(scene_node.materials[mat_id].double_sided) for _, mat_id, _ in scene_node.instances]
         by_mesh: dict = {}
+        group_geometry: dict = {}
         for i, (mesh_id, _, _) in enumerate(scene_node.instances):
             by_mesh.setdefault(mesh_id, []).append(i)
         for mesh_id, members in by_mesh.items():
@@ -363,9 +391,23 @@ class SurfaceProbeSiteLayout:
             t = p[:, mesh.indices.astype(np.int64)].astype(np.float32)  # [g, T, 3, 3]
             e = np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0]).astype(np.float64)
             a = 0.5 * np.linalg.norm(e, axis=2)
+            group_geometry[mesh_id] = (t, a)
             for j, i in enumerate(members):
                 tris[i], areas[i] = t[j], a[j]
         mesh_lists: dict = {}  # per mesh: boundary edges and used vertices, shared by its instances
+
+        def sample_by_mesh(per_instance, salt, densities=None):
+            """Area (x density) weighted surface points of every instance, the
+            instances of one mesh drawn together from one stream."""
+            out = [None] * n_inst
+            for mesh_id, members in by_mesh.items():
+                t, a = group_geometry[mesh_id]
+                dens = None if densities is None else np.stack([densities[i] for i in members])
+                rng = np.random.default_rng([int(seed), int(mesh_id), int(salt)])
+                for i, pts in zip(members, _surface_points_group(t, a, [per_instance[i] for i in members], rng,
+                                                                 dens)):
+                    out[i] = pts
+            return out
         totals = np.array([a.sum() for a in areas])
         target = int(target_probe_count)
         minimum = min(minimum_per_instance, max(1, target // max(len(totals), 1)))
@@ -382,9 +424,11 @@ class SurfaceProbeSiteLayout:
         t_pre = time.perf_counter()
         if adaptive_wse:
             refs, ref_w, queries = [], [], []
+            n_refs = [max(1, min(int(counts[i]) * min(max(1, int(oversample_factor)), 2), 131072))
+                      for i in range(n_inst)]
+            rnds = sample_by_mesh(n_refs, 17)
             for i, (t, a) in enumerate(zip(tris, areas)):
-                n_ref = min(int(counts[i]) * min(max(1, int(oversample_factor)), 2), 131072)
-                rnd = _surface_points(t, a, max(1, n_ref), np.random.default_rng([int(seed), i, 17]))
+                rnd = rnds[i]
                 cen = _centroids(t, t.shape[0], None)
                 refs.append(_concat([rnd, cen]))
                 ref_w.append(np.concatenate([np.full(rnd[0].shape[0], 0.5 * totals[i] / rnd[0].shape[0], np.float32),
@@ -400,9 +444,8 @@ class SurfaceProbeSiteLayout:
             masses = np.array([float(np.sum(a * d.astype(np.float64))) for a, d in zip(areas, tri_density)])
             counts = allocate_counts(masses, target, minimum_per_entry=minimum)
         t_pre_end = time.perf_counter()
-        cands = [_surface_points(t, a, int(counts[i]) * max(1, int(oversample_factor)),
-                                 np.random.default_rng([int(seed), i]), tri_density[i])
-                 for i, (t, a) in enumerate(zip(tris, areas))]
+        cands = sample_by_mesh([int(counts[i]) * max(1, int(oversample_factor)) for i in range(n_inst)], 0,
+                               tri_density if adaptive_wse else None)
         offsets = np.concatenate([[0], np.cumsum([c[0].shape[0] for c in cands])]).astype(np.int64)
         cand_density = None
         if adaptive_wse:
@@ -429,6 +472,7 @@ class SurfaceProbeSiteLayout:
             # candidates those that no selected base site or earlier
             # candidate duplicates bit for bit
             sources = []
+            seconds = sample_by_mesh([int(c) for c in counts], 7919)
             for i, (t, a) in enumerate(zip(tris, areas)):
                 rng = np.random.default_rng([int(seed), i, 7919])
                 k = int(counts[i])
@@ -440,7 +484,7 @@ class SurfaceProbeSiteLayout:
                 boundary = _boundary_edges(t, mesh.indices, float(kernels[i]) * 0.5, edge_list)
                 boundary = _take(boundary, _limit(boundary[0].shape[0], max(16, k), rng))
                 sources.append(_concat([boundary, _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
-                                        _centroids(t, max(16, k), rng), cands[i], _surface_points(t, a, k, rng),
+                                        _centroids(t, max(16, k), rng), cands[i], seconds[i],
                                         _render_vertices(mesh, scene_node.transforms[transform_id], max(16, k),
                                                          rng, vertex_list)]))
             src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])

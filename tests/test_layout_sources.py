@@ -59,3 +59,24 @@ def test_render_vertices_follow_the_transform():
     _, t = _instance_triangles(node, 6)
     rebuilt = t[tri, 0] * (1 - b1 - b2)[:, None] + t[tri, 1] * b1[:, None] + t[tri, 2] * b2[:, None]
     np.testing.assert_allclose(rebuilt, pos, atol=1e-5)
+
+
+def test_group_surface_sampling():
+    """Instances of one mesh sampled together: exact per-instance counts,
+    points on their own triangles, triangles drawn in proportion to area x
+    density."""
+    from nan_b200.surface_probe_layout import _surface_points_group
+
+    base = np.float32([[[0, 0, 0], [1, 0, 0], [0, 0, 1]], [[1, 0, 0], [3, 0, 0], [1, 0, 2]]])  # areas 0.5, 2
+    t = np.stack([base, base * 2.0, base + np.float32([5, 1, 0])])
+    areas = 0.5 * np.linalg.norm(np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0]), axis=2)
+    dens = np.array([[1.0, 1.0], [1.0, 1.0], [4.0, 1.0]])
+    counts = [20000, 5, 20000]
+    out = _surface_points_group(t, areas, counts, np.random.default_rng(3), dens)
+    for j, (pos, nrm, tri, b1, b2) in enumerate(out):
+        assert pos.shape[0] == counts[j]
+        rebuilt = (t[j, tri, 0] * (1 - b1 - b2)[:, None] + t[j, tri, 1] * b1[:, None] + t[j, tri, 2] * b2[:, None])
+        np.testing.assert_allclose(rebuilt, pos, atol=1e-5)
+        np.testing.assert_allclose(np.abs(nrm[:, 1]), 1.0)
+    assert abs((out[0][2] == 0).mean() - 0.2) < 0.02  # 0.5 / 2.5
+    assert abs((out[2][2] == 0).mean() - 0.5) < 0.02  # 4 x 0.5 / (2 + 2)
