@@ -494,8 +494,9 @@ class SurfaceProbeSiteLayout:
                 flat(sources, 0), flat(sources, 1), flat(cands, 0), flat(cands, 1), base_sel,
                 audit_cell_size=(kernels.astype(np.float64) * 0.5), normal_cosine_threshold=ncos,
                 candidate_sets=inst_of(sources), base_sets=inst_of(cands))
-            split = lambda idx: [idx[(idx >= src_starts[i]) & (idx < src_starts[i + 1])] - src_starts[i]
-                                 for i in range(len(sources))]
+            def split(idx):  # ascending global indices -> per-instance local ones
+                b = np.searchsorted(idx, src_starts)
+                return [idx[b[i]:b[i + 1]] - src_starts[i] for i in range(len(sources))]
             audits = [_take(sources[i], ix) for i, ix in enumerate(split(filt.audit_indices))]
             repairs = [_take(sources[i], ix) for i, ix in enumerate(split(filt.repair_indices))]
             result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
@@ -505,8 +506,9 @@ class SurfaceProbeSiteLayout:
             chosen = np.sort(result.selected_candidate_indices)
             repair_inst = inst_of(repairs)[chosen]
             repair_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in repairs])])
-            for i in np.unique(repair_inst):
-                local = chosen[repair_inst == i] - repair_starts[i]
+            rb = np.searchsorted(repair_inst, np.arange(n_inst + 1))  # chosen is sorted, so by instance
+            for i in np.flatnonzero(np.diff(rb)):
+                local = chosen[rb[i]:rb[i + 1]] - repair_starts[i]
                 sites[i] = _concat([sites[i], _take(repairs[i], local)])
                 flags[i] = np.concatenate([flags[i], np.zeros(local.shape[0], np.uint32)])
             repaired = int(chosen.shape[0])
@@ -527,8 +529,9 @@ class SurfaceProbeSiteLayout:
                     min_gather_count=repair_min_gather, max_repair_count=int(offers.shape[0]),
                     normal_cosine_threshold=ncos)
                 picked = np.sort(closure.selected_candidate_indices)
-                for i in np.unique(prot_inst[picked]):
-                    local = picked[prot_inst[picked] == i]
+                pb = np.searchsorted(prot_inst[picked], np.arange(n_inst + 1))  # offers follow the instances
+                for i in np.flatnonzero(np.diff(pb)):
+                    local = picked[pb[i]:pb[i + 1]]
                     sites[i] = _concat([sites[i], tuple(x[local] for x in prot)])
                     flags[i] = np.concatenate([flags[i], np.full(local.shape[0], SURFACE_PROBE_FLAG_PROTECTED,
                                                                  np.uint32)])
