@@ -109,6 +109,95 @@ def _surface_points_group(t, areas, counts, rng, densities=None):
     return [tuple(c[j] for c in cols) for j in range(g)]
 
 
+def _limit_rows(row_sizes, caps, rng):
+    """Per row r of a ragged list (row_sizes[r] items, rows back to back), at
+    most caps[r] items drawn at random (all when they fit), as ascending flat
+    indices: _limit for many rows at once."""
+    row_sizes = np.asarray(row_sizes, dtype=np.int64)
+    total = int(row_sizes.sum())
+    if total == 0:
+        return np.zeros(0, np.int64)
+    row = np.repeat(np.arange(row_sizes.shape[0]), row_sizes)
+    order = np.lexsort((rng.random(total), row))
+    starts = np.concatenate([[0], np.cumsum(row_sizes)[:-1]])
+    rank = np.arange(total) - starts[row[order]]
+    return np.sort(order[rank < np.asarray(caps, dtype=np.int64)[row[order]]])
+
+
+def _audit_sources_group(t, mesh, mats, kernels, caps, edge_list, vertex_list, rng):
+    """Boundary-edge points, inset corners, centroids and render vertices of
+    the g instances of one mesh at once (t f32[g, T, 3, 3], mats their
+    transforms, kernels and caps per instance); one random stream for the
+    group. Returns, per instance, the four point sets as 5-tuples."""
+    g, n_tri = t.shape[0], t.shape[1]
+    corners = np.array([[0, 1], [1, 2], [2, 0]])
+    out = [[] for _ in range(g)]
+
+    def emit(pos, nrm, tri, b1, b2, row):
+        bounds = np.searchsorted(row, np.arange(g + 1))
+        for j in range(g):
+            sl = slice(bounds[j], bounds[j + 1])
+            out[j].append((pos[sl], nrm[sl], tri[sl], b1[sl], b2[sl]))
+
+    # boundary-edge segment midpoints, spacing R / 2 per instance
+    face, local = edge_list
+    if face.size:
+        a, b = corners[local, 0], corners[local, 1]
+        p0, p1 = t[:, face, a], t[:, face, b]  # [g, E, 3]
+        spacing = np.maximum(np.asarray(kernels, dtype=np.float64) * 0.5, 1e-8)
+        seg = np.maximum(np.ceil(np.linalg.norm(p1 - p0, axis=2) / spacing[:, None]).astype(np.int64), 1)
+        flat_seg = seg.reshape(-1)
+        edge_of = np.repeat(np.arange(flat_seg.size), flat_seg)  # (instance, edge) per segment
+        first = np.concatenate([[0], np.cumsum(flat_seg)[:-1]])
+        u = ((np.arange(edge_of.size) - first[edge_of]).astype(np.float32) + np.float32(0.5)) / \
+            flat_seg[edge_of].astype(np.float32)
+        keep = _limit_rows(seg.sum(axis=1), caps, rng)
+        edge_of, u = edge_of[keep], u[keep]
+        row, e = edge_of // face.size, edge_of % face.size
+        pos = (p0[row, e] * (1.0 - u[:, None]) + p1[row, e] * u[:, None]).astype(np.float32)
+        bary = np.zeros((keep.size, 3), np.float32)
+        bary[np.arange(keep.size), a[e]] = 1.0 - u
+        bary[np.arange(keep.size), b[e]] = u
+        emit(pos, _face_normals(t[row, face[e]]), face[e].astype(np.uint32), bary[:, 1], bary[:, 2], row)
+    else:
+        emit(*(np.zeros((0, 3), np.float32),) * 2, np.zeros(0, np.uint32), *(np.zeros(0, np.float32),) * 2,
+             np.zeros(0, np.int64))
+    # inset corners (R / 20 inside the face)
+    keep = _limit_rows(np.full(g, 3 * n_tri), caps, rng)
+    row, c = keep // (3 * n_tri), keep % (3 * n_tri)
+    tri, corner = c // 3, c % 3
+    ts = t[row, tri]
+    edges = np.stack([np.linalg.norm(ts[:, 1] - ts[:, 0], axis=1), np.linalg.norm(ts[:, 2] - ts[:, 1], axis=1),
+                      np.linalg.norm(ts[:, 0] - ts[:, 2], axis=1)], axis=1)
+    inset_d = (np.asarray(kernels, dtype=np.float64) * 0.05)[row]
+    inset = np.clip(inset_d / np.maximum(edges.max(axis=1), 1e-8), 1e-4, 0.1).astype(np.float32)
+    bary = np.repeat(inset[:, None], 3, axis=1)
+    bary[np.arange(keep.size), corner] = 1.0 - 2.0 * inset
+    emit(np.einsum("ni,nij->nj", bary, ts).astype(np.float32), _face_normals(ts), tri.astype(np.uint32),
+         bary[:, 1], bary[:, 2], row)
+    # centroids
+    keep = _limit_rows(np.full(g, n_tri), caps, rng)
+    row, tri = keep // n_tri, keep % n_tri
+    ts = t[row, tri]
+    third = np.full(keep.size, 1.0 / 3.0, np.float32)
+    emit(ts.mean(axis=1, dtype=np.float32), _face_normals(ts), tri.astype(np.uint32), third, third, row)
+    # render vertices with their transformed normals
+    verts, first_slot = vertex_list
+    keep = _limit_rows(np.full(g, verts.size), caps, rng)
+    row, v = keep // verts.size, keep % verts.size
+    m = np.asarray(mats, dtype=np.float64)
+    vp = mesh.vertices[verts[v], :3].astype(np.float64)
+    vn = mesh.vertices[verts[v], 3:6].astype(np.float64)
+    pos = (np.einsum("nk,njk->nj", vp, m[row, :3, :3]) + m[row, :3, 3]).astype(np.float32)
+    inv = np.linalg.inv(m[:, :3, :3])
+    nrm = np.einsum("nk,nkj->nj", vn, inv[row]).astype(np.float32)
+    nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-20)
+    slot = first_slot[v]
+    emit(pos, nrm, (slot // 3).astype(np.uint32), (slot % 3 == 1).astype(np.float32),
+         (slot % 3 == 2).astype(np.float32), row)
+    return out
+
+
 def _face_normals(t):
     cr = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]).astype(np.float64)
     return (cr / np.maximum(np.linalg.norm(cr, axis=1, keepdims=True), 1e-30)).astype(np.float32)
@@ -394,7 +483,6 @@ class SurfaceProbeSiteLayout:
             group_geometry[mesh_id] = (t, a)
             for j, i in enumerate(members):
                 tris[i], areas[i] = t[j], a[j]
-        mesh_lists: dict = {}  # per mesh: boundary edges and used vertices, shared by its instances
 
         def sample_by_mesh(per_instance, salt, densities=None):
             """Area (x density) weighted surface points of every instance, the
@@ -471,22 +559,19 @@ class SurfaceProbeSiteLayout:
             # one audit point per cell of R/2 and normal cone, and as repair
             # candidates those that no selected base site or earlier
             # candidate duplicates bit for bit
-            sources = []
             seconds = sample_by_mesh([int(c) for c in counts], 7919)
-            for i, (t, a) in enumerate(zip(tris, areas)):
-                rng = np.random.default_rng([int(seed), i, 7919])
-                k = int(counts[i])
-                mesh_id, _, transform_id = scene_node.instances[i]
+            sources = [None] * n_inst
+            for mesh_id, members in by_mesh.items():
                 mesh = scene_node.meshes[mesh_id]
-                if mesh_id not in mesh_lists:
-                    mesh_lists[mesh_id] = (_boundary_edge_list(mesh.indices), _vertex_list(mesh))
-                edge_list, vertex_list = mesh_lists[mesh_id]
-                boundary = _boundary_edges(t, mesh.indices, float(kernels[i]) * 0.5, edge_list)
-                boundary = _take(boundary, _limit(boundary[0].shape[0], max(16, k), rng))
-                sources.append(_concat([boundary, _inset_corners(t, float(kernels[i]) * 0.05, max(16, k), rng),
-                                        _centroids(t, max(16, k), rng), cands[i], seconds[i],
-                                        _render_vertices(mesh, scene_node.transforms[transform_id], max(16, k),
-                                                         rng, vertex_list)]))
+                mats = np.stack([np.asarray(scene_node.transforms[scene_node.instances[i][2]], dtype=np.float64)
+                                 for i in members])
+                parts = _audit_sources_group(group_geometry[mesh_id][0], mesh, mats, kernels[members],
+                                             np.maximum(16, counts[members]), _boundary_edge_list(mesh.indices),
+                                             _vertex_list(mesh),
+                                             np.random.default_rng([int(seed), int(mesh_id), 7919, 1]))
+                for j, i in enumerate(members):
+                    boundary, inset, centroid, vertices = parts[j]
+                    sources[i] = _concat([boundary, inset, centroid, cands[i], seconds[i], vertices])
             src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])
             base_sel = np.concatenate([np.flatnonzero(keep[offsets[i]:offsets[i + 1]]) + offsets[i]
                                        for i in range(len(cands))])

@@ -80,3 +80,31 @@ def test_group_surface_sampling():
         np.testing.assert_allclose(np.abs(nrm[:, 1]), 1.0)
     assert abs((out[0][2] == 0).mean() - 0.2) < 0.02  # 0.5 / 2.5
     assert abs((out[2][2] == 0).mean() - 0.5) < 0.02  # 4 x 0.5 / (2 + 2)
+
+
+def test_group_audit_sources_equal_per_instance_helpers():
+    """With caps above every count (nothing drawn at random) the grouped
+    sources equal the per-instance helpers, instance by instance."""
+    from nan_b200.scene_node import Mesh
+    from nan_b200.scenes import make_transform
+    from nan_b200.surface_probe_layout import (_audit_sources_group, _boundary_edge_list, _boundary_edges,
+                                               _centroids, _inset_corners, _render_vertices, _vertex_list)
+
+    mesh = Mesh.cube((1.0, 2.0, 0.5))
+    mats = np.stack([make_transform((1.0, 0.0, 2.0), (0.0, 0.3, 0.0), (1.0, 1.0, 1.0)),
+                     make_transform((-3.0, 1.0, 0.0), (0.2, 0.0, 0.1), (0.5, 2.0, 1.5)),
+                     make_transform((0.0, 0.0, 0.0))]).astype(np.float64)
+    p = np.einsum("vk,gjk->gvj", mesh.vertices[:, :3].astype(np.float64), mats[:, :3, :3]) + mats[:, None, :3, 3]
+    t = p[:, mesh.indices.astype(np.int64)].astype(np.float32)
+    kernels = np.float32([0.3, 0.7, 0.2])
+    caps = np.full(3, 10 ** 6)
+    parts = _audit_sources_group(t, mesh, mats, kernels, caps, _boundary_edge_list(mesh.indices), _vertex_list(mesh),
+                                 np.random.default_rng(0))
+    for j in range(3):
+        expect = [_boundary_edges(t[j], mesh.indices, float(kernels[j]) * 0.5),
+                  _inset_corners(t[j], float(kernels[j]) * 0.05, 10 ** 6, None),
+                  _centroids(t[j], 10 ** 6, None),
+                  _render_vertices(mesh, mats[j], 10 ** 6, None)]
+        for got, ref in zip(parts[j], expect):
+            for a, b in zip(got, ref):
+                np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-6)
