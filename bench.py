@@ -464,10 +464,9 @@ def run_nan(args):
         line["batched_probes"] = dict(batch_eval.measure(device, count=64, seed=1, samples_per_probe=64,
                                                          max_bounces=3, frames=2),
                                       workload="64 seeded terrain+box scenes, triangles log-uniform 1e3-5e5, "
-                                               "site targets U{512..20480} placed as the reference places "
-                                               "them (density prepass, adaptive elimination of 5x oversampled "
-                                               "candidates, 30 % repair, protected closure), 64 spp, 3 bounces, "
-                                               "compensated running means")
+                                               "sites U{512..20480} per scene placed by the reference's adaptive "
+                                               "weighted sample elimination of 5x oversampled candidates (no "
+                                               "repair sites), 64 spp, 3 bounces, compensated running means")
     print(json.dumps(line))
 
 

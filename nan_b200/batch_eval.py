@@ -50,7 +50,10 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     for i, (node, n_sites) in enumerate(sc.batch_scenes(count, seed, tri_max=tri_max)):
         scene = Scene(device, node)
         prof: dict = {}
-        layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=seed + i, profile=prof)
+        # the config's sites: the adaptive elimination's output at the scene's
+        # target, without repair or closure sites
+        layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=seed + i, repair_min_gather=0,
+                                                  profile=prof)
         for k in placement:
             placement[k] += prof.get(k, 0)
         geometry = SurfaceProbeGpuGeometry.create(device, layout)
@@ -133,10 +136,9 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
         "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
         "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
         "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
-        "setup_s": setup_s, "site_placement": dict(placement, method="the reference's default placement on the GPU: "
-                                                                   "density prepass, adaptive weighted sample "
-                                                                   "elimination of 5x oversampled candidates, "
-                                                                   "budgeted deficit repair, protected closure"),
+        "setup_s": setup_s, "site_placement": dict(placement, method="the reference's adaptive weighted sample "
+                                                                   "elimination on the GPU (density prepass, 5x "
+                                                                   "oversampled candidates), no repair sites"),
         "autotune": tuned, "autotune_independent_samples": tuned_ind, "autotune_wavefront": tuned_wf,
         "autotune_wavefront_independent_samples": tuned_wfi,
         "ms_per_frame": {"per_scene_wavefront": per_scene_ms, "per_scene_megakernel": per_scene_mk_ms,
@@ -184,7 +186,8 @@ def main() -> None:
     for i, (node, n_sites) in enumerate(sc.batch_scenes(a.count, 1)):
         scene = Scene(device, node)
         geometry = SurfaceProbeGpuGeometry.create(
-            device, SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=1 + i))
+            device, SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=1 + i,
+                                                     repair_min_gather=0))
         baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=64, max_bounces=3,
                                                    compensated=True)
         rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)

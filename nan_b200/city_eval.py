@@ -1,8 +1,8 @@
 """One frame of the large workload on the seeded 4.16 M-triangle city
 (scenes.city): the screen at 3840x2160 with 4 spp and 5 path vertices (the
 learned-cache path tracer, and the plain one for comparison), a 20,480-site
-surface-probe pass (sites by weighted sample elimination of 5x oversampled
-candidates on the GPU; 64 spp, 3 bounces, compensated sums, batched launch
+surface-probe pass (sites by the adaptive weighted sample elimination of 5x
+oversampled candidates on the GPU, no repair sites; 64 spp, 3 bounces, compensated sums, batched launch
 with one RNG stream per sample, one wavefront path per probe and sample) and
 a Mesh Colors texel pass over the whole city (about 12.6 M texels, 1 sample,
 3 bounces). Every pass is timed with CUDA events on the launching stream
@@ -42,8 +42,10 @@ def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp:
     host_s = time.perf_counter() - t0
     t1 = time.perf_counter()
     placement: dict = {}
+    # the config's 20,480 sites: the adaptive elimination's output, without
+    # repair or closure sites
     sites = SurfaceProbeSiteLayout.build_wse(node, 20480, sampler=SurfaceProbeSampler(device), seed=1,
-                                             profile=placement)
+                                             repair_min_gather=0, profile=placement)
     placement["total_s"] = time.perf_counter() - t1
     info = scene.info()
     rd = RenderData(device)
