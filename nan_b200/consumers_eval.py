@@ -1,8 +1,9 @@
 """Timing of the passes that consume the accumulated caches, on the
 texel-tracer workload's scene and slots: Mesh Colors resolve (16-byte slots
 and RGB9E5), the RGB9E5 pack, one surface-filter pass over every slot, and
-on 20,480 probe sites placed on the same scene by weighted sample
-elimination of 5x oversampled candidates: the irradiance and PRT L2
+on a probe layout of the same scene built as the reference builds it
+(adaptive weighted sample elimination of 5x oversampled candidates for
+20,480 sites, deficit repair, protected closure): the irradiance and PRT L2
 bakers (16 spp, 3 bounces), the PRT evaluation and the probe resolve. Every
 pass runs once untimed, then `frames` times between CUDA events on the
 launching stream; rates are per second of that device time.
