@@ -240,6 +240,14 @@ __global__ void k_oct_leaf_keys(const unsigned long long* keys, const uint32_t* 
     if (q < n) leaf_key[idx[q]] = keys[q] & prefix_mask(leaf_l[q]);
 }
 
+// The emit offset at each set's first point (the set's first node entry),
+// gathered so the host reads all of them in one copy.
+__global__ void k_oct_set_firsts(uint32_t sets, const uint32_t* set_offsets, const uint32_t* emit_off,
+                                 uint32_t* out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k <= sets) out[k] = emit_off[set_offsets[k]];
+}
+
 __global__ void k_oct_iota(uint32_t n, uint32_t* v) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
@@ -264,11 +272,9 @@ int launch_build_point_octrees(NanContext* ctx, const float* positions, const ui
                                uint32_t node_capacity, uint32_t* node_offsets, uint32_t* order, double* roots,
                                cudaStream_t st) {
     const uint32_t n = set_offsets[set_count];
-    std::vector<uint32_t> set_of_host(n), begin_host(set_count);
-    for (uint32_t k = 0; k < set_count; ++k) {
-        begin_host[k] = set_offsets[k];
+    std::vector<uint32_t> set_of_host(n);
+    for (uint32_t k = 0; k < set_count; ++k)
         for (uint32_t i = set_offsets[k]; i < set_offsets[k + 1]; ++i) set_of_host[i] = k;
-    }
     std::vector<void*> owned;
     cudaError_t e = cudaSuccess;
     auto get = [&](size_t bytes) -> void* {
@@ -282,7 +288,8 @@ int launch_build_point_octrees(NanContext* ctx, const float* positions, const ui
         owned.clear();
     };
     uint32_t* set_of = (uint32_t*)get(n * 4ull);
-    uint32_t* set_begin = (uint32_t*)get(set_count * 4ull);
+    uint32_t* set_begin = (uint32_t*)get((set_count + 1) * 4ull);  // set_offsets on the device
+    uint32_t* firsts = (uint32_t*)get((set_count + 1) * 4ull);
     unsigned int* lo = (unsigned int*)get(set_count * 12ull);
     unsigned int* hi = (unsigned int*)get(set_count * 12ull);
     double4* root_dev = (double4*)get(set_count * sizeof(double4));
@@ -305,7 +312,7 @@ int launch_build_point_octrees(NanContext* ctx, const float* positions, const ui
         return cuda_fail(e, "octree scratch");
     }
     cudaMemcpyAsync(set_of, set_of_host.data(), n * 4ull, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(set_begin, begin_host.data(), set_count * 4ull, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(set_begin, set_offsets, (set_count + 1) * 4ull, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(lo, 0xff, set_count * 12ull, st);
     cudaMemsetAsync(hi, 0x00, set_count * 12ull, st);
     cudaMemsetAsync(status, 0, sizeof(int), st);
@@ -321,8 +328,8 @@ int launch_build_point_octrees(NanContext* ctx, const float* positions, const ui
     // node counts: the total and, per set, the first entry (the emit offset of its first point)
     std::vector<uint32_t> emit_host(set_count + 1);
     int host_status = 0;
-    for (uint32_t k = 0; k <= set_count; ++k)
-        cudaMemcpyAsync(&emit_host[k], emit_off + set_offsets[k], 4, cudaMemcpyDeviceToHost, st);
+    k_oct_set_firsts<<<blocks(set_count + 1, 256), 256, 0, st>>>(set_count, set_begin, emit_off, firsts);
+    cudaMemcpyAsync(emit_host.data(), firsts, (set_count + 1) * 4ull, cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess || host_status) {
