@@ -28,6 +28,7 @@ protected closure is not applied.
 
 from __future__ import annotations
 
+import dataclasses
 import math
 from dataclasses import dataclass
 
@@ -322,6 +323,33 @@ class SurfaceProbeSiteLayout:
     instance_infos: tuple
     total_probe_count: int
     max_density_multiplier: float
+    # build statistics under the reference's SurfaceProbeLayout names
+    # (surface_probes.py:1490-1533); build_wse fills them
+    target_surface_site_count: int = 0
+    total_base_surface_site_count: int = 0
+    total_repair_surface_site_count: int = 0
+    total_protected_surface_site_count: int = 0
+    repair_surface_site_budget: int = 0
+    total_surface_site_count: int = 0
+    total_candidate_count: int = 0
+    total_audit_point_count: int = 0
+    zero_gather_before: int = 0
+    zero_gather_after_repair: int = 0
+    zero_gather_after: int = 0
+    deficit_point_count_before: int = 0
+    deficit_point_count_after_repair: int = 0
+    deficit_point_count_after: int = 0
+    ess_p50_before: float = 0.0
+    ess_p50_after: float = 0.0
+    support_f_p10: float = 0.0
+    support_f_p50: float = 0.0
+    density_m_p95: float = 0.0
+    adaptive_wse: bool = False
+    total_surface_area: float = 0.0
+    total_vertex_anchor_site_count: int = 0
+    total_vertex_anchor_probe_count: int = 0
+    oversample_factor: int = 0
+    seed: int = 0
 
     @classmethod
     def from_sites(cls, scene_node, probes, *, leaf_capacity: int = 8, max_depth: int = 16,
@@ -552,6 +580,7 @@ class SurfaceProbeSiteLayout:
         # kernel radius per instance, fixed before the repair as the reference does
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
+        stats: dict = {}
         if repair_min_gather > 0:
             # audit source per instance (surface_probes.py:2026-2180): boundary
             # edge points, inset corners, centroids, every base candidate, a
@@ -622,6 +651,15 @@ class SurfaceProbeSiteLayout:
                                                                  np.uint32)])
                 protected = int(picked.shape[0])
                 closure_after[short] = closure.counts_after
+            stats.update(total_audit_point_count=int(result.counts_before.shape[0]),
+                         zero_gather_before=int((result.counts_before == 0).sum()),
+                         zero_gather_after_repair=int((result.counts_after == 0).sum()),
+                         zero_gather_after=int((closure_after == 0).sum()),
+                         deficit_point_count_before=int((result.counts_before < repair_min_gather).sum()),
+                         deficit_point_count_after_repair=int((result.counts_after < repair_min_gather).sum()),
+                         deficit_point_count_after=int((closure_after < repair_min_gather).sum()),
+                         ess_p50_before=float(np.median(result.ess_before)) if result.ess_before.size else 0.0,
+                         ess_p50_after=float(np.median(result.ess_after)) if result.ess_after.size else 0.0)
             if profile is not None:
                 profile.update(repair_sites=repaired, protected_sites=protected,
                                audits=int(result.counts_before.shape[0]),
@@ -686,6 +724,19 @@ class SurfaceProbeSiteLayout:
                                 normal_angle_degrees=normal_angle_degrees,
                                 max_density_multiplier=max_density_multiplier, vertex_anchors=anchors,
                                 sampler=sampler, **kwargs)
+        n_anchor_sites = sum(int(a[2]) for a in anchors) if anchors else 0
+        layout = dataclasses.replace(
+            layout, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
+            total_repair_surface_site_count=repaired, total_protected_surface_site_count=protected,
+            repair_surface_site_budget=budget if repair_min_gather > 0 else 0,
+            total_surface_site_count=int(sum(x[0].shape[0] for x in sites)), total_candidate_count=int(offsets[-1]),
+            support_f_p10=float(np.percentile(support, 10)) if support.size else 0.0,
+            support_f_p50=float(np.median(support)) if support.size else 0.0,
+            density_m_p95=float(np.percentile(density, 95)) if density.size else 0.0,
+            adaptive_wse=bool(adaptive_wse), total_surface_area=float(totals.sum()),
+            total_vertex_anchor_site_count=n_anchor_sites,
+            total_vertex_anchor_probe_count=int(sum(a[0].shape[0] for a in anchors)) if anchors else 0,
+            oversample_factor=int(oversample_factor), seed=int(seed), **stats)
         if profile is not None:
             profile.update(density_prepass_s=t_pre_end - t_pre, adaptive=bool(adaptive_wse),
                            candidates_s=t1 - t0, elimination_s=t2 - t1, repair_s=t3 - t2, support_s=t4 - t3,

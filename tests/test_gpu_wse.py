@@ -195,6 +195,8 @@ def test_adaptive_layout_reallocates_without_changing_base_budget(device):
                                                adaptive_wse=False, device=device, profile=pu)
     assert pa["adaptive"] and not pu["adaptive"]
     assert pa["base_sites"] == 80 and pu["base_sites"] == 80
+    assert adaptive.adaptive_wse and not uniform.adaptive_wse
+    assert adaptive.total_base_surface_site_count == 80 and uniform.total_base_surface_site_count == 80
     counts = lambda layout: [info.surface_site_count for info in layout.instance_infos]
     print("adaptive", counts(adaptive), "uniform", counts(uniform))
     assert counts(adaptive) != counts(uniform)
@@ -250,5 +252,12 @@ def test_protected_closure_eliminates_unbudgeted_gather_deficits(device):
     assert prof["protected_sites"] <= 4 * prof["audits_below_min_after_repair"]
     protected = (layout.probes["meta"][:, 3] & SURFACE_PROBE_FLAG_PROTECTED) != 0
     assert protected.any()
+    # the reference's layout statistics (test_surface_probes.py:1010-1022)
+    assert layout.total_repair_surface_site_count == 0
+    assert layout.zero_gather_after_repair > 0 and layout.deficit_point_count_after_repair > 0
+    assert layout.total_protected_surface_site_count == prof["protected_sites"] > 0
+    assert layout.zero_gather_after == 0 and layout.deficit_point_count_after == 0
+    assert layout.total_protected_surface_site_count <= layout.deficit_point_count_after_repair * 4
+    assert layout.total_surface_site_count == 8 + layout.total_protected_surface_site_count
     again = SurfaceProbeSiteLayout.build_wse(node, 8, **options)
     np.testing.assert_array_equal(again.probes, layout.probes)
