@@ -312,6 +312,15 @@ class SurfaceProbeSiteInstance:
     surface_area: float
     surface_site_count: int
     reconstruction_probe_count: int
+    # per-instance build statistics under the reference's
+    # SurfaceProbeInstanceInfo names (surface_probes.py:131-165)
+    base_surface_site_count: int = 0
+    repair_surface_site_count: int = 0
+    protected_surface_site_count: int = 0
+    candidate_count: int = 0
+    audit_point_count: int = 0
+    vertex_anchor_site_count: int = 0
+    vertex_anchor_probe_count: int = 0
 
 
 @dataclass(frozen=True)
@@ -581,6 +590,7 @@ class SurfaceProbeSiteLayout:
         kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
                                 float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
         stats: dict = {}
+        per_repair = per_protected = per_audit = np.zeros(n_inst, np.int64)
         if repair_min_gather > 0:
             # audit source per instance (surface_probes.py:2026-2180): boundary
             # edge points, inset corners, centroids, every base candidate, a
@@ -621,6 +631,8 @@ class SurfaceProbeSiteLayout:
             repair_inst = inst_of(repairs)[chosen]
             repair_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in repairs])])
             rb = np.searchsorted(repair_inst, np.arange(n_inst + 1))  # chosen is sorted, so by instance
+            per_repair = np.diff(rb)
+            per_audit = np.array([x[0].shape[0] for x in audits], np.int64)
             for i in np.flatnonzero(np.diff(rb)):
                 local = chosen[rb[i]:rb[i + 1]] - repair_starts[i]
                 sites[i] = _concat([sites[i], _take(repairs[i], local)])
@@ -644,6 +656,7 @@ class SurfaceProbeSiteLayout:
                     normal_cosine_threshold=ncos)
                 picked = np.sort(closure.selected_candidate_indices)
                 pb = np.searchsorted(prot_inst[picked], np.arange(n_inst + 1))  # offers follow the instances
+                per_protected = np.diff(pb)
                 for i in np.flatnonzero(np.diff(pb)):
                     local = picked[pb[i]:pb[i + 1]]
                     sites[i] = _concat([sites[i], tuple(x[local] for x in prot)])
@@ -725,8 +738,14 @@ class SurfaceProbeSiteLayout:
                                 max_density_multiplier=max_density_multiplier, vertex_anchors=anchors,
                                 sampler=sampler, **kwargs)
         n_anchor_sites = sum(int(a[2]) for a in anchors) if anchors else 0
+        infos = tuple(dataclasses.replace(
+            info, base_surface_site_count=int(counts[i]), repair_surface_site_count=int(per_repair[i]),
+            protected_surface_site_count=int(per_protected[i]), candidate_count=int(cands[i][0].shape[0]),
+            audit_point_count=int(per_audit[i]), vertex_anchor_site_count=int(anchors[i][2]) if anchors else 0,
+            vertex_anchor_probe_count=int(anchors[i][0].shape[0]) if anchors else 0)
+            for i, info in enumerate(layout.instance_infos))
         layout = dataclasses.replace(
-            layout, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
+            layout, instance_infos=infos, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
             total_repair_surface_site_count=repaired, total_protected_surface_site_count=protected,
             repair_surface_site_budget=budget if repair_min_gather > 0 else 0,
             total_surface_site_count=int(sum(x[0].shape[0] for x in sites)), total_candidate_count=int(offsets[-1]),

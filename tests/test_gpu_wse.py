@@ -197,7 +197,7 @@ def test_adaptive_layout_reallocates_without_changing_base_budget(device):
     assert pa["base_sites"] == 80 and pu["base_sites"] == 80
     assert adaptive.adaptive_wse and not uniform.adaptive_wse
     assert adaptive.total_base_surface_site_count == 80 and uniform.total_base_surface_site_count == 80
-    counts = lambda layout: [info.surface_site_count for info in layout.instance_infos]
+    counts = lambda layout: [info.base_surface_site_count for info in layout.instance_infos]
     print("adaptive", counts(adaptive), "uniform", counts(uniform))
     assert counts(adaptive) != counts(uniform)
 
@@ -259,5 +259,7 @@ def test_protected_closure_eliminates_unbudgeted_gather_deficits(device):
     assert layout.zero_gather_after == 0 and layout.deficit_point_count_after == 0
     assert layout.total_protected_surface_site_count <= layout.deficit_point_count_after_repair * 4
     assert layout.total_surface_site_count == 8 + layout.total_protected_surface_site_count
+    assert sum(i.protected_surface_site_count for i in layout.instance_infos) == prof["protected_sites"]
+    assert sum(i.base_surface_site_count for i in layout.instance_infos) == 8
     again = SurfaceProbeSiteLayout.build_wse(node, 8, **options)
     np.testing.assert_array_equal(again.probes, layout.probes)
