@@ -40,6 +40,17 @@ from .surface_probe_resources import (SURFACE_PROBE_DTYPE, SURFACE_PROBE_FLAG_PR
                                       SURFACE_PROBE_INSTANCE_SHIFT)
 
 
+def allocate_density_counts(weights, density: float, *, minimum_per_entry: int = 1) -> np.ndarray:
+    """Site counts from an absolute density (_allocate_density_counts,
+    surface_probes.py:296-324): floor(weight x density + 0.5) + the floor
+    per entry; the total is an output."""
+    w = np.asarray(weights, dtype=np.float64)
+    density = float(density)
+    if not math.isfinite(density) or density <= 0.0:
+        raise ValueError("Surface probe density must be finite and positive")
+    return np.floor(w * density + 0.5).astype(np.int64) + np.int64(max(1, int(minimum_per_entry)))
+
+
 def allocate_counts(weights, total: int, *, minimum_per_entry: int = 1) -> np.ndarray:
     """Largest-remainder split of `total` by `weights` with a floor per entry
     (_allocate_counts, surface_probes.py:265-293)."""
@@ -354,7 +365,10 @@ class SurfaceProbeSiteLayout:
     support_f_p50: float = 0.0
     density_m_p95: float = 0.0
     adaptive_wse: bool = False
+    density_driven: bool = False
+    density_scale: float = 1.0
     total_surface_area: float = 0.0
+    total_adaptive_mass: float = 0.0
     total_vertex_anchor_site_count: int = 0
     total_vertex_anchor_probe_count: int = 0
     oversample_factor: int = 0
@@ -469,8 +483,9 @@ class SurfaceProbeSiteLayout:
                   seed: int = 1, minimum_per_instance: int = 4, repair_budget_ratio: float = 0.30,
                   repair_min_gather: int = 4, kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
                   adaptive_wse: bool = True, max_density_multiplier: float = 8.0,
-                  build_vertex_anchors: bool = False, sampler=None,
-                  profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
+                  build_vertex_anchors: bool = False, adaptive_mass_site_density: float | None = None,
+                  density_reference_kernel_radius: float | None = None, density_scale: float = 1.0,
+                  sampler=None, profile: dict | None = None, **kwargs) -> "SurfaceProbeSiteLayout":
         """Sites by weighted sample elimination of oversampled candidates, then
         deficit repair: audit points (filtered from boundary-edge points, inset
         corners, centroids, the candidates, a second surface sample and the
@@ -494,7 +509,14 @@ class SurfaceProbeSiteLayout:
         build_vertex_anchors (off by default, as in the reference) adds one
         anchor probe per render vertex of each instance, flagged
         SURFACE_PROBE_FLAG_VERTEX_ANCHOR and kept outside the octree, and
-        the triangle map the resolve's vertex fallback reads."""
+        the triangle map the resolve's vertex fallback reads.
+
+        Density mode (target_probe_count None, with adaptive_mass_site_density
+        and density_reference_kernel_radius; surface_probes.py:1588-1626,
+        1838-1866): the kernel radius is the reference radius /
+        sqrt(density_scale) and each instance gets floor(adaptive mass x
+        density x scale + 0.5) + repair_min_gather sites, so the total is an
+        output of the world-space density."""
         import time
 
         from .surface_probe_sampler import SurfaceProbeSampler
@@ -534,14 +556,29 @@ class SurfaceProbeSiteLayout:
                     out[i] = pts
             return out
         totals = np.array([a.sum() for a in areas])
-        target = int(target_probe_count)
-        minimum = min(minimum_per_instance, max(1, target // max(len(totals), 1)))
-        counts = allocate_counts(totals, target, minimum_per_entry=minimum)
+        density_driven = target_probe_count is None
+        if density_driven:
+            if adaptive_mass_site_density is None or density_reference_kernel_radius is None:
+                raise ValueError("Surface probes require an explicit count or density mode")
+            if not (math.isfinite(density_scale) and density_scale > 0.0 and
+                    math.isfinite(adaptive_mass_site_density) and adaptive_mass_site_density > 0.0 and
+                    math.isfinite(density_reference_kernel_radius) and density_reference_kernel_radius > 0.0):
+                raise ValueError("density mode needs finite, positive density, kernel radius and scale")
+            global_kernel = max(float(density_reference_kernel_radius) / math.sqrt(density_scale), 1e-5)
+            spacing = global_kernel / kernel_radius_scale
+            minimum = max(1, int(repair_min_gather))
+            counts = allocate_density_counts(totals, 1.0 / max(spacing * spacing, 1e-20), minimum_per_entry=minimum)
+            target = int(counts.sum())
+        else:
+            target = int(target_probe_count)
+            minimum = min(minimum_per_instance, max(1, target // max(len(totals), 1)))
+            counts = allocate_counts(totals, target, minimum_per_entry=minimum)
+            global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale,
+                                1e-5)
         if sampler is None:
             from .scene import Device
 
             sampler = SurfaceProbeSampler(device if device is not None else Device(0))
-        global_kernel = max(math.sqrt(max(float(totals.sum()), 1e-20) / max(target, 1)) * kernel_radius_scale, 1e-5)
         ncos = math.cos(math.radians(normal_angle_degrees))
         flat = lambda sets, j: np.concatenate([x[j] for x in sets])
         inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
@@ -567,7 +604,16 @@ class SurfaceProbeSiteLayout:
             starts = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])])
             tri_density = [m[starts[i]:starts[i + 1]] for i in range(len(tris))]
             masses = np.array([float(np.sum(a * d.astype(np.float64))) for a, d in zip(areas, tri_density)])
-            counts = allocate_counts(masses, target, minimum_per_entry=minimum)
+            if density_driven:
+                counts = allocate_density_counts(masses, float(adaptive_mass_site_density) * float(density_scale),
+                                                 minimum_per_entry=minimum)
+                target = int(counts.sum())
+            else:
+                counts = allocate_counts(masses, target, minimum_per_entry=minimum)
+        elif density_driven:
+            counts = allocate_density_counts(totals, float(adaptive_mass_site_density) * float(density_scale),
+                                             minimum_per_entry=minimum)
+            target = int(counts.sum())
         t_pre_end = time.perf_counter()
         cands = sample_by_mesh([int(counts[i]) * max(1, int(oversample_factor)) for i in range(n_inst)], 0,
                                tri_density if adaptive_wse else None)
@@ -752,7 +798,9 @@ class SurfaceProbeSiteLayout:
             support_f_p10=float(np.percentile(support, 10)) if support.size else 0.0,
             support_f_p50=float(np.median(support)) if support.size else 0.0,
             density_m_p95=float(np.percentile(density, 95)) if density.size else 0.0,
-            adaptive_wse=bool(adaptive_wse), total_surface_area=float(totals.sum()),
+            adaptive_wse=bool(adaptive_wse), density_driven=bool(density_driven),
+            density_scale=float(density_scale) if density_driven else 1.0, total_surface_area=float(totals.sum()),
+            total_adaptive_mass=float(masses.sum()) if adaptive_wse else float(totals.sum()),
             total_vertex_anchor_site_count=n_anchor_sites,
             total_vertex_anchor_probe_count=int(sum(a[0].shape[0] for a in anchors)) if anchors else 0,
             oversample_factor=int(oversample_factor), seed=int(seed), **stats)
@@ -777,3 +825,15 @@ class SurfaceProbeSiteLayout:
 
     def query_probe_indices(self, instance_index: int, position, radius: float | None = None, normal=None):
         return query_probe_indices(self, instance_index, position, radius, normal)
+
+
+class SurfaceProbeLayout(SurfaceProbeSiteLayout):
+    """The reference's SurfaceProbeLayout name and build signature
+    (surface_probes.py:1536-1560): build() is build_wse with the reference's
+    keywords (sampler_backend and profile_build are accepted and ignored:
+    the passes run on the GPU)."""
+
+    @classmethod
+    def build(cls, scene_node, *, target_probe_count: int | None = 8192, device=None, sampler_backend=None,
+              profile_build: bool = False, **kwargs) -> "SurfaceProbeLayout":
+        return cls.build_wse(scene_node, target_probe_count, device=device, **kwargs)

@@ -263,3 +263,26 @@ def test_protected_closure_eliminates_unbudgeted_gather_deficits(device):
     assert sum(i.base_surface_site_count for i in layout.instance_infos) == 8
     again = SurfaceProbeSiteLayout.build_wse(node, 8, **options)
     np.testing.assert_array_equal(again.probes, layout.probes)
+
+
+def test_density_mode_makes_base_population_an_output(device):
+    """test_surface_probes.py:889-914 through the reference's class name and
+    keywords: in density mode the base site count is an output, at least the
+    floor of 4 per instance, and the sum of the instances' counts; a larger
+    density scale places more sites."""
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import SurfaceProbeLayout
+
+    node = scenes.reference_demo()
+    kw = dict(target_probe_count=None, adaptive_mass_site_density=0.5, density_reference_kernel_radius=2.5,
+              oversample_factor=1, seed=7, repair_budget_ratio=0.0, device=device)
+    layout = SurfaceProbeLayout.build(node, density_scale=1.0, **kw)
+    assert isinstance(layout, SurfaceProbeLayout)
+    assert layout.density_driven and layout.density_scale == 1.0
+    assert layout.total_surface_area > 0.0 and layout.total_adaptive_mass > 0.0
+    assert layout.total_base_surface_site_count >= 4 * len(layout.instance_infos)
+    assert layout.total_base_surface_site_count == sum(i.base_surface_site_count for i in layout.instance_infos)
+    denser = SurfaceProbeLayout.build(node, density_scale=16.0, **kw)
+    assert denser.total_base_surface_site_count > layout.total_base_surface_site_count
+    with pytest.raises(ValueError):
+        SurfaceProbeLayout.build(node, target_probe_count=None, device=device)
