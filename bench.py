@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
     ap.add_argument("--e2e-chunks", type=int, default=2,
                     help="texel chunks per e2e step (copies of one chunk overlap the tracing of the others)")
+    ap.add_argument("--traversal", type=int, default=0, help="wavefront traversal form (NanTuning.traversal)")
     ap.add_argument("--ray-order", type=int, choices=[0, 1], default=0,
                     help="wavefront extend queue: 0 path order, 1 regrouped by direction octant")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -305,7 +306,7 @@ def run_nan(args):
     tracer = nan_b200.TextureSpacePathTracer(device, scene, layout, samples_per_texel=1, max_bounces=3,
                                              max_paths_in_flight=args.paths or None)
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
-                    ray_order=args.ray_order)
+                    ray_order=args.ray_order, traversal=args.traversal)
     total = layout.total_surface_texels
     begin, end = shard_range(total, rank, world)
     slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device=device.torch_device)
@@ -322,7 +323,7 @@ def run_nan(args):
     # stage timing on inside the timed region: an event pair around each
     # wavefront launch, on the launching stream
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
-                    kernel_timing=True, ray_order=args.ray_order)
+                    kernel_timing=True, ray_order=args.ray_order, traversal=args.traversal)
     scene.context.read_kernel_times(reset=True)
 
     clocks = ClockSampler(local)
@@ -348,7 +349,7 @@ def run_nan(args):
     counters = scene.context.read_counters(reset=True)
     ktimes = scene.context.read_kernel_times(reset=True)
     scene.configure(args.integrator, trace_blocks_per_sm=args.blocks_per_sm, bvh_width=args.width,
-                    ray_order=args.ray_order)
+                    ray_order=args.ray_order, traversal=args.traversal)
     device.check()
     rays_local = counters["extend_rays"] + counters["shadow_rays"]
 

@@ -196,7 +196,9 @@ typedef struct NanTuning {
                                       use under stream capture */
     uint32_t ray_order;            /* wavefront extend queue: 0 = path order, 1 = regrouped by ray
                                       direction octant before each extend launch */
-    uint32_t reserved;
+    uint32_t traversal;            /* wavefront traversal over binary nodes, same results in every
+                                      form: 0 = a warp takes 32 rays and walks until all have ended;
+                                      1-4 = idle lanes are refilled from the queue */
 } NanTuning;
 
 /* Device time of the wavefront stages since the last reset, from CUDA events

@@ -114,7 +114,7 @@ class NanTuning(ctypes.Structure):
         ("bvh_width", ctypes.c_uint32),
         ("kernel_timing", ctypes.c_uint32),
         ("ray_order", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("traversal", ctypes.c_uint32),
     ]
 
 
@@ -423,9 +423,10 @@ class Context:
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
                   max_paths_in_flight: int = 0, bvh_builder: str = "ploc", bvh_width: int = 2,
-                  kernel_timing: bool = False, ray_order: int = 0) -> None:
+                  kernel_timing: bool = False, ray_order: int = 0, traversal: int = 0) -> None:
         t = NanTuning()
         t.ray_order = int(ray_order)
+        t.traversal = int(traversal)
         t.kernel_timing = int(bool(kernel_timing))
         t.bvh_builder = BVH_BUILDERS[bvh_builder]
         t.bvh_width = 8 if int(bvh_width) == 8 else 2

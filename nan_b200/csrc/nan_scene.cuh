@@ -436,6 +436,158 @@ __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d,
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// Resumable binary walks: the state of trace_closest_binary /
+// trace_any_binary between steps, so that a persistent kernel can advance a
+// lane's ray one node (or leaf) at a time and hand a lane whose ray has ended
+// a new one while the other lanes keep walking. A step does exactly what one
+// pass of the per-lane loop does, so the hit is the same.
+// ---------------------------------------------------------------------------
+struct ClosestWalk {
+    WtRay wr;
+    BoxRay br;
+    f3 o;
+    float tmin;
+    float best_t;
+    uint32_t best_key;
+    int best_tri;
+    int node;
+    int sp;
+};
+
+// False when there is nothing to walk (empty scene).
+__device__ __forceinline__ bool closest_begin(const SceneView& s, ClosestWalk& w, f3 o, f3 d, float tmin, float tmax) {
+    w.wr = wt_setup(d);
+    w.br = box_setup(o, d);
+    w.o = o;
+    w.tmin = tmin;
+    w.best_t = tmax;
+    w.best_key = 0xffffffffu;
+    w.best_tri = -1;
+    w.node = s.root;
+    w.sp = 0;
+    return s.tri_count != 0;
+}
+
+// One node or leaf; false once the walk has ended.
+template <int kDepth>
+__device__ __forceinline__ bool closest_step(const SceneView& s, ClosestWalk& w, int* stack) {
+    if (w.node >= 0) {
+        const float4* n = s.nodes + 4 * w.node;
+        const float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+        const int4 nd = __ldg(reinterpret_cast<const int4*>(n + 3));
+        float t0, t1;
+        bool h0, h1;
+        box2(w.br, na, nb, nc, w.tmin, w.best_t, &t0, &t1, &h0, &h1);
+        if (h0 && h1) {
+            int near_child = nd.x, far_child = nd.y;
+            if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
+            if (w.sp < kDepth) stack[w.sp++] = far_child;
+            else atomicOr(s.status, kStatusStackOverflow);
+            w.node = near_child;
+            return true;
+        }
+        if (h0) { w.node = nd.x; return true; }
+        if (h1) { w.node = nd.y; return true; }
+    } else {
+        const int leaf = ~w.node;
+        const int first = leaf >> 3, last = first + (leaf & 7);
+        for (int tri = first; tri <= last; ++tri) {
+            f3 v0, v1, v2;
+            uint32_t flat;
+            load_tri(s, tri, &v0, &v1, &v2, &flat);
+            float t, V, W, det;
+            if (wt_test(w.wr, w.o, v0, v1, v2, &t, &V, &W, &det) && t >= w.tmin &&
+                (t < w.best_t || (t == w.best_t && flat < w.best_key))) {
+                w.best_t = t;
+                w.best_key = flat;
+                w.best_tri = tri;
+            }
+        }
+    }
+    if (w.sp == 0) return false;
+    w.node = stack[--w.sp];
+    return true;
+}
+
+__device__ __forceinline__ HitInfo closest_end(const SceneView& s, const ClosestWalk& w) {
+    HitInfo hit;
+    hit.valid = false;
+    hit.flat = 0xffffffffu;
+    hit.t = w.best_t;
+    hit.b1 = 0.0f;
+    hit.b2 = 0.0f;
+    if (w.best_tri >= 0) {
+        f3 v0, v1, v2;
+        uint32_t flat;
+        load_tri(s, w.best_tri, &v0, &v1, &v2, &flat);
+        float t, V, W, det;
+        wt_test(w.wr, w.o, v0, v1, v2, &t, &V, &W, &det);
+        hit.valid = true;
+        hit.flat = w.best_key;
+        hit.b1 = V / det;
+        hit.b2 = W / det;
+    }
+    return hit;
+}
+
+struct AnyWalk {
+    WtRay wr;
+    BoxRay br;
+    f3 o;
+    float tmin;
+    float tmax;
+    int node;
+    int sp;
+};
+
+__device__ __forceinline__ bool any_begin(const SceneView& s, AnyWalk& w, f3 o, f3 d, float tmin, float tmax) {
+    w.wr = wt_setup(d);
+    w.br = box_setup(o, d);
+    w.o = o;
+    w.tmin = tmin;
+    w.tmax = tmax;
+    w.node = s.root;
+    w.sp = 0;
+    return s.tri_count != 0;
+}
+
+// One node or leaf: 0 = walk on, 1 = ended without a hit, 2 = hit.
+template <int kDepth>
+__device__ __forceinline__ int any_step(const SceneView& s, AnyWalk& w, int* stack) {
+    if (w.node >= 0) {
+        const float4* n = s.nodes + 4 * w.node;
+        const float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+        const int4 nd = __ldg(reinterpret_cast<const int4*>(n + 3));
+        float t0, t1;
+        bool h0, h1;
+        box2(w.br, na, nb, nc, w.tmin, w.tmax, &t0, &t1, &h0, &h1);
+        if (h0 && h1) {
+            int near_child = nd.x, far_child = nd.y;
+            if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
+            if (w.sp < kDepth) stack[w.sp++] = far_child;
+            else atomicOr(s.status, kStatusStackOverflow);
+            w.node = near_child;
+            return 0;
+        }
+        if (h0) { w.node = nd.x; return 0; }
+        if (h1) { w.node = nd.y; return 0; }
+    } else {
+        const int leaf = ~w.node;
+        const int first = leaf >> 3, last = first + (leaf & 7);
+        for (int tri = first; tri <= last; ++tri) {
+            f3 v0, v1, v2;
+            uint32_t flat;
+            load_tri(s, tri, &v0, &v1, &v2, &flat);
+            float t, V, W, det;
+            if (wt_test(w.wr, w.o, v0, v1, v2, &t, &V, &W, &det) && t >= w.tmin && t <= w.tmax) return 2;
+        }
+    }
+    if (w.sp == 0) return 1;
+    w.node = stack[--w.sp];
+    return 0;
+}
+
 // Width-specialised entry points (kWidth 2: binary nodes, 8: compressed
 // wide nodes) and a run-time dispatch for kernels that are not specialised.
 template <int kWidth>

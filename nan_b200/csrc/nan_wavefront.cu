@@ -209,6 +209,142 @@ __global__ void __launch_bounds__(128, 10) k_wf_shadow(Src src, const float4* __
     flush_tally(counters, tally, 0u, 0u);
 }
 
+// Persistent traversal with lane refill. Each lane walks its own ray
+// (closest_step / any_step); once at least kRefill lanes of the warp are
+// idle, the warp takes that many new rays from the queue in one atomic and
+// hands them to the idle lanes, while the other lanes keep their walks.
+// Finished rays write their results in the same refill round, so ray set-up
+// and result stores run for the idle lanes together. kBurst steps run
+// between two refill checks. Without refill, a warp that took 32 rays runs
+// until the slowest of them ends.
+template <int kRefill, int kBurst, class Src>
+__global__ void __launch_bounds__(128, 10) k_wf_extend_refill(Src src, const uint32_t* __restrict__ queue,
+                                                          uint32_t* ctl, const float4* __restrict__ ro,
+                                                          const float4* __restrict__ rd,
+                                                          const uint32_t* __restrict__ flags,
+                                                          float4* __restrict__ hit, unsigned long long* counters) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 0);
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    RayTally tally{0u, 0u};
+    ClosestWalk w;
+    int stack[kTraversalStack];
+    bool alive = false, pending = false, drained = false;
+    uint32_t p = 0u;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, !alive);
+        if (drained) {
+            if (idle == 0xffffffffu) break;
+        } else if (__popc(idle) >= kRefill) {
+            if (pending) {
+                const HitInfo h = closest_end(src.of(p), w);
+                hit[p] = make_float4(__uint_as_float(h.valid ? h.flat : 0xffffffffu), h.t, h.b1, h.b2);
+                pending = false;
+            }
+            const uint32_t n = (uint32_t)__popc(idle);
+            uint32_t base = 0u;
+            if (lane == 0u) base = atomicAdd(ctl + 1, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!alive) {
+                const uint32_t idx = base + (uint32_t)__popc(idle & below);
+                if (idx < count) {
+                    p = queue[idx];
+                    if (flags[p] & kFlagNoPath) {
+                        hit[p] = make_float4(__uint_as_float(0xffffffffu), 0.0f, 0.0f, 0.0f);
+                    } else {
+                        const float4 o = ro[p], d = rd[p];
+                        tally.extend++;
+                        alive = closest_begin(src.of(p), w, xyz(o), xyz(d), o.w, d.w);
+                        pending = !alive;
+                    }
+                }
+            }
+            if (base + n >= count) drained = true;
+            continue;
+        }
+        if (alive) {
+            const SceneView& s = src.of(p);
+#pragma unroll 1
+            for (int k = 0; k < kBurst; ++k) {
+                if (!closest_step<kTraversalStack>(s, w, stack)) {
+                    alive = false;
+                    pending = true;
+                    break;
+                }
+            }
+        }
+    }
+    if (pending) {
+        const HitInfo h = closest_end(src.of(p), w);
+        hit[p] = make_float4(__uint_as_float(h.valid ? h.flat : 0xffffffffu), h.t, h.b1, h.b2);
+    }
+    flush_tally(counters, tally, 0u, 0u);
+}
+
+template <int kRefill, int kBurst, class Src>
+__global__ void __launch_bounds__(128, 10) k_wf_shadow_refill(Src src, const float4* __restrict__ queue, uint32_t* ctl,
+                                                          float t_max, float4* __restrict__ rad,
+                                                          float4* __restrict__ si, unsigned long long* counters) {
+    const uint32_t count = *(volatile uint32_t*)(ctl + 2);
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned below = (1u << lane) - 1u;
+    RayTally tally{0u, 0u};
+    AnyWalk w;
+    int stack[kTraversalStack];
+    bool alive = false, pending = false, drained = false;
+    uint32_t p = 0u, e = 0u;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, !alive);
+        if (drained) {
+            if (idle == 0xffffffffu) break;
+        } else if (__popc(idle) >= kRefill) {
+            if (pending) {  // a ray that ended without a hit adds its contribution
+                const float4 b = queue[3u * e + 1u], c = queue[3u * e + 2u];
+                float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
+                const float4 v = target[p];
+                target[p] = make_float4(v.x + c.x, v.y + c.y, v.z + c.z, v.w);
+                pending = false;
+            }
+            const uint32_t n = (uint32_t)__popc(idle);
+            uint32_t base = 0u;
+            if (lane == 0u) base = atomicAdd(ctl + 3, n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!alive) {
+                const uint32_t idx = base + (uint32_t)__popc(idle & below);
+                if (idx < count) {
+                    e = idx;
+                    const float4 a = queue[3u * idx], b = queue[3u * idx + 1u], c = queue[3u * idx + 2u];
+                    tally.shadow++;
+                    p = __float_as_uint(a.w);
+                    alive = any_begin(src.of(p), w, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
+                    pending = !alive;
+                }
+            }
+            if (base + n >= count) drained = true;
+            continue;
+        }
+        if (alive) {
+            const SceneView& s = src.of(p);
+#pragma unroll 1
+            for (int k = 0; k < kBurst; ++k) {
+                const int r = any_step<kTraversalStack>(s, w, stack);
+                if (r != 0) {
+                    alive = false;
+                    pending = r == 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (pending) {
+        const float4 b = queue[3u * e + 1u], c = queue[3u * e + 2u];
+        float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
+        const float4 v = target[p];
+        target[p] = make_float4(v.x + c.x, v.y + c.y, v.z + c.z, v.w);
+    }
+    flush_tally(counters, tally, 0u, 0u);
+}
+
 // ---------------------------------------------------------------------------
 // Texture-space integrator stages (texture_space_path_tracer.slang:57-216).
 // ---------------------------------------------------------------------------
@@ -1041,6 +1177,38 @@ template <class T> T* carve(unsigned char*& cur, size_t count) {
     return p;
 }
 
+// Traversal launches of one wavefront round: node width from the scene,
+// the traversal form from the context's tuning (NanTuning.traversal).
+template <class Src>
+void launch_extend(const NanContext* ctx, int blocks, cudaStream_t st, bool wide, Src src, const uint32_t* queue,
+                   uint32_t* ctl, const WfState& S) {
+#define NAN_EXT_ARGS src, queue, ctl, S.ro, S.rd, S.flags, S.hit, ctx->d_counters
+    if (wide) k_wf_extend<8><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS);
+    else switch (ctx->tuning.traversal) {
+        case 1: k_wf_extend_refill<8, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        case 2: k_wf_extend_refill<16, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        case 3: k_wf_extend_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        case 4: k_wf_extend_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        default: k_wf_extend<2><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+    }
+#undef NAN_EXT_ARGS
+}
+
+template <class Src>
+void launch_shadow(const NanContext* ctx, int blocks, cudaStream_t st, bool wide, Src src, const float4* queue,
+                   uint32_t* ctl, float t_max, const WfState& S) {
+#define NAN_SHD_ARGS src, queue, ctl, t_max, S.rad, S.si, ctx->d_counters
+    if (wide) k_wf_shadow<8><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS);
+    else switch (ctx->tuning.traversal) {
+        case 1: k_wf_shadow_refill<8, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        case 2: k_wf_shadow_refill<16, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        case 3: k_wf_shadow_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        case 4: k_wf_shadow_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        default: k_wf_shadow<2><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+    }
+#undef NAN_SHD_ARGS
+}
+
 struct Grid {
     int persistent_blocks;
     int stream_blocks;
@@ -1222,23 +1390,13 @@ int wf_run(NanContext* ctx, cudaStream_t st, uint64_t begin, uint64_t end, uint3
                 ctx->launches += 2;
             }
             ev = timing_begin(ctx, st);
-            if (s.wnodes)
-                k_wf_extend<8><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                                   ctx->d_counters);
-            else
-                k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                                   ctx->d_counters);
+            launch_extend(ctx, g.persistent_blocks, st, s.wnodes != nullptr, OneScene{s}, q.ext[buf], ctl, S);
             timing_end(ctx, 0, ev, st);
             ev = timing_begin(ctx, st);
             shade(S, q, buf, ctl);
             timing_end(ctx, 2, ev, st);
             ev = timing_begin(ctx, st);
-            if (s.wnodes)
-                k_wf_shadow<8><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.shd[buf], ctl, t_max, S.rad, S.si,
-                                                                   ctx->d_counters);
-            else
-                k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(OneScene{s}, q.shd[buf], ctl, t_max, S.rad, S.si,
-                                                                   ctx->d_counters);
+            launch_shadow(ctx, g.persistent_blocks, st, s.wnodes != nullptr, OneScene{s}, q.shd[buf], ctl, t_max, S);
             timing_end(ctx, 1, ev, st);
             ev = timing_begin(ctx, st);
             fin(S, q, buf, ctl, ctl + 4);
@@ -1443,11 +1601,9 @@ int launch_batch_wavefront(NanContext* ctx, const void* sets, const uint32_t* pr
     for (uint32_t it = 0; it < iters; ++it) {
         const int buf = (int)(it & 1u);
         uint32_t* ctl = q.ctl + 4u * it;
-        k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                           ctx->d_counters);
+        launch_extend(ctx, g.persistent_blocks, st, false, src, q.ext[buf], ctl, S);
         k_wfb_probe_shade<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl);
-        k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.shd[buf], ctl, t_max, S.rad, S.si,
-                                                           ctx->d_counters);
+        launch_shadow(ctx, g.persistent_blocks, st, false, src, q.shd[buf], ctl, t_max, S);
         k_wfb_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl, ctl + 4);
         ctx->launches += 4;
     }
@@ -1496,11 +1652,9 @@ int launch_batch_wavefront_independent(NanContext* ctx, const void* sets, const 
         for (uint32_t it = 0; it < iters; ++it) {
             const int buf = (int)(it & 1u);
             uint32_t* ctl = q.ctl + 4u * it;
-            k_wf_extend<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.ext[buf], ctl, S.ro, S.rd, S.flags, S.hit,
-                                                               ctx->d_counters);
+            launch_extend(ctx, g.persistent_blocks, st, false, src, q.ext[buf], ctl, S);
             k_wfb_probe_shade<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl);
-            k_wf_shadow<2><<<g.persistent_blocks, 128, 0, st>>>(src, q.shd[buf], ctl, t_max, S.rad, S.si,
-                                                               ctx->d_counters);
+            launch_shadow(ctx, g.persistent_blocks, st, false, src, q.shd[buf], ctl, t_max, S);
             k_wfi_probe_finalize<<<g.stream_blocks, 128, 0, st>>>(m, S, q, buf, ctl, ctl + 4);
         }
         k_wfi_probe_fold<<<(m.units + 127) / 128, 128, 0, st>>>(m, ctx->d_counters);

@@ -156,7 +156,7 @@ class Scene:
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
                   max_paths_in_flight: int = 0, bvh_width: int = 2, kernel_timing: bool = False,
-                  ray_order: int = 0) -> None:
+                  ray_order: int = 0, traversal: int = 0) -> None:
         """Integrator form for passes on this scene: "wavefront" (default) or
         "megakernel" (one thread per pixel/texel/probe), launch shapes, the
         traversed node width (2: binary, the default; 8: compressed wide nodes),
@@ -164,7 +164,7 @@ class Scene:
         the wavefront's ray order (1: extend queue regrouped by direction
         octant)."""
         self._context.configure(integrator, trace_blocks_per_sm, max_paths_in_flight, self.bvh_builder, bvh_width,
-                                kernel_timing, ray_order)
+                                kernel_timing, ray_order, traversal)
 
     def area_light_table(self):
         """(f32[L, 16], power): every emissive triangle of the scene in world
