@@ -198,7 +198,8 @@ typedef struct NanTuning {
                                       direction octant before each extend launch */
     uint32_t traversal;            /* wavefront traversal over binary nodes, same results in every
                                       form: 0 = a warp takes 32 rays and walks until all have ended;
-                                      1-4 = idle lanes are refilled from the queue */
+                                      1-4 = idle lanes are refilled from the queue;
+                                      5 = stack top in shared memory */
 } NanTuning;
 
 /* Device time of the wavefront stages since the last reset, from CUDA events

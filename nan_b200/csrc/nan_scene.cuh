@@ -150,6 +150,19 @@ __device__ __forceinline__ BoxRay box_setup(f3 o, f3 d) {
     return b;
 }
 
+// Three-input float min / max (PTX min.f32 / max.f32 with three sources,
+// sm_100 and later). Both are exact, so any grouping gives the same value.
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 __device__ __forceinline__ void box2(const BoxRay& r, float4 na, float4 nb, float4 nc, float tmin, float tmax,
                                      float* t0, float* t1, bool* h0, bool* h1) {
     const float x0a = __fmaf_rn(na.x, r.ix, -r.ox), x0b = __fmaf_rn(na.y, r.ix, -r.ox);
@@ -158,10 +171,10 @@ __device__ __forceinline__ void box2(const BoxRay& r, float4 na, float4 nb, floa
     const float x1a = __fmaf_rn(nb.x, r.ix, -r.ox), x1b = __fmaf_rn(nb.y, r.ix, -r.ox);
     const float y1a = __fmaf_rn(nb.z, r.iy, -r.oy), y1b = __fmaf_rn(nb.w, r.iy, -r.oy);
     const float z1a = __fmaf_rn(nc.z, r.iz, -r.oz), z1b = __fmaf_rn(nc.w, r.iz, -r.oz);
-    const float lo0 = fmaxf(fmaxf(fminf(x0a, x0b), fminf(y0a, y0b)), fmaxf(fminf(z0a, z0b), tmin));
-    const float hi0 = fminf(fminf(fmaxf(x0a, x0b), fmaxf(y0a, y0b)), fminf(fmaxf(z0a, z0b), tmax));
-    const float lo1 = fmaxf(fmaxf(fminf(x1a, x1b), fminf(y1a, y1b)), fmaxf(fminf(z1a, z1b), tmin));
-    const float hi1 = fminf(fminf(fmaxf(x1a, x1b), fmaxf(y1a, y1b)), fminf(fmaxf(z1a, z1b), tmax));
+    const float lo0 = max3f(fminf(x0a, x0b), fminf(y0a, y0b), fmaxf(fminf(z0a, z0b), tmin));
+    const float hi0 = min3f(fmaxf(x0a, x0b), fmaxf(y0a, y0b), fminf(fmaxf(z0a, z0b), tmax));
+    const float lo1 = max3f(fminf(x1a, x1b), fminf(y1a, y1b), fmaxf(fminf(z1a, z1b), tmin));
+    const float hi1 = min3f(fmaxf(x1a, x1b), fmaxf(y1a, y1b), fminf(fmaxf(z1a, z1b), tmax));
     *t0 = lo0;
     *t1 = lo1;
     *h0 = lo0 <= hi0;
@@ -320,11 +333,33 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
     return false;
 }
 
+// Traversal stacks. LocalStack: the whole stack in the thread's local
+// memory. SplitStack: the first kShared entries in a shared-memory column of
+// the thread (entry k at top[k * kStride]), the rest in local memory.
+template <int kDepth>
+struct LocalStack {
+    int a[kDepth];
+    __device__ __forceinline__ void put(int i, int v) { a[i] = v; }
+    __device__ __forceinline__ int get(int i) const { return a[i]; }
+};
+
+template <int kShared, int kStride, int kDepth>
+struct SplitStack {
+    int* top;
+    int spill[kDepth - kShared];
+    __device__ __forceinline__ void put(int i, int v) {
+        if (i < kShared) top[i * kStride] = v;
+        else spill[i - kShared] = v;
+    }
+    __device__ __forceinline__ int get(int i) const { return i < kShared ? top[i * kStride] : spill[i - kShared]; }
+};
+
 // Closest hit in [tmin, tmax]; ties in t go to the lower flat triangle index
 // (lexicographic (instance, primitive)), so the result does not depend on
 // the traversal order. Binary-node traversal.
-template <int kDepth = kTraversalStack>
-__device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+template <int kDepth, class Stk>
+__device__ __forceinline__ HitInfo trace_closest_binary_s(const SceneView& s, Stk& stack, f3 o, f3 d, float tmin,
+                                                          float tmax) {
     HitInfo hit;
     hit.valid = false;
     hit.flat = 0xffffffffu;
@@ -334,7 +369,6 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
     if (s.tri_count == 0) return hit;
     const WtRay wr = wt_setup(d);
     const BoxRay br = box_setup(o, d);
-    int stack[kDepth];
     int sp = 0;
     int node = s.root;
     float best_t = tmax;
@@ -351,7 +385,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
             if (h0 && h1) {
                 int near_child = nd.x, far_child = nd.y;
                 if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kDepth) stack[sp++] = far_child;
+                if (sp < kDepth) stack.put(sp++, far_child);
                 else atomicOr(s.status, kStatusStackOverflow);
                 node = near_child;
                 continue;
@@ -375,7 +409,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
             }
         }
         if (sp == 0) break;
-        node = stack[--sp];
+        node = stack.get(--sp);
     }
     if (best_tri >= 0) {
         f3 v0, v1, v2;
@@ -392,13 +426,18 @@ __device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o
     return hit;
 }
 
-// Any hit in [tmin, tmax]. Binary-node traversal.
 template <int kDepth = kTraversalStack>
-__device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+__device__ __forceinline__ HitInfo trace_closest_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    LocalStack<kDepth> stack;
+    return trace_closest_binary_s<kDepth>(s, stack, o, d, tmin, tmax);
+}
+
+// Any hit in [tmin, tmax]. Binary-node traversal.
+template <int kDepth, class Stk>
+__device__ __forceinline__ bool trace_any_binary_s(const SceneView& s, Stk& stack, f3 o, f3 d, float tmin, float tmax) {
     if (s.tri_count == 0) return false;
     const WtRay wr = wt_setup(d);
     const BoxRay br = box_setup(o, d);
-    int stack[kDepth];
     int sp = 0;
     int node = s.root;
     for (;;) {
@@ -412,7 +451,7 @@ __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d,
             if (h0 && h1) {
                 int near_child = nd.x, far_child = nd.y;
                 if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kDepth) stack[sp++] = far_child;
+                if (sp < kDepth) stack.put(sp++, far_child);
                 else atomicOr(s.status, kStatusStackOverflow);
                 node = near_child;
                 continue;
@@ -431,9 +470,15 @@ __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d,
             }
         }
         if (sp == 0) break;
-        node = stack[--sp];
+        node = stack.get(--sp);
     }
     return false;
+}
+
+template <int kDepth = kTraversalStack>
+__device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    LocalStack<kDepth> stack;
+    return trace_any_binary_s<kDepth>(s, stack, o, d, tmin, tmax);
 }
 
 // ---------------------------------------------------------------------------

@@ -148,7 +148,9 @@ struct ManyScenes {
     __device__ __forceinline__ const SceneView& of(uint32_t p) const { return sets[set_of[p]].s; }
 };
 
-template <int kWidth, class Src>
+template <int kWidth, class Src, int kShared = 0>
+// kShared > 0 (binary nodes): the first kShared traversal-stack entries of a
+// thread live in a shared-memory column, the rest in local memory.
 // 10 resident blocks of 128 per SM (at most 51 registers a thread): measured
 // 1,941 against 1,895 Mrays/s with the register count left free (9 blocks),
 // 1,916 at 11 and 12 blocks, 1,639 at 16 (spills).
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* 
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const uint32_t lane = threadIdx.x & 31u;
     RayTally tally{0u, 0u};
+    __shared__ int stack_top[kShared > 0 ? kShared * 128 : 1];
     for (;;) {
         uint32_t base = 0u;
         if (lane == 0u) base = atomicAdd(ctl + 1, 32u);
@@ -173,7 +176,14 @@ __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* 
                 const SceneView s = src.of(p);
                 const float4 o = ro[p], d = rd[p];
                 tally.extend++;
-                const HitInfo h = trace_closest_w<kWidth>(s, xyz(o), xyz(d), o.w, d.w);
+                HitInfo h;
+                if constexpr (kShared > 0 && kWidth == 2) {
+                    SplitStack<kShared, 128, kTraversalStack> stk;
+                    stk.top = stack_top + threadIdx.x;
+                    h = trace_closest_binary_s<kTraversalStack>(s, stk, xyz(o), xyz(d), o.w, d.w);
+                } else {
+                    h = trace_closest_w<kWidth>(s, xyz(o), xyz(d), o.w, d.w);
+                }
                 hit[p] = make_float4(__uint_as_float(h.valid ? h.flat : 0xffffffffu), h.t, h.b1, h.b2);
             }
         }
@@ -181,13 +191,14 @@ __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* 
     flush_tally(counters, tally, 0u, 0u);
 }
 
-template <int kWidth, class Src>
+template <int kWidth, class Src, int kShared = 0>
 __global__ void __launch_bounds__(128, 10) k_wf_shadow(Src src, const float4* __restrict__ queue, uint32_t* ctl,
                                                    float t_max, float4* __restrict__ rad, float4* __restrict__ si,
                                                    unsigned long long* counters) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 2);
     const uint32_t lane = threadIdx.x & 31u;
     RayTally tally{0u, 0u};
+    __shared__ int stack_top[kShared > 0 ? kShared * 128 : 1];
     for (;;) {
         uint32_t base = 0u;
         if (lane == 0u) base = atomicAdd(ctl + 3, 32u);
@@ -199,7 +210,15 @@ __global__ void __launch_bounds__(128, 10) k_wf_shadow(Src src, const float4* __
             tally.shadow++;
             const uint32_t p = __float_as_uint(a.w);
             const SceneView s = src.of(p);
-            if (!trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max)) {
+            bool blocked;
+            if constexpr (kShared > 0 && kWidth == 2) {
+                SplitStack<kShared, 128, kTraversalStack> stk;
+                stk.top = stack_top + threadIdx.x;
+                blocked = trace_any_binary_s<kTraversalStack>(s, stk, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
+            } else {
+                blocked = trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
+            }
+            if (!blocked) {
                 float4* target = (__float_as_uint(b.w) == kKindNee) ? rad : si;
                 const float4 v = target[p];
                 target[p] = make_float4(v.x + c.x, v.y + c.y, v.z + c.z, v.w);
@@ -1189,6 +1208,7 @@ void launch_extend(const NanContext* ctx, int blocks, cudaStream_t st, bool wide
         case 2: k_wf_extend_refill<16, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         case 3: k_wf_extend_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         case 4: k_wf_extend_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        case 5: k_wf_extend<2, Src, 16><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         default: k_wf_extend<2><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
     }
 #undef NAN_EXT_ARGS
@@ -1204,6 +1224,7 @@ void launch_shadow(const NanContext* ctx, int blocks, cudaStream_t st, bool wide
         case 2: k_wf_shadow_refill<16, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         case 3: k_wf_shadow_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         case 4: k_wf_shadow_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        case 5: k_wf_shadow<2, Src, 16><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         default: k_wf_shadow<2><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
     }
 #undef NAN_SHD_ARGS

@@ -25,7 +25,7 @@ def test_traversal_forms_do_not_change_results(device, builder):
     w, h = 64, 48
     node.camera.begin_frame(w, h)
     results, rays = [], []
-    for form in (0, 1, 2, 3, 4):
+    for form in (0, 1, 2, 3, 4, 5):
         scene.configure("wavefront", traversal=form)
         scene.context.read_counters(reset=True)
         slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device="cuda")
