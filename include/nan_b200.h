@@ -267,7 +267,11 @@ NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void
  * It allocates nothing. Build scratch comes from one fixed 64 MiB array in
  * device memory (a file-scope __device__ array: every GPU that loads the
  * library holds it until the process exits), enough for scenes of about 300k
- * triangles; larger scenes return NAN_ERR_LIMIT. The BVH is written into the
+ * triangles; larger scenes return NAN_ERR_LIMIT. The tree is always an LBVH
+ * (Karras 2012) with binary nodes: the context's NanTuning bvh_builder and
+ * bvh_width are ignored. Hits equal nan_scene_build's (the closest hit is
+ * chosen by (t, flat index) in any tree), but the LBVH has a higher SAH cost
+ * than the default PLOC tree, so tracing it is slower. The BVH is written into the
  * caller's buffers, which must stay alive while the context traces them:
  *   out_nodes  >= 64 * max(T - 1, 1) bytes, 16-byte aligned
  *   out_tris   >= 48 * T bytes, 16-byte aligned
@@ -275,7 +279,8 @@ NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void
  * where T is the number of triangles over all instances. The context must
  * not hold a BVH from nan_scene_build. The first call on a device looks up
  * the scratch array's device address (cudaGetSymbolAddress); make that first
- * call before any stream capture. Every call shares the scratch array, so
+ * call before any stream capture. That address is cached for the process and
+ * does not survive cudaDeviceReset on the device. Every call shares the scratch array, so
  * calls that overlap on the GPU (other streams, other host threads) race.
  * Synchronises `stream`. */
 NAN_B200_API int nan_scene_build_noalloc(NanContext* ctx, const NanSceneDesc* desc, float* out_nodes,

@@ -1038,10 +1038,10 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
         ctx->leaf_count = n;
         uint32_t max_depth = 0;
         double sah_host = 0.0;
-        cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
-        err = cudaStreamSynchronize(s);
-        if (err != cudaSuccess) return cuda_fail(err, "scene build");
+        err = cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_fail(err, "scene build (depth and SAH readback)");
         ctx->max_depth = max_depth;
         ctx->sah_cost = sah_host;
     }
@@ -1106,7 +1106,10 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Device address of g_noalloc_scratch per device ordinal. In host code the
 // symbol is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, taken once per device with that device current.
+// cudaGetSymbolAddress, taken once per device with that device current. The
+// cached address belongs to the device's primary context: after
+// cudaDeviceReset it is stale, and the library must not be used for a
+// no-alloc build on that device again in this process.
 std::mutex g_noalloc_mutex;
 void* g_noalloc_address[128] = {};
 
@@ -1281,8 +1284,12 @@ extern "C" NAN_B200_API int nan_scene_build_noalloc(NanContext* ctx, const NanSc
         ctx->launches += 4;
         ctx->root = 0;
         ctx->node_count = interior;
-        cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+        err = cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+        if (err != cudaSuccess) {
+            forget_bvh();
+            return cuda_fail(err, "no-alloc scene build (depth and SAH readback)");
+        }
     }
     err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) {

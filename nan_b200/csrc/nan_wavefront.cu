@@ -151,7 +151,7 @@ struct ManyScenes {
 template <int kWidth, class Src, int kShared = 0>
 // kShared > 0 (binary nodes): the first kShared traversal-stack entries of a
 // thread live in a shared-memory column, the rest in local memory.
-// 10 resident blocks of 128 per SM (at most 51 registers a thread): measured
+// 10 resident blocks of 128 per SM (48 registers a thread, -Xptxas -v): measured
 // 1,941 against 1,895 Mrays/s with the register count left free (9 blocks),
 // 1,916 at 11 and 12 blocks, 1,639 at 16 (spills).
 __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* __restrict__ queue,

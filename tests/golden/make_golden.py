@@ -1,7 +1,8 @@
 """Generate golden input/output vectors from the reference's own Python code.
 
-Run in a container that holds the reference project (default root
-``/root/reference``, override with ``NAN_REFERENCE_ROOT``)::
+Run where the reference project is checked out (default: a ``reference``
+folder beside this repository's folder; override with
+``NAN_REFERENCE_ROOT``)::
 
     python tests/golden/make_golden.py
 
@@ -29,7 +30,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("NAN_REFERENCE_ROOT", "/root/reference"))
+REF = Path(os.environ.get("NAN_REFERENCE_ROOT", HERE.parents[2] / "reference"))
 
 
 class _Inert:

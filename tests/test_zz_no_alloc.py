@@ -2,12 +2,16 @@
 
 Some callers may not call cudaMalloc at all -- code living inside another
 framework's memory pool, or a real-time loop with an allocation ban. This
-entry point builds the same BVH as nan_scene_build from a fixed scratch array
-in device memory and writes it into buffers the caller already owns. The test
-calls it through the C ABI twice in a row on one context (a larger scene
-first, then a smaller one, so the second call starts from the first call's
-leftover scratch) and checks each result against nan_scene_build's with the
-same exact comparisons the parity tests use. This file is collected last.
+entry point builds an LBVH (binary nodes, whatever the context's tuning asks)
+from a fixed scratch array in device memory and writes it into buffers the
+caller already owns. Its tree differs from nan_scene_build's default PLOC
+tree, but the hits do not: the closest hit is chosen by (t, flat index) in
+any tree. The test calls it through the C ABI twice in a row on one context
+(a larger scene first, then a smaller one, so the second call starts from the
+first call's leftover scratch) and checks each result against
+nan_scene_build's with the same exact comparisons the parity tests use; then
+it checks the error paths, which return before the build touches the
+caller's buffers. This file is collected last.
 """
 
 import ctypes
@@ -84,3 +88,60 @@ def test_noalloc_build_matches_allocating_build_twice(device):
         keep.append(_noalloc_scene(device, scene, ctx))
         _compare(device, scene, ctx, seed=100 + k)
     ctx.close()
+
+
+def _call(ctx, scene, nodes, nodes_bytes, tris, tris_bytes, refs, refs_bytes):
+    from nan_b200 import _native
+
+    return _native.lib().nan_scene_build_noalloc(ctx.handle, ctypes.byref(scene._desc), nodes, nodes_bytes, tris,
+                                                 tris_bytes, refs, refs_bytes, _native.stream_handle(None))
+
+
+def _last_error():
+    from nan_b200 import _native
+
+    return _native.lib().nan_last_error().decode()
+
+
+def test_noalloc_build_error_paths(device):
+    import torch
+
+    import nan_b200
+    from nan_b200 import _native, scenes
+
+    scene = nan_b200.Scene(device, scenes.cornell_box(32, 32))
+    n = int(scene.info()["triangle_count"])
+    buf = torch.empty((max(n - 1, 1) * 16 + n * 12 + n * 2 + 64,), dtype=torch.float32, device=device.torch_device)
+    base = buf.data_ptr()
+    nodes, tris, refs = base, base + max(n - 1, 1) * 64, base + max(n - 1, 1) * 64 + n * 48
+    nb, tb, rb = max(n - 1, 1) * 64, n * 48, n * 8
+    ctx = device.new_context()
+    # output buffers too small
+    assert _call(ctx, scene, nodes, nb - 64, tris, tb, refs, rb) == _native.NAN_ERR_INVALID_ARGUMENT
+    assert "too small" in _last_error()
+    assert _call(ctx, scene, nodes, nb, tris, tb, refs, rb - 8) == _native.NAN_ERR_INVALID_ARGUMENT
+    # misaligned outputs
+    assert _call(ctx, scene, nodes + 4, nb, tris, tb, refs, rb) == _native.NAN_ERR_INVALID_ARGUMENT
+    assert "aligned" in _last_error()
+    assert _call(ctx, scene, nodes, nb, tris, tb, refs + 4, rb) == _native.NAN_ERR_INVALID_ARGUMENT
+    # nothing was built by the failed calls
+    info = _native.NanSceneInfo()
+    assert _native.lib().nan_scene_info(ctx.handle, ctypes.byref(info)) == _native.NAN_ERR_NO_SCENE
+    # the same buffers, right-sized and aligned, build
+    _native.check(_call(ctx, scene, nodes, nb, tris, tb, refs, rb))
+    _native.check(_native.lib().nan_scene_info(ctx.handle, ctypes.byref(info)))
+    assert info.triangle_count == n
+    ctx.close()
+    # a context that holds a BVH allocated by nan_scene_build is refused
+    assert _call(scene.context, scene, nodes, nb, tris, tb, refs, rb) == _native.NAN_ERR_INVALID_ARGUMENT
+    assert "nan_scene_build" in _last_error()
+    # a scene beyond the 64 MiB scratch (about 400k triangles) hits the limit
+    big = nan_b200.Scene(device, scenes.terrain_boxes(seed=2, grid=451, boxes=0))
+    m = int(big.info()["triangle_count"])
+    assert m > 350_000
+    ctx2 = device.new_context()
+    rc = _call(ctx2, big, nodes, nb, tris, tb, refs, rb)
+    assert rc == _native.NAN_ERR_LIMIT, (rc, _last_error())
+    assert "64 MiB" in _last_error()
+    ctx2.close()
+    torch.cuda.synchronize()
