@@ -302,6 +302,38 @@ NAN_B200_API int nan_intersect(NanContext* ctx, const float* rays, uint32_t coun
 NAN_B200_API int nan_occluded(NanContext* ctx, const float* rays, uint32_t count,
                               float* visibility, void* stream);
 
+/* Most rays per sample of the PMR visibility caster below. */
+#define NAN_VISIBILITY_MAX_RAYS 1024u
+/* Ray table of the reference's PMR visibility caster, make_ray_projections
+ * (vertex_baker/cpp/tinybvh_visibility.cpp:81-101, SH at :52-77): ray r of R
+ * has u0 = r / R, u1 = bit-reversed r * 2^-32, phi = 2 pi u0,
+ * cos theta = 1 - 2 u1, direction (cos phi sin theta, cos theta,
+ * sin phi sin theta), and the real SH basis of bands 0-3 times 4 pi / R.
+ * Writes host memory f32[R][20]: direction xyz, 0, the 16 weighted SH
+ * values. Host only (the C library's cosf/sinf, as the caster uses);
+ * 1 <= R <= NAN_VISIBILITY_MAX_RAYS. */
+NAN_B200_API int nan_visibility_ray_table(uint32_t ray_count, float* host_table);
+/* GPU form of the reference's PMR visibility caster,
+ * vbake_pmr_visibility_sh_tinybvh (vertex_baker/cpp/vertex_baking_utils.h:73-90,
+ * tinybvh_visibility.cpp:145-230), and of its hardware twin
+ * HWRTPMRVisibilitySHSampler.sample (vertex_baker/hwrt_visibility_baker.py:145-240).
+ * For every sample, the table's rays start at position + normalize(normal) *
+ * self_bias (a zero or non-finite normal: direction (0,0,1) and the origin
+ * moved one float towards each ray instead) and are tested for any hit in
+ * [0, max_distance] (max_distance <= 0 or non-finite: 1e30; self_bias below
+ * 0: 0) against the context's scene. The unoccluded rays' weighted SH values
+ * are summed in the caster's order (64-ray batches), into out_sh16
+ * f32[S][16]; out_visible_counts u32[S] (may be null) gets the number of
+ * unoccluded rays. Device pointers: sample_positions/normals f32[S][3],
+ * ray_table the table above copied to the device. The geometry is the built
+ * scene (all instances, world space) rather than a positions/indices pair,
+ * and the caster's thread count and BVH layout arguments have no meaning
+ * here. Non-finite sample inputs are not checked (the caster rejects them). */
+NAN_B200_API int nan_visibility_sh16(NanContext* ctx, const float* sample_positions, const float* sample_normals,
+                                     uint32_t sample_count, const float* ray_table, uint32_t ray_count,
+                                     float max_distance, float self_bias, float* out_sh16,
+                                     uint32_t* out_visible_counts, void* stream);
+
 /* One 1-spp frame of the screen path tracer into out_rgba f32[H][W][4]
  * (PathTracer.execute, path_tracer.py:21-40; path_tracer.slang:40-130).
  * max_vertices is the reference's hard-coded 5 (path_tracer.slang:42). */

@@ -37,12 +37,13 @@ from .surface_probe_layout import SurfaceProbeLayout, SurfaceProbeSiteLayout
 from .surface_probe_resolve import SurfaceProbeResolve
 from .surface_probe_resources import SurfaceProbeGpuGeometry
 from .texture_space_path_tracer import TextureSpacePathTracer
+from .visibility import PMRVisibilitySHSampler, trace_pmr_visibility_sh, visibility_ray_table
 
 __all__ = [
     "Accumulator", "CachedPathTracer", "Camera", "Device", "HaltonSamplePattern", "Lighting", "Material", "Mesh", "MeshColorsLayout",
     "MeshColorsRGB9E5Packer", "MeshColorsResolve", "MeshColorsSurfaceFilter", "PathTracer", "ProbeBatch", "RadianceCache", "RenderData", "Scene", "SceneNode", "SurfaceProbeAttachments",
     "SurfaceProbeDiffuseIrradianceBaker", "SurfaceProbeFieldBuffers", "SurfaceProbeGpuGeometry",
-    "SurfaceProbePathTracer", "SurfaceProbePrtBaker", "SurfaceProbeResolve", "SurfaceProbeLayout", "SurfaceProbeSiteLayout", "SurfaceProbePrtEvaluator", "evaluate_prt_l2_rgb", "surface_probe_sh_l2_basis", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "address_to_ij",
+    "SurfaceProbePathTracer", "SurfaceProbePrtBaker", "SurfaceProbeResolve", "SurfaceProbeLayout", "SurfaceProbeSiteLayout", "SurfaceProbePrtEvaluator", "evaluate_prt_l2_rgb", "surface_probe_sh_l2_basis", "SurfaceProbeRuntimeBuffers", "TextureSpacePathTracer", "PMRVisibilitySHSampler", "trace_pmr_visibility_sh", "visibility_ray_table", "address_to_ij",
     "barycentric_at", "colors_per_patch", "halton", "ij_to_address", "make_transform",
     "DIFFUSE_IRRADIANCE_ATTACHMENTS", "DIFFUSE_IRRADIANCE_RGB_FIELD", "MESH_COLORS_INVALID_OFFSET",
     "MESH_COLORS_PAYLOAD_SIZE", "MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED",

@@ -271,6 +271,8 @@ EXPORTS = {
     "nan_scene_world_triangles": (_I, [_VP, _VP, _VP]),
     "nan_intersect": (_I, [_VP, _VP, _U32, _VP, _VP, _VP]),
     "nan_occluded": (_I, [_VP, _VP, _U32, _VP, _VP]),
+    "nan_visibility_ray_table": (_I, [_U32, _VP]),
+    "nan_visibility_sh16": (_I, [_VP, _VP, _VP, _U32, _VP, _U32, ctypes.c_float, ctypes.c_float, _VP, _VP, _VP]),
     "nan_trace_screen": (_I, [_VP, _VP, _U32, _U32, _U32, _U32, ctypes.POINTER(NanCamera),
                               ctypes.POINTER(NanLighting), _VP]),
     "nan_accumulate": (_I, [_VP, _VP, _VP, _VP, _U32, _U32, _I, _VP]),

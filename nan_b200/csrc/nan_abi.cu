@@ -264,6 +264,33 @@ NAN_B200_API int nan_occluded(NanContext* ctx, const float* rays, uint32_t count
     return nan_host::launch_occluded(ctx, rays, count, visibility, as_stream(stream));
 }
 
+NAN_B200_API int nan_visibility_ray_table(uint32_t ray_count, float* host_table) {
+    if (ray_count == 0 || ray_count > NAN_VISIBILITY_MAX_RAYS)
+        return invalid("ray_count must be 1..1024 (NAN_VISIBILITY_MAX_RAYS)");
+    if (!host_table) return invalid("null table");
+    return nan_host::visibility_ray_table(ray_count, host_table);
+}
+
+NAN_B200_API int nan_visibility_sh16(NanContext* ctx, const float* sample_positions, const float* sample_normals,
+                                     uint32_t sample_count, const float* ray_table, uint32_t ray_count,
+                                     float max_distance, float self_bias, float* out_sh16,
+                                     uint32_t* out_visible_counts, void* stream) {
+    int rc = enter(ctx);
+    if (rc) return rc;
+    if ((rc = need_scene(ctx))) return rc;
+    if (ray_count == 0 || ray_count > NAN_VISIBILITY_MAX_RAYS)
+        return invalid("ray_count must be 1..1024 (NAN_VISIBILITY_MAX_RAYS)");
+    if (!ray_table) return invalid("null ray table");
+    if (sample_count && (!sample_positions || !sample_normals || !out_sh16))
+        return invalid("null sample or output buffer");
+    if (!std::isfinite(self_bias)) return invalid("self_bias must be finite");
+    if (!std::isfinite(max_distance) || max_distance <= 0.0f) max_distance = 1.0e30f;
+    self_bias = std::max(0.0f, self_bias);
+    return nan_host::launch_visibility_sh16(ctx, sample_positions, sample_normals, sample_count, ray_table, ray_count,
+                                            max_distance, self_bias, out_sh16, out_visible_counts,
+                                            as_stream(stream));
+}
+
 NAN_B200_API int nan_trace_screen(NanContext* ctx, float* out_rgba, uint32_t width, uint32_t height, uint32_t frame,
                                   uint32_t max_vertices, const NanCamera* camera, const NanLighting* lighting,
                                   void* stream) {

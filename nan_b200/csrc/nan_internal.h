@@ -102,6 +102,10 @@ int world_triangles(NanContext* ctx, float* out, cudaStream_t stream);
 int launch_intersect(NanContext* ctx, const float* rays, uint32_t count, uint32_t* ids, float* tb,
                      cudaStream_t stream);
 int launch_occluded(NanContext* ctx, const float* rays, uint32_t count, float* vis, cudaStream_t stream);
+int visibility_ray_table(uint32_t ray_count, float* host_table);
+int launch_visibility_sh16(NanContext* ctx, const float* positions, const float* normals, uint32_t count,
+                           const float* table, uint32_t ray_count, float max_distance, float self_bias, float* out,
+                           uint32_t* visible, cudaStream_t stream);
 int launch_trace_screen(NanContext* ctx, float* out, uint32_t w, uint32_t h, uint32_t frame,
                         uint32_t max_vertices, const NanCamera* cam, const NanLighting* light,
                         cudaStream_t stream);

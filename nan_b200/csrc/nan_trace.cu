@@ -4,6 +4,8 @@
 
 #include <algorithm>
 
+#include <cmath>
+
 #include "nan_internal.h"
 #include "nan_scene.cuh"
 #include "nan_sinks.cuh"
@@ -79,6 +81,81 @@ __global__ void k_occluded(SceneView s, const float4* __restrict__ rays, uint32_
     if (i >= n) return;
     const float4 a = rays[2u * i], b = rays[2u * i + 1];
     vis[i] = trace_any(s, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), a.w, b.w) ? 0.0f : 1.0f;
+}
+
+
+// ---------------------------------------------------------------------------
+// PMR visibility caster (vertex_baker/cpp/tinybvh_visibility.cpp:145-230):
+// per sample, the table's rays leave position + normalize(normal) * bias (a
+// zero or non-finite normal: (0,0,1) and an origin one float nearer each
+// ray, as tinybvh has no t_min) and are tested for any hit in
+// [0, t_max]. One warp per sample: lanes take rays r = lane + 32 w, a ballot
+// per 32 rays leaves mask word w in lane w; lanes 0-15 then sum coefficient
+// `lane` of the unoccluded rays' weighted SH in the caster's order (64-ray
+// batches, each summed in ray order, then added to the total).
+// ---------------------------------------------------------------------------
+constexpr uint32_t kVisTableStride = 20;  // floats per ray: direction xyz, 0, 16 weighted SH values
+
+__device__ __forceinline__ float nudge_toward(float o, float d) {
+    if (d > 0.0f) return nextafterf(o, __int_as_float(0x7f800000));
+    if (d < 0.0f) return nextafterf(o, __int_as_float(0xff800000));
+    return o;
+}
+
+__global__ void __launch_bounds__(128) k_visibility_sh16(SceneView s, const float* __restrict__ pos,
+                                                         const float* __restrict__ nrm, uint32_t n,
+                                                         const float* __restrict__ table, uint32_t rays, float tmax,
+                                                         float bias, float* __restrict__ out,
+                                                         uint32_t* __restrict__ counts, unsigned long long* counters) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t words = (rays + 31u) >> 5;
+    RayTally tally{0u, 0u};
+    for (uint32_t i = warp; i < n; i += warps) {
+        const float px = __ldg(pos + 3ull * i), py = __ldg(pos + 3ull * i + 1), pz = __ldg(pos + 3ull * i + 2);
+        const float nx = __ldg(nrm + 3ull * i), ny = __ldg(nrm + 3ull * i + 1), nz = __ldg(nrm + 3ull * i + 2);
+        const float ls = nx * nx + ny * ny + nz * nz;
+        const bool has_normal = isfinite(ls) && ls > 1.0e-16f;
+        f3 u = mk3(0.0f, 0.0f, 1.0f);
+        if (has_normal) {
+            const float inv = 1.0f / sqrtf(ls);
+            u = mk3(nx * inv, ny * inv, nz * inv);
+        }
+        const f3 o = mk3(px + u.x * bias, py + u.y * bias, pz + u.z * bias);
+        uint32_t word = 0u;
+        for (uint32_t w = 0; w < words; ++w) {
+            const uint32_t r = 32u * w + lane;
+            bool visible = false;
+            if (r < rays) {
+                const float* e = table + (size_t)kVisTableStride * r;
+                const f3 d = mk3(__ldg(e), __ldg(e + 1), __ldg(e + 2));
+                const f3 oo = has_normal ? o : mk3(nudge_toward(o.x, d.x), nudge_toward(o.y, d.y), nudge_toward(o.z, d.z));
+                visible = !trace_any(s, oo, d, 0.0f, tmax);
+                tally.shadow++;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, visible);
+            if (lane == w) word = m;
+        }
+        const uint32_t seen = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(word));
+        float total = 0.0f;
+        for (uint32_t b = 0; b < words; b += 2u) {
+            float batch = 0.0f;
+            const uint32_t wend = min(b + 2u, words);
+            for (uint32_t w = b; w < wend; ++w) {
+                unsigned m = __shfl_sync(0xffffffffu, word, w);
+                while (m) {
+                    const uint32_t j = (uint32_t)__ffs(m) - 1u;
+                    m &= m - 1u;
+                    if (lane < 16u) batch += __ldg(table + (size_t)kVisTableStride * (32u * w + j) + 4u + lane);
+                }
+            }
+            total += batch;
+        }
+        if (lane < 16u) out[16ull * i + lane] = total;
+        if (lane == 0u && counts) counts[i] = seen;
+    }
+    flush_tally(counters, tally, 0u, 0u);
 }
 
 // ---------------------------------------------------------------------------
@@ -806,6 +883,70 @@ int launch_intersect(NanContext* ctx, const float* rays, uint32_t count, uint32_
                                                         reinterpret_cast<uint4*>(ids), tb);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "intersect launch");
+}
+
+// Direction table of the caster's make_ray_projections
+// (tinybvh_visibility.cpp:81-101, 52-77): ray r has u0 = r / R, u1 = the
+// bit-reversed r times 2^-32, phi = 2 pi u0, cos theta = 1 - 2 u1, direction
+// (cos phi sin theta, cos theta, sin phi sin theta), and the real SH basis of
+// bands 0-3 at that direction times 4 pi / R. Evaluated in float with the C
+// library's cosf/sinf/sqrtf and the caster's operation order, so the rays
+// and weights are the caster's own.
+int visibility_ray_table(uint32_t ray_count, float* t) {
+    constexpr float kPiF = 3.14159265358979323846f;
+    const float weight = (4.0f * kPiF) / static_cast<float>(ray_count);
+    for (uint32_t r = 0; r < ray_count; ++r) {
+        uint32_t v = r;
+        v = (v << 16) | (v >> 16);
+        v = ((v & 0x55555555u) << 1) | ((v & 0xaaaaaaaau) >> 1);
+        v = ((v & 0x33333333u) << 2) | ((v & 0xccccccccu) >> 2);
+        v = ((v & 0x0f0f0f0fu) << 4) | ((v & 0xf0f0f0f0u) >> 4);
+        v = ((v & 0x00ff00ffu) << 8) | ((v & 0xff00ff00u) >> 8);
+        const float u0 = static_cast<float>(r) / static_cast<float>(ray_count);
+        const float u1 = static_cast<float>(v) * 2.3283064365386963e-10f;
+        const float phi = u0 * (2.0f * kPiF);
+        const float ct = 1.0f - 2.0f * u1;
+        const float st = std::sqrt(std::max(1.0f - ct * ct, 0.0f));
+        const float x = std::cos(phi) * st, y = ct, z = std::sin(phi) * st;
+        const float x2 = x * x, y2 = y * y, z2 = z * z;
+        float* e = t + (size_t)kVisTableStride * r;
+        e[0] = x;
+        e[1] = y;
+        e[2] = z;
+        e[3] = 0.0f;
+        float* sh = e + 4;
+        sh[0] = weight * 0.282094791774f;
+        sh[1] = weight * (-0.488602511903f * y);
+        sh[2] = weight * (0.488602511903f * z);
+        sh[3] = weight * (-0.488602511903f * x);
+        sh[4] = weight * (1.09254843059f * x * y);
+        sh[5] = weight * (-1.09254843059f * y * z);
+        sh[6] = weight * (0.315391565253f * (-1.0f + 3.0f * z2));
+        sh[7] = weight * (-1.09254843059f * x * z);
+        sh[8] = weight * (0.546274215296f * (x2 - y2));
+        sh[9] = weight * (-0.590043589927f * (3.0f * x2 * y - y2 * y));
+        sh[10] = weight * (2.89061144264f * x * y * z);
+        sh[11] = weight * (-0.457045799464f * y * (-1.0f + 5.0f * z2));
+        sh[12] = weight * (0.37317633259f * z * (-3.0f + 5.0f * z2));
+        sh[13] = weight * (-0.457045799464f * x * (-1.0f + 5.0f * z2));
+        sh[14] = weight * (1.44530572132f * (x2 - y2) * z);
+        sh[15] = weight * (-0.590043589927f * (x2 * x - 3.0f * x * y2));
+    }
+    return NAN_OK;
+}
+
+int launch_visibility_sh16(NanContext* ctx, const float* positions, const float* normals, uint32_t count,
+                           const float* table, uint32_t ray_count, float max_distance, float self_bias, float* out,
+                           uint32_t* visible, cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    int sms = 148, occ = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_visibility_sh16, 128, 0);
+    const uint32_t grid = std::min<uint32_t>((uint32_t)sms * (uint32_t)std::max(occ, 1), (count + 3u) / 4u);
+    k_visibility_sh16<<<grid, 128, 0, st>>>(scene_view(ctx), positions, normals, count, table, ray_count,
+                                            max_distance, self_bias, out, visible, ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "visibility launch");
 }
 
 int launch_occluded(NanContext* ctx, const float* rays, uint32_t count, float* vis, cudaStream_t st) {
