@@ -70,7 +70,6 @@ def parse_args():
     ap.add_argument("--no-city", action="store_true", help="skip the 4M-triangle city frame measurement")
     ap.add_argument("--no-consumers", action="store_true",
                     help="skip the resolve / filter / PRT / probe-resolve pass timings")
-    ap.add_argument("--cpu-seconds", type=float, default=4.0, help="target trace time of one CPU-baseline run")
     return ap.parse_args()
 
 
@@ -131,77 +130,82 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # Reference CPU caster (tinybvh) through ctypes.
 # ---------------------------------------------------------------------------
-def load_reference_caster():
-    for name in ("libvbake_bvh8.so", "libvbake_bvh.so"):
-        path = ROOT / "oracle" / "_ref" / name
-        if path.exists():
-            lib = ctypes.CDLL(str(path))
-            lib.vbake_tinybvh_has_bvh8_cpu.restype = ctypes.c_int
-            lib.vbake_pmr_visibility_sh_tinybvh.restype = ctypes.c_int
-            lib.vbake_last_error.restype = ctypes.c_char_p
-            layout = 1 if lib.vbake_tinybvh_has_bvh8_cpu() else 0
-            return lib, layout, name
-    return None, None, None
+VIS_SITES = 65536
+VIS_RAYS = 512
+VIS_DISTANCE = 1000.0
+VIS_WORKLOAD = (f"PMR visibility SH: {VIS_SITES} seeded surface sites (seed 11) x {VIS_RAYS} rays of the reference "
+                f"caster's direction table, self bias 1e-3, ray length {VIS_DISTANCE:g}, on the same world triangles")
 
 
-def reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, max_distance):
-    vp = ctypes.c_void_p
-    out = np.zeros((sites.shape[0], 16), np.float32)
-    build_ms, trace_ms = ctypes.c_double(), ctypes.c_double()
-    visible, threads = ctypes.c_ulonglong(), ctypes.c_int()
-    rc = lib.vbake_pmr_visibility_sh_tinybvh(
-        ctypes.c_int(positions.shape[0]), ctypes.c_int(indices.shape[0]), vp(positions.ctypes.data),
-        vp(indices.ctypes.data), ctypes.c_int(sites.shape[0]), vp(sites.ctypes.data), vp(normals.ctypes.data),
-        ctypes.c_int(rays_per_site), ctypes.c_float(max_distance), ctypes.c_float(1e-3), ctypes.c_int(0),
-        ctypes.c_int(layout), vp(out.ctypes.data), ctypes.byref(build_ms), ctypes.byref(trace_ms),
-        ctypes.byref(visible), ctypes.byref(threads))
-    if rc != 0:
-        raise RuntimeError(lib.vbake_last_error().decode())
-    return trace_ms.value, build_ms.value, int(visible.value), int(threads.value)
-
-
-def flattened_geometry(node):
-    """World-space vertices/indices of every instance (the caster has no instancing)."""
-    pos, idx, base = [], [], 0
-    for mesh_id, _, transform_id in node.instances:
-        mesh = node.meshes[mesh_id]
-        m = node.transforms[transform_id].astype(np.float64)
-        p = mesh.vertices[:, 0:3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
-        pos.append(p.astype(np.float32))
-        idx.append(mesh.indices.astype(np.uint32) + base)
-        base += mesh.vertex_count
-    return np.ascontiguousarray(np.concatenate(pos)), np.ascontiguousarray(np.concatenate(idx))
-
-
-def cpu_baseline(node, seconds: float, rays_per_site: int = 512):
-    """Reference tinybvh caster on a bounded sample of surface sites of the same scene."""
+def visibility_workload(node, world_triangles):
+    """The one site set that the reference arm, the CPU baseline and the GPU
+    visibility pass all trace: (positions, indices, sites, normals)."""
     from nan_b200 import scenes
+    from oracle import visibility as ov
 
-    lib, layout, name = load_reference_caster()
-    if lib is None:
-        return None
-    positions, indices = flattened_geometry(node)
-    probes, _ = scenes.surface_sites(node, 1024, seed=11, double_sided_backs=False)
-    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
-    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
-    trace_ms, _, _, threads = reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, 1000.0)
-    scale = max(1.0, seconds * 1000.0 / max(trace_ms, 1e-3))
-    count = int(min(1024 * scale, 2_000_000))
-    probes, _ = scenes.surface_sites(node, count, seed=12, double_sided_backs=False)
-    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
-    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
-    times = []
-    reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site, 1000.0)  # warm-up
-    for _ in range(3):
-        t, build, visible, threads = reference_cast(lib, layout, positions, indices, sites, normals, rays_per_site,
-                                                    1000.0)
-        times.append(t)
-    t = statistics.median(times)
-    rays = sites.shape[0] * rays_per_site
-    return {"value": rays / (t * 1e3), "unit": "Mrays/s", "cores": threads, "kind": "reference",
-            "sample": f"tinybvh {'BVH8_CPU' if layout == 1 else 'BVH'} any-hit ({name}), {sites.shape[0]} surface "
-                      f"sites x {rays_per_site} rays on the same flattened scene, median of 3 runs "
-                      f"({t:.0f} ms each), build {build:.0f} ms, {os.cpu_count()} host cpus"}
+    positions, indices = ov.world_geometry(world_triangles)
+    probes, _ = scenes.surface_sites(node, VIS_SITES, seed=11, double_sided_backs=False)
+    return (positions, indices, np.ascontiguousarray(probes["position_radius"][:, :3]),
+            np.ascontiguousarray(probes["normal_side"][:, :3]))
+
+
+def cpu_baseline(workload):
+    """The reference's own caster (tinybvh BVH8_CPU, all host threads) on the
+    visibility site set: warm-up, then the median of 3 runs. Returns the
+    cpu_baseline record and the caster's SH output."""
+    from oracle import visibility as ov
+
+    ref = ov.ReferenceCaster("bvh8")
+    if not ref.available:
+        return None, None
+    positions, indices, sites, normals = workload
+    ref.cast(positions, indices, sites, normals, VIS_RAYS, VIS_DISTANCE)
+    runs = [ref.cast(positions, indices, sites, normals, VIS_RAYS, VIS_DISTANCE) for _ in range(3)]
+    t = statistics.median(r[1]["trace_ms"] for r in runs)
+    stats = runs[0][1]
+    rays = sites.shape[0] * VIS_RAYS
+    return ({"value": rays / (t * 1e3), "unit": "Mrays/s", "cores": stats["threads"], "kind": "reference",
+             "sample": f"tinybvh {stats['layout']} any-hit ({stats['library']}): {VIS_WORKLOAD}; median of 3 runs "
+                       f"({t:.0f} ms each), build {stats['build_ms']:.0f} ms, {os.cpu_count()} host cpus"},
+            runs[0][0])
+
+
+def pmr_visibility_line(scene, workload, reference_sh, steps=10):
+    """GPU any-hit Mrays/s on exactly the CPU baseline's rays, and agreement
+    with the reference caster's output (BVH8_CPU on every site; the scalar
+    BVH layout, which runs the same watertight test, on the first 4096)."""
+    import torch
+
+    import nan_b200
+    from oracle import visibility as ov
+
+    positions, indices, sites, normals = workload
+    dev = scene.device.torch_device
+    sampler = nan_b200.PMRVisibilitySHSampler(scene.device)
+    sites_d = torch.from_numpy(sites).to(dev)
+    normals_d = torch.from_numpy(normals).to(dev)
+    for _ in range(2):
+        sh = sampler.sample(scene, sites_d, normals_d, ray_count=VIS_RAYS, max_distance=VIS_DISTANCE)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sh = sampler.sample(scene, sites_d, normals_d, ray_count=VIS_RAYS, max_distance=VIS_DISTANCE)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    got = sh.cpu().numpy()
+    rays = sites.shape[0] * VIS_RAYS
+    out = {"workload": VIS_WORKLOAD, "sites": int(sites.shape[0]), "rays_per_site": VIS_RAYS,
+           "gpu": {"ms": ms, "mrays_per_s": rays / (ms * 1e3), "kernel": "k_visibility_sh16"}}
+    if reference_sh is not None:
+        out["vs_reference_bvh8_cpu"] = ov.compare(reference_sh, got, VIS_RAYS)
+    scalar = ov.ReferenceCaster("bvh")
+    if scalar.available:
+        k = 4096
+        ref, _ = scalar.cast(positions, indices, sites[:k], normals[:k], VIS_RAYS, VIS_DISTANCE)
+        out["vs_reference_bvh_first_4096"] = ov.compare(ref, got[:k], VIS_RAYS)
+    return out
 
 
 def roofline_bytes_per_ray(node, layout, lighting, sample_units: int = 6000):
@@ -249,31 +253,29 @@ def run_reference(args):
     if rank != 0:
         return
     from nan_b200 import scenes
+    from oracle import visibility as ov
+    from oracle.oracle import OracleScene
 
-    node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
-    lib, layout, name = load_reference_caster()
-    if lib is None:
+    ref = ov.ReferenceCaster("bvh8")
+    if not ref.available:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref caster library not built"}))
         return
-    positions, indices = flattened_geometry(node)
-    probes, _ = scenes.surface_sites(node, 4096, seed=11, double_sided_backs=False)
-    sites = np.ascontiguousarray(probes["position_radius"][:, :3])
-    normals = np.ascontiguousarray(probes["normal_side"][:, :3])
+    node = scenes.terrain_boxes(seed=args.seed, grid=args.grid, boxes=args.boxes)
+    positions, indices, sites, normals = visibility_workload(node, OracleScene(**node.pack()).world_triangles())
     for _ in range(max(args.warmup, 0)):
-        reference_cast(lib, layout, positions, indices, sites, normals, 512, 1000.0)
-    total_ms, threads = 0.0, 0
+        ref.cast(positions, indices, sites, normals, VIS_RAYS, VIS_DISTANCE)
+    total_ms, stats = 0.0, None
     for _ in range(args.steps):
-        t, _, _, threads = reference_cast(lib, layout, positions, indices, sites, normals, 512, 1000.0)
-        total_ms += t
-    rays = args.steps * sites.shape[0] * 512
+        _, stats = ref.cast(positions, indices, sites, normals, VIS_RAYS, VIS_DISTANCE)
+        total_ms += stats["trace_ms"]
+    rays = args.steps * sites.shape[0] * VIS_RAYS
     value = rays / (total_ms * 1e3)
     line = {"impl": "reference", "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "reference_step": "any-hit sample"},
-            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": "reference",
-                             "sample": f"tinybvh {'BVH8_CPU' if layout == 1 else 'BVH'} ({name}): "
-                                       f"{sites.shape[0]} surface sites x 512 rays per step"},
+            "data": "synthetic", "config": {"workload": WORKLOAD, "reference_step": VIS_WORKLOAD},
+            "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": stats["threads"], "kind": "reference",
+                             "sample": f"tinybvh {stats['layout']} ({stats['library']}): one step = {VIS_WORKLOAD}"},
             "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -441,7 +443,9 @@ def run_nan(args):
         "clocks": clock_info,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(node, args.cpu_seconds)
+        workload = visibility_workload(node, scene.world_triangles().cpu().numpy())
+        line["cpu_baseline"], reference_sh = cpu_baseline(workload)
+        line["pmr_visibility"] = pmr_visibility_line(scene, workload, reference_sh)
     if world == 1 and not args.no_learned:
         line["learned_cache"] = learned_cache_line(device)
     if world == 1 and not args.no_consumers:
