@@ -133,12 +133,13 @@ def test_any_hit_bit_exact_vs_oracle(which, width, request):
     scene.configure()
 
 
-def test_screen_path_tracer_matches_oracle(cornell, device):
+@pytest.mark.parametrize("which", ["cornell", "terrain"])
+def test_screen_path_tracer_matches_oracle(which, request, device):
     import torch
 
     import nan_b200
 
-    scene, orc = cornell
+    scene, orc = request.getfixturevalue(which)
     cam = scene.camera
     w = h = 64
     out = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
