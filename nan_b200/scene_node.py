@@ -78,28 +78,28 @@ class Mesh:
 
     @classmethod
     def cube(cls, size=(1.0, 1.0, 1.0)) -> "Mesh":
-        """Box with outward faces, 24 vertices and 12 triangles."""
-        faces = [  # (normal, u axis, v axis)
-            ((0, -1, 0), (0, 0, 1), (1, 0, 0)),
-            ((0, 1, 0), (1, 0, 0), (0, 0, 1)),
-            ((0, 0, -1), (1, 0, 0), (0, 1, 0)),
-            ((0, 0, 1), (0, 1, 0), (1, 0, 0)),
-            ((-1, 0, 0), (0, 1, 0), (0, 0, 1)),
-            ((1, 0, 0), (0, 0, 1), (0, 1, 0)),
+        """Box with outward faces, 24 vertices and 12 triangles, in the
+        reference's vertex order and winding (mesh.py:131-189): faces -y, +y,
+        -z, +z, -x, +x; face corners (n + a + b, n + a - b, n - a - b,
+        n - a + b) / 2 with uvs (0,0), (1,0), (1,1), (0,1); triangles
+        (0, 2, 1) and (0, 3, 2) of each face."""
+        faces = [  # (normal n, edge a, edge b)
+            ((0, -1, 0), (-1, 0, 0), (0, 0, -1)),
+            ((0, 1, 0), (-1, 0, 0), (0, 0, 1)),
+            ((0, 0, -1), (-1, 0, 0), (0, 1, 0)),
+            ((0, 0, 1), (1, 0, 0), (0, 1, 0)),
+            ((-1, 0, 0), (0, 0, 1), (0, 1, 0)),
+            ((1, 0, 0), (0, 0, -1), (0, 1, 0)),
         ]
+        corners = ((1, 1), (1, -1), (-1, -1), (-1, 1))
+        uvs = ((0.0, 0.0), (1.0, 0.0), (1.0, 1.0), (0.0, 1.0))
         verts, idx = [], []
-        for n, u, w in faces:
-            n, u, w = np.array(n, float), np.array(u, float), np.array(w, float)
+        for n, a, b in faces:
+            n, a, b = np.array(n, float), np.array(a, float), np.array(b, float)
             base = len(verts)
-            for su, sw in ((-1, -1), (1, -1), (1, 1), (-1, 1)):
-                p = 0.5 * n + 0.5 * su * u + 0.5 * sw * w
-                verts.append([*p, *n, (su + 1) / 2, (sw + 1) / 2])
-            # wind so that cross(p1 - p0, p2 - p0) points along n
-            a, b, c = (np.array(verts[base + k][:3]) for k in (0, 1, 2))
-            if np.dot(np.cross(b - a, c - a), n) > 0:
-                idx += [[base, base + 1, base + 2], [base, base + 2, base + 3]]
-            else:
-                idx += [[base, base + 2, base + 1], [base, base + 3, base + 2]]
+            for (sa, sb), uv in zip(corners, uvs):
+                verts.append([*(0.5 * (n + sa * a + sb * b)), *n, *uv])
+            idx += [[base, base + 2, base + 1], [base, base + 3, base + 2]]
         v = np.array(verts, dtype=np.float32)
         v[:, 0:3] *= np.asarray(size, dtype=np.float32)
         return cls(v, np.array(idx, dtype=np.uint32))

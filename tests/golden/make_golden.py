@@ -33,7 +33,14 @@ HERE = Path(__file__).resolve().parent
 REF = Path(os.environ.get("NAN_REFERENCE_ROOT", HERE.parents[2] / "reference"))
 
 
-class _Inert:
+class _InertMeta(type):
+    """Class-level attribute lookups of a stub (``spy.KeyCode.a``) yield inert values too."""
+
+    def __getattr__(cls, name):
+        return _Inert()
+
+
+class _Inert(metaclass=_InertMeta):
     """Stand-in for any attribute of a stubbed graphics module."""
 
     def __init__(self, *args, **kwargs):
@@ -60,6 +67,75 @@ def _install_stubs() -> None:
     scene_node = types.ModuleType("scene_node")
     scene_node.SceneNode = _Inert  # type: ignore[attr-defined]
     sys.modules["scene_node"] = scene_node
+
+
+class _F32(np.ndarray):
+    """float32 vector standing in for slangpy's float2/float3 (components .x/.y/.z)."""
+
+    x = property(lambda self: self[0])
+    y = property(lambda self: self[1])
+    z = property(lambda self: self[2])
+
+
+def _f32(*components):
+    return np.asarray(components, dtype=np.float32).view(_F32)
+
+
+def _host_records(out: dict) -> None:
+    """Host-side records of the reference's own Python: the Halton jitter of
+    Camera.begin_frame (camera.py:4-23, 87-96), the mesh factories
+    (mesh.py:31-189) and the 16-byte descriptor packing (scene.py:85-108).
+    slangpy's float2 and frac are stood in by float32 numpy arrays; the
+    camera's image-plane basis and the transform matrices go through slangpy
+    math that is not installed here, so they are not recorded."""
+    for name in ("event_dispatcher", "event_dispatcher.sync_dispatcher"):
+        _stub(name)
+    import camera as ref_camera  # noqa: E402
+    import mesh as ref_mesh  # noqa: E402
+    import scene as ref_scene  # noqa: E402
+
+    spy = sys.modules["slangpy"]
+    spy.float2 = _f32
+    spy.math.frac = lambda v: (v - np.floor(v)).astype(np.float32).view(_F32)
+    out["halton_index"] = np.arange(0, 200, dtype=np.int64)
+    out["halton_base2"] = np.asarray([ref_camera.halton(i, 2) for i in range(200)], np.float64)
+    out["halton_base3"] = np.asarray([ref_camera.halton(i, 3) for i in range(200)], np.float64)
+    sizes = np.asarray([[256, 256], [1920, 1080], [3840, 2160], [64, 48]], np.int64)
+    jitter = np.zeros((sizes.shape[0], 40, 2), np.float32)
+    for k, (w, h) in enumerate(sizes):
+        cam = object.__new__(ref_camera.Camera)  # begin_frame's own code, without the slangpy basis
+        cam.sample_pattern = ref_camera.HaltonSamplePattern(16)
+        cam.jitter = _f32(0.0, 0.0)
+        cam.frame_index = 0
+        cam._has_prev_matrices = False
+        cam.recompute = lambda: None
+        for f in range(40):
+            cam.begin_frame(int(w), int(h))
+            jitter[k, f] = (cam.jitter.x, cam.jitter.y)
+    out["camera_sizes"] = sizes
+    out["camera_jitter"] = jitter
+
+    meshes = {
+        "cube_1": ref_mesh.Mesh.create_cube((1.0, 1.0, 1.0)),
+        "cube_a": ref_mesh.Mesh.create_cube((0.6, 1.2, 0.6)),
+        "cube_b": ref_mesh.Mesh.create_cube((2.5, 0.3, 1.1)),
+        "quad": ref_mesh.Mesh.create_quad((2.0, 3.0)),
+        "quad_yz_pos": ref_mesh.Mesh.create_quad_yz((2.0, 3.0), True),
+        "quad_yz_neg": ref_mesh.Mesh.create_quad_yz((2.0, 3.0), False),
+        "quad_xy_pos": ref_mesh.Mesh.create_quad_xy((2.0, 3.0), True),
+        "quad_xy_neg": ref_mesh.Mesh.create_quad_xy((2.0, 3.0), False),
+    }
+    for key, m in meshes.items():
+        out[f"mesh_{key}_vertices"] = np.asarray(m.vertices, np.float32)
+        out[f"mesh_{key}_indices"] = np.asarray(m.indices, np.uint32)
+    mesh_fields = np.asarray([[36, 108, 0, 0], [24, 36, 36, 108], [4, 6, 60, 144]], np.uint32)
+    inst_fields = np.asarray([[0, 1, 0, 0], [2, 0, 5, 1], [1, 3, 2, 0]], np.uint32)
+    out["desc_mesh_fields"] = mesh_fields
+    out["desc_mesh_packed"] = np.frombuffer(
+        b"".join(ref_scene.Scene.MeshDesc(*map(int, r)).pack() for r in mesh_fields), np.uint32).reshape(-1, 4)
+    out["desc_instance_fields"] = inst_fields
+    out["desc_instance_packed"] = np.frombuffer(
+        b"".join(ref_scene.Scene.InstanceDesc(*map(int, r)).pack() for r in inst_fields), np.uint32).reshape(-1, 4)
 
 
 def main() -> None:
@@ -388,6 +464,7 @@ def main() -> None:
         out[f"flt{k}_audit"] = indices(audit)
         out[f"flt{k}_repair"] = indices(repair)
 
+    _host_records(out)
     np.savez_compressed(HERE / "reference_vectors.npz", **out)
     print("wrote", HERE / "reference_vectors.npz", {k: v.shape for k, v in out.items()})
 

@@ -294,14 +294,63 @@ def test_baker_rejects_wrong_field_before_any_launch():
 
 # ---- camera host math (camera.py:4-96) -----------------------------------------
 
-def test_halton_pattern_cycles_sixteen_points():
-    from nan_b200.camera import HaltonSamplePattern, halton
+def test_halton_matches_reference(golden):
+    from nan_b200.camera import halton
 
-    assert halton(1, 2) == 0.5 and abs(halton(1, 3) - 1 / 3) < 1e-15
-    pattern = HaltonSamplePattern(16)
-    first = [tuple(pattern.next()) for _ in range(16)]
-    again = [tuple(pattern.next()) for _ in range(16)]
-    assert first == again and len(set(first)) == 16
+    got2 = np.asarray([halton(int(i), 2) for i in golden["halton_index"]])
+    got3 = np.asarray([halton(int(i), 3) for i in golden["halton_index"]])
+    np.testing.assert_array_equal(got2, golden["halton_base2"])
+    np.testing.assert_array_equal(got3, golden["halton_base3"])
+
+
+def test_camera_jitter_sequence_matches_reference(golden):
+    """Camera.begin_frame's jitter over 40 frames (two cycles of the 16-point
+    Halton(2,3) pattern) at four image sizes, bit for bit against the
+    reference's camera.py:87-96 run on the same frames."""
+    from nan_b200.camera import Camera
+
+    for (w, h), expect in zip(golden["camera_sizes"], golden["camera_jitter"]):
+        cam = Camera()
+        got = np.zeros_like(expect)
+        for f in range(expect.shape[0]):
+            cam.begin_frame(int(w), int(h))
+            got[f] = cam.jitter
+        np.testing.assert_array_equal(got.view(np.uint32), expect.view(np.uint32))
+
+
+def test_mesh_factories_match_reference(golden):
+    """Vertex records (position, normal, uv; 32 B) and triangle order of the
+    reference's mesh factories (mesh.py:31-189)."""
+    from nan_b200.scene_node import Mesh
+
+    made = {
+        "cube_1": Mesh.cube((1.0, 1.0, 1.0)), "cube_a": Mesh.cube((0.6, 1.2, 0.6)),
+        "cube_b": Mesh.cube((2.5, 0.3, 1.1)), "quad": Mesh.quad((2.0, 3.0)),
+        "quad_yz_pos": Mesh.quad_yz((2.0, 3.0), True), "quad_yz_neg": Mesh.quad_yz((2.0, 3.0), False),
+        "quad_xy_pos": Mesh.quad_xy((2.0, 3.0), True), "quad_xy_neg": Mesh.quad_xy((2.0, 3.0), False),
+    }
+    for key, m in made.items():
+        np.testing.assert_array_equal(m.vertices, golden[f"mesh_{key}_vertices"], err_msg=key)
+        np.testing.assert_array_equal(m.indices, golden[f"mesh_{key}_indices"], err_msg=key)
+
+
+def test_descriptor_records_match_reference(golden):
+    """SceneNode.pack's mesh and instance descriptors are the reference's
+    16-byte MeshDesc / InstanceDesc records (scene.py:85-108): fields in the
+    same order, one u32 each."""
+    from nan_b200.scene_node import Material, Mesh, SceneNode, make_transform
+
+    np.testing.assert_array_equal(golden["desc_mesh_packed"], golden["desc_mesh_fields"])
+    np.testing.assert_array_equal(golden["desc_instance_packed"], golden["desc_instance_fields"])
+    node = SceneNode()
+    a = node.add_mesh(Mesh.cube((1.0, 1.0, 1.0)))
+    b = node.add_mesh(Mesh.quad((2.0, 3.0)))
+    mat = node.add_material(Material())
+    node.add_instance(a, mat, node.add_transform(make_transform()))
+    node.add_instance(b, mat, node.add_transform(make_transform(scaling=(-1.0, 1.0, 1.0))))
+    packed = node.pack()
+    np.testing.assert_array_equal(packed["mesh_descs"], [[24, 36, 0, 0], [4, 6, 24, 36]])
+    np.testing.assert_array_equal(packed["instance_descs"], [[0, 0, 0, 0], [1, 0, 1, 1]])
 
 
 def test_camera_basis_is_orthogonal_and_scaled():
