@@ -140,7 +140,10 @@ def test_noalloc_build_error_paths(device):
     m = int(big.info()["triangle_count"])
     assert m > 350_000
     ctx2 = device.new_context()
-    rc = _call(ctx2, big, nodes, nb, tris, tb, refs, rb)
+    big_buf = torch.empty((max(m - 1, 1) * 16 + m * 12 + m * 2,), dtype=torch.float32, device=device.torch_device)
+    bn, bt = big_buf.data_ptr(), big_buf.data_ptr() + max(m - 1, 1) * 64
+    br = bt + m * 48
+    rc = _call(ctx2, big, bn, max(m - 1, 1) * 64, bt, m * 48, br, m * 8)
     assert rc == _native.NAN_ERR_LIMIT, (rc, _last_error())
     assert "64 MiB" in _last_error()
     ctx2.close()
