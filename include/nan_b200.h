@@ -671,7 +671,10 @@ typedef struct NanCacheConfig {
     float beta2;
     float epsilon;
     float loss_epsilon;        /* relative L2: (o - y)^2 / (o^2 + loss_epsilon) */
-    uint32_t reserved[4];
+    uint32_t table_update;     /* hash-table optimizer step: 0 = Adam over every entry; 1 = lazy
+                                  Adam, only entries whose gradient is nonzero in the step (their
+                                  moments and parameters; bias correction by the global step) */
+    uint32_t reserved[3];
 } NanCacheConfig;
 
 /* Scratch and outputs of one cached frame (nan_trace_screen_cached). */
@@ -716,6 +719,9 @@ NAN_B200_API int nan_cache_backward(NanCache* cache, const float* queries, const
 /* One Adam step from the accumulated gradients, which it then clears. */
 NAN_B200_API int nan_cache_step(NanCache* cache, void* stream);
 /* Train on `count` samples in batches of `batch`: backward + step each. */
+/* Learning rate of the following optimizer steps (a schedule set by the
+ * caller). Host state only. No counterpart in the reference. */
+NAN_B200_API int nan_cache_set_learning_rate(NanCache* cache, float learning_rate);
 NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const float* targets,
                                  uint32_t count, uint32_t batch, void* stream);
 

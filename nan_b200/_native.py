@@ -144,7 +144,8 @@ class NanCacheConfig(ctypes.Structure):
         ("beta2", ctypes.c_float),
         ("epsilon", ctypes.c_float),
         ("loss_epsilon", ctypes.c_float),
-        ("reserved", ctypes.c_uint32 * 4),
+        ("table_update", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32 * 3),
     ]
 
 
@@ -289,6 +290,7 @@ EXPORTS = {
     "nan_cache_infer": (_I, [_VP, _VP, _U32, _VP, _VP]),
     "nan_cache_backward": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
     "nan_cache_step": (_I, [_VP, _VP]),
+    "nan_cache_set_learning_rate": (_I, [_VP, ctypes.c_float]),
     "nan_cache_train": (_I, [_VP, _VP, _VP, _U32, _U32, _VP]),
     "nan_batch_create": (_I, [_VP, _VP, _U32, ctypes.POINTER(_VP)]),
     "nan_batch_destroy": (_I, [_VP]),

@@ -67,6 +67,7 @@ int check_config(const NanCacheConfig* c) {
     if (!(c->learning_rate > 0.0f) || !(c->beta1 >= 0.0f && c->beta1 < 1.0f) || !(c->beta2 >= 0.0f && c->beta2 < 1.0f) ||
         !(c->epsilon >= 0.0f) || !(c->loss_epsilon > 0.0f))
         return invalid("bad optimizer or loss parameter");
+    if (c->table_update > 1) return invalid("table_update must be 0 (dense Adam) or 1 (lazy Adam)");
     return NAN_OK;
 }
 }  // namespace
@@ -710,6 +711,13 @@ NAN_B200_API int nan_cache_step(NanCache* cache, void* stream) {
     int rc = cache_enter(cache);
     if (rc) return rc;
     return nan_host::launch_cache_step(cache, as_stream(stream));
+}
+
+NAN_B200_API int nan_cache_set_learning_rate(NanCache* cache, float learning_rate) {
+    if (!cache) return invalid("null cache");
+    if (!(learning_rate >= 0.0f) || !std::isfinite(learning_rate)) return invalid("learning rate must be finite and >= 0");
+    cache->cfg.learning_rate = learning_rate;
+    return NAN_OK;
 }
 
 NAN_B200_API int nan_cache_train(NanCache* cache, const float* queries, const float* targets, uint32_t count,

@@ -548,11 +548,16 @@ __global__ void k_cache_adam_mlp(float* __restrict__ p, float* __restrict__ m, f
     *reinterpret_cast<__nv_bfloat16*>(img + img_of(layer) + tc::tile_offset(row, col, cols)) = b;
 }
 
+// kLazy: only the entries with a nonzero gradient pair in this step are
+// updated (lazy Adam); the others keep their parameters and moments, and the
+// pass reads just their gradient.
+template <bool kLazy>
 __global__ void k_cache_adam_table(float2* __restrict__ p, float2* __restrict__ m, float2* __restrict__ v,
                                    float2* __restrict__ g, __half2* __restrict__ t16, size_t n, AdamArgs h) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        float2 pi = p[i], mi = m[i], vi = v[i];
         const float2 gi = g[i];
+        if (kLazy && gi.x == 0.0f && gi.y == 0.0f) continue;
+        float2 pi = p[i], mi = m[i], vi = v[i];
         pi.x = adam_one(pi.x, mi.x, vi.x, gi.x, h);
         pi.y = adam_one(pi.y, mi.y, vi.y, gi.y, h);
         p[i] = pi;
@@ -751,8 +756,12 @@ int launch_cache_step(NanCache* k, cudaStream_t st) {
     const size_t nt = k->table_params, pairs = nt / 2;
     float2* t = reinterpret_cast<float2*>(k->table);
     const int blocks = (int)std::min<size_t>((pairs + 255) / 256, (size_t)sm_count(k->ctx->device) * 16u);
-    k_cache_adam_table<<<blocks, 256, 0, st>>>(t, t + pairs, t + 2 * pairs, t + 3 * pairs,
-                                               reinterpret_cast<__half2*>(k->table16), pairs, h);
+    if (k->cfg.table_update == 1u)
+        k_cache_adam_table<true><<<blocks, 256, 0, st>>>(t, t + pairs, t + 2 * pairs, t + 3 * pairs,
+                                                         reinterpret_cast<__half2*>(k->table16), pairs, h);
+    else
+        k_cache_adam_table<false><<<blocks, 256, 0, st>>>(t, t + pairs, t + 2 * pairs, t + 3 * pairs,
+                                                          reinterpret_cast<__half2*>(k->table16), pairs, h);
     k->ctx->launches += 2;
     cudaError_t err = cudaGetLastError();
     if (err == cudaSuccess) err = cudaMemsetAsync(k->loss, 0, sizeof(float), st);

@@ -32,10 +32,19 @@ def scene_bounds(scene, margin: float = 1e-3):
 def compare(device, scene, width: int, height: int, *, reference_frames: int = 512, frames: int = 64,
             max_vertices: int = 5, train_samples: int = 65536, train_batch: int = 65536, log2_table: int = 19,
             base_resolution: int = 16, max_resolution: int = 2048, learning_rate: float = 1e-2,
-            checkpoints=None, seed: int = 0, cache_vertex: int = 1, warmup_frames: int = 0) -> dict:
+            checkpoints=None, seed: int = 0, cache_vertex: int = 1, warmup_frames: int = 0,
+            table_update: str = "dense", lr_decay: float = 1.0, lr_min: float = 0.0,
+            train_frames: int | None = None) -> dict:
     """Curves (frames, cumulative ms, relative RMSE) of the plain and the
     cached integrator, and the time each needs to reach the plain
-    integrator's RMSE after `frames` frames (within 1.1x for the cached one)."""
+    integrator's RMSE after `frames` frames (within 1.1x for the cached one).
+
+    Training schedule of the cached integrator: the learning rate of
+    training frame f (warm-up frames first) is max(learning_rate *
+    lr_decay**f, lr_min); after `train_frames` training frames (None: all)
+    the cache is frozen and frames only render. `frontier` lists, for every
+    plain checkpoint k, the time each integrator needs to reach the plain
+    RMSE after k frames (1.1x for the cached one)."""
     import torch
 
     from .cached_path_tracer import CachedPathTracer
@@ -61,12 +70,21 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
 
     warm_ms = {}
 
-    def run(tracer, warmup=0) -> list[tuple[int, float, float]]:
+    def schedule(tracer, f):
+        if not hasattr(tracer, "cache") or not getattr(tracer, "_schedule", False):
+            return
+        if train_frames is not None and f >= train_frames:
+            tracer.train = False
+        else:
+            tracer.cache.set_learning_rate(max(learning_rate * lr_decay ** f, lr_min))
+
+    def run(tracer, warmup=0, every=None) -> list[tuple[int, float, float]]:
         acc = torch.zeros((height, width, 3), dtype=torch.float64, device=device.torch_device)
         curve, total_ms = [], 0.0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         for f in range(warmup):
+            schedule(tracer, f)
             cam.begin_frame(width, height)
             e0.record(stream)
             tracer.execute(stream, out, frames + f)
@@ -75,6 +93,7 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
             total_ms += e0.elapsed_time(e1)
         warm_ms[id(tracer)] = total_ms
         for f in range(frames):
+            schedule(tracer, warmup + f)
             cam.begin_frame(width, height)
             e0.record(stream)
             tracer.execute(stream, out, f)
@@ -82,17 +101,19 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
             acc += out[..., :3].double()
             e1.synchronize()
             total_ms += e0.elapsed_time(e1)
-            if f + 1 in checkpoints:
+            if f + 1 in checkpoints or (every and (f + 1) % every == 0):
                 curve.append((f + 1, total_ms, _rel_rmse(acc / (f + 1), ref)))
         return curve
 
     plain_curve = run(plain)
     lo, hi = scene_bounds(scene)
     cache = RadianceCache(device, lo, hi, log2_table=log2_table, base_resolution=base_resolution,
-                          max_resolution=max_resolution, learning_rate=learning_rate, seed=seed)
+                          max_resolution=max_resolution, learning_rate=learning_rate, seed=seed,
+                          table_update=table_update)
     cached = CachedPathTracer(device, scene, cache, cache_vertex=cache_vertex, max_vertices=max_vertices,
                               train_samples=train_samples, train_batch=train_batch)
-    cached_curve = run(cached, warmup_frames)
+    cached._schedule = True
+    cached_curve = run(cached, warmup_frames, every=1)
     cached_warm_ms = warm_ms[id(cached)]
     # the same cached integrator with the cache left untrained: what training gains
     cold = RadianceCache(device, lo, hi, log2_table=log2_table, base_resolution=base_resolution,
@@ -103,6 +124,11 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
     target = plain_curve[-1][2]
     t_plain = plain_curve[-1][1]
     t_cached = next((ms for (_, ms, e) in cached_curve if e <= 1.1 * target), None)
+    frontier = []
+    for k, ms_p, e_p in plain_curve:
+        ms_c = next((ms for (_, ms, e) in cached_curve if e <= 1.1 * e_p), None)
+        frontier.append({"plain_frames": k, "target_rmse": e_p, "plain_ms": ms_p, "cached_ms": ms_c,
+                         "speedup": (ms_p / ms_c) if ms_c else None})
     device.check()
     return {
         "width": width, "height": height, "frames": frames, "reference_frames": reference_frames,
@@ -110,7 +136,9 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
         "cache_vertex": cache_vertex, "warmup_frames": warmup_frames,
         "plain": plain_curve, "cached": cached_curve, "untrained": untrained_curve,
         "target_rmse": target, "plain_ms_to_target": t_plain, "cached_ms_to_target": t_cached,
-        "speedup": (t_plain / t_cached) if t_cached else None,
+        "speedup": (t_plain / t_cached) if t_cached else None, "frontier": frontier,
+        "schedule": {"table_update": table_update, "learning_rate": learning_rate, "lr_decay": lr_decay,
+                     "lr_min": lr_min, "train_frames": train_frames},
         "plain_ms_per_frame": plain_curve[-1][1] / frames,
         "cached_ms_per_frame": (cached_curve[-1][1] - cached_warm_ms) / frames, "cached_warmup_ms": cached_warm_ms,
         "untrained_ms_per_frame": untrained_curve[-1][1] / frames,

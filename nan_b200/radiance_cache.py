@@ -24,6 +24,9 @@ from ._native import NanCacheConfig, check, lib, ptr, stream_handle
 LEVELS = 16
 LAYER_SHAPES = ((64, 48), (64, 64), (64, 64), (64, 64), (16, 64))
 MLP_PARAMS = sum(r * c for r, c in LAYER_SHAPES)
+# hash-table optimizer step: Adam over every entry, or lazy Adam over the
+# entries the step's samples touched
+TABLE_UPDATES = {"dense": 0, "lazy": 1}
 
 
 def initial_parameters(log2_table: int, seed: int = 0):
@@ -45,7 +48,8 @@ def initial_parameters(log2_table: int, seed: int = 0):
 class RadianceCache:
     def __init__(self, device, bounds_min, bounds_max, *, log2_table: int = 19, base_resolution: int = 16,
                  max_resolution: int = 2048, learning_rate: float = 1e-2, beta1: float = 0.9, beta2: float = 0.99,
-                 epsilon: float = 1e-15, loss_epsilon: float = 1e-2, seed: int = 0):
+                 epsilon: float = 1e-15, loss_epsilon: float = 1e-2, table_update: str = "dense",
+                 seed: int = 0):
         import torch
 
         self.device = device
@@ -61,6 +65,9 @@ class RadianceCache:
         cfg.beta2 = float(beta2)
         cfg.epsilon = float(epsilon)
         cfg.loss_epsilon = float(loss_epsilon)
+        if table_update not in TABLE_UPDATES:
+            raise ValueError(f"table_update must be one of {sorted(TABLE_UPDATES)}")
+        cfg.table_update = TABLE_UPDATES[table_update]
         self.config = cfg
         n_mlp, n_table = ctypes.c_uint64(), ctypes.c_uint64()
         check(lib().nan_cache_sizes(ctypes.byref(cfg), ctypes.byref(n_mlp), ctypes.byref(n_table)))
@@ -125,6 +132,11 @@ class RadianceCache:
         n = queries.shape[0]
         check(lib().nan_cache_backward(self.handle, ptr(queries), ptr(targets), n, int(batch or n),
                                        stream_handle(stream)))
+
+    def set_learning_rate(self, learning_rate: float) -> None:
+        """Learning rate of the following optimizer steps."""
+        check(lib().nan_cache_set_learning_rate(self.handle, float(learning_rate)))
+        self.config.learning_rate = float(learning_rate)
 
     def step(self, stream=None) -> None:
         check(lib().nan_cache_step(self.handle, stream_handle(stream)))

@@ -200,13 +200,24 @@ def loss_and_grads(cfg, table_f16, params, queries, targets, batch=None):
     return loss, gp, gt.reshape(-1)
 
 
-def adam(cfg, param, m, v, grad, step):
-    """One Adam step (float64); returns new (param, m, v). `step` counts from 1."""
-    m = cfg.beta1 * m + (1.0 - cfg.beta1) * grad
-    v = cfg.beta2 * v + (1.0 - cfg.beta2) * grad * grad
-    mh = m / (1.0 - cfg.beta1**step)
-    vh = v / (1.0 - cfg.beta2**step)
-    return param - cfg.lr * mh / (np.sqrt(vh) + cfg.eps), m, v
+def adam(cfg, param, m, v, grad, step, lazy=False):
+    """One Adam step (float64); returns new (param, m, v). `step` counts from 1.
+
+    lazy: the step applies only where the gradient is nonzero -- elsewhere the
+    parameter and both moments stay as they are -- with the bias correction
+    of the global step (lazy Adam, as for sparse embedding tables). The
+    table's entries come in (feature 0, feature 1) pairs, and a pair is
+    updated when either of its gradients is nonzero."""
+    m1 = cfg.beta1 * m + (1.0 - cfg.beta1) * grad
+    v1 = cfg.beta2 * v + (1.0 - cfg.beta2) * grad * grad
+    mh = m1 / (1.0 - cfg.beta1**step)
+    vh = v1 / (1.0 - cfg.beta2**step)
+    p1 = param - cfg.lr * mh / (np.sqrt(vh) + cfg.eps)
+    if not lazy:
+        return p1, m1, v1
+    g2 = grad.reshape(-1, 2)
+    on = np.repeat((g2[:, 0] != 0) | (g2[:, 1] != 0), 2)
+    return np.where(on, p1, param), np.where(on, m1, m), np.where(on, v1, v)
 
 
 def init_params(cfg: CacheConfig, seed: int = 0):

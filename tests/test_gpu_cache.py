@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 LOG2 = 14
 
 
-def _setup(device, seed=0, n=1000, table_scale=0.5):
+def _setup(device, seed=0, n=1000, table_scale=0.5, table_update="dense"):
     import torch
 
     import nan_b200
@@ -28,7 +28,8 @@ def _setup(device, seed=0, n=1000, table_scale=0.5):
     cfg = lrc.CacheConfig(log2_table=LOG2, base_resolution=4, max_resolution=256,
                           bounds_min=(-2.0, -1.0, -3.0), bounds_max=(2.0, 3.0, 1.0))
     cache = nan_b200.RadianceCache(device, cfg.bounds_min, cfg.bounds_max, log2_table=LOG2,
-                                   base_resolution=cfg.base_resolution, max_resolution=cfg.max_resolution)
+                                   base_resolution=cfg.base_resolution, max_resolution=cfg.max_resolution,
+                                   table_update=table_update)
     rng = np.random.default_rng(seed)
     params, _ = lrc.init_params(cfg, seed=seed)
     table = rng.uniform(-table_scale, table_scale, lrc.LEVELS * cfg.table_size * 2).astype(np.float32)
@@ -104,6 +105,40 @@ def test_cache_adam_step_matches_oracle(device):
     # the step cleared the gradients
     g2, gt2, loss2 = cache.gradients()
     assert float(g2.abs().max()) == 0.0 and float(gt2.abs().max()) == 0.0 and float(loss2[0]) == 0.0
+
+
+def test_cache_lazy_table_steps_match_oracle(device):
+    """Lazy Adam on the table: two steps on different samples equal the
+    oracle's lazy steps from the GPU's own gradients; entries no sample
+    touched keep their parameters bit for bit."""
+    import torch
+
+    from oracle import lrc
+
+    cfg, cache, params, table, table16, q, y = _setup(device, seed=4, n=512, table_update="lazy")
+    cfg.lr, cfg.beta1, cfg.beta2, cfg.eps = 1e-2, 0.9, 0.99, 1e-15
+    p = params.astype(np.float64)
+    t = table.astype(np.float64)
+    mp, vp = np.zeros_like(p), np.zeros_like(p)
+    mt, vt = np.zeros_like(t), np.zeros_like(t)
+    touched = np.zeros(t.size, bool)
+    for s, part in enumerate((slice(0, 256), slice(256, 512))):
+        cache.backward(torch.from_numpy(np.ascontiguousarray(q[part])).cuda(),
+                       torch.from_numpy(np.ascontiguousarray(y[part])).cuda())
+        g, gt, _ = cache.gradients()
+        g = g.cpu().numpy().astype(np.float64)
+        gt = gt.cpu().numpy().astype(np.float64)
+        touched |= np.repeat((gt.reshape(-1, 2) != 0).any(axis=1), 2)
+        cache.step()
+        p, mp, vp = lrc.adam(cfg, p, mp, vp, g, s + 1)
+        t, mt, vt = lrc.adam(cfg, t, mt, vt, gt, s + 1, lazy=True)
+    p_new, t_new = cache.get_params()
+    p_new, t_new = p_new.cpu().numpy(), t_new.cpu().numpy()
+    assert np.allclose(p_new, p, rtol=1e-5, atol=1e-6)
+    assert np.allclose(t_new, t, rtol=1e-5, atol=1e-6)
+    assert 0 < touched.sum() < touched.size
+    np.testing.assert_array_equal(t_new[~touched], table[~touched])
+    cache.check()
 
 
 def test_cache_training_fits_a_smooth_field(device):
