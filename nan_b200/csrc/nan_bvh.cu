@@ -281,7 +281,7 @@ __global__ void k_emit(uint32_t interior, const int2* __restrict__ children, con
 // smallest surface area, mutual nearest neighbours merge into a new interior
 // node, and the cluster list is compacted (order preserved).
 // ---------------------------------------------------------------------------
-constexpr int kPlocRadius = 16;
+constexpr int kPlocRadius = 64;
 constexpr int kPlocBlock = 256;
 constexpr int kMaxLeafTris = 3;  // the wide nodes' leaf encoding holds up to 3 triangles
 
