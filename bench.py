@@ -537,16 +537,20 @@ def learned_cache_line(device) -> dict:
            "image": "1920x1080, 1 spp per frame, 5 path vertices", "runs": []}
     for cv, batch in ((1, 16384), (0, 8192)):
         r = learned_eval.compare(device, scene, 1920, 1080, reference_frames=256, frames=64, cache_vertex=cv,
-                                 warmup_frames=32, train_batch=batch)
+                                 warmup_frames=32, train_batch=batch, table_update="lazy")
         out["runs"].append({
             "cache_vertex": cv, "warmup_frames": 32, "train_samples_per_frame": 65536, "train_batch": batch,
+            "table_update": "lazy Adam (touched entries only)",
+            "frontier": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in f.items()}
+                         for f in r["frontier"]],
             "target_rmse": r["target_rmse"], "plain_ms_to_target": r["plain_ms_to_target"],
             "cached_ms_to_target": r["cached_ms_to_target"], "speedup": r["speedup"],
             "rmse_after_64_frames": r["rmse_per_frame_count"],
             "ms_per_frame": {"plain": r["plain_ms_per_frame"], "cached": r["cached_ms_per_frame"],
                              "cached_without_training": r["untrained_ms_per_frame"]},
             "cached_warmup_ms": r["cached_warmup_ms"],
-            "cached_curve": [[n, round(ms, 2), round(e, 5)] for n, ms, e in r["cached"]],
+            "cached_curve": [[n, round(ms, 2), round(e, 5)] for n, ms, e in r["cached"]
+                             if n in (1, 2, 4, 8, 12, 16, 24, 32, 48, 64)],
             "plain_curve": [[n, round(ms, 2), round(e, 5)] for n, ms, e in r["plain"]],
         })
         del r
