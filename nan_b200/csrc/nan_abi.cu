@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "nan_internal.h"
@@ -10,6 +11,47 @@
 namespace nan_host {
 
 thread_local std::string g_last_error;
+
+namespace {
+// One memory pool per device for the builders' stream-ordered scratch. The
+// CUDA default pool returns unused memory to the driver at every
+// synchronisation, so a build that synchronises between passes re-maps its
+// scratch each time; this pool keeps it until a context is destroyed.
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[128] = {};
+}  // namespace
+
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mutex);
+        if (!g_pools[dev]) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            err = cudaMemPoolCreate(&g_pools[dev], &props);
+            if (err != cudaSuccess) {
+                g_pools[dev] = nullptr;
+                return err;
+            }
+            uint64_t keep = ~0ull;
+            err = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+            if (err != cudaSuccess) return err;
+        }
+        pool = g_pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+void trim_scratch(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (device >= 0 && device < 128 && g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
+}
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -114,6 +156,7 @@ NAN_B200_API int nan_ctx_destroy(NanContext* ctx) {
     cudaFree(ctx->scratch);
     cudaFree(ctx->d_status);
     cudaFree(ctx->d_counters);
+    nan_host::trim_scratch(ctx->device);
     delete ctx;
     return NAN_OK;
 }

@@ -198,7 +198,7 @@ int launch_filter_audit_repair(NanContext* ctx, const float* cand_pos, const flo
     cudaError_t e = cudaSuccess;
     auto get = [&](size_t bytes) -> void* {
         void* p = nullptr;
-        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) e = nan_host::scratch_alloc(&p, std::max<size_t>(bytes, 16), st);
         if (e == cudaSuccess) owned.push_back(p);
         return p;
     };

@@ -248,29 +248,40 @@ __device__ __forceinline__ float half_area(float4 l, float4 h) {
 }
 
 // 64-byte nodes with padded child boxes; also accumulates the SAH cost.
+// Adds each lane's SAH term into *sah with one atomic per warp (a single
+// address takes one atomic per node otherwise, which serialises millions of
+// them). Every lane of the warp must call it.
+__device__ __forceinline__ void add_sah(double* sah, double cost) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cost += __shfl_down_sync(0xffffffffu, cost, o);
+    if ((threadIdx.x & 31u) == 0u && cost != 0.0) atomicAdd(sah, cost);
+}
+
 __global__ void k_emit(uint32_t interior, const int2* __restrict__ children, const float4* __restrict__ node_lo,
                        const float4* __restrict__ node_hi, const float4* __restrict__ leaf_lo,
                        const float4* __restrict__ leaf_hi, const Bounds* __restrict__ bounds,
                        float4* __restrict__ nodes, double* __restrict__ sah) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= interior) return;
-    const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;  // 2^-18 relative
-    const int2 ch = children[i];
-    float4 al, ah, bl, bh;
-    child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
-    child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
-    nodes[4u * i + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
-    nodes[4u * i + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
-    nodes[4u * i + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
-    // leaves (single triangles in LBVH) as ~(first << 3 | count - 1)
-    const int rx = ch.x < 0 ? ~((~ch.x) << 3) : ch.x;
-    const int ry = ch.y < 0 ? ~((~ch.y) << 3) : ch.y;
-    nodes[4u * i + 3] = make_float4(__int_as_float(rx), __int_as_float(ry), 0.0f, 0.0f);
-    const float root_area = fmaxf(half_area(node_lo[0], node_hi[0]), 1e-30f);
-    double cost = (double)(half_area(node_lo[i], node_hi[i]) / root_area);  // one traversal step
-    if (ch.x < 0) cost += (double)(half_area(al, ah) / root_area);          // one triangle per leaf
-    if (ch.y < 0) cost += (double)(half_area(bl, bh) / root_area);
-    atomicAdd(sah, cost);
+    double cost = 0.0;
+    if (i < interior) {
+        const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;  // 2^-18 relative
+        const int2 ch = children[i];
+        float4 al, ah, bl, bh;
+        child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
+        child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
+        nodes[4u * i + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
+        nodes[4u * i + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
+        nodes[4u * i + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
+        // leaves (single triangles in LBVH) as ~(first << 3 | count - 1)
+        const int rx = ch.x < 0 ? ~((~ch.x) << 3) : ch.x;
+        const int ry = ch.y < 0 ? ~((~ch.y) << 3) : ch.y;
+        nodes[4u * i + 3] = make_float4(__int_as_float(rx), __int_as_float(ry), 0.0f, 0.0f);
+        const float root_area = fmaxf(half_area(node_lo[0], node_hi[0]), 1e-30f);
+        cost = (double)(half_area(node_lo[i], node_hi[i]) / root_area);  // one traversal step
+        if (ch.x < 0) cost += (double)(half_area(al, ah) / root_area);   // one triangle per leaf
+        if (ch.y < 0) cost += (double)(half_area(bl, bh) / root_area);
+    }
+    add_sah(sah, cost);
 }
 
 
@@ -283,6 +294,9 @@ __global__ void k_emit(uint32_t interior, const int2* __restrict__ children, con
 // ---------------------------------------------------------------------------
 constexpr int kPlocRadius = 64;
 constexpr int kPlocBlock = 256;
+constexpr int kPlocBatch = 8;       // PLOC iterations between two host checks of the count
+constexpr int kWideBatch = 4;       // wide-conversion levels between two host checks
+constexpr int kWideMaxLevels = 256;
 constexpr int kMaxLeafTris = 3;  // the wide nodes' leaf encoding holds up to 3 triangles
 
 __device__ __forceinline__ float area_union(float4 al, float4 ah, float4 bl, float4 bh) {
@@ -297,8 +311,15 @@ __global__ void k_ploc_init(uint32_t n, int* __restrict__ idx) {
     if (i < n) idx[i] = ~(int)i;
 }
 
-__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(int c, const float4* __restrict__ lo,
+// The PLOC kernels read the current cluster count from device memory
+// (*count), so that several iterations run back to back without the host;
+// grids are sized for an upper bound of the count, and with one cluster left
+// every kernel does nothing.
+__global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(const uint32_t* __restrict__ count,
+                                                         const float4* __restrict__ lo,
                                                          const float4* __restrict__ hi, int* __restrict__ nn) {
+    const int c = (int)*count;
+    if (c <= 1) return;
     __shared__ float4 slo[kPlocBlock + 2 * kPlocRadius];
     __shared__ float4 shi[kPlocBlock + 2 * kPlocRadius];
     const int b0 = blockIdx.x * kPlocBlock;
@@ -327,13 +348,21 @@ __global__ void __launch_bounds__(kPlocBlock) k_ploc_nn(int c, const float4* __r
     nn[i] = bj;
 }
 
-__global__ void k_ploc_merge(int c, const int* __restrict__ nn, const int* __restrict__ idx,
+// Also clears valid[c .. bound] (bound + 1 flags are scanned).
+__global__ void k_ploc_merge(const uint32_t* __restrict__ count, int bound, const int* __restrict__ nn,
+                             const int* __restrict__ idx,
                              const float4* __restrict__ lo, const float4* __restrict__ hi, int* __restrict__ idx2,
                              float4* __restrict__ lo2, float4* __restrict__ hi2, uint32_t* __restrict__ valid,
                              int2* __restrict__ children, int* __restrict__ node_parent, int* __restrict__ leaf_parent,
                              float4* __restrict__ node_lo, float4* __restrict__ node_hi, uint32_t* node_counter) {
+    const int c = (int)*count;
+    if (c <= 1) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c) return;
+    if (i > bound) return;
+    if (i >= c) {
+        valid[i] = 0u;
+        return;
+    }
     const int j = nn[i];
     if (j >= 0 && nn[j] == i) {
         if (i > j) {
@@ -361,10 +390,16 @@ __global__ void k_ploc_merge(int c, const int* __restrict__ nn, const int* __res
     valid[i] = 1u;
 }
 
-__global__ void k_ploc_compact(int c, const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos,
+// Also writes the next iteration's count (the kept clusters) to *next_count:
+// the count is double-buffered, iteration k reading slot k & 1.
+__global__ void k_ploc_compact(const uint32_t* __restrict__ count, uint32_t* __restrict__ next_count,
+                               const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos,
                                const int* __restrict__ idx2, const float4* __restrict__ lo2,
                                const float4* __restrict__ hi2, int* __restrict__ idx, float4* __restrict__ lo,
                                float4* __restrict__ hi) {
+    const int c = (int)*count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *next_count = c <= 1 ? (uint32_t)c : pos[c];
+    if (c <= 1) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c || !valid[i]) return;
     const uint32_t p = pos[i];
@@ -518,25 +553,26 @@ __global__ void k_emit_dfs(uint32_t interior, const int2* __restrict__ children,
                            const uint32_t* __restrict__ tri_off, const uint32_t* __restrict__ tri_pos, int root,
                            float4* __restrict__ nodes, double* __restrict__ sah) {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= interior) return;
-    const int slot = dfs[x];
-    if (slot < 0 || info[x].collapsed) return;
-    const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;
-    const int2 ch = children[x];
-    float4 al, ah, bl, bh;
-    child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
-    child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
-    nodes[4u * slot + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
-    nodes[4u * slot + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
-    nodes[4u * slot + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
-    const int ra = child_ref(ch.x, dfs, tri_off, tri_pos, info);
-    const int rb = child_ref(ch.y, dfs, tri_off, tri_pos, info);
-    nodes[4u * slot + 3] = make_float4(__int_as_float(ra), __int_as_float(rb), 0.0f, 0.0f);
-    const float root_area = fmaxf(half_area4(node_lo[root], node_hi[root]), 1e-30f);
-    double cost = (double)(half_area4(node_lo[x], node_hi[x]) / root_area);
-    if (ra < 0) cost += (double)(half_area4(al, ah) / root_area) * (double)(((~ra) & 7) + 1);
-    if (rb < 0) cost += (double)(half_area4(bl, bh) / root_area) * (double)(((~rb) & 7) + 1);
-    atomicAdd(sah, cost);
+    const int slot = x < interior ? dfs[x] : -1;
+    double cost = 0.0;
+    if (slot >= 0 && !info[x].collapsed) {
+        const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;
+        const int2 ch = children[x];
+        float4 al, ah, bl, bh;
+        child_box(ch.x, node_lo, node_hi, leaf_lo, leaf_hi, &al, &ah);
+        child_box(ch.y, node_lo, node_hi, leaf_lo, leaf_hi, &bl, &bh);
+        nodes[4u * slot + 0] = make_float4(al.x - pad, ah.x + pad, al.y - pad, ah.y + pad);
+        nodes[4u * slot + 1] = make_float4(bl.x - pad, bh.x + pad, bl.y - pad, bh.y + pad);
+        nodes[4u * slot + 2] = make_float4(al.z - pad, ah.z + pad, bl.z - pad, bh.z + pad);
+        const int ra = child_ref(ch.x, dfs, tri_off, tri_pos, info);
+        const int rb = child_ref(ch.y, dfs, tri_off, tri_pos, info);
+        nodes[4u * slot + 3] = make_float4(__int_as_float(ra), __int_as_float(rb), 0.0f, 0.0f);
+        const float root_area = fmaxf(half_area4(node_lo[root], node_hi[root]), 1e-30f);
+        cost = (double)(half_area4(node_lo[x], node_hi[x]) / root_area);
+        if (ra < 0) cost += (double)(half_area4(al, ah) / root_area) * (double)(((~ra) & 7) + 1);
+        if (rb < 0) cost += (double)(half_area4(bl, bh) / root_area) * (double)(((~rb) & 7) + 1);
+    }
+    add_sah(sah, cost);
 }
 
 
@@ -572,7 +608,16 @@ __device__ __forceinline__ void entry_box(int c, const float4* node_lo, const fl
     }
 }
 
-__global__ void k_wide_level(const WideItem* __restrict__ items, uint32_t count, WideItem* __restrict__ items_out,
+// The first level of the wide conversion: the binary root (the last cluster).
+__global__ void k_wide_root(const int* __restrict__ root, WideItem* __restrict__ items) {
+    items[0] = WideItem{root[0], 0u};
+}
+
+// One level of the wide conversion: *count_in items of this level in, the
+// next level's items appended at *count_out (counters[0] and [1] count the
+// wide nodes and triangles written so far).
+__global__ void k_wide_level(const WideItem* __restrict__ items, const uint32_t* __restrict__ count_in,
+                             WideItem* __restrict__ items_out, uint32_t* __restrict__ count_out,
                              uint32_t* __restrict__ counters, const int2* __restrict__ children,
                              const float4* __restrict__ node_lo, const float4* __restrict__ node_hi,
                              const float4* __restrict__ leaf_lo, const float4* __restrict__ leaf_hi,
@@ -581,7 +626,7 @@ __global__ void k_wide_level(const WideItem* __restrict__ items, uint32_t count,
                              const Bounds* __restrict__ bounds, uint4* __restrict__ wnodes,
                              float4* __restrict__ wtris) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
+    if (k >= *count_in) return;
     const WideItem it = items[k];
     int ent[8];
     float4 elo[8], ehi[8];
@@ -663,7 +708,7 @@ __global__ void k_wide_level(const WideItem* __restrict__ items, uint32_t count,
     }
     const uint32_t child_base = n_int ? atomicAdd(&counters[0], n_int) : 0u;
     const uint32_t tri_base = n_tri ? atomicAdd(&counters[1], n_tri) : 0u;
-    const uint32_t out_base = n_int ? atomicAdd(&counters[2], n_int) : 0u;
+    const uint32_t out_base = n_int ? atomicAdd(count_out, n_int) : 0u;
     // quantization grid: p = node lo, scale 2^e with 255 * 2^e >= extent
     const float pad = ordered_to_float(bounds->max_abs) * 3.814697265625e-6f + 1e-30f;
     const double lo3[3] = {(double)plo.x - pad, (double)plo.y - pad, (double)plo.z - pad};
@@ -735,7 +780,7 @@ __global__ void k_wide_level(const WideItem* __restrict__ items, uint32_t count,
 
 template <class T> T* dmalloc(size_t count, cudaStream_t s, cudaError_t* err) {
     void* p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), s);
+    cudaError_t e = nan_host::scratch_alloc(&p, std::max<size_t>(count, 1) * sizeof(T), s);
     if (e != cudaSuccess && *err == cudaSuccess) *err = e;
     return static_cast<T*>(p);
 }
@@ -745,6 +790,13 @@ uint32_t blocks(uint64_t n) { return (uint32_t)((n + kThreads - 1) / kThreads); 
 }  // namespace
 
 namespace nan_host {
+
+void forget_scene(NanContext* ctx) {
+    ctx->wide_count = 0;
+    ctx->wide_built = false;
+    ctx->has_scene = false;
+    ctx->tri_count = ctx->node_count = ctx->leaf_count = ctx->max_depth = 0;
+}
 
 void free_scene(NanContext* ctx) {
     if (!ctx->caller_owned_bvh) {
@@ -756,14 +808,13 @@ void free_scene(NanContext* ctx) {
     cudaFree(ctx->wtris);
     ctx->wnodes = nullptr;
     ctx->wtris = nullptr;
-    ctx->wide_count = 0;
     ctx->caller_owned_bvh = false;
     ctx->nodes = nullptr;
     ctx->tris = nullptr;
     ctx->tri_refs = nullptr;
-    ctx->has_scene = false;
-    ctx->tri_count = ctx->node_count = ctx->leaf_count = ctx->max_depth = 0;
+    ctx->bvh_capacity = ctx->wide_capacity = 0;
     ctx->device_bytes = 0;
+    forget_scene(ctx);
 }
 
 
@@ -783,7 +834,8 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     int* nn = dmalloc<int>(n, s, &err);
     uint32_t* valid = dmalloc<uint32_t>(n + 1, s, &err);
     uint32_t* pos = dmalloc<uint32_t>(n + 1, s, &err);
-    uint32_t* counter = dmalloc<uint32_t>(2, s, &err);
+    // [0] interior nodes made; [1], [2] live clusters (double-buffered)
+    uint32_t* counter = dmalloc<uint32_t>(3, s, &err);
     SubtreeInfo* info = dmalloc<SubtreeInfo>(interior, s, &err);
     int* dfs = dmalloc<int>(interior, s, &err);
     uint32_t* tri_off = dmalloc<uint32_t>(interior, s, &err);
@@ -793,29 +845,41 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
     if (err != cudaSuccess) return cuda_fail(err, "PLOC scratch allocation");
     cudaMemsetAsync(node_parent, 0xff, interior * sizeof(int), s);
-    cudaMemsetAsync(counter, 0, 2 * sizeof(uint32_t), s);
+    {
+        const uint32_t init[3] = {0u, n, n};
+        cudaMemcpyAsync(counter, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    }
     cudaMemsetAsync(valid, 0, (n + 1) * sizeof(uint32_t), s);
     k_ploc_init<<<blocks(n), kThreads, 0, s>>>(n, idx_a);
     cudaMemcpyAsync(lo_a, leaf_lo, n * sizeof(float4), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(hi_a, leaf_hi, n * sizeof(float4), cudaMemcpyDeviceToDevice, s);
     ctx->launches++;
+    // Iterations run in batches of kPlocBatch without the host: each kernel
+    // reads the live count (counter[1]); the host reads it back once per
+    // batch to size the next batch's grids and to check progress.
     uint32_t c = n;
     int iterations = 0;
     while (c > 1) {
-        if (++iterations > 4096) {
+        if (iterations > 4096) {
             set_error("PLOC did not converge");
             return NAN_ERR_LIMIT;
         }
         const uint32_t grid = (c + kPlocBlock - 1) / kPlocBlock;
-        k_ploc_nn<<<grid, kPlocBlock, 0, s>>>((int)c, lo_a, hi_a, nn);
-        k_ploc_merge<<<blocks(c), kThreads, 0, s>>>((int)c, nn, idx_a, lo_a, hi_a, idx_b, lo_b, hi_b, valid, children,
-                                                    node_parent, leaf_parent, node_lo, node_hi, counter);
-        cudaMemsetAsync(valid + c, 0, sizeof(uint32_t), s);
-        cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, valid, pos, c + 1, s);
-        k_ploc_compact<<<blocks(c), kThreads, 0, s>>>((int)c, valid, pos, idx_b, lo_b, hi_b, idx_a, lo_a, hi_a);
-        ctx->launches += 4;
+        for (int k = 0; k < kPlocBatch; ++k, ++iterations) {
+            uint32_t* live = counter + 1 + (iterations & 1);
+            uint32_t* next_live = counter + 1 + ((iterations + 1) & 1);
+            k_ploc_nn<<<grid, kPlocBlock, 0, s>>>(live, lo_a, hi_a, nn);
+            k_ploc_merge<<<blocks(c + 1), kThreads, 0, s>>>(live, (int)c, nn, idx_a, lo_a, hi_a, idx_b, lo_b, hi_b,
+                                                            valid, children, node_parent, leaf_parent, node_lo,
+                                                            node_hi, counter);
+            cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, valid, pos, c + 1, s);
+            k_ploc_compact<<<blocks(c), kThreads, 0, s>>>(live, next_live, valid, pos, idx_b, lo_b, hi_b, idx_a,
+                                                          lo_a, hi_a);
+            ctx->launches += 4;
+        }
         uint32_t next = 0;
-        err = cudaMemcpyAsync(&next, pos + c, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+        // kPlocBatch is even, so after a batch the live count is in slot 1 + 0
+        err = cudaMemcpyAsync(&next, counter + 1 + (iterations & 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaStreamSynchronize(s);
         if (err != cudaSuccess) return cuda_fail(err, "PLOC iteration");
         if (next >= c) {
@@ -832,48 +896,62 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     k_dfs_nodes<<<blocks(interior), kThreads, 0, s>>>(interior, children, node_parent, info, dfs, tri_off);
     k_dfs_leaves<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, info, tri_pos);
     k_scatter_tris<<<blocks(n), kThreads, 0, s>>>(n, tri_pos, tris_sorted, ctx->tris);
-    err = cudaStreamSynchronize(s);
+    err = cudaGetLastError();
     if (err != cudaSuccess) return cuda_fail(err, "PLOC collapse");
 
     // compressed 8-wide BVH from the collapsed binary tree, level by level
-    if (cudaMalloc(&ctx->wnodes, (size_t)(interior + 1) * 5 * sizeof(uint4)) != cudaSuccess ||
-        cudaMalloc(&ctx->wtris, (size_t)n * 3 * sizeof(float4)) != cudaSuccess) {
-        set_error("out of device memory for the wide BVH");
-        return NAN_ERR_OUT_OF_MEMORY;
+    if (ctx->wide_capacity < n) {
+        cudaFree(ctx->wnodes);
+        cudaFree(ctx->wtris);
+        ctx->wnodes = nullptr;
+        ctx->wtris = nullptr;
+        ctx->wide_capacity = 0;
+        if (cudaMalloc(&ctx->wnodes, (size_t)n * 5 * sizeof(uint4)) != cudaSuccess ||
+            cudaMalloc(&ctx->wtris, (size_t)n * 3 * sizeof(float4)) != cudaSuccess) {
+            set_error("out of device memory for the wide BVH");
+            return NAN_ERR_OUT_OF_MEMORY;
+        }
+        ctx->device_bytes += (uint64_t)n * (5 * sizeof(uint4) + 3 * sizeof(float4));
+        ctx->wide_capacity = n;
     }
-    ctx->device_bytes += (uint64_t)(interior + 1) * 5 * sizeof(uint4) + (uint64_t)n * 3 * sizeof(float4);
     WideItem* items_a = dmalloc<WideItem>(interior + 1, s, &err);
     WideItem* items_b = dmalloc<WideItem>(interior + 1, s, &err);
-    uint32_t* wcount = dmalloc<uint32_t>(3, s, &err);
+    // [0] wide nodes, [1] wide triangles, [2 + l] items of level l
+    uint32_t* wcount = dmalloc<uint32_t>(2 + kWideMaxLevels + 1, s, &err);
     if (err != cudaSuccess) return cuda_fail(err, "wide BVH scratch allocation");
     {
-        int root_host = 0;
-        cudaMemcpyAsync(&root_host, idx_a, sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        const WideItem first{root_host, 0u};
-        const uint32_t init[3] = {1u, 0u, 0u};
-        cudaMemcpyAsync(items_a, &first, sizeof(WideItem), cudaMemcpyHostToDevice, s);
+        // the root item: the binary root; levels run in batches of
+        // kWideBatch without the host, each grid bounded by 8x the last
+        k_wide_root<<<1, 1, 0, s>>>(idx_a, items_a);
+        cudaMemsetAsync(wcount, 0, (2 + kWideMaxLevels + 1) * sizeof(uint32_t), s);
+        const uint32_t init[3] = {1u, 0u, 1u};
         cudaMemcpyAsync(wcount, init, sizeof(init), cudaMemcpyHostToDevice, s);
-        uint32_t level_count = 1u;
-        int levels = 0;
-        while (level_count > 0u) {
-            if (++levels > 256) {
-                set_error("wide BVH conversion did not terminate");
-                return NAN_ERR_LIMIT;
+        uint64_t bound = 1;
+        int level = 0;
+        for (;;) {
+            for (int k = 0; k < kWideBatch; ++k, ++level) {
+                if (level >= kWideMaxLevels) {
+                    set_error("wide BVH conversion did not terminate");
+                    return NAN_ERR_LIMIT;
+                }
+                const WideItem* in = (level & 1) ? items_b : items_a;
+                WideItem* out = (level & 1) ? items_a : items_b;
+                k_wide_level<<<blocks(bound), kThreads, 0, s>>>(in, wcount + 2 + level, out, wcount + 3 + level,
+                                                                wcount, children, node_lo, node_hi, leaf_lo, leaf_hi,
+                                                                info, tri_off, tri_pos, ctx->tris, bounds,
+                                                                ctx->wnodes, ctx->wtris);
+                ctx->launches++;
+                bound = std::min<uint64_t>(bound * 8u, (uint64_t)interior + 1u);
             }
-            cudaMemsetAsync(wcount + 2, 0, sizeof(uint32_t), s);
-            k_wide_level<<<blocks(level_count), kThreads, 0, s>>>(items_a, level_count, items_b, wcount, children,
-                                                                  node_lo, node_hi, leaf_lo, leaf_hi, info, tri_off,
-                                                                  tri_pos, ctx->tris, bounds, ctx->wnodes, ctx->wtris);
-            ctx->launches++;
-            uint32_t counts[3];
-            err = cudaMemcpyAsync(counts, wcount, sizeof(counts), cudaMemcpyDeviceToHost, s);
+            uint32_t pending = 0;
+            err = cudaMemcpyAsync(&pending, wcount + 2 + level, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+            if (err == cudaSuccess) err = cudaMemcpyAsync(&ctx->wide_count, wcount, sizeof(uint32_t),
+                                                          cudaMemcpyDeviceToHost, s);
             if (err == cudaSuccess) err = cudaStreamSynchronize(s);
             if (err != cudaSuccess) return cuda_fail(err, "wide BVH level");
-            level_count = counts[2];
-            ctx->wide_count = counts[0];
-            std::swap(items_a, items_b);
+            if (pending == 0u) break;
         }
+        ctx->wide_built = true;
     }
     cudaFreeAsync(items_a, s);
     cudaFreeAsync(items_b, s);
@@ -910,7 +988,8 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
 
 int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
     cudaError_t err = cudaSuccess;
-    free_scene(ctx);
+    if (ctx->caller_owned_bvh) free_scene(ctx);  // never reuse caller memory
+    else forget_scene(ctx);
     ctx->scene = *sd;
     const uint32_t I = sd->instance_count;
 
@@ -945,18 +1024,29 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
     const uint32_t n = total;
     ctx->tri_count = n;
 
-    // Persistent storage.
+    // Persistent storage, kept from an earlier build when it is large enough.
     const uint32_t interior = n > 1 ? n - 1 : 0;
-    if (cudaMalloc(&ctx->tris, std::max<size_t>(n, 1) * 3 * sizeof(float4)) != cudaSuccess ||
-        cudaMalloc(&ctx->tri_refs, std::max<size_t>(n, 1) * sizeof(uint2)) != cudaSuccess ||
-        cudaMalloc(&ctx->nodes, std::max<size_t>(interior, 1) * 4 * sizeof(float4)) != cudaSuccess) {
-        cudaFreeAsync(offsets, s);
-        free_scene(ctx);
-        set_error("out of device memory for the BVH");
-        return NAN_ERR_OUT_OF_MEMORY;
+    const uint32_t cap = std::max<uint32_t>(n, 1);
+    if (ctx->bvh_capacity < cap) {
+        cudaFree(ctx->tris);
+        cudaFree(ctx->tri_refs);
+        cudaFree(ctx->nodes);
+        ctx->tris = nullptr;
+        ctx->tri_refs = nullptr;
+        ctx->nodes = nullptr;
+        ctx->bvh_capacity = 0;
+        if (cudaMalloc(&ctx->tris, (size_t)cap * 3 * sizeof(float4)) != cudaSuccess ||
+            cudaMalloc(&ctx->tri_refs, (size_t)cap * sizeof(uint2)) != cudaSuccess ||
+            cudaMalloc(&ctx->nodes, (size_t)cap * 4 * sizeof(float4)) != cudaSuccess) {
+            cudaFreeAsync(offsets, s);
+            free_scene(ctx);
+            set_error("out of device memory for the BVH");
+            return NAN_ERR_OUT_OF_MEMORY;
+        }
+        ctx->bvh_capacity = cap;
     }
-    ctx->device_bytes = (uint64_t)n * 3 * sizeof(float4) + (uint64_t)n * sizeof(uint2) +
-                        (uint64_t)std::max<uint32_t>(interior, 1) * 4 * sizeof(float4);
+    ctx->device_bytes = (uint64_t)ctx->bvh_capacity * (3 * sizeof(float4) + sizeof(uint2) + 4 * sizeof(float4)) +
+                        (uint64_t)ctx->wide_capacity * (5 * sizeof(uint4) + 3 * sizeof(float4));
 
     if (n == 0) {
         cudaFreeAsync(offsets, s);

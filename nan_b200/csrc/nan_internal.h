@@ -25,6 +25,11 @@ struct NanContext {
     uint4* wnodes = nullptr;        // compressed 8-wide nodes, 5 uint4 each (PLOC builds only)
     float4* wtris = nullptr;        // triangles in the wide nodes' leaf order
     uint32_t wide_count = 0;
+    bool wide_built = false;        // wnodes/wtris hold this scene's wide BVH
+    // Triangles the owned storage holds: nodes/tris/tri_refs, and the wide
+    // nodes/triangles. A rebuild that fits reuses them (grow-only).
+    uint32_t bvh_capacity = 0;
+    uint32_t wide_capacity = 0;
     int root = 0;
     uint32_t tri_count = 0;
     uint32_t node_count = 0;
@@ -87,9 +92,16 @@ struct NanBatch {
 namespace nan_host {
 
 void set_error(const std::string& msg);
+// Stream-ordered scratch from this library's pool on the current device
+// (freed with cudaFreeAsync; the memory stays in the pool until
+// trim_scratch, which nan_ctx_destroy calls).
+cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
+void trim_scratch(int device);
 int cuda_fail(cudaError_t err, const char* what);
 
 void free_scene(NanContext* ctx);
+// Drops the scene's metadata but keeps owned BVH storage for a rebuild.
+void forget_scene(NanContext* ctx);
 // Stage timing: begin returns the start event (or nullptr when timing is
 // off); end records the stop event and queues the pair.
 cudaEvent_t timing_begin(NanContext* ctx, cudaStream_t stream);

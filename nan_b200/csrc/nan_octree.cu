@@ -279,7 +279,7 @@ int launch_build_point_octrees(NanContext* ctx, const float* positions, const ui
     cudaError_t e = cudaSuccess;
     auto get = [&](size_t bytes) -> void* {
         void* p = nullptr;
-        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) e = nan_host::scratch_alloc(&p, std::max<size_t>(bytes, 16), st);
         if (e == cudaSuccess) owned.push_back(p);
         return p;
     };

@@ -33,7 +33,7 @@ SceneView scene_view(const NanContext* ctx) {
     SceneView v;
     v.nodes = ctx->nodes;
     v.tris = ctx->tris;
-    const bool wide = ctx->wnodes != nullptr && ctx->tuning.bvh_width == 8;
+    const bool wide = ctx->wide_built && ctx->wnodes != nullptr && ctx->tuning.bvh_width == 8;
     v.wnodes = wide ? ctx->wnodes : nullptr;
     v.wtris = wide ? ctx->wtris : nullptr;
     v.tri_refs = ctx->tri_refs;

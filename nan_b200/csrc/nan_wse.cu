@@ -311,7 +311,7 @@ __global__ void k_wse_keep(uint32_t n, const uint32_t* idx, const uint32_t* set_
 
 template <class T>
 cudaError_t alloc(T** p, size_t count, cudaStream_t s) {
-    return cudaMallocAsync(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T), s);
+    return nan_host::scratch_alloc(reinterpret_cast<void**>(p), std::max<size_t>(count, 1) * sizeof(T), s);
 }
 
 uint32_t blocks(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
@@ -945,7 +945,7 @@ int launch_wse_eliminate(NanContext* ctx, const float* positions, const float* n
     uint32_t *tmp_u = nullptr;
     cub::DeviceRadixSort::SortPairs(nullptr, need, set_of, set_sorted, idx, tmp_u, (int)n, 0, 32, st);
     tmp_bytes = std::max(tmp_bytes, need);
-    if (!ok(cudaMallocAsync(&tmp, std::max<size_t>(tmp_bytes, 1), st))) {
+    if (!ok(nan_host::scratch_alloc(&tmp, std::max<size_t>(tmp_bytes, 1), st))) {
         release();
         return cuda_fail(e, "wse sort scratch");
     }
@@ -1046,7 +1046,7 @@ int launch_deficit_repair(NanContext* ctx, const float* const* base, const uint3
     cudaError_t e = cudaSuccess;
     auto get = [&](size_t bytes) -> void* {
         void* p = nullptr;
-        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) e = nan_host::scratch_alloc(&p, std::max<size_t>(bytes, 16), st);
         if (e == cudaSuccess) owned.push_back(p);
         return p;
     };
@@ -1227,7 +1227,7 @@ int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* 
     cudaError_t e = cudaSuccess;
     auto get = [&](size_t bytes) -> void* {
         void* p = nullptr;
-        if (e == cudaSuccess) e = cudaMallocAsync(&p, std::max<size_t>(bytes, 16), st);
+        if (e == cudaSuccess) e = nan_host::scratch_alloc(&p, std::max<size_t>(bytes, 16), st);
         if (e == cudaSuccess) owned.push_back(p);
         return p;
     };
