@@ -57,6 +57,17 @@ typedef struct NanLighting {
     uint32_t flags;             /* bit 0: add the sun disk on primary misses; bit 1: screen
                                    tracer NEE toward the context's area lights with MIS
                                    (nan_ctx_set_area_lights; not in the reference) */
+    /* Sky-view LUT (sample_sky_lut, scene.slang:469-518). Null: every miss sees the
+     * constant sky_radiance. Otherwise device memory f32[height][width][4] (RGBA32F, the
+     * reference's 200x200 sky-view LUT): a miss in direction d reads it bilinearly
+     * (wrapped addressing) at u = azimuth / 2pi + 1/2 and the LUT's altitude mapping,
+     * times sun_color * sun_intensity. */
+    const float* sky_view_lut;
+    uint32_t sky_view_width;
+    uint32_t sky_view_height;
+    float sky_view_up[3];        /* unit vector from the planet's centre to the view position */
+    float sky_view_horizon_angle; /* acos(sqrt(h^2 - R^2) / h) - pi/2 at view height h, ground
+                                     radius R (the reference's atmosphere: h = 6.3602, R = 6.36) */
 } NanLighting;
 
 /* Pinhole camera: the fields compute_ray_pinhole reads (camera.slang:173-236,

@@ -45,6 +45,11 @@ class NanLighting(ctypes.Structure):
         ("ray_t_max", ctypes.c_float),
         ("sky_radiance", ctypes.c_float * 3),
         ("flags", ctypes.c_uint32),
+        ("sky_view_lut", ctypes.c_void_p),
+        ("sky_view_width", ctypes.c_uint32),
+        ("sky_view_height", ctypes.c_uint32),
+        ("sky_view_up", ctypes.c_float * 3),
+        ("sky_view_horizon_angle", ctypes.c_float),
     ]
 
 

@@ -342,6 +342,7 @@ NAN_B200_API int nan_trace_screen(NanContext* ctx, float* out_rgba, uint32_t wid
     if (rc) return rc;
     if ((rc = need_scene(ctx))) return rc;
     if (!camera || !lighting) return invalid("null camera or lighting");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if ((width || height) && (!out_rgba || !aligned16(out_rgba))) return invalid("output must be 16-byte aligned");
     if (max_vertices > 64) return invalid("max_vertices above 64");
     if (ctx->tuning.integrator == 0)
@@ -369,6 +370,7 @@ NAN_B200_API int nan_trace_texels(NanContext* ctx, const NanMeshColorsDesc* layo
     if (rc) return rc;
     if ((rc = need_scene(ctx))) return rc;
     if (!layout || !lighting) return invalid("null layout or lighting");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (layout->instance_count == 0) return invalid("layout has no instances");
     if (!layout->face_infos || !layout->instance_infos || !layout->side_infos || !layout->surface_prefix || !slots)
         return invalid("null layout buffer");
@@ -394,6 +396,7 @@ NAN_B200_API int nan_trace_probes(NanContext* ctx, float* values, uint32_t* samp
     if (rc) return rc;
     if ((rc = need_scene(ctx))) return rc;
     if (!lighting) return invalid("null lighting");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (probe_count && (!values || !sample_counts || !self_hits || !radial || !probes || !probe_instances))
         return invalid("null probe buffer");
     if (probe_count && (!aligned16(probes) || !aligned16(probe_instances) ||
@@ -420,6 +423,7 @@ NAN_B200_API int nan_resolve_mesh_colors(NanContext* ctx, const NanMeshColorsDes
     rc = need_scene(ctx);
     if (rc) return rc;
     if (!layout || !colors || !out || !camera || !lighting) return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (!layout->face_infos || !layout->instance_infos || !layout->side_infos) return invalid("null layout buffer");
     if (layout->instance_count < ctx->scene.instance_count)
         return invalid("the layout covers fewer instances than the scene");
@@ -457,6 +461,7 @@ NAN_B200_API int nan_trace_probes_prt(NanContext* ctx, float* values, uint32_t* 
     if (probe_count && (!values || !sample_counts || !self_hits || !radial || !static_source || !probes ||
                         !probe_instances || !lighting))
         return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (!aligned16(probes) || !aligned16(probe_instances)) return invalid("probe records must be 16-byte aligned");
     return nan_host::launch_trace_probes_prt(ctx, values, sample_counts, self_hits, radial, static_source, probes,
                                              probe_count, probe_instances, probe_instance_count, iteration,
@@ -469,6 +474,7 @@ NAN_B200_API int nan_prt_project_lighting(NanContext* ctx, float* lighting_sh, u
     int rc = enter(ctx);
     if (rc) return rc;
     if (!lighting_sh || !lighting) return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (!aligned16(lighting_sh)) return invalid("lighting_sh must be 16-byte aligned");
     return nan_host::launch_prt_project_lighting(ctx, lighting_sh, sample_count, lighting, as_stream(stream));
 }
@@ -496,6 +502,7 @@ NAN_B200_API int nan_resolve_probes(NanContext* ctx, const NanProbeLayoutDesc* l
     rc = need_scene(ctx);
     if (rc) return rc;
     if (!layout || !options || !camera || !lighting) return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if ((uint64_t)width * height == 0) return NAN_OK;
     if (!out || !layout->instances || (layout->probe_count && (!layout->probes || !values || !sample_counts ||
                                                                !self_hits || !radial)) ||
@@ -788,6 +795,7 @@ NAN_B200_API int nan_trace_points(NanContext* ctx, const float* points, uint32_t
     rc = need_scene(ctx);
     if (rc) return rc;
     if (count && (!points || !out || !lighting)) return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (!aligned16(points) || !aligned16(out)) return invalid("points and out must be 16-byte aligned");
     if (flags & ~(uint32_t)NAN_POINTS_INDIRECT_ONLY) return invalid("unknown points flag");
     return nan_host::launch_trace_points_wavefront(ctx, points, count, out, iteration, samples, max_bounces, flags,
@@ -802,6 +810,7 @@ NAN_B200_API int nan_trace_screen_cached(NanContext* ctx, NanCache* cache, float
     rc = need_scene(ctx);
     if (rc) return rc;
     if (!cache || !out || !camera || !lighting || !fd) return invalid("null argument");
+    if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (cache->ctx->device != ctx->device) return invalid("cache and context are on different devices");
     const uint64_t P = (uint64_t)width * height;
     if (P == 0) return NAN_OK;

@@ -261,6 +261,7 @@ int batch_create(NanContext* ctx, const NanProbeSet* in, uint32_t count, NanBatc
     float t_max = 0.0f;
     for (uint32_t i = 0; i < count; ++i) {
         const NanProbeSet& p = in[i];
+        if (const int lrc = check_lighting(&p.lighting)) return lrc;
         BatchSet& b = sets[i];
         b.s = scene_view_for_batch(p.scene);
         memcpy(&b.light, &p.lighting, sizeof(b.light));

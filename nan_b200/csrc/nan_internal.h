@@ -99,6 +99,24 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
 void trim_scratch(int device);
 int cuda_fail(cudaError_t err, const char* what);
 
+// A lighting record the kernels can read: a sky-view LUT needs a size and a
+// 16-byte aligned address. Returns NAN_OK or sets the error and returns
+// NAN_ERR_INVALID_ARGUMENT.
+inline int check_lighting(const NanLighting* l) {
+    if (l && l->sky_view_lut) {
+        if (l->sky_view_width == 0u || l->sky_view_height == 0u || l->sky_view_width > 16384u ||
+            l->sky_view_height > 16384u) {
+            set_error("sky_view_lut needs a width and height in 1..16384");
+            return NAN_ERR_INVALID_ARGUMENT;
+        }
+        if (reinterpret_cast<uintptr_t>(l->sky_view_lut) & 15u) {
+            set_error("sky_view_lut must be 16-byte aligned");
+            return NAN_ERR_INVALID_ARGUMENT;
+        }
+    }
+    return NAN_OK;
+}
+
 void free_scene(NanContext* ctx);
 // Drops the scene's metadata but keeps owned BVH storage for a rebuild.
 void forget_scene(NanContext* ctx);

@@ -176,4 +176,37 @@ __device__ __forceinline__ f3 adjust_shading_normal(f3 sn, f3 gn, f3 d) {
     return sn;
 }
 
+// atan2 and asin of float arguments, from the mathematics: for
+// t = min(|x|, |y|) / max(|x|, |y|) in [0, 1], two half-angle steps
+// t -> t / (1 + sqrt(1 + t^2)) (atan t = 2 atan of the result) bring t below
+// tan(pi/16) ~ 0.2, where the odd Taylor series of atan to t^15 (truncation
+// below 1e-12) is summed by Horner's rule with fused steps; the octant and
+// quadrant come from the signs. The oracle runs the same operations (C fmaf
+// is correctly rounded too), so GPU and oracle agree bit for bit.
+// asin x = atan2(x, sqrt(1 - x^2)).
+__device__ __forceinline__ float nan_atan01(float t) {
+    t = t / (1.0f + sqrtf(1.0f + t * t));
+    t = t / (1.0f + sqrtf(1.0f + t * t));
+    const float s = t * t;
+    float p = -6.66666666666666667e-2f;
+    p = __fmaf_rn(p, s, 7.69230769230769231e-2f);
+    p = __fmaf_rn(p, s, -9.09090909090909091e-2f);
+    p = __fmaf_rn(p, s, 1.11111111111111111e-1f);
+    p = __fmaf_rn(p, s, -1.42857142857142857e-1f);
+    p = __fmaf_rn(p, s, 2.0e-1f);
+    p = __fmaf_rn(p, s, -3.33333333333333333e-1f);
+    return 4.0f * __fmaf_rn(t * s, p, t);
+}
+
+__device__ __forceinline__ float nan_atan2(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    float a = mx > 0.0f ? nan_atan01(mn / mx) : 0.0f;
+    if (ay > ax) a = 1.57079632679489662f - a;
+    if (x < 0.0f) a = 3.14159265358979324f - a;
+    return y < 0.0f ? -a : a;
+}
+
+__device__ __forceinline__ float nan_asin(float x) { return nan_atan2(x, sqrtf(fmaxf(0.0f, 1.0f - x * x))); }
+
 }  // namespace nbd

@@ -100,7 +100,7 @@ __device__ __forceinline__ ProbeSample probe_sample(const SceneView& s, const Li
             const HitInfo hit = Tr::closest(s, o, d, 0.0f, L.t_max);
             if (!hit.valid) {
                 if (bounce == 0u) first_hit = radial_max;
-                rad = rad + thp * L.sky;
+                rad = rad + thp * sky_radiance(L, d);
                 break;
             }
             if (bounce == 0u) first_hit = minf(hit.t, radial_max);

@@ -826,7 +826,10 @@ __device__ __forceinline__ f3 world_flat_normal(const SceneView& s, uint32_t ins
 }
 
 // ---------------------------------------------------------------------------
-// Lights (scene.slang:408-527, 940-1009) with the LUTs reduced to constants.
+// Lights (scene.slang:408-527, 940-1009). The sun transmittance is one value
+// per frame (get_sun_transmittance_at_view reads the LUT at the fixed view
+// position), so it arrives as a constant; the sky is a constant radiance or
+// the sky-view LUT looked up per direction (sample_sky_lut).
 // ---------------------------------------------------------------------------
 struct LightParams {
     f3 sun_dir;
@@ -838,6 +841,11 @@ struct LightParams {
     float t_max;
     bool sun_disk;
     bool area_nee;  // screen tracer: NEE toward the emissive triangles, MIS with the BSDF
+    // sky-view LUT (null: the constant sky): RGBA32F [height][width]
+    const float4* sky_lut;
+    uint32_t sky_w, sky_h;
+    f3 sky_up;          // unit vector from the planet's centre to the view position
+    float sky_horizon;  // horizon angle at the view height (scene.slang:474)
 };
 
 struct LightingRaw {  // layout of NanLighting
@@ -849,6 +857,11 @@ struct LightingRaw {  // layout of NanLighting
     float ray_t_max;
     float sky_radiance[3];
     uint32_t flags;
+    const float* sky_view_lut;
+    uint32_t sky_view_width;
+    uint32_t sky_view_height;
+    float sky_view_up[3];
+    float sky_view_horizon_angle;
 };
 
 __device__ __forceinline__ LightParams make_light(const LightingRaw& p) {
@@ -862,7 +875,53 @@ __device__ __forceinline__ LightParams make_light(const LightingRaw& p) {
     L.t_max = p.ray_t_max;
     L.sun_disk = (p.flags & 1u) != 0u;
     L.area_nee = (p.flags & 2u) != 0u;
+    L.sky_lut = reinterpret_cast<const float4*>(p.sky_view_lut);
+    L.sky_w = p.sky_view_width;
+    L.sky_h = p.sky_view_height;
+    L.sky_up = mk3(p.sky_view_up[0], p.sky_view_up[1], p.sky_view_up[2]);
+    L.sky_horizon = p.sky_view_horizon_angle;
     return L;
+}
+
+// sample_sky_lut (scene.slang:469-518): altitude asin(d . up) clamped 0.01
+// short of the poles, azimuth atan2 against the frame (right = sun x up,
+// forward = up x right), the LUT's non-linear altitude mapping inverted,
+// v = (1 -+ sqrt|adjV|) / 2, u = azimuth / 2pi + 1/2; a bilinear fetch with
+// wrapped addressing (the default sampler), times the sun's outer-space
+// illuminance. A direction with no azimuth (straight along up) takes u = 1/2.
+__device__ __forceinline__ float4 sky_texel(const LightParams& L, int x, int y) {
+    x %= (int)L.sky_w;
+    y %= (int)L.sky_h;
+    if (x < 0) x += (int)L.sky_w;
+    if (y < 0) y += (int)L.sky_h;
+    return __ldg(L.sky_lut + (size_t)y * L.sky_w + (size_t)x);
+}
+
+__device__ __forceinline__ f3 sky_radiance(const LightParams& L, f3 d) {
+    if (!L.sky_lut) return L.sky;
+    const float kHalfPiF = 1.57079632679489662f;
+    const float altitude = fminf(fmaxf(nan_asin(dot3(d, L.sky_up)), -kHalfPiF + 1e-2f), kHalfPiF - 1e-2f);
+    float azimuth = 0.0f;
+    if (!(fabsf(altitude) > kHalfPiF - 1e-4f)) {
+        const f3 right = cross3(L.sun_dir, L.sky_up);
+        const f3 forward = cross3(L.sky_up, right);
+        const f3 proj = normalize3(d - L.sky_up * dot3(d, L.sky_up));
+        azimuth = nan_atan2(dot3(proj, right), dot3(proj, forward));
+    }
+    const float adj = (altitude + L.sky_horizon) / kHalfPiF;
+    const float v = adj < 0.0f ? 0.5f * (1.0f - sqrtf(fminf(fmaxf(-adj, 0.0f), 1.0f)))
+                               : 0.5f * (1.0f + sqrtf(fminf(fmaxf(adj, 0.0f), 1.0f)));
+    float u = azimuth / (2.0f * 3.14159265358979324f) + 0.5f;
+    if (!(u >= 0.0f && u <= 1.0f)) u = 0.5f;
+    const float fx = u * (float)L.sky_w - 0.5f, fy = v * (float)L.sky_h - 0.5f;
+    const float x0 = floorf(fx), y0 = floorf(fy);
+    const float tx = fx - x0, ty = fy - y0;
+    const float4 a = sky_texel(L, (int)x0, (int)y0), b = sky_texel(L, (int)x0 + 1, (int)y0);
+    const float4 c = sky_texel(L, (int)x0, (int)y0 + 1), e = sky_texel(L, (int)x0 + 1, (int)y0 + 1);
+    const f3 top = mk3(a.x + tx * (b.x - a.x), a.y + tx * (b.y - a.y), a.z + tx * (b.z - a.z));
+    const f3 bot = mk3(c.x + tx * (e.x - c.x), c.y + tx * (e.y - c.y), c.z + tx * (e.z - c.z));
+    const f3 rgb = mk3(top.x + ty * (bot.x - top.x), top.y + ty * (bot.y - top.y), top.z + ty * (bot.z - top.z));
+    return rgb * L.outer;
 }
 
 // Area-light next-event estimation (no counterpart in the reference, whose

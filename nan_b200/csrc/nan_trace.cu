@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(128) k_trace_screen(SceneView s, LightingRaw l
     for (uint32_t vi = 0; vi < max_vertices; ++vi) {
         const HitInfo hit = closest(s, o, dir, tmin, tmax, tally);
         if (!hit.valid) {
-            f3 sky = L.sky;
+            f3 sky = sky_radiance(L, dir);
             if (vi == 0u && L.sun_disk) sky = sky + sun_disk(L, dir);
             Lr = Lr + thp * sky;
             break;
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(128) k_resolve_mesh_colors(SceneView s, Lighti
     const HitInfo hit = trace_closest(s, o, dir, cam.near_clip * inv_cos, cam.far_clip * inv_cos);
     const size_t pix = (size_t)py * w + px;
     if (!hit.valid) {
-        f3 sky = L.sky;
+        f3 sky = sky_radiance(L, dir);
         if (L.sun_disk) sky = sky + sun_disk(L, dir);
         out[pix] = make_float4(sky.x, sky.y, sky.z, 1.0f);
         return;
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(128) k_resolve_probes(SceneView s, LightingRaw
     if (!hit.valid) {
         f3 c = mk3(0.02f, 0.02f, 0.02f);
         if (beauty) {
-            c = L.sky;
+            c = sky_radiance(L, dir);
             if (L.sun_disk) c = c + sun_disk(L, dir);
         }
         out[pix] = make_float4(c.x, c.y, c.z, 1.0f);
@@ -656,7 +656,7 @@ __device__ __forceinline__ f3 ts_trace_radiance(const SceneView& s, const LightP
     f3 thp = mk3(1.0f, 1.0f, 1.0f), rad = mk3(0.0f, 0.0f, 0.0f);
     for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
         const HitInfo hit = closest(s, o, d, 0.0f, L.t_max, tally);
-        if (!hit.valid) return rad + thp * L.sky;
+        if (!hit.valid) return rad + thp * sky_radiance(L, d);
         const uint2 ref = __ldg(s.tri_refs + hit.flat);
         const Shading sd = shading_data(s, ref.x, ref.y, hit.b1, hit.b2, -d);
         rad = rad + thp * sd.emissive;
@@ -791,7 +791,7 @@ __global__ void __launch_bounds__(256) k_prt_project_lighting(LightingRaw lraw, 
             nan_sincos(kTwoPi * v, &sn, &cs);
             const f3 d = mk3(r * cs, y, r * sn);
             for (uint32_t c = 0; c < 9u; ++c) {
-                const f3 t = L.sky * sh_l2_basis(c, d);
+                const f3 t = sky_radiance(L, d) * sh_l2_basis(c, d);
                 terms[3 * c][tid] = t.x;
                 terms[3 * c + 1][tid] = t.y;
                 terms[3 * c + 2][tid] = t.z;

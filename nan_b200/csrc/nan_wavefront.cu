@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(128) k_wf_texel_shade(SceneView s, LightingRaw
         f3 thp = xyz(st.thp[p]), rad = xyz(st.rad[p]);
         const uint32_t flat = __float_as_uint(h.x);
         if (flat == 0xffffffffu) {
-            rad = rad + thp * L.sky;
+            rad = rad + thp * sky_radiance(L, d);
             st.rad[p] = f4(rad, 0.0f);
             st.flags[p] = flags | kFlagEnd;
             continue;
@@ -664,7 +664,7 @@ __global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRa
         const uint32_t vertex = (flags & kBounceMask) >> kBounceShift;
         const uint32_t flat = __float_as_uint(h.x);
         if (flat == 0xffffffffu) {
-            f3 sky = L.sky;
+            f3 sky = sky_radiance(L, d);
             if (vertex == 0u && L.sun_disk) sky = sky + sun_disk(L, d);
             rad = rad + thp * sky;
             st.rad[p] = f4(rad, 0.0f);
@@ -858,7 +858,7 @@ __device__ __forceinline__ void probe_shade_path(const SceneView& s, const Light
     const uint32_t flat = __float_as_uint(h.x);
     if (flat == 0xffffffffu) {
         if (bounce == 0u) pa.w = radial_max;
-        rad = rad + thp * L.sky;
+        rad = rad + thp * sky_radiance(L, d);
         st.pa[p] = pa;
         st.rad[p] = f4(rad, 0.0f);
         st.flags[p] = flags | kFlagEnd;

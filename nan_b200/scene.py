@@ -56,13 +56,59 @@ class Device:
         return self.context.launch_count + sum(c.launch_count for c in list(self._contexts))
 
 
+# The reference atmosphere (atmosphere.slang:4-8): radii in megametres, the
+# view 200 m above the ground.
+GROUND_RADIUS_MM = 6.360
+ATMOSPHERE_RADIUS_MM = 6.460
+VIEW_HEIGHT_MM = GROUND_RADIUS_MM + 0.0002
+
+
+def sky_view_horizon_angle(view_height: float = VIEW_HEIGHT_MM, ground_radius: float = GROUND_RADIUS_MM) -> float:
+    """acos(sqrt(h^2 - R^2) / h) - pi/2 in float32 (scene.slang:474)."""
+    f = np.float32
+    h, r = f(view_height), f(ground_radius)
+    c = np.sqrt(h * h - r * r) / h
+    return float(f(np.arccos(np.clip(c, f(-1), f(1)))) - f(0.5) * f(math.pi))
+
+
+def sun_transmittance_from_lut(lut, sun_direction, up=(0.0, 1.0, 0.0), view_height: float = VIEW_HEIGHT_MM,
+                               ground_radius: float = GROUND_RADIUS_MM,
+                               atmosphere_radius: float = ATMOSPHERE_RADIUS_MM) -> tuple:
+    """get_sun_transmittance_at_view (scene.slang:997-1009): the
+    transmittance LUT (float32 [H, W, >=3], e.g. 64 x 256) read bilinearly
+    with clamp-to-edge at u = 0.5 + 0.5 cos(sun zenith), v = the view
+    height's fraction of the atmosphere. Returns the rgb factor for
+    Lighting.sun_transmittance."""
+    t = np.asarray(lut.cpu() if hasattr(lut, "cpu") else lut, dtype=np.float32)
+    d = np.asarray(sun_direction, np.float64)
+    mu = float(np.dot(d / np.linalg.norm(d), np.asarray(up, np.float64)))
+    u = min(max(0.5 + 0.5 * mu, 0.0), 1.0)
+    v = min(max((view_height - ground_radius) / (atmosphere_radius - ground_radius), 0.0), 1.0)
+    h, w = t.shape[0], t.shape[1]
+    x, y = u * w - 0.5, v * h - 0.5
+    x0, y0 = math.floor(x), math.floor(y)
+    fx, fy = x - x0, y - y0
+
+    def at(i, j):
+        return t[min(max(j, 0), h - 1), min(max(i, 0), w - 1), :3].astype(np.float64)
+
+    top = at(x0, y0) * (1 - fx) + at(x0 + 1, y0) * fx
+    bottom = at(x0, y0 + 1) * (1 - fx) + at(x0 + 1, y0 + 1) * fx
+    return tuple(float(c) for c in top * (1 - fy) + bottom * fy)
+
+
 @dataclass
 class Lighting:
-    """Directional sun + constant sky.
+    """Directional sun and sky.
 
     Defaults follow Scene.__init__ (scene.py:135-147): sun toward
     (0, 0.5, 0.866), color white, intensity pi, half apex angle 0.26785 deg.
-    The sky-view and transmittance LUTs are replaced by constants.
+    The sky is the constant `sky_radiance`, or, with `sky_view_lut` set (a
+    float32 [H, W, 4] CUDA tensor, the reference's sky-view LUT), the LUT
+    looked up per miss direction as sample_sky_lut does (scene.slang:469-518).
+    The sun transmittance is one value per frame in the reference
+    (get_sun_transmittance_at_view reads its LUT at the fixed view position,
+    scene.slang:997-1009): `sun_transmittance_from_lut` computes it.
     """
 
     sun_direction: tuple = (0.0, 0.5, 0.866)
@@ -76,6 +122,9 @@ class Lighting:
     # screen tracer only, not in the reference: NEE toward the scene's emissive
     # triangles with MIS (Scene.enable_area_lights builds the table)
     area_nee: bool = False
+    sky_view_lut: object = None
+    sky_view_up: tuple = (0.0, 1.0, 0.0)
+    sky_view_horizon_angle: float | None = None  # None: the reference atmosphere's view height
 
     def __post_init__(self):
         d = np.asarray(self.sun_direction, dtype=np.float64)
@@ -96,6 +145,18 @@ class Lighting:
         s.ray_t_max = float(self.ray_t_max)
         s.sky_radiance[:] = [float(x) for x in self.sky_radiance]
         s.flags = self.flags
+        lut = self.sky_view_lut
+        if lut is not None:
+            import torch
+
+            if not (isinstance(lut, torch.Tensor) and lut.is_cuda and lut.dtype == torch.float32 and lut.dim() == 3
+                    and lut.shape[2] == 4 and lut.is_contiguous()):
+                raise ValueError("sky_view_lut must be a contiguous float32 [H, W, 4] CUDA tensor")
+            s.sky_view_lut = int(lut.data_ptr())
+            s.sky_view_height, s.sky_view_width = int(lut.shape[0]), int(lut.shape[1])
+        s.sky_view_up[:] = [float(x) for x in self.sky_view_up]
+        s.sky_view_horizon_angle = (sky_view_horizon_angle() if self.sky_view_horizon_angle is None
+                                    else float(self.sky_view_horizon_angle))
         return s
 
     @classmethod

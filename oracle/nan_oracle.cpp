@@ -137,15 +137,48 @@ float spec_log2(float x) {
     return (float)e + ln_m * 1.44269504088896341f;
 }
 
+// atan2 / asin of floats: two half-angle steps t -> t / (1 + sqrt(1 + t^2))
+// on t = min / max in [0, 1], the odd Taylor series of atan to t^15 by
+// Horner's rule with fused steps, octant and quadrant from the signs; asin x
+// = atan2(x, sqrt(1 - x^2)). The same operations as the kernels (nan_math.cuh).
+float own_atan01(float t) {
+    t = t / (1.0f + std::sqrt(1.0f + t * t));
+    t = t / (1.0f + std::sqrt(1.0f + t * t));
+    const float s = t * t;
+    float p = -6.66666666666666667e-2f;
+    p = std::fmaf(p, s, 7.69230769230769231e-2f);
+    p = std::fmaf(p, s, -9.09090909090909091e-2f);
+    p = std::fmaf(p, s, 1.11111111111111111e-1f);
+    p = std::fmaf(p, s, -1.42857142857142857e-1f);
+    p = std::fmaf(p, s, 2.0e-1f);
+    p = std::fmaf(p, s, -3.33333333333333333e-1f);
+    return 4.0f * std::fmaf(t * s, p, t);
+}
+
+float own_atan2(float y, float x) {
+    const float ax = std::fabs(x), ay = std::fabs(y);
+    const float mx = std::fmax(ax, ay), mn = std::fmin(ax, ay);
+    float a = mx > 0.0f ? own_atan01(mn / mx) : 0.0f;
+    if (ay > ax) a = 1.57079632679489662f - a;
+    if (x < 0.0f) a = 3.14159265358979324f - a;
+    return y < 0.0f ? -a : a;
+}
+
+float own_asin(float x) { return own_atan2(x, std::sqrt(std::fmax(0.0f, 1.0f - x * x))); }
+
 template <class T> struct Ops;
 template <> struct Ops<float> {
     static float fma(float a, float b, float c) { return std::fmaf(a, b, c); }
     static float sqrt(float a) { return std::sqrt(a); }
     static void sincos(float a, float* s, float* c) { own_sincos(a, s, c); }
+    static float atan2(float y, float x) { return own_atan2(y, x); }
+    static float asin(float x) { return own_asin(x); }
 };
 template <> struct Ops<double> {
     static double fma(double a, double b, double c) { return std::fma(a, b, c); }
     static double sqrt(double a) { return std::sqrt(a); }
+    static double atan2(double y, double x) { return std::atan2(y, x); }
+    static double asin(double x) { return std::asin(std::fmax(-1.0, std::fmin(1.0, x))); }
     static void sincos(double a, double* s, double* c) {
         *s = std::sin(a);
         *c = std::cos(a);
@@ -926,13 +959,18 @@ template <class T> V3<T> world_flat_normal(const Scene& s, uint32_t inst, uint32
 }
 
 // ---------------------------------------------------------------------------
-// Lights: scene.slang:940-990 (sun NEE), constant sky stand-in for the LUT
-// (scene.slang:469-518), sun disk (scene.slang:408-465).
+// Lights: scene.slang:940-990 (sun NEE), the sky as a constant or the
+// sky-view LUT (sample_sky_lut, scene.slang:469-518), sun disk
+// (scene.slang:408-465).
 // ---------------------------------------------------------------------------
 template <class T> struct LightCtx {
     V3<T> sun_dir, outer, trans, illum, sky;
     T cos_half, t_max;
     bool sun_disk, area_nee;
+    const float* lut;
+    int lut_w, lut_h;
+    V3<T> up;
+    T horizon;
     explicit LightCtx(const OracleLighting& p) {
         sun_dir = mk<T>(T(p.sun_direction[0]), T(p.sun_direction[1]), T(p.sun_direction[2]));
         V3<T> color = mk<T>(T(p.sun_color[0]), T(p.sun_color[1]), T(p.sun_color[2]));
@@ -944,6 +982,49 @@ template <class T> struct LightCtx {
         t_max = T(p.ray_t_max);
         sun_disk = (p.flags & 1u) != 0;
         area_nee = (p.flags & 2u) != 0;
+        lut = p.sky_view_lut;
+        lut_w = (int)p.sky_view_width;
+        lut_h = (int)p.sky_view_height;
+        up = mk<T>(T(p.sky_view_up[0]), T(p.sky_view_up[1]), T(p.sky_view_up[2]));
+        horizon = T(p.sky_view_horizon_angle);
+    }
+
+    V3<T> texel(int x, int y) const {
+        x %= lut_w;
+        y %= lut_h;
+        if (x < 0) x += lut_w;
+        if (y < 0) y += lut_h;
+        const float* e = lut + 4 * ((size_t)y * lut_w + x);
+        return mk<T>(T(e[0]), T(e[1]), T(e[2]));
+    }
+
+    // sample_sky_lut, scene.slang:469-518 (a direction with no azimuth takes
+    // u = 1/2; the bilinear fetch wraps, as the default sampler does).
+    V3<T> sky_at(V3<T> d) const {
+        if (!lut) return sky;
+        const T half_pi = T(1.57079632679489662), two_pi = T(2) * T(3.14159265358979324);
+        const T altitude = std::fmin(std::fmax(Ops<T>::asin(dot(d, up)), -half_pi + T(1e-2)), half_pi - T(1e-2));
+        T azimuth = T(0);
+        if (!(std::fabs(altitude) > half_pi - T(1e-4))) {
+            const V3<T> right = cross(sun_dir, up);
+            const V3<T> forward = cross(up, right);
+            const V3<T> proj = normalize(d - up * dot(d, up));
+            azimuth = Ops<T>::atan2(dot(proj, right), dot(proj, forward));
+        }
+        const T adj = (altitude + horizon) / half_pi;
+        const T v = adj < T(0) ? T(0.5) * (T(1) - Ops<T>::sqrt(std::fmin(std::fmax(-adj, T(0)), T(1))))
+                               : T(0.5) * (T(1) + Ops<T>::sqrt(std::fmin(std::fmax(adj, T(0)), T(1))));
+        T u = azimuth / two_pi + T(0.5);
+        if (!(u >= T(0) && u <= T(1))) u = T(0.5);
+        const T fx = u * T(lut_w) - T(0.5), fy = v * T(lut_h) - T(0.5);
+        const T x0 = std::floor(fx), y0 = std::floor(fy);
+        const T tx = fx - x0, ty = fy - y0;
+        const V3<T> a = texel((int)x0, (int)y0), b = texel((int)x0 + 1, (int)y0);
+        const V3<T> c = texel((int)x0, (int)y0 + 1), e = texel((int)x0 + 1, (int)y0 + 1);
+        const V3<T> top = mk<T>(a.x + tx * (b.x - a.x), a.y + tx * (b.y - a.y), a.z + tx * (b.z - a.z));
+        const V3<T> bot = mk<T>(c.x + tx * (e.x - c.x), c.y + tx * (e.y - c.y), c.z + tx * (e.z - c.z));
+        const V3<T> rgb = mk<T>(top.x + ty * (bot.x - top.x), top.y + ty * (bot.y - top.y), top.z + ty * (bot.z - top.z));
+        return rgb * outer;
     }
 };
 
@@ -1077,7 +1158,7 @@ void screen_pixel(Tracer<T>& tr, const OracleLighting& lp, const OracleCamera& c
     for (uint32_t vi = 0; vi < max_vertices; ++vi) {
         HitRec hit = tr.closest(o, dir, tmin, tmax);
         if (!hit.valid) {
-            V3<T> sky = tr.L.sky;
+            V3<T> sky = tr.L.sky_at(dir);
             if (vi == 0 && tr.L.sun_disk) sky = sky + tr.sun_disk(dir);
             Lr = Lr + thp * sky;
             break;
@@ -1126,7 +1207,7 @@ V3<T> ts_trace_radiance(Tracer<T>& tr, V3<T> o, V3<T> d, Rng& rng, uint32_t max_
     for (uint32_t bounce = 0; bounce < max_bounces; ++bounce) {
         HitRec hit = tr.closest(o, d, T(0), tr.L.t_max);
         if (!hit.valid) {
-            rad = rad + thp * tr.L.sky;
+            rad = rad + thp * tr.L.sky_at(d);
             return rad;
         }
         uint32_t inst = tr.s.flat_instance[hit.flat], prim = tr.s.flat_prim[hit.flat];
@@ -1199,7 +1280,7 @@ template <class T> void probe_trace_radiance(Tracer<T>& tr, ProbePath<T>& p, Rng
         HitRec hit = tr.closest(p.o, p.d, T(0), tr.L.t_max);
         if (!hit.valid) {
             if (bounce == 0u) p.first_hit = p.radial_max;
-            p.rad = p.rad + p.thp * tr.L.sky;
+            p.rad = p.rad + p.thp * tr.L.sky_at(p.d);
             return;
         }
         T ht = T(hit.t);
@@ -1358,7 +1439,7 @@ void resolve_pixel(Tracer<T>& tr, const OracleCamera& cam, uint32_t w, uint32_t 
     HitRec hit = tr.closest(o, dir, T(cam.near_clip) * inv_cos, T(cam.far_clip) * inv_cos);
     out[3] = 1.0f;
     if (!hit.valid) {
-        V3<T> sky = tr.L.sky;
+        V3<T> sky = tr.L.sky_at(dir);
         if (tr.L.sun_disk) sky = sky + tr.sun_disk(dir);
         out[0] = (float)sky.x; out[1] = (float)sky.y; out[2] = (float)sky.z;
         return;
@@ -1702,6 +1783,33 @@ void oracle_rng_sequence(uint32_t x, uint32_t y, uint32_t sample_index, int coun
 
 void oracle_sincos(const float* a, int count, float* s, float* c) {
     for (int i = 0; i < count; ++i) own_sincos(a[i], &s[i], &c[i]);
+}
+
+void oracle_atan2_asin(const float* y, const float* x, int count, float* out_atan2, float* out_asin) {
+    for (int i = 0; i < count; ++i) {
+        out_atan2[i] = own_atan2(y[i], x[i]);
+        out_asin[i] = own_asin(y[i]);
+    }
+}
+
+void oracle_sky_radiance(const OracleLighting* lighting, const float* dirs, int count, int precision, float* out) {
+    if (precision == ORACLE_F64) {
+        LightCtx<double> L(*lighting);
+        for (int i = 0; i < count; ++i) {
+            const V3<double> v = L.sky_at(mk<double>(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+            out[3 * i] = (float)v.x;
+            out[3 * i + 1] = (float)v.y;
+            out[3 * i + 2] = (float)v.z;
+        }
+        return;
+    }
+    LightCtx<float> L(*lighting);
+    for (int i = 0; i < count; ++i) {
+        const V3<float> v = L.sky_at(mk<float>(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+        out[3 * i] = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    }
 }
 
 void oracle_pack_rgb9e5(const float* rgb, int count, uint32_t* out) {
@@ -2372,7 +2480,7 @@ void resolve_probe_pixel(Tracer<float>& tr, const OracleCamera& cam, uint32_t w,
     if (!hit.valid) {
         F3 c = mk<float>(0.02f, 0.02f, 0.02f);
         if (beauty) {
-            c = tr.L.sky;
+            c = tr.L.sky_at(dir);
             if (tr.L.sun_disk) c = c + tr.sun_disk(dir);
         }
         put(c);
@@ -2944,7 +3052,8 @@ void oracle_prt_project_lighting(const OracleLighting* lighting, uint32_t sample
             const float r = std::sqrt(std::fmax(1.0f - y * y, 0.0f));
             float sn, cs;
             own_sincos(6.28318530717958647692f * v, &sn, &cs);
-            acc = acc + L.sky * sh_l2_basis<float>(c, mk<float>(r * cs, y, r * sn));
+            const V3<float> dd = mk<float>(r * cs, y, r * sn);
+            acc = acc + L.sky_at(dd) * sh_l2_basis<float>(c, dd);
         }
         acc = acc * ((4.0f * 3.14159265358979323846f) / (float)n);
         sh[4 * c] = acc.x;

@@ -44,6 +44,11 @@ typedef struct OracleLighting {
     float ray_t_max;
     float sky_radiance[3];
     uint32_t flags; /* bit 0: sun disk on primary misses */
+    const float* sky_view_lut; /* host f32[height][width][4], or null: constant sky */
+    uint32_t sky_view_width;
+    uint32_t sky_view_height;
+    float sky_view_up[3];
+    float sky_view_horizon_angle;
 } OracleLighting;
 
 typedef struct OracleCamera {
@@ -72,6 +77,11 @@ void oracle_rng_sequence(uint32_t x, uint32_t y, uint32_t sample_index,
 void oracle_sincos(const float* angles, int count, float* out_sin,
                    float* out_cos);
 void oracle_pack_rgb9e5(const float* rgb, int count, uint32_t* out);
+/* The own atan2 and asin (float) of the kernels, elementwise: atan2(y, x), asin(y). */
+void oracle_atan2_asin(const float* y, const float* x, int count, float* out_atan2, float* out_asin);
+/* sample_sky_lut (scene.slang:469-518) for unit directions f32[N][3] -> f32[N][3];
+ * precision ORACLE_F32 (the kernels' operations) or ORACLE_F64. */
+void oracle_sky_radiance(const OracleLighting* lighting, const float* dirs, int count, int precision, float* out);
 void oracle_unpack_rgb9e5(const uint32_t* packed, int count, float* out_rgb);
 void oracle_f32_to_f16(const float* values, int count, uint16_t* out);
 void oracle_hemi_oct_encode(const float* dirs, int count, float* out_uv);

@@ -32,6 +32,11 @@ class OracleLighting(ctypes.Structure):
         ("ray_t_max", ctypes.c_float),
         ("sky_radiance", ctypes.c_float * 3),
         ("flags", ctypes.c_uint32),
+        ("sky_view_lut", ctypes.c_void_p),
+        ("sky_view_width", ctypes.c_uint32),
+        ("sky_view_height", ctypes.c_uint32),
+        ("sky_view_up", ctypes.c_float * 3),
+        ("sky_view_horizon_angle", ctypes.c_float),
     ]
 
 
@@ -107,6 +112,8 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_last_error.restype = ctypes.c_char_p
     l.oracle_rng_sequence.argtypes = [u32, u32, u32, i, vp]
     l.oracle_sincos.argtypes = [vp, i, vp, vp]
+    l.oracle_atan2_asin.argtypes = [vp, vp, i, vp, vp]
+    l.oracle_sky_radiance.argtypes = [ctypes.POINTER(OracleLighting), vp, i, i, vp]
     l.oracle_pack_rgb9e5.argtypes = [vp, i, vp]
     l.oracle_unpack_rgb9e5.argtypes = [vp, i, vp]
     l.oracle_f32_to_f16.argtypes = [vp, i, vp]
@@ -308,6 +315,25 @@ def rng_sequence(x: int, y: int, sample_index: int, count: int) -> np.ndarray:
     return out
 
 
+def atan2_asin(y: np.ndarray, x: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The kernels' own atan2(y, x) and asin(y), float32."""
+    yy = np.ascontiguousarray(y, dtype=np.float32)
+    xx = np.ascontiguousarray(x, dtype=np.float32)
+    a = np.zeros_like(yy)
+    s = np.zeros_like(yy)
+    lib().oracle_atan2_asin(_p(yy), _p(xx), yy.size, _p(a), _p(s))
+    return a, s
+
+
+def sky_radiance(lighting, dirs: np.ndarray, precision: int = F32) -> np.ndarray:
+    """sample_sky_lut of `lighting` (a NanLighting-like object) for unit directions f32[N, 3]."""
+    d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+    out = np.zeros_like(d)
+    s = lighting_struct(lighting)
+    lib().oracle_sky_radiance(ctypes.byref(s), _p(d), d.shape[0], precision, _p(out))
+    return out
+
+
 def sincos(angles: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     a = np.ascontiguousarray(angles, dtype=np.float32)
     s = np.zeros_like(a)
@@ -379,6 +405,19 @@ def lighting_struct(lighting) -> OracleLighting:
     s.ray_t_max = float(lighting.ray_t_max)
     s.sky_radiance[:] = [float(x) for x in lighting.sky_radiance]
     s.flags = int(lighting.flags)
+    lut = getattr(lighting, "sky_view_lut", None)
+    if lut is not None:
+        host = np.ascontiguousarray((lut.cpu().numpy() if hasattr(lut, "cpu") else lut), dtype=np.float32)
+        s._sky_view_host = host  # keeps the host copy alive with the struct
+        s.sky_view_lut = host.ctypes.data
+        s.sky_view_height, s.sky_view_width = int(host.shape[0]), int(host.shape[1])
+    s.sky_view_up[:] = [float(x) for x in getattr(lighting, "sky_view_up", (0.0, 1.0, 0.0))]
+    horizon = getattr(lighting, "sky_view_horizon_angle", None)
+    if horizon is None:
+        # the reference atmosphere's view height (scene.slang:474), in float32
+        h, r = np.float32(6.3602), np.float32(6.36)
+        horizon = float(np.float32(np.arccos(np.sqrt(h * h - r * r) / h)) - np.float32(0.5) * np.float32(np.pi))
+    s.sky_view_horizon_angle = float(horizon)
     return s
 
 
