@@ -47,14 +47,14 @@ def test_binding_loads_and_reports_version():
 def test_struct_layouts_match_header():
     from nan_b200 import _native
 
-    assert ctypes.sizeof(_native.NanLighting) == 64
+    assert ctypes.sizeof(_native.NanLighting) == 96
     assert ctypes.sizeof(_native.NanCamera) == 64
     assert ctypes.sizeof(_native.NanCounters) == 32
     assert ctypes.sizeof(_native.NanTuning) == 32
     assert ctypes.sizeof(_native.NanKernelTimes) == 48
     assert ctypes.sizeof(_native.NanCacheConfig) == 72
     assert ctypes.sizeof(_native.NanCachedFrame) == 64
-    assert ctypes.sizeof(_native.NanProbeSet) == 144
+    assert ctypes.sizeof(_native.NanProbeSet) == 176
     assert ctypes.sizeof(_native.NanBatchTuning) == 16
 
 
