@@ -215,6 +215,16 @@ def _face_normals(t):
     return (cr / np.maximum(np.linalg.norm(cr, axis=1, keepdims=True), 1e-30)).astype(np.float32)
 
 
+def _group_centroids(t):
+    """Every triangle's centroid and face normal for the g instances of one
+    mesh at once (t f32[g, T, 3, 3]): per element the operations of
+    _centroids(t[j], T, None), so the values are the same."""
+    cen = t.mean(axis=2, dtype=np.float32)
+    cr = np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0]).astype(np.float64)
+    nrm = (cr / np.maximum(np.linalg.norm(cr, axis=2, keepdims=True), 1e-30)).astype(np.float32)
+    return cen, nrm
+
+
 def _limit(n, k, rng):
     return np.arange(n) if n <= k else np.sort(rng.choice(n, size=k, replace=False))
 
@@ -589,9 +599,17 @@ class SurfaceProbeSiteLayout:
             n_refs = [max(1, min(int(counts[i]) * min(max(1, int(oversample_factor)), 2), 131072))
                       for i in range(n_inst)]
             rnds = sample_by_mesh(n_refs, 17)
+            centroid_sets = [None] * n_inst
+            for mesh_id, members in by_mesh.items():
+                t_g, _ = group_geometry[mesh_id]
+                cm, cn = _group_centroids(t_g)
+                ids = np.arange(t_g.shape[1], dtype=np.uint32)
+                third = np.full(t_g.shape[1], 1.0 / 3.0, np.float32)
+                for j, i in enumerate(members):
+                    centroid_sets[i] = (cm[j], cn[j], ids, third, third)
             for i, (t, a) in enumerate(zip(tris, areas)):
                 rnd = rnds[i]
-                cen = _centroids(t, t.shape[0], None)
+                cen = centroid_sets[i]
                 refs.append(_concat([rnd, cen]))
                 ref_w.append(np.concatenate([np.full(rnd[0].shape[0], 0.5 * totals[i] / rnd[0].shape[0], np.float32),
                                              (0.5 * a).astype(np.float32)]))
