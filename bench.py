@@ -449,13 +449,13 @@ def run_nan(args):
     if world == 1 and not args.no_learned:
         line["learned_cache"] = learned_cache_line(device)
     if world == 1 and not args.no_consumers:
-        from nan_b200 import consumers_eval
+        from benchmarks import consumers_eval
 
         line["consumers"] = consumers_eval.measure(device, scene, node, layout, slots, frames=5)
     if world == 1 and not args.no_cornell:
         line["cornell_area_light"] = cornell_line(device)
     if world == 1 and not args.no_city:
-        from nan_b200 import city_eval
+        from benchmarks import city_eval
 
         # start the 4M-triangle section from released memory: the earlier
         # sections' scenes and buffers otherwise stay cached
@@ -464,7 +464,7 @@ def run_nan(args):
         torch.cuda.empty_cache()
         line["city_frame"] = city_eval.measure(device, frames=2)
     if world == 1 and not args.no_batched:
-        from nan_b200 import batch_eval
+        from benchmarks import batch_eval
 
         line["batched_probes"] = dict(batch_eval.measure(device, count=64, seed=1, samples_per_probe=64,
                                                          max_bounces=3, frames=2),
@@ -529,7 +529,7 @@ def learned_cache_line(device) -> dict:
     import torch
 
     import nan_b200
-    from nan_b200 import learned_eval, scenes
+    from benchmarks import learned_eval, scenes
 
     node = scenes.terrain_boxes(seed=1, grid=699, boxes=2000)
     scene = nan_b200.Scene(device, node)

@@ -31,16 +31,16 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
             frames: int = 3, tri_max: float = 5e5) -> dict:
     import torch
 
-    from . import scenes as sc
-    from .probe_batch import ProbeBatch
-    from .render_data import RenderData
-    from .scene import Scene
-    from .surface_probe_fields import SurfaceProbeRuntimeBuffers
-    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
-    from .surface_probe_resources import SurfaceProbeGpuGeometry
+    from nan_b200 import scenes as sc
+    from nan_b200.probe_batch import ProbeBatch
+    from nan_b200.render_data import RenderData
+    from nan_b200.scene import Scene
+    from nan_b200.surface_probe_fields import SurfaceProbeRuntimeBuffers
+    from nan_b200.surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from nan_b200.surface_probe_resources import SurfaceProbeGpuGeometry
 
-    from .surface_probe_layout import SurfaceProbeSiteLayout
-    from .surface_probe_sampler import SurfaceProbeSampler
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
 
     t0 = time.perf_counter()
     items, tris, sites = [], [], []
@@ -163,13 +163,13 @@ def main() -> None:
 
     import torch
 
-    from . import scenes as sc
-    from .probe_batch import ProbeBatch
-    from .render_data import RenderData
-    from .scene import Device, Scene
-    from .surface_probe_fields import SurfaceProbeRuntimeBuffers
-    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
-    from .surface_probe_resources import SurfaceProbeGpuGeometry
+    from nan_b200 import scenes as sc
+    from nan_b200.probe_batch import ProbeBatch
+    from nan_b200.render_data import RenderData
+    from nan_b200.scene import Device, Scene
+    from nan_b200.surface_probe_fields import SurfaceProbeRuntimeBuffers
+    from nan_b200.surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from nan_b200.surface_probe_resources import SurfaceProbeGpuGeometry
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--count", type=int, default=16)
@@ -179,8 +179,8 @@ def main() -> None:
     a = ap.parse_args()
     device = Device(0)
     items = []
-    from .surface_probe_layout import SurfaceProbeSiteLayout
-    from .surface_probe_sampler import SurfaceProbeSampler
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
 
     sampler = SurfaceProbeSampler(device)
     for i, (node, n_sites) in enumerate(sc.batch_scenes(a.count, 1)):

@@ -17,22 +17,22 @@ import time
 def measure(device, frames: int = 2, width: int = 3840, height: int = 2160, spp: int = 4) -> dict:
     import torch
 
-    from . import scenes as sc
-    from .accumulator import Accumulator
-    from .cached_path_tracer import CachedPathTracer
-    from .learned_eval import scene_bounds
-    from .mesh_colors import MeshColorsLayout
-    from .path_tracer import PathTracer
-    from .probe_batch import ProbeBatch
-    from .radiance_cache import RadianceCache
-    from .render_data import RenderData
-    from .scene import Scene
-    from .surface_probe_fields import SurfaceProbeRuntimeBuffers
-    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
-    from .surface_probe_layout import SurfaceProbeSiteLayout
-    from .surface_probe_resources import SurfaceProbeGpuGeometry
-    from .surface_probe_sampler import SurfaceProbeSampler
-    from .texture_space_path_tracer import TextureSpacePathTracer
+    from nan_b200 import scenes as sc
+    from nan_b200.accumulator import Accumulator
+    from nan_b200.cached_path_tracer import CachedPathTracer
+    from nan_b200.radiance_cache import scene_bounds
+    from nan_b200.mesh_colors import MeshColorsLayout
+    from nan_b200.path_tracer import PathTracer
+    from nan_b200.probe_batch import ProbeBatch
+    from nan_b200.radiance_cache import RadianceCache
+    from nan_b200.render_data import RenderData
+    from nan_b200.scene import Scene
+    from nan_b200.surface_probe_fields import SurfaceProbeRuntimeBuffers
+    from nan_b200.surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_resources import SurfaceProbeGpuGeometry
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
+    from nan_b200.texture_space_path_tracer import TextureSpacePathTracer
 
     t0 = time.perf_counter()
     node = sc.city(width=width, height=height)

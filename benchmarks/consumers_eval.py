@@ -19,18 +19,18 @@ def measure(device, scene, node, layout, slots, *, frames: int = 5, width: int =
             probe_sites: int = 20480) -> dict:
     import torch
 
-    from .mesh_colors_resolve import MeshColorsResolve
-    from .mesh_colors_rgb9e5 import MeshColorsRGB9E5Packer
-    from .mesh_colors_surface_filter import MeshColorsSurfaceFilter
-    from .render_data import RenderData
-    from .surface_probe_fields import (DIFFUSE_PRT_ATTACHMENTS, DIFFUSE_PRT_L2_RGB_FIELD,
+    from nan_b200.mesh_colors_resolve import MeshColorsResolve
+    from nan_b200.mesh_colors_rgb9e5 import MeshColorsRGB9E5Packer
+    from nan_b200.mesh_colors_surface_filter import MeshColorsSurfaceFilter
+    from nan_b200.render_data import RenderData
+    from nan_b200.surface_probe_fields import (DIFFUSE_PRT_ATTACHMENTS, DIFFUSE_PRT_L2_RGB_FIELD,
                                        SurfaceProbeRuntimeBuffers)
-    from .surface_probe_layout import SurfaceProbeSiteLayout
-    from .surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
-    from .surface_probe_prt import SurfaceProbePrtBaker, SurfaceProbePrtEvaluator
-    from .surface_probe_resolve import SurfaceProbeResolve
-    from .surface_probe_resources import SurfaceProbeGpuGeometry
-    from .texture_space_path_tracer import TextureSpacePathTracer
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_path_tracer import SurfaceProbeDiffuseIrradianceBaker
+    from nan_b200.surface_probe_prt import SurfaceProbePrtBaker, SurfaceProbePrtEvaluator
+    from nan_b200.surface_probe_resolve import SurfaceProbeResolve
+    from nan_b200.surface_probe_resources import SurfaceProbeGpuGeometry
+    from nan_b200.texture_space_path_tracer import TextureSpacePathTracer
 
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -106,10 +106,10 @@ def main(argv=None) -> None:
 
     import torch
 
-    from . import scenes
-    from .mesh_colors import MeshColorsLayout
-    from .scene import Device, Scene
-    from .texture_space_path_tracer import TextureSpacePathTracer
+    from nan_b200 import scenes
+    from nan_b200.mesh_colors import MeshColorsLayout
+    from nan_b200.scene import Device, Scene
+    from nan_b200.texture_space_path_tracer import TextureSpacePathTracer
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--frames", type=int, default=5)

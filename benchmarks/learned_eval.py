@@ -13,20 +13,14 @@ its relative RMSE against the reference over all pixels and channels.
 
 from __future__ import annotations
 
+from nan_b200.radiance_cache import scene_bounds
+
 
 def _rel_rmse(img, ref) -> float:
     import torch
 
     d = img - ref
     return float(torch.sqrt(torch.mean(d * d)) / torch.sqrt(torch.mean(ref * ref)))
-
-
-def scene_bounds(scene, margin: float = 1e-3):
-    tris = scene.world_triangles().reshape(-1, 3)
-    lo = tris.min(dim=0).values.cpu().numpy()
-    hi = tris.max(dim=0).values.cpu().numpy()
-    pad = margin * float((hi - lo).max())
-    return tuple(float(x) - pad for x in lo), tuple(float(x) + pad for x in hi)
 
 
 def compare(device, scene, width: int, height: int, *, reference_frames: int = 512, frames: int = 64,
@@ -47,9 +41,9 @@ def compare(device, scene, width: int, height: int, *, reference_frames: int = 5
     RMSE after k frames (1.1x for the cached one)."""
     import torch
 
-    from .cached_path_tracer import CachedPathTracer
-    from .path_tracer import PathTracer
-    from .radiance_cache import RadianceCache
+    from nan_b200.cached_path_tracer import CachedPathTracer
+    from nan_b200.path_tracer import PathTracer
+    from nan_b200.radiance_cache import RadianceCache
 
     stream = torch.cuda.current_stream()
     cam = scene.camera
@@ -169,10 +163,10 @@ def main() -> None:
 
     import torch
 
-    from . import scenes
-    from .cached_path_tracer import CachedPathTracer
-    from .radiance_cache import RadianceCache
-    from .scene import Device, Scene
+    from nan_b200 import scenes
+    from nan_b200.cached_path_tracer import CachedPathTracer
+    from nan_b200.radiance_cache import RadianceCache
+    from nan_b200.scene import Device, Scene
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--frames", type=int, default=6)

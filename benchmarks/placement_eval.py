@@ -22,9 +22,9 @@ def _wse(device, grid: int, repeats: int) -> dict:
     import numpy as np
     import torch
 
-    from . import scenes
-    from .surface_probe_layout import _surface_points
-    from .surface_probe_sampler import SurfaceProbeSampler
+    from nan_b200 import scenes
+    from nan_b200.surface_probe_layout import _surface_points
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
 
     node = scenes.terrain_boxes(seed=2, grid=grid, boxes=0)
     mesh_id, _, transform_id = node.instances[0]
@@ -53,10 +53,10 @@ def _wse(device, grid: int, repeats: int) -> dict:
 def main(argv=None) -> None:
     import argparse
 
-    from . import scenes
-    from .scene import Device
-    from .surface_probe_layout import SurfaceProbeSiteLayout
-    from .surface_probe_sampler import SurfaceProbeSampler
+    from nan_b200 import scenes
+    from nan_b200.scene import Device
+    from nan_b200.surface_probe_layout import SurfaceProbeSiteLayout
+    from nan_b200.surface_probe_sampler import SurfaceProbeSampler
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--mode", choices=("layout", "wse"), default="layout")

@@ -45,6 +45,16 @@ def initial_parameters(log2_table: int, seed: int = 0):
     return mlp, table
 
 
+def scene_bounds(scene, margin: float = 1e-3):
+    """The scene's world-space box grown by `margin` x its largest extent on
+    every side: the bounds a RadianceCache normalises positions to."""
+    tris = scene.world_triangles().reshape(-1, 3)
+    lo = tris.min(dim=0).values.cpu().numpy()
+    hi = tris.max(dim=0).values.cpu().numpy()
+    pad = margin * float((hi - lo).max())
+    return tuple(float(x) - pad for x in lo), tuple(float(x) + pad for x in hi)
+
+
 class RadianceCache:
     def __init__(self, device, bounds_min, bounds_max, *, log2_table: int = 19, base_resolution: int = 16,
                  max_resolution: int = 2048, learning_rate: float = 1e-2, beta1: float = 0.9, beta2: float = 0.99,

@@ -68,7 +68,7 @@ def test_cached_frame_records_queries_and_training_points(device):
 
     import nan_b200
     from nan_b200 import scenes
-    from nan_b200.learned_eval import scene_bounds
+    from nan_b200.radiance_cache import scene_bounds
 
     node = scenes.terrain_boxes(seed=1, grid=129, boxes=120)
     scene = nan_b200.Scene(device, node)
@@ -108,7 +108,8 @@ def tracer_offset(frame, p):
 @pytest.mark.parametrize("which", ["cornell", "terrain"])
 def test_trained_cache_gains_over_untrained(which, device):
     import nan_b200
-    from nan_b200 import learned_eval, scenes
+    from benchmarks import learned_eval
+    from nan_b200 import scenes
 
     if which == "cornell":
         node, w, h = scenes.cornell_box(64, 64), 64, 64
