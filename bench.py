@@ -529,7 +529,8 @@ def learned_cache_line(device) -> dict:
     import torch
 
     import nan_b200
-    from benchmarks import learned_eval, scenes
+    from benchmarks import learned_eval
+    from nan_b200 import scenes
 
     node = scenes.terrain_boxes(seed=1, grid=699, boxes=2000)
     scene = nan_b200.Scene(device, node)
