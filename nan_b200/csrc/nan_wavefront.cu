@@ -364,6 +364,12 @@ __global__ void __launch_bounds__(128, 10) k_wf_shadow_refill(Src src, const flo
     flush_tally(counters, tally, 0u, 0u);
 }
 
+// The path-state stages (generate / shade / finalize) are bound by the
+// latency of their gathers (scene records, path state) more than by
+// bandwidth: their launch bound of 6 blocks of 128 per SM (at most 80
+// registers, no spills in the texel stages; they used 111-128) doubles the
+// resident warps. Measured on the 200k texel iteration: 5.54 -> 5.03 ms of
+// stage time per step.
 // ---------------------------------------------------------------------------
 // Texture-space integrator stages (texture_space_path_tracer.slang:57-216).
 // ---------------------------------------------------------------------------
@@ -414,7 +420,7 @@ __device__ __forceinline__ void texel_start_sample(const SceneView& s, const Lig
     q.ext[buf][slot] = p;
 }
 
-__global__ void __launch_bounds__(128) k_wf_texel_generate(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_texel_generate(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
                                                            WfQueues q, uint32_t begin, uint32_t count,
                                                            unsigned long long* counters) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,7 +469,7 @@ __global__ void __launch_bounds__(128) k_wf_point_generate(SceneView s, Lighting
 
 // One bounce of trace_radiance (texture_space_path_tracer.slang:60-83) after
 // the extend stage found the hit.
-__global__ void __launch_bounds__(128) k_wf_texel_shade(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_texel_shade(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
                                                         WfQueues q, int buf, uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -516,7 +522,7 @@ __global__ void __launch_bounds__(128) k_wf_texel_shade(SceneView s, LightingRaw
 
 // Close finished samples: si += L*|z|/pdf, irr += si, next sample / side, or
 // the running-mean store (texture_space_path_tracer.slang:111-138, 203-215).
-__global__ void __launch_bounds__(128) k_wf_texel_finalize(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_texel_finalize(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
                                                            WfQueues q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -650,7 +656,7 @@ __device__ __forceinline__ f3 fold_area_term(const WfState& st, uint32_t p, f3 r
     return rad + xyz(a);
 }
 
-__global__ void __launch_bounds__(128) k_wf_screen_shade(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_screen_shade(SceneView s, LightingRaw lraw, ScreenArgs a, WfState st,
                                                          WfQueues q, int buf, uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -973,7 +979,7 @@ __global__ void __launch_bounds__(128) k_wf_probe_generate(SceneView s, Lighting
     flush_tally(counters, none, 1u, a.n);
 }
 
-__global__ void __launch_bounds__(128) k_wf_probe_shade(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_probe_shade(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
                                                         WfQueues q, int buf, uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -981,7 +987,7 @@ __global__ void __launch_bounds__(128) k_wf_probe_shade(SceneView s, LightingRaw
         probe_shade_path(s, L, a, st, q, buf, ctl, q.ext[buf][idx]);
 }
 
-__global__ void __launch_bounds__(128) k_wf_probe_finalize(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
+__global__ void __launch_bounds__(128, 6) k_wf_probe_finalize(SceneView s, LightingRaw lraw, ProbeArgs a, WfState st,
                                                            WfQueues q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -1139,7 +1145,7 @@ __global__ void __launch_bounds__(128) k_wfi_probe_fold(BatchWfArgs m, unsigned 
     flush_tally(counters, none, 1u, m.n);
 }
 
-__global__ void __launch_bounds__(128) k_wfb_probe_shade(BatchWfArgs m, WfState st, WfQueues q, int buf,
+__global__ void __launch_bounds__(128, 6) k_wfb_probe_shade(BatchWfArgs m, WfState st, WfQueues q, int buf,
                                                          uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
@@ -1149,7 +1155,7 @@ __global__ void __launch_bounds__(128) k_wfb_probe_shade(BatchWfArgs m, WfState 
     }
 }
 
-__global__ void __launch_bounds__(128) k_wfb_probe_finalize(BatchWfArgs m, WfState st, WfQueues q, int buf,
+__global__ void __launch_bounds__(128, 6) k_wfb_probe_finalize(BatchWfArgs m, WfState st, WfQueues q, int buf,
                                                             uint32_t* ctl, uint32_t* ctl_next) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
