@@ -311,6 +311,34 @@ def _render_vertices(mesh, transform, k, rng, vertex_list=None):
     return pos, nrm, tri.astype(np.uint32), (corner == 1).astype(np.float32), (corner == 2).astype(np.float32)
 
 
+def _instance_areas(scene_node, chunk_triangles: int = 1 << 20):
+    """Per instance: world-space surface area (float64: transformed
+    vertices, |cross| / 2 summed over its triangles) and triangle count. The
+    instances of one mesh are transformed together, in chunks of about
+    chunk_triangles triangles; each instance's arithmetic is the one its own
+    transform alone would do."""
+    n = len(scene_node.instances)
+    areas = np.zeros(n)
+    tri_counts = np.zeros(n, np.int64)
+    groups: dict = {}
+    for i, (mesh_id, _, _) in enumerate(scene_node.instances):
+        groups.setdefault(mesh_id, []).append(i)
+    for mesh_id, members in groups.items():
+        mesh = scene_node.meshes[mesh_id]
+        v = mesh.vertices[:, :3].astype(np.float64)
+        idx = mesh.indices.astype(np.int64).reshape(-1, 3)
+        step = max(1, chunk_triangles // max(idx.shape[0], 1))
+        for c in range(0, len(members), step):
+            part = members[c:c + step]
+            m = np.stack([np.asarray(scene_node.transforms[scene_node.instances[i][2]], dtype=np.float64)
+                          for i in part])
+            t = (v @ m[:, :3, :3].transpose(0, 2, 1) + m[:, None, :3, 3])[:, idx]  # [g, T, 3, 3]
+            cr = np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0])
+            areas[part] = 0.5 * np.linalg.norm(cr, axis=2).sum(axis=1)
+            tri_counts[part] = idx.shape[0]
+    return areas, tri_counts
+
+
 def _take(points, idx):
     return tuple(x[idx] for x in points)
 
@@ -388,8 +416,12 @@ class SurfaceProbeSiteLayout:
     def from_sites(cls, scene_node, probes, *, leaf_capacity: int = 8, max_depth: int = 16,
                    kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
                    max_density_multiplier: float = 8.0, poisson_radii=None,
-                   kernel_radii=None, vertex_anchors=None, sampler=None) -> "SurfaceProbeSiteLayout":
-        """vertex_anchors (optional, per instance None or (records, map,
+                   kernel_radii=None, vertex_anchors=None, sampler=None,
+                   instance_stats=None) -> "SurfaceProbeSiteLayout":
+        """instance_stats (optional): further SurfaceProbeSiteInstance fields
+        as {name: one value per instance}, e.g. a site builder's counts.
+
+        vertex_anchors (optional, per instance None or (records, map,
         anchor site count)): anchor probe records (fronts, then backs for a
         double-sided instance) kept after the instance's octree-ordered probes
         and outside its octree, and map u32[T, 3] naming each triangle's three
@@ -399,94 +431,112 @@ class SurfaceProbeSiteLayout:
         GPU in one call (nan_build_point_octrees), else by
         build_point_octree on the host; both give the same nodes and order."""
         probes = np.asarray(probes, dtype=SURFACE_PROBE_DTYPE)
-        instance_of = probes["meta"][:, 3] >> SURFACE_PROBE_INSTANCE_SHIFT
+        instance_of = (probes["meta"][:, 3] >> SURFACE_PROBE_INSTANCE_SHIFT).astype(np.int64)
         n_inst = len(scene_node.instances)
         if probes.shape[0] and int(instance_of.max()) >= n_inst:
             raise ValueError("a probe names an instance the scene does not have")
-        areas = np.zeros(n_inst)
-        tri_counts = np.zeros(n_inst, np.int64)
-        for i, (mesh_id, _, transform_id) in enumerate(scene_node.instances):
-            mesh = scene_node.meshes[mesh_id]
-            m = scene_node.transforms[transform_id].astype(np.float64)
-            p = mesh.vertices[:, :3].astype(np.float64) @ m[:3, :3].T + m[:3, 3]
-            t = p[mesh.indices.astype(np.int64).reshape(-1, 3)]
-            areas[i] = 0.5 * np.linalg.norm(np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0]), axis=1).sum()
-            tri_counts[i] = t.shape[0]
+        areas, tri_counts = _instance_areas(scene_node)
         fronts = np.bincount(instance_of[(probes["meta"][:, 3] & 1) == 0], minlength=n_inst)
         total_sites = max(int(fronts.sum()), 1)
         global_kernel = max(math.sqrt(max(float(areas.sum()), 1e-20) / total_sites) * kernel_radius_scale, 1e-5)
         normal_cos = math.cos(math.radians(normal_angle_degrees))
+        if kernel_radii is not None:
+            kernel = np.asarray(kernel_radii, dtype=np.float64).reshape(-1)[:n_inst]
+        else:
+            with np.errstate(divide="ignore", invalid="ignore"):
+                per_site = np.where(fronts > 0, np.sqrt(areas / np.maximum(fronts, 1)) * kernel_radius_scale, 0.0)
+            kernel = np.maximum(np.maximum(global_kernel, per_site), 1e-5)
+            if poisson_radii is not None:
+                kernel = np.maximum(kernel, np.asarray(poisson_radii, dtype=np.float64).reshape(-1)[:n_inst] *
+                                    kernel_radius_scale)
 
-        gpu = np.zeros(n_inst, dtype=SURFACE_PROBE_INSTANCE_DTYPE)
-        out_probes, out_nodes, out_maps, infos = [], [], [], []
-        node_offset = probe_offset = map_offset = 0
+        # the records grouped by instance, each group in its octree's order
         by_instance = np.argsort(instance_of, kind="stable")
-        bounds = np.searchsorted(instance_of[by_instance], np.arange(n_inst + 1))
-        gpu_trees = None
+        counts = np.bincount(instance_of, minlength=n_inst).astype(np.int64)
+        starts = np.concatenate([[0], np.cumsum(counts)])
+        rec_all = probes[by_instance]
+        inst_sorted = instance_of[by_instance]
+        rec_all["position_radius"][:, 3] = kernel[inst_sorted]
+        roots = np.zeros((n_inst, 4), np.float64)
         if sampler is not None and probes.shape[0]:
-            gpu_trees = sampler.build_point_octrees(
-                [probes["position_radius"][by_instance[bounds[i]:bounds[i + 1]], :3] for i in range(n_inst)],
-                leaf_capacity=leaf_capacity, max_depth=max_depth)
-        for i in range(n_inst):
-            rec = probes[by_instance[bounds[i]:bounds[i + 1]]].copy()
-            sites = int(fronts[i])
-            if kernel_radii is not None:
-                kernel = float(kernel_radii[i])
-            else:
-                kernel = max(global_kernel, math.sqrt(areas[i] / sites) * kernel_radius_scale if sites else 0.0,
-                             float(poisson_radii[i]) * kernel_radius_scale if poisson_radii is not None else 0.0,
-                             1e-5)
-            maps = np.full((int(tri_counts[i]) * 2, 4), 0xFFFFFFFF, np.uint32)
-            maps[:, 3] = 0
-            if rec.shape[0]:
-                rec["position_radius"][:, 3] = kernel
-                if gpu_trees is not None:
-                    nodes, order, center, extent = gpu_trees[i]
-                else:
-                    nodes, order, center, extent = build_point_octree(rec["position_radius"][:, :3],
-                                                                      leaf_capacity=leaf_capacity,
-                                                                      max_depth=max_depth)
-                rec = rec[order]
-                nodes = nodes.copy()
-                branch = nodes[:, 1] != 0
-                nodes[branch, 0] += np.uint32(node_offset)
-                nodes[~branch, 2] += np.uint32(probe_offset)
-            else:
-                nodes = np.zeros((0, 4), np.uint32)
-                center, extent = (0.0, 0.0, 0.0), 0.0
-            recon = int(rec.shape[0])
-            if vertex_anchors is not None and vertex_anchors[i] is not None:
-                anchor_rec, tri_map, anchor_sites = vertex_anchors[i]
-                anchor_rec = np.asarray(anchor_rec, dtype=SURFACE_PROBE_DTYPE).copy()
-                anchor_rec["position_radius"][:, 3] = kernel
-                rec = np.concatenate([rec, anchor_rec])
-                tri_map = np.asarray(tri_map, dtype=np.uint32).reshape(-1, 3)
-                valid = np.flatnonzero(np.all(tri_map != 0xFFFFFFFF, axis=1))
-                front = tri_map[valid] + np.uint32(probe_offset + recon)
-                back = front + np.uint32(anchor_sites) if anchor_rec.shape[0] > anchor_sites else front
-                maps[2 * valid, :3] = front
-                maps[2 * valid + 1, :3] = back
-                maps[2 * valid, 3] |= 1
-                maps[2 * valid + 1, 3] |= 1
-            plane_sigma = max(kernel * 0.25, 1e-6)
-            gpu["root_center_extent"][i] = (*center, extent)
-            gpu["offsets"][i] = (node_offset, nodes.shape[0], probe_offset, rec.shape[0])
-            gpu["params"][i] = (kernel, normal_cos, plane_sigma,
-                                np.asarray(map_offset, dtype=np.uint32).view(np.float32).item())
-            infos.append(SurfaceProbeSiteInstance(center, extent, node_offset, int(nodes.shape[0]), probe_offset,
-                                                  int(rec.shape[0]), kernel, normal_cos, plane_sigma,
-                                                  float(areas[i]), sites, recon))
-            out_probes.append(rec)
-            out_nodes.append(nodes)
-            out_maps.append(maps)
-            node_offset += nodes.shape[0]
-            probe_offset += rec.shape[0]
-            map_offset += maps.shape[0]
-        all_nodes = np.concatenate(out_nodes) if node_offset else np.zeros((1, 4), np.uint32)
-        all_maps = np.concatenate(out_maps) if map_offset else np.zeros((2, 4), np.uint32)
-        return cls(np.concatenate(out_probes), np.ascontiguousarray(all_nodes, np.uint32),
-                   np.ascontiguousarray(all_maps, np.uint32), gpu, tuple(infos), int(probe_offset),
-                   float(max_density_multiplier))
+            tree_nodes, tree_node_offsets, order, roots[:] = sampler.build_point_octrees_flat(
+                rec_all["position_radius"][:, :3], starts, leaf_capacity=leaf_capacity, max_depth=max_depth)
+            node_counts = np.diff(tree_node_offsets.astype(np.int64))
+        else:
+            parts, order_parts = [], []
+            node_counts = np.zeros(n_inst, np.int64)
+            for i in np.flatnonzero(counts):
+                nodes, order_i, center, extent = build_point_octree(
+                    rec_all["position_radius"][starts[i]:starts[i + 1], :3], leaf_capacity=leaf_capacity,
+                    max_depth=max_depth)
+                parts.append(nodes)
+                order_parts.append(order_i)
+                node_counts[i] = nodes.shape[0]
+                roots[i] = (*center, extent)
+            tree_nodes = np.concatenate(parts) if parts else np.zeros((0, 4), np.uint32)
+            order = np.concatenate(order_parts) if order_parts else np.zeros(0, np.int64)
+        node_counts[counts == 0] = 0
+        roots[counts == 0] = 0.0
+        rec_all = rec_all[starts[inst_sorted] + order]
+        # anchor records follow their instance's octree records
+        anchor_counts = np.zeros(n_inst, np.int64)
+        anchored = [] if vertex_anchors is None else [i for i in range(n_inst) if vertex_anchors[i] is not None]
+        for i in anchored:
+            anchor_counts[i] = np.asarray(vertex_anchors[i][0]).shape[0]
+        rec_counts = counts + anchor_counts
+        probe_offsets = np.concatenate([[0], np.cumsum(rec_counts)])
+        node_offsets = np.concatenate([[0], np.cumsum(node_counts)])
+        map_offsets = np.concatenate([[0], np.cumsum(tri_counts * 2)])
+        if anchored:
+            out_probes = np.zeros(int(probe_offsets[-1]), dtype=SURFACE_PROBE_DTYPE)
+            out_probes[probe_offsets[inst_sorted] + (np.arange(inst_sorted.shape[0]) - starts[inst_sorted])] = rec_all
+        else:
+            out_probes = rec_all
+        nodes_all = np.ascontiguousarray(tree_nodes, np.uint32).copy()
+        node_inst = np.repeat(np.arange(n_inst), node_counts)
+        branch = nodes_all[:, 1] != 0
+        nodes_all[branch, 0] += node_offsets[node_inst[branch]].astype(np.uint32)
+        nodes_all[~branch, 2] += probe_offsets[node_inst[~branch]].astype(np.uint32)
+        maps_all = np.full((int(map_offsets[-1]), 4), 0xFFFFFFFF, np.uint32)
+        maps_all[:, 3] = 0
+        for i in anchored:
+            anchor_rec, tri_map, anchor_sites = vertex_anchors[i]
+            anchor_rec = np.asarray(anchor_rec, dtype=SURFACE_PROBE_DTYPE).copy()
+            anchor_rec["position_radius"][:, 3] = kernel[i]
+            first = int(probe_offsets[i] + counts[i])
+            out_probes[first:first + anchor_rec.shape[0]] = anchor_rec
+            tri_map = np.asarray(tri_map, dtype=np.uint32).reshape(-1, 3)
+            valid = np.flatnonzero(np.all(tri_map != 0xFFFFFFFF, axis=1))
+            front = tri_map[valid] + np.uint32(first)
+            back = front + np.uint32(anchor_sites) if anchor_rec.shape[0] > anchor_sites else front
+            maps = maps_all[map_offsets[i]:map_offsets[i + 1]]
+            maps[2 * valid, :3] = front
+            maps[2 * valid + 1, :3] = back
+            maps[2 * valid, 3] |= 1
+            maps[2 * valid + 1, 3] |= 1
+
+        plane_sigma = np.maximum(kernel * 0.25, 1e-6)
+        gpu = np.zeros(n_inst, dtype=SURFACE_PROBE_INSTANCE_DTYPE)
+        gpu["root_center_extent"] = roots
+        gpu["offsets"] = np.stack([node_offsets[:-1], node_counts, probe_offsets[:-1], rec_counts],
+                                  axis=1).astype(np.uint32)
+        gpu["params"][:, 0] = kernel
+        gpu["params"][:, 1] = normal_cos
+        gpu["params"][:, 2] = plane_sigma
+        gpu["params"][:, 3] = map_offsets[:-1].astype(np.uint32).view(np.float32)
+        roots_l, kernel_l, sigma_l, areas_l = roots.tolist(), kernel.tolist(), plane_sigma.tolist(), areas.tolist()
+        stats = instance_stats or {}
+        stat_l = {k: np.asarray(v).tolist() for k, v in stats.items()}
+        infos = tuple(
+            SurfaceProbeSiteInstance(tuple(roots_l[i][:3]), roots_l[i][3], no, nc, po, pc, kernel_l[i], normal_cos,
+                                     sigma_l[i], areas_l[i], fr, co, **{k: v[i] for k, v in stat_l.items()})
+            for i, (no, nc, po, pc, fr, co) in enumerate(zip(node_offsets[:-1].tolist(), node_counts.tolist(),
+                                                             probe_offsets[:-1].tolist(), rec_counts.tolist(),
+                                                             fronts.tolist(), counts.tolist())))
+        all_nodes = nodes_all if nodes_all.shape[0] else np.zeros((1, 4), np.uint32)
+        all_maps = maps_all if maps_all.shape[0] else np.zeros((2, 4), np.uint32)
+        return cls(out_probes, np.ascontiguousarray(all_nodes, np.uint32), np.ascontiguousarray(all_maps, np.uint32),
+                   gpu, infos, int(probe_offsets[-1]), float(max_density_multiplier))
 
     @classmethod
     def build_wse(cls, scene_node, target_probe_count: int, *, device=None, oversample_factor: int = 5,

@@ -183,22 +183,45 @@ class SurfaceProbeSampler:
         GPU call, as build_point_octree builds each: per set (nodes u32
         [M, 4], order i64 [n], root centre, root half extent), or None for an
         empty set."""
+        sets = [np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3) for x in position_sets]
+        offsets = np.concatenate([[0], np.cumsum([x.shape[0] for x in sets])]).astype(np.uint32)
+        if int(offsets[-1]) == 0:
+            return [None] * len(sets)
+        nodes_h, node_offsets, order_h, roots = self.build_point_octrees_flat(
+            np.concatenate(sets), offsets, leaf_capacity=leaf_capacity, max_depth=max_depth, stream=stream)
+        out = []
+        for k in range(len(sets)):
+            if offsets[k + 1] == offsets[k]:
+                out.append(None)
+                continue
+            out.append((nodes_h[node_offsets[k]:node_offsets[k + 1]].copy(), order_h[offsets[k]:offsets[k + 1]],
+                        tuple(float(v) for v in roots[k, :3]), float(roots[k, 3])))
+        return out
+
+    def build_point_octrees_flat(self, positions, set_offsets, *, leaf_capacity: int = 8, max_depth: int = 16,
+                                 stream=None):
+        """build_point_octrees over sets stored back to back (positions f32
+        [N, 3], set k at set_offsets[k]:set_offsets[k + 1]): (nodes u32 [M,
+        4] with set k's nodes at node_offsets[k]:node_offsets[k + 1], child
+        and probe indices local to the set; node_offsets u32 [S + 1]; order
+        i64 [N], set k's permutation of its own points at its offsets; roots
+        f64 [S, 4], centre and half extent). An empty set has no nodes."""
         import torch
 
         dev = self.device.torch_device if hasattr(self.device, "torch_device") else torch.device("cuda")
-        sets = [np.ascontiguousarray(x, dtype=np.float32).reshape(-1, 3) for x in position_sets]
-        offsets = np.concatenate([[0], np.cumsum([x.shape[0] for x in sets])]).astype(np.uint32)
+        offsets = np.ascontiguousarray(set_offsets, dtype=np.uint32).reshape(-1)
+        sets = offsets.shape[0] - 1
         n = int(offsets[-1])
-        if n == 0:
-            return [None] * len(sets)
-        pos = torch.as_tensor(np.concatenate(sets), device=dev)
-        order = torch.empty(n, dtype=torch.int32, device=dev)
-        node_offsets = np.zeros(len(sets) + 1, np.uint32)
-        roots = np.zeros((len(sets), 4), np.float64)
-        capacity = max(64, n // max(int(leaf_capacity), 1) * 3 + 2 * len(sets))
+        pos = torch.as_tensor(np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3), device=dev)
+        if pos.shape[0] != n:
+            raise ValueError("set_offsets must end at the number of positions")
+        order = torch.empty(max(n, 1), dtype=torch.int32, device=dev)
+        node_offsets = np.zeros(sets + 1, np.uint32)
+        roots = np.zeros((max(sets, 1), 4), np.float64)
+        capacity = max(64, n // max(int(leaf_capacity), 1) * 3 + 2 * sets)
         for _ in range(2):
             nodes = torch.empty((capacity, 4), dtype=torch.int32, device=dev)
-            rc = lib().nan_build_point_octrees(self.context.handle, ptr(pos), offsets.ctypes.data, len(sets),
+            rc = lib().nan_build_point_octrees(self.context.handle, ptr(pos), offsets.ctypes.data, sets,
                                                int(leaf_capacity), int(max_depth), ptr(nodes), capacity,
                                                node_offsets.ctypes.data, ptr(order), roots.ctypes.data,
                                                stream_handle(stream))
@@ -208,15 +231,7 @@ class SurfaceProbeSampler:
             check(rc)
             break
         nodes_h = nodes[:int(node_offsets[-1])].cpu().numpy().view(np.uint32)
-        order_h = order.cpu().numpy().astype(np.int64)
-        out = []
-        for k in range(len(sets)):
-            if offsets[k + 1] == offsets[k]:
-                out.append(None)
-                continue
-            out.append((nodes_h[node_offsets[k]:node_offsets[k + 1]].copy(), order_h[offsets[k]:offsets[k + 1]],
-                        tuple(float(v) for v in roots[k, :3]), float(roots[k, 3])))
-        return out
+        return nodes_h, node_offsets, order[:n].cpu().numpy().astype(np.int64), roots[:sets]
 
     def deficit_repair(self, base_positions, base_normals, base_instances, candidate_positions, candidate_normals,
                        candidate_instances, audit_positions, audit_normals, audit_instances, instance_radii, *,
