@@ -634,190 +634,234 @@ __global__ void k_rep_count_chosen(uint32_t n, const uint8_t* chosen, unsigned i
 // summed by the pairwise scheme, the buffer sums added in order;
 // f = clip(support / (pi R^2 / 3), 0, 1), m = min(M, 1 / max(f, 1/M)).
 //
-// A query's points are the 27 grid cells around it, each an index-sorted
-// run of the sorted grid: one pass counts the terms, a second merges the
-// runs by index and streams the terms into the summation, so no query holds
-// its terms and none is capped.
+// The queries are grouped by (instance, grid cell). A cell's candidates --
+// the reference points of its 3x3x3 neighbourhood, nine column ranges of
+// the sorted grid -- are listed once and sorted by reference index, and one
+// warp takes up to 32 of the cell's queries through that list in tiles of 32
+// candidates staged in shared memory, so every lane tests the same candidate
+// at the same step. A first pass counts each query's terms (the shape of the
+// pairwise scheme depends on the count), a second feeds them to the sum.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kNumpyBuffer = 8192;  // numpy's default ufunc buffer (elements)
+constexpr uint32_t kSupportWarps = 4;    // warps per block of k_support_sum
+constexpr unsigned long long kSupportBatch = 1ull << 26;  // list entries sorted at once
 
-// The non-empty cell runs around a query, with each run's head (the
-// reference index at its cursor) cached.
-struct CellRuns {
-    uint32_t b[27], e[27], head[27];
-    int n;
+// numpy's float64 sum of a float32 array, fed one term at a time, for a term
+// count known before the first term: buffers of 8192 terms whose sums are
+// added in order; each buffer by the pairwise scheme -- above 128 terms the
+// left part takes n/2 rounded down to a multiple of 8; a leaf of 8 to 128
+// terms keeps eight running sums over its whole 8-blocks, combines them
+// pairwise and adds the remainder in order; a leaf of fewer than 8 terms is
+// summed in order from 0. The path from a buffer's root to the current leaf
+// is a stack of (node length, left sum, taking the right child); a buffer of
+// 8192 terms is at most 7 levels deep.
+struct PairwiseFeed {
+    double acc[8];
+    double leaf, total;
+    double frame_left[8];
+    uint32_t frame_len[8];
+    uint32_t remaining, leaf_len, leaf_pos, depth, right;
+
+    __device__ void descend(uint32_t len) {
+        while (len > 128u) {
+            frame_len[depth] = len;
+            right &= ~(1u << depth);
+            ++depth;
+            len = len / 2u - (len / 2u) % 8u;
+        }
+        leaf_len = len;
+        leaf_pos = 0;
+        leaf = 0.0;
+    }
+    __device__ void next_buffer() {
+        const uint32_t len = min(kNumpyBuffer, remaining);
+        remaining -= len;
+        depth = 0;
+        right = 0;
+        descend(len);
+    }
+    __device__ void begin(uint32_t n) {
+        total = 0.0;
+        remaining = n;
+        if (n) next_buffer();
+    }
+    __device__ void finish_leaf() {
+        double v = leaf;
+        for (;;) {
+            if (depth == 0) {
+                total = total + v;
+                if (remaining) next_buffer();
+                return;
+            }
+            const uint32_t d = depth - 1;
+            if (!((right >> d) & 1u)) {  // the left child is done: take the right one
+                frame_left[d] = v;
+                right |= 1u << d;
+                descend(frame_len[d] - (frame_len[d] / 2u - (frame_len[d] / 2u) % 8u));
+                return;
+            }
+            v = frame_left[d] + v;
+            depth = d;
+        }
+    }
+    __device__ __forceinline__ void push(double v) {
+        if (leaf_len < 8u) {
+            leaf += v;
+        } else {
+            const uint32_t blocks_end = leaf_len - leaf_len % 8u;
+            if (leaf_pos < blocks_end) {
+                const uint32_t j = leaf_pos & 7u;
+                acc[j] = leaf_pos < 8u ? v : acc[j] + v;
+                if (leaf_pos + 1u == blocks_end)
+                    leaf = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+            } else {
+                leaf += v;
+            }
+        }
+        if (++leaf_pos == leaf_len) finish_leaf();
+    }
 };
 
-__device__ __forceinline__ void support_runs(const RepairGrid& g, uint32_t k, const int c[3], CellRuns& r) {
-    r.n = 0;
+// Reference points in index order as two float4: position and area weight,
+// normal and 0.
+__global__ void k_support_pack(RepairSet ref, const float* area, float4* packed) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ref.n) return;
+    const float* p = ref.pos + 3 * (size_t)j;
+    const float* n = ref.nrm + 3 * (size_t)j;
+    packed[2 * (size_t)j] = make_float4(p[0], p[1], p[2], area[j]);
+    packed[2 * (size_t)j + 1] = make_float4(n[0], n[1], n[2], 0.0f);
+}
+
+// Per query cell: the sorted-grid ranges of its nine neighbouring columns
+// (three cells each), its candidate count and its number of 32-query warps.
+// Keys are (instance 16 | x 16 | y 16 | z 16) bits, coordinates below 65535,
+// so column + z + 2 is the first key past the column's cell z + 1.
+__global__ void k_support_cells(uint32_t cells, const unsigned long long* cell_keys, const uint32_t* cell_queries,
+                                RepairGrid g, uint32_t* range_b, uint32_t* range_e, unsigned long long* list_len,
+                                uint32_t* warps) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= cells) return;
+    const unsigned long long key = cell_keys[u];
+    const int c0 = (int)((key >> 32) & 0xffffu), c1 = (int)((key >> 16) & 0xffffu), c2 = (int)(key & 0xffffu);
+    const unsigned long long inst = (key >> 48) << 48;
+    unsigned long long total = 0;
+    int r = 0;
     for (int dx = -1; dx <= 1; ++dx)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dz = -1; dz <= 1; ++dz) {
-                const int r0 = c[0] + dx, r1 = c[1] + dy, r2 = c[2] + dz;
-                if (r0 < 0 || r1 < 0 || r2 < 0) continue;
-                const unsigned long long key = ((unsigned long long)k << 48) | ((unsigned long long)r0 << 32) |
-                                               ((unsigned long long)r1 << 16) | (unsigned long long)r2;
-                const uint32_t b = lower_bound_key(g.keys, g.n, key);
-                const uint32_t e = lower_bound_key(g.keys, g.n, key + 1);
-                if (b < e) {
-                    r.b[r.n] = b;
-                    r.e[r.n] = e;
-                    r.head[r.n] = g.idx[b];
-                    ++r.n;
-                }
+        for (int dy = -1; dy <= 1; ++dy, ++r) {
+            uint32_t b = 0, e = 0;
+            const int r0 = c0 + dx, r1 = c1 + dy;
+            if (r0 >= 0 && r1 >= 0) {
+                const unsigned long long column = inst + ((unsigned long long)r0 << 32) +
+                                                  ((unsigned long long)r1 << 16);
+                b = lower_bound_key(g.keys, g.n, column + (unsigned long long)max(c2 - 1, 0));
+                e = lower_bound_key(g.keys, g.n, column + (unsigned long long)(c2 + 2));
             }
+            range_b[9 * (size_t)u + r] = b;
+            range_e[9 * (size_t)u + r] = e;
+            total += e - b;
+        }
+    list_len[u] = total;
+    warps[u] = (cell_queries[u] + 31u) / 32u;
 }
 
-struct SupportTerm {
-    const RepairParams& rp;
-    const RepairInst& ri;
-    const RepairSet& ref;
-    const float* q;
-    const float* qn;
-    const float* area;
-
-    __device__ __forceinline__ bool valid(uint32_t j, float* d2_out, float* nc_out, float* t_out) const {
-        const float* p = ref.pos + 3 * j;
-        const float* pn = ref.nrm + 3 * j;
-        const float dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
-        const float d2 = (dx * dx + dy * dy) + dz * dz;
-        const float nc = (pn[0] * qn[0] + pn[1] * qn[1]) + pn[2] * qn[2];
-        *d2_out = d2;
-        *nc_out = nc;
-        *t_out = ((dx * qn[0] + dy * qn[1]) + dz * qn[2]) / ri.plane_sigma;
-        return d2 <= ri.r2 && nc >= kRepairHardCos;
-    }
-    __device__ __forceinline__ float value(uint32_t j, float d2, float nc, float t) const {
-        const float pw = nbd::nan_exp(-0.5f * (t * t));
-        const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
-        const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
-        const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
-        float kw = ((sp * sp) * pw) * soft;
-        kw = kw > rp.eps ? kw : 0.0f;
-        return kw * area[j];
-    }
-};
-
-// The valid terms of the runs in ascending reference index.
-struct TermStream {
-    const SupportTerm& term;
-    const uint32_t* idx;
-    CellRuns& runs;
-
-    __device__ __forceinline__ double next() {
-        for (;;) {
-            if (runs.n == 0) return 0.0;  // not reached: the count pass found every term
-            int best = 0;
-            uint32_t best_j = runs.head[0];
-            for (int t = 1; t < runs.n; ++t)
-                if (runs.head[t] < best_j) {
-                    best_j = runs.head[t];
-                    best = t;
-                }
-            const uint32_t nb = ++runs.b[best];
-            if (nb < runs.e[best]) {
-                runs.head[best] = idx[nb];
-            } else {  // the run is spent: the last one takes its slot
-                const int last = --runs.n;
-                runs.b[best] = runs.b[last];
-                runs.e[best] = runs.e[last];
-                runs.head[best] = runs.head[last];
-            }
-            float d2, nc, tt;
-            if (term.valid(best_j, &d2, &nc, &tt)) return (double)term.value(best_j, d2, nc, tt);
-        }
-    }
-};
-
-// numpy's pairwise sum of n <= 128 terms: eight running sums, combined
-// pairwise, then the remainder in order (fewer than 8: in order).
-__device__ __forceinline__ double pairwise_leaf(uint32_t n, TermStream& s) {
-    if (n < 8u) {
-        double r = 0.0;
-        for (uint32_t i = 0; i < n; ++i) r += s.next();
-        return r;
-    }
-    double r[8];
-    for (int j = 0; j < 8; ++j) r[j] = s.next();
-    uint32_t i = 8;
-    for (; i < n - (n % 8u); i += 8)
-        for (int j = 0; j < 8; ++j) r[j] += s.next();
-    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
-    for (; i < n; ++i) res += s.next();
-    return res;
-}
-
-// numpy's pairwise sum of n <= 8192 streamed terms: above 128 terms the left
-// part holds n/2 rounded down to a multiple of 8. Walked with an explicit
-// stack (at most 8 levels for 8192 terms).
-__device__ double pairwise_streamed(uint32_t n, TermStream& s) {
-    uint32_t len[12];
-    uint8_t stage[12];
-    double left[12];
-    int sp = 0;
-    len[0] = n;
-    stage[0] = 0;
-    for (;;) {
-        const uint32_t L = len[sp];
-        if (L > 128u && stage[sp] == 0 && sp < 11) {
-            uint32_t h = L / 2u;
-            h -= h % 8u;
-            stage[sp] = 1;
-            len[sp + 1] = h;
-            stage[sp + 1] = 0;
-            ++sp;
-            continue;
-        }
-        double v = pairwise_leaf(L, s);
-        for (;;) {
-            if (sp == 0) return v;
-            --sp;
-            if (stage[sp] == 1) {
-                uint32_t h = len[sp] / 2u;
-                h -= h % 8u;
-                left[sp] = v;
-                stage[sp] = 2;
-                len[sp + 1] = len[sp] - h;
-                stage[sp + 1] = 0;
-                ++sp;
-                break;
-            }
-            v = left[sp] + v;
-        }
+// One block per cell of [u0, u1): its candidates as (cell - u0) << 32 |
+// reference index, at its list offset; a key sort then orders each cell's
+// list by reference index.
+__global__ void k_support_fill(uint32_t u0, const uint32_t* range_b, const uint32_t* range_e,
+                               const unsigned long long* list_off, const uint32_t* grid_idx,
+                               unsigned long long* list_keys) {
+    const uint32_t u = u0 + blockIdx.x;
+    unsigned long long at = list_off[u] - list_off[u0];
+    const unsigned long long tag = (unsigned long long)blockIdx.x << 32;
+    for (int r = 0; r < 9; ++r) {
+        const uint32_t b = range_b[9 * (size_t)u + r], e = range_e[9 * (size_t)u + r];
+        for (uint32_t p = b + threadIdx.x; p < e; p += blockDim.x) list_keys[at + (p - b)] = tag | grid_idx[p];
+        at += e - b;
     }
 }
 
-__global__ void k_support(RepairParams rp, RepairSet query, RepairSet ref, RepairGrid ref_grid,
-                          const float* area_weight, const double* flat_support, double max_density, float* support_f,
-                          float* density_m, int* status) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= query.n) return;
-    const uint32_t k = query.inst[i];
+// The cell list's tile at t0 (m <= 32 entries) into this warp's shared tile.
+__device__ __forceinline__ void support_tile(const unsigned long long* list, uint32_t t0, uint32_t m, uint32_t lane,
+                                             const float4* packed, float4 (*tile)[2]) {
+    __syncwarp();
+    if (lane < m) {
+        const size_t j = (uint32_t)list[t0 + lane];
+        tile[lane][0] = packed[2 * j];
+        tile[lane][1] = packed[2 * j + 1];
+    }
+    __syncwarp();
+}
+
+// One warp per (cell, 32 of its queries) of the cells [u0, u1); lane = query.
+__global__ void __launch_bounds__(32 * kSupportWarps)
+    k_support_sum(RepairParams rp, RepairSet query, const float4* packed, uint32_t u0, uint32_t u1,
+                  const uint32_t* warp_off, const unsigned long long* cell_keys, const uint32_t* cell_first,
+                  const uint32_t* cell_queries, const uint32_t* query_order, const unsigned long long* list_off,
+                  const unsigned long long* list_keys, const double* flat_support, double max_density,
+                  float* support_f, float* density_m) {
+    __shared__ float4 tiles[kSupportWarps][32][2];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    const uint32_t item = warp_off[u0] + blockIdx.x * kSupportWarps + w;
+    if (item >= warp_off[u1]) return;  // the whole warp
+    uint32_t lo = u0, hi = u1;         // warp_off[lo] <= item < warp_off[hi]
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (warp_off[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t u = lo, chunk = item - warp_off[u];
+    const bool active = lane < cell_queries[u] - 32u * chunk;
+    const uint32_t qi = active ? query_order[cell_first[u] + 32u * chunk + lane] : 0u;
+    const uint32_t k = (uint32_t)(cell_keys[u] >> 48);
     const RepairInst ri = rp.inst[k];
-    const float* q = query.pos + 3 * i;
-    const float* qn = query.nrm + 3 * i;
-    double support = 0.0;
-    int c[3];
-    if (rep_cell(ri, q, c)) {
-        CellRuns runs;
-        support_runs(ref_grid, k, c, runs);
-        const SupportTerm term{rp, ri, ref, q, qn, area_weight};
-        uint32_t n = 0;
-        for (int t = 0; t < runs.n; ++t)
-            for (uint32_t r = runs.b[t]; r < runs.e[t]; ++r) {
-                float d2, nc, tt;
-                n += term.valid(ref_grid.idx[r], &d2, &nc, &tt) ? 1u : 0u;
+    const float q0 = query.pos[3 * (size_t)qi], q1 = query.pos[3 * (size_t)qi + 1], q2 = query.pos[3 * (size_t)qi + 2];
+    const float n0 = query.nrm[3 * (size_t)qi], n1 = query.nrm[3 * (size_t)qi + 1], n2 = query.nrm[3 * (size_t)qi + 2];
+    const unsigned long long* list = list_keys + (list_off[u] - list_off[u0]);
+    const uint32_t len = (uint32_t)(list_off[u + 1] - list_off[u]);
+    float4(*tile)[2] = tiles[w];
+
+    uint32_t n = 0;
+    for (uint32_t t0 = 0; t0 < len; t0 += 32u) {
+        const uint32_t m = min(32u, len - t0);
+        support_tile(list, t0, m, lane, packed, tile);
+        if (active)
+            for (uint32_t e = 0; e < m; ++e) {
+                const float4 a = tile[e][0], b = tile[e][1];
+                const float dx = a.x - q0, dy = a.y - q1, dz = a.z - q2;
+                const float d2 = (dx * dx + dy * dy) + dz * dz;
+                const float nc = (b.x * n0 + b.y * n1) + b.z * n2;
+                n += (d2 <= ri.r2 && nc >= kRepairHardCos) ? 1u : 0u;
             }
-        TermStream stream{term, ref_grid.idx, runs};
-        for (uint32_t done = 0; done < n; done += kNumpyBuffer)
-            support = support + pairwise_streamed(min(kNumpyBuffer, n - done), stream);
-    } else {
-        atomicOr(status, 2);
     }
+    PairwiseFeed sum;
+    sum.begin(n);
+    for (uint32_t t0 = 0; t0 < len; t0 += 32u) {
+        const uint32_t m = min(32u, len - t0);
+        support_tile(list, t0, m, lane, packed, tile);
+        if (n)
+            for (uint32_t e = 0; e < m; ++e) {
+                const float4 a = tile[e][0], b = tile[e][1];
+                const float dx = a.x - q0, dy = a.y - q1, dz = a.z - q2;
+                const float d2 = (dx * dx + dy * dy) + dz * dz;
+                const float nc = (b.x * n0 + b.y * n1) + b.z * n2;
+                if (d2 <= ri.r2 && nc >= kRepairHardCos) {
+                    const float t = ((dx * n0 + dy * n1) + dz * n2) / ri.plane_sigma;
+                    const float pw = nbd::nan_exp(-0.5f * (t * t));
+                    const float sp = fmaxf(1.0f - d2 / ri.r2, 0.0f);
+                    const float g = fminf(fmaxf((nc - kRepairHardCos) / rp.ncos_span, 0.0f), 1.0f);
+                    const float soft = ((g * g) * (3.0f - 2.0f * g)) * fmaxf(nc, 0.0f);
+                    float kw = ((sp * sp) * pw) * soft;
+                    kw = kw > rp.eps ? kw : 0.0f;
+                    sum.push((double)(kw * a.w));
+                }
+            }
+    }
+    if (!active) return;
     const double flat = flat_support[k];
-    const double v = fmin(fmax(support / fmax(flat, 1e-30), 0.0), 1.0);
-    support_f[i] = (float)v;
-    density_m[i] = (float)fmin(max_density, 1.0 / fmax(v, 1.0 / max_density));
+    const double v = fmin(fmax(sum.total / fmax(flat, 1e-30), 0.0), 1.0);
+    support_f[qi] = (float)v;
+    density_m[qi] = (float)fmin(max_density, 1.0 / fmax(v, 1.0 / max_density));
 }
 
 __global__ void k_rep_deficit(uint32_t n, const uint32_t* counts, uint32_t min_gather, int* deficit) {
@@ -1237,14 +1281,24 @@ int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* 
     };
     RepairInst* inst = (RepairInst*)get(instance_count * sizeof(RepairInst));
     double* flat_dev = (double*)get(instance_count * sizeof(double));
-    int* status = (int*)get(sizeof(int));
-    const uint32_t nmax = std::max(ref_count, 1u);
-    unsigned long long* keys_in = (unsigned long long*)get(nmax * 8ull);
-    uint32_t* idx_in = (uint32_t*)get(nmax * 4ull);
+    // counters: [0] status, [1] query cells
+    int* counters = (int*)get(2 * sizeof(int));
+    const uint32_t nmax = std::max(ref_count, 1u), qmax = std::max(query_count, 1u);
+    unsigned long long* keys_in = (unsigned long long*)get(std::max(nmax, qmax) * 8ull);
+    uint32_t* idx_in = (uint32_t*)get(std::max(nmax, qmax) * 4ull);
     unsigned long long* rkeys = (unsigned long long*)get(nmax * 8ull);
     uint32_t* ridx = (uint32_t*)get(nmax * 4ull);
-    size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_in, rkeys, idx_in, ridx, (int)nmax, 0, 64, st);
+    float4* packed = (float4*)get(nmax * 32ull);
+    unsigned long long* qkeys = (unsigned long long*)get(qmax * 8ull);
+    uint32_t* qorder = (uint32_t*)get(qmax * 4ull);
+    unsigned long long* cell_keys = (unsigned long long*)get(qmax * 8ull);
+    uint32_t* cell_queries = (uint32_t*)get(qmax * 4ull);
+    size_t tmp_bytes = 0, need = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, need, keys_in, rkeys, idx_in, ridx, (int)std::max(nmax, qmax), 0, 64,
+                                    st);
+    tmp_bytes = std::max(tmp_bytes, need);
+    cub::DeviceRunLengthEncode::Encode(nullptr, need, qkeys, cell_keys, cell_queries, counters + 1, (int)qmax, st);
+    tmp_bytes = std::max(tmp_bytes, need);
     void* tmp = get(tmp_bytes);
     if (e != cudaSuccess) {
         release();
@@ -1252,16 +1306,26 @@ int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* 
     }
     cudaMemcpyAsync(inst, host_inst.data(), instance_count * sizeof(RepairInst), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(flat_dev, flat.data(), instance_count * sizeof(double), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(status, 0, sizeof(int), st);
+    cudaMemsetAsync(counters, 0, 2 * sizeof(int), st);
+    int* status = counters;
     for (const RepairSet* set : {&R, &Q})
         if (set->n) k_rep_cmin<<<blocks(set->n, 256), 256, 0, st>>>(*set, inst, instance_count, status);
     if (ref_count) {
         k_rep_keys<<<blocks(ref_count, 256), 256, 0, st>>>(R, inst, instance_count, keys_in, idx_in, status);
         cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, rkeys, idx_in, ridx, (int)ref_count, 0, 64, st);
+        k_support_pack<<<blocks(ref_count, 256), 256, 0, st>>>(R, area_weights, packed);
     }
-    int host_status = 0;
-    cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (query_count) {
+        k_rep_keys<<<blocks(query_count, 256), 256, 0, st>>>(Q, inst, instance_count, keys_in, idx_in, status);
+        cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, qkeys, idx_in, qorder, (int)query_count, 0, 64, st);
+        cub::DeviceRunLengthEncode::Encode(tmp, tmp_bytes, qkeys, cell_keys, cell_queries, counters + 1,
+                                           (int)query_count, st);
+    }
+    ctx->launches += 6;
+    int host_counters[2] = {0, 0};
+    cudaMemcpyAsync(host_counters, counters, sizeof(host_counters), cudaMemcpyDeviceToHost, st);
     e = cudaStreamSynchronize(st);
+    const int host_status = host_counters[0];
     if (e != cudaSuccess || host_status) {
         release();
         if (e != cudaSuccess) return cuda_fail(e, "support grid");
@@ -1270,23 +1334,97 @@ int launch_estimate_support(NanContext* ctx, const float* ref_pos, const float* 
                                     : "positions must be finite");
         return NAN_ERR_INVALID_ARGUMENT;
     }
-    RepairParams rp{inst, instance_count,
-                    (float)(std::max((double)opt->normal_cosine_threshold, hard + 1e-3) - hard), opt->weight_epsilon,
-                    1u};
+    const uint32_t cells = (uint32_t)host_counters[1];
+    if (cells == 0) {
+        release();
+        return NAN_OK;
+    }
+    // per query cell: candidate ranges, list lengths and warps, and their
+    // exclusive sums (cells + 1 entries: the last is the total)
+    uint32_t* range_b = (uint32_t*)get(9ull * cells * 4);
+    uint32_t* range_e = (uint32_t*)get(9ull * cells * 4);
+    unsigned long long* list_len = (unsigned long long*)get((cells + 1ull) * 8);
+    unsigned long long* list_off = (unsigned long long*)get((cells + 1ull) * 8);
+    uint32_t* warps = (uint32_t*)get((cells + 1ull) * 4);
+    uint32_t* warp_off = (uint32_t*)get((cells + 1ull) * 4);
+    uint32_t* cell_first = (uint32_t*)get((cells + 1ull) * 4);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, list_len, list_off, (int)cells + 1, st);
+    scan_bytes = std::max(scan_bytes, need);
+    cub::DeviceScan::ExclusiveSum(nullptr, need, warps, warp_off, (int)cells + 1, st);
+    scan_bytes = std::max(scan_bytes, need);
+    void* scan_tmp = get(scan_bytes);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "support cell scratch");
+    }
     const RepairGrid RG{rkeys, ridx, ref_count};
-    if (query_count)
-        k_support<<<blocks(query_count, 64), 64, 0, st>>>(rp, Q, R, RG, area_weights, flat_dev,
-                                                          std::max(1.0, (double)opt->max_density_multiplier),
-                                                          support_f, density_m, status);
+    cudaMemsetAsync(list_len + cells, 0, 8, st);
+    cudaMemsetAsync(warps + cells, 0, 4, st);
+    k_support_cells<<<blocks(cells, 128), 128, 0, st>>>(cells, cell_keys, cell_queries, RG, range_b, range_e,
+                                                       list_len, warps);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, list_len, list_off, (int)cells + 1, st);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, warps, warp_off, (int)cells + 1, st);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cell_queries, cell_first, (int)cells, st);
     ctx->launches += 4;
-    cudaMemcpyAsync(&host_status, status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    std::vector<unsigned long long> host_off(cells + 1ull);
+    std::vector<uint32_t> host_warp_off(cells + 1ull);
+    cudaMemcpyAsync(host_off.data(), list_off, (cells + 1ull) * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(host_warp_off.data(), warp_off, (cells + 1ull) * 4, cudaMemcpyDeviceToHost, st);
     e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "support cells");
+    }
+    // batches of whole cells of at most kSupportBatch list entries (a single
+    // larger cell is a batch of its own)
+    std::vector<uint32_t> cuts{0};
+    while (cuts.back() < cells) {
+        const uint32_t u0 = cuts.back();
+        uint32_t u1 = u0 + 1;
+        while (u1 < cells && host_off[u1 + 1] - host_off[u0] <= kSupportBatch) ++u1;
+        if (host_off[u1] - host_off[u0] >= (1ull << 31)) {
+            release();
+            set_error("a query cell has 2^31 or more candidate reference points");
+            return NAN_ERR_LIMIT;
+        }
+        cuts.push_back(u1);
+    }
+    unsigned long long widest = 0;
+    for (size_t b = 0; b + 1 < cuts.size(); ++b) widest = std::max(widest, host_off[cuts[b + 1]] - host_off[cuts[b]]);
+    unsigned long long* list_in = (unsigned long long*)get(std::max(widest, 1ull) * 8);
+    unsigned long long* list_sorted = (unsigned long long*)get(std::max(widest, 1ull) * 8);
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, list_in, list_sorted, (int)std::max(widest, 1ull), 0, 64,
+                                   st);
+    void* sort_tmp = get(sort_bytes);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "support list scratch");
+    }
+    const RepairParams rp{inst, instance_count,
+                          (float)(std::max((double)opt->normal_cosine_threshold, hard + 1e-3) - hard),
+                          opt->weight_epsilon, 1u};
+    const double max_density = std::max(1.0, (double)opt->max_density_multiplier);
+    for (size_t b = 0; b + 1 < cuts.size(); ++b) {
+        const uint32_t u0 = cuts[b], u1 = cuts[b + 1];
+        const int count = (int)(host_off[u1] - host_off[u0]);
+        const uint32_t batch_warps = host_warp_off[u1] - host_warp_off[u0];
+        int end_bit = 32;
+        for (uint32_t span = u1 - u0 - 1; span; span >>= 1) ++end_bit;
+        if (count) {
+            k_support_fill<<<u1 - u0, 128, 0, st>>>(u0, range_b, range_e, list_off, ridx, list_in);
+            cub::DeviceRadixSort::SortKeys(sort_tmp, sort_bytes, list_in, list_sorted, count, 0, end_bit, st);
+        }
+        k_support_sum<<<blocks(batch_warps, kSupportWarps), 32 * kSupportWarps, 0, st>>>(
+            rp, Q, packed, u0, u1, warp_off, cell_keys, cell_first, cell_queries, qorder, list_off, list_sorted,
+            flat_dev, max_density, support_f, density_m);
+        ctx->launches += count ? 3 : 1;
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     release();
     if (e != cudaSuccess) return cuda_fail(e, "support estimate");
-    if (host_status & 2) {
-        set_error("an instance spans more than 65535 kernel radii on an axis");
-        return NAN_ERR_INVALID_ARGUMENT;
-    }
     return NAN_OK;
 }
 
