@@ -98,6 +98,15 @@ def _surface_points_group(t, areas, counts, rng, densities=None):
     """_surface_points for the g instances of one mesh at once: t f32[g, T,
     3, 3], areas [g, T], counts[g] points per instance, densities [g, T] or
     None; one random stream for the group. Returns one tuple per instance."""
+    cols = _surface_points_group_flat(t, areas, counts, rng, densities)
+    parts = np.cumsum(np.asarray(counts, dtype=np.int64))[:-1]
+    cols = [np.split(c, parts) for c in cols]
+    return [tuple(c[j] for c in cols) for j in range(areas.shape[0])]
+
+
+def _surface_points_group_flat(t, areas, counts, rng, densities=None):
+    """_surface_points_group's points back to back, instance by instance:
+    (pos, nrm, tri, b1, b2)."""
     g, n = areas.shape
     w = areas if densities is None else areas * np.asarray(densities, dtype=np.float64)
     cdf = np.cumsum(w, axis=1, dtype=np.float64)
@@ -115,10 +124,81 @@ def _surface_points_group(t, areas, counts, rng, densities=None):
     b2 = (su * uv[:, 1]).astype(np.float32)
     tt = t[rows, choice]
     pos = (tt[:, 0] + (tt[:, 1] - tt[:, 0]) * b1[:, None] + (tt[:, 2] - tt[:, 0]) * b2[:, None]).astype(np.float32)
-    parts = np.cumsum(counts)[:-1]
-    cols = (np.split(pos, parts), np.split(_face_normals(tt), parts), np.split(choice.astype(np.uint32), parts),
-            np.split(b1, parts), np.split(b2, parts))
-    return [tuple(c[j] for c in cols) for j in range(g)]
+    return pos, _face_normals(tt), choice.astype(np.uint32), b1, b2
+
+
+class _PointSets:
+    """Surface points of every instance back to back, instance by instance:
+    pos f32[N, 3], nrm f32[N, 3], tri u32[N], b1, b2 f32[N]; instance i's
+    points at starts[i]:starts[i + 1]."""
+
+    __slots__ = ("cols", "starts")
+
+    def __init__(self, cols, counts):
+        self.cols = tuple(cols)
+        self.starts = np.concatenate([[0], np.cumsum(np.asarray(counts, dtype=np.int64))])
+
+    @property
+    def n(self) -> int:
+        return int(self.starts[-1])
+
+    @property
+    def counts(self) -> np.ndarray:
+        return np.diff(self.starts)
+
+    @property
+    def inst(self) -> np.ndarray:
+        return np.repeat(np.arange(self.starts.shape[0] - 1, dtype=np.uint32), self.counts)
+
+    def take(self, idx) -> "_PointSets":
+        """The points at ascending global indices idx."""
+        idx = np.asarray(idx, dtype=np.int64)
+        return _PointSets((c[idx] for c in self.cols), np.diff(np.searchsorted(idx, self.starts)))
+
+    @classmethod
+    def from_groups(cls, groups, n_inst: int) -> "_PointSets":
+        """Point sets from per-mesh-group outputs -- (members, counts per
+        member, columns back to back in member order) -- in instance order."""
+        if not groups:
+            return cls((np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros(0, np.uint32),
+                        np.zeros(0, np.float32), np.zeros(0, np.float32)), np.zeros(n_inst, np.int64))
+        inst = np.concatenate([np.repeat(np.asarray(m, dtype=np.int64), c) for m, c, _ in groups])
+        order = np.argsort(inst, kind="stable")
+        cols = [np.concatenate([g[2][j] for g in groups])[order] for j in range(len(groups[0][2]))]
+        return cls(cols, np.bincount(inst, minlength=n_inst))
+
+    @staticmethod
+    def _dest(sets):
+        """Per set, where its points go when each instance takes its points
+        of every set in turn; and the combined counts."""
+        counts = sum(s.counts for s in sets)
+        starts = np.concatenate([[0], np.cumsum(counts)])
+        before, dests = np.zeros_like(counts), []
+        for s in sets:
+            inst = s.inst
+            dests.append(starts[inst] + before[inst] + (np.arange(s.n) - s.starts[inst]))
+            before = before + s.counts
+        return dests, counts
+
+    @classmethod
+    def interleave(cls, sets) -> "_PointSets":
+        """Per instance, its points of each set in turn (the per-instance
+        concatenation of the sets)."""
+        dests, counts = cls._dest(sets)
+        cols = [np.empty((int(counts.sum()),) + c.shape[1:], c.dtype) for c in sets[0].cols]
+        for s, dest in zip(sets, dests):
+            for o, c in zip(cols, s.cols):
+                o[dest] = c
+        return cls(cols, counts)
+
+    @classmethod
+    def interleave_values(cls, values, sets) -> np.ndarray:
+        """interleave for one per-point array per set."""
+        dests, counts = cls._dest(sets)
+        out = np.empty(int(counts.sum()), np.asarray(values[0]).dtype)
+        for v, dest in zip(values, dests):
+            out[dest] = v
+        return out
 
 
 def _limit_rows(row_sizes, caps, rng):
@@ -141,15 +221,24 @@ def _audit_sources_group(t, mesh, mats, kernels, caps, edge_list, vertex_list, r
     the g instances of one mesh at once (t f32[g, T, 3, 3], mats their
     transforms, kernels and caps per instance); one random stream for the
     group. Returns, per instance, the four point sets as 5-tuples."""
+    g = t.shape[0]
+    out = [[] for _ in range(g)]
+    for counts, cols in _audit_sources_group_flat(t, mesh, mats, kernels, caps, edge_list, vertex_list, rng):
+        bounds = np.concatenate([[0], np.cumsum(counts)])
+        for j in range(g):
+            out[j].append(tuple(c[bounds[j]:bounds[j + 1]] for c in cols))
+    return out
+
+
+def _audit_sources_group_flat(t, mesh, mats, kernels, caps, edge_list, vertex_list, rng):
+    """_audit_sources_group's four point kinds, each as (points per
+    instance, (pos, nrm, tri, b1, b2) back to back in instance order)."""
     g, n_tri = t.shape[0], t.shape[1]
     corners = np.array([[0, 1], [1, 2], [2, 0]])
-    out = [[] for _ in range(g)]
+    out = []
 
     def emit(pos, nrm, tri, b1, b2, row):
-        bounds = np.searchsorted(row, np.arange(g + 1))
-        for j in range(g):
-            sl = slice(bounds[j], bounds[j + 1])
-            out[j].append((pos[sl], nrm[sl], tri[sl], b1[sl], b2[sl]))
+        out.append((np.bincount(row, minlength=g), (pos, nrm, tri, b1, b2)))
 
     # boundary-edge segment midpoints, spacing R / 2 per instance
     face, local = edge_list
@@ -338,13 +427,6 @@ def _instance_areas(scene_node, chunk_triangles: int = 1 << 20):
             tri_counts[part] = idx.shape[0]
     return areas, tri_counts
 
-
-def _take(points, idx):
-    return tuple(x[idx] for x in points)
-
-
-def _concat(sets):
-    return tuple(np.concatenate([s[j] for s in sets]) for j in range(5))
 
 
 @dataclass(frozen=True)
@@ -603,19 +685,30 @@ class SurfaceProbeSiteLayout:
             for j, i in enumerate(members):
                 tris[i], areas[i] = t[j], a[j]
 
+        # each instance's triangles at tri_starts[i] in per-triangle arrays
+        tri_starts = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])]).astype(np.int64)
+
+        def group_rows(values, members):
+            """[g, T] rows of a per-triangle array for the instances of one mesh."""
+            return values[tri_starts[np.asarray(members)][:, None] + np.arange(tris[members[0]].shape[0])]
+
         def sample_by_mesh(per_instance, salt, densities=None):
             """Area (x density) weighted surface points of every instance, the
-            instances of one mesh drawn together from one stream."""
-            out = [None] * n_inst
+            instances of one mesh drawn together from one stream; densities
+            per triangle (all instances' triangles back to back) or None."""
+            per_instance = np.asarray(per_instance, dtype=np.int64)
+            groups = []
             for mesh_id, members in by_mesh.items():
                 t, a = group_geometry[mesh_id]
-                dens = None if densities is None else np.stack([densities[i] for i in members])
+                dens = None if densities is None else group_rows(densities, members)
                 rng = np.random.default_rng([int(seed), int(mesh_id), int(salt)])
-                for i, pts in zip(members, _surface_points_group(t, a, [per_instance[i] for i in members], rng,
-                                                                 dens)):
-                    out[i] = pts
-            return out
-        totals = np.array([a.sum() for a in areas])
+                groups.append((members, per_instance[members],
+                               _surface_points_group_flat(t, a, per_instance[members], rng, dens)))
+            return _PointSets.from_groups(groups, n_inst)
+
+        totals = np.zeros(n_inst)
+        for mesh_id, members in by_mesh.items():
+            totals[members] = group_geometry[mesh_id][1].sum(axis=1)
         density_driven = target_probe_count is None
         if density_driven:
             if adaptive_mass_site_density is None or density_reference_kernel_radius is None:
@@ -640,38 +733,35 @@ class SurfaceProbeSiteLayout:
 
             sampler = SurfaceProbeSampler(device if device is not None else Device(0))
         ncos = math.cos(math.radians(normal_angle_degrees))
-        flat = lambda sets, j: np.concatenate([x[j] for x in sets])
-        inst_of = lambda sets: np.concatenate([np.full(x[0].shape[0], i, np.uint32) for i, x in enumerate(sets)])
-        tri_density = [None] * len(tris)
+        tri_density = None  # per triangle, all instances back to back
         t_pre = time.perf_counter()
         if adaptive_wse:
-            refs, ref_w, queries = [], [], []
-            n_refs = [max(1, min(int(counts[i]) * min(max(1, int(oversample_factor)), 2), 131072))
-                      for i in range(n_inst)]
+            n_refs = np.clip(np.asarray(counts, dtype=np.int64) * min(max(1, int(oversample_factor)), 2), 1, 131072)
             rnds = sample_by_mesh(n_refs, 17)
-            centroid_sets = [None] * n_inst
+            cen_groups, half_area = [], []
             for mesh_id, members in by_mesh.items():
-                t_g, _ = group_geometry[mesh_id]
+                t_g, a_g = group_geometry[mesh_id]
                 cm, cn = _group_centroids(t_g)
-                ids = np.arange(t_g.shape[1], dtype=np.uint32)
-                third = np.full(t_g.shape[1], 1.0 / 3.0, np.float32)
-                for j, i in enumerate(members):
-                    centroid_sets[i] = (cm[j], cn[j], ids, third, third)
-            for i, (t, a) in enumerate(zip(tris, areas)):
-                rnd = rnds[i]
-                cen = centroid_sets[i]
-                refs.append(_concat([rnd, cen]))
-                ref_w.append(np.concatenate([np.full(rnd[0].shape[0], 0.5 * totals[i] / rnd[0].shape[0], np.float32),
-                                             (0.5 * a).astype(np.float32)]))
-                queries.append(cen)
-            _, m = sampler.estimate_support(flat(refs, 0), flat(refs, 1), inst_of(refs), np.concatenate(ref_w),
-                                            flat(queries, 0), flat(queries, 1), inst_of(queries),
-                                            np.full(len(tris), global_kernel, np.float32),
-                                            normal_cosine_threshold=ncos,
-                                            max_density_multiplier=max_density_multiplier)
-            starts = np.concatenate([[0], np.cumsum([t.shape[0] for t in tris])])
-            tri_density = [m[starts[i]:starts[i + 1]] for i in range(len(tris))]
-            masses = np.array([float(np.sum(a * d.astype(np.float64))) for a, d in zip(areas, tri_density)])
+                g, n_tri = a_g.shape
+                third = np.full(g * n_tri, 1.0 / 3.0, np.float32)
+                cen_groups.append((members, np.full(g, n_tri), (cm.reshape(-1, 3), cn.reshape(-1, 3),
+                                                                np.tile(np.arange(n_tri, dtype=np.uint32), g), third,
+                                                                third)))
+                half_area.append((members, np.full(g, n_tri), ((0.5 * a_g).astype(np.float32).reshape(-1),)))
+            cens = _PointSets.from_groups(cen_groups, n_inst)
+            rnd_w = np.repeat((0.5 * totals / np.maximum(rnds.counts, 1)).astype(np.float32), rnds.counts)
+            ref_w = _PointSets.interleave_values([rnd_w, _PointSets.from_groups(half_area, n_inst).cols[0]],
+                                                 [rnds, cens])
+            refs = _PointSets.interleave([rnds, cens])
+            _, tri_density = sampler.estimate_support(refs.cols[0], refs.cols[1], refs.inst, ref_w, cens.cols[0],
+                                                      cens.cols[1], cens.inst,
+                                                      np.full(n_inst, global_kernel, np.float32),
+                                                      normal_cosine_threshold=ncos,
+                                                      max_density_multiplier=max_density_multiplier)
+            masses = np.zeros(n_inst)
+            for mesh_id, members in by_mesh.items():
+                a_g = group_geometry[mesh_id][1]
+                masses[members] = (a_g * group_rows(tri_density, members).astype(np.float64)).sum(axis=1)
             if density_driven:
                 counts = allocate_density_counts(masses, float(adaptive_mass_site_density) * float(density_scale),
                                                  minimum_per_entry=minimum)
@@ -683,26 +773,35 @@ class SurfaceProbeSiteLayout:
                                              minimum_per_entry=minimum)
             target = int(counts.sum())
         t_pre_end = time.perf_counter()
-        cands = sample_by_mesh([int(counts[i]) * max(1, int(oversample_factor)) for i in range(n_inst)], 0,
-                               tri_density if adaptive_wse else None)
-        offsets = np.concatenate([[0], np.cumsum([c[0].shape[0] for c in cands])]).astype(np.int64)
+        counts = np.asarray(counts, dtype=np.int64)
+        cands = sample_by_mesh(counts * max(1, int(oversample_factor)), 0, tri_density if adaptive_wse else None)
+        offsets = cands.starts
         cand_density = None
         if adaptive_wse:
-            cand_density = np.concatenate([
-                (tri_density[i][c[2]] / max(masses[i] / max(totals[i], 1e-30), 1e-6)).astype(np.float32)
-                for i, c in enumerate(cands)])
+            # a candidate's density over its instance's mean density (mass /
+            # area, at least 1e-6: below it the float32 quotient by 1e-6)
+            ratio = masses / np.maximum(totals, 1e-30)
+            inst = cands.inst
+            d = tri_density[tri_starts[inst] + cands.cols[2]]
+            cand_density = (d / np.maximum(ratio, 1e-6)[inst]).astype(np.float32)
+            low = (ratio < 1e-6)[inst]
+            if low.any():
+                cand_density[low] = d[low] / np.float32(1e-6)
         t1 = time.perf_counter()
-        keep, radii = sampler.eliminate(np.concatenate([c[0] for c in cands]), np.concatenate([c[1] for c in cands]),
-                                        offsets, counts, totals, relative_densities=cand_density)
+        keep, radii = sampler.eliminate(cands.cols[0], cands.cols[1], offsets, counts, totals,
+                                        relative_densities=cand_density)
         keep = keep.cpu().numpy().astype(bool)
         t2 = time.perf_counter()
-        sites = [_take(c, np.flatnonzero(keep[offsets[i]:offsets[i + 1]])) for i, c in enumerate(cands)]
-        flags = [np.zeros(x[0].shape[0], np.uint32) for x in sites]
+        base_sel = np.flatnonzero(keep)
+        sites = cands.take(base_sel)
+        flags = np.zeros(sites.n, np.uint32)
         repaired = protected = 0
         budget = int(math.floor(target * float(repair_budget_ratio)))
         # kernel radius per instance, fixed before the repair as the reference does
-        kernels = np.array([max(global_kernel, math.sqrt(totals[i] / max(int(counts[i]), 1)) * kernel_radius_scale,
-                                float(radii[i]) * kernel_radius_scale, 1e-5) for i in range(len(tris))], np.float32)
+        kernels = np.maximum.reduce([np.full(n_inst, global_kernel),
+                                     np.sqrt(totals / np.maximum(counts, 1)) * kernel_radius_scale,
+                                     np.asarray(radii, dtype=np.float64) * kernel_radius_scale,
+                                     np.full(n_inst, 1e-5)]).astype(np.float32)
         stats: dict = {}
         per_repair = per_protected = per_audit = np.zeros(n_inst, np.int64)
         if repair_min_gather > 0:
@@ -712,46 +811,36 @@ class SurfaceProbeSiteLayout:
             # one audit point per cell of R/2 and normal cone, and as repair
             # candidates those that no selected base site or earlier
             # candidate duplicates bit for bit
-            seconds = sample_by_mesh([int(c) for c in counts], 7919)
-            sources = [None] * n_inst
+            seconds = sample_by_mesh(counts, 7919)
+            kinds = [[] for _ in range(4)]  # boundary, inset, centroid, vertices
             for mesh_id, members in by_mesh.items():
                 mesh = scene_node.meshes[mesh_id]
                 mats = np.stack([np.asarray(scene_node.transforms[scene_node.instances[i][2]], dtype=np.float64)
                                  for i in members])
-                parts = _audit_sources_group(group_geometry[mesh_id][0], mesh, mats, kernels[members],
-                                             np.maximum(16, counts[members]), _boundary_edge_list(mesh.indices),
-                                             _vertex_list(mesh),
-                                             np.random.default_rng([int(seed), int(mesh_id), 7919, 1]))
-                for j, i in enumerate(members):
-                    boundary, inset, centroid, vertices = parts[j]
-                    sources[i] = _concat([boundary, inset, centroid, cands[i], seconds[i], vertices])
-            src_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sources])])
-            base_sel = np.concatenate([np.flatnonzero(keep[offsets[i]:offsets[i + 1]]) + offsets[i]
-                                       for i in range(len(cands))])
+                parts = _audit_sources_group_flat(group_geometry[mesh_id][0], mesh, mats, kernels[members],
+                                                  np.maximum(16, counts[members]), _boundary_edge_list(mesh.indices),
+                                                  _vertex_list(mesh),
+                                                  np.random.default_rng([int(seed), int(mesh_id), 7919, 1]))
+                for kind, (c, cols) in zip(kinds, parts):
+                    kind.append((members, c, cols))
+            boundary, inset, centroid, vertices = (_PointSets.from_groups(k, n_inst) for k in kinds)
+            sources = _PointSets.interleave([boundary, inset, centroid, cands, seconds, vertices])
             filt = sampler.filter_audit_repair_candidates(
-                flat(sources, 0), flat(sources, 1), flat(cands, 0), flat(cands, 1), base_sel,
+                sources.cols[0], sources.cols[1], cands.cols[0], cands.cols[1], base_sel,
                 audit_cell_size=(kernels.astype(np.float64) * 0.5), normal_cosine_threshold=ncos,
-                candidate_sets=inst_of(sources), base_sets=inst_of(cands))
-            def split(idx):  # ascending global indices -> per-instance local ones
-                b = np.searchsorted(idx, src_starts)
-                return [idx[b[i]:b[i + 1]] - src_starts[i] for i in range(len(sources))]
-            audits = [_take(sources[i], ix) for i, ix in enumerate(split(filt.audit_indices))]
-            repairs = [_take(sources[i], ix) for i, ix in enumerate(split(filt.repair_indices))]
-            result = sampler.deficit_repair(flat(sites, 0), flat(sites, 1), inst_of(sites), flat(repairs, 0),
-                                            flat(repairs, 1), inst_of(repairs), flat(audits, 0), flat(audits, 1),
-                                            inst_of(audits), kernels, min_gather_count=repair_min_gather,
+                candidate_sets=sources.inst, base_sets=cands.inst)
+            audits = sources.take(filt.audit_indices)
+            repairs = sources.take(filt.repair_indices)
+            result = sampler.deficit_repair(sites.cols[0], sites.cols[1], sites.inst, repairs.cols[0],
+                                            repairs.cols[1], repairs.inst, audits.cols[0], audits.cols[1],
+                                            audits.inst, kernels, min_gather_count=repair_min_gather,
                                             max_repair_count=budget, normal_cosine_threshold=ncos)
-            chosen = np.sort(result.selected_candidate_indices)
-            repair_inst = inst_of(repairs)[chosen]
-            repair_starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in repairs])])
-            rb = np.searchsorted(repair_inst, np.arange(n_inst + 1))  # chosen is sorted, so by instance
-            per_repair = np.diff(rb)
-            per_audit = np.array([x[0].shape[0] for x in audits], np.int64)
-            for i in np.flatnonzero(np.diff(rb)):
-                local = chosen[rb[i]:rb[i + 1]] - repair_starts[i]
-                sites[i] = _concat([sites[i], _take(repairs[i], local)])
-                flags[i] = np.concatenate([flags[i], np.zeros(local.shape[0], np.uint32)])
-            repaired = int(chosen.shape[0])
+            chosen = repairs.take(np.sort(result.selected_candidate_indices))
+            per_repair = chosen.counts
+            per_audit = audits.counts
+            flags = _PointSets.interleave_values([flags, np.zeros(chosen.n, np.uint32)], [sites, chosen])
+            sites = _PointSets.interleave([sites, chosen])
+            repaired = chosen.n
             # protected closure (surface_probes.py:2462-2587): every audit point
             # still short of the gather target offers its residual deficit as
             # colocated candidates, chosen without a budget
@@ -759,24 +848,23 @@ class SurfaceProbeSiteLayout:
             short = np.flatnonzero(deficits)
             closure_after = result.counts_after.copy()
             if short.size:
-                audit_inst = inst_of(audits)
+                audit_inst = audits.inst
                 offers = np.repeat(short, deficits[short])
-                prot = tuple(np.concatenate([x[j] for x in audits])[offers] for j in range(5))
+                prot = tuple(c[offers] for c in audits.cols)
                 prot_inst = audit_inst[offers]
                 closure = sampler.deficit_repair(
-                    flat(sites, 0), flat(sites, 1), inst_of(sites), prot[0], prot[1], prot_inst,
-                    flat(audits, 0)[short], flat(audits, 1)[short], audit_inst[short], kernels,
+                    sites.cols[0], sites.cols[1], sites.inst, prot[0], prot[1], prot_inst,
+                    audits.cols[0][short], audits.cols[1][short], audit_inst[short], kernels,
                     min_gather_count=repair_min_gather, max_repair_count=int(offers.shape[0]),
                     normal_cosine_threshold=ncos)
                 picked = np.sort(closure.selected_candidate_indices)
-                pb = np.searchsorted(prot_inst[picked], np.arange(n_inst + 1))  # offers follow the instances
-                per_protected = np.diff(pb)
-                for i in np.flatnonzero(np.diff(pb)):
-                    local = picked[pb[i]:pb[i + 1]]
-                    sites[i] = _concat([sites[i], tuple(x[local] for x in prot)])
-                    flags[i] = np.concatenate([flags[i], np.full(local.shape[0], SURFACE_PROBE_FLAG_PROTECTED,
-                                                                 np.uint32)])
-                protected = int(picked.shape[0])
+                # offers follow the instances, so the picked ones do too
+                taken = _PointSets((c[picked] for c in prot), np.bincount(prot_inst[picked], minlength=n_inst))
+                per_protected = taken.counts
+                flags = _PointSets.interleave_values(
+                    [flags, np.full(taken.n, SURFACE_PROBE_FLAG_PROTECTED, np.uint32)], [sites, taken])
+                sites = _PointSets.interleave([sites, taken])
+                protected = taken.n
                 closure_after[short] = closure.counts_after
             stats.update(total_audit_point_count=int(result.counts_before.shape[0]),
                          zero_gather_before=int((result.counts_before == 0).sum()),
@@ -800,31 +888,37 @@ class SurfaceProbeSiteLayout:
         # support f of every site against the candidate population: area /
         # candidates each, or, for density-drawn candidates, area x
         # (1 / density) normalised to the instance area
-        ref_area = []
-        for i, c in enumerate(cands):
-            if adaptive_wse:
-                w = 1.0 / np.maximum(tri_density[i][c[2]].astype(np.float64), 1e-12)
-                ref_area.append((w * (totals[i] / max(float(w.sum()), 1e-30))).astype(np.float32))
-            else:
-                ref_area.append(np.full(c[0].shape[0], totals[i] / max(c[0].shape[0], 1), np.float32))
-        support, density = sampler.estimate_support(flat(cands, 0), flat(cands, 1), inst_of(cands),
-                                                    np.concatenate(ref_area), flat(sites, 0), flat(sites, 1),
-                                                    inst_of(sites), kernels, normal_cosine_threshold=ncos,
+        cand_inst = cands.inst
+        if adaptive_wse:
+            w = 1.0 / np.maximum(tri_density[tri_starts[cand_inst] + cands.cols[2]].astype(np.float64), 1e-12)
+            # each instance's sum as numpy forms it for the instance alone
+            w_sum = np.array([w[b:e].sum() for b, e in zip(offsets[:-1].tolist(), offsets[1:].tolist())])
+            ref_area = (w * (totals / np.maximum(w_sum, 1e-30))[cand_inst]).astype(np.float32)
+        else:
+            ref_area = np.repeat((totals / np.maximum(cands.counts, 1)).astype(np.float32), cands.counts)
+        support, density = sampler.estimate_support(cands.cols[0], cands.cols[1], cand_inst, ref_area,
+                                                    sites.cols[0], sites.cols[1], sites.inst, kernels,
+                                                    normal_cosine_threshold=ncos,
                                                     max_density_multiplier=max_density_multiplier)
-        starts = np.concatenate([[0], np.cumsum([x[0].shape[0] for x in sites])])
         t4 = time.perf_counter()
-        records = []
-        for i, (pos, nrm, tri, b1, b2) in enumerate(sites):
-            for side in range(2 if double_sided[i] else 1):
-                r = np.zeros(pos.shape[0], dtype=SURFACE_PROBE_DTYPE)
-                r["position_radius"][:, :3] = pos
-                r["normal_side"][:, :3] = nrm * (-1.0 if side else 1.0)
-                r["normal_side"][:, 3] = support[starts[i]:starts[i + 1]]
-                r["meta"][:, 0] = tri
-                r["meta"][:, 1] = b1.view(np.uint32)
-                r["meta"][:, 2] = b2.view(np.uint32)
-                r["meta"][:, 3] = (1 if side else 0) | flags[i] | (i << SURFACE_PROBE_INSTANCE_SHIFT)
-                records.append(r)
+        # records per instance: its sites' fronts, then their backs when double-sided
+        site_inst = sites.inst
+        sides = 1 + np.asarray(double_sided, dtype=np.int64)
+        rec_starts = np.concatenate([[0], np.cumsum(sites.counts * sides)])
+        local = np.arange(sites.n) - sites.starts[site_inst]
+        records = np.zeros(int(rec_starts[-1]), dtype=SURFACE_PROBE_DTYPE)
+        inst_bits = site_inst.astype(np.uint32) << np.uint32(SURFACE_PROBE_INSTANCE_SHIFT)
+        back = sides[site_inst] == 2
+        for side, sel, dest in ((0, slice(None), rec_starts[site_inst] + local),
+                                (1, back, (rec_starts[site_inst] + sites.counts[site_inst] + local)[back])):
+            pos, nrm, tri, b1, b2 = (c[sel] for c in sites.cols)
+            records["position_radius"][dest, :3] = pos
+            records["normal_side"][dest, :3] = nrm * np.float32(-1.0) if side else nrm
+            records["normal_side"][dest, 3] = support[sel]
+            records["meta"][dest, 0] = tri
+            records["meta"][dest, 1] = b1.view(np.uint32)
+            records["meta"][dest, 2] = b2.view(np.uint32)
+            records["meta"][dest, 3] = np.uint32(side) | flags[sel] | inst_bits[sel]
         anchors = None
         if build_vertex_anchors:
             anchors = []
@@ -847,22 +941,22 @@ class SurfaceProbeSiteLayout:
                                        | (i << SURFACE_PROBE_INSTANCE_SHIFT))
                     recs.append(r)
                 anchors.append((np.concatenate(recs), lookup[mesh.indices.astype(np.int64)], pos.shape[0]))
-        layout = cls.from_sites(scene_node, np.concatenate(records), kernel_radii=kernels,
+        n_anchor_sites = sum(int(a[2]) for a in anchors) if anchors else 0
+        zeros = np.zeros(n_inst, np.int64)
+        instance_stats = dict(
+            base_surface_site_count=counts, repair_surface_site_count=per_repair,
+            protected_surface_site_count=per_protected, candidate_count=cands.counts, audit_point_count=per_audit,
+            vertex_anchor_site_count=np.array([a[2] for a in anchors], np.int64) if anchors else zeros,
+            vertex_anchor_probe_count=np.array([a[0].shape[0] for a in anchors], np.int64) if anchors else zeros)
+        layout = cls.from_sites(scene_node, records, kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees,
                                 max_density_multiplier=max_density_multiplier, vertex_anchors=anchors,
-                                sampler=sampler, **kwargs)
-        n_anchor_sites = sum(int(a[2]) for a in anchors) if anchors else 0
-        infos = tuple(dataclasses.replace(
-            info, base_surface_site_count=int(counts[i]), repair_surface_site_count=int(per_repair[i]),
-            protected_surface_site_count=int(per_protected[i]), candidate_count=int(cands[i][0].shape[0]),
-            audit_point_count=int(per_audit[i]), vertex_anchor_site_count=int(anchors[i][2]) if anchors else 0,
-            vertex_anchor_probe_count=int(anchors[i][0].shape[0]) if anchors else 0)
-            for i, info in enumerate(layout.instance_infos))
+                                sampler=sampler, instance_stats=instance_stats, **kwargs)
         layout = dataclasses.replace(
-            layout, instance_infos=infos, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
+            layout, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
             total_repair_surface_site_count=repaired, total_protected_surface_site_count=protected,
             repair_surface_site_budget=budget if repair_min_gather > 0 else 0,
-            total_surface_site_count=int(sum(x[0].shape[0] for x in sites)), total_candidate_count=int(offsets[-1]),
+            total_surface_site_count=sites.n, total_candidate_count=int(offsets[-1]),
             support_f_p10=float(np.percentile(support, 10)) if support.size else 0.0,
             support_f_p50=float(np.median(support)) if support.size else 0.0,
             density_m_p95=float(np.percentile(density, 95)) if density.size else 0.0,
