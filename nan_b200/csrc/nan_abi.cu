@@ -48,6 +48,22 @@ cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
     return cudaMallocFromPoolAsync(p, bytes, pool, st);
 }
 
+cudaError_t replace_context_scratch(NanContext* ctx, size_t bytes) {
+    if (ctx->scratch) cudaFreeAsync(ctx->scratch, 0);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    if (bytes == 0) return cudaStreamSynchronize(0);
+    cudaError_t err = scratch_alloc(&ctx->scratch, bytes, 0);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(0);  // usable from every stream once this returns
+    if (err != cudaSuccess) {
+        if (ctx->scratch) cudaFreeAsync(ctx->scratch, 0);
+        ctx->scratch = nullptr;
+        return err;
+    }
+    ctx->scratch_bytes = bytes;
+    return cudaSuccess;
+}
+
 void trim_scratch(int device) {
     std::lock_guard<std::mutex> lock(g_pool_mutex);
     if (device >= 0 && device < 128 && g_pools[device]) cudaMemPoolTrimTo(g_pools[device], 0);
@@ -153,7 +169,7 @@ NAN_B200_API int nan_ctx_destroy(NanContext* ctx) {
     cudaDeviceSynchronize();
     nan_host::free_scene(ctx);
     nan_host::release_timing(ctx);
-    cudaFree(ctx->scratch);
+    nan_host::replace_context_scratch(ctx, 0);
     cudaFree(ctx->d_status);
     cudaFree(ctx->d_counters);
     nan_host::trim_scratch(ctx->device);
@@ -217,15 +233,8 @@ NAN_B200_API int nan_ctx_reserve(NanContext* ctx, uint64_t scratch_bytes) {
     if (scratch_bytes <= ctx->scratch_bytes) return NAN_OK;
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) return cuda_fail(err, "reserve (synchronize)");
-    cudaFree(ctx->scratch);
-    ctx->scratch = nullptr;
-    ctx->scratch_bytes = 0;
-    err = cudaMalloc(&ctx->scratch, scratch_bytes);
-    if (err != cudaSuccess) {
-        ctx->scratch = nullptr;
-        return cuda_fail(err, "reserve wavefront scratch");
-    }
-    ctx->scratch_bytes = scratch_bytes;
+    err = nan_host::replace_context_scratch(ctx, scratch_bytes);
+    if (err != cudaSuccess) return cuda_fail(err, "reserve wavefront scratch");
     return NAN_OK;
 }
 

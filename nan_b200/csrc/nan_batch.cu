@@ -366,13 +366,7 @@ int batch_set_mode(NanBatch* b, uint32_t mode) {
             err = cudaMalloc(&m->samples, nan_host::probe_sample_bytes() * paths);
             if (err == cudaSuccess) m->sample_paths = paths;
         }
-        if (err == cudaSuccess && ctx->scratch_bytes < need) {
-            cudaFree(ctx->scratch);
-            ctx->scratch = nullptr;
-            ctx->scratch_bytes = 0;
-            err = cudaMalloc(&ctx->scratch, need);
-            if (err == cudaSuccess) ctx->scratch_bytes = need;
-        }
+        if (err == cudaSuccess && ctx->scratch_bytes < need) err = nan_host::replace_context_scratch(ctx, need);
         if (err != cudaSuccess) return cuda_fail(err, "batch wavefront scratch");
         b->mode = mode;
         int occ = 0;

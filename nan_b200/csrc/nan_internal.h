@@ -97,6 +97,10 @@ void set_error(const std::string& msg);
 // trim_scratch, which nan_ctx_destroy calls).
 cudaError_t scratch_alloc(void** p, size_t bytes, cudaStream_t stream);
 void trim_scratch(int device);
+// The context's wavefront scratch replaced by `bytes` from the pool (0:
+// released). The caller has synchronised the device: nothing still uses
+// the old scratch.
+cudaError_t replace_context_scratch(NanContext* ctx, size_t bytes);
 int cuda_fail(cudaError_t err, const char* what);
 
 // A lighting record the kernels can read: a sky-view LUT needs a size and a

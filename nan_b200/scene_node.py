@@ -191,15 +191,18 @@ class SceneNode:
             v_off += m.vertex_count
             i_off += m.index_count
         instance_descs = np.zeros((len(self.instances), 4), dtype=np.uint32)
-        for k, (mesh_id, material_id, transform_id) in enumerate(self.instances):
-            m = self.transforms[transform_id].astype(np.float64)
-            det = np.dot(np.cross(m[0, :3], m[1, :3]), m[2, :3])
-            flags = INSTANCE_FLAG_ODD_NEGATIVE_TRANSFORM if det <= 0 else 0
-            instance_descs[k] = (mesh_id, material_id, transform_id, flags)
-        transforms = np.stack(self.transforms).astype(np.float32).reshape(-1, 16)
-        inverse_transposes = np.stack(
-            [np.linalg.inv(t.astype(np.float64)).T.astype(np.float32) for t in self.transforms]
-        ).reshape(-1, 16)
+        stacked = np.stack(self.transforms).astype(np.float64).reshape(-1, 4, 4)
+        if self.instances:
+            ids = np.asarray(self.instances, dtype=np.int64).reshape(-1, 3)
+            m = stacked[ids[:, 2], :3, :3]
+            det = (np.cross(m[:, 0], m[:, 1]) * m[:, 2]).sum(axis=1)
+            # the sign decides; near zero it is taken as np.dot forms it
+            for k in np.flatnonzero(np.abs(det) <= 1e-9):
+                det[k] = np.dot(np.cross(m[k, 0], m[k, 1]), m[k, 2])
+            instance_descs[:, :3] = ids
+            instance_descs[:, 3] = np.where(det <= 0, INSTANCE_FLAG_ODD_NEGATIVE_TRANSFORM, 0)
+        transforms = stacked.astype(np.float32).reshape(-1, 16)
+        inverse_transposes = np.linalg.inv(stacked).transpose(0, 2, 1).astype(np.float32).reshape(-1, 16)
         materials = np.stack([m.pack() for m in self.materials]).astype(np.float32)
         return {
             "vertices": np.ascontiguousarray(vertices, dtype=np.float32),

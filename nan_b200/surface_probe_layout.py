@@ -499,9 +499,11 @@ class SurfaceProbeSiteLayout:
                    kernel_radius_scale: float = 2.5, normal_angle_degrees: float = 45.0,
                    max_density_multiplier: float = 8.0, poisson_radii=None,
                    kernel_radii=None, vertex_anchors=None, sampler=None,
-                   instance_stats=None) -> "SurfaceProbeSiteLayout":
+                   instance_stats=None, instance_areas=None) -> "SurfaceProbeSiteLayout":
         """instance_stats (optional): further SurfaceProbeSiteInstance fields
         as {name: one value per instance}, e.g. a site builder's counts.
+        instance_areas (optional): each instance's surface area when the
+        caller has it already (else from the scene's transformed triangles).
 
         vertex_anchors (optional, per instance None or (records, map,
         anchor site count)): anchor probe records (fronts, then backs for a
@@ -517,7 +519,12 @@ class SurfaceProbeSiteLayout:
         n_inst = len(scene_node.instances)
         if probes.shape[0] and int(instance_of.max()) >= n_inst:
             raise ValueError("a probe names an instance the scene does not have")
-        areas, tri_counts = _instance_areas(scene_node)
+        if instance_areas is None:
+            areas, tri_counts = _instance_areas(scene_node)
+        else:
+            areas = np.asarray(instance_areas, dtype=np.float64).reshape(-1)
+            mesh_tris = [m.indices.reshape(-1, 3).shape[0] for m in scene_node.meshes]
+            tri_counts = np.array([mesh_tris[mesh_id] for mesh_id, _, _ in scene_node.instances], np.int64)
         fronts = np.bincount(instance_of[(probes["meta"][:, 3] & 1) == 0], minlength=n_inst)
         total_sites = max(int(fronts.sum()), 1)
         global_kernel = max(math.sqrt(max(float(areas.sum()), 1e-20) / total_sites) * kernel_radius_scale, 1e-5)
@@ -951,7 +958,7 @@ class SurfaceProbeSiteLayout:
         layout = cls.from_sites(scene_node, records, kernel_radii=kernels,
                                 normal_angle_degrees=normal_angle_degrees,
                                 max_density_multiplier=max_density_multiplier, vertex_anchors=anchors,
-                                sampler=sampler, instance_stats=instance_stats, **kwargs)
+                                sampler=sampler, instance_stats=instance_stats, instance_areas=totals, **kwargs)
         layout = dataclasses.replace(
             layout, target_surface_site_count=target, total_base_surface_site_count=int(sum(counts)),
             total_repair_surface_site_count=repaired, total_protected_surface_site_count=protected,
