@@ -104,9 +104,10 @@ def _surface_points_group(t, areas, counts, rng, densities=None):
     return [tuple(c[j] for c in cols) for j in range(areas.shape[0])]
 
 
-def _surface_points_group_flat(t, areas, counts, rng, densities=None):
+def _surface_points_group_flat(t, areas, counts, rng, densities=None, normals=None):
     """_surface_points_group's points back to back, instance by instance:
-    (pos, nrm, tri, b1, b2)."""
+    (pos, nrm, tri, b1, b2). normals: the triangles' _face_normals [g, T, 3]
+    when already known."""
     g, n = areas.shape
     w = areas if densities is None else areas * np.asarray(densities, dtype=np.float64)
     cdf = np.cumsum(w, axis=1, dtype=np.float64)
@@ -124,7 +125,8 @@ def _surface_points_group_flat(t, areas, counts, rng, densities=None):
     b2 = (su * uv[:, 1]).astype(np.float32)
     tt = t[rows, choice]
     pos = (tt[:, 0] + (tt[:, 1] - tt[:, 0]) * b1[:, None] + (tt[:, 2] - tt[:, 0]) * b2[:, None]).astype(np.float32)
-    return pos, _face_normals(tt), choice.astype(np.uint32), b1, b2
+    nrm = _face_normals(tt) if normals is None else normals[rows, choice]
+    return pos, nrm, choice.astype(np.uint32), b1, b2
 
 
 class _PointSets:
@@ -162,10 +164,15 @@ class _PointSets:
         if not groups:
             return cls((np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros(0, np.uint32),
                         np.zeros(0, np.float32), np.zeros(0, np.float32)), np.zeros(n_inst, np.int64))
-        inst = np.concatenate([np.repeat(np.asarray(m, dtype=np.int64), c) for m, c, _ in groups])
-        order = np.argsort(inst, kind="stable")
-        cols = [np.concatenate([g[2][j] for g in groups])[order] for j in range(len(groups[0][2]))]
-        return cls(cols, np.bincount(inst, minlength=n_inst))
+        members = np.concatenate([np.asarray(m, dtype=np.int64) for m, _, _ in groups])
+        member_counts = np.concatenate([np.asarray(c, dtype=np.int64) for _, c, _ in groups])
+        counts = np.bincount(members, member_counts, minlength=n_inst).astype(np.int64)
+        cols = [np.concatenate([g[2][j] for g in groups]) if len(groups) > 1 else g0
+                for j, g0 in enumerate(groups[0][2])]
+        if np.any(np.diff(members) < 0):  # the groups interleave instances: put the points in instance order
+            order = np.argsort(np.repeat(members, member_counts), kind="stable")
+            cols = [c[order] for c in cols]
+        return cls(cols, counts)
 
     @staticmethod
     def _dest(sets):
@@ -677,6 +684,7 @@ class SurfaceProbeSiteLayout:
         double_sided = [bool(scene_node.materials[mat_id].double_sided) for _, mat_id, _ in scene_node.instances]
         by_mesh: dict = {}
         group_geometry: dict = {}
+        group_normals: dict = {}
         for i, (mesh_id, _, _) in enumerate(scene_node.instances):
             by_mesh.setdefault(mesh_id, []).append(i)
         for mesh_id, members in by_mesh.items():
@@ -687,7 +695,10 @@ class SurfaceProbeSiteLayout:
                 mats[:, None, :3, 3]
             t = p[:, mesh.indices.astype(np.int64)].astype(np.float32)  # [g, T, 3, 3]
             e = np.cross(t[:, :, 1] - t[:, :, 0], t[:, :, 2] - t[:, :, 0]).astype(np.float64)
-            a = 0.5 * np.linalg.norm(e, axis=2)
+            norm_e = np.linalg.norm(e, axis=2)
+            a = 0.5 * norm_e
+            # face normals as _face_normals forms them, kept for every sampled point
+            group_normals[mesh_id] = (e / np.maximum(norm_e[..., None], 1e-30)).astype(np.float32)
             group_geometry[mesh_id] = (t, a)
             for j, i in enumerate(members):
                 tris[i], areas[i] = t[j], a[j]
@@ -710,7 +721,8 @@ class SurfaceProbeSiteLayout:
                 dens = None if densities is None else group_rows(densities, members)
                 rng = np.random.default_rng([int(seed), int(mesh_id), int(salt)])
                 groups.append((members, per_instance[members],
-                               _surface_points_group_flat(t, a, per_instance[members], rng, dens)))
+                               _surface_points_group_flat(t, a, per_instance[members], rng, dens,
+                                                          normals=group_normals[mesh_id])))
             return _PointSets.from_groups(groups, n_inst)
 
         totals = np.zeros(n_inst)
@@ -748,7 +760,7 @@ class SurfaceProbeSiteLayout:
             cen_groups, half_area = [], []
             for mesh_id, members in by_mesh.items():
                 t_g, a_g = group_geometry[mesh_id]
-                cm, cn = _group_centroids(t_g)
+                cm, cn = t_g.mean(axis=2, dtype=np.float32), group_normals[mesh_id]  # as _group_centroids
                 g, n_tri = a_g.shape
                 third = np.full(g * n_tri, 1.0 / 3.0, np.float32)
                 cen_groups.append((members, np.full(g, n_tri), (cm.reshape(-1, 3), cn.reshape(-1, 3),
