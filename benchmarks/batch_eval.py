@@ -12,6 +12,9 @@ counted on the device.
 
 from __future__ import annotations
 
+import concurrent.futures
+import os
+import threading
 import time
 
 
@@ -47,27 +50,41 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
     scene_nodes = list(sc.batch_scenes(count, seed, tri_max=tri_max))
     generation_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    items, tris, sites = [], [], []
-    sampler = SurfaceProbeSampler(device)
     placement = {"candidates": 0, "base_sites": 0, "repair_sites": 0, "protected_sites": 0, "density_prepass_s": 0.0,
                  "candidates_s": 0.0, "elimination_s": 0.0, "repair_s": 0.0, "support_s": 0.0, "packing_s": 0.0}
-    for i, (node, n_sites) in enumerate(scene_nodes):
+    # The scenes are independent and each placement is seeded per scene, so
+    # they are set up by a few worker threads (one sampler context each): the
+    # host's numpy work and the library's GPU calls release the GIL and
+    # overlap. The results do not depend on the number of workers.
+    workers = max(1, min(8, (os.cpu_count() or 1) // 2))
+    local = threading.local()
+
+    def set_up(i):
+        node, n_sites = scene_nodes[i]
+        if not hasattr(local, "sampler"):
+            local.sampler = SurfaceProbeSampler(device)
         scene = Scene(device, node)
         prof: dict = {}
         # the config's sites: the adaptive elimination's output at the scene's
         # target, without repair or closure sites
-        layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=sampler, seed=seed + i, repair_min_gather=0,
-                                                  profile=prof)
-        for k in placement:
-            placement[k] += prof.get(k, 0)
+        layout = SurfaceProbeSiteLayout.build_wse(node, n_sites, sampler=local.sampler, seed=seed + i,
+                                                  repair_min_gather=0, profile=prof)
         geometry = SurfaceProbeGpuGeometry.create(device, layout)
         baker = SurfaceProbeDiffuseIrradianceBaker(device, scene, geometry, samples_per_probe=samples_per_probe,
                                                    max_bounces=max_bounces, compensated=True)
         rt = SurfaceProbeRuntimeBuffers.acquire(RenderData(device), geometry.probe_count)
-        items.append((scene, baker, rt.field, rt.attachments))
-        tris.append(scene.triangle_count)
-        sites.append(int(geometry.probe_count))
+        return (scene, baker, rt.field, rt.attachments), prof, int(geometry.probe_count)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
+        done = list(pool.map(set_up, range(len(scene_nodes))))
+    torch.cuda.synchronize()
     setup_s = time.perf_counter() - t0
+    items = [d[0] for d in done]
+    for _, prof, _ in done:
+        for k in placement:
+            placement[k] += prof.get(k, 0)
+    tris = [item[0].triangle_count for item in items]
+    sites = [d[2] for d in done]
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
@@ -140,7 +157,7 @@ def measure(device, count: int = 64, seed: int = 1, samples_per_probe: int = 64,
         "scenes": count, "triangles_total": int(sum(tris)), "triangles_min": int(min(tris)),
         "triangles_max": int(max(tris)), "sites_total": int(sum(sites)), "sites_min": int(min(sites)),
         "sites_max": int(max(sites)), "samples_per_probe": samples_per_probe, "max_bounces": max_bounces,
-        "scene_generation_s": generation_s, "setup_s": setup_s, "site_placement": dict(placement, method="the reference's adaptive weighted sample "
+        "scene_generation_s": generation_s, "setup_s": setup_s, "setup_workers": workers, "site_placement": dict(placement, method="the reference's adaptive weighted sample "
                                                                    "elimination on the GPU (density prepass, 5x "
                                                                    "oversampled candidates), no repair sites"),
         "autotune": tuned, "autotune_independent_samples": tuned_ind, "autotune_wavefront": tuned_wf,
