@@ -210,7 +210,9 @@ typedef struct NanTuning {
     uint32_t traversal;            /* wavefront traversal over binary nodes, same results in every
                                       form: 0 = a warp takes 32 rays and walks until all have ended;
                                       1-4 = idle lanes are refilled from the queue;
-                                      5 = stack top in shared memory */
+                                      5 = stack top in shared memory;
+                                      6 = speculative while-while walk (a lane parks its
+                                      first leaf until every lane holds one) */
 } NanTuning;
 
 /* Device time of the wavefront stages since the last reset, from CUDA events

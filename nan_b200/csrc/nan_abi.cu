@@ -257,7 +257,7 @@ NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
         return invalid("bvh_width must be 0 or 2 (binary) or 8 (compressed wide)");
     if (tuning->kernel_timing > 1) return invalid("kernel_timing must be 0 or 1");
     if (tuning->ray_order > 1) return invalid("ray_order must be 0 (path order) or 1 (by direction octant)");
-    if (tuning->traversal > 5) return invalid("traversal must be 0..5");
+    if (tuning->traversal > 6) return invalid("traversal must be 0..6");
     ctx->tuning = *tuning;
     return NAN_OK;
 }

@@ -482,6 +482,158 @@ __device__ __forceinline__ bool trace_any_binary(const SceneView& s, f3 o, f3 d,
 }
 
 // ---------------------------------------------------------------------------
+// Speculative while-while walks (after Aila and Laine, "Understanding the
+// efficiency of ray traversal on GPUs", HPG 2009). A lane that reaches a leaf
+// parks it and keeps descending; once every lane still descending holds a
+// parked leaf, the lanes test their leaves together. Leaf tests then run
+// with more lanes active, at the price of some speculative node visits. The
+// closest hit does not depend on the visit order (the (t, flat) tie-break),
+// and an any-hit query answers the same either way.
+// kWalkDone marks an ended walk: a leaf is ~(first << 3 | last - first)
+// with at most 8 triangles, so no leaf encodes to it.
+// ---------------------------------------------------------------------------
+constexpr int kWalkDone = -2147483647 - 1;
+
+template <int kDepth>
+__device__ __forceinline__ int spec_pop(const int* stack, int& sp) {
+    return sp ? stack[--sp] : kWalkDone;
+}
+
+// One interior node of a binary walk: the next node (near child, the other
+// hit child, or a popped entry), pushing the far child when both are hit.
+template <int kDepth>
+__device__ __forceinline__ int spec_interior(const SceneView& s, const BoxRay& br, int node, float tmin, float tmax,
+                                             int* stack, int& sp) {
+    const float4* n = s.nodes + 4 * node;
+    const float4 na = __ldg(n), nb = __ldg(n + 1), nc = __ldg(n + 2);
+    const int4 nd = __ldg(reinterpret_cast<const int4*>(n + 3));
+    float t0, t1;
+    bool h0, h1;
+    box2(br, na, nb, nc, tmin, tmax, &t0, &t1, &h0, &h1);
+    if (h0 && h1) {
+        int near_child = nd.x, far_child = nd.y;
+        if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
+        if (sp < kDepth) stack[sp++] = far_child;
+        else atomicOr(s.status, kStatusStackOverflow);
+        return near_child;
+    }
+    if (h0) return nd.x;
+    if (h1) return nd.y;
+    return spec_pop<kDepth>(stack, sp);
+}
+
+template <int kDepth = kTraversalStack>
+__device__ __forceinline__ HitInfo trace_closest_binary_spec(const SceneView& s, f3 o, f3 d, float tmin,
+                                                             float tmax) {
+    HitInfo hit;
+    hit.valid = false;
+    hit.flat = 0xffffffffu;
+    hit.t = tmax;
+    hit.b1 = 0.0f;
+    hit.b2 = 0.0f;
+    if (s.tri_count == 0) return hit;
+    const WtRay wr = wt_setup(d);
+    const BoxRay br = box_setup(o, d);
+    int stack[kDepth];
+    int sp = 0;
+    int node = s.root;
+    int leaf = 0;  // the parked leaf (< 0), or 0
+    float best_t = tmax;
+    uint32_t best_key = 0xffffffffu;
+    int best_tri = -1;
+    while (node != kWalkDone) {
+        while (node >= 0) {
+            node = spec_interior<kDepth>(s, br, node, tmin, best_t, stack, sp);
+            if (node < 0 && node != kWalkDone && leaf == 0) {
+                leaf = node;
+                node = spec_pop<kDepth>(stack, sp);
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;
+        }
+        if (leaf == 0 && node < 0 && node != kWalkDone) {
+            leaf = node;
+            node = spec_pop<kDepth>(stack, sp);
+        }
+        while (leaf < 0) {
+            const int l = ~leaf;
+            const int first = l >> 3, last = first + (l & 7);
+            for (int tri = first; tri <= last; ++tri) {
+                f3 v0, v1, v2;
+                uint32_t flat;
+                load_tri(s, tri, &v0, &v1, &v2, &flat);
+                float t, V, W, det;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin &&
+                    (t < best_t || (t == best_t && flat < best_key))) {
+                    best_t = t;
+                    best_key = flat;
+                    best_tri = tri;
+                }
+            }
+            leaf = 0;
+            if (node < 0 && node != kWalkDone) {
+                leaf = node;
+                node = spec_pop<kDepth>(stack, sp);
+            }
+        }
+    }
+    if (best_tri >= 0) {
+        f3 v0, v1, v2;
+        uint32_t flat;
+        load_tri(s, best_tri, &v0, &v1, &v2, &flat);
+        float t, V, W, det;
+        wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det);
+        hit.valid = true;
+        hit.flat = best_key;
+        hit.t = best_t;
+        hit.b1 = V / det;
+        hit.b2 = W / det;
+    }
+    return hit;
+}
+
+template <int kDepth = kTraversalStack>
+__device__ __forceinline__ bool trace_any_binary_spec(const SceneView& s, f3 o, f3 d, float tmin, float tmax) {
+    if (s.tri_count == 0) return false;
+    const WtRay wr = wt_setup(d);
+    const BoxRay br = box_setup(o, d);
+    int stack[kDepth];
+    int sp = 0;
+    int node = s.root;
+    int leaf = 0;
+    while (node != kWalkDone) {
+        while (node >= 0) {
+            node = spec_interior<kDepth>(s, br, node, tmin, tmax, stack, sp);
+            if (node < 0 && node != kWalkDone && leaf == 0) {
+                leaf = node;
+                node = spec_pop<kDepth>(stack, sp);
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;
+        }
+        if (leaf == 0 && node < 0 && node != kWalkDone) {
+            leaf = node;
+            node = spec_pop<kDepth>(stack, sp);
+        }
+        while (leaf < 0) {
+            const int l = ~leaf;
+            const int first = l >> 3, last = first + (l & 7);
+            for (int tri = first; tri <= last; ++tri) {
+                f3 v0, v1, v2;
+                uint32_t flat;
+                load_tri(s, tri, &v0, &v1, &v2, &flat);
+                float t, V, W, det;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) return true;
+            }
+            leaf = 0;
+            if (node < 0 && node != kWalkDone) {
+                leaf = node;
+                node = spec_pop<kDepth>(stack, sp);
+            }
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
 // Resumable binary walks: the state of trace_closest_binary /
 // trace_any_binary between steps, so that a persistent kernel can advance a
 // lane's ray one node (or leaf) at a time and hand a lane whose ray has ended

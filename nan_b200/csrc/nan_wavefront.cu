@@ -148,9 +148,10 @@ struct ManyScenes {
     __device__ __forceinline__ const SceneView& of(uint32_t p) const { return sets[set_of[p]].s; }
 };
 
-template <int kWidth, class Src, int kShared = 0>
+template <int kWidth, class Src, int kShared = 0, bool kSpec = false>
 // kShared > 0 (binary nodes): the first kShared traversal-stack entries of a
-// thread live in a shared-memory column, the rest in local memory.
+// thread live in a shared-memory column, the rest in local memory. kSpec
+// (binary nodes): the speculative while-while walk.
 // 10 resident blocks of 128 per SM (48 registers a thread, -Xptxas -v): measured
 // 1,941 against 1,895 Mrays/s with the register count left free (9 blocks),
 // 1,916 at 11 and 12 blocks, 1,639 at 16 (spills).
@@ -181,6 +182,8 @@ __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* 
                     SplitStack<kShared, 128, kTraversalStack> stk;
                     stk.top = stack_top + threadIdx.x;
                     h = trace_closest_binary_s<kTraversalStack>(s, stk, xyz(o), xyz(d), o.w, d.w);
+                } else if constexpr (kSpec && kWidth == 2) {
+                    h = trace_closest_binary_spec(s, xyz(o), xyz(d), o.w, d.w);
                 } else {
                     h = trace_closest_w<kWidth>(s, xyz(o), xyz(d), o.w, d.w);
                 }
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(128, 10) k_wf_extend(Src src, const uint32_t* 
     flush_tally(counters, tally, 0u, 0u);
 }
 
-template <int kWidth, class Src, int kShared = 0>
+template <int kWidth, class Src, int kShared = 0, bool kSpec = false>
 __global__ void __launch_bounds__(128, 10) k_wf_shadow(Src src, const float4* __restrict__ queue, uint32_t* ctl,
                                                    float t_max, float4* __restrict__ rad, float4* __restrict__ si,
                                                    unsigned long long* counters) {
@@ -215,6 +218,8 @@ __global__ void __launch_bounds__(128, 10) k_wf_shadow(Src src, const float4* __
                 SplitStack<kShared, 128, kTraversalStack> stk;
                 stk.top = stack_top + threadIdx.x;
                 blocked = trace_any_binary_s<kTraversalStack>(s, stk, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
+            } else if constexpr (kSpec && kWidth == 2) {
+                blocked = trace_any_binary_spec(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
             } else {
                 blocked = trace_any_w<kWidth>(s, xyz(a), xyz(b), 0.0f, c.w > 0.0f ? c.w : t_max);
             }
@@ -1215,6 +1220,7 @@ void launch_extend(const NanContext* ctx, int blocks, cudaStream_t st, bool wide
         case 3: k_wf_extend_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         case 4: k_wf_extend_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         case 5: k_wf_extend<2, Src, 16><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
+        case 6: k_wf_extend<2, Src, 0, true><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
         default: k_wf_extend<2><<<blocks, 128, 0, st>>>(NAN_EXT_ARGS); break;
     }
 #undef NAN_EXT_ARGS
@@ -1231,6 +1237,7 @@ void launch_shadow(const NanContext* ctx, int blocks, cudaStream_t st, bool wide
         case 3: k_wf_shadow_refill<24, 1, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         case 4: k_wf_shadow_refill<16, 4, Src><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         case 5: k_wf_shadow<2, Src, 16><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
+        case 6: k_wf_shadow<2, Src, 0, true><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
         default: k_wf_shadow<2><<<blocks, 128, 0, st>>>(NAN_SHD_ARGS); break;
     }
 #undef NAN_SHD_ARGS

@@ -1,5 +1,6 @@
 """Every wavefront traversal form (NanTuning.traversal: whole-warp ray
-grabs, or lanes refilled from the queue at several thresholds) changes only
+grabs, lanes refilled from the queue at several thresholds, a shared-memory
+stack top, the speculative while-while walk) changes only
 which lane walks which ray and when: texel slots, probe fields, screen
 pixels and the ray counts equal those of the default form bit for bit, on
 PLOC and LBVH trees (LBVH leaves hold up to 8 triangles)."""
@@ -25,7 +26,7 @@ def test_traversal_forms_do_not_change_results(device, builder):
     w, h = 64, 48
     node.camera.begin_frame(w, h)
     results, rays = [], []
-    for form in (0, 1, 2, 3, 4, 5):
+    for form in (0, 1, 2, 3, 4, 5, 6):
         scene.configure("wavefront", traversal=form)
         scene.context.read_counters(reset=True)
         slots = torch.zeros((layout.total_payload_count, 4), dtype=torch.int32, device="cuda")
