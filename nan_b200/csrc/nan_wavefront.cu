@@ -374,7 +374,8 @@ __global__ void __launch_bounds__(128, 10) k_wf_shadow_refill(Src src, const flo
 // bandwidth: their launch bound of 6 blocks of 128 per SM (at most 80
 // registers, no spills in the texel stages; they used 111-128) doubles the
 // resident warps. Measured on the 200k texel iteration: 5.54 -> 5.03 ms of
-// stage time per step.
+// stage time per step. Shade and finalize take 8 blocks (64 registers, about
+// 112 B of spills each): 5.04 -> 4.92 ms; generate stays at 6.
 // ---------------------------------------------------------------------------
 // Texture-space integrator stages (texture_space_path_tracer.slang:57-216).
 // ---------------------------------------------------------------------------
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(128) k_wf_point_generate(SceneView s, Lighting
 
 // One bounce of trace_radiance (texture_space_path_tracer.slang:60-83) after
 // the extend stage found the hit.
-__global__ void __launch_bounds__(128, 6) k_wf_texel_shade(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+__global__ void __launch_bounds__(128, 8) k_wf_texel_shade(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
                                                         WfQueues q, int buf, uint32_t* ctl) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
@@ -527,7 +528,7 @@ __global__ void __launch_bounds__(128, 6) k_wf_texel_shade(SceneView s, Lighting
 
 // Close finished samples: si += L*|z|/pdf, irr += si, next sample / side, or
 // the running-mean store (texture_space_path_tracer.slang:111-138, 203-215).
-__global__ void __launch_bounds__(128, 6) k_wf_texel_finalize(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
+__global__ void __launch_bounds__(128, 8) k_wf_texel_finalize(SceneView s, LightingRaw lraw, TexelArgs a, WfState st,
                                                            WfQueues q, int buf, uint32_t* ctl, uint32_t* ctl_next) {
     const uint32_t count = *(volatile uint32_t*)(ctl + 0);
     const LightParams L = make_light(lraw);
