@@ -374,6 +374,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary_s(const SceneView& s, St
     float best_t = tmax;
     uint32_t best_key = 0xffffffffu;
     int best_tri = -1;
+    bool overflow = false;
     for (;;) {
         if (node >= 0) {
             const float4* n = s.nodes + 4 * node;
@@ -382,16 +383,17 @@ __device__ __forceinline__ HitInfo trace_closest_binary_s(const SceneView& s, St
             float t0, t1;
             bool h0, h1;
             box2(br, na, nb, nc, tmin, best_t, &t0, &t1, &h0, &h1);
-            if (h0 && h1) {
-                int near_child = nd.x, far_child = nd.y;
-                if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kDepth) stack.put(sp++, far_child);
-                else atomicOr(s.status, kStatusStackOverflow);
-                node = near_child;
+            if (h0 || h1) {
+                // near child first; the far one is pushed when both are hit
+                // (selects and a predicated push: one branch per node)
+                const bool both = h0 && h1, swap = both && t1 < t0;
+                const bool push = both && sp < kDepth;
+                overflow |= both && sp >= kDepth;
+                if (push) stack.put(sp, swap ? nd.x : nd.y);
+                sp += push ? 1 : 0;
+                node = (h0 && !swap) ? nd.x : nd.y;
                 continue;
             }
-            if (h0) { node = nd.x; continue; }
-            if (h1) { node = nd.y; continue; }
         } else {
             const int leaf = ~node;
             const int first = leaf >> 3, last = first + (leaf & 7);
@@ -411,6 +413,7 @@ __device__ __forceinline__ HitInfo trace_closest_binary_s(const SceneView& s, St
         if (sp == 0) break;
         node = stack.get(--sp);
     }
+    if (overflow) atomicOr(s.status, kStatusStackOverflow);
     if (best_tri >= 0) {
         f3 v0, v1, v2;
         uint32_t flat;
@@ -440,6 +443,7 @@ __device__ __forceinline__ bool trace_any_binary_s(const SceneView& s, Stk& stac
     const BoxRay br = box_setup(o, d);
     int sp = 0;
     int node = s.root;
+    bool overflow = false, blocked = false;
     for (;;) {
         if (node >= 0) {
             const float4* n = s.nodes + 4 * node;
@@ -448,16 +452,15 @@ __device__ __forceinline__ bool trace_any_binary_s(const SceneView& s, Stk& stac
             float t0, t1;
             bool h0, h1;
             box2(br, na, nb, nc, tmin, tmax, &t0, &t1, &h0, &h1);
-            if (h0 && h1) {
-                int near_child = nd.x, far_child = nd.y;
-                if (t1 < t0) { near_child = nd.y; far_child = nd.x; }
-                if (sp < kDepth) stack.put(sp++, far_child);
-                else atomicOr(s.status, kStatusStackOverflow);
-                node = near_child;
+            if (h0 || h1) {
+                const bool both = h0 && h1, swap = both && t1 < t0;
+                const bool push = both && sp < kDepth;
+                overflow |= both && sp >= kDepth;
+                if (push) stack.put(sp, swap ? nd.x : nd.y);
+                sp += push ? 1 : 0;
+                node = (h0 && !swap) ? nd.x : nd.y;
                 continue;
             }
-            if (h0) { node = nd.x; continue; }
-            if (h1) { node = nd.y; continue; }
         } else {
             const int leaf = ~node;
             const int first = leaf >> 3, last = first + (leaf & 7);
@@ -466,13 +469,18 @@ __device__ __forceinline__ bool trace_any_binary_s(const SceneView& s, Stk& stac
                 uint32_t flat;
                 load_tri(s, tri, &v0, &v1, &v2, &flat);
                 float t, V, W, det;
-                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) return true;
+                if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin && t <= tmax) {
+                    blocked = true;
+                    break;
+                }
             }
+            if (blocked) break;
         }
         if (sp == 0) break;
         node = stack.get(--sp);
     }
-    return false;
+    if (overflow) atomicOr(s.status, kStatusStackOverflow);
+    return blocked;
 }
 
 template <int kDepth = kTraversalStack>
