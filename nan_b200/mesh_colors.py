@@ -102,6 +102,44 @@ def _patch(r: np.ndarray) -> np.ndarray:
     return (r + 1) * (r + 2) // 2
 
 
+def _wanted_resolutions(scene_node, texels_per_unit: float, min_resolution: int, max_resolution: int,
+                        chunk_triangles: int = 1 << 20) -> list:
+    """Per instance, each triangle's patch resolution before the texel
+    budget: the power of two at or above its longest world-space edge x
+    texels_per_unit, clamped to [min_resolution, max_resolution]. The
+    instances of one mesh are transformed together (in chunks of about
+    chunk_triangles triangles), each with the arithmetic of its own
+    transform alone."""
+    out = [None] * len(scene_node.instances)
+    groups: dict = {}
+    for i, (mesh_id, _, _) in enumerate(scene_node.instances):
+        groups.setdefault(mesh_id, []).append(i)
+    for mesh_id, members in groups.items():
+        mesh = scene_node.meshes[mesh_id]
+        p = mesh.vertices[:, 0:3].astype(np.float32)
+        idx = mesh.indices.astype(np.int64)
+        step = max(1, chunk_triangles // max(mesh.triangle_count, 1))
+        for c in range(0, len(members), step):
+            part = members[c:c + step]
+            m = np.stack([np.asarray(scene_node.transforms[scene_node.instances[i][2]], dtype=np.float32)
+                          for i in part])
+            world = (p @ m[:, :3, :3].transpose(0, 2, 1) + m[:, None, :3, 3]).astype(np.float32).astype(np.float64)
+            tri = world[:, idx]  # [g, T, 3, 3]
+            e = np.stack([
+                np.linalg.norm(tri[:, :, 1] - tri[:, :, 0], axis=2),
+                np.linalg.norm(tri[:, :, 2] - tri[:, :, 1], axis=2),
+                np.linalg.norm(tri[:, :, 0] - tri[:, :, 2], axis=2),
+            ], axis=2).max(axis=2)
+            want = np.maximum(min_resolution, np.ceil(e * texels_per_unit)).astype(np.int64)
+            want = np.maximum(want, 1)
+            res = np.left_shift(1, np.ceil(np.log2(want)).astype(np.int64))
+            res = np.where(res < want, res * 2, res)  # guard log2 rounding
+            res = np.minimum(res, max_resolution)
+            for j, i in enumerate(part):
+                out[i] = res[j]
+    return out
+
+
 class MeshColorsLayout:
     """Layout arrays: face_infos u32[F,2], instance_infos u32[I,4], side_infos u32[I,2]."""
 
@@ -150,30 +188,48 @@ class MeshColorsLayout:
             )
         max_total_texels = max(1, int(max_total_texels))
         faces, instances, sides = [], [], []
+        face_count = 0
         total_surface = 0
         total_payload = 0
-        for mesh_id, material_id, transform_id in scene_node.instances:
-            mesh = scene_node.meshes[mesh_id]
-            material = scene_node.materials[material_id]
-            double_sided = bool(getattr(material, "double_sided", False))
+        wanted = _wanted_resolutions(scene_node, texels_per_unit, min_resolution, max_resolution)
+        n_inst = len(scene_node.instances)
+        double = np.array([bool(getattr(scene_node.materials[mat], "double_sided", False))
+                           for _, mat, _ in scene_node.instances], dtype=bool)
+        mult_all = np.where(double, 2, 1).astype(np.int64)
+        # the instances before the first one that would exceed the budget at
+        # its wanted resolutions are laid out in one pass
+        tri_n = np.array([w.shape[0] for w in wanted], np.int64)
+        flat_res = np.concatenate(wanted) if n_inst else np.zeros(0, np.int64)
+        flat_patch = _patch(flat_res)
+        tri_start = np.concatenate([[0], np.cumsum(tri_n)])
+        patch_cum = np.concatenate([[0], np.cumsum(flat_patch)])
+        local_totals = patch_cum[tri_start[1:]] - patch_cum[tri_start[:-1]]
+        payload_after = np.cumsum(local_totals * mult_all)
+        over = np.flatnonzero((tri_n > 0) & (payload_after > max_total_texels))
+        k0 = int(over[0]) if over.size else n_inst
+        if k0:
+            e = int(tri_start[k0])
+            owner = np.repeat(np.arange(k0), tri_n[:k0])
+            addresses = (patch_cum[1:e + 1] - patch_cum[tri_start[owner]] - flat_patch[:e]).astype(np.uint32)
+            faces.append(np.stack([addresses, flat_res[:e].astype(np.uint32)], axis=1))
+            face_off = tri_start[:k0]
+            pay_off = np.concatenate([[0], payload_after[:k0 - 1]]) if k0 > 1 else np.zeros(1, np.int64)
+            instances.extend(zip(face_off.tolist(), tri_n[:k0].tolist(), pay_off.tolist(),
+                                 local_totals[:k0].tolist()))
+            back = np.where(double[:k0], pay_off + local_totals[:k0], MESH_COLORS_INVALID_OFFSET)
+            flag = np.where(double[:k0], MESH_COLORS_SIDE_FLAG_DOUBLE_SIDED, 0)
+            sides.extend(zip(back.tolist(), flag.tolist()))
+            face_count = e
+            total_surface = int(local_totals[:k0].sum())
+            total_payload = int(payload_after[k0 - 1])
+        for inst_k in range(k0, n_inst):
+            mesh = scene_node.meshes[scene_node.instances[inst_k][0]]
+            double_sided = bool(double[inst_k])
             mult = 2 if double_sided else 1
-            m = np.asarray(scene_node.transforms[transform_id], dtype=np.float32)
-            p = mesh.vertices[:, 0:3].astype(np.float32)
-            world = (p @ m[:3, :3].T + m[:3, 3]).astype(np.float32).astype(np.float64)
-            tri = world[mesh.indices.astype(np.int64)]  # [T,3,3]
-            e = np.stack([
-                np.linalg.norm(tri[:, 1] - tri[:, 0], axis=1),
-                np.linalg.norm(tri[:, 2] - tri[:, 1], axis=1),
-                np.linalg.norm(tri[:, 0] - tri[:, 2], axis=1),
-            ], axis=1).max(axis=1)
-            want = np.maximum(min_resolution, np.ceil(e * texels_per_unit)).astype(np.int64)
-            want = np.maximum(want, 1)
-            res = np.left_shift(1, np.ceil(np.log2(want)).astype(np.int64))
-            res = np.where(res < want, res * 2, res)  # guard log2 rounding
-            res = np.minimum(res, max_resolution)
+            res = wanted[inst_k]
             patch = _patch(res)
             cum = np.cumsum(patch)
-            face_offset = len(faces) and sum(len(f) for f in faces)
+            face_offset = face_count
             if mesh.triangle_count and total_payload + int(cum[-1]) * mult > max_total_texels:
                 res = res.copy()
                 local = 0
@@ -201,6 +257,7 @@ class MeshColorsLayout:
                 cum = np.cumsum(patch)
             addresses = (cum - patch).astype(np.uint32)
             faces.append(np.stack([addresses, res.astype(np.uint32)], axis=1))
+            face_count += faces[-1].shape[0]
             local_total = int(cum[-1]) if mesh.triangle_count else 0
             instances.append((face_offset, mesh.triangle_count, total_payload, local_total))
             back = total_payload + local_total if double_sided else MESH_COLORS_INVALID_OFFSET
