@@ -207,10 +207,12 @@ __device__ __forceinline__ WideRay wide_setup(f3 o, f3 d) {
     return r;
 }
 
+// Slot bits of m reordered by the ray's octant (bit i moves to i ^ oct), by
+// selects: oct is fixed per ray but differs between the lanes of a warp.
 __device__ __forceinline__ uint32_t octant_permute(uint32_t m, uint32_t oct) {
-    if (oct & 1u) m = ((m & 0x55u) << 1) | ((m & 0xaau) >> 1);
-    if (oct & 2u) m = ((m & 0x33u) << 2) | ((m & 0xccu) >> 2);
-    if (oct & 4u) m = ((m & 0x0fu) << 4) | ((m & 0xf0u) >> 4);
+    m = (oct & 1u) ? (((m & 0x55u) << 1) | ((m & 0xaau) >> 1)) : m;
+    m = (oct & 2u) ? (((m & 0x33u) << 2) | ((m & 0xccu) >> 2)) : m;
+    m = (oct & 4u) ? (((m & 0x0fu) << 4) | ((m & 0xf0u) >> 4)) : m;
     return m;
 }
 
@@ -267,6 +269,7 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
     uint32_t g_base = 0u, g_imask = 1u, g_mask = 1u << r.oct;  // the root as slot 0 of a virtual group
     float best_t = tmax;
     uint32_t best_key = 0xffffffffu, best_tri = 0xffffffffu;
+    bool overflow = false;
     for (;;) {
         if (g_mask == 0u) {
             if (sp == 0) break;
@@ -280,10 +283,10 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
         g_mask &= g_mask - 1u;
         const uint32_t slot = pos ^ r.oct;
         const uint32_t child = g_base + (uint32_t)__popc(g_imask & ((1u << slot) - 1u));
-        if (g_mask != 0u) {
-            if (sp < kWideStack) stack[sp++] = make_uint2(g_base, (g_imask << 8) | g_mask);
-            else atomicOr(s.status, kStatusStackOverflow);
-        }
+        const bool push = g_mask != 0u && sp < kWideStack;
+        overflow |= g_mask != 0u && sp >= kWideStack;
+        if (push) stack[sp] = make_uint2(g_base, (g_imask << 8) | g_mask);
+        sp += push ? 1 : 0;
         const uint4* w = s.wnodes + 5u * child;
         const uint4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
         const uint32_t imask = w0.w >> 24;
@@ -303,7 +306,10 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
                 float t, V, W, det;
                 if (wt_test(wr, o, v0, v1, v2, &t, &V, &W, &det) && t >= tmin) {
                     if (kAnyHit) {
-                        if (t <= tmax) return true;
+                        if (t <= tmax) {
+                            if (overflow) atomicOr(s.status, kStatusStackOverflow);
+                            return true;
+                        }
                     } else if (t < best_t || (t == best_t && flat < best_key)) {
                         best_t = t;
                         best_key = flat;
@@ -316,6 +322,7 @@ __device__ __forceinline__ bool trace_wide(const SceneView& s, f3 o, f3 d, float
         g_imask = imask;
         g_mask = octant_permute(hits & imask, r.oct);
     }
+    if (overflow) atomicOr(s.status, kStatusStackOverflow);
     if (kAnyHit) return false;
     if (best_tri != 0xffffffffu) {
         f3 v0, v1, v2;
