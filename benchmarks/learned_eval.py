@@ -173,13 +173,15 @@ def main() -> None:
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--cache-vertex", type=int, default=1)
+    ap.add_argument("--table-update", choices=("dense", "lazy"), default="lazy",
+                    help="Adam over the whole hash table or only the entries a step touched (the bench's)")
     a = ap.parse_args()
     device = Device(0)
     node = scenes.terrain_boxes(seed=1, grid=699, boxes=2000)
     scene = Scene(device, node)
     lo, hi = scene_bounds(scene)
-    tracer = CachedPathTracer(device, scene, RadianceCache(device, lo, hi), cache_vertex=a.cache_vertex,
-                              train_batch=16384)
+    tracer = CachedPathTracer(device, scene, RadianceCache(device, lo, hi, table_update=a.table_update),
+                              cache_vertex=a.cache_vertex, train_batch=16384)
     out = torch.zeros((a.height, a.width, 4), dtype=torch.float32, device=device.torch_device)
     for f in range(a.frames):
         node.camera.begin_frame(a.width, a.height)

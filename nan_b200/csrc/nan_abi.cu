@@ -807,6 +807,12 @@ NAN_B200_API int nan_trace_points(NanContext* ctx, const float* points, uint32_t
     if (const int lrc = nan_host::check_lighting(lighting)) return lrc;
     if (!aligned16(points) || !aligned16(out)) return invalid("points and out must be 16-byte aligned");
     if (flags & ~(uint32_t)NAN_POINTS_INDIRECT_ONLY) return invalid("unknown points flag");
+    // Up to kPointsPerThreadMax points (the learned cache's training sets) a
+    // thread per point beats the wavefront's rounds of small launches.
+    constexpr uint32_t kPointsPerThreadMax = 1u << 18;
+    if (ctx->tuning.integrator != 0 || count <= kPointsPerThreadMax)
+        return nan_host::launch_trace_points(ctx, points, count, out, iteration, samples, max_bounces, flags, lighting,
+                                             as_stream(stream));
     return nan_host::launch_trace_points_wavefront(ctx, points, count, out, iteration, samples, max_bounces, flags,
                                                    lighting, as_stream(stream));
 }

@@ -189,6 +189,11 @@ int launch_cache_step(NanCache* k, cudaStream_t st);
 int launch_trace_points_wavefront(NanContext* ctx, const float* points, uint32_t count, float* out,
                                   uint32_t iteration, uint32_t samples, uint32_t max_bounces, uint32_t flags,
                                   const NanLighting* light, cudaStream_t st);
+// The same values with one thread per point (one launch): the choice for
+// small point sets, whose wavefront rounds are bound by launch latency.
+int launch_trace_points(NanContext* ctx, const float* points, uint32_t count, float* out, uint32_t iteration,
+                        uint32_t samples, uint32_t max_bounces, uint32_t flags, const NanLighting* light,
+                        cudaStream_t st);
 int launch_trace_screen_cached(NanContext* ctx, NanCache* cache, float* out, uint32_t w, uint32_t h,
                                uint32_t frame, const NanCamera* cam, const NanLighting* light,
                                const NanCachedFrame* fd, cudaStream_t st);

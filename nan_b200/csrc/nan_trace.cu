@@ -730,6 +730,52 @@ __global__ void __launch_bounds__(128) k_trace_texels(SceneView s, LightingRaw l
     flush_tally(counters, tally, 1u, paths);
 }
 
+// The texel estimator at listed surface points (b1, b2, instance bits,
+// primitive bits | back side << 31), one thread per point: RNG(index,
+// 0xFFFFFFFF, iteration * n), view = the flat normal (negated for the back
+// side); indirect_only drops the first vertex's sun term but still draws its
+// two numbers. Out: (E, 0), or (0, 0, 0, -1) for a point whose instance is
+// ~0. The same values as the wavefront points pass (k_wf_point_generate and
+// the texel stages); one launch instead of a round of launches per bounce,
+// for the small point sets that train the learned cache.
+__global__ void __launch_bounds__(128) k_trace_points(SceneView s, LightingRaw lraw, const float4* __restrict__ points,
+                                                      uint32_t count, float4* __restrict__ out, uint32_t iteration,
+                                                      uint32_t n, uint32_t max_bounces, int indirect_only,
+                                                      unsigned long long* counters) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= count) return;
+    const float4 pt = points[u];
+    const uint32_t inst = __float_as_uint(pt.z), primw = __float_as_uint(pt.w);
+    const uint32_t prim = primw & 0x7fffffffu;
+    if (inst == 0xffffffffu || !valid_prim(s, inst, prim)) {
+        if (inst != 0xffffffffu) atomicOr(s.status, kStatusBadRecord);
+        out[u] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        return;
+    }
+    const LightParams L = make_light(lraw);
+    Rng rng(u, 0xffffffffu, iteration * n);
+    RayTally tally{0u, 0u};
+    f3 view = world_flat_normal(s, inst, prim);
+    if (primw >> 31) view = -view;
+    const Shading sd = shading_data(s, inst, prim, pt.x, pt.y, view);
+    f3 irr = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t k = 0; k < n; ++k) {
+        const float u0 = rng.next_1d(), u1 = rng.next_1d();
+        f3 si = indirect_only ? mk3(0.0f, 0.0f, 0.0f) : sun_irradiance(s, L, sd, u0, u1, tally);
+        const float e0 = rng.next_1d(), e1 = rng.next_1d();
+        float pdf;
+        const f3 dir = cosine_sample_hemisphere(e0, e1, &pdf);
+        if (pdf > 1e-6f) {
+            const f3 rad = ts_trace_radiance(s, L, sd.origin_front, sd.frame.to_global(dir), rng, max_bounces, tally);
+            si = si + ((rad * fabsf(dir.z)) / pdf);
+        }
+        irr = irr + si;
+    }
+    const f3 e = irr / (float)n;
+    out[u] = make_float4(e.x, e.y, e.z, 0.0f);
+    flush_tally(counters, tally, 1u, n);
+}
+
 // ---------------------------------------------------------------------------
 // Surface-probe baker: surface_probe_path_tracer.slang:47-315.
 // ---------------------------------------------------------------------------
@@ -1087,6 +1133,18 @@ int launch_trace_texels(NanContext* ctx, const NanMeshColorsDesc* lay, uint8_t* 
                                                                   max_bounces, reset, begin, end, ctx->d_counters);
     ctx->launches++;
     return cuda_fail(cudaGetLastError(), "trace_texels launch");
+}
+
+int launch_trace_points(NanContext* ctx, const float* points, uint32_t count, float* out, uint32_t iteration,
+                        uint32_t samples, uint32_t max_bounces, uint32_t flags, const NanLighting* light,
+                        cudaStream_t st) {
+    if (count == 0) return NAN_OK;
+    k_trace_points<<<blocks_for(count, 128), 128, 0, st>>>(
+        scene_view(ctx), to_raw(light), reinterpret_cast<const float4*>(points), count, reinterpret_cast<float4*>(out),
+        iteration, std::max(samples, 1u), std::max(max_bounces, 1u), (flags & NAN_POINTS_INDIRECT_ONLY) ? 1 : 0,
+        ctx->d_counters);
+    ctx->launches++;
+    return cuda_fail(cudaGetLastError(), "trace_points launch");
 }
 
 int launch_trace_probes(NanContext* ctx, float* values, uint32_t* counts, uint32_t* self_hits, uint32_t* radial,
