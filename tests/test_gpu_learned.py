@@ -63,6 +63,29 @@ def test_points_pass_matches_oracle(which, device):
     device.check()
 
 
+def test_points_pass_forms_agree(device):
+    """Up to 2^18 points are traced one thread per point, larger sets by the
+    wavefront stages. A point's sample stream depends on its index only, so
+    the first points of a large set (wavefront) equal the same points traced
+    alone (one thread each) bit for bit, indirect-only mode included."""
+    import torch
+
+    import nan_b200
+    from nan_b200 import scenes
+
+    node = scenes.terrain_boxes(seed=1, grid=129, boxes=120)
+    scene = nan_b200.Scene(device, node)
+    big = _random_points(node, (1 << 18) + 4096, seed=9)
+    small = big[:8192].copy()
+    for it, indirect in ((0, False), (3, True)):
+        wide = scene.trace_points(torch.from_numpy(big).cuda(), it, samples=2, max_bounces=3,
+                                  indirect_only=indirect).cpu().numpy()
+        one = scene.trace_points(torch.from_numpy(small).cuda(), it, samples=2, max_bounces=3,
+                                 indirect_only=indirect).cpu().numpy()
+        assert np.array_equal(wide[:8192].view(np.uint32), one.view(np.uint32))
+    device.check()
+
+
 def test_cached_frame_records_queries_and_training_points(device):
     import torch
 
