@@ -963,10 +963,10 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     SubtreeInfo root_info;
     uint32_t max_depth = 0;
     double sah_host = 0.0;
-    cudaMemcpyAsync(&root_info, info + root, sizeof(SubtreeInfo), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
-    err = cudaStreamSynchronize(s);
+    err = cudaMemcpyAsync(&root_info, info + root, sizeof(SubtreeInfo), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) return cuda_fail(err, "PLOC emit");
     for (void* p : {(void*)idx_a, (void*)idx_b, (void*)lo_a, (void*)hi_a, (void*)lo_b, (void*)hi_b, (void*)nn,
                     (void*)valid, (void*)pos, (void*)counter, (void*)info, (void*)dfs, (void*)tri_off, (void*)tri_pos,
