@@ -55,7 +55,7 @@ def parse_args():
     ap.add_argument("--boxes", type=int, default=500)
     ap.add_argument("--integrator", choices=["wavefront", "megakernel"], default="wavefront")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent traversal blocks per SM (0 = auto)")
-    ap.add_argument("--bvh", choices=["ploc", "lbvh"], default="ploc")
+    ap.add_argument("--bvh", choices=["sah", "ploc", "lbvh"], default="sah")
     ap.add_argument("--width", type=int, choices=[2, 8], default=2, help="traversed BVH node width")
     ap.add_argument("--paths", type=int, default=0, help="wavefront paths in flight (0 = one per texel)")
     ap.add_argument("--e2e-chunks", type=int, default=2,

@@ -195,13 +195,14 @@ typedef struct NanSupportOptions {
 
 /* Execution choices of a context. The defaults (all zero) are the wavefront
  * integrator with occupancy-sized persistent traversal grids, as many paths
- * in flight as the reserved scratch holds, and the PLOC BVH builder. */
+ * in flight as the reserved scratch holds, and the binned-SAH BVH builder. */
 typedef struct NanTuning {
     uint32_t integrator;           /* 0: wavefront; 1: one thread per pixel/texel/probe */
     uint32_t trace_blocks_per_sm;  /* persistent traversal blocks per SM, 0 = occupancy limit */
     uint32_t max_paths_in_flight;  /* wavefront chunk size, 0 = as many as the scratch holds */
-    uint32_t bvh_builder;          /* nan_scene_build: 0 = PLOC + SAH leaf collapse, 1 = LBVH */
-    uint32_t bvh_width;            /* traversed nodes: 0 or 2 = binary, 8 = compressed 8-wide (PLOC builds) */
+    uint32_t bvh_builder;          /* nan_scene_build: 0 = binned SAH, 1 = LBVH, 2 = PLOC; 0 and 2
+                                      collapse subtrees of up to 3 triangles into leaves by SAH */
+    uint32_t bvh_width;            /* traversed nodes: 0 or 2 = binary, 8 = compressed 8-wide (SAH or PLOC builds) */
     uint32_t kernel_timing;        /* 1: record CUDA events around each wavefront stage launch on the
                                       launching stream (read with nan_ctx_read_kernel_times); not for
                                       use under stream capture */
@@ -284,7 +285,7 @@ NAN_B200_API int nan_scene_build(NanContext* ctx, const NanSceneDesc* desc, void
  * (Karras 2012) with binary nodes: the context's NanTuning bvh_builder and
  * bvh_width are ignored. Hits equal nan_scene_build's (the closest hit is
  * chosen by (t, flat index) in any tree), but the LBVH has a higher SAH cost
- * than the default PLOC tree, so tracing it is slower. The BVH is written into the
+ * than the default binned-SAH tree, so tracing it is slower. The BVH is written into the
  * caller's buffers, which must stay alive while the context traces them:
  *   out_nodes  >= 64 * max(T - 1, 1) bytes, 16-byte aligned
  *   out_tris   >= 48 * T bytes, 16-byte aligned

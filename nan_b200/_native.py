@@ -241,7 +241,7 @@ class NanSupportOptions(ctypes.Structure):
 
 
 INTEGRATORS = {"wavefront": 0, "megakernel": 1}
-BVH_BUILDERS = {"ploc": 0, "lbvh": 1}
+BVH_BUILDERS = {"sah": 0, "lbvh": 1, "ploc": 2}
 
 
 class NanCounters(ctypes.Structure):
@@ -431,7 +431,7 @@ class Context:
         return t.as_dict()
 
     def configure(self, integrator: str = "wavefront", trace_blocks_per_sm: int = 0,
-                  max_paths_in_flight: int = 0, bvh_builder: str = "ploc", bvh_width: int = 2,
+                  max_paths_in_flight: int = 0, bvh_builder: str = "sah", bvh_width: int = 2,
                   kernel_timing: bool = False, ray_order: int = 0, traversal: int = 0) -> None:
         t = NanTuning()
         t.ray_order = int(ray_order)

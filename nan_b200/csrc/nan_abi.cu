@@ -252,7 +252,7 @@ NAN_B200_API int nan_ctx_configure(NanContext* ctx, const NanTuning* tuning) {
     if (!ctx || !tuning) return invalid("null argument");
     if (tuning->integrator > 1) return invalid("integrator must be 0 (wavefront) or 1 (one thread per unit)");
     if (tuning->trace_blocks_per_sm > 64) return invalid("trace_blocks_per_sm above 64");
-    if (tuning->bvh_builder > 1) return invalid("bvh_builder must be 0 (PLOC) or 1 (LBVH)");
+    if (tuning->bvh_builder > 2) return invalid("bvh_builder must be 0 (binned SAH), 1 (LBVH) or 2 (PLOC)");
     if (tuning->bvh_width != 0 && tuning->bvh_width != 2 && tuning->bvh_width != 8)
         return invalid("bvh_width must be 0 or 2 (binary) or 8 (compressed wide)");
     if (tuning->kernel_timing > 1) return invalid("kernel_timing must be 0 or 1");

@@ -207,6 +207,15 @@ __device__ __forceinline__ void child_box(int c, const float4* node_lo, const fl
     }
 }
 
+// Every walk from a leaf or node up to the root stops after kMaxWalk steps
+// or at a parent index outside [0, interior): a malformed hierarchy then
+// yields a depth above the traversal stack's (rejected by the host) instead of
+// a walk that never ends. Valid trees have depth <= 96 here.
+constexpr uint32_t kMaxWalk = 4096u;
+__device__ __forceinline__ bool walk_on(int p, uint32_t interior, uint32_t steps) {
+    return p >= 0 && (uint32_t)p < interior && steps < kMaxWalk;
+}
+
 // Bottom-up refit: the second thread to reach a node computes its box.
 __global__ void k_refit(uint32_t n, const int2* __restrict__ children, const int* __restrict__ node_parent,
                         const int* __restrict__ leaf_parent, const float4* __restrict__ leaf_lo,
@@ -215,7 +224,7 @@ __global__ void k_refit(uint32_t n, const int2* __restrict__ children, const int
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int p = leaf_parent[i];
-    while (p >= 0) {
+    for (uint32_t steps = 0; walk_on(p, n - 1u, steps); ++steps) {
         __threadfence();
         if (atomicAdd(&arrivals[p], 1u) == 0u) return;
         const int2 ch = children[p];
@@ -235,10 +244,11 @@ __global__ void k_depth(uint32_t n, const int* __restrict__ node_parent, const i
     if (i >= n) return;
     uint32_t depth = 1;
     int p = leaf_parent[i];
-    while (p >= 0 && depth < 4096u) {
+    while (walk_on(p, n - 1u, depth)) {
         ++depth;
         p = node_parent[p];
     }
+    if (p >= 0) depth = kMaxWalk;  // a parent out of range or a walk too long: reject
     atomicMax(max_depth, depth);
 }
 
@@ -444,7 +454,7 @@ __global__ void k_subtree(uint32_t n, const int2* __restrict__ children, const i
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int p = leaf_parent[i];
-    while (p >= 0) {
+    for (uint32_t steps = 0; walk_on(p, n - 1u, steps); ++steps) {
         __threadfence();
         if (atomicAdd(&arrivals[p], 1u) == 0u) return;
         const int2 ch = children[p];
@@ -490,7 +500,7 @@ __global__ void k_dfs_nodes(uint32_t interior, const int2* __restrict__ children
     uint32_t toff = 0u;
     bool hidden = false;
     int p = node_parent[node];
-    while (p >= 0) {
+    for (uint32_t steps = 0; walk_on(p, interior, steps); ++steps) {
         const SubtreeInfo pi = info[p];
         if (pi.collapsed) hidden = true;
         const int2 ch = children[p];
@@ -519,7 +529,7 @@ __global__ void k_dfs_leaves(uint32_t n, const int2* __restrict__ children, cons
     int node = ~(int)i;
     uint32_t toff = 0u;
     int p = leaf_parent[i];
-    while (p >= 0) {
+    for (uint32_t steps = 0; walk_on(p, n - 1u, steps); ++steps) {
         const int2 ch = children[p];
         if (ch.y == node) toff += ch.x >= 0 ? info[ch.x].tris : 1u;
         node = p;
@@ -778,6 +788,527 @@ __global__ void k_wide_level(const WideItem* __restrict__ items, const uint32_t*
     w[4] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
 }
 
+// ---------------------------------------------------------------------------
+// Top-down binned SAH (Wald, "On fast construction of SAH-based bounding
+// volume hierarchies", 2007): every node bins its triangles' centroids into
+// kSahBins equal intervals of the node's centroid bounds on each axis and
+// splits at the bin boundary of least (left area x left count + right area x
+// right count), down to single triangles; the SAH leaf collapse and the
+// depth-first emission above then run on this tree as on PLOC's.
+// Nodes of more than kSahSeqMax triangles are split level by level over the
+// whole GPU: bins accumulate with atomics (per block in shared memory for the
+// block's main node), one thread per node picks the split, and a scan of the
+// left flags partitions each node's range stably. Nodes of at most
+// kSahSeqMax triangles are built by one thread each, with the same split rule.
+// A node whose centroids coincide on every axis splits its range in half.
+// ---------------------------------------------------------------------------
+constexpr int kSahBins = 32;
+constexpr uint32_t kSahSeqMax = 64;
+constexpr int kSahBinWords = 13;  // box lo, hi, centroid lo, hi (ordered ints), count
+constexpr int kSahTaskWords = 3 * kSahBins * kSahBinWords;
+constexpr int kSahMaxLevels = 512;
+
+struct SahTask {
+    uint32_t first, count;
+    int node;
+    int axis;           // split axis, -1: halve the range
+    uint32_t clo[3], chi[3];  // centroid bounds (ordered ints)
+    uint32_t split_bin;       // bins <= split_bin go left
+    uint32_t left_count;
+    int child_task[2];  // next-level large task, or -1
+};
+
+struct SahSmall {
+    uint32_t first, count;
+    int node;
+};
+
+// interior nodes allocated, large tasks of the next level (appended), small
+// tasks (appended), large tasks of the current level
+struct SahCounters {
+    uint32_t nodes, large, small, level;
+    uint32_t overflow;  // nonzero: a bound below was exceeded (nothing was written past it)
+};
+
+// Capacities of the next-level task list, the small-task list and the
+// interior nodes (n - 1).
+struct SahLimits {
+    uint32_t large, small, nodes;
+};
+
+__device__ __forceinline__ float sah_half_area(float lx, float ly, float lz, float hx, float hy, float hz) {
+    const float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    if (!(dx >= 0.0f)) return 0.0f;  // empty box
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Bin of centroid c on an axis with centroid bounds [lo, hi]; every centroid
+// lands in bin 0 when the bounds have no extent.
+__device__ __forceinline__ int sah_bin(float c, float lo, float hi) {
+    const float ext = hi - lo;
+    if (!(ext > 0.0f)) return 0;
+    const float scale = (float)kSahBins / ext;
+    const int b = (int)((c - lo) * scale);
+    return min(max(b, 0), kSahBins - 1);
+}
+
+__device__ __forceinline__ float3 sah_centroid(float4 lo, float4 hi) {
+    return make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+}
+
+__global__ void k_sah_init(uint32_t n, int* __restrict__ ids, int* __restrict__ task_of, int first_task) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    ids[i] = (int)i;
+    task_of[i] = first_task;
+}
+
+__global__ void k_sah_root(uint32_t n, const Bounds* __restrict__ bounds, SahTask* __restrict__ tasks,
+                           SahSmall* __restrict__ small, SahCounters* __restrict__ ctr) {
+    ctr->nodes = 1u;
+    ctr->large = 0u;
+    ctr->level = n > kSahSeqMax ? 1u : 0u;
+    ctr->overflow = 0u;
+    if (n > kSahSeqMax) {
+        SahTask t;
+        t.first = 0u;
+        t.count = n;
+        t.node = 0;
+        t.axis = -1;
+        for (int a = 0; a < 3; ++a) {
+            t.clo[a] = bounds->lo[a];
+            t.chi[a] = bounds->hi[a];
+        }
+        t.split_bin = 0u;
+        t.left_count = 0u;
+        t.child_task[0] = t.child_task[1] = -1;
+        tasks[0] = t;
+        ctr->small = 0u;
+    } else {
+        small[0] = SahSmall{0u, n, 0};
+        ctr->small = 1u;
+    }
+}
+
+__global__ void k_sah_bins_reset(uint32_t words, uint32_t* __restrict__ bins) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= words) return;
+    const uint32_t w = i % kSahBinWords;
+    // min fields start at the largest ordered value, max fields and counts at 0
+    bins[i] = (w < 3 || (w >= 6 && w < 9)) ? 0xffffffffu : 0u;
+}
+
+__device__ __forceinline__ void sah_bin_add(uint32_t* b, float4 lo, float4 hi, float3 c) {
+    const uint32_t v[12] = {float_to_ordered(lo.x), float_to_ordered(lo.y), float_to_ordered(lo.z),
+                            float_to_ordered(hi.x), float_to_ordered(hi.y), float_to_ordered(hi.z),
+                            float_to_ordered(c.x),  float_to_ordered(c.y),  float_to_ordered(c.z),
+                            float_to_ordered(c.x),  float_to_ordered(c.y),  float_to_ordered(c.z)};
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        if (k < 3 || (k >= 6 && k < 9)) atomicMin(b + k, v[k]);
+        else atomicMax(b + k, v[k]);
+    }
+    atomicAdd(b + 12, 1u);
+}
+
+constexpr int kSahBinPerThread = 4;
+
+// Bins of every triangle in a large node. A block covers kThreads x
+// kSahBinPerThread consecutive positions and keeps the bins of the node at
+// its first position in shared memory.
+__global__ void __launch_bounds__(kThreads) k_sah_bin(uint32_t n, const int* __restrict__ ids,
+                                                      const int* __restrict__ task_of,
+                                                      const SahTask* __restrict__ tasks,
+                                                      const float4* __restrict__ leaf_lo,
+                                                      const float4* __restrict__ leaf_hi, uint32_t* __restrict__ bins) {
+    __shared__ uint32_t s_bins[kSahTaskWords];
+    __shared__ uint32_t s_first;
+    const uint32_t base = blockIdx.x * (uint32_t)(kThreads * kSahBinPerThread);
+    if (threadIdx.x == 0) s_first = 0xffffffffu;
+    for (int i = threadIdx.x; i < kSahTaskWords; i += kThreads) {
+        const int w = i % kSahBinWords;
+        s_bins[i] = (w < 3 || (w >= 6 && w < 9)) ? 0xffffffffu : 0u;
+    }
+    __syncthreads();
+    for (int k = 0; k < kSahBinPerThread; ++k) {
+        const uint32_t p = base + (uint32_t)k * kThreads + threadIdx.x;
+        if (p < n && task_of[p] >= 0) {
+            atomicMin(&s_first, p);
+            break;
+        }
+    }
+    __syncthreads();
+    if (s_first == 0xffffffffu) return;
+    const int main_task = task_of[s_first];
+    for (int k = 0; k < kSahBinPerThread; ++k) {
+        const uint32_t p = base + (uint32_t)k * kThreads + threadIdx.x;
+        if (p >= n) break;
+        const int t = task_of[p];
+        if (t < 0) continue;
+        const int prim = ids[p];
+        const float4 lo = leaf_lo[prim], hi = leaf_hi[prim];
+        const float3 c = sah_centroid(lo, hi);
+        const SahTask& task = tasks[t];
+        const float cc[3] = {c.x, c.y, c.z};
+        uint32_t* dst = t == main_task ? s_bins : bins + (size_t)t * kSahTaskWords;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int b = sah_bin(cc[a], ordered_to_float(task.clo[a]), ordered_to_float(task.chi[a]));
+            sah_bin_add(dst + (a * kSahBins + b) * kSahBinWords, lo, hi, c);
+        }
+    }
+    __syncthreads();
+    uint32_t* g = bins + (size_t)main_task * kSahTaskWords;
+    for (int i = threadIdx.x; i < kSahTaskWords; i += kThreads) {
+        const int w = i % kSahBinWords;
+        const uint32_t v = s_bins[i];
+        if (w < 3 || (w >= 6 && w < 9)) {
+            if (v != 0xffffffffu) atomicMin(g + i, v);
+        } else if (v != 0u) {
+            if (w == 12) atomicAdd(g + i, v);
+            else atomicMax(g + i, v);
+        }
+    }
+}
+
+// One thread per large node: its box (the union of its bins on axis 0), the
+// best split, and the children: interior ids, next-level or small tasks.
+__global__ void k_sah_split(const uint32_t* __restrict__ count, SahTask* __restrict__ tasks,
+                            const uint32_t* __restrict__ bins, SahTask* __restrict__ next, SahSmall* __restrict__ small,
+                            SahCounters* __restrict__ ctr, SahLimits lim, int2* __restrict__ children,
+                            int* __restrict__ node_parent, float4* __restrict__ node_lo, float4* __restrict__ node_hi) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *count) return;
+    SahTask task = tasks[t];
+    const uint32_t* tb = bins + (size_t)t * kSahTaskWords;
+    // node box: the union of the axis-0 bins
+    uint32_t box[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    for (int b = 0; b < kSahBins; ++b) {
+        const uint32_t* w = tb + b * kSahBinWords;
+        for (int k = 0; k < 3; ++k) {
+            box[k] = min(box[k], w[k]);
+            box[3 + k] = max(box[3 + k], w[3 + k]);
+        }
+    }
+    node_lo[task.node] = make_float4(ordered_to_float(box[0]), ordered_to_float(box[1]), ordered_to_float(box[2]), 0.f);
+    node_hi[task.node] = make_float4(ordered_to_float(box[3]), ordered_to_float(box[4]), ordered_to_float(box[5]), 0.f);
+    float best_cost = INFINITY;
+    int best_axis = -1, best_bin = 0;
+    for (int a = 0; a < 3; ++a) {
+        const float ext = ordered_to_float(task.chi[a]) - ordered_to_float(task.clo[a]);
+        if (!(ext > 0.0f)) continue;
+        const uint32_t* ab = tb + a * kSahBins * kSahBinWords;
+        float right_area[kSahBins];
+        uint32_t right_n[kSahBins];
+        {
+            float rl[3] = {INFINITY, INFINITY, INFINITY}, rh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t rn = 0u;
+            for (int b = kSahBins - 1; b >= 1; --b) {
+                const uint32_t* w = ab + b * kSahBinWords;
+                if (w[12]) {
+                    for (int k = 0; k < 3; ++k) {
+                        rl[k] = fminf(rl[k], ordered_to_float(w[k]));
+                        rh[k] = fmaxf(rh[k], ordered_to_float(w[3 + k]));
+                    }
+                }
+                rn += w[12];
+                right_area[b] = sah_half_area(rl[0], rl[1], rl[2], rh[0], rh[1], rh[2]);
+                right_n[b] = rn;
+            }
+        }
+        float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t ln = 0u;
+        for (int b = 0; b < kSahBins - 1; ++b) {
+            const uint32_t* w = ab + b * kSahBinWords;
+            if (w[12]) {
+                for (int k = 0; k < 3; ++k) {
+                    ll[k] = fminf(ll[k], ordered_to_float(w[k]));
+                    lh[k] = fmaxf(lh[k], ordered_to_float(w[3 + k]));
+                }
+            }
+            ln += w[12];
+            const uint32_t rn = right_n[b + 1];
+            if (ln == 0u || rn == 0u) continue;
+            const float c = sah_half_area(ll[0], ll[1], ll[2], lh[0], lh[1], lh[2]) * (float)ln +
+                            right_area[b + 1] * (float)rn;
+            if (c < best_cost) {
+                best_cost = c;
+                best_axis = a;
+                best_bin = b;
+            }
+        }
+    }
+    uint32_t left = task.count / 2u;
+    uint32_t cb[2][6];  // children's centroid bounds
+    if (best_axis >= 0) {
+        const uint32_t* ab = tb + best_axis * kSahBins * kSahBinWords;
+        for (int s = 0; s < 2; ++s)
+            for (int k = 0; k < 3; ++k) {
+                cb[s][k] = 0xffffffffu;
+                cb[s][3 + k] = 0u;
+            }
+        left = 0u;
+        for (int b = 0; b < kSahBins; ++b) {
+            const uint32_t* w = ab + b * kSahBinWords;
+            const int s = b <= best_bin ? 0 : 1;
+            if (s == 0) left += w[12];
+            for (int k = 0; k < 3; ++k) {
+                cb[s][k] = min(cb[s][k], w[6 + k]);
+                cb[s][3 + k] = max(cb[s][3 + k], w[9 + k]);
+            }
+        }
+    } else {
+        for (int s = 0; s < 2; ++s)
+            for (int k = 0; k < 3; ++k) {
+                cb[s][k] = task.clo[k];
+                cb[s][3 + k] = task.chi[k];
+            }
+    }
+    task.axis = best_axis;
+    task.split_bin = (uint32_t)best_bin;
+    task.left_count = left;
+    const uint32_t counts[2] = {left, task.count - left};
+    int refs[2] = {0, 0};
+    for (int s = 0; s < 2; ++s) {
+        task.child_task[s] = -1;
+        if (counts[s] == 1u) continue;  // a leaf: the scatter writes it
+        const int id = (int)atomicAdd(&ctr->nodes, 1u);
+        if ((uint32_t)id >= lim.nodes) {
+            atomicOr(&ctr->overflow, 1u);
+            continue;
+        }
+        refs[s] = id;
+        node_parent[id] = task.node;
+        const uint32_t first = task.first + (s ? left : 0u);
+        if (counts[s] > kSahSeqMax) {
+            const uint32_t ti = atomicAdd(&ctr->large, 1u);
+            if (ti >= lim.large) {
+                atomicOr(&ctr->overflow, 2u);
+                continue;
+            }
+            SahTask c;
+            c.first = first;
+            c.count = counts[s];
+            c.node = id;
+            c.axis = -1;
+            for (int k = 0; k < 3; ++k) {
+                c.clo[k] = cb[s][k];
+                c.chi[k] = cb[s][3 + k];
+            }
+            c.split_bin = 0u;
+            c.left_count = 0u;
+            c.child_task[0] = c.child_task[1] = -1;
+            next[ti] = c;
+            task.child_task[s] = (int)ti;
+        } else {
+            const uint32_t si = atomicAdd(&ctr->small, 1u);
+            if (si >= lim.small) {
+                atomicOr(&ctr->overflow, 4u);
+                continue;
+            }
+            small[si] = SahSmall{first, counts[s], id};
+        }
+    }
+    if (counts[0] != 1u) children[task.node].x = refs[0];
+    if (counts[1] != 1u) children[task.node].y = refs[1];
+    tasks[t] = task;
+}
+
+__device__ __forceinline__ bool sah_goes_left(const SahTask& task, uint32_t p, const int* ids, const float4* leaf_lo,
+                                              const float4* leaf_hi) {
+    if (task.axis < 0) return p - task.first < task.left_count;
+    const int prim = ids[p];
+    const float3 c = sah_centroid(leaf_lo[prim], leaf_hi[prim]);
+    const float cc = task.axis == 0 ? c.x : task.axis == 1 ? c.y : c.z;
+    const int b = sah_bin(cc, ordered_to_float(task.clo[task.axis]), ordered_to_float(task.chi[task.axis]));
+    return (uint32_t)b <= task.split_bin;
+}
+
+__global__ void k_sah_flags(uint32_t n, const int* __restrict__ ids, const int* __restrict__ task_of,
+                            const SahTask* __restrict__ tasks, const float4* __restrict__ leaf_lo,
+                            const float4* __restrict__ leaf_hi, uint32_t* __restrict__ flags) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n) return;
+    uint32_t f = 0u;
+    if (p < n) {
+        const int t = task_of[p];
+        if (t >= 0) f = sah_goes_left(tasks[t], p, ids, leaf_lo, leaf_hi) ? 1u : 0u;
+    }
+    flags[p] = f;
+}
+
+// Stable partition of every large node's range (rank = left flags before the
+// position, from an exclusive scan), and the leaves of its children.
+__global__ void k_sah_scatter(uint32_t n, const int* __restrict__ ids, const int* __restrict__ task_of,
+                              const SahTask* __restrict__ tasks, const uint32_t* __restrict__ flags,
+                              const uint32_t* __restrict__ rank, int* __restrict__ ids_out,
+                              int* __restrict__ task_of_out, int2* __restrict__ children,
+                              int* __restrict__ leaf_parent, SahCounters* __restrict__ ctr) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int t = task_of[p];
+    const int prim = ids[p];
+    if (t < 0) {
+        ids_out[p] = prim;
+        task_of_out[p] = -1;
+        return;
+    }
+    const SahTask& task = tasks[t];
+    const uint32_t r = rank[p] - rank[task.first];
+    const bool left = flags[p] != 0u;
+    // a left rank past the left count (or a right rank past the right count)
+    // means the flags and the bins disagree: stop before writing
+    if (left ? r >= task.left_count : (p - task.first - r) >= task.count - task.left_count) {
+        atomicOr(&ctr->overflow, 8u);
+        return;
+    }
+    const uint32_t q = left ? task.first + r : task.first + task.left_count + (p - task.first - r);
+    ids_out[q] = prim;
+    const int s = left ? 0 : 1;
+    task_of_out[q] = task.child_task[s];
+    const uint32_t cn = left ? task.left_count : task.count - task.left_count;
+    if (cn == 1u) {
+        if (s == 0) children[task.node].x = ~prim;
+        else children[task.node].y = ~prim;
+        leaf_parent[prim] = task.node;
+    }
+}
+
+// One thread builds the whole subtree of a small node, with the same split
+// rule, partitioning its range of ids in place (stably, through a local copy).
+__global__ void k_sah_small(const uint32_t* __restrict__ count, const SahSmall* __restrict__ small,
+                            int* __restrict__ ids, const float4* __restrict__ leaf_lo,
+                            const float4* __restrict__ leaf_hi, SahCounters* __restrict__ ctr, SahLimits lim,
+                            int2* __restrict__ children, int* __restrict__ node_parent, int* __restrict__ leaf_parent,
+                            float4* __restrict__ node_lo, float4* __restrict__ node_hi) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *count || i >= lim.small) return;
+    const SahSmall root = small[i];
+    if (root.count < 2u || root.count > kSahSeqMax) {
+        atomicOr(&ctr->overflow, 16u);
+        return;
+    }
+    int next_id = root.count > 2u ? (int)atomicAdd(&ctr->nodes, root.count - 2u) : 0;
+    if (root.count > 2u && (uint32_t)next_id + (root.count - 2u) > lim.nodes) {
+        atomicOr(&ctr->overflow, 1u);
+        return;
+    }
+    uint32_t st_first[kSahSeqMax], st_count[kSahSeqMax];
+    int st_node[kSahSeqMax];
+    int sp = 0;
+    st_first[0] = root.first;
+    st_count[0] = root.count;
+    st_node[0] = root.node;
+    sp = 1;
+    int tmp[kSahSeqMax];
+    while (sp > 0) {
+        --sp;
+        const uint32_t first = st_first[sp], cnt = st_count[sp];
+        const int node = st_node[sp];
+        float bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        float cl[3] = {INFINITY, INFINITY, INFINITY}, ch[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const int prim = ids[first + k];
+            const float4 lo = leaf_lo[prim], hi = leaf_hi[prim];
+            const float3 c = sah_centroid(lo, hi);
+            bl[0] = fminf(bl[0], lo.x); bl[1] = fminf(bl[1], lo.y); bl[2] = fminf(bl[2], lo.z);
+            bh[0] = fmaxf(bh[0], hi.x); bh[1] = fmaxf(bh[1], hi.y); bh[2] = fmaxf(bh[2], hi.z);
+            cl[0] = fminf(cl[0], c.x); cl[1] = fminf(cl[1], c.y); cl[2] = fminf(cl[2], c.z);
+            ch[0] = fmaxf(ch[0], c.x); ch[1] = fmaxf(ch[1], c.y); ch[2] = fmaxf(ch[2], c.z);
+        }
+        node_lo[node] = make_float4(bl[0], bl[1], bl[2], 0.0f);
+        node_hi[node] = make_float4(bh[0], bh[1], bh[2], 0.0f);
+        float best_cost = INFINITY;
+        int best_axis = -1, best_bin = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (!(ch[a] - cl[a] > 0.0f)) continue;
+            float lo3[kSahBins][3], hi3[kSahBins][3];
+            uint32_t nb[kSahBins];
+            for (int b = 0; b < kSahBins; ++b) {
+                nb[b] = 0u;
+                for (int k = 0; k < 3; ++k) {
+                    lo3[b][k] = INFINITY;
+                    hi3[b][k] = -INFINITY;
+                }
+            }
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const int prim = ids[first + k];
+                const float4 lo = leaf_lo[prim], hi = leaf_hi[prim];
+                const float3 c = sah_centroid(lo, hi);
+                const float cc = a == 0 ? c.x : a == 1 ? c.y : c.z;
+                const int b = sah_bin(cc, cl[a], ch[a]);
+                nb[b]++;
+                lo3[b][0] = fminf(lo3[b][0], lo.x); lo3[b][1] = fminf(lo3[b][1], lo.y); lo3[b][2] = fminf(lo3[b][2], lo.z);
+                hi3[b][0] = fmaxf(hi3[b][0], hi.x); hi3[b][1] = fmaxf(hi3[b][1], hi.y); hi3[b][2] = fmaxf(hi3[b][2], hi.z);
+            }
+            float right_area[kSahBins];
+            uint32_t right_n[kSahBins];
+            float rl[3] = {INFINITY, INFINITY, INFINITY}, rh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t rn = 0u;
+            for (int b = kSahBins - 1; b >= 1; --b) {
+                for (int k = 0; k < 3; ++k) {
+                    rl[k] = fminf(rl[k], lo3[b][k]);
+                    rh[k] = fmaxf(rh[k], hi3[b][k]);
+                }
+                rn += nb[b];
+                right_area[b] = sah_half_area(rl[0], rl[1], rl[2], rh[0], rh[1], rh[2]);
+                right_n[b] = rn;
+            }
+            float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t ln = 0u;
+            for (int b = 0; b < kSahBins - 1; ++b) {
+                for (int k = 0; k < 3; ++k) {
+                    ll[k] = fminf(ll[k], lo3[b][k]);
+                    lh[k] = fmaxf(lh[k], hi3[b][k]);
+                }
+                ln += nb[b];
+                if (ln == 0u || right_n[b + 1] == 0u) continue;
+                const float c = sah_half_area(ll[0], ll[1], ll[2], lh[0], lh[1], lh[2]) * (float)ln +
+                                right_area[b + 1] * (float)right_n[b + 1];
+                if (c < best_cost) {
+                    best_cost = c;
+                    best_axis = a;
+                    best_bin = b;
+                }
+            }
+        }
+        // stable partition through tmp
+        uint32_t left = 0u;
+        if (best_axis >= 0) {
+            uint32_t r = 0u;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const int prim = ids[first + k];
+                const float3 c = sah_centroid(leaf_lo[prim], leaf_hi[prim]);
+                const float cc = best_axis == 0 ? c.x : best_axis == 1 ? c.y : c.z;
+                if (sah_bin(cc, cl[best_axis], ch[best_axis]) <= best_bin) ids[first + left++] = prim;
+                else tmp[r++] = prim;
+            }
+            for (uint32_t k = 0; k < r; ++k) ids[first + left + k] = tmp[k];
+        } else {
+            left = cnt / 2u;
+        }
+        const uint32_t counts[2] = {left, cnt - left};
+        int refs[2];
+        for (int s = 0; s < 2; ++s) {
+            const uint32_t f = first + (s ? left : 0u);
+            if (counts[s] == 1u) {
+                const int prim = ids[f];
+                refs[s] = ~prim;
+                leaf_parent[prim] = node;
+            } else {
+                const int id = next_id++;
+                refs[s] = id;
+                node_parent[id] = node;
+                st_first[sp] = f;
+                st_count[sp] = counts[s];
+                st_node[sp] = id;
+                ++sp;
+            }
+        }
+        children[node] = make_int2(refs[0], refs[1]);
+    }
+}
+
 template <class T> T* dmalloc(size_t count, cudaStream_t s, cudaError_t* err) {
     void* p = nullptr;
     cudaError_t e = nan_host::scratch_alloc(&p, std::max<size_t>(count, 1) * sizeof(T), s);
@@ -818,6 +1349,100 @@ void free_scene(NanContext* ctx) {
 }
 
 
+int finish_binary(NanContext* ctx, uint32_t n, const float4* tris_sorted, const float4* leaf_lo,
+                  const float4* leaf_hi, int2* children, int* node_parent, int* leaf_parent, float4* node_lo,
+                  float4* node_hi, uint32_t* arrivals, uint32_t* depth, double* sah, const Bounds* bounds,
+                  const int* root_dev, cudaStream_t s);
+
+// Binned-SAH hierarchy over the leaves (kernels k_sah_*): large nodes level by
+// level, one host readback of the next level's node count per level, then
+// the small nodes in one launch; the root is interior node 0.
+int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const float4* leaf_lo,
+                 const float4* leaf_hi, int2* children, int* node_parent, int* leaf_parent, float4* node_lo,
+                 float4* node_hi, uint32_t* arrivals, uint32_t* depth, double* sah, const Bounds* bounds,
+                 cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    const uint32_t max_large = n / (kSahSeqMax + 1u) + 1u;
+    const SahLimits lim{max_large, n / 2u + 1u, n - 1u};
+    int* ids_a = dmalloc<int>(n, s, &err);
+    int* ids_b = dmalloc<int>(n, s, &err);
+    int* task_a = dmalloc<int>(n, s, &err);
+    int* task_b = dmalloc<int>(n, s, &err);
+    uint32_t* flags = dmalloc<uint32_t>(n + 1, s, &err);
+    uint32_t* rank = dmalloc<uint32_t>(n + 1, s, &err);
+    SahTask* level_a = dmalloc<SahTask>(max_large, s, &err);
+    SahTask* level_b = dmalloc<SahTask>(max_large, s, &err);
+    SahSmall* small = dmalloc<SahSmall>(n / 2u + 1u, s, &err);
+    uint32_t* bins = dmalloc<uint32_t>((size_t)max_large * kSahTaskWords, s, &err);
+    SahCounters* ctr = dmalloc<SahCounters>(1, s, &err);
+    int* root_dev = dmalloc<int>(1, s, &err);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags, rank, n + 1, s);
+    void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "binned SAH scratch allocation");
+    cudaMemsetAsync(root_dev, 0, sizeof(int), s);
+    cudaMemsetAsync(node_parent, 0xff, (n - 1u) * sizeof(int), s);  // the root's parent stays -1
+    k_sah_init<<<blocks(n), kThreads, 0, s>>>(n, ids_a, task_a, n > kSahSeqMax ? 0 : -1);
+    k_sah_root<<<1, 1, 0, s>>>(n, bounds, level_a, small, ctr);
+    ctx->launches += 2;
+    uint32_t large = n > kSahSeqMax ? 1u : 0u;
+    int levels = 0;
+    const uint32_t bin_grid = (uint32_t)((n + kThreads * kSahBinPerThread - 1) / (kThreads * kSahBinPerThread));
+    while (large > 0u) {
+        if (++levels > kSahMaxLevels) {
+            set_error("binned SAH build did not terminate");
+            return NAN_ERR_LIMIT;
+        }
+        const uint32_t words = large * (uint32_t)kSahTaskWords;
+        k_sah_bins_reset<<<blocks(words), kThreads, 0, s>>>(words, bins);
+        k_sah_bin<<<bin_grid, kThreads, 0, s>>>(n, ids_a, task_a, level_a, leaf_lo, leaf_hi, bins);
+        k_sah_split<<<blocks(large), kThreads, 0, s>>>(&ctr->level, level_a, bins, level_b, small, ctr, lim, children,
+                                                       node_parent, node_lo, node_hi);
+        k_sah_flags<<<blocks(n + 1), kThreads, 0, s>>>(n, ids_a, task_a, level_a, leaf_lo, leaf_hi, flags);
+        cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, flags, rank, n + 1, s);
+        k_sah_scatter<<<blocks(n), kThreads, 0, s>>>(n, ids_a, task_a, level_a, flags, rank, ids_b, task_b, children,
+                                                     leaf_parent, ctr);
+        ctx->launches += 6;
+        // the next level's count becomes the current one
+        SahCounters lc{};
+        cudaMemcpyAsync(&ctr->level, &ctr->large, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        err = cudaMemcpyAsync(&lc, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
+        if (err == cudaSuccess) err = cudaMemsetAsync(&ctr->large, 0, sizeof(uint32_t), s);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+        if (err != cudaSuccess) return cuda_fail(err, "binned SAH level");
+        large = lc.large;
+        if (lc.overflow != 0u || large > max_large) {
+            set_error("binned SAH build exceeded a bound of its node lists");
+            return NAN_ERR_LIMIT;
+        }
+        std::swap(ids_a, ids_b);
+        std::swap(task_a, task_b);
+        std::swap(level_a, level_b);
+    }
+    SahCounters c{};
+    err = cudaMemcpyAsync(&c, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "binned SAH counters");
+    if (c.small > 0u) {
+        k_sah_small<<<(c.small + 127u) / 128u, 128, 0, s>>>(&ctr->small, small, ids_a, leaf_lo, leaf_hi, ctr, lim,
+                                                             children, node_parent, leaf_parent, node_lo, node_hi);
+        ctx->launches++;
+    }
+    err = cudaMemcpyAsync(&c, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "binned SAH small nodes");
+    if (c.overflow != 0u || c.nodes != n - 1u) {
+        set_error("binned SAH build made the wrong number of interior nodes");
+        return NAN_ERR_LIMIT;
+    }
+    const int rc = finish_binary(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent, node_lo,
+                                 node_hi, arrivals, depth, sah, bounds, root_dev, s);
+    for (void* p : {(void*)ids_a, (void*)ids_b, (void*)task_a, (void*)task_b, (void*)flags, (void*)rank,
+                    (void*)level_a, (void*)level_b, (void*)small, (void*)bins, (void*)ctr, (void*)root_dev, scan_tmp})
+        cudaFreeAsync(p, s);
+    return rc;
+}
+
 // PLOC hierarchy over the Morton-sorted leaves, SAH leaf collapse, and a
 // depth-first emission of nodes and triangles (see the kernels above).
 int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const float4* leaf_lo, const float4* leaf_hi,
@@ -836,10 +1461,6 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     uint32_t* pos = dmalloc<uint32_t>(n + 1, s, &err);
     // [0] interior nodes made; [1], [2] live clusters (double-buffered)
     uint32_t* counter = dmalloc<uint32_t>(3, s, &err);
-    SubtreeInfo* info = dmalloc<SubtreeInfo>(interior, s, &err);
-    int* dfs = dmalloc<int>(interior, s, &err);
-    uint32_t* tri_off = dmalloc<uint32_t>(interior, s, &err);
-    uint32_t* tri_pos = dmalloc<uint32_t>(n, s, &err);
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, valid, pos, n + 1, s);
     void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
@@ -888,8 +1509,32 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
         }
         c = next;
     }
+    const int rc = finish_binary(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent, node_lo,
+                                 node_hi, arrivals, depth, sah, bounds, idx_a, s);
+    for (void* p : {(void*)idx_a, (void*)idx_b, (void*)lo_a, (void*)hi_a, (void*)lo_b, (void*)hi_b, (void*)nn,
+                    (void*)valid, (void*)pos, (void*)counter, scan_tmp})
+        cudaFreeAsync(p, s);
+    return rc;
+}
+
+// SAH leaf collapse, depth-first emission of nodes and triangles, and the
+// compressed 8-wide conversion of a binary hierarchy over the n leaves
+// (children / parents / interior boxes; root_dev[0] is the root's index).
+int finish_binary(NanContext* ctx, uint32_t n, const float4* tris_sorted, const float4* leaf_lo,
+                  const float4* leaf_hi, int2* children, int* node_parent, int* leaf_parent, float4* node_lo,
+                  float4* node_hi, uint32_t* arrivals, uint32_t* depth, double* sah, const Bounds* bounds,
+                  const int* root_dev, cudaStream_t s) {
+    cudaError_t err = cudaSuccess;
+    const uint32_t interior = n - 1;
+    SubtreeInfo* info = dmalloc<SubtreeInfo>(interior, s, &err);
+    int* dfs = dmalloc<int>(interior, s, &err);
+    uint32_t* tri_off = dmalloc<uint32_t>(interior, s, &err);
+    uint32_t* tri_pos = dmalloc<uint32_t>(n, s, &err);
+    if (err != cudaSuccess) return cuda_fail(err, "BVH collapse scratch allocation");
     int root = 0;
-    cudaMemcpyAsync(&root, idx_a, sizeof(int), cudaMemcpyDeviceToHost, s);
+    err = cudaMemcpyAsync(&root, root_dev, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    if (err != cudaSuccess) return cuda_fail(err, "BVH root readback");
     cudaMemsetAsync(arrivals, 0, interior * sizeof(uint32_t), s);
     k_subtree<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, leaf_lo, leaf_hi, node_lo, node_hi,
                                             info, arrivals);
@@ -897,7 +1542,7 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     k_dfs_leaves<<<blocks(n), kThreads, 0, s>>>(n, children, node_parent, leaf_parent, info, tri_pos);
     k_scatter_tris<<<blocks(n), kThreads, 0, s>>>(n, tri_pos, tris_sorted, ctx->tris);
     err = cudaGetLastError();
-    if (err != cudaSuccess) return cuda_fail(err, "PLOC collapse");
+    if (err != cudaSuccess) return cuda_fail(err, "BVH collapse");
 
     // compressed 8-wide BVH from the collapsed binary tree, level by level
     if (ctx->wide_capacity < n) {
@@ -922,7 +1567,7 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     {
         // the root item: the binary root; levels run in batches of
         // kWideBatch without the host, each grid bounded by 8x the last
-        k_wide_root<<<1, 1, 0, s>>>(idx_a, items_a);
+        k_wide_root<<<1, 1, 0, s>>>(root_dev, items_a);
         cudaMemsetAsync(wcount, 0, (2 + kWideMaxLevels + 1) * sizeof(uint32_t), s);
         const uint32_t init[3] = {1u, 0u, 1u};
         cudaMemcpyAsync(wcount, init, sizeof(init), cudaMemcpyHostToDevice, s);
@@ -967,11 +1612,8 @@ int build_ploc(NanContext* ctx, uint32_t n, const float4* tris_sorted, const flo
     if (err == cudaSuccess) err = cudaMemcpyAsync(&max_depth, depth, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaMemcpyAsync(&sah_host, sah, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    if (err != cudaSuccess) return cuda_fail(err, "PLOC emit");
-    for (void* p : {(void*)idx_a, (void*)idx_b, (void*)lo_a, (void*)hi_a, (void*)lo_b, (void*)hi_b, (void*)nn,
-                    (void*)valid, (void*)pos, (void*)counter, (void*)info, (void*)dfs, (void*)tri_off, (void*)tri_pos,
-                    scan_tmp})
-        cudaFreeAsync(p, s);
+    if (err != cudaSuccess) return cuda_fail(err, "BVH emit");
+    for (void* p : {(void*)info, (void*)dfs, (void*)tri_off, (void*)tri_pos}) cudaFreeAsync(p, s);
     if (root_info.collapsed) {  // the whole scene is one leaf
         ctx->root = ~(int)(n - 1u);
         ctx->node_count = 0;
@@ -1098,8 +1740,10 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
     void* sort_tmp = dmalloc<uint8_t>(sort_bytes, s, &err);
     if (err != cudaSuccess) return cuda_fail(err, "scene build sort allocation");
     cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys_sorted, vals, order, (int)n, 0, 63, s);
-    const bool use_ploc = ctx->tuning.bvh_builder == 0 && n > 1;
-    float4* tris_sorted = use_ploc ? dmalloc<float4>(3ull * n, s, &err) : ctx->tris;
+    // NanTuning.bvh_builder: 0 binned SAH, 1 LBVH, 2 PLOC
+    const bool use_sah = ctx->tuning.bvh_builder == 0 && n > 1;
+    const bool use_ploc = ctx->tuning.bvh_builder == 2 && n > 1;
+    float4* tris_sorted = (use_sah || use_ploc) ? dmalloc<float4>(3ull * n, s, &err) : ctx->tris;
     if (err != cudaSuccess) return cuda_fail(err, "scene build scratch allocation");
     k_gather_leaves<<<blocks(n), kThreads, 0, s>>>(order, n, tris_flat, lo_flat, hi_flat, tris_sorted, leaf_lo, leaf_hi);
     ctx->launches += 4;
@@ -1109,9 +1753,11 @@ int build_scene(NanContext* ctx, const NanSceneDesc* sd, cudaStream_t s) {
         ctx->leaf_count = 1;
         ctx->max_depth = 1;
         ctx->sah_cost = 1.0;
-    } else if (use_ploc) {
-        int rc = build_ploc(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent, node_lo, node_hi,
-                            arrivals, depth, sah, bounds, s);
+    } else if (use_sah || use_ploc) {
+        int rc = use_sah ? build_binned(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent,
+                                        node_lo, node_hi, arrivals, depth, sah, bounds, s)
+                         : build_ploc(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent,
+                                      node_lo, node_hi, arrivals, depth, sah, bounds, s);
         cudaFreeAsync(tris_sorted, s);
         if (rc != NAN_OK) return rc;
     } else {

@@ -172,7 +172,7 @@ class Scene:
     """Scene buffers on the GPU + BVH (replaces Scene.__init__/bind)."""
 
     def __init__(self, device: Device, scene_node: SceneNode, lighting: Lighting | None = None, stream=None,
-                 bvh_builder: str = "ploc"):
+                 bvh_builder: str = "sah"):
         import torch
 
         self.device = device

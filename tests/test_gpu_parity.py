@@ -11,7 +11,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _build(device, node, bvh_builder="ploc"):
+def _build(device, node, bvh_builder="sah"):
     import nan_b200
 
     scene = nan_b200.Scene(device, node, bvh_builder=bvh_builder)
@@ -63,7 +63,14 @@ def terrain_lbvh(device):
     return _build(device, scenes.terrain_boxes(seed=1, grid=129, boxes=120), bvh_builder="lbvh")
 
 
-@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
+@pytest.fixture(scope="module")
+def terrain_ploc(device):
+    from nan_b200 import scenes
+
+    return _build(device, scenes.terrain_boxes(seed=1, grid=129, boxes=120), bvh_builder="ploc")
+
+
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh", "terrain_ploc"])
 def test_bvh_world_triangles_match_oracle(which, request):
     scene, orc = request.getfixturevalue(which)
     np.testing.assert_array_equal(scene.world_triangles().cpu().numpy(), orc.world_triangles())
@@ -72,10 +79,12 @@ def test_bvh_world_triangles_match_oracle(which, request):
     assert info["max_depth"] <= 96
     if scene.bvh_builder == "ploc":  # SAH quality close to the binned-SAH reference
         assert info["sah_cost"] <= 1.25 * orc.bvh_stats()["sah_cost"], (info["sah_cost"], orc.bvh_stats())
+    if scene.bvh_builder == "sah":
+        assert info["sah_cost"] <= 1.05 * orc.bvh_stats()["sah_cost"], (info["sah_cost"], orc.bvh_stats())
 
 
 @pytest.mark.parametrize("width", [2, 8])
-@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh", "terrain_ploc"])
 def test_closest_hit_bit_exact_vs_oracle(which, width, request):
     import torch
 
@@ -118,7 +127,7 @@ def test_closest_hit_vs_fp64_bruteforce(which, request):
 
 
 @pytest.mark.parametrize("width", [2, 8])
-@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh"])
+@pytest.mark.parametrize("which", ["cornell", "terrain", "terrain_lbvh", "terrain_ploc"])
 def test_any_hit_bit_exact_vs_oracle(which, width, request):
     import torch
 

@@ -49,8 +49,8 @@ def test_rebuild_reuses_storage_and_matches_fresh_builds(device):
     small = nan_b200.Scene(device, scenes.cornell_box(32, 32))
     large = nan_b200.Scene(device, scenes.terrain_boxes(seed=3, grid=161, boxes=120))
     ctx = device.new_context()
-    for scene, builder, width in ((mid, "ploc", 8), (small, "ploc", 2), (large, "ploc", 8), (mid, "lbvh", 8),
-                                  (large, "lbvh", 2)):
+    for scene, builder, width in ((mid, "sah", 8), (small, "sah", 2), (large, "sah", 2), (mid, "ploc", 8),
+                                  (small, "ploc", 2), (large, "ploc", 8), (mid, "lbvh", 8), (large, "lbvh", 2)):
         ctx.configure(bvh_builder=builder, bvh_width=width)
         _native.check(_native.lib().nan_scene_build(ctx.handle, ctypes.byref(scene._desc),
                                                     _native.stream_handle(None)))

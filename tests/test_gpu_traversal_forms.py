@@ -10,7 +10,7 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("builder", ["ploc", "lbvh"])
+@pytest.mark.parametrize("builder", ["sah", "ploc", "lbvh"])
 def test_traversal_forms_do_not_change_results(device, builder):
     import torch
 
