@@ -8,9 +8,15 @@
 //   2. flatten: transform every triangle to world space, write its box,
 //   3. scene bounds of the centroids (block reduction + ordered-int atomics),
 //   4. 63-bit Morton codes of the centroids, radix sort (CUB),
-//   5. hierarchy from the sorted codes (Karras 2012, "Maximizing parallelism
-//      in the construction of BVHs, octrees, and k-d trees"),
-//   6. bottom-up box refit with one atomic arrival counter per node,
+//   5. a binary hierarchy over the sorted triangles, by one of three builders
+//      (NanTuning.bvh_builder):
+//      0. top-down binned SAH (k_sah_*, the default),
+//      1. LBVH from the sorted codes (Karras 2012, "Maximizing parallelism in
+//         the construction of BVHs, octrees, and k-d trees") with a
+//         bottom-up box refit (one atomic arrival counter per node),
+//      2. PLOC clustering (k_ploc_*),
+//   6. for 0 and 2: SAH leaf collapse (up to 3 triangles per leaf), depth-first
+//      placement and the compressed 8-wide conversion,
 //   7. emission of 64-byte two-box nodes and leaf-ordered triangles.
 #include <cub/cub.cuh>
 
