@@ -3172,3 +3172,238 @@ int oracle_trace_probes_independent(void* sp, const OracleLighting* lighting, fl
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Restatement of this library's default BVH builder (nan_bvh.cu, k_sah_* and
+// the collapse/emission that follow it). This is the library's own
+// algorithm, not the reference's: the reference leaves the BVH to the
+// driver. It pins the GPU builder's tree through its node count and SAH cost.
+//   * top-down binned SAH: 32 bins of each node's centroid bounds per axis,
+//     cost = left half-area x left count + right half-area x right count,
+//     the first minimum over axes 0..2 and bins 0..30; a node whose
+//     centroids coincide on every axis halves its range; split down to
+//     single triangles; stable partitions;
+//   * bottom-up collapse (k_subtree): a subtree of at most 3 triangles becomes
+//     one leaf when tris <= 1 + (aa ca + ab cb) / ap (C_trav = C_int = 1);
+//   * cost sum (k_emit_dfs): per kept interior node its half-area / the
+//     root's, plus each leaf child's half-area / the root's x its triangles.
+// ===========================================================================
+namespace {
+
+struct SahBox {
+    float lo[3], hi[3];
+};
+
+float sah_half_area_f(float lx, float ly, float lz, float hx, float hy, float hz) {
+    const float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    if (!(dx >= 0.0f)) return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+float sah_half_area4(const SahBox& b) {  // half_area4: no empty-box test
+    const float x = b.hi[0] - b.lo[0], y = b.hi[1] - b.lo[1], z = b.hi[2] - b.lo[2];
+    return x * y + y * z + z * x;
+}
+
+int sah_bin_of(float c, float lo, float hi) {
+    const float ext = hi - lo;
+    if (!(ext > 0.0f)) return 0;
+    const float scale = 32.0f / ext;
+    const int b = (int)((c - lo) * scale);
+    return std::min(std::max(b, 0), 31);
+}
+
+}  // namespace
+
+extern "C" {
+
+// tris9: n world triangles (9 floats each, the flattened order). out3 =
+// (kept interior nodes, unused, SAH cost).
+int oracle_sah_build_stats(const float* tris9, uint32_t n, double* out3) {
+    out3[0] = out3[1] = out3[2] = 0.0;
+    if (n == 0) return 0;
+    std::vector<SahBox> box(n);
+    std::vector<float> cent(3 * (size_t)n);
+    for (uint32_t t = 0; t < n; ++t) {
+        for (int a = 0; a < 3; ++a) {
+            const float v0 = tris9[9 * (size_t)t + a], v1 = tris9[9 * (size_t)t + 3 + a], v2 = tris9[9 * (size_t)t + 6 + a];
+            box[t].lo[a] = std::min(std::min(v0, v1), v2);
+            box[t].hi[a] = std::max(std::max(v0, v1), v2);
+            cent[3 * (size_t)t + a] = 0.5f * (box[t].lo[a] + box[t].hi[a]);
+        }
+    }
+    if (n == 1) {
+        out3[2] = 1.0;
+        return 0;
+    }
+    // binary tree down to single triangles: child refs, >= 0 interior, ~t leaf
+    std::vector<std::array<int, 2>> child;
+    std::vector<SahBox> nbox;
+    std::vector<uint32_t> ids(n);
+    for (uint32_t i = 0; i < n; ++i) ids[i] = i;
+    child.reserve(n - 1);
+    nbox.reserve(n - 1);
+    struct Item {
+        uint32_t first, count;
+        int node;
+    };
+    child.push_back({0, 0});
+    nbox.push_back(SahBox{});
+    std::vector<Item> stack{{0u, n, 0}};
+    std::vector<uint32_t> tmp;
+    while (!stack.empty()) {
+        const Item it = stack.back();
+        stack.pop_back();
+        SahBox b, cb;
+        for (int a = 0; a < 3; ++a) {
+            b.lo[a] = cb.lo[a] = INFINITY;
+            b.hi[a] = cb.hi[a] = -INFINITY;
+        }
+        for (uint32_t k = 0; k < it.count; ++k) {
+            const uint32_t p = ids[it.first + k];
+            for (int a = 0; a < 3; ++a) {
+                b.lo[a] = std::min(b.lo[a], box[p].lo[a]);
+                b.hi[a] = std::max(b.hi[a], box[p].hi[a]);
+                cb.lo[a] = std::min(cb.lo[a], cent[3 * (size_t)p + a]);
+                cb.hi[a] = std::max(cb.hi[a], cent[3 * (size_t)p + a]);
+            }
+        }
+        nbox[it.node] = b;
+        float best_cost = INFINITY;
+        int best_axis = -1, best_bin = 0;
+        for (int a = 0; a < 3; ++a) {
+            if (!(cb.hi[a] - cb.lo[a] > 0.0f)) continue;
+            SahBox bins[32];
+            uint32_t nb[32] = {0};
+            for (auto& x : bins)
+                for (int k = 0; k < 3; ++k) {
+                    x.lo[k] = INFINITY;
+                    x.hi[k] = -INFINITY;
+                }
+            for (uint32_t k = 0; k < it.count; ++k) {
+                const uint32_t p = ids[it.first + k];
+                const int bi = sah_bin_of(cent[3 * (size_t)p + a], cb.lo[a], cb.hi[a]);
+                nb[bi]++;
+                for (int q = 0; q < 3; ++q) {
+                    bins[bi].lo[q] = std::min(bins[bi].lo[q], box[p].lo[q]);
+                    bins[bi].hi[q] = std::max(bins[bi].hi[q], box[p].hi[q]);
+                }
+            }
+            float right_area[32];
+            uint32_t right_n[32];
+            float rl[3] = {INFINITY, INFINITY, INFINITY}, rh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t rn = 0;
+            for (int bi = 31; bi >= 1; --bi) {
+                for (int q = 0; q < 3; ++q) {
+                    rl[q] = std::min(rl[q], bins[bi].lo[q]);
+                    rh[q] = std::max(rh[q], bins[bi].hi[q]);
+                }
+                rn += nb[bi];
+                right_area[bi] = sah_half_area_f(rl[0], rl[1], rl[2], rh[0], rh[1], rh[2]);
+                right_n[bi] = rn;
+            }
+            float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+            uint32_t ln = 0;
+            for (int bi = 0; bi < 31; ++bi) {
+                for (int q = 0; q < 3; ++q) {
+                    ll[q] = std::min(ll[q], bins[bi].lo[q]);
+                    lh[q] = std::max(lh[q], bins[bi].hi[q]);
+                }
+                ln += nb[bi];
+                if (ln == 0 || right_n[bi + 1] == 0) continue;
+                const float c = sah_half_area_f(ll[0], ll[1], ll[2], lh[0], lh[1], lh[2]) * (float)ln +
+                                right_area[bi + 1] * (float)right_n[bi + 1];
+                if (c < best_cost) {
+                    best_cost = c;
+                    best_axis = a;
+                    best_bin = bi;
+                }
+            }
+        }
+        uint32_t left = it.count / 2;
+        if (best_axis >= 0) {
+            tmp.clear();
+            left = 0;
+            for (uint32_t k = 0; k < it.count; ++k) {
+                const uint32_t p = ids[it.first + k];
+                if (sah_bin_of(cent[3 * (size_t)p + best_axis], cb.lo[best_axis], cb.hi[best_axis]) <= best_bin)
+                    ids[it.first + left++] = p;
+                else
+                    tmp.push_back(p);
+            }
+            for (size_t k = 0; k < tmp.size(); ++k) ids[it.first + left + k] = tmp[k];
+        }
+        const uint32_t counts[2] = {left, it.count - left};
+        for (int s = 0; s < 2; ++s) {
+            const uint32_t f = it.first + (s ? left : 0u);
+            if (counts[s] == 1) {
+                child[it.node][s] = ~(int)ids[f];
+            } else {
+                const int id = (int)child.size();
+                child.push_back({0, 0});
+                nbox.push_back(SahBox{});
+                child[it.node][s] = id;
+                stack.push_back({f, counts[s], id});
+            }
+        }
+    }
+    // collapse, bottom-up (children have larger ids than their parent)
+    const size_t m = child.size();
+    std::vector<uint32_t> tris(m);
+    std::vector<float> cost(m);
+    std::vector<char> collapsed(m);
+    for (size_t i = m; i-- > 0;) {
+        uint32_t t2[2];
+        float c2[2], a2[2];
+        for (int s = 0; s < 2; ++s) {
+            const int c = child[i][s];
+            if (c < 0) {
+                t2[s] = 1;
+                c2[s] = 1.0f;
+                a2[s] = sah_half_area4(box[~c]);
+            } else {
+                t2[s] = tris[c];
+                c2[s] = cost[c];
+                a2[s] = sah_half_area4(nbox[c]);
+            }
+        }
+        const float ap = std::max(sah_half_area4(nbox[i]), 1e-30f);
+        const float split = 1.0f + (a2[0] * c2[0] + a2[1] * c2[1]) / ap;
+        tris[i] = t2[0] + t2[1];
+        if (tris[i] <= 3u && (float)tris[i] <= split) {
+            cost[i] = (float)tris[i];
+            collapsed[i] = 1;
+        } else {
+            cost[i] = split;
+            collapsed[i] = 0;
+        }
+    }
+    if (collapsed[0]) {
+        out3[2] = (double)n;
+        return 0;
+    }
+    const float root_area = std::max(sah_half_area4(nbox[0]), 1e-30f);
+    double sah = 0.0, kept = 0.0;
+    std::vector<int> walk{0};
+    while (!walk.empty()) {
+        const int i = walk.back();
+        walk.pop_back();
+        kept += 1.0;
+        sah += (double)(sah_half_area4(nbox[i]) / root_area);
+        for (int s = 0; s < 2; ++s) {
+            const int c = child[i][s];
+            if (c < 0) {
+                sah += (double)(sah_half_area4(box[~c]) / root_area) * 1.0;
+            } else if (collapsed[c]) {
+                sah += (double)(sah_half_area4(nbox[c]) / root_area) * (double)tris[c];
+            } else {
+                walk.push_back(c);
+            }
+        }
+    }
+    out3[0] = kept;
+    out3[2] = sah;
+    return 0;
+}
+
+}  // extern "C"

@@ -127,6 +127,7 @@ def _declare(l: ctypes.CDLL) -> None:
     l.oracle_scene_triangle_count.argtypes = [vp]
     l.oracle_scene_world_triangles.argtypes = [vp, vp]
     l.oracle_scene_bvh_stats.argtypes = [vp, vp]
+    l.oracle_sah_build_stats.argtypes = [vp, ctypes.c_uint32, vp]
     l.oracle_intersect.argtypes = [vp, vp, i, i, vp, vp, vp]
     l.oracle_visibility.argtypes = [vp, vp, i, i, vp, vp]
     l.oracle_trace_screen.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, i, i, i, vp, vp]
@@ -276,6 +277,16 @@ def estimate_support(reference_positions, reference_normals, reference_instances
     if rc != 0:
         raise RuntimeError("support estimate: an instance index is out of range")
     return f, m
+
+
+def sah_build_stats(world_triangles) -> dict:
+    """The library's default BVH builder (binned SAH, 32 bins, then the SAH
+    leaf collapse of up to 3 triangles) restated on the CPU: its kept interior
+    node count and SAH cost for world triangles f32[T, 9] in flattened order."""
+    w = np.ascontiguousarray(world_triangles, dtype=np.float32).reshape(-1, 9)
+    out = np.zeros(3, np.float64)
+    lib().oracle_sah_build_stats(_p(w), w.shape[0], _p(out))
+    return {"nodes": int(out[0]), "sah_cost": float(out[2])}
 
 
 def own_exp(x: float) -> float:

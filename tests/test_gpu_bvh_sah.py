@@ -6,8 +6,9 @@ cover the builder's own paths: scenes of 2 to 66 triangles around the size
 where one thread builds a whole subtree (64), larger random soups that split
 level by level first, triangles whose centroids coincide (no binned split
 exists, so the range is halved), and the test scenes, where a second build
-must reproduce the tree and its SAH cost must stay within 5 % of the oracle's
-binned-SAH tree (and below PLOC's on the terrain).
+must reproduce the tree, the CPU restatement of the builder must give the same
+node count and SAH cost, and that cost must stay within 5 % of the oracle's
+8-bin binned-SAH tree (and below PLOC's on the terrain).
 """
 
 import numpy as np
@@ -116,5 +117,10 @@ def test_sah_cost_and_repeatability(device, which):
     # the oracle's binned tree: 8 bins, leaves of any size; this one: 32 bins,
     # leaves of at most 3 triangles
     assert a["sah_cost"] <= 1.05 * orc.bvh_stats()["sah_cost"], (a, orc.bvh_stats())
+    # the CPU restatement of this builder makes the same tree
+    from oracle.oracle import sah_build_stats
+
+    r = sah_build_stats(orc.world_triangles())
+    assert r["nodes"] == a["node_count"] and abs(r["sah_cost"] - a["sah_cost"]) <= 1e-9 * r["sah_cost"], (r, a)
     print(which, "sah", a["sah_cost"], "ploc", p["sah_cost"], "oracle binned", orc.bvh_stats()["sah_cost"])
     device.check()
