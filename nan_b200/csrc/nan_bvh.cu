@@ -595,9 +595,10 @@ __global__ void k_emit_dfs(uint32_t interior, const int2* __restrict__ children,
 // ---------------------------------------------------------------------------
 // Compressed 8-wide BVH (after Ylitie, Karras and Laine, "Efficient Incoherent
 // Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017), converted
-// top-down from the PLOC tree: each wide node takes up to 8 subtrees by
-// repeatedly opening the largest-area interior binary node, places them in
-// slots ordered by octant direction, stores its interior children
+// top-down from the collapsed binary tree (binned SAH or PLOC): each wide
+// node takes up to 8 subtrees by repeatedly opening the largest-area interior
+// binary node, places them in slots ordered by octant direction, stores its
+// interior children
 // contiguously (child_base) and its leaf triangles contiguously (tri_base),
 // and quantizes the children's boxes to 8 bits against the node's box.
 // Node (80 B): w0 = (p.xyz, e.x | e.y << 8 | e.z << 16 | imask << 24)

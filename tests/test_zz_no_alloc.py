@@ -4,8 +4,8 @@ Some callers may not call cudaMalloc at all -- code living inside another
 framework's memory pool, or a real-time loop with an allocation ban. This
 entry point builds an LBVH (binary nodes, whatever the context's tuning asks)
 from a fixed scratch array in device memory and writes it into buffers the
-caller already owns. Its tree differs from nan_scene_build's default PLOC
-tree, but the hits do not: the closest hit is chosen by (t, flat index) in
+caller already owns. Its tree differs from nan_scene_build's default
+binned-SAH tree, but the hits do not: the closest hit is chosen by (t, flat index) in
 any tree. The test calls it through the C ABI twice in a row on one context
 (a larger scene first, then a smaller one, so the second call starts from the
 first call's leftover scratch) and checks each result against
