@@ -1386,7 +1386,23 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
     size_t scan_bytes = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, flags, rank, n + 1, s);
     void* scan_tmp = dmalloc<uint8_t>(scan_bytes, s, &err);
-    if (err != cudaSuccess) return cuda_fail(err, "binned SAH scratch allocation");
+    auto release = [&] {
+        for (void* p : {(void*)ids_a, (void*)ids_b, (void*)task_a, (void*)task_b, (void*)flags, (void*)rank,
+                        (void*)level_a, (void*)level_b, (void*)small, (void*)bins, (void*)ctr, (void*)root_dev,
+                        scan_tmp})
+            if (p) cudaFreeAsync(p, s);
+    };
+    // every exit releases the scratch
+    auto fail = [&](cudaError_t e, const char* what) {
+        release();
+        return cuda_fail(e, what);
+    };
+    auto limit = [&](const char* what) {
+        release();
+        set_error(what);
+        return NAN_ERR_LIMIT;
+    };
+    if (err != cudaSuccess) return fail(err, "binned SAH scratch allocation");
     cudaMemsetAsync(root_dev, 0, sizeof(int), s);
     cudaMemsetAsync(node_parent, 0xff, (n - 1u) * sizeof(int), s);  // the root's parent stays -1
     k_sah_init<<<blocks(n), kThreads, 0, s>>>(n, ids_a, task_a, n > kSahSeqMax ? 0 : -1);
@@ -1396,10 +1412,7 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
     int levels = 0;
     const uint32_t bin_grid = (uint32_t)((n + kThreads * kSahBinPerThread - 1) / (kThreads * kSahBinPerThread));
     while (large > 0u) {
-        if (++levels > kSahMaxLevels) {
-            set_error("binned SAH build did not terminate");
-            return NAN_ERR_LIMIT;
-        }
+        if (++levels > kSahMaxLevels) return limit("binned SAH build did not terminate");
         const uint32_t words = large * (uint32_t)kSahTaskWords;
         k_sah_bins_reset<<<blocks(words), kThreads, 0, s>>>(words, bins);
         k_sah_bin<<<bin_grid, kThreads, 0, s>>>(n, ids_a, task_a, level_a, leaf_lo, leaf_hi, bins);
@@ -1416,12 +1429,9 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
         err = cudaMemcpyAsync(&lc, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
         if (err == cudaSuccess) err = cudaMemsetAsync(&ctr->large, 0, sizeof(uint32_t), s);
         if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-        if (err != cudaSuccess) return cuda_fail(err, "binned SAH level");
+        if (err != cudaSuccess) return fail(err, "binned SAH level");
         large = lc.large;
-        if (lc.overflow != 0u || large > max_large) {
-            set_error("binned SAH build exceeded a bound of its node lists");
-            return NAN_ERR_LIMIT;
-        }
+        if (lc.overflow != 0u || large > max_large) return limit("binned SAH build exceeded a bound of its node lists");
         std::swap(ids_a, ids_b);
         std::swap(task_a, task_b);
         std::swap(level_a, level_b);
@@ -1429,7 +1439,7 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
     SahCounters c{};
     err = cudaMemcpyAsync(&c, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    if (err != cudaSuccess) return cuda_fail(err, "binned SAH counters");
+    if (err != cudaSuccess) return fail(err, "binned SAH counters");
     if (c.small > 0u) {
         k_sah_small<<<(c.small + 127u) / 128u, 128, 0, s>>>(&ctr->small, small, ids_a, leaf_lo, leaf_hi, ctr, lim,
                                                              children, node_parent, leaf_parent, node_lo, node_hi);
@@ -1437,16 +1447,11 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
     }
     err = cudaMemcpyAsync(&c, ctr, sizeof(SahCounters), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
-    if (err != cudaSuccess) return cuda_fail(err, "binned SAH small nodes");
-    if (c.overflow != 0u || c.nodes != n - 1u) {
-        set_error("binned SAH build made the wrong number of interior nodes");
-        return NAN_ERR_LIMIT;
-    }
+    if (err != cudaSuccess) return fail(err, "binned SAH small nodes");
+    if (c.overflow != 0u || c.nodes != n - 1u) return limit("binned SAH build made the wrong number of interior nodes");
     const int rc = finish_binary(ctx, n, tris_sorted, leaf_lo, leaf_hi, children, node_parent, leaf_parent, node_lo,
                                  node_hi, arrivals, depth, sah, bounds, root_dev, s);
-    for (void* p : {(void*)ids_a, (void*)ids_b, (void*)task_a, (void*)task_b, (void*)flags, (void*)rank,
-                    (void*)level_a, (void*)level_b, (void*)small, (void*)bins, (void*)ctr, (void*)root_dev, scan_tmp})
-        cudaFreeAsync(p, s);
+    release();
     return rc;
 }
 
