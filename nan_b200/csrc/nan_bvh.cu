@@ -978,91 +978,103 @@ __global__ void __launch_bounds__(kThreads) k_sah_bin(uint32_t n, const int* __r
     }
 }
 
-// One thread per large node: its box (the union of its bins on axis 0), the
-// best split, and the children: interior ids, next-level or small tasks.
-__global__ void k_sah_split(const uint32_t* __restrict__ count, SahTask* __restrict__ tasks,
+// One warp per large node, lane b holding bin b of each axis: the node's box
+// (the union of its axis-0 bins), the best split (left and right sweeps as
+// warp scans of the bins' ordered-int boxes and counts; the first minimum over
+// axes 0..2, then bins 0..30), and the children, which lane 0 allocates:
+// interior ids, next-level or small tasks.
+static_assert(kSahBins == 32, "one bin per lane");
+__global__ void __launch_bounds__(128) k_sah_split(const uint32_t* __restrict__ count, SahTask* __restrict__ tasks,
                             const uint32_t* __restrict__ bins, SahTask* __restrict__ next, SahSmall* __restrict__ small,
                             SahCounters* __restrict__ ctr, SahLimits lim, int2* __restrict__ children,
                             int* __restrict__ node_parent, float4* __restrict__ node_lo, float4* __restrict__ node_hi) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= *count) return;
+    constexpr uint32_t kFull = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= *count) return;  // the whole warp leaves together
     SahTask task = tasks[t];
     const uint32_t* tb = bins + (size_t)t * kSahTaskWords;
-    // node box: the union of the axis-0 bins
-    uint32_t box[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-    for (int b = 0; b < kSahBins; ++b) {
-        const uint32_t* w = tb + b * kSahBinWords;
+    {
+        const uint32_t* w = tb + lane * kSahBinWords;
+        uint32_t box[6];
         for (int k = 0; k < 3; ++k) {
-            box[k] = min(box[k], w[k]);
-            box[3 + k] = max(box[3 + k], w[3 + k]);
+            box[k] = __reduce_min_sync(kFull, w[k]);
+            box[3 + k] = __reduce_max_sync(kFull, w[3 + k]);
+        }
+        if (lane == 0) {
+            node_lo[task.node] =
+                make_float4(ordered_to_float(box[0]), ordered_to_float(box[1]), ordered_to_float(box[2]), 0.f);
+            node_hi[task.node] =
+                make_float4(ordered_to_float(box[3]), ordered_to_float(box[4]), ordered_to_float(box[5]), 0.f);
         }
     }
-    node_lo[task.node] = make_float4(ordered_to_float(box[0]), ordered_to_float(box[1]), ordered_to_float(box[2]), 0.f);
-    node_hi[task.node] = make_float4(ordered_to_float(box[3]), ordered_to_float(box[4]), ordered_to_float(box[5]), 0.f);
     float best_cost = INFINITY;
     int best_axis = -1, best_bin = 0;
     for (int a = 0; a < 3; ++a) {
         const float ext = ordered_to_float(task.chi[a]) - ordered_to_float(task.clo[a]);
-        if (!(ext > 0.0f)) continue;
-        const uint32_t* ab = tb + a * kSahBins * kSahBinWords;
-        float right_area[kSahBins];
-        uint32_t right_n[kSahBins];
-        {
-            float rl[3] = {INFINITY, INFINITY, INFINITY}, rh[3] = {-INFINITY, -INFINITY, -INFINITY};
-            uint32_t rn = 0u;
-            for (int b = kSahBins - 1; b >= 1; --b) {
-                const uint32_t* w = ab + b * kSahBinWords;
-                if (w[12]) {
-                    for (int k = 0; k < 3; ++k) {
-                        rl[k] = fminf(rl[k], ordered_to_float(w[k]));
-                        rh[k] = fmaxf(rh[k], ordered_to_float(w[3 + k]));
-                    }
+        if (!(ext > 0.0f)) continue;  // uniform across the warp
+        const uint32_t* w = tb + (a * kSahBins + lane) * kSahBinWords;
+        // empty bins hold the identities (min fields all ones, max fields 0)
+        uint32_t pl[3] = {w[0], w[1], w[2]}, ph[3] = {w[3], w[4], w[5]}, pn = w[12];
+        uint32_t sl[3] = {w[0], w[1], w[2]}, sh[3] = {w[3], w[4], w[5]}, sn = w[12];
+        for (uint32_t d = 1; d < 32u; d <<= 1) {
+            uint32_t ul[3], uh[3], dl[3], dh[3];
+            for (int k = 0; k < 3; ++k) {
+                ul[k] = __shfl_up_sync(kFull, pl[k], d);
+                uh[k] = __shfl_up_sync(kFull, ph[k], d);
+                dl[k] = __shfl_down_sync(kFull, sl[k], d);
+                dh[k] = __shfl_down_sync(kFull, sh[k], d);
+            }
+            const uint32_t un = __shfl_up_sync(kFull, pn, d), dn = __shfl_down_sync(kFull, sn, d);
+            if (lane >= d) {
+                for (int k = 0; k < 3; ++k) {
+                    pl[k] = min(pl[k], ul[k]);
+                    ph[k] = max(ph[k], uh[k]);
                 }
-                rn += w[12];
-                right_area[b] = sah_half_area(rl[0], rl[1], rl[2], rh[0], rh[1], rh[2]);
-                right_n[b] = rn;
+                pn += un;
+            }
+            if (lane + d < 32u) {
+                for (int k = 0; k < 3; ++k) {
+                    sl[k] = min(sl[k], dl[k]);
+                    sh[k] = max(sh[k], dh[k]);
+                }
+                sn += dn;
             }
         }
-        float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
-        uint32_t ln = 0u;
-        for (int b = 0; b < kSahBins - 1; ++b) {
-            const uint32_t* w = ab + b * kSahBinWords;
-            if (w[12]) {
-                for (int k = 0; k < 3; ++k) {
-                    ll[k] = fminf(ll[k], ordered_to_float(w[k]));
-                    lh[k] = fmaxf(lh[k], ordered_to_float(w[3 + k]));
-                }
-            }
-            ln += w[12];
-            const uint32_t rn = right_n[b + 1];
-            if (ln == 0u || rn == 0u) continue;
-            const float c = sah_half_area(ll[0], ll[1], ll[2], lh[0], lh[1], lh[2]) * (float)ln +
-                            right_area[b + 1] * (float)rn;
-            if (c < best_cost) {
-                best_cost = c;
-                best_axis = a;
-                best_bin = b;
-            }
+        // split after bin `lane`: left = bins 0..lane (prefix), right = bins lane+1..31
+        uint32_t rl[3], rh[3];
+        for (int k = 0; k < 3; ++k) {
+            rl[k] = __shfl_down_sync(kFull, sl[k], 1);
+            rh[k] = __shfl_down_sync(kFull, sh[k], 1);
+        }
+        const uint32_t rn = __shfl_down_sync(kFull, sn, 1);
+        float cost = INFINITY;
+        if (lane < 31u && pn != 0u && rn != 0u) {
+            const float la = sah_half_area(ordered_to_float(pl[0]), ordered_to_float(pl[1]), ordered_to_float(pl[2]),
+                                           ordered_to_float(ph[0]), ordered_to_float(ph[1]), ordered_to_float(ph[2]));
+            const float ra = sah_half_area(ordered_to_float(rl[0]), ordered_to_float(rl[1]), ordered_to_float(rl[2]),
+                                           ordered_to_float(rh[0]), ordered_to_float(rh[1]), ordered_to_float(rh[2]));
+            cost = la * (float)pn + ra * (float)rn;
+        }
+        float m = cost;
+        for (int d = 16; d > 0; d >>= 1) m = fminf(m, __shfl_xor_sync(kFull, m, d));
+        if (m < best_cost) {  // strictly cheaper than the earlier axes' best
+            best_cost = m;
+            best_axis = a;
+            best_bin = __ffs(__ballot_sync(kFull, cost == m)) - 1;  // the first bin reaching it
         }
     }
     uint32_t left = task.count / 2u;
     uint32_t cb[2][6];  // children's centroid bounds
     if (best_axis >= 0) {
-        const uint32_t* ab = tb + best_axis * kSahBins * kSahBinWords;
-        for (int s = 0; s < 2; ++s)
-            for (int k = 0; k < 3; ++k) {
-                cb[s][k] = 0xffffffffu;
-                cb[s][3 + k] = 0u;
-            }
-        left = 0u;
-        for (int b = 0; b < kSahBins; ++b) {
-            const uint32_t* w = ab + b * kSahBinWords;
-            const int s = b <= best_bin ? 0 : 1;
-            if (s == 0) left += w[12];
-            for (int k = 0; k < 3; ++k) {
-                cb[s][k] = min(cb[s][k], w[6 + k]);
-                cb[s][3 + k] = max(cb[s][3 + k], w[9 + k]);
-            }
+        const uint32_t* w = tb + (best_axis * kSahBins + lane) * kSahBinWords;
+        const bool in_left = (int)lane <= best_bin;
+        left = __reduce_add_sync(kFull, in_left ? w[12] : 0u);
+        for (int k = 0; k < 3; ++k) {
+            cb[0][k] = __reduce_min_sync(kFull, in_left ? w[6 + k] : 0xffffffffu);
+            cb[0][3 + k] = __reduce_max_sync(kFull, in_left ? w[9 + k] : 0u);
+            cb[1][k] = __reduce_min_sync(kFull, in_left ? 0xffffffffu : w[6 + k]);
+            cb[1][3 + k] = __reduce_max_sync(kFull, in_left ? 0u : w[9 + k]);
         }
     } else {
         for (int s = 0; s < 2; ++s)
@@ -1071,6 +1083,7 @@ __global__ void k_sah_split(const uint32_t* __restrict__ count, SahTask* __restr
                 cb[s][3 + k] = task.chi[k];
             }
     }
+    if (lane != 0u) return;
     task.axis = best_axis;
     task.split_bin = (uint32_t)best_bin;
     task.left_count = left;
@@ -1416,8 +1429,8 @@ int build_binned(NanContext* ctx, uint32_t n, const float4* tris_sorted, const f
         const uint32_t words = large * (uint32_t)kSahTaskWords;
         k_sah_bins_reset<<<blocks(words), kThreads, 0, s>>>(words, bins);
         k_sah_bin<<<bin_grid, kThreads, 0, s>>>(n, ids_a, task_a, level_a, leaf_lo, leaf_hi, bins);
-        k_sah_split<<<blocks(large), kThreads, 0, s>>>(&ctr->level, level_a, bins, level_b, small, ctr, lim, children,
-                                                       node_parent, node_lo, node_hi);
+        k_sah_split<<<(large * 32u + 127u) / 128u, 128, 0, s>>>(&ctr->level, level_a, bins, level_b, small, ctr, lim,
+                                                                children, node_parent, node_lo, node_hi);
         k_sah_flags<<<blocks(n + 1), kThreads, 0, s>>>(n, ids_a, task_a, level_a, leaf_lo, leaf_hi, flags);
         cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, flags, rank, n + 1, s);
         k_sah_scatter<<<blocks(n), kThreads, 0, s>>>(n, ids_a, task_a, level_a, flags, rank, ids_b, task_b, children,
