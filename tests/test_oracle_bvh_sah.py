@@ -12,6 +12,7 @@ import pytest
 GPU_REPORTS = [
     ("bench_terrain_200k", None, 54.36327457155585),  # bench.py's texel workload
     ("cornell", 17, 11.965000253170729),
+    ("city_4m", None, 54.74312487383861),  # 4.16 M triangles, about 20 levels of large nodes
 ]
 
 
@@ -19,8 +20,12 @@ def _world(which):
     from nan_b200 import scenes
     from oracle.oracle import OracleScene
 
-    node = (scenes.terrain_boxes(seed=1, grid=313, boxes=500) if which == "bench_terrain_200k"
-            else scenes.cornell_box(64, 64))
+    if which == "bench_terrain_200k":
+        node = scenes.terrain_boxes(seed=1, grid=313, boxes=500)
+    elif which == "city_4m":
+        node = scenes.city()
+    else:
+        node = scenes.cornell_box(64, 64)
     return OracleScene(**node.pack()).world_triangles()
 
 
